@@ -1,0 +1,130 @@
+/* jaxrans_b200: the pseudo-transient Newton-Krylov hot path of JAX-RANS on NVIDIA B200.
+ *
+ * A C ABI (plain pointers and sizes) over hand-written sm_100a CUDA kernels.  A plan is
+ * one case (one canvas: the grid's blocks and their ghost rings) with every static table
+ * the kernels read, the device work buffers and the solver state.  Fields are
+ * variable-major (nvar, NI*NJ) FP64 arrays, nvar = 4 (Euler, laminar) or 5 (SA).
+ *
+ * Every function returns 0 on success or a JR_E* code; jr_last_error() gives a message.
+ * Functions taking device pointers run on the plan's stream and do not synchronise it
+ * unless stated; functions taking host pointers copy in/out and synchronise.
+ *
+ * The reference (giovannicatalani/jax-rans, src/jaxrans) has no FFI: each entry point
+ * below replaces a Python/JAX function, cited beside it, that a binding would call.
+ */
+#ifndef JAXRANS_B200_H
+#define JAXRANS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define JR_OK 0
+#define JR_EINVAL 1      /* a bad argument */
+#define JR_ENOMEM 2      /* a device allocation failed */
+#define JR_ECUDA 3       /* a CUDA error (message in jr_last_error) */
+#define JR_EMISMATCH 4   /* buffers that do not fit the plan */
+
+typedef struct jr_plan jr_plan;
+
+/* Everything a plan is built from (host memory; copied by jr_plan_create). */
+typedef struct jr_plan_desc {
+  int32_t NI, NJ, nvar;
+  const uint8_t* interior;      /* NI*NJ */
+  const double* volume;         /* NI*NJ */
+  const double* faces_i;        /* 2 x (NI+1) x NJ: sx plane, sy plane */
+  const double* faces_j;        /* 2 x NI x (NJ+1) */
+  const double* centres;        /* 2 x (NI+2) x (NJ+2): cell centres with one reflected ghost ring */
+  const double* distance;       /* NI*NJ wall distance (SA), or NULL */
+  const int32_t* neighbours;    /* NI*NJ */
+  int32_t n_ghost[2];           /* two gather stages */
+  const int32_t* ghost[2];
+  const int32_t* source[2];
+  const int32_t* kind[2];       /* 0 copy, 1 slip wall, 2 no-slip wall, 3 symmetry, 4 far field, 5 inflow, 6 outflow */
+  const double* geom[2];        /* 4 per record: nx, ny, mx, my */
+  int32_t n_walls;
+  const int32_t* wall_cell;
+  const int32_t* wall_family;
+  const int32_t* wall_face;
+  const double* wall_into;
+  const double* wall_mid;       /* 2 per wall face */
+  int32_t n_chains, chain_L;
+  const int32_t* chain_cells;   /* [k * n_chains + c], -1 past the end */
+  const int32_t* chain_len;
+  const int32_t* chain_up_face;
+  const int32_t* chain_up_sign;
+  const int32_t* chain_down_face;
+  const int32_t* chain_down_sign;
+  /* physics */
+  double gamma, mu_inf, sutherland, c_cr1, kappa;   /* mu_inf 0: inviscid; sutherland < 0: constant viscosity */
+  int32_t flux, limiter, far_field;                  /* flux 0 hllc 1 roe; limiter 0 none 1 minmod 2 van_albada
+                                                        3 van_albada_smooth 4 kappa; far field 0 uniform 1 point vortex */
+  double q_inf[5];
+  double quarter_chord[2];
+  /* implicit solver */
+  double cfl, cfl_max, cfl_growth, cfl_cutback, cfl_min;
+  double krylov_tol, krylov_success, max_relative_update;   /* max_relative_update <= 0: none */
+  int32_t krylov_subspace, krylov_restarts, preconditioner; /* preconditioner 0 none, 1 line_j */
+  int32_t precision;                                        /* 0 fp64, 1 mixed (fp32 line factor and Krylov basis) */
+  double force_length, moment_centre[2];
+} jr_plan_desc;
+
+/* Build a plan (device copies of every table, work buffers, a stream). */
+int jr_plan_create(const jr_plan_desc* desc, jr_plan** out);
+int jr_plan_destroy(jr_plan* plan);
+const char* jr_last_error(void);
+/* Number of canvas cells NI*NJ and of face entries (NI+1)*NJ + NI*(NJ+1). */
+int jr_plan_sizes(const jr_plan* plan, int64_t* n_canvas, int64_t* n_faces);
+/* The plan's CUDA stream (a cudaStream_t), for callers that order their own work on it. */
+void* jr_plan_stream(jr_plan* plan);
+int jr_synchronize(jr_plan* plan);
+
+/* R(U): the residual on the canvas, where(interior, net flux, U - U_inf); second order,
+ * or first order when first_order != 0.  Replaces make_residual(...).residual
+ * (src/jaxrans/numerics/residual.py:273-334, residual() at :324-327).  Device pointers. */
+int jr_residual(jr_plan* plan, const double* U, double* R, int first_order);
+
+/* dR1/dU . v: the exact tangent of the first-order residual at U (forward-mode duals).
+ * Replaces jax.linearize(jacobian_source.residual, U)'s jvp
+ * (src/jaxrans/solvers/implicit.py:104-108).  Device pointers. */
+int jr_jvp(jr_plan* plan, const double* U, const double* v, double* Jv);
+
+/* lambda on every canvas face, i-faces then j-faces (length n_faces).  Replaces
+ * ResidualOperator.wave_speeds / face_wave_speeds (src/jaxrans/numerics/residual.py:169-192). */
+int jr_wave_speeds(jr_plan* plan, const double* U, double* lam);
+
+/* Factor the line_j preconditioner at (U, cfl) and apply it: z = M^-1 r.  Replaces
+ * get_preconditioner("line_j")(...)(U, lambdas, cfl) and its solve
+ * (src/jaxrans/solvers/preconditioners.py:291-306).  Device pointers. */
+int jr_precond_factor(jr_plan* plan, const double* U, double cfl);
+int jr_precond_apply(jr_plan* plan, const double* r, double* z);
+
+/* The solver state: U (device or host copy in/out), CFL and the previous |R|.
+ * Replaces ImplicitState (src/jaxrans/solvers/implicit.py:35-51). */
+int jr_state_set(jr_plan* plan, const double* U_host, double cfl, double residual_norm);
+int jr_state_get(jr_plan* plan, double* U_host, double* cfl, double* residual_norm, int32_t* status);
+/* Device pointer to the plan's own state U (nvar x NI*NJ), valid until jr_plan_destroy. */
+double* jr_state_device(jr_plan* plan);
+
+/* n_steps pseudo-transient Newton steps on the plan's state, one captured CUDA graph per
+ * step; history (host, n_steps) receives |R| before each step.  Synchronises once.
+ * Replaces make_newton_step (src/jaxrans/solvers/implicit.py:84-168) run as the
+ * driver's block (src/jaxrans/solvers/driver.py:87-104). */
+int jr_newton_steps(jr_plan* plan, int32_t n_steps, double* history);
+
+/* The same step count without synchronising: history_device (n_steps doubles on the
+ * device) receives the norms.  For timing with events on the plan's stream. */
+int jr_newton_steps_async(jr_plan* plan, int32_t n_steps, double* history_device);
+
+/* Force coefficients at the plan's state (or at U if not NULL, a device pointer):
+ * out (host) = cl, cd, cm, cd_friction, fx, fy.  Replaces force_coefficients
+ * (src/jaxrans/post/forces.py:108-161).  Synchronises. */
+int jr_forces(jr_plan* plan, const double* U, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JAXRANS_B200_H */

@@ -1,0 +1,92 @@
+// Device-side views of a case plan and the per-case solver scalars, and the launch
+// wrappers every translation unit shares.  A "canvas" is one case's grid with its
+// ghost ring: NI x NJ cells, j contiguous; fields are variable-major (nvar, NI*NJ) FP64.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "physics.cuh"
+
+namespace jr {
+
+constexpr int MAX_KRYLOV = 64;   // largest GMRES subspace
+constexpr int TILE_I = 15;       // residual tile: 15 x 16 cells, 256 threads
+constexpr int TILE_J = 16;
+constexpr int TILE_THREADS = 256;
+constexpr int GHOST_THREADS = 512;
+
+// Ghost-record kinds (the order the host plan uses)
+enum GhostKind { G_COPY = 0, G_SLIP = 1, G_NOSLIP = 2, G_SYMMETRY = 3, G_FARFIELD = 4, G_INFLOW = 5, G_OUTFLOW = 6 };
+
+// Status bits of a case (device-side status word)
+enum Status : int {
+  ST_OK = 0,
+  ST_NONFINITE = 1,       // a non-finite value met in a reduction
+  ST_REJECTED = 2,        // the last Newton step was rejected
+  ST_GMRES_BREAKDOWN = 4, // an Arnoldi vector of zero norm
+};
+
+struct Canvas {
+  int NI, NJ, nvar;
+  int n_cells;                 // interior cells
+  const uint8_t* interior;     // NI*NJ
+  const double* volume;        // NI*NJ
+  const double* fi;            // i-faces: sx plane then sy plane, each (NI+1)*NJ
+  const double* fj;            // j-faces: sx plane then sy plane, each NI*(NJ+1)
+  const double* centres;       // x plane then y plane, each (NI+2)*(NJ+2): one ring beyond the canvas
+  const double* distance;      // NI*NJ (SA) or null
+  const int* neighbours;       // NI*NJ: the partner across a block face, or the cell itself
+  int n_ghost[2];
+  const int* g_ghost[2];
+  const int* g_source[2];
+  const int* g_kind[2];
+  const double* g_geom[2];     // 4 per record: nx, ny, mx, my
+  int n_walls;
+  const int* w_cell;
+  const int* w_family;
+  const int* w_face;
+  const double* w_into;        // +1 where the canvas face vector points into the fluid
+  const double* w_mid;         // 2 per wall face
+  double volume_sum;           // over interior cells
+  // line chains, one thread per chain: cells [n_chains * L] chain-major-by-row
+  int n_chains, L;
+  const int* ch_cells;         // [k * n_chains + c], -1 past a chain's end
+  const int* ch_len;           // [c]
+  const int* ch_up_face;       // flat face index (i-faces first, then j-faces)
+  const int* ch_up_sign;
+  const int* ch_down_face;
+  const int* ch_down_sign;
+  int n_offchain;              // canvas cells on no chain
+  const int* offchain;
+
+  __device__ __forceinline__ int nfi() const { return (NI + 1) * NJ; }
+  __device__ __forceinline__ int nfj() const { return NI * (NJ + 1); }
+  __device__ __forceinline__ int ncanvas() const { return NI * NJ; }
+};
+
+// Per-case solver scalars, resident on the device across a whole block of steps.
+struct Scalars {
+  double cfl, res_prev, norm, bnorm, rnorm, beta;
+  double omega, lin_red, rnorm_sq_partial;
+  double nrm, inv_nrm, worst;
+  double H[(MAX_KRYLOV + 1) * MAX_KRYLOV];   // column-major: H[i + (m+1) j]
+  double h1[MAX_KRYLOV + 1], h2[MAX_KRYLOV + 1];
+  double y[MAX_KRYLOV], hy[MAX_KRYLOV + 1];
+  int active, cycle, accept, status;
+  int steps, rejected, hpos;
+};
+
+struct Config {
+  double cfl_max, cfl_growth, cfl_cutback, cfl_min;
+  double krylov_tol, krylov_success, max_relative_update;  // < 0: none
+  int restart, maxiter, preconditioner;                    // preconditioner: 0 none, 1 line_j
+};
+
+// Reduction scratch: partial sums per block, a ticket for the last-block reduction.
+struct Reduce {
+  double* partial;     // [blocks * width]
+  unsigned int* ticket;
+  int blocks;
+};
+
+}  // namespace jr

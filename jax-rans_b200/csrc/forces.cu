@@ -1,0 +1,141 @@
+// Wall loads and force coefficients in FP64 (src/jaxrans/post/forces.py:48-161): gauge
+// pressure from the cell on each wall face, the laminar viscous shear of the same
+// diamond-gradient viscous flux the residual uses, lift normal and drag along the
+// freestream, the pressure moment about the moment centre.  One CTA reduces all wall
+// faces in a fixed order.
+#include "device.cuh"
+
+namespace jr {
+
+__device__ __forceinline__ double q_at(const Canvas& c, const Physics& P, const double* U, const double* qg, int idx,
+                                       int v) {
+  const int N = c.ncanvas();
+  if (c.interior[idx]) {
+    double u[5], q[5];
+    for (int k = 0; k < 4; ++k) u[k] = U[k * N + idx];
+    to_prim(u, q, 4, P.gamma);
+    return q[v];
+  }
+  return qg[v * N + idx];
+}
+
+// laminar F_v . S at the wall face (family a) below canvas cell (i, j) or above it
+__device__ void wall_viscous(const Canvas& c, const Physics& P, const double* U, const double* qg, int family, int face,
+                             double sx, double sy, double& fx, double& fy) {
+  const int NJ = c.NJ;
+  int ai, aj, bi, bj;
+  if (family == 0) {
+    int i = face / NJ, j = face % NJ;
+    ai = i - 1; aj = j; bi = i; bj = j;
+  } else {
+    int i = face / (NJ + 1), j = face % (NJ + 1);
+    ai = i; aj = j - 1; bi = i; bj = j;
+  }
+  const double g = P.gamma;
+  auto phi = [&](int i, int j, int k) {
+    int idx = i * NJ + j;
+    if (k < 2) return q_at(c, P, U, qg, idx, 1 + k);
+    return g * q_at(c, P, U, qg, idx, 3) / q_at(c, P, U, qg, idx, 0);
+  };
+  const int CJ = NJ + 2, CN = (c.NI + 2) * CJ;
+  auto cx = [&](int i, int j) { return c.centres[(i + 1) * CJ + j + 1]; };
+  auto cy = [&](int i, int j) { return c.centres[CN + (i + 1) * CJ + j + 1]; };
+  int n0[4][2], n1[4][2];
+  if (family == 0) {
+    int n0_[4][2] = {{ai, aj - 1}, {ai + 1, aj - 1}, {ai, aj}, {ai + 1, aj}};
+    int n1_[4][2] = {{ai, aj}, {ai + 1, aj}, {ai, aj + 1}, {ai + 1, aj + 1}};
+    for (int k = 0; k < 4; ++k) for (int t = 0; t < 2; ++t) { n0[k][t] = n0_[k][t]; n1[k][t] = n1_[k][t]; }
+  } else {
+    int n0_[4][2] = {{ai - 1, aj}, {ai, aj}, {ai - 1, aj + 1}, {ai, aj + 1}};
+    int n1_[4][2] = {{ai, aj}, {ai + 1, aj}, {ai, aj + 1}, {ai + 1, aj + 1}};
+    for (int k = 0; k < 4; ++k) for (int t = 0; t < 2; ++t) { n0[k][t] = n0_[k][t]; n1[k][t] = n1_[k][t]; }
+  }
+  auto corner = [&](int (*n)[2], auto f) { return 0.25 * (((f(n[0][0], n[0][1]) + f(n[1][0], n[1][1])) + f(n[2][0], n[2][1])) + f(n[3][0], n[3][1])); };
+  double d1x = cx(bi, bj) - cx(ai, aj), d1y = cy(bi, bj) - cy(ai, aj);
+  double d2x = corner(n1, cx) - corner(n0, cx), d2y = corner(n1, cy) - corner(n0, cy);
+  double det = d1x * d2y - d2x * d1y;
+  double gx[3], gy[3];
+  for (int k = 0; k < 3; ++k) {
+    auto pk = [&](int i, int j) { return phi(i, j, k); };
+    double dpc = phi(bi, bj, k) - phi(ai, aj, k);
+    double dpn = corner(n1, pk) - corner(n0, pk);
+    gx[k] = (dpc * d2y - dpn * d1y) / det;
+    gy[k] = (d1x * dpn - d2x * dpc) / det;
+  }
+  double Tf = 0.5 * (phi(ai, aj, 2) + phi(bi, bj, 2));
+  double mu = viscosity(P, Tf);
+  double g00 = gx[0], g01 = gy[0], g10 = gx[1], g11 = gy[1];
+  double div = g00 + g11, ttd = (2.0 / 3.0) * div;
+  double t00 = mu * (2.0 * g00 - ttd), t11 = mu * (2.0 * g11 - ttd), t01 = mu * (g01 + g10);
+  fx = t00 * sx + t01 * sy;
+  fy = t01 * sx + t11 * sy;
+}
+
+// out: cl, cd, cm, cd_friction, fx, fy
+__global__ void k_forces(Canvas c, Physics P, const double* U, const double* qg, double length, double cx0,
+                         double cy0, double* out) {
+  __shared__ double red[6][32];
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  const double rho = P.q_inf[0], u = P.q_inf[1], v = P.q_inf[2];
+  const double speed = hypot(u, v);
+  const double dx = u / speed, dy = v / speed;   // drag direction
+  const double lx = -dy, ly = dx;                  // lift direction
+  const double q_area = 0.5 * rho * speed * speed * length;
+  for (int w = threadIdx.x; w < c.n_walls; w += blockDim.x) {
+    int cell = c.w_cell[w], fam = c.w_family[w], f = c.w_face[w];
+    double into = c.w_into[w];
+    double sx, sy;
+    if (fam == 0) {
+      sx = c.fi[f];
+      sy = c.fi[c.nfi() + f];
+    } else {
+      sx = c.fj[f];
+      sy = c.fj[c.nfj() + f];
+    }
+    double Sx = into * sx, Sy = into * sy;
+    double p = q_at(c, P, U, qg, cell, 3) - 1.0 / P.gamma;
+    double px = -p * Sx, py = -p * Sy;
+    double shx = 0.0, shy = 0.0;
+    if (P.mu_inf > 0.0) {
+      double fx, fy;
+      wall_viscous(c, P, U, qg, fam, f, sx, sy, fx, fy);
+      shx = into * fx;
+      shy = into * fy;
+    }
+    double Lx = px + shx, Ly = py + shy;
+    double rx = c.w_mid[2 * w] - cx0, ry = c.w_mid[2 * w + 1] - cy0;
+    double moment = ry * px - rx * py;
+    acc[0] += (lx * Lx + ly * Ly) / q_area;
+    acc[1] += (dx * Lx + dy * Ly) / q_area;
+    acc[2] += (moment / length) / q_area;
+    acc[3] += dx * shx + dy * shy;
+    acc[4] += Lx;
+    acc[5] += Ly;
+  }
+  for (int k = 0; k < 6; ++k) {
+    double x = acc[k];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t[6];
+    for (int k = 0; k < 6; ++k) {
+      t[k] = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t[k] += red[k][w];
+    }
+    out[0] = t[0];
+    out[1] = t[1];
+    out[2] = t[2];
+    out[3] = t[3] / q_area;
+    out[4] = t[4];
+    out[5] = t[5];
+  }
+}
+
+void launch_forces(const Canvas& c, const Physics& P, const double* U, const double* qg, double length, double cx0,
+                   double cy0, double* out, cudaStream_t st) {
+  k_forces<<<1, 1024, 0, st>>>(c, P, U, qg, length, cx0, cy0, out);
+}
+
+}  // namespace jr

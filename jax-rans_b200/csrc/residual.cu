@@ -1,0 +1,750 @@
+// The residual R(U) of one canvas and the exact first-order J.v, in one tile kernel.
+//
+// Follows src/jaxrans/numerics/residual.py:54-334 (block_residual, the ghost fill, the
+// edge pad that interior cells never reach), with the SA row of turbulence.py:112-151
+// and the viscous flux of residual.py:94-124.  Each CTA owns a 15 x 16 tile of canvas
+// cells: it stages the primitive state of the tile plus a 2-cell halo in shared memory
+// (prim(U) computed on the fly for block cells, ghost cells read from the ghost-filled
+// buffer), computes every face flux of the tile once into shared memory, then sums the
+// faces of each cell -- a per-cell reduction with no atomics.  The same source gives
+// R(U) (T = double) and dR1/dU . v (T = Dual, first-order faces).
+#include "device.cuh"
+
+namespace jr {
+
+__device__ __forceinline__ bool interior_at(const Canvas& c, int i, int j) {
+  return i >= 0 && i < c.NI && j >= 0 && j < c.NJ && c.interior[i * c.NJ + j];
+}
+
+template <class T> struct Tangent;
+template <> struct Tangent<double> {
+  __device__ static double make(double v, const double*, int) { return v; }
+};
+template <> struct Tangent<Dual> {
+  __device__ static Dual make(double v, const double* dv, int k) { return Dual{v, dv[k]}; }
+};
+
+// primitive state of canvas cell `idx`: prim(U) on block cells, the ghost buffer elsewhere
+template <class T>
+__device__ __forceinline__ void load_prim(const Canvas& c, const Physics& P, int idx, const double* U,
+                                          const double* V, const double* qg, const double* dqg, T* q) {
+  const int N = c.ncanvas();
+  if (c.interior[idx]) {
+    T u[5];
+    for (int v = 0; v < c.nvar; ++v) {
+      double x = U[v * N + idx];
+      if constexpr (sizeof(T) == sizeof(Dual)) {
+        u[v] = T{x, V[v * N + idx]};
+      } else {
+        u[v] = x;
+      }
+    }
+    to_prim(u, q, c.nvar, P.gamma);
+  } else {
+    for (int v = 0; v < c.nvar; ++v) {
+      double x = qg[v * N + idx];
+      if constexpr (sizeof(T) == sizeof(Dual)) {
+        q[v] = T{x, dqg[v * N + idx]};
+      } else {
+        q[v] = x;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Ghost fill (src/jaxrans/numerics/boundary.py:257-267 and the stages of
+// src/jaxrans/mesh/atlas.py:331-367): one CTA per case; stage 1 (j sides), then
+// stage 2 (i sides and corners, which read stage-1 ghosts).  T = Dual fills the
+// tangent of the ghosts (dqg) for a J.v; the base ghosts are left as they are.
+// ------------------------------------------------------------------------------------
+
+template <class T>
+__device__ void point_vortex_state(const Physics& P, double dx, double dy, T circ, T* out) {
+  const double g = P.gamma;
+  double rho_f = P.q_inf[0], u_f = P.q_inf[1], v_f = P.q_inf[2], p_f = P.q_inf[3];
+  double a2 = g * p_f / rho_f;
+  double speed2 = u_f * u_f + v_f * v_f;
+  double mach2 = speed2 / a2;
+  double alpha = atan2(v_f, u_f);
+  double r = hypot(dx, dy);
+  double theta = atan2(dy, dx);
+  double st = sin(theta - alpha);
+  T strength = circ * sqrt(1.0 - mach2) / (2.0 * 3.141592653589793 * r * (1.0 - mach2 * (st * st)));
+  T u = u_f + strength * sin(theta);
+  T v = v_f - strength * cos(theta);
+  T ratio = 1.0 + 0.5 * (g - 1.0) * (speed2 - u * u - v * v) / a2;
+  out[0] = rho_f * dpow(ratio, 1.0 / (g - 1.0));
+  out[1] = u;
+  out[2] = v;
+  out[3] = p_f * dpow(ratio, g / (g - 1.0));
+  out[4] = cst<T>(P.q_inf[4]);
+}
+
+template <class T>
+__device__ void condition(const Physics& P, int kind, const T* q, const double* geom, T circ, T* out) {
+  const int nv = P.nvar;
+  const double nx = geom[0], ny = geom[1];
+  const double g = P.gamma;
+  switch (kind) {
+    case G_SLIP:
+    case G_SYMMETRY: {
+      T vn = q[1] * nx + q[2] * ny;
+      out[0] = q[0];
+      out[1] = q[1] - 2.0 * vn * nx;
+      out[2] = q[2] - 2.0 * vn * ny;
+      out[3] = q[3];
+      if (nv > 4) out[4] = kind == G_SLIP ? -q[4] : q[4];
+      return;
+    }
+    case G_NOSLIP:
+      out[0] = q[0];
+      out[1] = -q[1];
+      out[2] = -q[2];
+      out[3] = q[3];
+      if (nv > 4) out[4] = -q[4];
+      return;
+    case G_FARFIELD: {
+      T ref[5];
+      if (P.far_field == 1) {
+        point_vortex_state(P, geom[2] - P.quarter_chord[0], geom[3] - P.quarter_chord[1], circ, ref);
+      } else {
+        for (int v = 0; v < 5; ++v) ref[v] = cst<T>(P.q_inf[v]);
+      }
+      characteristic(q, nx, ny, ref, nv, g, out);
+      return;
+    }
+    case G_INFLOW: {
+      double g1 = g - 1.0;
+      double t_f = g * P.q_inf[3] / P.q_inf[0];
+      double speed_f = hypot(P.q_inf[1], P.q_inf[2]);
+      double t_total = t_f + 0.5 * g1 * speed_f * speed_f;
+      double p_total = P.q_inf[3] * pow(t_total / t_f, g / g1);
+      T pb = q[3];
+      T mach2 = dmax(2.0 / g1 * (dpow(p_total / pb, g1 / g) - 1.0), 0.0);
+      T tb = t_total / (1.0 + 0.5 * g1 * mach2);
+      T speed = dsqrt(mach2 * tb);
+      out[0] = g * pb / tb;
+      out[1] = speed * P.q_inf[1] / speed_f;
+      out[2] = speed * P.q_inf[2] / speed_f;
+      out[3] = pb;
+      if (nv > 4) out[4] = cst<T>(P.q_inf[4]);
+      return;
+    }
+    case G_OUTFLOW:
+      for (int v = 0; v < nv; ++v) out[v] = q[v];
+      out[3] = cst<T>(P.q_inf[3]);
+      return;
+    default:
+      for (int v = 0; v < nv; ++v) out[v] = q[v];
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(GHOST_THREADS) k_ghosts(Canvas c, Physics P, const double* U, const double* V,
+                                                          double* qg, double* dqg, const int* active) {
+  if (active != nullptr && *active == 0) return;
+  const int N = c.ncanvas();
+  __shared__ double red_v[GHOST_THREADS / 32][2], red_d[GHOST_THREADS / 32][2];
+  __shared__ T circ_s;
+  T circ = cst<T>(0.0);
+  if (P.far_field == 1) {
+    // Kutta-Joukowski circulation of the wall pressure lift (boundary.py:227-240)
+    T fx = cst<T>(0.0), fy = cst<T>(0.0);
+    for (int w = threadIdx.x; w < c.n_walls; w += blockDim.x) {
+      int cell = c.w_cell[w];
+      T q[5];
+      load_prim<T>(c, P, cell, U, V, qg, dqg, q);
+      T p = q[3] - P.q_inf[3];
+      int f = c.w_face[w];
+      double sx, sy;
+      if (c.w_family[w] == 0) {
+        sx = c.fi[f];
+        sy = c.fi[c.nfi() + f];
+      } else {
+        sx = c.fj[f];
+        sy = c.fj[c.nfj() + f];
+      }
+      double into = c.w_into[w];
+      fx = fx + p * (into * sx);
+      fy = fy + p * (into * sy);
+    }
+    // block reduction in a fixed order
+    double vals[4] = {val(fx), val(fy), 0.0, 0.0};
+    if constexpr (sizeof(T) == sizeof(Dual)) {
+      vals[2] = fx.d;
+      vals[3] = fy.d;
+    }
+    for (int o = 16; o > 0; o >>= 1)
+      for (int k = 0; k < 4; ++k) vals[k] += __shfl_down_sync(0xffffffffu, vals[k], o);
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+      red_v[warp][0] = vals[0];
+      red_v[warp][1] = vals[1];
+      red_d[warp][0] = vals[2];
+      red_d[warp][1] = vals[3];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s[4] = {0, 0, 0, 0};
+      for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+        s[0] += red_v[k][0];
+        s[1] += red_v[k][1];
+        s[2] += red_d[k][0];
+        s[3] += red_d[k][1];
+      }
+      T Fx, Fy;
+      if constexpr (sizeof(T) == sizeof(Dual)) {
+        Fx = T{-s[0], -s[2]};
+        Fy = T{-s[1], -s[3]};
+      } else {
+        Fx = -s[0];
+        Fy = -s[1];
+      }
+      double u_f = P.q_inf[1], v_f = P.q_inf[2];
+      double speed = hypot(u_f, v_f);
+      circ_s = (Fy * u_f - Fx * v_f) / speed / (P.q_inf[0] * speed);
+    }
+    __syncthreads();
+    circ = circ_s;
+  }
+  for (int s = 0; s < 2; ++s) {
+    const int n = c.n_ghost[s];
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+      int src = c.g_source[s][r], ghost = c.g_ghost[s][r], kind = c.g_kind[s][r];
+      T q[5], out[5];
+      load_prim<T>(c, P, src, U, V, qg, dqg, q);
+      if (kind == G_COPY) {
+        for (int v = 0; v < c.nvar; ++v) out[v] = q[v];
+      } else {
+        condition<T>(P, kind, q, c.g_geom[s] + 4 * r, circ, out);
+      }
+      for (int v = 0; v < c.nvar; ++v) {
+        if constexpr (sizeof(T) == sizeof(Dual)) {
+          dqg[v * N + ghost] = out[v].d;
+        } else {
+          qg[v * N + ghost] = out[v];
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// The tile kernel
+// ------------------------------------------------------------------------------------
+
+constexpr int HI = TILE_I + 4, HJ = TILE_J + 4;
+constexpr double PR_LAM = 0.72, PR_TURB = 0.9;
+
+template <class T, int NV> struct TileSmem {
+  T q[NV][HI][HJ];
+  double cx[TILE_I + 2][TILE_J + 2], cy[TILE_I + 2][TILE_J + 2];
+  double Fi[NV][TILE_I + 1][TILE_J];
+  double Fj[NV][TILE_I][TILE_J + 1];
+  double red[TILE_THREADS / 32];
+};
+
+// Flux through one face of the tile: inviscid (MUSCL or first-order faces), minus the
+// viscous flux, plus the SA convection-diffusion flux.  The face lies between the tile
+// cells A (lower) and B (upper) along `axis`; (ai, aj) is A's position in the staged
+// tile (halo included).  Returns the total flux in F[0..nvar).
+template <class T, int NV, bool SECOND, int VISC>
+__device__ __forceinline__ void face_flux(const Physics& P, TileSmem<T, NV>& s, int axis, int ai, int aj,
+                                          double sx, double sy, T* F) {
+  const double g = P.gamma;
+  const int di = axis == 0 ? 1 : 0, dj = axis == 0 ? 0 : 1;
+  T qL[4], qR[4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    T qm = s.q[v][ai][aj], qp = s.q[v][ai + di][aj + dj];
+    if constexpr (SECOND) {
+      T qmm = s.q[v][ai - di][aj - dj], qpp = s.q[v][ai + 2 * di][aj + 2 * dj];
+      T dm = qm - qmm, d0 = qp - qm, dp = qpp - qp;
+      if (P.limiter == 4) {
+        double lo = 0.25 * (1.0 - P.kappa), hi = 0.25 * (1.0 + P.kappa);
+        qL[v] = qm + lo * dm + hi * d0;
+        qR[v] = qp - lo * dp - hi * d0;
+      } else {
+        qL[v] = qm + 0.5 * limit(dm, d0, P.limiter);
+        qR[v] = qp - 0.5 * limit(d0, dp, P.limiter);
+      }
+    } else {
+      qL[v] = qm;
+      qR[v] = qp;
+    }
+  }
+  T Finv[4];
+  riemann(P.flux, qL, qR, sx, sy, g, Finv);
+#pragma unroll
+  for (int v = 0; v < 4; ++v) F[v] = Finv[v];
+  if constexpr (VISC > 0) {
+    // cells either side and the two nodes of the face (node = mean of 4 cells)
+    const T* qa[NV];
+    // phi = (u, v, T[, nu_hat]) at A and B
+    auto phi = [&](int i, int j, int k) -> T {
+      if (k < 2) return s.q[1 + k][i][j];
+      if (k == 2) return g * s.q[3][i][j] / s.q[0][i][j];
+      return s.q[4][i][j];
+    };
+    (void)qa;
+    const int bi = ai + di, bj = aj + dj;
+    // node corners in staged-tile coordinates: n0 and n1 (the face's two ends)
+    int n0i[4], n0j[4], n1i[4], n1j[4];
+    if (axis == 0) {
+      // i-face between (ai, aj) and (ai+1, aj): nodes at (i, j) and (i, j+1)
+      n0i[0] = ai; n0j[0] = aj - 1; n0i[1] = ai + 1; n0j[1] = aj - 1;
+      n0i[2] = ai; n0j[2] = aj;     n0i[3] = ai + 1; n0j[3] = aj;
+      n1i[0] = ai; n1j[0] = aj;     n1i[1] = ai + 1; n1j[1] = aj;
+      n1i[2] = ai; n1j[2] = aj + 1; n1i[3] = ai + 1; n1j[3] = aj + 1;
+    } else {
+      // j-face between (ai, aj) and (ai, aj+1): nodes at (i, j) and (i+1, j)
+      n0i[0] = ai - 1; n0j[0] = aj; n0i[1] = ai;     n0j[1] = aj;
+      n0i[2] = ai - 1; n0j[2] = aj + 1; n0i[3] = ai; n0j[3] = aj + 1;
+      n1i[0] = ai;     n1j[0] = aj; n1i[1] = ai + 1; n1j[1] = aj;
+      n1i[2] = ai;     n1j[2] = aj + 1; n1i[3] = ai + 1; n1j[3] = aj + 1;
+    }
+    // centres: staged with a 1-cell halo, offset 1 from the q tile's 2-cell halo
+    auto cxv = [&](int i, int j) { return s.cx[i - 1][j - 1]; };
+    auto cyv = [&](int i, int j) { return s.cy[i - 1][j - 1]; };
+    double d1x = cxv(bi, bj) - cxv(ai, aj), d1y = cyv(bi, bj) - cyv(ai, aj);
+    double xn0 = 0.25 * (((cxv(n0i[0], n0j[0]) + cxv(n0i[1], n0j[1])) + cxv(n0i[2], n0j[2])) + cxv(n0i[3], n0j[3]));
+    double yn0 = 0.25 * (((cyv(n0i[0], n0j[0]) + cyv(n0i[1], n0j[1])) + cyv(n0i[2], n0j[2])) + cyv(n0i[3], n0j[3]));
+    double xn1 = 0.25 * (((cxv(n1i[0], n1j[0]) + cxv(n1i[1], n1j[1])) + cxv(n1i[2], n1j[2])) + cxv(n1i[3], n1j[3]));
+    double yn1 = 0.25 * (((cyv(n1i[0], n1j[0]) + cyv(n1i[1], n1j[1])) + cyv(n1i[2], n1j[2])) + cyv(n1i[3], n1j[3]));
+    double d2x = xn1 - xn0, d2y = yn1 - yn0;
+    double det = d1x * d2y - d2x * d1y;
+    constexpr int NPHI = VISC == 2 ? 4 : 3;
+    T gx[NPHI], gy[NPHI];
+#pragma unroll
+    for (int k = 0; k < NPHI; ++k) {
+      T dpc = phi(bi, bj, k) - phi(ai, aj, k);
+      T p0 = 0.25 * (((phi(n0i[0], n0j[0], k) + phi(n0i[1], n0j[1], k)) + phi(n0i[2], n0j[2], k)) + phi(n0i[3], n0j[3], k));
+      T p1 = 0.25 * (((phi(n1i[0], n1j[0], k) + phi(n1i[1], n1j[1], k)) + phi(n1i[2], n1j[2], k)) + phi(n1i[3], n1j[3], k));
+      T dpn = p1 - p0;
+      gx[k] = (dpc * d2y - dpn * d1y) / det;
+      gy[k] = (d1x * dpn - d2x * dpc) / det;
+    }
+    // face velocity and temperature: two-cell means
+    T vel0 = 0.5 * (s.q[1][ai][aj] + s.q[1][bi][bj]);
+    T vel1 = 0.5 * (s.q[2][ai][aj] + s.q[2][bi][bj]);
+    T Tf = 0.5 * (phi(ai, aj, 2) + phi(bi, bj, 2));
+    T mu = viscosity(P, Tf);
+    T k = mu / (PR_LAM * (g - 1.0));
+    // gv[comp][dir]
+    T g00 = gx[0], g01 = gy[0], g10 = gx[1], g11 = gy[1];
+    T mut = cst<T>(0.0);
+    T ex00 = cst<T>(0.0), ex01 = cst<T>(0.0), ex10 = cst<T>(0.0), ex11 = cst<T>(0.0);
+    bool extra = false;
+    T rho_f, nuh_f, Tface;
+    if constexpr (VISC == 2) {
+      rho_f = 0.5 * (s.q[0][ai][aj] + s.q[0][bi][bj]);
+      T p_f = 0.5 * (s.q[3][ai][aj] + s.q[3][bi][bj]);
+      nuh_f = 0.5 * (s.q[4][ai][aj] + s.q[4][bi][bj]);
+      Tface = g * p_f / rho_f;
+      T mu_face = viscosity(P, Tface);
+      mut = eddy_viscosity(P.sa, rho_f, nuh_f * P.mu_inf, mu_face / rho_f);
+      mu = mu + mut;
+      k = k + mut / (PR_TURB * (g - 1.0));
+      if (P.c_cr1 != 0.0) {
+        extra = true;
+        T square = ((g00 * g00 + g01 * g01) + g10 * g10) + g11 * g11;
+        bool pos = val(square) > 0.0;
+        T nrm = pos ? dsqrt(square) : cst<T>(1.0);
+        T r01 = (g01 - g10) / nrm, r10 = (g10 - g01) / nrm;
+        T r00 = (g00 - g00) / nrm, r11 = (g11 - g11) / nrm;
+        T div = g00 + g11;
+        T t00 = mut * (g00 + g00 - (2.0 / 3.0) * div * 1.0);
+        T t01 = mut * (g01 + g10 - (2.0 / 3.0) * div * 0.0);
+        T t10 = mut * (g10 + g01 - (2.0 / 3.0) * div * 0.0);
+        T t11 = mut * (g11 + g11 - (2.0 / 3.0) * div * 1.0);
+        T p00 = r00 * t00 + r01 * t01, p01 = r00 * t10 + r01 * t11;
+        T p10 = r10 * t00 + r11 * t01, p11 = r10 * t10 + r11 * t11;
+        ex00 = -P.c_cr1 * (p00 + p00);
+        ex01 = -P.c_cr1 * (p01 + p10);
+        ex10 = -P.c_cr1 * (p10 + p01);
+        ex11 = -P.c_cr1 * (p11 + p11);
+      }
+    }
+    T div = g00 + g11;
+    T ttd = (2.0 / 3.0) * div;
+    T t00 = mu * (2.0 * g00 - ttd), t11 = mu * (2.0 * g11 - ttd), t01 = mu * (g01 + g10);
+    T t10 = t01;
+    if (extra) {
+      t00 = t00 + ex00;
+      t01 = t01 + ex01;
+      t10 = t10 + ex10;
+      t11 = t11 + ex11;
+    }
+    T fx = t00 * sx + t01 * sy;
+    T fy = t10 * sx + t11 * sy;
+    T energy = (vel0 * fx + vel1 * fy) + k * (gx[2] * sx + gy[2] * sy);
+    F[1] = F[1] - fx;
+    F[2] = F[2] - fy;
+    F[3] = F[3] - energy;
+    if constexpr (VISC == 2) {
+      // SA face flux: upwind nu_hat on the inviscid mass flux, diffusion through the
+      // face gradient (turbulence.py:129-135)
+      T mass = Finv[0];
+      T up = val(mass) > 0.0 ? s.q[4][ai][aj] : s.q[4][bi][bj];
+      T mu_face = viscosity(P, Tface);
+      T coef = diffusion_coefficient(P.sa, rho_f, nuh_f * P.mu_inf, mu_face);
+      F[4] = mass * up - coef * (gx[3] * sx + gy[3] * sy);
+    }
+  }
+}
+
+template <class T> __device__ __forceinline__ double tangent_or_value(const T& x);
+template <> __device__ __forceinline__ double tangent_or_value<double>(const double& x) { return x; }
+template <> __device__ __forceinline__ double tangent_or_value<Dual>(const Dual& x) { return x.d; }
+
+// T = double: out = R(U) (second or first order); partial[block] = sum vol R0^2.
+// T = Dual:   out = vdt * V + dR1/dU . V.
+template <class T, int NV, bool SECOND, int VISC>
+__global__ void __launch_bounds__(TILE_THREADS) k_residual(Canvas c, Physics P, const double* __restrict__ U,
+                                                          const double* __restrict__ qg, const double* __restrict__ V,
+                                                          const double* __restrict__ dqg,
+                                                          const double* __restrict__ vdt, double* __restrict__ out,
+                                                          double* __restrict__ partial, const int* active) {
+  if (active != nullptr && *active == 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TileSmem<T, NV>& s = *reinterpret_cast<TileSmem<T, NV>*>(smem_raw);
+  const int NI = c.NI, NJ = c.NJ, N = c.ncanvas();
+  const int i0 = blockIdx.y * TILE_I, j0 = blockIdx.x * TILE_J;
+  const int tid = threadIdx.x;
+  // 1. stage the primitive state of the tile and its halo
+  for (int e = tid; e < HI * HJ; e += TILE_THREADS) {
+    int li = e / HJ, lj = e % HJ;
+    int i = i0 - 2 + li, j = j0 - 2 + lj;
+    T q[5];
+    if (i >= 0 && i < NI && j >= 0 && j < NJ) {
+      load_prim<T>(c, P, i * NJ + j, U, V, qg, dqg, q);
+    } else {
+      for (int v = 0; v < NV; ++v) q[v] = cst<T>(1.0);
+    }
+    for (int v = 0; v < NV; ++v) s.q[v][li][lj] = q[v];
+  }
+  if constexpr (VISC > 0) {
+    const int CI = NI + 2, CJ = NJ + 2;
+    for (int e = tid; e < (TILE_I + 2) * (TILE_J + 2); e += TILE_THREADS) {
+      int li = e / (TILE_J + 2), lj = e % (TILE_J + 2);
+      int i = i0 - 1 + li, j = j0 - 1 + lj;   // canvas cell; centres carry one more ring
+      int ci = min(max(i + 1, 0), CI - 1), cj = min(max(j + 1, 0), CJ - 1);
+      s.cx[li][lj] = c.centres[ci * CJ + cj];
+      s.cy[li][lj] = c.centres[CI * CJ + ci * CJ + cj];
+    }
+  }
+  __syncthreads();
+  // 2. i-faces of the tile: face (i, j) lies between canvas cells (i-1, j) and (i, j)
+  for (int e = tid; e < (TILE_I + 1) * TILE_J; e += TILE_THREADS) {
+    int fi = e / TILE_J, fj = e % TILE_J;
+    int i = i0 + fi, j = j0 + fj;
+    T F[5];
+    bool live = j < NJ && (interior_at(c, i - 1, j) || interior_at(c, i, j));
+    if (live) {
+      int f = i * NJ + j;
+      face_flux<T, NV, SECOND, VISC>(P, s, 0, fi + 1, fj + 2, c.fi[f], c.fi[c.nfi() + f], F);
+    }
+    for (int v = 0; v < NV; ++v) s.Fi[v][fi][fj] = live ? tangent_or_value(F[v]) : 0.0;
+  }
+  // 3. j-faces: face (i, j) lies between (i, j-1) and (i, j)
+  for (int e = tid; e < TILE_I * (TILE_J + 1); e += TILE_THREADS) {
+    int fi = e / (TILE_J + 1), fj = e % (TILE_J + 1);
+    int i = i0 + fi, j = j0 + fj;
+    T F[5];
+    bool live = i < NI && (interior_at(c, i, j - 1) || interior_at(c, i, j));
+    if (live) {
+      int f = i * (NJ + 1) + j;
+      face_flux<T, NV, SECOND, VISC>(P, s, 1, fi + 2, fj + 1, c.fj[f], c.fj[c.nfj() + f], F);
+    }
+    for (int v = 0; v < NV; ++v) s.Fj[v][fi][fj] = live ? tangent_or_value(F[v]) : 0.0;
+  }
+  __syncthreads();
+  // 4. cells: the net flux, the SA source, the output
+  double acc = 0.0;
+  if (tid < TILE_I * TILE_J) {
+    int li = tid / TILE_J, lj = tid % TILE_J;
+    int i = i0 + li, j = j0 + lj;
+    if (i < NI && j < NJ) {
+      int idx = i * NJ + j;
+      if (c.interior[idx]) {
+        double R[NV];
+        for (int v = 0; v < NV; ++v)
+          R[v] = (s.Fi[v][li + 1][lj] - s.Fi[v][li][lj]) + (s.Fj[v][li][lj + 1] - s.Fj[v][li][lj]);
+        if constexpr (VISC == 2) {
+          const int si = li + 2, sj = lj + 2;
+          const double g = P.gamma, vol = c.volume[idx];
+          const int fl = i * NJ + j, fh = (i + 1) * NJ + j;
+          const int gl = i * (NJ + 1) + j, gh = i * (NJ + 1) + j + 1;
+          double sxl = c.fi[fl], syl = c.fi[c.nfi() + fl], sxh = c.fi[fh], syh = c.fi[c.nfi() + fh];
+          double txl = c.fj[gl], tyl = c.fj[c.nfj() + gl], txh = c.fj[gh], tyh = c.fj[c.nfj() + gh];
+          auto avg = [&](int v, int a, int b2, int cc, int dd) { return 0.5 * (s.q[v][a][b2] + s.q[v][cc][dd]); };
+          // Green-Gauss over face-averaged values: g[c][v] = (1/V) sum phi_f S_f,c
+          T gg[2][3];
+          for (int v = 0; v < 3; ++v) {
+            int row = v < 2 ? 1 + v : 4;
+            T pil = avg(row, si - 1, sj, si, sj), pih = avg(row, si, sj, si + 1, sj);
+            T pjl = avg(row, si, sj - 1, si, sj), pjh = avg(row, si, sj, si, sj + 1);
+            gg[0][v] = ((pih * sxh - pil * sxl) + (pjh * txh - pjl * txl)) / vol;
+            gg[1][v] = ((pih * syh - pil * syl) + (pjh * tyh - pjl * tyl)) / vol;
+          }
+          T omega = dabs(gg[0][1] - gg[1][0]);
+          T rho = s.q[0][si][sj];
+          T mu = viscosity(P, g * s.q[3][si][sj] / rho);
+          T Pr, D;
+          sa_source(P.sa, s.q[4][si][sj] * P.mu_inf, mu / rho, omega, c.distance[idx], Pr, D);
+          T src = rho * ((Pr - D) / P.mu_inf +
+                         P.sa.c_b2 / P.sa.sigma * P.mu_inf * (gg[0][2] * gg[0][2] + gg[1][2] * gg[1][2]));
+          R[4] = R[4] - tangent_or_value(src) * vol;
+        }
+        if constexpr (sizeof(T) == sizeof(Dual)) {
+          double w = vdt[idx];
+          for (int v = 0; v < NV; ++v) out[v * N + idx] = w * V[v * N + idx] + R[v];
+        } else {
+          for (int v = 0; v < NV; ++v) out[v * N + idx] = R[v];
+          acc = c.volume[idx] * (R[0] * R[0]);
+        }
+      } else {
+        if constexpr (sizeof(T) == sizeof(Dual)) {
+          double w = vdt[idx];
+          for (int v = 0; v < NV; ++v) out[v * N + idx] = w * V[v * N + idx] + V[v * N + idx];
+        } else {
+          for (int v = 0; v < NV; ++v) out[v * N + idx] = U[v * N + idx] - P.U_inf[v];
+        }
+      }
+    }
+  }
+  if constexpr (sizeof(T) == sizeof(double)) {
+    if (partial != nullptr) {
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+      if ((tid & 31) == 0) s.red[tid >> 5] = acc;
+      __syncthreads();
+      if (tid == 0) {
+        double t = 0.0;
+        for (int k = 0; k < TILE_THREADS / 32; ++k) t += s.red[k];
+        partial[blockIdx.y * gridDim.x + blockIdx.x] = t;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Wave speeds and the per-face terms of the preconditioner (residual.py:169-203,
+// preconditioners.py:557-563): lambda from face-averaged states (a block face's
+// partner from the neighbour map), the SA mass flux and diffusion per face.
+// ------------------------------------------------------------------------------------
+
+__device__ __forceinline__ void prim_raw(const Canvas& c, const Physics& P, const double* U, int idx, double* q) {
+  const int N = c.ncanvas();
+  double u[5];
+  for (int v = 0; v < c.nvar; ++v) u[v] = U[v * N + idx];
+  to_prim(u, q, c.nvar, P.gamma);
+}
+
+template <int VISC>
+__global__ void k_faces(Canvas c, Physics P, const double* __restrict__ U, double* __restrict__ lam,
+                        double* __restrict__ mflux, double* __restrict__ dflux) {
+  const int nfi = c.nfi(), nf = nfi + c.nfj();
+  const int NI = c.NI, NJ = c.NJ;
+  const double g = P.gamma;
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += gridDim.x * blockDim.x) {
+    int a, b;
+    double sx, sy;
+    bool live;
+    if (f < nfi) {
+      int i = f / NJ, j = f % NJ;
+      a = max(i - 1, 0) * NJ + j;
+      b = min(i, NI - 1) * NJ + j;
+      live = (i >= 1 && c.interior[a]) || (i < NI && c.interior[b]);
+      sx = c.fi[f];
+      sy = c.fi[nfi + f];
+    } else {
+      int ff = f - nfi;
+      int i = ff / (NJ + 1), j = ff % (NJ + 1);
+      a = i * NJ + max(j - 1, 0);
+      b = i * NJ + min(j, NJ - 1);
+      live = (j >= 1 && c.interior[a]) || (j < NJ && c.interior[b]);
+      sx = c.fj[ff];
+      sy = c.fj[c.nfj() + ff];
+    }
+    if (!live) {
+      lam[f] = 0.0;
+      if (VISC == 2) {
+        mflux[f] = 0.0;
+        dflux[f] = 0.0;
+      }
+      continue;
+    }
+    int na = c.neighbours[a], nb = c.neighbours[b];
+    double qa[5], qb[5], qf[5];
+    prim_raw(c, P, U, na, qa);
+    prim_raw(c, P, U, nb, qb);
+    for (int v = 0; v < c.nvar; ++v) qf[v] = 0.5 * (qa[v] + qb[v]);
+    double vn = qf[1] * sx + qf[2] * sy;
+    double l = fabs(vn) + sqrt(g * qf[3] / qf[0]) * hypot(sx, sy);
+    if (VISC > 0) {
+      double vol = 0.5 * (c.volume[na] + c.volume[nb]);
+      double mu = viscosity(P, g * qf[3] / qf[0]);
+      double mu_all = mu;
+      if (VISC == 2) mu_all = mu + eddy_viscosity(P.sa, qf[0], qf[4] * P.mu_inf, mu / qf[0]);
+      double factor = 2.0 * g / PR_LAM;
+      l = l + factor * mu_all * (sx * sx + sy * sy) / (qf[0] * vol);
+      if (VISC == 2) {
+        double kap = diffusion_coefficient(P.sa, qf[0], qf[4] * P.mu_inf, mu);
+        mflux[f] = qf[0] * (qf[1] * sx + qf[2] * sy);
+        dflux[f] = kap * (sx * sx + sy * sy) / vol;
+      }
+    }
+    lam[f] = l;
+  }
+}
+
+// Per cell: V/dt = sum lambda / CFL; the flow chains' diagonal scalar sum lambda (1/CFL + 1/2);
+// the SA chains' diagonal (preconditioners.py:564-578).
+template <int VISC>
+__global__ void k_cells(Canvas c, Physics P, const double* __restrict__ U, const double* __restrict__ lam,
+                        const double* __restrict__ mflux, const double* __restrict__ dflux,
+                        const Scalars* __restrict__ sc, double* __restrict__ vdt, double* __restrict__ dflow,
+                        double* __restrict__ dsa) {
+  const int NI = c.NI, NJ = c.NJ, N = c.ncanvas(), nfi = c.nfi();
+  const double cfl = sc->cfl, g = P.gamma;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < N; idx += gridDim.x * blockDim.x) {
+    if (!c.interior[idx]) {
+      vdt[idx] = 0.0;
+      continue;
+    }
+    int i = idx / NJ, j = idx % NJ;
+    int fl = i * NJ + j, fh = (i + 1) * NJ + j;
+    int gl = nfi + i * (NJ + 1) + j, gh = gl + 1;
+    double sum = ((lam[fl] + lam[fh]) + lam[gl]) + lam[gh];
+    vdt[idx] = sum / cfl;
+    dflow[idx] = sum * (1.0 / cfl + 0.5);
+    if constexpr (VISC == 2) {
+      auto out_f = [&](int f) { return fmax(mflux[f], 0.0) + dflux[f]; };
+      auto in_f = [&](int f) { return fmax(-mflux[f], 0.0) + dflux[f]; };
+      double q[5];
+      prim_raw(c, P, U, idx, q);
+      double diag = ((out_f(fh) + in_f(fl)) + out_f(gh)) + in_f(gl);
+      diag = diag / q[0];
+      // vorticity from face-averaged velocities (neighbour-filled raw states)
+      double sxl = c.fi[fl], syl = c.fi[nfi + fl], sxh = c.fi[fh], syh = c.fi[nfi + fh];
+      int jl = i * (NJ + 1) + j, jh = jl + 1;
+      double txl = c.fj[jl], tyl = c.fj[c.nfj() + jl], txh = c.fj[jh], tyh = c.fj[c.nfj() + jh];
+      auto favg = [&](int a, int b, int v) {
+        double qa[5], qb[5];
+        prim_raw(c, P, U, c.neighbours[a], qa);
+        prim_raw(c, P, U, c.neighbours[b], qb);
+        return 0.5 * (qa[v] + qb[v]);
+      };
+      int im = max(i - 1, 0) * NJ + j, ip = min(i + 1, NI - 1) * NJ + j;
+      int jm = i * NJ + max(j - 1, 0), jp = i * NJ + min(j + 1, NJ - 1);
+      double vol = c.volume[idx];
+      double gxv[2], gyv[2];
+      for (int v = 0; v < 2; ++v) {
+        double pil = favg(im, idx, 1 + v), pih = favg(idx, ip, 1 + v);
+        double pjl = favg(jm, idx, 1 + v), pjh = favg(idx, jp, 1 + v);
+        gxv[v] = ((pih * sxh - pil * sxl) + (pjh * txh - pjl * txl)) / vol;
+        gyv[v] = ((pih * syh - pil * syl) + (pjh * tyh - pjl * tyl)) / vol;
+      }
+      double omega = fabs(gxv[1] - gyv[0]);
+      double nu = viscosity(P, g * q[3] / q[0]) / q[0];
+      double d = c.distance[idx];
+      double nut = q[4] * P.mu_inf;
+      double st = s_tilde(P.sa, omega, nut, nu, d);
+      double fw = f_w(P.sa, r_of(P.sa, nut, st, d));
+      double dest = q[4] > 0.0 ? 2.0 * P.sa.c_w1 * fw * P.mu_inf * q[4] / (d * d) : 0.0;
+      dsa[idx] = diag + dest * vol + sum / cfl;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Launch wrappers
+// ------------------------------------------------------------------------------------
+
+size_t tile_smem(bool dual, int nv) {
+  if (dual) return nv == 5 ? sizeof(TileSmem<Dual, 5>) : sizeof(TileSmem<Dual, 4>);
+  return nv == 5 ? sizeof(TileSmem<double, 5>) : sizeof(TileSmem<double, 4>);
+}
+
+dim3 tile_grid(const Canvas& c) { return dim3((c.NJ + TILE_J - 1) / TILE_J, (c.NI + TILE_I - 1) / TILE_I); }
+
+template <class T, int NV, bool SECOND, int VISC> static void configure_one() {
+  cudaFuncSetAttribute(k_residual<T, NV, SECOND, VISC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(TileSmem<T, NV>));
+}
+
+// the tile kernels' dynamic shared memory limits, set once before any launch or capture
+void configure_kernels() {
+  static bool done = false;
+  if (done) return;
+  configure_one<double, 5, true, 2>();
+  configure_one<double, 5, false, 2>();
+  configure_one<double, 4, true, 1>();
+  configure_one<double, 4, false, 1>();
+  configure_one<double, 4, true, 0>();
+  configure_one<double, 4, false, 0>();
+  configure_one<Dual, 5, false, 2>();
+  configure_one<Dual, 4, false, 1>();
+  configure_one<Dual, 4, false, 0>();
+  done = true;
+}
+
+template <class T, int NV, bool SECOND, int VISC>
+static void launch_tile(const Canvas& c, const Physics& P, const double* U, const double* qg, const double* V,
+                        const double* dqg, const double* vdt, double* out, double* partial, const int* active,
+                        cudaStream_t st) {
+  k_residual<T, NV, SECOND, VISC><<<tile_grid(c), TILE_THREADS, sizeof(TileSmem<T, NV>), st>>>(
+      c, P, U, qg, V, dqg, vdt, out, partial, active);
+}
+
+// R(U): second (or first) order, double
+void launch_residual(const Canvas& c, const Physics& P, int visc, bool second, const double* U, const double* qg,
+                     double* R, double* partial, cudaStream_t st) {
+  if (visc == 2) {
+    if (second) launch_tile<double, 5, true, 2>(c, P, U, qg, nullptr, nullptr, nullptr, R, partial, nullptr, st);
+    else launch_tile<double, 5, false, 2>(c, P, U, qg, nullptr, nullptr, nullptr, R, partial, nullptr, st);
+  } else if (visc == 1) {
+    if (second) launch_tile<double, 4, true, 1>(c, P, U, qg, nullptr, nullptr, nullptr, R, partial, nullptr, st);
+    else launch_tile<double, 4, false, 1>(c, P, U, qg, nullptr, nullptr, nullptr, R, partial, nullptr, st);
+  } else {
+    if (second) launch_tile<double, 4, true, 0>(c, P, U, qg, nullptr, nullptr, nullptr, R, partial, nullptr, st);
+    else launch_tile<double, 4, false, 0>(c, P, U, qg, nullptr, nullptr, nullptr, R, partial, nullptr, st);
+  }
+}
+
+// w = vdt * V + dR1/dU . V (the first-order residual's exact tangent)
+void launch_jvp(const Canvas& c, const Physics& P, int visc, const double* U, const double* qg, const double* V,
+                const double* dqg, const double* vdt, double* w, const int* active, cudaStream_t st) {
+  if (visc == 2) launch_tile<Dual, 5, false, 2>(c, P, U, qg, V, dqg, vdt, w, nullptr, active, st);
+  else if (visc == 1) launch_tile<Dual, 4, false, 1>(c, P, U, qg, V, dqg, vdt, w, nullptr, active, st);
+  else launch_tile<Dual, 4, false, 0>(c, P, U, qg, V, dqg, vdt, w, nullptr, active, st);
+}
+
+void launch_ghosts(const Canvas& c, const Physics& P, bool dual, const double* U, const double* V, double* qg,
+                   double* dqg, const int* active, cudaStream_t st) {
+  if (dual) k_ghosts<Dual><<<1, GHOST_THREADS, 0, st>>>(c, P, U, V, qg, dqg, active);
+  else k_ghosts<double><<<1, GHOST_THREADS, 0, st>>>(c, P, U, V, qg, dqg, active);
+}
+
+void launch_faces(const Canvas& c, const Physics& P, int visc, const double* U, double* lam, double* mflux,
+                  double* dflux, cudaStream_t st) {
+  int n = c.NI * (c.NJ + 1) + (c.NI + 1) * c.NJ;
+  int blocks = min((n + 255) / 256, 148 * 8);
+  if (visc == 2) k_faces<2><<<blocks, 256, 0, st>>>(c, P, U, lam, mflux, dflux);
+  else if (visc == 1) k_faces<1><<<blocks, 256, 0, st>>>(c, P, U, lam, mflux, dflux);
+  else k_faces<0><<<blocks, 256, 0, st>>>(c, P, U, lam, mflux, dflux);
+}
+
+void launch_cells(const Canvas& c, const Physics& P, int visc, const double* U, const double* lam,
+                  const double* mflux, const double* dflux, const Scalars* sc, double* vdt, double* dflow,
+                  double* dsa, cudaStream_t st) {
+  int n = c.NI * c.NJ;
+  int blocks = min((n + 255) / 256, 148 * 8);
+  if (visc == 2) k_cells<2><<<blocks, 256, 0, st>>>(c, P, U, lam, mflux, dflux, sc, vdt, dflow, dsa);
+  else if (visc == 1) k_cells<1><<<blocks, 256, 0, st>>>(c, P, U, lam, mflux, dflux, sc, vdt, dflow, dsa);
+  else k_cells<0><<<blocks, 256, 0, st>>>(c, P, U, lam, mflux, dflux, sc, vdt, dflow, dsa);
+}
+
+}  // namespace jr

@@ -1,0 +1,311 @@
+"""The C-ABI library: loading it, and a plan object over ``jr_plan``.
+
+The library (``lib/libjaxrans_b200.so``, built by ``jaxrans_b200.build``) holds the
+sm_100a kernels.  There is no CPU fallback: without the library, or without a CUDA
+device, every entry point raises.  Device buffers are passed as raw pointers; the
+helpers here take ``torch`` CUDA tensors (torch is only the allocator) or NumPy arrays,
+which are copied to the device and back.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from .config import FlowConditions, ImplicitConfig, NumericsConfig, freestream_primitive
+from .plan import Plan
+
+LIB_NAME = "libjaxrans_b200.so"
+LIB_PATH = Path(__file__).resolve().parent / "lib" / LIB_NAME
+
+FLUX_CODES = {"hllc": 0, "roe": 1}
+LIMITER_CODES = {"none": 0, "minmod": 1, "van_albada": 2, "van_albada_smooth": 3}
+FAR_FIELD_CODES = {"characteristic": 0, "characteristic_point_vortex": 1}
+
+_i32p = C.POINTER(C.c_int32)
+_f64p = C.POINTER(C.c_double)
+_u8p = C.POINTER(C.c_uint8)
+
+
+class PlanDesc(C.Structure):
+    """``jr_plan_desc`` (include/jaxrans_b200.h)."""
+
+    _fields_ = [
+        ("NI", C.c_int32), ("NJ", C.c_int32), ("nvar", C.c_int32),
+        ("interior", _u8p), ("volume", _f64p), ("faces_i", _f64p), ("faces_j", _f64p),
+        ("centres", _f64p), ("distance", _f64p), ("neighbours", _i32p),
+        ("n_ghost", C.c_int32 * 2), ("ghost", _i32p * 2), ("source", _i32p * 2), ("kind", _i32p * 2),
+        ("geom", _f64p * 2),
+        ("n_walls", C.c_int32), ("wall_cell", _i32p), ("wall_family", _i32p), ("wall_face", _i32p),
+        ("wall_into", _f64p), ("wall_mid", _f64p),
+        ("n_chains", C.c_int32), ("chain_L", C.c_int32), ("chain_cells", _i32p), ("chain_len", _i32p),
+        ("chain_up_face", _i32p), ("chain_up_sign", _i32p), ("chain_down_face", _i32p),
+        ("chain_down_sign", _i32p),
+        ("gamma", C.c_double), ("mu_inf", C.c_double), ("sutherland", C.c_double), ("c_cr1", C.c_double),
+        ("kappa", C.c_double),
+        ("flux", C.c_int32), ("limiter", C.c_int32), ("far_field", C.c_int32),
+        ("q_inf", C.c_double * 5), ("quarter_chord", C.c_double * 2),
+        ("cfl", C.c_double), ("cfl_max", C.c_double), ("cfl_growth", C.c_double), ("cfl_cutback", C.c_double),
+        ("cfl_min", C.c_double), ("krylov_tol", C.c_double), ("krylov_success", C.c_double),
+        ("max_relative_update", C.c_double),
+        ("krylov_subspace", C.c_int32), ("krylov_restarts", C.c_int32), ("preconditioner", C.c_int32),
+        ("precision", C.c_int32),
+        ("force_length", C.c_double), ("moment_centre", C.c_double * 2),
+    ]
+
+
+EXPORTS = ("jr_plan_create", "jr_plan_destroy", "jr_last_error", "jr_plan_sizes", "jr_plan_stream",
+           "jr_synchronize", "jr_residual", "jr_jvp", "jr_wave_speeds", "jr_precond_factor", "jr_precond_apply",
+           "jr_state_set", "jr_state_get", "jr_state_device", "jr_newton_steps", "jr_newton_steps_async",
+           "jr_forces")
+
+_LIB = None
+
+
+class NativeError(RuntimeError):
+    """A failure reported by the C-ABI library."""
+
+
+def load_library(path: Path | None = None) -> C.CDLL:
+    """The C-ABI library; raises if it has not been built."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    path = Path(path) if path is not None else LIB_PATH
+    if not path.is_file():
+        raise NativeError(f"{path} is missing: build it with `python -m jaxrans_b200.build` "
+                          f"(there is no CPU fallback)")
+    lib = C.CDLL(str(path))
+    vp = C.c_void_p
+    sig = {
+        "jr_plan_create": (C.c_int, [C.POINTER(PlanDesc), C.POINTER(vp)]),
+        "jr_plan_destroy": (C.c_int, [vp]),
+        "jr_last_error": (C.c_char_p, []),
+        "jr_plan_sizes": (C.c_int, [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+        "jr_plan_stream": (vp, [vp]),
+        "jr_synchronize": (C.c_int, [vp]),
+        "jr_residual": (C.c_int, [vp, vp, vp, C.c_int]),
+        "jr_jvp": (C.c_int, [vp, vp, vp, vp]),
+        "jr_wave_speeds": (C.c_int, [vp, vp, vp]),
+        "jr_precond_factor": (C.c_int, [vp, vp, C.c_double]),
+        "jr_precond_apply": (C.c_int, [vp, vp, vp]),
+        "jr_state_set": (C.c_int, [vp, vp, C.c_double, C.c_double]),
+        "jr_state_get": (C.c_int, [vp, vp, _f64p, _f64p, _i32p]),
+        "jr_state_device": (vp, [vp]),
+        "jr_newton_steps": (C.c_int, [vp, C.c_int32, vp]),
+        "jr_newton_steps_async": (C.c_int, [vp, C.c_int32, vp]),
+        "jr_forces": (C.c_int, [vp, vp, vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype, fn.argtypes = res, args
+    if path == LIB_PATH:
+        _LIB = lib
+    return lib
+
+
+def _check(lib, rc: int, what: str) -> None:
+    if rc != 0:
+        msg = lib.jr_last_error().decode(errors="replace")
+        raise NativeError(f"{what} failed (code {rc}): {msg}")
+
+
+def _ptr(a: np.ndarray, kind):
+    return a.ctypes.data_as(kind)
+
+
+class DevicePlan:
+    """One case on the device: ``jr_plan`` with its tables, buffers and state."""
+
+    def __init__(self, plan: Plan, flow: FlowConditions, numerics: NumericsConfig,
+                 implicit: ImplicitConfig | None = None, force_length: float = 1.0,
+                 moment_centre=(0.25, 0.0), library: Path | None = None):
+        self.lib = load_library(library)
+        self.plan, self.flow, self.numerics = plan, flow, numerics
+        self.implicit = implicit or ImplicitConfig()
+        nvar = flow.nvar
+        if nvar == 5 and plan.distance is None:
+            raise ValueError("the SA model needs the plan's wall distance (build_plan(..., with_distance=True))")
+        keep = []
+
+        def arr(a, dtype):
+            a = np.ascontiguousarray(a, dtype=dtype)
+            keep.append(a)
+            return a
+
+        d = PlanDesc()
+        d.NI, d.NJ, d.nvar = plan.NI, plan.NJ, nvar
+        d.interior = _ptr(arr(plan.interior, np.uint8), _u8p)
+        d.volume = _ptr(arr(plan.volume, np.float64), _f64p)
+        d.faces_i = _ptr(arr(plan.faces_i, np.float64), _f64p)
+        d.faces_j = _ptr(arr(plan.faces_j, np.float64), _f64p)
+        d.centres = _ptr(arr(plan.centres, np.float64), _f64p)
+        d.distance = _ptr(arr(plan.distance, np.float64), _f64p) if (nvar == 5) else _f64p()
+        d.neighbours = _ptr(arr(plan.neighbours, np.int32), _i32p)
+        for s, st in enumerate(plan.stages):
+            d.n_ghost[s] = len(st.ghost)
+            d.ghost[s] = _ptr(arr(st.ghost, np.int32), _i32p)
+            d.source[s] = _ptr(arr(st.source, np.int32), _i32p)
+            d.kind[s] = _ptr(arr(st.kind, np.int32), _i32p)
+            d.geom[s] = _ptr(arr(np.stack([st.normal[0], st.normal[1], st.midpoint[0], st.midpoint[1]], axis=1),
+                                 np.float64), _f64p)
+        W = plan.walls
+        d.n_walls = len(W.cell)
+        d.wall_cell = _ptr(arr(W.cell, np.int32), _i32p)
+        d.wall_family = _ptr(arr(W.family, np.int32), _i32p)
+        d.wall_face = _ptr(arr(W.face, np.int32), _i32p)
+        d.wall_into = _ptr(arr(W.into_fluid, np.float64), _f64p)
+        d.wall_mid = _ptr(arr(W.mid if len(W.cell) else np.zeros((0, 2)), np.float64), _f64p)
+        ch = plan.chains
+        d.n_chains, d.chain_L = ch.cells.shape
+        d.chain_cells = _ptr(arr(ch.cells.T, np.int32), _i32p)
+        d.chain_len = _ptr(arr(ch.lengths, np.int32), _i32p)
+        d.chain_up_face = _ptr(arr(ch.up_face.T, np.int32), _i32p)
+        d.chain_up_sign = _ptr(arr(ch.up_sign.T, np.int32), _i32p)
+        d.chain_down_face = _ptr(arr(ch.down_face.T, np.int32), _i32p)
+        d.chain_down_sign = _ptr(arr(ch.down_sign.T, np.int32), _i32p)
+        d.gamma = flow.gamma
+        d.mu_inf = 0.0 if flow.inviscid else flow.mu_inf
+        d.sutherland = -1.0 if flow.sutherland_ratio is None else flow.sutherland_ratio
+        d.c_cr1 = 0.3 if flow.turbulence == "sa_noft2_qcr" else 0.0
+        d.kappa = numerics.kappa
+        d.flux = FLUX_CODES[numerics.flux]
+        d.limiter = 4 if numerics.kappa != 0.0 else LIMITER_CODES[numerics.limiter]
+        d.far_field = FAR_FIELD_CODES[numerics.far_field]
+        q = freestream_primitive(flow)
+        for k, v in enumerate(q):
+            d.q_inf[k] = v
+        d.quarter_chord[0], d.quarter_chord[1] = plan.quarter_chord
+        imp = self.implicit
+        d.cfl, d.cfl_max, d.cfl_growth = imp.cfl, imp.cfl_max, imp.cfl_growth
+        d.cfl_cutback, d.cfl_min = imp.cfl_cutback, imp.cfl_min
+        d.krylov_tol, d.krylov_success = imp.krylov_tol, imp.krylov_success
+        d.max_relative_update = -1.0 if imp.max_relative_update is None else imp.max_relative_update
+        d.krylov_subspace, d.krylov_restarts = imp.krylov_subspace, imp.krylov_restarts
+        d.preconditioner = 1 if imp.preconditioner == "line_j" else 0
+        d.precision = 1 if imp.precision == "mixed" else 0
+        d.force_length = force_length
+        d.moment_centre[0], d.moment_centre[1] = moment_centre[0], moment_centre[1]
+        handle = C.c_void_p()
+        _check(self.lib, self.lib.jr_plan_create(C.byref(d), C.byref(handle)), "jr_plan_create")
+        self.handle = handle
+        self.nvar = nvar
+        self.shape = (nvar, plan.NI, plan.NJ)
+        self.n_faces = (plan.NI + 1) * plan.NJ + plan.NI * (plan.NJ + 1)
+
+    # -- lifetime ---------------------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.jr_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- device buffers ---------------------------------------------------------------
+    @staticmethod
+    def _device(a):
+        """A CUDA float64 tensor of ``a``; torch's stream is drained so the plan's
+        own stream sees the data."""
+        import torch
+        if isinstance(a, torch.Tensor):
+            if a.device.type != "cuda" or a.dtype != torch.float64 or not a.is_contiguous():
+                raise ValueError("device buffers must be contiguous float64 CUDA tensors")
+            t = a
+        else:
+            t = torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device="cuda")
+        torch.cuda.synchronize()
+        return t
+
+    @staticmethod
+    def _like_input(x, t):
+        import torch
+        return t if isinstance(x, torch.Tensor) else t.cpu().numpy()
+
+    def _empty(self, n):
+        import torch
+        return torch.empty(n, dtype=torch.float64, device="cuda")
+
+    def sync(self) -> None:
+        _check(self.lib, self.lib.jr_synchronize(self.handle), "jr_synchronize")
+
+    # -- entry points --------------------------------------------------------------------
+    def residual(self, U, first_order: bool = False):
+        u = self._device(U)
+        out = self._empty(self.shape)
+        _check(self.lib, self.lib.jr_residual(self.handle, u.data_ptr(), out.data_ptr(), int(first_order)),
+               "jr_residual")
+        self.sync()
+        return self._like_input(U, out)
+
+    def jvp(self, U, v):
+        u, t = self._device(U), self._device(v)
+        out = self._empty(self.shape)
+        _check(self.lib, self.lib.jr_jvp(self.handle, u.data_ptr(), t.data_ptr(), out.data_ptr()), "jr_jvp")
+        self.sync()
+        return self._like_input(U, out)
+
+    def wave_speeds(self, U):
+        u = self._device(U)
+        out = self._empty(self.n_faces)
+        _check(self.lib, self.lib.jr_wave_speeds(self.handle, u.data_ptr(), out.data_ptr()), "jr_wave_speeds")
+        self.sync()
+        lam = self._like_input(U, out)
+        nfi = (self.plan.NI + 1) * self.plan.NJ
+        return (lam[:nfi].reshape(self.plan.NI + 1, self.plan.NJ),
+                lam[nfi:].reshape(self.plan.NI, self.plan.NJ + 1))
+
+    def precondition(self, U, cfl: float, r):
+        u, rr = self._device(U), self._device(r)
+        out = self._empty(self.shape)
+        _check(self.lib, self.lib.jr_precond_factor(self.handle, u.data_ptr(), float(cfl)), "jr_precond_factor")
+        _check(self.lib, self.lib.jr_precond_apply(self.handle, rr.data_ptr(), out.data_ptr()), "jr_precond_apply")
+        self.sync()
+        return self._like_input(r, out)
+
+    def set_state(self, U=None, cfl: float | None = None, residual_norm: float = float("inf")) -> None:
+        cfl = self.implicit.cfl if cfl is None else cfl
+        ptr = None
+        if U is not None:
+            U = np.ascontiguousarray(U, dtype=np.float64)
+            if U.shape != self.shape:
+                raise ValueError(f"state must be {self.shape}, got {U.shape}")
+            ptr = U.ctypes.data
+        _check(self.lib, self.lib.jr_state_set(self.handle, ptr, float(cfl), float(residual_norm)), "jr_state_set")
+
+    def get_state(self):
+        U = np.empty(self.shape)
+        cfl, res, status = C.c_double(), C.c_double(), C.c_int32()
+        _check(self.lib, self.lib.jr_state_get(self.handle, U.ctypes.data, C.byref(cfl), C.byref(res),
+                                                C.byref(status)), "jr_state_get")
+        return U, cfl.value, res.value, status.value
+
+    def newton_steps(self, n: int) -> np.ndarray:
+        hist = np.empty(n)
+        _check(self.lib, self.lib.jr_newton_steps(self.handle, int(n), hist.ctypes.data), "jr_newton_steps")
+        return hist
+
+    def newton_steps_async(self, n: int, history_device=None) -> None:
+        ptr = None if history_device is None else history_device.data_ptr()
+        _check(self.lib, self.lib.jr_newton_steps_async(self.handle, int(n), ptr), "jr_newton_steps_async")
+
+    def stream_handle(self) -> int:
+        return int(self.lib.jr_plan_stream(self.handle) or 0)
+
+    def state_device_ptr(self) -> int:
+        return int(self.lib.jr_state_device(self.handle))
+
+    def forces(self, U=None) -> np.ndarray:
+        out = np.empty(6)
+        ptr = None
+        keep = None
+        if U is not None:
+            keep = self._device(U)
+            ptr = keep.data_ptr()
+        _check(self.lib, self.lib.jr_forces(self.handle, ptr, out.ctypes.data), "jr_forces")
+        return out

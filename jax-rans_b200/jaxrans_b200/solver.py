@@ -1,0 +1,212 @@
+"""The iteration driver and ``run``: blocks of Newton steps on the device, the host
+between blocks for the exit tests and force monitoring.
+
+Exit semantics follow ``src/jaxrans/solvers/driver.py:123-201`` and
+``src/jaxrans/simulation.py:40-50, 243-284``: converged when the last residual of a
+block is ``tol`` times the running peak; settled when CL, CD and CM each vary by less
+than ``forces_tol`` over the last quarter of the blocks (at least four samples there);
+stalled when a whole block's residual is bitwise constant; non-finite on any NaN.
+One device->host synchronisation per block (the residual history and the forces).
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .case import Case
+from .config import freestream_primitive
+from .plan import Plan
+
+
+class ExitReason:
+    CONVERGED = "converged"
+    SETTLED = "settled"
+    MAX_ITERS = "max_iters"
+    NON_FINITE = "non_finite"
+    STALLED = "stalled"
+
+
+@dataclass
+class ConvergenceHistory:
+    residual: np.ndarray
+    reason: str
+    n_iters: int
+    seconds: float = float("nan")
+    first_block_seconds: float = float("nan")
+    case_reasons: tuple = ()
+
+    @property
+    def converged(self) -> bool:
+        return self.reason == ExitReason.CONVERGED
+
+    @property
+    def peak(self) -> float:
+        finite = self.residual[np.isfinite(self.residual)]
+        return float(finite.max()) if finite.size else float("nan")
+
+    @property
+    def orders_dropped(self) -> float:
+        if self.residual.size == 0:
+            return 0.0
+        peak, last = self.peak, self.residual[-1]
+        if not (np.isfinite(peak) and np.isfinite(last)) or peak <= 0 or last <= 0:
+            return float("nan")
+        return float(np.log10(peak / last))
+
+    def summary(self) -> str:
+        return (f"{self.reason} after {self.n_iters} iterations, residual peak {self.peak:.6e} -> "
+                f"{self.residual[-1]:.6e} ({self.orders_dropped:.2f} orders from peak)")
+
+
+@dataclass(frozen=True)
+class Forces:
+    cl: float
+    cd: float
+    cm: float
+    fx: float
+    fy: float
+    cd_friction: float = 0.0
+
+    def summary(self) -> str:
+        friction = f" (friction {self.cd_friction:+.6f})" if self.cd_friction else ""
+        return f"CL = {self.cl:+.6f}   CD = {self.cd:+.6f}{friction}   CM = {self.cm:+.6f}"
+
+
+def forces_of(values) -> Forces:
+    cl, cd, cm, cdf, fx, fy = (float(v) for v in values)
+    return Forces(cl, cd, cm, fx, fy, cdf)
+
+
+@dataclass(frozen=True)
+class Timing:
+    total: float
+    first_block: float
+    iterations: int
+    block_iters: int
+    cells: int
+    cases: int = 1
+
+    @property
+    def per_iteration(self) -> float:
+        later = self.iterations - self.block_iters
+        return (self.total - self.first_block) / later if later > 0 else float("nan")
+
+    def record(self) -> dict:
+        return {"total_s": self.total, "per_iteration_s": self.per_iteration, "iterations": self.iterations,
+                "cells": self.cells, "cases": self.cases}
+
+
+@dataclass
+class Result:
+    """A run: ``U`` on the canvas ``(nvar, NI, NJ)``, forces, the residual history,
+    the lift at the end of every block (``src/jaxrans/simulation.py:104-169``)."""
+
+    case: Case
+    grid: Plan
+    U: np.ndarray
+    forces: Forces
+    history: ConvergenceHistory
+    cl_history: np.ndarray
+    timing: Timing
+    coefficients: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))
+
+    @property
+    def cells(self) -> int:
+        return self.grid.cells
+
+    @property
+    def cl_spread(self) -> float:
+        return cl_spread(self.cl_history)
+
+
+def cl_spread(history) -> float:
+    """The range over the last quarter of the blocks; NaN with fewer than 4 samples there."""
+    tail = np.asarray(history)[3 * len(history) // 4:]
+    return float(tail.max() - tail.min()) if tail.size >= 4 else float("nan")
+
+
+def freestream_state(case: Case, plan: Plan) -> np.ndarray:
+    """The freestream on every canvas cell, conservative (``src/jaxrans/numerics/residual.py:250-258``)."""
+    q = freestream_primitive(case.flow)
+    g = case.flow.gamma
+    rho, u, v, p = q[:4]
+    rows = [rho, rho * u, rho * v, p / (g - 1.0) + 0.5 * rho * (u * u + v * v)]
+    if len(q) > 4:
+        rows.append(rho * q[4])
+    return np.broadcast_to(np.array(rows)[:, None, None], (len(rows),) + plan.shape).copy()
+
+
+def device_for(case: Case, plan: Plan):
+    from .native import DevicePlan
+    spec = case.grid_spec
+    return DevicePlan(plan, case.flow, case.numerics, case.implicit, spec.reference_length,
+                      tuple(spec.moment_centre[:2]))
+
+
+def march(case: Case, plan: Plan, progress=None, initial=None, device=None, max_iters=None) -> Result:
+    """One grid to steady state from the freestream, or from ``initial`` on the block cells."""
+    num = case.numerics
+    dev = device if device is not None else device_for(case, plan)
+    U0 = freestream_state(case, plan)
+    if initial is not None:
+        U0 = np.where(plan.interior, np.asarray(initial), U0)
+    dev.set_state(U0, case.implicit.cfl, float("inf"))
+    block_iters = case.block_iters
+    max_iters = num.max_iters if max_iters is None else max_iters
+    n_blocks = max(1, -(-max_iters // block_iters))
+    blocks, cl_history, coefficients = [], [], []
+    peak, reason = 0.0, ExitReason.MAX_ITERS
+    started = time.perf_counter()
+    first_block = float("nan")
+    for b in range(n_blocks):
+        hist = dev.newton_steps(block_iters)
+        if b == 0:
+            first_block = time.perf_counter() - started
+        blocks.append(hist)
+        f = forces_of(dev.forces())
+        cl_history.append(f.cl)
+        coefficients.append((f.cl, f.cd, f.cm))
+        finite = hist[np.isfinite(hist)]
+        if finite.size:
+            peak = max(peak, float(finite.max()))
+        if progress is not None:
+            last = float(hist[-1])
+            orders = float(np.log10(peak / last)) if peak > 0 and last > 0 else 0.0
+            progress((b + 1) * block_iters, last, orders, f)
+        stop = num.forces_tol is not None and all(cl_spread(h) < num.forces_tol
+                                                  for h in np.transpose(coefficients))
+        last = hist[-1]
+        failed = not np.all(np.isfinite(hist)) or not np.all(np.isfinite([f.cl, f.cd, f.cm]))
+        if failed:
+            reason = ExitReason.NON_FINITE
+        elif peak > 0 and last <= num.tol * peak:
+            reason = ExitReason.CONVERGED
+        elif len(hist) > 1 and np.all(hist == hist[0]):
+            reason = ExitReason.STALLED
+        elif stop:
+            reason = ExitReason.SETTLED
+        if reason != ExitReason.MAX_ITERS:
+            break
+    seconds = time.perf_counter() - started
+    residual = np.concatenate(blocks)
+    U, _, _, _ = dev.get_state()
+    history = ConvergenceHistory(residual, reason, int(residual.size), seconds, first_block)
+    return Result(case=case, grid=plan, U=U, forces=forces_of(dev.forces()), history=history,
+                  cl_history=np.asarray(cl_history),
+                  timing=Timing(seconds, first_block, int(residual.size), block_iters, plan.cells),
+                  coefficients=np.asarray(coefficients))
+
+
+def run(case: Case, grid: Plan | None = None, progress=None, on_level=None, devices=None, *, initial=None) -> Result:
+    """March ``case`` to steady state on ``grid`` (default ``case.grid()``) on one GPU
+    (``src/jaxrans/simulation.py:213-240``).  ``devices`` (slabs over several GPUs) is
+    not part of this build."""
+    if devices is not None and len(devices) > 1:
+        raise ValueError("splitting one case over several devices is not implemented in this build")
+    plan = case.grid() if grid is None else grid
+    if on_level is not None:
+        on_level(0, plan)
+    return march(case, plan, progress=progress, initial=initial)

@@ -1,0 +1,43 @@
+"""The C-ABI library: built for sm_100a, loadable, exporting every symbol the header declares."""
+
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "jaxrans_b200.h"
+
+
+def declared() -> list[str]:
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:int|void\*|double\*|const char\*)\s+(jr_\w+)\(", text, re.M)))
+
+
+def test_library_builds_and_loads():
+    from jaxrans_b200.build import build
+    from jaxrans_b200.native import load_library
+    lib = build()
+    assert lib.is_file()
+    load_library()
+
+
+def test_every_declared_symbol_is_exported():
+    from jaxrans_b200.build import build
+    from jaxrans_b200.native import EXPORTS
+    lib = ctypes.CDLL(str(build()))
+    names = declared()
+    assert len(names) >= 15
+    for name in names:
+        assert hasattr(lib, name), name
+    assert sorted(EXPORTS) == names
+
+
+def test_errors_without_a_device_are_reported_not_crashed():
+    from jaxrans_b200.native import load_library
+    lib = load_library()
+    assert lib.jr_plan_create(None, None) == 1          # JR_EINVAL on a null descriptor
+    assert b"null" in lib.jr_last_error()
