@@ -109,7 +109,7 @@ def test_freestream_preserved_on_device(cuda, name):
         assert np.abs(block[:, :, 0]).max() > 1e-8     # the wall does disturb a uniform flow
 
 
-@pytest.mark.parametrize("name", ["o_euler", "c_sa"])
+@pytest.mark.parametrize("name", ["o_euler", "c_sa", "c_laminar"])
 def test_converged_forces_match_reference(cuda, name):
     """Run to the reference's convergence test and compare CL, CD, CM with the
     reference's converged run on the same grid (1e-6)."""
