@@ -107,6 +107,10 @@ int jr_state_set(jr_plan* plan, const double* U_host, double cfl, double residua
 int jr_state_get(jr_plan* plan, double* U_host, double* cfl, double* residual_norm, int32_t* status);
 /* Device pointer to the plan's own state U (nvar x NI*NJ), valid until jr_plan_destroy. */
 double* jr_state_device(jr_plan* plan);
+/* The state from a device buffer (a restart with the inputs already in HBM). */
+int jr_state_set_device(jr_plan* plan, const double* U_device, double cfl, double residual_norm);
+/* Kernels launched by one captured Newton step (the graph's kernel nodes). */
+int jr_graph_kernels(jr_plan* plan, int64_t* kernels_per_step);
 
 /* n_steps pseudo-transient Newton steps on the plan's state, one captured CUDA graph per
  * step; history (host, n_steps) receives |R| before each step.  Synchronises once.

@@ -464,6 +464,43 @@ int jr_state_get(jr_plan* plan, double* U_host, double* cfl, double* residual_no
 
 double* jr_state_device(jr_plan* plan) { return plan ? plan->U : nullptr; }
 
+int jr_state_set_device(jr_plan* plan, const double* U_device, double cfl, double residual_norm) {
+  if (!plan || !U_device) return fail(JR_EINVAL, "null argument");
+  cudaMemcpyAsync(plan->U, U_device, (size_t)plan->n_vec * sizeof(double), cudaMemcpyDeviceToDevice, plan->st);
+  Scalars s{};
+  s.cfl = cfl;
+  s.res_prev = residual_norm;
+  static thread_local Scalars staged;
+  staged = s;
+  cudaMemcpyAsync(plan->sc, &staged, sizeof(Scalars), cudaMemcpyHostToDevice, plan->st);
+  if (cudaStreamSynchronize(plan->st) != cudaSuccess) return cuda_check("jr_state_set_device");
+  return cuda_check("jr_state_set_device");
+}
+
+static int ensure_graph(jr_plan* plan);
+
+int jr_graph_kernels(jr_plan* plan, int64_t* kernels_per_step) {
+  if (!plan || !kernels_per_step) return fail(JR_EINVAL, "null argument");
+  cudaGraph_t g;
+  if (cudaStreamBeginCapture(plan->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    return cuda_check("begin capture");
+  enqueue_step(plan);
+  if (cudaStreamEndCapture(plan->st, &g) != cudaSuccess) return cuda_check("end capture");
+  size_t n = 0;
+  cudaGraphGetNodes(g, nullptr, &n);
+  std::vector<cudaGraphNode_t> nodes(n);
+  cudaGraphGetNodes(g, nodes.data(), &n);
+  int64_t kernels = 0;
+  for (auto node : nodes) {
+    cudaGraphNodeType t;
+    cudaGraphNodeGetType(node, &t);
+    if (t == cudaGraphNodeTypeKernel) ++kernels;
+  }
+  cudaGraphDestroy(g);
+  *kernels_per_step = kernels;
+  return cuda_check("jr_graph_kernels");
+}
+
 static int ensure_graph(jr_plan* plan) {
   if (plan->graph) return JR_OK;
   cudaGraph_t g;

@@ -72,7 +72,7 @@ __device__ void wall_viscous(const Canvas& c, const Physics& P, const double* U,
 }
 
 // out: cl, cd, cm, cd_friction, fx, fy
-__global__ void k_forces(Canvas c, Physics P, const double* U, const double* qg, double length, double cx0,
+__global__ void __launch_bounds__(256) k_forces(Canvas c, Physics P, const double* U, const double* qg, double length, double cx0,
                          double cy0, double* out) {
   __shared__ double red[6][32];
   double acc[6] = {0, 0, 0, 0, 0, 0};
@@ -135,7 +135,7 @@ __global__ void k_forces(Canvas c, Physics P, const double* U, const double* qg,
 
 void launch_forces(const Canvas& c, const Physics& P, const double* U, const double* qg, double length, double cx0,
                    double cy0, double* out, cudaStream_t st) {
-  k_forces<<<1, 1024, 0, st>>>(c, P, U, qg, length, cx0, cy0, out);
+  k_forces<<<1, 256, 0, st>>>(c, P, U, qg, length, cx0, cy0, out);
 }
 
 }  // namespace jr

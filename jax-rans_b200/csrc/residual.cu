@@ -549,14 +549,14 @@ __global__ void k_faces(Canvas c, Physics P, const double* __restrict__ U, doubl
   const int NI = c.NI, NJ = c.NJ;
   const double g = P.gamma;
   for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += gridDim.x * blockDim.x) {
+    // every canvas face, as the reference computes them: the canvas edge copied
+    // (a face on the edge averages the edge cell with itself)
     int a, b;
     double sx, sy;
-    bool live;
     if (f < nfi) {
       int i = f / NJ, j = f % NJ;
       a = max(i - 1, 0) * NJ + j;
       b = min(i, NI - 1) * NJ + j;
-      live = (i >= 1 && c.interior[a]) || (i < NI && c.interior[b]);
       sx = c.fi[f];
       sy = c.fi[nfi + f];
     } else {
@@ -564,17 +564,8 @@ __global__ void k_faces(Canvas c, Physics P, const double* __restrict__ U, doubl
       int i = ff / (NJ + 1), j = ff % (NJ + 1);
       a = i * NJ + max(j - 1, 0);
       b = i * NJ + min(j, NJ - 1);
-      live = (j >= 1 && c.interior[a]) || (j < NJ && c.interior[b]);
       sx = c.fj[ff];
       sy = c.fj[c.nfj() + ff];
-    }
-    if (!live) {
-      lam[f] = 0.0;
-      if (VISC == 2) {
-        mflux[f] = 0.0;
-        dflux[f] = 0.0;
-      }
-      continue;
     }
     int na = c.neighbours[a], nb = c.neighbours[b];
     double qa[5], qb[5], qf[5];
@@ -609,11 +600,9 @@ __global__ void k_cells(Canvas c, Physics P, const double* __restrict__ U, const
                         double* __restrict__ dsa) {
   const int NI = c.NI, NJ = c.NJ, N = c.ncanvas(), nfi = c.nfi();
   const double cfl = sc->cfl, g = P.gamma;
+  // every canvas cell: V/dt enters the Krylov operator on ghost cells too (there the
+  // residual is U - U_inf, its tangent the identity)
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < N; idx += gridDim.x * blockDim.x) {
-    if (!c.interior[idx]) {
-      vdt[idx] = 0.0;
-      continue;
-    }
     int i = idx / NJ, j = idx % NJ;
     int fl = i * NJ + j, fh = (i + 1) * NJ + j;
     int gl = nfi + i * (NJ + 1) + j, gh = gl + 1;

@@ -59,7 +59,7 @@ class PlanDesc(C.Structure):
 EXPORTS = ("jr_plan_create", "jr_plan_destroy", "jr_last_error", "jr_plan_sizes", "jr_plan_stream",
            "jr_synchronize", "jr_residual", "jr_jvp", "jr_wave_speeds", "jr_precond_factor", "jr_precond_apply",
            "jr_state_set", "jr_state_get", "jr_state_device", "jr_newton_steps", "jr_newton_steps_async",
-           "jr_forces")
+           "jr_forces", "jr_state_set_device", "jr_graph_kernels")
 
 _LIB = None
 
@@ -97,6 +97,8 @@ def load_library(path: Path | None = None) -> C.CDLL:
         "jr_newton_steps": (C.c_int, [vp, C.c_int32, vp]),
         "jr_newton_steps_async": (C.c_int, [vp, C.c_int32, vp]),
         "jr_forces": (C.c_int, [vp, vp, vp]),
+        "jr_state_set_device": (C.c_int, [vp, vp, C.c_double, C.c_double]),
+        "jr_graph_kernels": (C.c_int, [vp, C.POINTER(C.c_int64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -293,6 +295,17 @@ class DevicePlan:
     def newton_steps_async(self, n: int, history_device=None) -> None:
         ptr = None if history_device is None else history_device.data_ptr()
         _check(self.lib, self.lib.jr_newton_steps_async(self.handle, int(n), ptr), "jr_newton_steps_async")
+
+    def set_state_device(self, U_device, cfl: float | None = None, residual_norm: float = float("inf")) -> None:
+        """The state from a device tensor (no host copy)."""
+        cfl = self.implicit.cfl if cfl is None else cfl
+        _check(self.lib, self.lib.jr_state_set_device(self.handle, U_device.data_ptr(), float(cfl),
+                                                       float(residual_norm)), "jr_state_set_device")
+
+    def kernels_per_step(self) -> int:
+        n = C.c_int64()
+        _check(self.lib, self.lib.jr_graph_kernels(self.handle, C.byref(n)), "jr_graph_kernels")
+        return int(n.value)
 
     def stream_handle(self) -> int:
         return int(self.lib.jr_plan_stream(self.handle) or 0)

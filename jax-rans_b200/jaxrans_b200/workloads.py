@@ -1,0 +1,58 @@
+"""The benchmark workloads as two-JSON case documents.
+
+Seeded synthetic inputs stand in for nothing external: every case is a generated NACA
+4-digit section on a generated grid, so the same documents give the same grids here,
+on a GPU box and in the oracle.
+
+* ``o_euler_257`` -- 2D Euler, NACA 0012, single-block O-grid 257 x 65 nodes (256 x 64
+  cells), far field at 50 chords, M 0.8, alpha 1.25 deg, HLLC with MUSCL van Albada,
+  4 variables, freestream start, converged when the density residual has dropped 1e-10
+  below its running peak.
+* ``c_sa_385`` -- 2D SA-noft2 RANS, NACA 4412, single-block C-grid 385 x 97 nodes (256
+  cells round the airfoil, 64 along each wake side, 96 normal), first cell 1e-6 chord with
+  a normal growth starting at 1.1 and rising linearly to reach the far field at 50
+  chords, Re 6e6, M 0.2, alpha 8 deg, Roe with MUSCL minmod, 5 variables, GMRES restart
+  30, steps bounded to 20 % relative change.  Converged when the residual has dropped
+  1e-10 below its peak or CL, CD and CM have each settled within 1e-7 over the last
+  quarter of the run (a force change far below the 0.1 drag-count tolerance).
+"""
+
+from __future__ import annotations
+
+import copy
+
+from .case import Case, parse_case
+
+WORKLOADS = {
+    "o_euler_257": (
+        {"general": {"case_name": "o_euler_257"},
+         "domain": {"grid": "o_grid", "airfoil": "naca0012", "cells_airfoil": 256, "cells_normal": 64,
+                    "wall_spacing": 1e-3, "far_field": 50.0},
+         "boundary_conditions": {"wall": {"type": "slip_wall"}, "farfield": {"type": "far_field"}},
+         "freestream": {"mach": 0.8, "alpha_deg": 1.25}},
+        {"convective_fluxes": {"riemann_solver": "hllc", "limiter": "van_albada"},
+         "time_integration": {"solver": "implicit"},
+         "convergence": {"max_iters": 6000, "tol": 1e-10, "forces_tol": None, "block_iters": 20}},
+    ),
+    "c_sa_385": (
+        {"general": {"case_name": "c_sa_385"},
+         "domain": {"grid": "c_grid", "airfoil": "naca4412", "cells_airfoil": 256, "cells_wake": 64,
+                    "cells_normal": 96, "wall_spacing": 1e-6, "far_field": 50.0, "normal_stretching": 1.1},
+         "boundary_conditions": {"wall": {"type": "no_slip_wall"}, "farfield": {"type": "far_field"}},
+         "freestream": {"mach": 0.2, "alpha_deg": 8.0, "reynolds": 6e6},
+         "turbulence": {"model": "sa_noft2"}},
+        {"convective_fluxes": {"riemann_solver": "roe", "limiter": "minmod"},
+         "time_integration": {"solver": "implicit"},
+         "implicit": {"krylov_subspace": 30, "max_relative_update": 0.2},
+         "convergence": {"max_iters": 8000, "tol": 1e-10, "forces_tol": 1e-7, "block_iters": 20}},
+    ),
+}
+
+
+def workload(name: str, **numerical) -> Case:
+    """The case of a named workload; ``numerical`` entries ``section.key=value`` override."""
+    case_doc, num_doc = copy.deepcopy(WORKLOADS[name])
+    for path, value in numerical.items():
+        section, key = path.split(".")
+        num_doc.setdefault(section, {})[key] = value
+    return parse_case(case_doc, num_doc)

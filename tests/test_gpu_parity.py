@@ -2,8 +2,10 @@
 
 Every comparison is against a golden array the reference produced
 (``tests/golden/make_golden.py``), or the oracle where the golden holds none.
-Tolerances (FP64): residuals and J.v 1e-12 relative to each row's largest entry
-(the plain-path target); wave speeds 1e-13; the line solve 1e-10 (block Thomas on
+Tolerances (FP64): residuals 1e-12 relative to each row's largest entry (the
+plain-path target); J.v 1e-12 on the mean-flow rows and 1e-10 on the SA row, whose
+tangent in a near-uniform state is a difference of source terms O(1e3) larger than
+itself (fused multiply-adds move it by 4e-11, plain multiplies by 1e-12); wave speeds 1e-13; the line solve 1e-10 (block Thomas on
 the device against the reference's cyclic reduction: the same solve to round-off,
 amplified by the blocks' conditioning); forces 1e-12.
 """
@@ -44,8 +46,10 @@ def test_residual_matches_reference(cuda, name, state):
 @pytest.mark.parametrize("state", ["sin", "rand0"])
 def test_jvp_matches_reference(cuda, name, state):
     z, case, plan, dev = device_plan(name)
-    Jv = dev.jvp(z[f"{state}_U"], z[f"{state}_v"])
-    assert row_rel(Jv, z[f"{state}_Jv"]) < 1e-12
+    Jv, ref = dev.jvp(z[f"{state}_U"], z[f"{state}_v"]), z[f"{state}_Jv"]
+    assert row_rel(Jv[:4], ref[:4]) < 1e-12
+    if ref.shape[0] > 4:
+        assert row_rel(Jv[4:], ref[4:]) < 1e-10
 
 
 @pytest.mark.parametrize("name", CASES)
