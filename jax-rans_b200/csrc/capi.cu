@@ -25,7 +25,8 @@ void configure_kernels();
 // linesolve.cu
 void launch_chain_factor(const Canvas&, const Physics&, bool sa, bool fp32, const double* U, const double* lam,
                          const double* mflux, const double* dflux, const double* dflow, const double* dsa, void* fflow,
-                         void* fsa, cudaStream_t);
+                         void* fsa, void* scratch, cudaStream_t);
+void configure_line_kernels(const Canvas&);
 void launch_chain_apply(const Canvas&, bool sa, bool fp32, const void* fflow, const void* fsa, const double* r,
                         const double* scale, const int* skip, void* vout, bool vout_fp32, double* z, cudaStream_t);
 // krylov.cu
@@ -84,7 +85,7 @@ struct jr_plan {
   double *r = nullptr, *w = nullptr, *z = nullptr, *tmp = nullptr, *zero = nullptr, *vdt = nullptr;
   double *dflow = nullptr, *dsa = nullptr, *lam = nullptr, *mflux = nullptr, *dflux = nullptr;
   double *tile_partial = nullptr, *history = nullptr, *force_out = nullptr;
-  void *V = nullptr, *fflow = nullptr, *fsa = nullptr;
+  void *V = nullptr, *fflow = nullptr, *fsa = nullptr, *scratch = nullptr;
   Scalars* sc = nullptr;
   Reduce red{};
   int hist_cap = 0;
@@ -145,7 +146,7 @@ static void enqueue_step(jr_plan* p) {
   launch_cells(c, p->P, p->visc, p->U, p->lam, p->mflux, p->dflux, p->sc, p->vdt, p->dflow, p->dsa, st);
   if (p->cfg.preconditioner == 1)
     launch_chain_factor(c, p->P, sa, p->mixed, p->U, p->lam, p->mflux, p->dflux, p->dflow, p->dsa, p->fflow, p->fsa,
-                        st);
+                        p->scratch, st);
   const size_t vbytes = p->mixed ? sizeof(float) : sizeof(double);
   for (int cyc = 0; cyc < p->cfg.maxiter; ++cyc) {
     launch_cycle_start(p->sc, p->cfg, st);
@@ -277,6 +278,17 @@ int jr_plan_create(const jr_plan_desc* d, jr_plan** out) {
   TRY(dev_copy(plan, (int**)&c.ch_up_sign, d->chain_up_sign, (size_t)nc * L));
   TRY(dev_copy(plan, (int**)&c.ch_down_face, d->chain_down_face, (size_t)nc * L));
   TRY(dev_copy(plan, (int**)&c.ch_down_sign, d->chain_down_sign, (size_t)nc * L));
+  if (L > 1024) {
+    jr_plan_destroy(plan);
+    return fail(JR_EINVAL, "line chains longer than 1024 cells are not supported");
+  }
+  std::vector<int> fbase(nc);
+  size_t fbase_total = 0;
+  for (int k = 0; k < nc; ++k) {
+    fbase[k] = (int)fbase_total;
+    fbase_total += (size_t)d->chain_len[k] + 16;
+  }
+  TRY(dev_copy(plan, (int**)&c.ch_fbase, fbase.data(), (size_t)nc));
 
   Physics& P = plan->P;
   P.gamma = d->gamma;
@@ -355,14 +367,18 @@ int jr_plan_create(const jr_plan_desc* d, jr_plan** out) {
   TRY(dev_copy<double>(plan, &plan->force_out, nullptr, 8));
   const size_t tb = plan->mixed ? sizeof(float) : sizeof(double);
   TRY(dev_alloc(plan, &plan->V, (size_t)(plan->m + 1) * vec * tb));
-  TRY(dev_alloc(plan, &plan->fflow, (size_t)L * 48 * nc * tb));
-  TRY(dev_alloc(plan, &plan->fsa, (size_t)L * 3 * nc * tb));
+  // cyclic-reduction factor: per chain at most 80 (flow) and 5 (SA) entries per row of
+  // (length + 16) rows; the level systems in scratch at most 104 per row
+  TRY(dev_alloc(plan, &plan->fflow, fbase_total * 80 * tb));
+  TRY(dev_alloc(plan, &plan->fsa, fbase_total * 5 * tb));
+  TRY(dev_alloc(plan, &plan->scratch, fbase_total * 104 * tb));
   TRY(dev_alloc(plan, (void**)&plan->sc, sizeof(Scalars)));
   int rb = reduce_blocks(plan->n_vec);
   plan->red.blocks = rb;
   TRY(dev_alloc(plan, (void**)&plan->red.partial, (size_t)rb * (MAX_KRYLOV + 1) * sizeof(double)));
   TRY(dev_alloc(plan, (void**)&plan->red.ticket, sizeof(unsigned)));
   configure_kernels();
+  configure_line_kernels(c);
   if (cudaDeviceSynchronize() != cudaSuccess) {
     int rc = cuda_check("plan create");
     jr_plan_destroy(plan);
@@ -426,7 +442,7 @@ int jr_precond_factor(jr_plan* plan, const double* U, double cfl) {
   launch_cells(plan->cv, plan->P, plan->visc, U, plan->lam, plan->mflux, plan->dflux, plan->sc, plan->vdt,
                plan->dflow, plan->dsa, plan->st);
   launch_chain_factor(plan->cv, plan->P, plan->cv.nvar == 5, plan->mixed, U, plan->lam, plan->mflux, plan->dflux,
-                      plan->dflow, plan->dsa, plan->fflow, plan->fsa, plan->st);
+                      plan->dflow, plan->dsa, plan->fflow, plan->fsa, plan->scratch, plan->st);
   return cuda_check("jr_precond_factor");
 }
 

@@ -56,6 +56,7 @@ struct Canvas {
   const int* ch_up_sign;
   const int* ch_down_face;
   const int* ch_down_sign;
+  const int* ch_fbase;         // [c]: sum over earlier chains of (length + 16), the factor's row offset
   int n_offchain;              // canvas cells on no chain
   const int* offchain;
 

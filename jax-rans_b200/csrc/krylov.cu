@@ -13,6 +13,7 @@
 namespace jr {
 
 constexpr int RED_THREADS = 256;
+constexpr int MD_E = 4;   // elements per thread in the basis passes
 
 __device__ __forceinline__ double warp_sum(double x) {
   for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
@@ -76,9 +77,11 @@ __device__ __forceinline__ void chunk(int n, int& lo, int& hi) {
 
 // Start of a Newton step: b = -R, x = action = 0, r = b; |b|; the residual norm of the
 // density row from the tile partials; the history entry.
-__global__ void k_gmres_init(Scalars* sc, const double* R, double* b, double* x, double* action, double* r, int n,
-                             const double* tile_partial, int n_tiles, double volume_sum, double* history,
-                             double* partial, unsigned* ticket) {
+__global__ void __launch_bounds__(RED_THREADS) k_gmres_init(Scalars* sc, const double* R, double* b, double* x,
+                                                            double* action, double* r, int n,
+                                                            const double* tile_partial, int n_tiles,
+                                                            double volume_sum, double* history, double* partial,
+                                                            unsigned* ticket) {
   int lo, hi;
   chunk(n, lo, hi);
   double acc[1] = {0.0};
@@ -114,22 +117,61 @@ __global__ void k_cycle_start(Scalars* sc, Config cfg) {
   for (int k = 0; k < (cfg.restart + 1) * cfg.restart; ++k) sc->H[k] = 0.0;
 }
 
-// Block partial dots of w with V_0..V_{nk-1}, finished by the last block into hout.
-template <class TV>
-__device__ void dots_tail(const TV* V, size_t ldv, int nk, const double* w, int lo, int hi, double* partial,
-                          unsigned* ticket, double* hout) {
-  __shared__ double sm[RED_THREADS / 32][MAX_KRYLOV + 1];
+// The three passes of CGS2 over the basis, one kernel: MODE 0 h = V^T w; MODE 1
+// w -= V hin, then h = V^T w; MODE 2 w -= V hin, then |w| and column j of H.  Each
+// thread owns MD_E elements and keeps NK accumulators in registers; all loads of a
+// pass are independent of one another.
+template <class TV, int NK, int MODE>
+__global__ void __launch_bounds__(RED_THREADS) k_mdot(Scalars* sc, const TV* __restrict__ V, size_t ldv, int nk,
+                                                      double* __restrict__ w, int n, const double* __restrict__ hin,
+                                                      double* __restrict__ partial, unsigned* __restrict__ ticket,
+                                                      double* __restrict__ hout, int j, int m) {
+  if (sc->active == 0) return;
+  constexpr int NA = MODE == 2 ? 1 : NK;
+  __shared__ double sm[RED_THREADS / 32][NA];
   __shared__ bool last;
+  double acc[NA];
+#pragma unroll
+  for (int k = 0; k < NA; ++k) acc[k] = 0.0;
+  double h[MODE == 0 ? 1 : NK];
+  if constexpr (MODE != 0) {
+#pragma unroll
+    for (int k = 0; k < NK; ++k) h[k] = k < nk ? hin[k] : 0.0;
+  }
+  const int base = blockIdx.x * blockDim.x * MD_E + threadIdx.x;
+#pragma unroll
+  for (int t = 0; t < MD_E; ++t) {
+    const int i = base + t * blockDim.x;
+    if (i < n) {
+      double wi = w[i];
+      if constexpr (MODE != 0) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < NK; ++k)
+          if (k < nk) s += h[k] * double(V[k * ldv + i]);
+        wi = wi - s;
+        w[i] = wi;
+      }
+      if constexpr (MODE == 2) {
+        acc[0] += wi * wi;
+      } else {
+#pragma unroll
+        for (int k = 0; k < NK; ++k)
+          if (k < nk) acc[k] += double(V[k * ldv + i]) * wi;
+      }
+    }
+  }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int k = 0; k < nk; ++k) {
-    const TV* vk = V + k * ldv;
-    double s = 0.0;
-    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) s += double(vk[i]) * w[i];
-    s = warp_sum(s);
-    if (lane == 0) sm[warp][k] = s;
+  const int width = MODE == 2 ? 1 : nk;
+#pragma unroll
+  for (int k = 0; k < NA; ++k) {
+    if (k < width) {
+      double x = warp_sum(acc[k]);
+      if (lane == 0) sm[warp][k] = x;
+    }
   }
   __syncthreads();
-  if (threadIdx.x < nk) {
+  if ((int)threadIdx.x < width) {
     double t = 0.0;
     for (int ww = 0; ww < nw; ++ww) t += sm[ww][threadIdx.x];
     partial[blockIdx.x * (MAX_KRYLOV + 1) + threadIdx.x] = t;
@@ -140,116 +182,88 @@ __device__ void dots_tail(const TV* V, size_t ldv, int nk, const double* w, int 
   __syncthreads();
   if (!last) return;
   __threadfence();
-  if (threadIdx.x < nk) {
+  if ((int)threadIdx.x < width) {
     const volatile double* p = partial;
     double t = 0.0;
     for (int b = 0; b < (int)gridDim.x; ++b) t += p[b * (MAX_KRYLOV + 1) + threadIdx.x];
-    hout[threadIdx.x] = t;
+    if constexpr (MODE == 2) {
+      double nrm = sqrt(t);
+      for (int k = 0; k < nk; ++k) sc->H[k + (m + 1) * j] = sc->h1[k] + sc->h2[k];
+      sc->H[j + 1 + (m + 1) * j] = nrm;
+      sc->nrm = nrm;
+      sc->inv_nrm = 1.0 / fmax(nrm, 2.2250738585072014e-308);
+      if (nrm == 0.0) sc->status |= ST_GMRES_BREAKDOWN;
+    } else {
+      hout[threadIdx.x] = t;
+    }
   }
   __syncthreads();
   if (threadIdx.x == 0) *ticket = 0u;
 }
 
-// h1[k] = V_k . w for k <= j
-template <class TV>
-__global__ void __launch_bounds__(RED_THREADS) k_dots(const Scalars* sc, const TV* V, size_t ldv, int nk,
-                                                      const double* w, int n, double* partial, unsigned* ticket,
-                                                      double* hout) {
-  if (sc->active == 0) return;
-  int lo, hi;
-  chunk(n, lo, hi);
-  dots_tail(V, ldv, nk, w, lo, hi, partial, ticket, hout);
-}
-
-// w -= sum_k h1_k V_k; h2 = V^T w  (the first CGS2 update fused with the second dots)
-template <class TV>
-__global__ void __launch_bounds__(RED_THREADS) k_update_dots(const Scalars* sc, const TV* V, size_t ldv, int nk,
-                                                             double* w, int n, const double* hin, double* partial,
-                                                             unsigned* ticket, double* hout) {
-  if (sc->active == 0) return;
-  __shared__ double h[MAX_KRYLOV + 1];
-  if (threadIdx.x < nk) h[threadIdx.x] = hin[threadIdx.x];
-  __syncthreads();
-  int lo, hi;
-  chunk(n, lo, hi);
-  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-    double s = 0.0;
-    for (int k = 0; k < nk; ++k) s += h[k] * double(V[k * ldv + i]);
-    w[i] = w[i] - s;
-  }
-  dots_tail(V, ldv, nk, w, lo, hi, partial, ticket, hout);
-}
-
-// w -= sum_k h2_k V_k; |w|; column j of H; 1/|w| for the next vector
-template <class TV>
-__global__ void __launch_bounds__(RED_THREADS) k_update_norm(Scalars* sc, const TV* V, size_t ldv, int nk, double* w,
-                                                             int n, int j, int m, double* partial, unsigned* ticket) {
-  if (sc->active == 0) return;
-  __shared__ double h[MAX_KRYLOV + 1];
-  if (threadIdx.x < nk) h[threadIdx.x] = sc->h2[threadIdx.x];
-  __syncthreads();
-  int lo, hi;
-  chunk(n, lo, hi);
-  double acc[1] = {0.0};
-  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-    double s = 0.0;
-    for (int k = 0; k < nk; ++k) s += h[k] * double(V[k * ldv + i]);
-    double wi = w[i] - s;
-    w[i] = wi;
-    acc[0] += wi * wi;
-  }
-  if (reduce_last<1>(acc, partial, ticket)) {
-    double nrm = sqrt(acc[0]);
-    for (int k = 0; k < nk; ++k) sc->H[k + (m + 1) * j] = sc->h1[k] + sc->h2[k];
-    sc->H[j + 1 + (m + 1) * j] = nrm;
-    sc->nrm = nrm;
-    sc->inv_nrm = 1.0 / fmax(nrm, 2.2250738585072014e-308);
-    if (nrm == 0.0) sc->status |= ST_GMRES_BREAKDOWN;
-  }
-}
-
 // argmin |beta e1 - H y| by Givens rotations, pivots below rcond * the largest dropped
-// (krylov.py:100-137); hy = H y
-__global__ void k_lstsq(Scalars* sc, int m) {
+// (krylov.py:100-137); hy = H y.  One CTA: rotation j, once formed, is applied to rows
+// j, j+1 of every later column at once -- each entry sees the same rotations in the
+// same order as column-by-column elimination.
+__global__ void __launch_bounds__(64) k_lstsq(Scalars* sc, int m) {
   if (sc->active == 0) return;
-  const double rcond = 2.220446049250313e-16 * (m + 1);
-  double h[MAX_KRYLOV + 1][MAX_KRYLOV];  // local copy (m small)
-  double g[MAX_KRYLOV + 1], cs[MAX_KRYLOV], sn[MAX_KRYLOV];
-  for (int i = 0; i <= m; ++i)
-    for (int j = 0; j < m; ++j) h[i][j] = sc->H[i + (m + 1) * j];
-  g[0] = sc->beta;
-  for (int i = 1; i <= m; ++i) g[i] = 0.0;
+  __shared__ double h[MAX_KRYLOV + 1][MAX_KRYLOV + 1];
+  __shared__ double g[MAX_KRYLOV + 1], cs[MAX_KRYLOV], sn[MAX_KRYLOV], y[MAX_KRYLOV];
+  __shared__ double largest;
+  const int t = threadIdx.x;
+  for (int e = t; e < (m + 1) * m; e += blockDim.x) {
+    int i = e % (m + 1), jj = e / (m + 1);
+    h[i][jj] = sc->H[e];
+  }
+  if (t <= m) g[t] = t == 0 ? sc->beta : 0.0;
+  __syncthreads();
   for (int j = 0; j < m; ++j) {
-    for (int i = 0; i < j; ++i) {
-      double a = h[i][j], c = h[i + 1][j];
-      h[i][j] = cs[i] * a + sn[i] * c;
-      h[i + 1][j] = cs[i] * c - sn[i] * a;
+    if (t == 0) {
+      double a = h[j][j], c = h[j + 1][j];
+      double r = sqrt(a * a + c * c);
+      double safe = r > 0.0 ? r : 1.0;
+      double cj = r > 0.0 ? a / safe : 1.0, sj = r > 0.0 ? c / safe : 0.0;
+      cs[j] = cj;
+      sn[j] = sj;
+      h[j][j] = r;
+      h[j + 1][j] = 0.0;
+      double gj = g[j];
+      g[j] = cj * gj;
+      g[j + 1] = -sj * gj;
     }
-    double a = h[j][j], c = h[j + 1][j];
-    double r = sqrt(a * a + c * c);
-    double safe = r > 0.0 ? r : 1.0;
-    cs[j] = r > 0.0 ? a / safe : 1.0;
-    sn[j] = r > 0.0 ? c / safe : 0.0;
-    h[j][j] = r;
-    h[j + 1][j] = 0.0;
-    double gj = g[j];
-    g[j] = cs[j] * gj;
-    g[j + 1] = -sn[j] * gj;
+    __syncthreads();
+    for (int col = j + 1 + t; col < m; col += blockDim.x) {
+      double a = h[j][col], c = h[j + 1][col];
+      h[j][col] = cs[j] * a + sn[j] * c;
+      h[j + 1][col] = cs[j] * c - sn[j] * a;
+    }
+    __syncthreads();
   }
-  double largest = fabs(h[0][0]);
-  for (int j = 1; j < m; ++j) largest = fmax(largest, fabs(h[j][j]));
-  double y[MAX_KRYLOV];
+  if (t == 0) {
+    double l = fabs(h[0][0]);
+    for (int jj = 1; jj < m; ++jj) l = fmax(l, fabs(h[jj][jj]));
+    largest = l;
+  }
+  __syncthreads();
+  const double rcond = 2.220446049250313e-16 * (m + 1);
   for (int j = m - 1; j >= 0; --j) {
-    double rest = g[j];
-    for (int k = j + 1; k < m; ++k) rest = rest - h[j][k] * y[k];
-    bool keep = fabs(h[j][j]) > rcond * largest;
-    y[j] = keep ? rest / h[j][j] : 0.0;
+    if (t < 32) {
+      double s = 0.0;
+      for (int k = j + 1 + t; k < m; k += 32) s += h[j][k] * y[k];
+      s = warp_sum(s);
+      if (t == 0) {
+        double rest = g[j] - s;
+        bool keep = fabs(h[j][j]) > rcond * largest;
+        y[j] = keep ? rest / h[j][j] : 0.0;
+      }
+    }
+    __syncthreads();
   }
-  for (int j = 0; j < m; ++j) sc->y[j] = y[j];
-  for (int i = 0; i <= m; ++i) {
+  if (t < m) sc->y[t] = y[t];
+  if (t <= m) {
     double s = 0.0;
-    for (int j = 0; j < m; ++j) s += sc->H[i + (m + 1) * j] * y[j];
-    sc->hy[i] = s;
+    for (int jj = 0; jj < m; ++jj) s += sc->H[t + (m + 1) * jj] * y[jj];
+    sc->hy[t] = s;
   }
 }
 
@@ -258,15 +272,19 @@ template <class TV>
 __global__ void k_combine(const Scalars* sc, const TV* V, size_t ldv, int m, const double* w, double* tmp,
                           double* action, int n) {
   if (sc->active == 0) return;
+  __shared__ double y[MAX_KRYLOV], hy[MAX_KRYLOV + 1];
+  if ((int)threadIdx.x < m) y[threadIdx.x] = sc->y[threadIdx.x];
+  if ((int)threadIdx.x <= m) hy[threadIdx.x] = sc->hy[threadIdx.x];
+  __syncthreads();
   const double inv = sc->inv_nrm;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     double s = 0.0, a = 0.0;
     for (int k = 0; k < m; ++k) {
       double v = double(V[k * ldv + i]);
-      s += sc->y[k] * v;
-      a += sc->hy[k] * v;
+      s += y[k] * v;
+      a += hy[k] * v;
     }
-    a += sc->hy[m] * double(TV(w[i] * inv));
+    a += hy[m] * double(TV(w[i] * inv));
     tmp[i] = s;
     action[i] += a;
   }
@@ -385,25 +403,40 @@ __global__ void k_update(const Scalars* sc, double* U, const double* dU, int n) 
 
 // ---- launch wrappers ------------------------------------------------------------------
 
-int reduce_blocks(int n) { return max(1, min(2 * 148, (n + 1023) / 1024)); }
+// blocks of the basis passes (and the largest block count any reduction uses)
+int reduce_blocks(int n) { return max(2 * 148, (n + RED_THREADS * MD_E - 1) / (RED_THREADS * MD_E)); }
+
+static int chunk_blocks(int n) { return max(1, min(2 * 148, (n + 1023) / 1024)); }
 
 void launch_gmres_init(Scalars* sc, const double* R, double* b, double* x, double* action, double* r, int n,
                        const double* tile_partial, int n_tiles, double volume_sum, double* history, Reduce red,
                        cudaStream_t st) {
-  k_gmres_init<<<reduce_blocks(n), RED_THREADS, 0, st>>>(sc, R, b, x, action, r, n, tile_partial, n_tiles,
-                                                         volume_sum, history, red.partial, red.ticket);
+  k_gmres_init<<<chunk_blocks(n), RED_THREADS, 0, st>>>(sc, R, b, x, action, r, n, tile_partial, n_tiles, volume_sum,
+                                                        history, red.partial, red.ticket);
 }
 
 void launch_cycle_start(Scalars* sc, Config cfg, cudaStream_t st) { k_cycle_start<<<1, 1, 0, st>>>(sc, cfg); }
 
+template <class TV, int NK>
+static void arnoldi_nk(Scalars* sc, const TV* V, size_t ldv, int j, int m, double* w, int n, Reduce red,
+                       cudaStream_t st) {
+  int blocks = (n + RED_THREADS * MD_E - 1) / (RED_THREADS * MD_E);
+  k_mdot<TV, NK, 0><<<blocks, RED_THREADS, 0, st>>>(sc, V, ldv, j + 1, w, n, nullptr, red.partial, red.ticket,
+                                                     sc->h1, j, m);
+  k_mdot<TV, NK, 1><<<blocks, RED_THREADS, 0, st>>>(sc, V, ldv, j + 1, w, n, sc->h1, red.partial, red.ticket,
+                                                     sc->h2, j, m);
+  k_mdot<TV, NK, 2><<<blocks, RED_THREADS, 0, st>>>(sc, V, ldv, j + 1, w, n, sc->h2, red.partial, red.ticket,
+                                                     nullptr, j, m);
+}
+
 template <class TV>
 static void arnoldi_t(Scalars* sc, const TV* V, size_t ldv, int j, int m, double* w, int n, Reduce red,
                       cudaStream_t st) {
-  int blocks = reduce_blocks(n);
-  k_dots<TV><<<blocks, RED_THREADS, 0, st>>>(sc, V, ldv, j + 1, w, n, red.partial, red.ticket, sc->h1);
-  k_update_dots<TV><<<blocks, RED_THREADS, 0, st>>>(sc, V, ldv, j + 1, w, n, sc->h1, red.partial, red.ticket,
-                                                    sc->h2);
-  k_update_norm<TV><<<blocks, RED_THREADS, 0, st>>>(sc, V, ldv, j + 1, w, n, j, m, red.partial, red.ticket);
+  const int nk = j + 1;
+  if (nk <= 8) arnoldi_nk<TV, 8>(sc, V, ldv, j, m, w, n, red, st);
+  else if (nk <= 16) arnoldi_nk<TV, 16>(sc, V, ldv, j, m, w, n, red, st);
+  else if (nk <= 32) arnoldi_nk<TV, 32>(sc, V, ldv, j, m, w, n, red, st);
+  else arnoldi_nk<TV, 64>(sc, V, ldv, j, m, w, n, red, st);
 }
 
 void launch_arnoldi_orth(Scalars* sc, const void* V, bool fp32, size_t ldv, int j, int m, double* w, int n,
@@ -412,7 +445,7 @@ void launch_arnoldi_orth(Scalars* sc, const void* V, bool fp32, size_t ldv, int 
   else arnoldi_t<double>(sc, (const double*)V, ldv, j, m, w, n, red, st);
 }
 
-void launch_lstsq(Scalars* sc, int m, cudaStream_t st) { k_lstsq<<<1, 1, 0, st>>>(sc, m); }
+void launch_lstsq(Scalars* sc, int m, cudaStream_t st) { k_lstsq<<<1, 64, 0, st>>>(sc, m); }
 
 void launch_combine(const Scalars* sc, const void* V, bool fp32, size_t ldv, int m, const double* w, double* tmp,
                     double* action, int n, cudaStream_t st) {
@@ -423,14 +456,14 @@ void launch_combine(const Scalars* sc, const void* V, bool fp32, size_t ldv, int
 
 void launch_cycle_end(Scalars* sc, double* x, const double* z, const double* b, const double* action, double* r,
                       int n, Reduce red, cudaStream_t st) {
-  k_cycle_end<<<reduce_blocks(n), RED_THREADS, 0, st>>>(sc, x, z, b, action, r, n, red.partial, red.ticket);
+  k_cycle_end<<<chunk_blocks(n), RED_THREADS, 0, st>>>(sc, x, z, b, action, r, n, red.partial, red.ticket);
 }
 
 void launch_newton_update(Scalars* sc, const Canvas& c, const Physics& P, Config cfg, double* U, const double* dU,
                           const double* action, const double* R, Reduce red, cudaStream_t st) {
   int N = c.NI * c.NJ, n = c.nvar * N;
-  k_relax<<<reduce_blocks(N), RED_THREADS, 0, st>>>(sc, c, P, cfg, U, dU, red.partial, red.ticket);
-  k_accept<<<reduce_blocks(n), RED_THREADS, 0, st>>>(sc, c, P, cfg, U, dU, action, R, red.partial, red.ticket);
+  k_relax<<<chunk_blocks(N), RED_THREADS, 0, st>>>(sc, c, P, cfg, U, dU, red.partial, red.ticket);
+  k_accept<<<chunk_blocks(n), RED_THREADS, 0, st>>>(sc, c, P, cfg, U, dU, action, R, red.partial, red.ticket);
   k_update<<<min((n + 255) / 256, 148 * 4), 256, 0, st>>>(sc, U, dU, n);
 }
 

@@ -3,19 +3,24 @@
 // through the C-grid wake cut), with the first-order Rusanov approximate Jacobian
 //   diag  = sum_f lambda_f (1/CFL + 1/2) I
 //   off   = 1/2 A(U_nb, S_out) - 1/2 lambda_f I
-// for the mean flow, and scalar chains for the SA row.  Each chain is factored and
-// solved exactly; one thread owns one chain and runs the block Thomas recurrence (the
-// reference's cyclic reduction gives the same solve to round-off).  Factor rows are
-// stored row-major across chains, [(k * E + e) * n_chains + c], so a warp's loads of one
-// row are coalesced.  TF is the factor's type (double; float in the mixed form).
+// for the mean flow (4x4 blocks), and scalar chains for the SA row.
+//
+// Each chain is factored and solved by block cyclic reduction, the reference's own
+// algorithm (src/jaxrans/core/linalg.py:159-200): ceil(log2 L) levels, each eliminating
+// the even rows of a block-tridiagonal system and leaving one on the odd rows.  One CTA
+// owns one chain and its threads own rows, so a solve is 2 log2(L) short barriers
+// instead of 2L dependent steps.  A chain's factor lives in global memory (L2 resident
+// at these sizes), level after level: for the even rows the inverse of the diagonal and
+// the off-diagonal blocks, for the odd rows the multipliers alpha and gamma; entries are
+// stored [entry][row] so a level's loads are coalesced.  TF is the factor's type
+// (double; float in the mixed form).
 #include "device.cuh"
 
 namespace jr {
 
-constexpr int FLOW_E = 48;   // lower, pivot inverse, c_hat: 3 x 16
-constexpr int SA_E = 3;      // the scalar chain's lower, pivot inverse, c_hat
+constexpr int LS_THREADS = 128;
 
-// A = d(F.S)/dU (4x4, [row][col]): columns by forward-mode tangents of the flux of the
+// A = d(F.S)/dU (4x4, [row][col]) by forward-mode tangents of the flux of the
 // conservative state (physics/euler.py:55-71)
 __device__ __forceinline__ void flux_jacobian(const double* q, double sx, double sy, double g, double A[4][4]) {
   double U[4];
@@ -64,6 +69,38 @@ template <class S> __device__ __forceinline__ void invert4(const S M[4][4], S In
     for (int c = 0; c < 4; ++c) Inv[r][c] = a[r][4 + c];
 }
 
+template <class S> __device__ __forceinline__ void mm4(const S A[4][4], const S B[4][4], S C[4][4]) {
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      S s = A[r][0] * B[0][c];
+#pragma unroll
+      for (int t = 1; t < 4; ++t) s = s + A[r][t] * B[t][c];
+      C[r][c] = s;
+    }
+}
+
+template <class S> __device__ __forceinline__ void mv4(const S A[4][4], const S* x, S* y) {
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    S s = A[r][0] * x[0];
+#pragma unroll
+    for (int t = 1; t < 4; ++t) s = s + A[r][t] * x[t];
+    y[r] = s;
+  }
+}
+
+// block (16 entries) of row r in an [entry][row] array of `rows` rows
+template <class S> __device__ __forceinline__ void load4(const S* base, int rows, int r, S B[4][4]) {
+#pragma unroll
+  for (int e = 0; e < 16; ++e) B[e >> 2][e & 3] = base[(size_t)e * rows + r];
+}
+template <class S> __device__ __forceinline__ void store4(S* base, int rows, int r, const S B[4][4]) {
+#pragma unroll
+  for (int e = 0; e < 16; ++e) base[(size_t)e * rows + r] = B[e >> 2][e & 3];
+}
+
 __device__ __forceinline__ void face_vector(const Canvas& cv, int f, double& sx, double& sy) {
   const int nfi = cv.nfi();
   if (f < nfi) {
@@ -105,72 +142,51 @@ __device__ __forceinline__ void coupling(const Canvas& cv, const Physics& P, con
     for (int c = 0; c < 4; ++c) B[r][c] = 0.5 * A[r][c] - (r == c ? 0.5 * l : 0.0);
 }
 
+// Sizes of the cyclic-reduction levels of a chain of length L: level l has n_l rows,
+// ne = ceil(n/2) even and no = n/2 odd; n_{l+1} = no.  The flow factor of level l is
+// 3*16*ne + 2*16*no entries (inverse, lower, upper of the evens; alpha, gamma of the
+// odds); after the last level one inverse (16).  The SA factor is the same in scalars.
+__device__ __forceinline__ int level_rows(int L, int level) {
+  int n = L;
+  for (int k = 0; k < level; ++k) n >>= 1;
+  return n;
+}
+
+// ------------------------------------------------------------------------------------
+// Factor: assemble the chain blocks (rows in parallel), then reduce level by level.
+// scratch holds the level's reduced system (a, d, c: 3 x 16 x rows) and the next one's.
+// ------------------------------------------------------------------------------------
 template <class TF, bool SA>
-__global__ void k_chain_factor(Canvas cv, Physics P, const double* __restrict__ U, const double* __restrict__ lam,
-                               const double* __restrict__ mflux, const double* __restrict__ dflux,
-                               const double* __restrict__ dflow, const double* __restrict__ dsa,
-                               TF* __restrict__ fflow, TF* __restrict__ fsa) {
-  const int n = cv.n_chains;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n) return;
-  const int len = cv.ch_len[c];
-  const int N = cv.ncanvas();
-  TF Cp[4][4];
-#pragma unroll
-  for (int r = 0; r < 4; ++r)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) Cp[r][q] = TF(0);
-  TF cps = TF(0);
-  for (int k = 0; k < len; ++k) {
+__global__ void __launch_bounds__(LS_THREADS) k_cr_factor(Canvas cv, Physics P, const double* __restrict__ U,
+                                                          const double* __restrict__ lam,
+                                                          const double* __restrict__ mflux,
+                                                          const double* __restrict__ dflux,
+                                                          const double* __restrict__ dflow,
+                                                          const double* __restrict__ dsa, TF* __restrict__ fflow,
+                                                          TF* __restrict__ fsa, TF* __restrict__ scratch) {
+  const int c = blockIdx.x, n = cv.n_chains;
+  const int L = cv.ch_len[c];
+  TF* F = fflow + (size_t)cv.ch_fbase[c] * 80;   // flow factor: <= 80 entries per row
+  TF* Fs = fsa + (size_t)cv.ch_fbase[c] * 5;     // SA factor: <= 5 scalars per row
+  TF* s0 = scratch + (size_t)cv.ch_fbase[c] * 104;   // two level systems: 3*16*L + 3*16*L/2 (+ SA)
+  TF* A0 = s0;                 // a, d, c of the current level: 3 x 16 x L
+  TF* A1 = s0 + (size_t)48 * L;   // the next level's: 3 x 16 x L/2
+  TF* S0 = A1 + (size_t)48 * ((L + 1) / 2);   // SA scalars, current: 3 x L
+  TF* S1 = S0 + (size_t)3 * L;                // SA, next: 3 x L/2
+  // 1. the blocks of every row
+  for (int k = threadIdx.x; k < L; k += blockDim.x) {
     const int cell = cv.ch_cells[k * n + c];
     double Lb[4][4], Ub[4][4];
-    if (k > 0) {
-      coupling(cv, P, U, lam, cv.ch_down_sign[(k - 1) * n + c], cv.ch_down_face[(k - 1) * n + c],
-               cv.ch_cells[(k - 1) * n + c], Lb);
-    } else {
-      coupling(cv, P, U, lam, 0, 0, 0, Lb);
-    }
-    if (k + 1 < len) {
-      coupling(cv, P, U, lam, cv.ch_up_sign[k * n + c], cv.ch_up_face[k * n + c], cv.ch_cells[(k + 1) * n + c],
-               Ub);
-    } else {
-      coupling(cv, P, U, lam, 0, 0, 0, Ub);
-    }
+    coupling(cv, P, U, lam, k > 0 ? cv.ch_down_sign[(k - 1) * n + c] : 0,
+             k > 0 ? cv.ch_down_face[(k - 1) * n + c] : 0, k > 0 ? cv.ch_cells[(k - 1) * n + c] : 0, Lb);
+    coupling(cv, P, U, lam, k + 1 < L ? cv.ch_up_sign[k * n + c] : 0, k + 1 < L ? cv.ch_up_face[k * n + c] : 0,
+             k + 1 < L ? cv.ch_cells[(k + 1) * n + c] : 0, Ub);
     const double d = dflow[cell];
-    TF M[4][4], Pv[4][4], Cn[4][4], Lt[4][4], Ut[4][4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        Lt[r][q] = TF(Lb[r][q]);
-        Ut[r][q] = TF(Ub[r][q]);
-      }
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        TF s = TF(0);
-#pragma unroll
-        for (int t = 0; t < 4; ++t) s = s + Lt[r][t] * Cp[t][q];
-        M[r][q] = (r == q ? TF(d) : TF(0)) - s;
-      }
-    invert4(M, Pv);
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        TF s = TF(0);
-#pragma unroll
-        for (int t = 0; t < 4; ++t) s = s + Pv[r][t] * Ut[t][q];
-        Cn[r][q] = s;
-      }
-    TF* row = fflow + (size_t)k * FLOW_E * n + c;
 #pragma unroll
     for (int e = 0; e < 16; ++e) {
-      row[(size_t)e * n] = Lt[e / 4][e % 4];
-      row[(size_t)(16 + e) * n] = Pv[e / 4][e % 4];
-      row[(size_t)(32 + e) * n] = Cn[e / 4][e % 4];
-      Cp[e / 4][e % 4] = Cn[e / 4][e % 4];
+      A0[(size_t)e * L + k] = TF(Lb[e >> 2][e & 3]);
+      A0[(size_t)(16 + e) * L + k] = TF((e >> 2) == (e & 3) ? d : 0.0);
+      A0[(size_t)(32 + e) * L + k] = TF(Ub[e >> 2][e & 3]);
     }
     if constexpr (SA) {
       double ls = 0.0, us = 0.0;
@@ -178,139 +194,320 @@ __global__ void k_chain_factor(Canvas cv, Physics P, const double* __restrict__ 
         int sg = cv.ch_down_sign[(k - 1) * n + c], f = cv.ch_down_face[(k - 1) * n + c];
         if (sg != 0) ls = -(fmax(-sg * mflux[f], 0.0) + dflux[f]) / U[cv.ch_cells[(k - 1) * n + c]];
       }
-      if (k + 1 < len) {
+      if (k + 1 < L) {
         int sg = cv.ch_up_sign[k * n + c], f = cv.ch_up_face[k * n + c];
         if (sg != 0) us = -(fmax(-sg * mflux[f], 0.0) + dflux[f]) / U[cv.ch_cells[(k + 1) * n + c]];
       }
-      TF ps = TF(1) / (TF(dsa[cell]) - TF(ls) * cps);
-      TF cs = ps * TF(us);
-      TF* srow = fsa + (size_t)k * SA_E * n + c;
-      srow[0] = TF(ls);
-      srow[(size_t)n] = ps;
-      srow[(size_t)2 * n] = cs;
-      cps = cs;
+      S0[k] = TF(ls);
+      S0[L + k] = TF(dsa[cell]);
+      S0[2 * L + k] = TF(us);
     }
-    (void)N;
+  }
+  __syncthreads();
+  // 2. the levels
+  int rows = L;
+  size_t off = 0, offs = 0;
+  TF *cur = A0, *nxt = A1, *scur = S0, *snxt = S1;
+  while (rows > 1) {
+    const int ne = (rows + 1) / 2, no = rows / 2;
+    TF* inv = F + off;                    // [16][ne]
+    TF* low = inv + (size_t)16 * ne;      // [16][ne]
+    TF* upp = low + (size_t)16 * ne;      // [16][ne]
+    TF* alp = upp + (size_t)16 * ne;      // [16][no]
+    TF* gam = alp + (size_t)16 * no;      // [16][no]
+    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+      TF D[4][4], I[4][4], B[4][4];
+      load4(cur + (size_t)16 * rows, rows, 2 * e, D);
+      invert4(D, I);
+      store4(inv, ne, e, I);
+      load4(cur, rows, 2 * e, B);
+      store4(low, ne, e, B);
+      load4(cur + (size_t)32 * rows, rows, 2 * e, B);
+      store4(upp, ne, e, B);
+      if constexpr (SA) {
+        TF* sf = Fs + offs;
+        sf[e] = TF(1) / scur[rows + 2 * e];            // inverse
+        sf[ne + e] = scur[2 * e];                      // lower
+        sf[2 * ne + e] = scur[2 * rows + 2 * e];       // upper
+      }
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < no; o += blockDim.x) {
+      TF Ao[4][4], Co[4][4], I0[4][4], al[4][4], ga[4][4], T[4][4], X[4][4];
+      load4(cur, rows, 2 * o + 1, Ao);
+      load4(inv, ne, o, I0);
+      mm4(Ao, I0, al);
+      load4(cur + (size_t)32 * rows, rows, 2 * o + 1, Co);
+      const bool has_next = o + 1 < ne;
+      if (has_next) {
+        TF I1[4][4];
+        load4(inv, ne, o + 1, I1);
+        mm4(Co, I1, ga);
+      } else {
+#pragma unroll
+        for (int e = 0; e < 16; ++e) ga[e >> 2][e & 3] = TF(0);
+      }
+      store4(alp, no, o, al);
+      store4(gam, no, o, ga);
+      // the odd row's new lower, diagonal and upper blocks
+      TF lw[4][4], up[4][4], Dn[4][4];
+      load4(low, ne, o, lw);
+      mm4(al, lw, T);
+#pragma unroll
+      for (int e = 0; e < 16; ++e) X[e >> 2][e & 3] = -T[e >> 2][e & 3];
+      store4(nxt, no, o, X);
+      load4(cur + (size_t)16 * rows, rows, 2 * o + 1, Dn);
+      load4(upp, ne, o, up);
+      mm4(al, up, T);
+#pragma unroll
+      for (int e = 0; e < 16; ++e) Dn[e >> 2][e & 3] = Dn[e >> 2][e & 3] - T[e >> 2][e & 3];
+      if (has_next) {
+        load4(low, ne, o + 1, lw);
+        mm4(ga, lw, T);
+#pragma unroll
+        for (int e = 0; e < 16; ++e) Dn[e >> 2][e & 3] = Dn[e >> 2][e & 3] - T[e >> 2][e & 3];
+        load4(upp, ne, o + 1, up);
+        mm4(ga, up, T);
+#pragma unroll
+        for (int e = 0; e < 16; ++e) X[e >> 2][e & 3] = -T[e >> 2][e & 3];
+      } else {
+#pragma unroll
+        for (int e = 0; e < 16; ++e) X[e >> 2][e & 3] = TF(0);
+      }
+      store4(nxt + (size_t)16 * no, no, o, Dn);
+      store4(nxt + (size_t)32 * no, no, o, X);
+      if constexpr (SA) {
+        TF* sf = Fs + offs;
+        TF* sal = sf + 3 * ne;
+        TF* sga = sal + no;
+        TF a_ = scur[2 * o + 1] * sf[o];
+        TF g_ = has_next ? scur[2 * rows + 2 * o + 1] * sf[o + 1] : TF(0);
+        sal[o] = a_;
+        sga[o] = g_;
+        snxt[o] = -(a_ * sf[ne + o]);
+        TF dn = scur[rows + 2 * o + 1] - a_ * sf[2 * ne + o];
+        if (has_next) dn = dn - g_ * sf[ne + o + 1];
+        snxt[no + o] = dn;
+        snxt[2 * no + o] = has_next ? -(g_ * sf[2 * ne + o + 1]) : TF(0);
+      }
+    }
+    __syncthreads();
+    off += (size_t)48 * ne + (size_t)32 * no;
+    offs += (size_t)3 * ne + (size_t)2 * no;
+    TF* t = cur;
+    cur = nxt;
+    nxt = t;
+    TF* ts = scur;
+    scur = snxt;
+    snxt = ts;
+    rows = no;
+  }
+  if (threadIdx.x == 0) {
+    TF D[4][4], I[4][4];
+    load4(cur + 16, 1, 0, D);   // rows == 1: the diagonal block at entries 16..31
+    invert4(D, I);
+    store4(F + off, 1, 0, I);
+    if constexpr (SA) Fs[offs] = TF(1) / scur[1];
   }
 }
 
-// z = M^-1 (scale * r); with `vout`, also vout = scale * r (the normalised Arnoldi vector).
-// Threads past the chains copy the cells on no chain (z = scale * r there).
+// ------------------------------------------------------------------------------------
+// Apply: z = M^-1 (scale * r) on one chain per CTA.  With `vout`, the scaled input is
+// also written there (the normalised Arnoldi vector).  The right-hand side of every
+// level is kept in shared memory for the back substitution.
+// ------------------------------------------------------------------------------------
 template <class TF, class TV, bool SA>
-__global__ void k_chain_apply(Canvas cv, const TF* __restrict__ fflow, const TF* __restrict__ fsa,
-                              const double* __restrict__ r, const double* __restrict__ scale_ptr,
-                              const int* __restrict__ skip, TV* __restrict__ vout, double* __restrict__ z) {
+__global__ void __launch_bounds__(LS_THREADS) k_cr_apply(Canvas cv, const TF* __restrict__ fflow,
+                                                         const TF* __restrict__ fsa, const double* __restrict__ r,
+                                                         const double* __restrict__ scale_ptr,
+                                                         const int* __restrict__ skip, TV* __restrict__ vout,
+                                                         double* __restrict__ z) {
   if (skip != nullptr && *skip == 0) return;
-  const int n = cv.n_chains;
-  const int N = cv.ncanvas();
-  const int nv = cv.nvar;
+  const int N = cv.ncanvas(), nv = cv.nvar, n = cv.n_chains;
   const double scale = scale_ptr != nullptr ? *scale_ptr : 1.0;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) {
-    t -= n;
-    const int stride = gridDim.x * blockDim.x - n;
-    for (int e = t; e < cv.n_offchain; e += stride) {
+  if ((int)blockIdx.x >= n) {
+    // the cells on no chain: z = scale * r
+    const int stride = (gridDim.x - n) * blockDim.x;
+    for (int e = (blockIdx.x - n) * blockDim.x + threadIdx.x; e < cv.n_offchain; e += stride) {
       int idx = cv.offchain[e];
       for (int v = 0; v < nv; ++v) {
         double b = scale * r[v * N + idx];
-        if (vout != nullptr) vout[v * N + idx] = TV(b);
-        z[v * N + idx] = vout != nullptr ? double(TV(b)) : b;
+        if (vout != nullptr) {
+          TV bv = TV(b);
+          vout[v * N + idx] = bv;
+          b = double(bv);
+        }
+        z[v * N + idx] = b;
       }
     }
     return;
   }
-  const int c = t;
-  const int len = cv.ch_len[c];
-  TF d[4] = {TF(0), TF(0), TF(0), TF(0)};
-  TF ds = TF(0);
-  for (int k = 0; k < len; ++k) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int c = blockIdx.x;
+  const int L = cv.ch_len[c];
+  TF* bs = reinterpret_cast<TF*>(smem_raw);   // [level-concatenated rows][5]
+  const TF* F = fflow + (size_t)cv.ch_fbase[c] * 80;
+  const TF* Fs = fsa + (size_t)cv.ch_fbase[c] * 5;
+  // gather the right-hand side
+  for (int k = threadIdx.x; k < L; k += blockDim.x) {
     const int cell = cv.ch_cells[k * n + c];
-    TF b[5];
     for (int v = 0; v < nv; ++v) {
-      double x = scale * r[v * N + cell];
+      double b = scale * r[v * N + cell];
       if (vout != nullptr) {
-        TV xv = TV(x);
-        vout[v * N + cell] = xv;
-        x = double(xv);
+        TV bv = TV(b);
+        vout[v * N + cell] = bv;
+        b = double(bv);
       }
-      b[v] = TF(x);
-    }
-    const TF* row = fflow + (size_t)k * FLOW_E * n + c;
-    TF t4[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      TF s = TF(0);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) s = s + row[(size_t)(i * 4 + j) * n] * d[j];
-      t4[i] = b[i] - s;
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      TF s = TF(0);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) s = s + row[(size_t)(16 + i * 4 + j) * n] * t4[j];
-      d[i] = s;
-    }
-    for (int v = 0; v < 4; ++v) z[v * N + cell] = double(d[v]);
-    if constexpr (SA) {
-      const TF* srow = fsa + (size_t)k * SA_E * n + c;
-      ds = srow[(size_t)n] * (b[4] - srow[0] * ds);
-      z[4 * N + cell] = double(ds);
+      bs[k * 5 + v] = TF(b);
     }
   }
-  TF x[4] = {TF(0), TF(0), TF(0), TF(0)};
-  TF xs = TF(0);
-  for (int k = len - 1; k >= 0; --k) {
+  __syncthreads();
+  // reduce: b_odd <- b_odd - alpha b_even - gamma b_next_even, level by level
+  int rows = L;
+  size_t off = 0, offs = 0, boff = 0;
+  while (rows > 1) {
+    const int ne = (rows + 1) / 2, no = rows / 2;
+    const TF* alp = F + off + (size_t)48 * ne;
+    const TF* gam = alp + (size_t)16 * no;
+    TF* b = bs + boff * 5;
+    TF* bn = bs + (boff + rows) * 5;
+    for (int o = threadIdx.x; o < no; o += blockDim.x) {
+      TF al[4][4], ga[4][4], t[4], u[4];
+      load4(alp, no, o, al);
+      load4(gam, no, o, ga);
+      TF be[4], bo[4], bx[4];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        be[v] = b[(2 * o) * 5 + v];
+        bo[v] = b[(2 * o + 1) * 5 + v];
+        bx[v] = 2 * o + 2 < rows ? b[(2 * o + 2) * 5 + v] : TF(0);
+      }
+      mv4(al, be, t);
+      mv4(ga, bx, u);
+#pragma unroll
+      for (int v = 0; v < 4; ++v) bn[o * 5 + v] = bo[v] - t[v] - u[v];
+      if constexpr (SA) {
+        const TF* sal = Fs + offs + 3 * ne;
+        const TF* sga = sal + no;
+        TF bx4 = 2 * o + 2 < rows ? b[(2 * o + 2) * 5 + 4] : TF(0);
+        bn[o * 5 + 4] = b[(2 * o + 1) * 5 + 4] - sal[o] * b[(2 * o) * 5 + 4] - sga[o] * bx4;
+      }
+    }
+    __syncthreads();
+    off += (size_t)48 * ne + (size_t)32 * no;
+    offs += (size_t)3 * ne + (size_t)2 * no;
+    boff += rows;
+    rows = no;
+  }
+  // the last row, then substitute back level by level; x of a level overwrites its b
+  if (threadIdx.x == 0) {
+    TF* b = bs + boff * 5;
+    TF I[4][4], x[4];
+    load4(F + off, 1, 0, I);
+    mv4(I, b, x);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) b[v] = x[v];
+    if constexpr (SA) b[4] = Fs[offs] * b[4];
+  }
+  __syncthreads();
+  // walk the levels back: recompute their offsets from the top
+  int depth = 0;
+  for (int m = L; m > 1; m >>= 1) ++depth;
+  for (int lev = depth - 1; lev >= 0; --lev) {
+    int rws = L;
+    size_t of = 0, ofs = 0, bo_ = 0;
+    for (int k = 0; k < lev; ++k) {
+      int ne_ = (rws + 1) / 2, no_ = rws / 2;
+      of += (size_t)48 * ne_ + (size_t)32 * no_;
+      ofs += (size_t)3 * ne_ + (size_t)2 * no_;
+      bo_ += rws;
+      rws = no_;
+    }
+    const int ne = (rws + 1) / 2, no = rws / 2;
+    const TF* inv = F + of;
+    const TF* low = inv + (size_t)16 * ne;
+    const TF* upp = low + (size_t)16 * ne;
+    TF* b = bs + bo_ * 5;           // this level's right-hand side; becomes its solution
+    const TF* x = bs + (bo_ + rws) * 5;   // the next level's solution (the odd rows)
+    // evens from the odd solution; the odds copied into place after a barrier
+    TF xe[4 * 4];   // up to 4 even rows per thread kept in registers when rows <= 4*threads
+    TF xs[4];
+    int cnt = 0;
+    for (int e = threadIdx.x; e < ne; e += blockDim.x, ++cnt) {
+      TF I[4][4], lw[4][4], up[4][4], t[4], u[4], w[4], res[4];
+      load4(inv, ne, e, I);
+      load4(low, ne, e, lw);
+      load4(upp, ne, e, up);
+      TF xp[4], xn[4];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        xp[v] = e >= 1 ? x[(e - 1) * 5 + v] : TF(0);
+        xn[v] = e < no ? x[e * 5 + v] : TF(0);
+      }
+      mv4(lw, xp, t);
+      mv4(up, xn, u);
+#pragma unroll
+      for (int v = 0; v < 4; ++v) w[v] = b[(2 * e) * 5 + v] - t[v] - u[v];
+      mv4(I, w, res);
+#pragma unroll
+      for (int v = 0; v < 4; ++v) xe[cnt * 4 + v] = res[v];
+      if constexpr (SA) {
+        const TF* si = Fs + ofs;
+        TF xps = e >= 1 ? x[(e - 1) * 5 + 4] : TF(0);
+        TF xns = e < no ? x[e * 5 + 4] : TF(0);
+        xs[cnt] = si[e] * (b[(2 * e) * 5 + 4] - si[ne + e] * xps - si[2 * ne + e] * xns);
+      }
+    }
+    __syncthreads();
+    cnt = 0;
+    for (int e = threadIdx.x; e < ne; e += blockDim.x, ++cnt) {
+#pragma unroll
+      for (int v = 0; v < 4; ++v) b[(2 * e) * 5 + v] = xe[cnt * 4 + v];
+      if constexpr (SA) b[(2 * e) * 5 + 4] = xs[cnt];
+    }
+    for (int o = threadIdx.x; o < no; o += blockDim.x)
+      for (int v = 0; v < 5; ++v) b[(2 * o + 1) * 5 + v] = x[o * 5 + v];
+    __syncthreads();
+  }
+  // scatter
+  for (int k = threadIdx.x; k < L; k += blockDim.x) {
     const int cell = cv.ch_cells[k * n + c];
-    const TF* row = fflow + (size_t)k * FLOW_E * n + c;
-    TF nx[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      TF s = TF(0);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) s = s + row[(size_t)(32 + i * 4 + j) * n] * x[j];
-      nx[i] = TF(z[i * N + cell]) - s;
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      x[i] = nx[i];
-      z[i * N + cell] = double(nx[i]);
-    }
-    if constexpr (SA) {
-      const TF* srow = fsa + (size_t)k * SA_E * n + c;
-      xs = TF(z[4 * N + cell]) - srow[(size_t)2 * n] * xs;
-      z[4 * N + cell] = double(xs);
-    }
+    for (int v = 0; v < nv; ++v) z[v * N + cell] = double(bs[k * 5 + v]);
   }
 }
+
+size_t cr_apply_smem(const Canvas& c, bool fp32) { return (size_t)2 * c.L * 5 * (fp32 ? 4 : 8) + 64; }
 
 template <class TF>
 void launch_chain_factor_t(const Canvas& c, const Physics& P, bool sa, const double* U, const double* lam,
                            const double* mflux, const double* dflux, const double* dflow, const double* dsa,
-                           void* fflow, void* fsa, cudaStream_t st) {
-  int blocks = (c.n_chains + 63) / 64;
+                           void* fflow, void* fsa, void* scratch, cudaStream_t st) {
   if (sa)
-    k_chain_factor<TF, true><<<blocks, 64, 0, st>>>(c, P, U, lam, mflux, dflux, dflow, dsa, (TF*)fflow, (TF*)fsa);
+    k_cr_factor<TF, true><<<c.n_chains, LS_THREADS, 0, st>>>(c, P, U, lam, mflux, dflux, dflow, dsa, (TF*)fflow,
+                                                            (TF*)fsa, (TF*)scratch);
   else
-    k_chain_factor<TF, false><<<blocks, 64, 0, st>>>(c, P, U, lam, mflux, dflux, dflow, dsa, (TF*)fflow, (TF*)fsa);
+    k_cr_factor<TF, false><<<c.n_chains, LS_THREADS, 0, st>>>(c, P, U, lam, mflux, dflux, dflow, dsa, (TF*)fflow,
+                                                             (TF*)fsa, (TF*)scratch);
 }
 
 void launch_chain_factor(const Canvas& c, const Physics& P, bool sa, bool fp32, const double* U, const double* lam,
                          const double* mflux, const double* dflux, const double* dflow, const double* dsa,
-                         void* fflow, void* fsa, cudaStream_t st) {
-  if (fp32) launch_chain_factor_t<float>(c, P, sa, U, lam, mflux, dflux, dflow, dsa, fflow, fsa, st);
-  else launch_chain_factor_t<double>(c, P, sa, U, lam, mflux, dflux, dflow, dsa, fflow, fsa, st);
+                         void* fflow, void* fsa, void* scratch, cudaStream_t st) {
+  if (fp32) launch_chain_factor_t<float>(c, P, sa, U, lam, mflux, dflux, dflow, dsa, fflow, fsa, scratch, st);
+  else launch_chain_factor_t<double>(c, P, sa, U, lam, mflux, dflux, dflow, dsa, fflow, fsa, scratch, st);
 }
 
 template <class TF, class TV>
 static void apply_t(const Canvas& c, bool sa, const void* fflow, const void* fsa, const double* r, const double* scale,
                     const int* skip, TV* vout, double* z, cudaStream_t st) {
-  int threads = c.n_chains + 1024;
-  int blocks = (threads + 63) / 64;
+  int extra = max(1, min(64, (c.n_offchain + LS_THREADS - 1) / LS_THREADS));
+  size_t smem = cr_apply_smem(c, sizeof(TF) == 4);
   if (sa)
-    k_chain_apply<TF, TV, true><<<blocks, 64, 0, st>>>(c, (const TF*)fflow, (const TF*)fsa, r, scale, skip, vout, z);
+    k_cr_apply<TF, TV, true><<<c.n_chains + extra, LS_THREADS, smem, st>>>(c, (const TF*)fflow, (const TF*)fsa, r,
+                                                                           scale, skip, vout, z);
   else
-    k_chain_apply<TF, TV, false><<<blocks, 64, 0, st>>>(c, (const TF*)fflow, (const TF*)fsa, r, scale, skip, vout, z);
+    k_cr_apply<TF, TV, false><<<c.n_chains + extra, LS_THREADS, smem, st>>>(c, (const TF*)fflow, (const TF*)fsa, r,
+                                                                            scale, skip, vout, z);
 }
 
 void launch_chain_apply(const Canvas& c, bool sa, bool fp32, const void* fflow, const void* fsa, const double* r,
@@ -322,6 +519,18 @@ void launch_chain_apply(const Canvas& c, bool sa, bool fp32, const void* fflow, 
     if (vout_fp32) apply_t<double, float>(c, sa, fflow, fsa, r, scale, skip, (float*)vout, z, st);
     else apply_t<double, double>(c, sa, fflow, fsa, r, scale, skip, (double*)vout, z, st);
   }
+}
+
+void configure_line_kernels(const Canvas& c) {
+  size_t s8 = cr_apply_smem(c, false), s4 = cr_apply_smem(c, true);
+  cudaFuncSetAttribute(k_cr_apply<double, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s8);
+  cudaFuncSetAttribute(k_cr_apply<double, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s8);
+  cudaFuncSetAttribute(k_cr_apply<double, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s8);
+  cudaFuncSetAttribute(k_cr_apply<double, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s8);
+  cudaFuncSetAttribute(k_cr_apply<float, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s4);
+  cudaFuncSetAttribute(k_cr_apply<float, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s4);
+  cudaFuncSetAttribute(k_cr_apply<float, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s4);
+  cudaFuncSetAttribute(k_cr_apply<float, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s4);
 }
 
 }  // namespace jr
