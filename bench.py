@@ -1,0 +1,313 @@
+#!/usr/bin/env python3
+"""Benchmark: converged RANS solves per hour on one B200 (or N replicas).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload c_sa_385] [--precision fp64|mixed]
+
+A step is one converged solve of the workload (``jaxrans_b200.workloads``; by default
+the 2D SA-noft2 NACA 4412 C-grid 385 x 97, Roe + MUSCL minmod, GMRES(30)) from the
+freestream, stopped by the reference's own exit test.  ``value`` times the solves with
+the start state already in HBM (a device-to-device restart); ``e2e`` times them through
+the C ABI from a pinned host state, the final state and forces read back each solve.
+With N GPUs each rank runs its own replica of the same solves (the cases are
+independent: no collective on the data path) and the whole-job rate is reported.
+
+``--impl reference`` times the CPU restatement of the reference (``oracle``; the
+reference itself is JAX, absent here) on a bounded sample of the same workload: each
+step one Newton step, extrapolated by the number of Newton steps a converged solve takes.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+for _p in (ROOT, ROOT / "jax-rans_b200"):
+    if str(_p) not in sys.path:
+        sys.path.insert(0, str(_p))
+
+import numpy as np  # noqa: E402
+
+METRIC = "converged RANS solves/hr"
+# Newton steps of one converged solve of each workload, measured on the device path (the
+# bench line's config.newton_steps_per_solve); the reference arm's sample is scaled by it.
+STEPS_PER_SOLVE = {"c_sa_385": 940, "o_euler_257": 3840}
+# algorithmic bytes per cell of one J.v tile launch: U, v and w (nvar each), V/dt, the
+# volume, the two face vectors a cell owns (4 doubles), the centre (2), the wall distance
+# (SA only), all FP64
+def jvp_bytes_per_cell(nvar: int) -> int:
+    return 8 * (3 * nvar + 1 + 1 + 4 + 2 + (1 if nvar == 5 else 0))
+
+
+def rank_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in getattr(self, "lines", []):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.is_file():
+        return {**json.loads(path.read_text()), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+def profiled_traffic(workload: str):
+    """dram bytes per launch of the J.v tile from the committed ncu summary, if any."""
+    path = ROOT / "profiles" / f"jvp_tile_{workload}.txt"
+    if not path.is_file():
+        return None
+    for ln in path.read_text().splitlines():
+        if ln.startswith("dram_bytes_per_launch:"):
+            return float(ln.split(":", 1)[1].split()[0])
+    return None
+
+
+def reference_sample(case, plan, steps: int, warmup: int, precision: str):
+    """Newton steps of the CPU restatement (the oracle) from the freestream."""
+    from jaxrans_b200.config import freestream_primitive
+    from oracle import implicit as im
+    from oracle import numerics as nm
+    flow, num = case.flow, case.numerics
+    model = nm.Model(plan, np.array(freestream_primitive(flow)), flow.gamma, num.flux, num.limiter, num.kappa,
+                     None if flow.inviscid else flow.mu_inf, flow.sutherland_ratio, flow.turbulence is not None,
+                     0.3 if flow.turbulence == "sa_noft2_qcr" else 0.0, num.far_field, plan.distance)
+    state = im.NewtonState(nm.initial_state(model), case.implicit.cfl, float("inf"))
+    times = []
+    with np.errstate(all="ignore"):
+        for k in range(warmup + steps):
+            t = time.perf_counter()
+            state, _ = im.newton_step(state, model, case.implicit)
+            if k >= warmup:
+                times.append(time.perf_counter() - t)
+    return times
+
+
+def run_reference(args) -> int:
+    rank, _, world = rank_info()
+    if rank != 0:
+        return 0
+    from jaxrans_b200.workloads import workload
+    case = workload(args.workload, **{"implicit.precision": args.precision})
+    plan = case.grid()
+    times = reference_sample(case, plan, args.steps, args.warmup, args.precision)
+    per_step = statistics.mean(times)
+    n = STEPS_PER_SOLVE[args.workload]
+    value = 3600.0 / (per_step * n)
+    sample = (f"{args.steps} Newton steps of the oracle (NumPy FP64, complex-step J.v) from the freestream on "
+              f"the {args.workload} case after {args.warmup} warm-up steps, {per_step:.2f} s each, scaled by "
+              f"{n} Newton steps per converged solve")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/hr", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * per_step * n,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (generated NACA section and grid)",
+            "config": {"workload": args.workload, "cells": plan.cells, "newton_steps_per_solve": n},
+            "cpu_baseline": {"value": value, "unit": "solves/hr", "cores": 1, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "solves/hr", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_device(args) -> int:
+    import torch
+    rank, local, world = rank_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from jaxrans_b200.build import build
+    from jaxrans_b200.solver import device_for, freestream_state, run_blocks
+    from jaxrans_b200.workloads import workload
+    build()
+    case = workload(args.workload, **{"implicit.precision": args.precision})
+    plan = case.grid()
+    dev = device_for(case, plan)
+    U0 = freestream_state(case, plan)
+    U0_pinned = torch.from_numpy(U0).pin_memory()
+    U0_dev = U0_pinned.to("cuda")
+    stream = torch.cuda.ExternalStream(dev.stream_handle())
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB > L2
+    torch.cuda.synchronize()
+    kps = dev.kernels_per_step()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def device_solve():
+        dev.set_state_device(U0_dev, case.implicit.cfl)
+        return run_blocks(case, dev)
+
+    def host_solve():
+        dev.set_state(U0_pinned.numpy(), case.implicit.cfl)
+        out = run_blocks(case, dev)
+        U, _, _, _ = dev.get_state()
+        return out, U
+
+    for _ in range(args.warmup):
+        device_solve()
+    # timed: device-resident restarts
+    starts, ends, solves = [], [], []
+    with Clocks(local) as clocks:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            torch.cuda.synchronize()
+            barrier()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            solves.append(device_solve())
+            e.record(stream)
+            torch.cuda.synchronize()
+            starts.append(s)
+            ends.append(e)
+    per_solve = [s.elapsed_time(e) / 1e3 for s, e in zip(starts, ends)]
+    total = sum(per_solve)
+    # e2e: host state in, state and forces out, through the C ABI
+    e2e_times = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        torch.cuda.synchronize()
+        barrier()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        out, U = host_solve()
+        e.record(stream)
+        torch.cuda.synchronize()
+        e2e_times.append(s.elapsed_time(e) / 1e3)
+    e2e_total = sum(e2e_times)
+    if dist is not None:
+        t = torch.tensor([total, e2e_total], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total, e2e_total = float(t[0]), float(t[1])
+    value = 3600.0 * args.steps * world / total
+    e2e_value = 3600.0 * args.steps * world / e2e_total
+    iters = [int(b.residual.size) for b in solves]
+    blocks = [int(b.blocks) for b in solves]
+    launches = sum(i * kps + b * 2 for i, b in zip(iters, blocks))
+    kern = dev.time_kernels(20)
+    peaks = measured_peaks()
+    nvar = case.flow.nvar
+    bpc = jvp_bytes_per_cell(nvar)
+    achieved = bpc * plan.cells / (kern["jvp_tile"] * 1e-3) / 1e9
+    traffic = profiled_traffic(args.workload)
+    result = {
+        "metric": METRIC, "value": value, "unit": "solves/hr", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32",
+        "data": "synthetic (generated NACA section and grid, freestream start)",
+        "config": {"workload": args.workload, "cells": plan.cells, "canvas": list(plan.shape), "nvar": nvar,
+                   "precision": args.precision, "newton_steps_per_solve": int(np.median(iters)),
+                   "exit_reasons": sorted({b.reason for b in solves}), "l2": "flushed (256 MB write) per step",
+                   "parallelism": f"replicas x{world}",
+                   "forces": {"cl": solves[-1].last_forces.cl, "cd": solves[-1].last_forces.cd,
+                              "cm": solves[-1].last_forces.cm}},
+        "latency_s": {"p50": float(np.percentile(per_solve, 50)), "p99": float(np.percentile(per_solve, 99))},
+        "e2e": {"value": e2e_value, "unit": "solves/hr", "h2d_bytes_per_step": int(U0.nbytes),
+                "d2h_bytes_per_step": int(U0.nbytes + sum(b.blocks for b in [out]) * 8 * (case.block_iters + 6))},
+        "gpu_launches": launches,
+        "roofline": {"kernel": "jvp_tile", "bound": "hbm", "achieved": achieved,
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                     "traffic": None if traffic is None else traffic,
+                     "algorithmic_bytes_per_launch": bpc * plan.cells, "launch_ms": kern["jvp_tile"],
+                     "peak_source": peaks.get("source", "measured")},
+        "kernel_ms": kern,
+    }
+    if rank == 0:
+        with Clocks(local) as _:
+            pass
+        result["clocks"] = clocks.summary()
+        if world == 1 and not args.no_cpu_baseline:
+            times = reference_sample(case, plan, 1, 0, args.precision)
+            per_step = times[0]
+            n = int(np.median(iters))
+            result["cpu_baseline"] = {
+                "value": 3600.0 / (per_step * n), "unit": "solves/hr", "cores": 1, "kind": "port",
+                "sample": (f"one Newton step of the oracle (NumPy FP64, complex-step J.v) from the freestream, "
+                           f"{per_step:.2f} s, scaled by the {n} Newton steps of a converged solve")}
+        print(json.dumps(result), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    dev.close()
+    return 0
+
+
+def main(argv=None) -> int:
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=("b200", "reference"))
+    p.add_argument("--workload", default="c_sa_385", choices=sorted(STEPS_PER_SOLVE))
+    p.add_argument("--precision", default="fp64", choices=("fp64", "mixed"))
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    args = p.parse_args(argv)
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be at least 3")
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_device(args)
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -111,6 +111,12 @@ double* jr_state_device(jr_plan* plan);
 int jr_state_set_device(jr_plan* plan, const double* U_device, double cfl, double residual_norm);
 /* Kernels launched by one captured Newton step (the graph's kernel nodes). */
 int jr_graph_kernels(jr_plan* plan, int64_t* kernels_per_step);
+/* Average device time (ms, CUDA events on the plan's stream, reps launches each, after one
+ * untimed launch) of the hot kernels at the plan's state, out[0..5]: the residual tile, the
+ * J.v tile, the tangent ghost fill, the line-solve apply, the line factor, and one CGS2
+ * orthogonalisation against the full basis (three passes).  Replaces the timing loop of
+ * the reference's scripts/benchmark.py:40-47,88-108 for these pieces. */
+int jr_time_kernels(jr_plan* plan, int32_t reps, double* ms_out);
 
 /* n_steps pseudo-transient Newton steps on the plan's state, one captured CUDA graph per
  * step; history (host, n_steps) receives |R| before each step.  Synchronises once.

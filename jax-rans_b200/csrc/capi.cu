@@ -556,6 +556,53 @@ int jr_newton_steps(jr_plan* plan, int32_t n_steps, double* history) {
   return cuda_check("jr_newton_steps");
 }
 
+int jr_time_kernels(jr_plan* plan, int32_t reps, double* ms) {
+  if (!plan || !ms || reps < 1) return fail(JR_EINVAL, "bad argument");
+  jr_plan* p = plan;
+  const Canvas& c = p->cv;
+  const bool sa = c.nvar == 5;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  // a consistent state for every kernel: base ghosts, wave speeds, the factor, an
+  // active Krylov cycle with z = the residual
+  launch_ghosts(c, p->P, false, p->U, nullptr, p->qg, nullptr, nullptr, p->st);
+  launch_residual(c, p->P, p->visc, true, p->U, p->qg, p->R, p->tile_partial, p->st);
+  launch_faces(c, p->P, p->visc, p->U, p->lam, p->mflux, p->dflux, p->st);
+  launch_cells(c, p->P, p->visc, p->U, p->lam, p->mflux, p->dflux, p->sc, p->vdt, p->dflow, p->dsa, p->st);
+  launch_chain_factor(c, p->P, sa, p->mixed, p->U, p->lam, p->mflux, p->dflux, p->dflow, p->dsa, p->fflow, p->fsa,
+                      p->scratch, p->st);
+  cudaMemcpyAsync(p->z, p->R, (size_t)p->n_vec * sizeof(double), cudaMemcpyDeviceToDevice, p->st);
+  int one = 1;
+  cudaMemcpyAsync(&p->sc->active, &one, sizeof(int), cudaMemcpyHostToDevice, p->st);
+  cudaStreamSynchronize(p->st);
+  auto timed = [&](int k, auto&& launch) {
+    launch();
+    cudaEventRecord(e0, p->st);
+    for (int r = 0; r < reps; ++r) launch();
+    cudaEventRecord(e1, p->st);
+    cudaEventSynchronize(e1);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    ms[k] = (double)t / reps;
+  };
+  timed(0, [&] { launch_residual(c, p->P, p->visc, true, p->U, p->qg, p->R, p->tile_partial, p->st); });
+  timed(1, [&] { launch_jvp(c, p->P, p->visc, p->U, p->qg, p->z, p->dqg, p->vdt, p->w, nullptr, p->st); });
+  timed(2, [&] { launch_ghosts(c, p->P, true, p->U, p->z, p->qg, p->dqg, nullptr, p->st); });
+  timed(3, [&] {
+    launch_chain_apply(c, sa, p->mixed, p->fflow, p->fsa, p->R, nullptr, nullptr, nullptr, false, p->tmp, p->st);
+  });
+  timed(4, [&] {
+    launch_chain_factor(c, p->P, sa, p->mixed, p->U, p->lam, p->mflux, p->dflux, p->dflow, p->dsa, p->fflow, p->fsa,
+                        p->scratch, p->st);
+  });
+  timed(5, [&] { launch_arnoldi_orth(p->sc, p->V, p->mixed, (size_t)p->n_vec, p->m - 1, p->m, p->w, p->n_vec,
+                                     p->red, p->st); });
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return cuda_check("jr_time_kernels");
+}
+
 int jr_forces(jr_plan* plan, const double* U, double* out) {
   if (!plan || !out) return fail(JR_EINVAL, "null argument");
   const double* u = U ? U : plan->U;

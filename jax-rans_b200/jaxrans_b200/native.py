@@ -59,7 +59,9 @@ class PlanDesc(C.Structure):
 EXPORTS = ("jr_plan_create", "jr_plan_destroy", "jr_last_error", "jr_plan_sizes", "jr_plan_stream",
            "jr_synchronize", "jr_residual", "jr_jvp", "jr_wave_speeds", "jr_precond_factor", "jr_precond_apply",
            "jr_state_set", "jr_state_get", "jr_state_device", "jr_newton_steps", "jr_newton_steps_async",
-           "jr_forces", "jr_state_set_device", "jr_graph_kernels")
+           "jr_forces", "jr_state_set_device", "jr_graph_kernels", "jr_time_kernels")
+
+TIMED_KERNELS = ("residual_tile", "jvp_tile", "ghosts_tangent", "line_apply", "line_factor", "cgs2_full_basis")
 
 _LIB = None
 
@@ -99,6 +101,7 @@ def load_library(path: Path | None = None) -> C.CDLL:
         "jr_forces": (C.c_int, [vp, vp, vp]),
         "jr_state_set_device": (C.c_int, [vp, vp, C.c_double, C.c_double]),
         "jr_graph_kernels": (C.c_int, [vp, C.POINTER(C.c_int64)]),
+        "jr_time_kernels": (C.c_int, [vp, C.c_int32, _f64p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -306,6 +309,13 @@ class DevicePlan:
         n = C.c_int64()
         _check(self.lib, self.lib.jr_graph_kernels(self.handle, C.byref(n)), "jr_graph_kernels")
         return int(n.value)
+
+    def time_kernels(self, reps: int = 20) -> dict:
+        """Average ms per launch of the hot kernels at the current state (CUDA events
+        on the plan's stream)."""
+        out = np.zeros(len(TIMED_KERNELS))
+        _check(self.lib, self.lib.jr_time_kernels(self.handle, int(reps), _ptr(out, _f64p)), "jr_time_kernels")
+        return dict(zip(TIMED_KERNELS, out.tolist()))
 
     def stream_handle(self) -> int:
         return int(self.lib.jr_plan_stream(self.handle) or 0)

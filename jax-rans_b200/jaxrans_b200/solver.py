@@ -146,6 +146,65 @@ def device_for(case: Case, plan: Plan):
                       tuple(spec.moment_centre[:2]))
 
 
+@dataclass
+class Blocks:
+    """What ``run_blocks`` returns: the history, the exit reason, the force monitor."""
+
+    residual: np.ndarray
+    reason: str
+    cl_history: np.ndarray
+    coefficients: np.ndarray
+    last_forces: Forces
+    seconds: float
+    first_block: float
+    blocks: int
+
+
+def run_blocks(case: Case, dev, max_iters=None, progress=None) -> Blocks:
+    """Blocks of ``block_iters`` Newton steps from the device's current state until the
+    exit test of ``src/jaxrans/solvers/driver.py:123-201`` stops the case."""
+    num = case.numerics
+    block_iters = case.block_iters
+    max_iters = num.max_iters if max_iters is None else max_iters
+    n_blocks = max(1, -(-max_iters // block_iters))
+    blocks, cl_history, coefficients = [], [], []
+    peak, reason = 0.0, ExitReason.MAX_ITERS
+    started = time.perf_counter()
+    first_block = float("nan")
+    f = None
+    for b in range(n_blocks):
+        hist = dev.newton_steps(block_iters)
+        if b == 0:
+            first_block = time.perf_counter() - started
+        blocks.append(hist)
+        f = forces_of(dev.forces())
+        cl_history.append(f.cl)
+        coefficients.append((f.cl, f.cd, f.cm))
+        finite = hist[np.isfinite(hist)]
+        if finite.size:
+            peak = max(peak, float(finite.max()))
+        if progress is not None:
+            last = float(hist[-1])
+            orders = float(np.log10(peak / last)) if peak > 0 and last > 0 else 0.0
+            progress((b + 1) * block_iters, last, orders, f)
+        stop = num.forces_tol is not None and all(cl_spread(h) < num.forces_tol
+                                                  for h in np.transpose(coefficients))
+        last = hist[-1]
+        failed = not np.all(np.isfinite(hist)) or not np.all(np.isfinite([f.cl, f.cd, f.cm]))
+        if failed:
+            reason = ExitReason.NON_FINITE
+        elif peak > 0 and last <= num.tol * peak:
+            reason = ExitReason.CONVERGED
+        elif len(hist) > 1 and np.all(hist == hist[0]):
+            reason = ExitReason.STALLED
+        elif stop:
+            reason = ExitReason.SETTLED
+        if reason != ExitReason.MAX_ITERS:
+            break
+    return Blocks(np.concatenate(blocks), reason, np.asarray(cl_history), np.asarray(coefficients), f,
+                  time.perf_counter() - started, first_block, len(blocks))
+
+
 def march(case: Case, plan: Plan, progress=None, initial=None, device=None, max_iters=None) -> Result:
     """One grid to steady state from the freestream, or from ``initial`` on the block cells."""
     num = case.numerics

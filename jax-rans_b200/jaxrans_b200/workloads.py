@@ -12,9 +12,11 @@ on a GPU box and in the oracle.
   cells round the airfoil, 64 along each wake side, 96 normal), first cell 1e-6 chord with
   a normal growth starting at 1.1 and rising linearly to reach the far field at 50
   chords, Re 6e6, M 0.2, alpha 8 deg, Roe with MUSCL minmod, 5 variables, GMRES restart
-  30, steps bounded to 20 % relative change.  Converged when the residual has dropped
-  1e-10 below its peak or CL, CD and CM have each settled within 1e-7 over the last
-  quarter of the run (a force change far below the 0.1 drag-count tolerance).
+  30, steps bounded to 20 % relative change.  With minmod the SA solution on this grid
+  settles onto a limiter limit cycle about two orders below its peak residual, so a solve
+  ends by the reference's own exit test with its own defaults: converged at 1e-12 of the
+  peak, or settled once CL, CD and CM each vary by less than 1e-4 over the last quarter
+  of the run.
 """
 
 from __future__ import annotations
@@ -44,7 +46,7 @@ WORKLOADS = {
         {"convective_fluxes": {"riemann_solver": "roe", "limiter": "minmod"},
          "time_integration": {"solver": "implicit"},
          "implicit": {"krylov_subspace": 30, "max_relative_update": 0.2},
-         "convergence": {"max_iters": 8000, "tol": 1e-10, "forces_tol": 1e-7, "block_iters": 20}},
+         "convergence": {"max_iters": 8000, "tol": 1e-12, "forces_tol": 1e-4, "block_iters": 20}},
     ),
 }
 
