@@ -39,7 +39,7 @@ import numpy as np  # noqa: E402
 METRIC = "converged RANS solves/hr"
 # Newton steps of one converged solve of each workload, measured on the device path (the
 # bench line's config.newton_steps_per_solve); the reference arm's sample is scaled by it.
-STEPS_PER_SOLVE = {"c_sa_385": 940, "o_euler_257": 3840}
+STEPS_PER_SOLVE = {"c_sa_385": 620, "o_euler_257": 3840}
 # algorithmic bytes per cell of one J.v tile launch: U, v and w (nvar each), V/dt, the
 # volume, the two face vectors a cell owns (4 doubles), the centre (2), the wall distance
 # (SA only), all FP64

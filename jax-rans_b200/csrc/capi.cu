@@ -249,6 +249,14 @@ int jr_plan_create(const jr_plan_desc* d, jr_plan** out) {
     TRY(dev_copy(plan, (int**)&c.g_kind[s], d->kind[s], (size_t)n));
     TRY(dev_copy(plan, (double**)&c.g_geom[s], d->geom[s], (size_t)4 * n));
   }
+  {
+    // stage 2 reads stage-1 ghosts at the corners: which stage-1 record fills each source
+    std::vector<int> rec_of(N, -1), src_rec(d->n_ghost[1], -1);
+    for (int k = 0; k < d->n_ghost[0]; ++k) rec_of[d->ghost[0][k]] = k;
+    for (int k = 0; k < d->n_ghost[1]; ++k)
+      if (!d->interior[d->source[1][k]]) src_rec[k] = rec_of[d->source[1][k]];
+    TRY(dev_copy(plan, (int**)&c.g_src_rec, src_rec.data(), src_rec.size()));
+  }
   c.n_walls = d->n_walls;
   TRY(dev_copy(plan, (int**)&c.w_cell, d->wall_cell, (size_t)d->n_walls));
   TRY(dev_copy(plan, (int**)&c.w_family, d->wall_family, (size_t)d->n_walls));

@@ -10,10 +10,11 @@
 namespace jr {
 
 constexpr int MAX_KRYLOV = 64;   // largest GMRES subspace
-constexpr int TILE_I = 15;       // residual tile: 15 x 16 cells, 256 threads
+constexpr int TILE_I = 7;        // residual tile: 7 x 16 cells, 128 threads (8 x 16 i-faces)
 constexpr int TILE_J = 16;
-constexpr int TILE_THREADS = 256;
-constexpr int GHOST_THREADS = 512;
+constexpr int TILE_THREADS = 128;
+constexpr int TILE_MIN_BLOCKS = 3;   // three CTAs per SM at <= 168 registers
+constexpr int GHOST_THREADS = 128;
 
 // Ghost-record kinds (the order the host plan uses)
 enum GhostKind { G_COPY = 0, G_SLIP = 1, G_NOSLIP = 2, G_SYMMETRY = 3, G_FARFIELD = 4, G_INFLOW = 5, G_OUTFLOW = 6 };
@@ -41,6 +42,7 @@ struct Canvas {
   const int* g_source[2];
   const int* g_kind[2];
   const double* g_geom[2];     // 4 per record: nx, ny, mx, my
+  const int* g_src_rec;        // stage 2: the stage-1 record that fills its source, or -1
   int n_walls;
   const int* w_cell;
   const int* w_family;

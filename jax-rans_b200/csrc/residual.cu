@@ -140,6 +140,21 @@ __device__ void condition(const Physics& P, int kind, const T* q, const double* 
   }
 }
 
+// the value a ghost record gives, from its source state
+template <class T>
+__device__ __forceinline__ void eval_record(const Canvas& c, const Physics& P, int s, int r, const T* q, T circ,
+                                            T* out) {
+  const int kind = c.g_kind[s][r];
+  if (kind == G_COPY) {
+    for (int v = 0; v < c.nvar; ++v) out[v] = q[v];
+  } else {
+    condition<T>(P, kind, q, c.g_geom[s] + 4 * r, circ, out);
+  }
+}
+
+// Both stages in one launch: a stage-2 record whose source is a stage-1 ghost (a
+// corner) evaluates that stage-1 record itself rather than reading it, so no record
+// waits on another and every CTA works independently.
 template <class T>
 __global__ void __launch_bounds__(GHOST_THREADS) k_ghosts(Canvas c, Physics P, const double* U, const double* V,
                                                           double* qg, double* dqg, const int* active) {
@@ -208,26 +223,27 @@ __global__ void __launch_bounds__(GHOST_THREADS) k_ghosts(Canvas c, Physics P, c
     __syncthreads();
     circ = circ_s;
   }
-  for (int s = 0; s < 2; ++s) {
-    const int n = c.n_ghost[s];
-    for (int r = threadIdx.x; r < n; r += blockDim.x) {
-      int src = c.g_source[s][r], ghost = c.g_ghost[s][r], kind = c.g_kind[s][r];
-      T q[5], out[5];
-      load_prim<T>(c, P, src, U, V, qg, dqg, q);
-      if (kind == G_COPY) {
-        for (int v = 0; v < c.nvar; ++v) out[v] = q[v];
+  const int n0 = c.n_ghost[0], total = n0 + c.n_ghost[1];
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int s = t < n0 ? 0 : 1, r = t < n0 ? t : t - n0;
+    T q[5], out[5];
+    const int r1 = s == 1 ? c.g_src_rec[r] : -1;
+    if (r1 >= 0) {
+      T q1[5];
+      load_prim<T>(c, P, c.g_source[0][r1], U, V, qg, dqg, q1);
+      eval_record<T>(c, P, 0, r1, q1, circ, q);
+    } else {
+      load_prim<T>(c, P, c.g_source[s][r], U, V, qg, dqg, q);
+    }
+    eval_record<T>(c, P, s, r, q, circ, out);
+    const int ghost = c.g_ghost[s][r];
+    for (int v = 0; v < c.nvar; ++v) {
+      if constexpr (sizeof(T) == sizeof(Dual)) {
+        dqg[v * N + ghost] = out[v].d;
       } else {
-        condition<T>(P, kind, q, c.g_geom[s] + 4 * r, circ, out);
-      }
-      for (int v = 0; v < c.nvar; ++v) {
-        if constexpr (sizeof(T) == sizeof(Dual)) {
-          dqg[v * N + ghost] = out[v].d;
-        } else {
-          qg[v * N + ghost] = out[v];
-        }
+        qg[v * N + ghost] = out[v];
       }
     }
-    __syncthreads();
   }
 }
 
@@ -402,7 +418,7 @@ template <> __device__ __forceinline__ double tangent_or_value<Dual>(const Dual&
 // T = double: out = R(U) (second or first order); partial[block] = sum vol R0^2.
 // T = Dual:   out = vdt * V + dR1/dU . V.
 template <class T, int NV, bool SECOND, int VISC>
-__global__ void __launch_bounds__(TILE_THREADS) k_residual(Canvas c, Physics P, const double* __restrict__ U,
+__global__ void __launch_bounds__(TILE_THREADS, TILE_MIN_BLOCKS) k_residual(Canvas c, Physics P, const double* __restrict__ U,
                                                           const double* __restrict__ qg, const double* __restrict__ V,
                                                           const double* __restrict__ dqg,
                                                           const double* __restrict__ vdt, double* __restrict__ out,
@@ -713,8 +729,9 @@ void launch_jvp(const Canvas& c, const Physics& P, int visc, const double* U, co
 
 void launch_ghosts(const Canvas& c, const Physics& P, bool dual, const double* U, const double* V, double* qg,
                    double* dqg, const int* active, cudaStream_t st) {
-  if (dual) k_ghosts<Dual><<<1, GHOST_THREADS, 0, st>>>(c, P, U, V, qg, dqg, active);
-  else k_ghosts<double><<<1, GHOST_THREADS, 0, st>>>(c, P, U, V, qg, dqg, active);
+  int blocks = max(1, (c.n_ghost[0] + c.n_ghost[1] + GHOST_THREADS - 1) / GHOST_THREADS);
+  if (dual) k_ghosts<Dual><<<blocks, GHOST_THREADS, 0, st>>>(c, P, U, V, qg, dqg, active);
+  else k_ghosts<double><<<blocks, GHOST_THREADS, 0, st>>>(c, P, U, V, qg, dqg, active);
 }
 
 void launch_faces(const Canvas& c, const Physics& P, int visc, const double* U, double* lam, double* mflux,

@@ -31,3 +31,11 @@ def cuda():
     if not gpu_available():
         pytest.skip("no CUDA device")
     return True
+
+
+@pytest.fixture(scope="session", autouse=True)
+def fresh_library(request):
+    """The C-ABI library rebuilt in place when a source is newer (nvcc is on the GPU box too)."""
+    if any(item.get_closest_marker("gpu") for item in request.session.items) and gpu_available():
+        from jaxrans_b200.build import build
+        build()
