@@ -79,6 +79,9 @@ const char* jr_last_error(void);
 int jr_plan_sizes(const jr_plan* plan, int64_t* n_canvas, int64_t* n_faces);
 /* The plan's CUDA stream (a cudaStream_t), for callers that order their own work on it. */
 void* jr_plan_stream(jr_plan* plan);
+/* Issue the plan's work on a caller's cudaStream_t (an XLA FFI handler passes XLA's);
+ * NULL returns to the plan's own stream.  The stream in use is drained first. */
+int jr_plan_set_stream(jr_plan* plan, void* stream);
 int jr_synchronize(jr_plan* plan);
 
 /* R(U): the residual on the canvas, where(interior, net flux, U - U_inf); second order,

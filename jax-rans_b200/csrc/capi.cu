@@ -79,7 +79,8 @@ struct jr_plan {
   int n_vec = 0;     // nvar * NI * NJ
   int n_faces = 0;
   int n_tiles = 0;
-  cudaStream_t st = nullptr;
+  cudaStream_t st = nullptr;             // the stream work is issued on
+  cudaStream_t owned_stream = nullptr;   // the plan's own stream
   std::vector<void*> allocs;
   double *U = nullptr, *qg = nullptr, *dqg = nullptr, *R = nullptr, *b = nullptr, *x = nullptr, *action = nullptr;
   double *r = nullptr, *w = nullptr, *z = nullptr, *tmp = nullptr, *zero = nullptr, *vdt = nullptr;
@@ -190,7 +191,7 @@ int jr_plan_destroy(jr_plan* plan) {
   if (plan->graph) cudaGraphExecDestroy(plan->graph);
   if (plan->st) cudaStreamSynchronize(plan->st);
   for (void* a : plan->allocs) cudaFree(a);
-  if (plan->st) cudaStreamDestroy(plan->st);
+  if (plan->owned_stream) cudaStreamDestroy(plan->owned_stream);
   delete plan;
   return JR_OK;
 }
@@ -211,7 +212,8 @@ int jr_plan_create(const jr_plan_desc* d, jr_plan** out) {
   plan->n_faces = (int)(nfi + nfj);
   plan->m = d->krylov_subspace;
   plan->mixed = d->precision == 1;
-  if (cudaStreamCreateWithFlags(&plan->st, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&plan->owned_stream, cudaStreamNonBlocking) == cudaSuccess) plan->st = plan->owned_stream;
+  if (plan->st == nullptr) {
     delete plan;
     return fail(JR_ECUDA, "cudaStreamCreate failed");
   }
@@ -413,6 +415,16 @@ int jr_plan_sizes(const jr_plan* plan, int64_t* n_canvas, int64_t* n_faces) {
 }
 
 void* jr_plan_stream(jr_plan* plan) { return plan ? (void*)plan->st : nullptr; }
+
+int jr_plan_set_stream(jr_plan* plan, void* stream) {
+  if (!plan) return fail(JR_EINVAL, "null plan");
+  if (cudaStreamSynchronize(plan->st) != cudaSuccess) return cuda_check("jr_plan_set_stream");
+  if (plan->owned_stream && plan->st != plan->owned_stream) {
+    // a caller's stream was in use: nothing to release
+  }
+  plan->st = stream != nullptr ? (cudaStream_t)stream : plan->owned_stream;
+  return JR_OK;
+}
 
 int jr_synchronize(jr_plan* plan) {
   if (!plan) return fail(JR_EINVAL, "null plan");

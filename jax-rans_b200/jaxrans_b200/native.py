@@ -59,7 +59,7 @@ class PlanDesc(C.Structure):
 EXPORTS = ("jr_plan_create", "jr_plan_destroy", "jr_last_error", "jr_plan_sizes", "jr_plan_stream",
            "jr_synchronize", "jr_residual", "jr_jvp", "jr_wave_speeds", "jr_precond_factor", "jr_precond_apply",
            "jr_state_set", "jr_state_get", "jr_state_device", "jr_newton_steps", "jr_newton_steps_async",
-           "jr_forces", "jr_state_set_device", "jr_graph_kernels", "jr_time_kernels")
+           "jr_forces", "jr_state_set_device", "jr_graph_kernels", "jr_time_kernels", "jr_plan_set_stream")
 
 TIMED_KERNELS = ("residual_tile", "jvp_tile", "ghosts_tangent", "line_apply", "line_factor", "cgs2_full_basis")
 
@@ -102,6 +102,7 @@ def load_library(path: Path | None = None) -> C.CDLL:
         "jr_state_set_device": (C.c_int, [vp, vp, C.c_double, C.c_double]),
         "jr_graph_kernels": (C.c_int, [vp, C.POINTER(C.c_int64)]),
         "jr_time_kernels": (C.c_int, [vp, C.c_int32, _f64p]),
+        "jr_plan_set_stream": (C.c_int, [vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
