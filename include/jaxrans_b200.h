@@ -1,9 +1,12 @@
 /* jaxrans_b200: the pseudo-transient Newton-Krylov hot path of JAX-RANS on NVIDIA B200.
  *
  * A C ABI (plain pointers and sizes) over hand-written sm_100a CUDA kernels.  A plan is
- * one case (one canvas: the grid's blocks and their ghost rings) with every static table
- * the kernels read, the device work buffers and the solver state.  Fields are
- * variable-major (nvar, NI*NJ) FP64 arrays, nvar = 4 (Euler, laminar) or 5 (SA).
+ * a batch of cases (each one canvas: the grid's blocks and their ghost rings) with every
+ * static table the kernels read, the device work buffers and the solver state; every
+ * launch advances all cases of the batch at once, and a single case is a batch of one.
+ * Fields are variable-major (nvar, NI*NJ) FP64 arrays, nvar = 4 (Euler, laminar) or 5
+ * (SA).  Arrays that span a batch hold the cases back to back in case order (a case's
+ * offsets from jr_case_sizes); for a single case they are that case's arrays.
  *
  * Every function returns 0 on success or a JR_E* code; jr_last_error() gives a message.
  * Functions taking device pointers run on the plan's stream and do not synchronise it
@@ -73,9 +76,30 @@ typedef struct jr_plan_desc {
 
 /* Build a plan (device copies of every table, work buffers, a stream). */
 int jr_plan_create(const jr_plan_desc* desc, jr_plan** out);
+/* A plan of n_cases cases advanced together (a polar of angles of attack, a batch of
+ * requests).  The cases may differ in grid, flow and CFL settings but must share nvar,
+ * viscous or not, precision, krylov_subspace, krylov_restarts and preconditioner.
+ * Replaces the jax.vmap of one Newton step over the freestreams of a polar
+ * (src/jaxrans/polar.py:80-121): each case keeps its own state, CFL ramp, rejections
+ * and history, and the cases never interact. */
+int jr_batch_create(const jr_plan_desc* descs, int32_t n_cases, jr_plan** out);
+int jr_plan_cases(const jr_plan* plan);
+/* Case c's canvas cells and face entries and its offsets in batch-long arrays (a field's
+ * offset is nvar * canvas_offset). */
+int jr_case_sizes(const jr_plan* plan, int32_t c, int64_t* n_canvas, int64_t* n_faces, int64_t* canvas_offset,
+                  int64_t* face_offset);
+/* Take case c out of (enabled 0) or back into (1) every launch: a free slot of a serving
+ * batch.  Its state and scalars stay as they are. */
+int jr_case_enable(jr_plan* plan, int32_t c, int32_t enabled);
+/* New freestream primitives q_inf (nvar values: rho, u, v, p[, nu_hat]) for case c: the
+ * far-field state and the freestream of the force coefficients.  Replaces at_alpha and
+ * freestream_primitive (src/jaxrans/polar.py:75-77, src/jaxrans/core/state.py:107-121):
+ * the angle of attack or Mach number enters the solver only through this vector. */
+int jr_case_set_inflow(jr_plan* plan, int32_t c, const double* q_inf);
 int jr_plan_destroy(jr_plan* plan);
 const char* jr_last_error(void);
-/* Number of canvas cells NI*NJ and of face entries (NI+1)*NJ + NI*(NJ+1). */
+/* Number of canvas cells NI*NJ and of face entries (NI+1)*NJ + NI*(NJ+1), summed over
+ * the cases of the plan. */
 int jr_plan_sizes(const jr_plan* plan, int64_t* n_canvas, int64_t* n_faces);
 /* The plan's CUDA stream (a cudaStream_t), for callers that order their own work on it. */
 void* jr_plan_stream(jr_plan* plan);
@@ -105,9 +129,14 @@ int jr_precond_factor(jr_plan* plan, const double* U, double cfl);
 int jr_precond_apply(jr_plan* plan, const double* r, double* z);
 
 /* The solver state: U (device or host copy in/out), CFL and the previous |R|.
- * Replaces ImplicitState (src/jaxrans/solvers/implicit.py:35-51). */
+ * Replaces ImplicitState (src/jaxrans/solvers/implicit.py:35-51).  jr_state_set gives
+ * every case the same CFL and |R|; jr_state_get fills one cfl, residual_norm and status
+ * per case (any may be NULL).  The jr_case_ forms read or write case c alone. */
 int jr_state_set(jr_plan* plan, const double* U_host, double cfl, double residual_norm);
 int jr_state_get(jr_plan* plan, double* U_host, double* cfl, double* residual_norm, int32_t* status);
+int jr_case_state_set(jr_plan* plan, int32_t c, const double* U_host, double cfl, double residual_norm);
+int jr_case_state_get(jr_plan* plan, int32_t c, double* U_host, double* cfl, double* residual_norm,
+                      int32_t* status);
 /* Device pointer to the plan's own state U (nvar x NI*NJ), valid until jr_plan_destroy. */
 double* jr_state_device(jr_plan* plan);
 /* The state from a device buffer (a restart with the inputs already in HBM). */
@@ -122,17 +151,18 @@ int jr_graph_kernels(jr_plan* plan, int64_t* kernels_per_step);
 int jr_time_kernels(jr_plan* plan, int32_t reps, double* ms_out);
 
 /* n_steps pseudo-transient Newton steps on the plan's state, one captured CUDA graph per
- * step; history (host, n_steps) receives |R| before each step.  Synchronises once.
+ * step for the whole batch; history (host, n_steps x n_cases, step-major) receives each
+ * case's |R| before each step.  Synchronises once.
  * Replaces make_newton_step (src/jaxrans/solvers/implicit.py:84-168) run as the
  * driver's block (src/jaxrans/solvers/driver.py:87-104). */
 int jr_newton_steps(jr_plan* plan, int32_t n_steps, double* history);
 
-/* The same step count without synchronising: history_device (n_steps doubles on the
- * device) receives the norms.  For timing with events on the plan's stream. */
+/* The same step count without synchronising: history_device (n_steps x n_cases doubles
+ * on the device) receives the norms.  For timing with events on the plan's stream. */
 int jr_newton_steps_async(jr_plan* plan, int32_t n_steps, double* history_device);
 
-/* Force coefficients at the plan's state (or at U if not NULL, a device pointer):
- * out (host) = cl, cd, cm, cd_friction, fx, fy.  Replaces force_coefficients
+/* Force coefficients at the plan's state (or at U if not NULL, a device pointer): out
+ * (host, 6 per case) = cl, cd, cm, cd_friction, fx, fy.  Replaces force_coefficients
  * (src/jaxrans/post/forces.py:108-161).  Synchronises. */
 int jr_forces(jr_plan* plan, const double* U, double* out);
 

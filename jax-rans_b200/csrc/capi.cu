@@ -1,5 +1,6 @@
-// The C ABI: plans (device copies of a case's static tables, work buffers, solver
-// state, a stream), the per-call entry points, and the Newton step as one CUDA graph.
+// The C ABI: plans (a batch of cases: device copies of each case's static tables, work
+// buffers and solver state, one stream), the per-call entry points, and the Newton step
+// of every case of the batch as one CUDA graph.  A single case is a batch of one.
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -10,88 +11,61 @@
 
 namespace jr {
 // residual.cu
-void launch_residual(const Canvas&, const Physics&, int visc, bool second, const double* U, const double* qg,
-                     double* R, double* partial, cudaStream_t);
-void launch_jvp(const Canvas&, const Physics&, int visc, const double* U, const double* qg, const double* V,
-                const double* dqg, const double* vdt, double* w, const int* active, cudaStream_t);
-void launch_ghosts(const Canvas&, const Physics&, bool dual, const double* U, const double* V, double* qg,
-                   double* dqg, const int* active, cudaStream_t);
-void launch_faces(const Canvas&, const Physics&, int visc, const double* U, double* lam, double* mflux,
-                  double* dflux, cudaStream_t);
-void launch_cells(const Canvas&, const Physics&, int visc, const double* U, const double* lam, const double* mflux,
-                  const double* dflux, const Scalars*, double* vdt, double* dflow, double* dsa, cudaStream_t);
+void launch_residual(const CaseDev*, const BatchDims&, int visc, bool second, int out_id, cudaStream_t);
+void launch_jvp(const CaseDev*, const BatchDims&, int visc, int tangent_id, int vdt_id, int out_id, int check_active,
+                cudaStream_t);
+void launch_ghosts(const CaseDev*, const BatchDims&, int tangent_id, int check_active, cudaStream_t);
+void launch_faces(const CaseDev*, const BatchDims&, int visc, cudaStream_t);
+void launch_cells(const CaseDev*, const BatchDims&, int visc, cudaStream_t);
 dim3 tile_grid(const Canvas&);
 void configure_kernels();
 // linesolve.cu
-void launch_chain_factor(const Canvas&, const Physics&, bool sa, bool fp32, const double* U, const double* lam,
-                         const double* mflux, const double* dflux, const double* dflow, const double* dsa, void* fflow,
-                         void* fsa, void* scratch, cudaStream_t);
-void configure_line_kernels(const Canvas&);
-void launch_chain_apply(const Canvas&, bool sa, bool fp32, const void* fflow, const void* fsa, const double* r,
-                        const double* scale, const int* skip, void* vout, bool vout_fp32, double* z, cudaStream_t);
+void launch_chain_factor(const CaseDev*, const BatchDims&, bool sa, bool fp32, cudaStream_t);
+void launch_chain_apply(const CaseDev*, const BatchDims&, bool sa, bool fp32, int src_id, int scale_on, int vout_j,
+                        int out_id, int check_active, cudaStream_t);
+int chain_grid_blocks(int n_chains, int n_offchain);
+void configure_line_kernels(int max_L);
 // krylov.cu
-void launch_gmres_init(Scalars*, const double* R, double* b, double* x, double* action, double* r, int n,
-                       const double* tile_partial, int n_tiles, double volume_sum, double* history, Reduce,
-                       cudaStream_t);
-void launch_cycle_start(Scalars*, Config, cudaStream_t);
-void launch_arnoldi_orth(Scalars*, const void* V, bool fp32, size_t ldv, int j, int m, double* w, int n, Reduce,
-                         cudaStream_t);
-void launch_lstsq(Scalars*, int m, cudaStream_t);
-void launch_combine(const Scalars*, const void* V, bool fp32, size_t ldv, int m, const double* w, double* tmp,
-                    double* action, int n, cudaStream_t);
-void launch_cycle_end(Scalars*, double* x, const double* z, const double* b, const double* action, double* r, int n,
-                      Reduce, cudaStream_t);
-void launch_newton_update(Scalars*, const Canvas&, const Physics&, Config, double* U, const double* dU,
-                          const double* action, const double* R, Reduce, cudaStream_t);
+void launch_gmres_init(const CaseDev*, const BatchDims&, cudaStream_t);
+void launch_cycle_start(const CaseDev*, const BatchDims&, cudaStream_t);
+void launch_arnoldi_orth(const CaseDev*, const BatchDims&, bool fp32, int j, cudaStream_t);
+void launch_lstsq(const CaseDev*, const BatchDims&, cudaStream_t);
+void launch_combine(const CaseDev*, const BatchDims&, bool fp32, cudaStream_t);
+void launch_cycle_end(const CaseDev*, const BatchDims&, cudaStream_t);
+void launch_scale_copy(const CaseDev*, const BatchDims&, bool fp32, int src_id, int scale_on, int vout_j, int out_id,
+                       int check_active, cudaStream_t);
+void launch_newton_update(const CaseDev*, const BatchDims&, cudaStream_t);
 int reduce_blocks(int n);
 // forces.cu
-void launch_forces(const Canvas&, const Physics&, const double* U, const double* qg, double length, double cx0,
-                   double cy0, double* out, cudaStream_t);
-
-// V_j = scale * src, z = V_j: the Arnoldi step without a preconditioner
-template <class TV>
-__global__ void k_scale_copy(const double* src, const double* scale_ptr, const int* skip, TV* vout, double* z, int n) {
-  if (skip != nullptr && *skip == 0) return;
-  const double s = scale_ptr != nullptr ? *scale_ptr : 1.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    double x = s * src[i];
-    if (vout != nullptr) {
-      TV xv = TV(x);
-      vout[i] = xv;
-      x = double(xv);
-    }
-    z[i] = x;
-  }
-}
+void launch_forces(const CaseDev*, const BatchDims&, cudaStream_t);
 }  // namespace jr
 
 using namespace jr;
 
 static thread_local std::string g_error;
 
+constexpr int MAX_CHAIN = 1024;   // longest line chain (one CTA of the line solve)
+constexpr int HIST_STEPS = 4096;  // Newton steps per jr_newton_steps call
+
 struct jr_plan {
-  Canvas cv{};
-  Physics P{};
-  Config cfg{};
-  int visc = 0;
+  int n_cases = 0;
+  int nvar = 4, visc = 0, m = 10;
   bool mixed = false;
-  int m = 10;
-  int n_vec = 0;     // nvar * NI * NJ
-  int n_faces = 0;
-  int n_tiles = 0;
+  Config cfg{};                          // the settings every case shares (restart, restarts, preconditioner)
+  BatchDims dims{};
+  std::vector<CaseDev> host;             // the resident case table (host copy)
+  CaseDev* cases = nullptr;              // ... on the device: the graph's table
+  CaseDev* adhoc = nullptr;              // the table of a call on caller buffers
+  std::vector<size_t> vec_off, can_off, face_off;   // offsets of each case in batch-long arrays
+  size_t total_vec = 0, total_can = 0, total_faces = 0;
   cudaStream_t st = nullptr;             // the stream work is issued on
   cudaStream_t owned_stream = nullptr;   // the plan's own stream
   std::vector<void*> allocs;
-  double *U = nullptr, *qg = nullptr, *dqg = nullptr, *R = nullptr, *b = nullptr, *x = nullptr, *action = nullptr;
-  double *r = nullptr, *w = nullptr, *z = nullptr, *tmp = nullptr, *zero = nullptr, *vdt = nullptr;
-  double *dflow = nullptr, *dsa = nullptr, *lam = nullptr, *mflux = nullptr, *dflux = nullptr;
-  double *tile_partial = nullptr, *history = nullptr, *force_out = nullptr;
-  void *V = nullptr, *fflow = nullptr, *fsa = nullptr, *scratch = nullptr;
-  Scalars* sc = nullptr;
-  Reduce red{};
-  int hist_cap = 0;
+  double* U = nullptr;                   // every case's state, back to back
+  double* history = nullptr;             // [step][case]
+  double* force_out = nullptr;           // 8 per case
+  Scalars* sc = nullptr;                 // one per case
   cudaGraphExec_t graph = nullptr;
-  double force_length = 1.0, cx0 = 0.25, cy0 = 0.0;
 };
 
 static int fail(int code, const std::string& msg) {
@@ -117,107 +91,30 @@ template <class T> static int dev_copy(jr_plan* p, T** dst, const T* src, size_t
 }
 
 static int dev_alloc(jr_plan* p, void** dst, size_t bytes) {
+  *dst = nullptr;
+  if (bytes == 0) bytes = 16;
   if (cudaMalloc(dst, bytes) != cudaSuccess) return fail(JR_ENOMEM, "cudaMalloc failed");
   p->allocs.push_back(*dst);
   cudaMemset(*dst, 0, bytes);
   return JR_OK;
 }
 
-#define TRY(x)                \
-  do {                        \
-    int _rc = (x);            \
-    if (_rc != JR_OK) {       \
-      jr_plan_destroy(plan);  \
-      return _rc;             \
-    }                         \
+#define TRY(x)               \
+  do {                       \
+    int _rc = (x);           \
+    if (_rc != JR_OK) return _rc; \
   } while (0)
 
-// The launch sequence of one Newton step on the plan's state (captured as a graph).
-static void enqueue_step(jr_plan* p) {
-  const Canvas& c = p->cv;
-  const int n = p->n_vec, N = c.NI * c.NJ, m = p->m;
-  const bool sa = c.nvar == 5;
-  const size_t ldv = (size_t)n;
-  cudaStream_t st = p->st;
-  launch_ghosts(c, p->P, false, p->U, nullptr, p->qg, nullptr, nullptr, st);
-  launch_residual(c, p->P, p->visc, true, p->U, p->qg, p->R, p->tile_partial, st);
-  launch_gmres_init(p->sc, p->R, p->b, p->x, p->action, p->r, n, p->tile_partial, p->n_tiles, c.volume_sum,
-                    p->history, p->red, st);
-  launch_faces(c, p->P, p->visc, p->U, p->lam, p->mflux, p->dflux, st);
-  launch_cells(c, p->P, p->visc, p->U, p->lam, p->mflux, p->dflux, p->sc, p->vdt, p->dflow, p->dsa, st);
-  if (p->cfg.preconditioner == 1)
-    launch_chain_factor(c, p->P, sa, p->mixed, p->U, p->lam, p->mflux, p->dflux, p->dflow, p->dsa, p->fflow, p->fsa,
-                        p->scratch, st);
-  const size_t vbytes = p->mixed ? sizeof(float) : sizeof(double);
-  for (int cyc = 0; cyc < p->cfg.maxiter; ++cyc) {
-    launch_cycle_start(p->sc, p->cfg, st);
-    for (int j = 0; j < m; ++j) {
-      const double* src = j == 0 ? p->r : p->w;
-      void* vj = (char*)p->V + (size_t)j * ldv * vbytes;
-      if (p->cfg.preconditioner == 1) {
-        launch_chain_apply(c, sa, p->mixed, p->fflow, p->fsa, src, &p->sc->inv_nrm, &p->sc->active, vj, p->mixed,
-                           p->z, st);
-      } else {
-        int blocks = std::min((n + 255) / 256, 148 * 4);
-        if (p->mixed)
-          k_scale_copy<float><<<blocks, 256, 0, st>>>(src, &p->sc->inv_nrm, &p->sc->active, (float*)vj, p->z, n);
-        else
-          k_scale_copy<double><<<blocks, 256, 0, st>>>(src, &p->sc->inv_nrm, &p->sc->active, (double*)vj, p->z, n);
-      }
-      launch_ghosts(c, p->P, true, p->U, p->z, p->qg, p->dqg, &p->sc->active, st);
-      launch_jvp(c, p->P, p->visc, p->U, p->qg, p->z, p->dqg, p->vdt, p->w, &p->sc->active, st);
-      launch_arnoldi_orth(p->sc, p->V, p->mixed, ldv, j, m, p->w, n, p->red, st);
-    }
-    launch_lstsq(p->sc, m, st);
-    launch_combine(p->sc, p->V, p->mixed, ldv, m, p->w, p->tmp, p->action, n, st);
-    if (p->cfg.preconditioner == 1) {
-      launch_chain_apply(c, sa, p->mixed, p->fflow, p->fsa, p->tmp, nullptr, &p->sc->active, nullptr, false, p->z, st);
-    } else {
-      int blocks = std::min((n + 255) / 256, 148 * 4);
-      k_scale_copy<double><<<blocks, 256, 0, st>>>(p->tmp, nullptr, &p->sc->active, nullptr, p->z, n);
-    }
-    launch_cycle_end(p->sc, p->x, p->z, p->b, p->action, p->r, n, p->red, st);
-  }
-  launch_newton_update(p->sc, c, p->P, p->cfg, p->U, p->x, p->action, p->R, p->red, st);
-  (void)N;
-}
-
-extern "C" {
-
-const char* jr_last_error(void) { return g_error.c_str(); }
-
-int jr_plan_destroy(jr_plan* plan) {
-  if (plan == nullptr) return JR_OK;
-  if (plan->graph) cudaGraphExecDestroy(plan->graph);
-  if (plan->st) cudaStreamSynchronize(plan->st);
-  for (void* a : plan->allocs) cudaFree(a);
-  if (plan->owned_stream) cudaStreamDestroy(plan->owned_stream);
-  delete plan;
-  return JR_OK;
-}
-
-int jr_plan_create(const jr_plan_desc* d, jr_plan** out) {
-  if (d == nullptr || out == nullptr) return fail(JR_EINVAL, "null argument");
-  *out = nullptr;
+// Static tables, physics and solver settings of one case (the work buffers come later).
+static int build_case(jr_plan* plan, const jr_plan_desc* d, CaseDev& cd, size_t& factor_rows) {
   if (d->NI < 5 || d->NJ < 5 || (d->nvar != 4 && d->nvar != 5))
     return fail(JR_EINVAL, "canvas must be at least 5 x 5 with nvar 4 or 5");
   if (d->krylov_subspace < 1 || d->krylov_subspace > MAX_KRYLOV)
     return fail(JR_EINVAL, "krylov_subspace must lie in [1, 64]");
   if (d->nvar == 5 && d->distance == nullptr) return fail(JR_EINVAL, "the SA model needs the wall distance");
-  if (d->far_field == 1 && d->nvar == 4 && false) return fail(JR_EINVAL, "unreachable");
-  jr_plan* plan = new jr_plan();
   const int NI = d->NI, NJ = d->NJ, N = NI * NJ, nv = d->nvar;
   const size_t nfi = (size_t)(NI + 1) * NJ, nfj = (size_t)NI * (NJ + 1);
-  plan->n_vec = nv * N;
-  plan->n_faces = (int)(nfi + nfj);
-  plan->m = d->krylov_subspace;
-  plan->mixed = d->precision == 1;
-  if (cudaStreamCreateWithFlags(&plan->owned_stream, cudaStreamNonBlocking) == cudaSuccess) plan->st = plan->owned_stream;
-  if (plan->st == nullptr) {
-    delete plan;
-    return fail(JR_ECUDA, "cudaStreamCreate failed");
-  }
-  Canvas& c = plan->cv;
+  Canvas& c = cd.c;
   c.NI = NI;
   c.NJ = NJ;
   c.nvar = nv;
@@ -242,10 +139,8 @@ int jr_plan_create(const jr_plan_desc* d, jr_plan** out) {
     c.n_ghost[s] = n;
     for (int k = 0; k < n; ++k)
       if (d->ghost[s][k] < 0 || d->ghost[s][k] >= N || d->source[s][k] < 0 || d->source[s][k] >= N ||
-          d->kind[s][k] < 0 || d->kind[s][k] > 6) {
-        jr_plan_destroy(plan);
+          d->kind[s][k] < 0 || d->kind[s][k] > 6)
         return fail(JR_EINVAL, "a ghost record out of range");
-      }
     TRY(dev_copy(plan, (int**)&c.g_ghost[s], d->ghost[s], (size_t)n));
     TRY(dev_copy(plan, (int**)&c.g_source[s], d->source[s], (size_t)n));
     TRY(dev_copy(plan, (int**)&c.g_kind[s], d->kind[s], (size_t)n));
@@ -266,15 +161,13 @@ int jr_plan_create(const jr_plan_desc* d, jr_plan** out) {
   TRY(dev_copy(plan, (double**)&c.w_into, d->wall_into, (size_t)d->n_walls));
   TRY(dev_copy(plan, (double**)&c.w_mid, d->wall_mid, (size_t)2 * d->n_walls));
   const int nc = d->n_chains, L = d->chain_L;
+  if (L > MAX_CHAIN) return fail(JR_EINVAL, "line chains longer than 1024 cells are not supported");
   c.n_chains = nc;
   c.L = L;
   std::vector<int> on_chain(N, 0);
   for (size_t k = 0; k < (size_t)nc * L; ++k) {
     int cell = d->chain_cells[k];
-    if (cell >= N) {
-      jr_plan_destroy(plan);
-      return fail(JR_EINVAL, "a chain cell out of range");
-    }
+    if (cell >= N) return fail(JR_EINVAL, "a chain cell out of range");
     if (cell >= 0) on_chain[cell] = 1;
   }
   std::vector<int> off;
@@ -288,19 +181,16 @@ int jr_plan_create(const jr_plan_desc* d, jr_plan** out) {
   TRY(dev_copy(plan, (int**)&c.ch_up_sign, d->chain_up_sign, (size_t)nc * L));
   TRY(dev_copy(plan, (int**)&c.ch_down_face, d->chain_down_face, (size_t)nc * L));
   TRY(dev_copy(plan, (int**)&c.ch_down_sign, d->chain_down_sign, (size_t)nc * L));
-  if (L > 1024) {
-    jr_plan_destroy(plan);
-    return fail(JR_EINVAL, "line chains longer than 1024 cells are not supported");
-  }
   std::vector<int> fbase(nc);
   size_t fbase_total = 0;
   for (int k = 0; k < nc; ++k) {
     fbase[k] = (int)fbase_total;
     fbase_total += (size_t)d->chain_len[k] + 16;
   }
+  factor_rows = fbase_total;
   TRY(dev_copy(plan, (int**)&c.ch_fbase, fbase.data(), (size_t)nc));
 
-  Physics& P = plan->P;
+  Physics& P = cd.P;
   P.gamma = d->gamma;
   P.mu_inf = d->mu_inf;
   P.sutherland = d->sutherland;
@@ -337,13 +227,10 @@ int jr_plan_create(const jr_plan_desc* d, jr_plan** out) {
   s.c_v1_3 = s.c_v1 * s.c_v1 * s.c_v1;
   s.c_w3_6 = s.c_w3 * s.c_w3 * s.c_w3 * s.c_w3 * s.c_w3 * s.c_w3;
   s.c_2_2 = s.c_2 * s.c_2;
-  plan->visc = d->mu_inf > 0.0 ? (nv == 5 ? 2 : 1) : 0;
-  if (nv == 5 && plan->visc != 2) {
-    jr_plan_destroy(plan);
-    return fail(JR_EINVAL, "the SA model needs a viscous flow");
-  }
+  cd.visc = d->mu_inf > 0.0 ? (nv == 5 ? 2 : 1) : 0;
+  if (nv == 5 && cd.visc != 2) return fail(JR_EINVAL, "the SA model needs a viscous flow");
 
-  Config& cf = plan->cfg;
+  Config& cf = cd.cfg;
   cf.cfl_max = d->cfl_max;
   cf.cfl_growth = d->cfl_growth;
   cf.cfl_cutback = d->cfl_cutback;
@@ -354,51 +241,243 @@ int jr_plan_create(const jr_plan_desc* d, jr_plan** out) {
   cf.restart = d->krylov_subspace;
   cf.maxiter = d->krylov_restarts;
   cf.preconditioner = d->preconditioner;
-  plan->force_length = d->force_length;
-  plan->cx0 = d->moment_centre[0];
-  plan->cy0 = d->moment_centre[1];
-
-  const size_t vec = (size_t)plan->n_vec;
-  double** vecs[] = {&plan->U, &plan->qg, &plan->dqg, &plan->R, &plan->b, &plan->x, &plan->action,
-                     &plan->r, &plan->w, &plan->z, &plan->tmp};
-  for (double** v : vecs) TRY(dev_copy<double>(plan, v, nullptr, vec));
-  TRY(dev_copy<double>(plan, &plan->zero, nullptr, (size_t)N));
-  TRY(dev_copy<double>(plan, &plan->vdt, nullptr, (size_t)N));
-  TRY(dev_copy<double>(plan, &plan->dflow, nullptr, (size_t)N));
-  TRY(dev_copy<double>(plan, &plan->dsa, nullptr, (size_t)N));
-  TRY(dev_copy<double>(plan, &plan->lam, nullptr, nfi + nfj));
-  TRY(dev_copy<double>(plan, &plan->mflux, nullptr, nfi + nfj));
-  TRY(dev_copy<double>(plan, &plan->dflux, nullptr, nfi + nfj));
+  cd.force_length = d->force_length;
+  cd.moment_centre[0] = d->moment_centre[0];
+  cd.moment_centre[1] = d->moment_centre[1];
+  cd.n_vec = nv * N;
+  cd.m = d->krylov_subspace;
+  cd.mixed = d->precision == 1;
   dim3 tg = tile_grid(c);
-  plan->n_tiles = (int)(tg.x * tg.y);
-  TRY(dev_copy<double>(plan, &plan->tile_partial, nullptr, (size_t)plan->n_tiles));
-  plan->hist_cap = 4096;
-  TRY(dev_copy<double>(plan, &plan->history, nullptr, (size_t)plan->hist_cap));
-  TRY(dev_copy<double>(plan, &plan->force_out, nullptr, 8));
-  const size_t tb = plan->mixed ? sizeof(float) : sizeof(double);
-  TRY(dev_alloc(plan, &plan->V, (size_t)(plan->m + 1) * vec * tb));
+  cd.tiles_x = (int)tg.x;
+  cd.tiles_y = (int)tg.y;
+  cd.n_tiles = (int)(tg.x * tg.y);
+  cd.enabled = 1;
+  return JR_OK;
+}
+
+// Work buffers: each kind is one allocation holding every case's part back to back.
+static int build_buffers(jr_plan* p, const std::vector<size_t>& factor_rows) {
+  const int nc = p->n_cases;
+  std::vector<size_t> tile_off(nc), fb_off(nc), part_off(nc);
+  size_t tiles = 0, fb = 0, part = 0;
+  p->vec_off.assign(nc, 0);
+  p->can_off.assign(nc, 0);
+  p->face_off.assign(nc, 0);
+  for (int k = 0; k < nc; ++k) {
+    const Canvas& c = p->host[k].c;
+    const size_t N = (size_t)c.NI * c.NJ, nf = (size_t)(c.NI + 1) * c.NJ + (size_t)c.NI * (c.NJ + 1);
+    p->vec_off[k] = p->total_vec;
+    p->can_off[k] = p->total_can;
+    p->face_off[k] = p->total_faces;
+    tile_off[k] = tiles;
+    fb_off[k] = fb;
+    part_off[k] = part;
+    p->total_vec += (size_t)c.nvar * N;
+    p->total_can += N;
+    p->total_faces += nf;
+    tiles += (size_t)p->host[k].n_tiles;
+    fb += factor_rows[k];
+    part += (size_t)reduce_blocks(p->host[k].n_vec) * (MAX_KRYLOV + 1);
+  }
+  const size_t tb = p->mixed ? sizeof(float) : sizeof(double);
+  const int NVEC = 11;
+  double* vec[NVEC];
+  for (int v = 0; v < NVEC; ++v) TRY(dev_alloc(p, (void**)&vec[v], p->total_vec * sizeof(double)));
+  double *vdt, *dflow, *dsa, *lam, *mflux, *dflux, *tile_partial, *partial;
+  unsigned* ticket;
+  void *V, *fflow, *fsa, *scratch;
+  TRY(dev_alloc(p, (void**)&vdt, p->total_can * sizeof(double)));
+  TRY(dev_alloc(p, (void**)&dflow, p->total_can * sizeof(double)));
+  TRY(dev_alloc(p, (void**)&dsa, p->total_can * sizeof(double)));
+  TRY(dev_alloc(p, (void**)&lam, p->total_faces * sizeof(double)));
+  TRY(dev_alloc(p, (void**)&mflux, p->total_faces * sizeof(double)));
+  TRY(dev_alloc(p, (void**)&dflux, p->total_faces * sizeof(double)));
+  TRY(dev_alloc(p, (void**)&tile_partial, tiles * sizeof(double)));
+  TRY(dev_alloc(p, (void**)&partial, part * sizeof(double)));
+  TRY(dev_alloc(p, (void**)&ticket, (size_t)nc * sizeof(unsigned)));
+  TRY(dev_alloc(p, &V, (size_t)(p->m + 1) * p->total_vec * tb));
   // cyclic-reduction factor: per chain at most 80 (flow) and 5 (SA) entries per row of
   // (length + 16) rows; the level systems in scratch at most 104 per row
-  TRY(dev_alloc(plan, &plan->fflow, fbase_total * 80 * tb));
-  TRY(dev_alloc(plan, &plan->fsa, fbase_total * 5 * tb));
-  TRY(dev_alloc(plan, &plan->scratch, fbase_total * 104 * tb));
-  TRY(dev_alloc(plan, (void**)&plan->sc, sizeof(Scalars)));
-  int rb = reduce_blocks(plan->n_vec);
-  plan->red.blocks = rb;
-  TRY(dev_alloc(plan, (void**)&plan->red.partial, (size_t)rb * (MAX_KRYLOV + 1) * sizeof(double)));
-  TRY(dev_alloc(plan, (void**)&plan->red.ticket, sizeof(unsigned)));
+  TRY(dev_alloc(p, &fflow, fb * 80 * tb));
+  TRY(dev_alloc(p, &fsa, fb * 5 * tb));
+  TRY(dev_alloc(p, &scratch, fb * 104 * tb));
+  TRY(dev_alloc(p, (void**)&p->sc, (size_t)nc * sizeof(Scalars)));
+  TRY(dev_alloc(p, (void**)&p->history, (size_t)HIST_STEPS * nc * sizeof(double)));
+  TRY(dev_alloc(p, (void**)&p->force_out, (size_t)8 * nc * sizeof(double)));
+  p->U = vec[0];
+  for (int k = 0; k < nc; ++k) {
+    CaseDev& cd = p->host[k];
+    const size_t vo = p->vec_off[k], co = p->can_off[k], fo = p->face_off[k];
+    double** mine[NVEC] = {&cd.U, &cd.qg, &cd.dqg, &cd.R, &cd.b, &cd.x, &cd.action, &cd.r, &cd.w, &cd.z, &cd.tmp};
+    for (int v = 0; v < NVEC; ++v) *mine[v] = vec[v] + vo;
+    cd.vdt = vdt + co;
+    cd.dflow = dflow + co;
+    cd.dsa = dsa + co;
+    cd.lam = lam + fo;
+    cd.mflux = mflux + fo;
+    cd.dflux = dflux + fo;
+    cd.tile_partial = tile_partial + tile_off[k];
+    cd.partial = partial + part_off[k];
+    cd.ticket = ticket + k;
+    cd.V = (char*)V + (size_t)(p->m + 1) * vo * tb;
+    cd.fflow = (char*)fflow + fb_off[k] * 80 * tb;
+    cd.fsa = (char*)fsa + fb_off[k] * 5 * tb;
+    cd.scratch = (char*)scratch + fb_off[k] * 104 * tb;
+    cd.sc = p->sc + k;
+    cd.history = p->history;
+    cd.force_out = p->force_out + 8 * k;
+  }
+  TRY(dev_alloc(p, (void**)&p->cases, (size_t)nc * sizeof(CaseDev)));
+  TRY(dev_alloc(p, (void**)&p->adhoc, (size_t)nc * sizeof(CaseDev)));
+  if (cudaMemcpy(p->cases, p->host.data(), (size_t)nc * sizeof(CaseDev), cudaMemcpyHostToDevice) != cudaSuccess)
+    return cuda_check("case table");
+  return JR_OK;
+}
+
+static void compute_dims(jr_plan* p) {
+  BatchDims& d = p->dims;
+  d = BatchDims{};
+  d.n_cases = p->n_cases;
+  for (const CaseDev& cd : p->host) {
+    const Canvas& c = cd.c;
+    d.tiles_x = std::max(d.tiles_x, cd.tiles_x);
+    d.tiles_y = std::max(d.tiles_y, cd.tiles_y);
+    d.ghost_records = std::max(d.ghost_records, c.n_ghost[0] + c.n_ghost[1]);
+    d.faces = std::max(d.faces, (c.NI + 1) * c.NJ + c.NI * (c.NJ + 1));
+    d.cells = std::max(d.cells, c.NI * c.NJ);
+    d.n_vec = std::max(d.n_vec, cd.n_vec);
+    d.chain_blocks = std::max(d.chain_blocks, chain_grid_blocks(c.n_chains, c.n_offchain));
+    d.max_L = std::max(d.max_L, c.L);
+  }
+  d.chain_blocks = std::max(d.chain_blocks, 1);
+}
+
+// The table of a call on caller buffers: the resident table with the named buffers of
+// every case moved to its part of the caller's batch-long arrays.
+struct Adhoc {
+  jr_plan* p;
+  std::vector<CaseDev> t;
+  explicit Adhoc(jr_plan* plan) : p(plan), t(plan->host) {}
+  void vec(double* CaseDev::*field, const double* base) {
+    for (int k = 0; k < p->n_cases; ++k) t[k].*field = const_cast<double*>(base) + p->vec_off[k];
+  }
+  void faces(double* CaseDev::*field, double* base) {
+    for (int k = 0; k < p->n_cases; ++k) t[k].*field = base + p->face_off[k];
+  }
+  const CaseDev* upload() {
+    // from pageable memory: staged before the call returns, so `t` may go
+    cudaMemcpyAsync(p->adhoc, t.data(), t.size() * sizeof(CaseDev), cudaMemcpyHostToDevice, p->st);
+    return p->adhoc;
+  }
+};
+
+static int upload_table(jr_plan* p) {
+  cudaMemcpyAsync(p->cases, p->host.data(), p->host.size() * sizeof(CaseDev), cudaMemcpyHostToDevice, p->st);
+  if (cudaStreamSynchronize(p->st) != cudaSuccess) return cuda_check("case table");
+  return cuda_check("case table");
+}
+
+// The launch sequence of one Newton step of every case (captured as a graph).
+static void enqueue_step(jr_plan* p) {
+  const CaseDev* t = p->cases;
+  const BatchDims& d = p->dims;
+  const bool sa = p->nvar == 5, pre = p->cfg.preconditioner == 1;
+  cudaStream_t st = p->st;
+  launch_ghosts(t, d, -1, 0, st);
+  launch_residual(t, d, p->visc, true, B_R, st);
+  launch_gmres_init(t, d, st);
+  launch_faces(t, d, p->visc, st);
+  launch_cells(t, d, p->visc, st);
+  if (pre) launch_chain_factor(t, d, sa, p->mixed, st);
+  for (int cyc = 0; cyc < p->cfg.maxiter; ++cyc) {
+    launch_cycle_start(t, d, st);
+    for (int j = 0; j < p->m; ++j) {
+      const int src = j == 0 ? B_RR : B_W;
+      if (pre) launch_chain_apply(t, d, sa, p->mixed, src, 1, j, B_Z, 1, st);
+      else launch_scale_copy(t, d, p->mixed, src, 1, j, B_Z, 1, st);
+      launch_ghosts(t, d, B_Z, 1, st);
+      launch_jvp(t, d, p->visc, B_Z, B_VDT, B_W, 1, st);
+      launch_arnoldi_orth(t, d, p->mixed, j, st);
+    }
+    launch_lstsq(t, d, st);
+    launch_combine(t, d, p->mixed, st);
+    if (pre) launch_chain_apply(t, d, sa, p->mixed, B_TMP, 0, -1, B_Z, 1, st);
+    else launch_scale_copy(t, d, false, B_TMP, 0, -1, B_Z, 1, st);
+    launch_cycle_end(t, d, st);
+  }
+  launch_newton_update(t, d, st);
+}
+
+extern "C" {
+
+const char* jr_last_error(void) { return g_error.c_str(); }
+
+int jr_plan_destroy(jr_plan* plan) {
+  if (plan == nullptr) return JR_OK;
+  if (plan->graph) cudaGraphExecDestroy(plan->graph);
+  if (plan->st) cudaStreamSynchronize(plan->st);
+  for (void* a : plan->allocs) cudaFree(a);
+  if (plan->owned_stream) cudaStreamDestroy(plan->owned_stream);
+  delete plan;
+  return JR_OK;
+}
+
+int jr_batch_create(const jr_plan_desc* descs, int32_t n_cases, jr_plan** out) {
+  if (descs == nullptr || out == nullptr || n_cases < 1) return fail(JR_EINVAL, "null argument or no cases");
+  *out = nullptr;
+  const jr_plan_desc& d0 = descs[0];
+  for (int k = 1; k < n_cases; ++k) {
+    const jr_plan_desc& d = descs[k];
+    if (d.nvar != d0.nvar || (d.mu_inf > 0.0) != (d0.mu_inf > 0.0) || d.precision != d0.precision ||
+        d.krylov_subspace != d0.krylov_subspace || d.krylov_restarts != d0.krylov_restarts ||
+        d.preconditioner != d0.preconditioner)
+      return fail(JR_EINVAL,
+                  "the cases of a batch must share the model, the precision and the Krylov and preconditioner "
+                  "settings");
+  }
+  jr_plan* plan = new jr_plan();
+  plan->n_cases = n_cases;
+  plan->host.resize(n_cases);
+  if (cudaStreamCreateWithFlags(&plan->owned_stream, cudaStreamNonBlocking) == cudaSuccess)
+    plan->st = plan->owned_stream;
+  if (plan->st == nullptr) {
+    delete plan;
+    return fail(JR_ECUDA, "cudaStreamCreate failed");
+  }
+  std::vector<size_t> rows(n_cases);
+  int rc = JR_OK;
+  for (int k = 0; k < n_cases && rc == JR_OK; ++k) rc = build_case(plan, &descs[k], plan->host[k], rows[k]);
+  if (rc == JR_OK) {
+    plan->nvar = d0.nvar;
+    plan->visc = plan->host[0].visc;
+    plan->m = d0.krylov_subspace;
+    plan->mixed = d0.precision == 1;
+    plan->cfg = plan->host[0].cfg;
+    rc = build_buffers(plan, rows);
+  }
+  if (rc != JR_OK) {
+    jr_plan_destroy(plan);
+    return rc;
+  }
+  compute_dims(plan);
   configure_kernels();
-  configure_line_kernels(c);
+  configure_line_kernels(MAX_CHAIN);
   if (cudaDeviceSynchronize() != cudaSuccess) {
-    int rc = cuda_check("plan create");
+    rc = cuda_check("plan create");
     jr_plan_destroy(plan);
     return rc ? rc : fail(JR_ECUDA, "plan create");
   }
-  // the freestream state, CFL and |R| = inf
-  std::vector<double> U0((size_t)plan->n_vec);
-  for (int v = 0; v < nv; ++v)
-    for (int k = 0; k < N; ++k) U0[(size_t)v * N + k] = P.U_inf[v];
-  int rc = jr_state_set(plan, U0.data(), d->cfl, INFINITY);
+  // the freestream state of every case, its CFL and |R| = inf
+  std::vector<double> U0(plan->total_vec);
+  for (int k = 0; k < n_cases; ++k) {
+    const CaseDev& cd = plan->host[k];
+    const size_t N = (size_t)cd.c.NI * cd.c.NJ;
+    for (int v = 0; v < cd.c.nvar; ++v)
+      for (size_t i = 0; i < N; ++i) U0[plan->vec_off[k] + v * N + i] = cd.P.U_inf[v];
+  }
+  rc = jr_state_set(plan, U0.data(), d0.cfl, INFINITY);
+  for (int k = 1; k < n_cases && rc == JR_OK; ++k)
+    if (descs[k].cfl != d0.cfl) rc = jr_case_state_set(plan, k, nullptr, descs[k].cfl, INFINITY);
   if (rc) {
     jr_plan_destroy(plan);
     return rc;
@@ -407,10 +486,25 @@ int jr_plan_create(const jr_plan_desc* d, jr_plan** out) {
   return JR_OK;
 }
 
+int jr_plan_create(const jr_plan_desc* desc, jr_plan** out) { return jr_batch_create(desc, 1, out); }
+
+int jr_plan_cases(const jr_plan* plan) { return plan ? plan->n_cases : 0; }
+
 int jr_plan_sizes(const jr_plan* plan, int64_t* n_canvas, int64_t* n_faces) {
   if (!plan) return fail(JR_EINVAL, "null plan");
-  if (n_canvas) *n_canvas = (int64_t)plan->cv.NI * plan->cv.NJ;
-  if (n_faces) *n_faces = plan->n_faces;
+  if (n_canvas) *n_canvas = (int64_t)plan->total_can;
+  if (n_faces) *n_faces = (int64_t)plan->total_faces;
+  return JR_OK;
+}
+
+int jr_case_sizes(const jr_plan* plan, int32_t c, int64_t* n_canvas, int64_t* n_faces, int64_t* canvas_offset,
+                  int64_t* face_offset) {
+  if (!plan || c < 0 || c >= plan->n_cases) return fail(JR_EINVAL, "bad plan or case");
+  const Canvas& cv = plan->host[c].c;
+  if (n_canvas) *n_canvas = (int64_t)cv.NI * cv.NJ;
+  if (n_faces) *n_faces = (int64_t)(cv.NI + 1) * cv.NJ + (int64_t)cv.NI * (cv.NJ + 1);
+  if (canvas_offset) *canvas_offset = (int64_t)plan->can_off[c];
+  if (face_offset) *face_offset = (int64_t)plan->face_off[c];
   return JR_OK;
 }
 
@@ -419,9 +513,6 @@ void* jr_plan_stream(jr_plan* plan) { return plan ? (void*)plan->st : nullptr; }
 int jr_plan_set_stream(jr_plan* plan, void* stream) {
   if (!plan) return fail(JR_EINVAL, "null plan");
   if (cudaStreamSynchronize(plan->st) != cudaSuccess) return cuda_check("jr_plan_set_stream");
-  if (plan->owned_stream && plan->st != plan->owned_stream) {
-    // a caller's stream was in use: nothing to release
-  }
   plan->st = stream != nullptr ? (cudaStream_t)stream : plan->owned_stream;
   return JR_OK;
 }
@@ -434,67 +525,113 @@ int jr_synchronize(jr_plan* plan) {
 
 int jr_residual(jr_plan* plan, const double* U, double* R, int first_order) {
   if (!plan || !U || !R) return fail(JR_EINVAL, "null argument");
-  launch_ghosts(plan->cv, plan->P, false, U, nullptr, plan->qg, nullptr, nullptr, plan->st);
-  launch_residual(plan->cv, plan->P, plan->visc, first_order == 0, U, plan->qg, R, plan->tile_partial, plan->st);
+  Adhoc a(plan);
+  a.vec(&CaseDev::U, U);
+  a.vec(&CaseDev::R, R);
+  const CaseDev* t = a.upload();
+  launch_ghosts(t, plan->dims, -1, 0, plan->st);
+  launch_residual(t, plan->dims, plan->visc, first_order == 0, B_R, plan->st);
   return cuda_check("jr_residual");
 }
 
 int jr_jvp(jr_plan* plan, const double* U, const double* v, double* Jv) {
   if (!plan || !U || !v || !Jv) return fail(JR_EINVAL, "null argument");
-  launch_ghosts(plan->cv, plan->P, false, U, nullptr, plan->qg, nullptr, nullptr, plan->st);
-  launch_ghosts(plan->cv, plan->P, true, U, v, plan->qg, plan->dqg, nullptr, plan->st);
-  launch_jvp(plan->cv, plan->P, plan->visc, U, plan->qg, v, plan->dqg, plan->zero, Jv, nullptr, plan->st);
+  Adhoc a(plan);
+  a.vec(&CaseDev::U, U);
+  a.vec(&CaseDev::z, v);
+  a.vec(&CaseDev::w, Jv);
+  const CaseDev* t = a.upload();
+  launch_ghosts(t, plan->dims, -1, 0, plan->st);
+  launch_ghosts(t, plan->dims, B_Z, 0, plan->st);
+  launch_jvp(t, plan->dims, plan->visc, B_Z, -1, B_W, 0, plan->st);
   return cuda_check("jr_jvp");
 }
 
 int jr_wave_speeds(jr_plan* plan, const double* U, double* lam) {
   if (!plan || !U || !lam) return fail(JR_EINVAL, "null argument");
-  launch_faces(plan->cv, plan->P, plan->visc, U, lam, plan->mflux, plan->dflux, plan->st);
+  Adhoc a(plan);
+  a.vec(&CaseDev::U, U);
+  a.faces(&CaseDev::lam, lam);
+  launch_faces(a.upload(), plan->dims, plan->visc, plan->st);
   return cuda_check("jr_wave_speeds");
 }
 
 int jr_precond_factor(jr_plan* plan, const double* U, double cfl) {
   if (!plan || !U) return fail(JR_EINVAL, "null argument");
   if (!(cfl > 0.0)) return fail(JR_EINVAL, "cfl must be positive");
-  cudaMemcpyAsync(&plan->sc->cfl, &cfl, sizeof(double), cudaMemcpyHostToDevice, plan->st);
-  cudaStreamSynchronize(plan->st);
-  launch_faces(plan->cv, plan->P, plan->visc, U, plan->lam, plan->mflux, plan->dflux, plan->st);
-  launch_cells(plan->cv, plan->P, plan->visc, U, plan->lam, plan->mflux, plan->dflux, plan->sc, plan->vdt,
-               plan->dflow, plan->dsa, plan->st);
-  launch_chain_factor(plan->cv, plan->P, plan->cv.nvar == 5, plan->mixed, U, plan->lam, plan->mflux, plan->dflux,
-                      plan->dflow, plan->dsa, plan->fflow, plan->fsa, plan->scratch, plan->st);
+  for (int k = 0; k < plan->n_cases; ++k)
+    cudaMemcpyAsync(&plan->sc[k].cfl, &cfl, sizeof(double), cudaMemcpyHostToDevice, plan->st);
+  Adhoc a(plan);
+  a.vec(&CaseDev::U, U);
+  const CaseDev* t = a.upload();
+  launch_faces(t, plan->dims, plan->visc, plan->st);
+  launch_cells(t, plan->dims, plan->visc, plan->st);
+  launch_chain_factor(t, plan->dims, plan->nvar == 5, plan->mixed, plan->st);
+  if (cudaStreamSynchronize(plan->st) != cudaSuccess) return cuda_check("jr_precond_factor");
   return cuda_check("jr_precond_factor");
 }
 
 int jr_precond_apply(jr_plan* plan, const double* r, double* z) {
   if (!plan || !r || !z) return fail(JR_EINVAL, "null argument");
-  launch_chain_apply(plan->cv, plan->cv.nvar == 5, plan->mixed, plan->fflow, plan->fsa, r, nullptr, nullptr, nullptr,
-                     false, z, plan->st);
+  Adhoc a(plan);
+  a.vec(&CaseDev::r, r);
+  a.vec(&CaseDev::z, z);
+  launch_chain_apply(a.upload(), plan->dims, plan->nvar == 5, plan->mixed, B_RR, 0, -1, B_Z, 0, plan->st);
   return cuda_check("jr_precond_apply");
+}
+
+int jr_case_state_set(jr_plan* plan, int32_t c, const double* U_host, double cfl, double residual_norm) {
+  if (!plan || c < 0 || c >= plan->n_cases) return fail(JR_EINVAL, "bad plan or case");
+  if (U_host)
+    cudaMemcpyAsync(plan->host[c].U, U_host, (size_t)plan->host[c].n_vec * sizeof(double), cudaMemcpyHostToDevice,
+                    plan->st);
+  Scalars s{};
+  s.cfl = cfl;
+  s.res_prev = residual_norm;
+  cudaMemcpyAsync(plan->sc + c, &s, sizeof(Scalars), cudaMemcpyHostToDevice, plan->st);
+  if (cudaStreamSynchronize(plan->st) != cudaSuccess) return cuda_check("jr_case_state_set");
+  return cuda_check("jr_case_state_set");
+}
+
+int jr_case_state_get(jr_plan* plan, int32_t c, double* U_host, double* cfl, double* residual_norm, int32_t* status) {
+  if (!plan || c < 0 || c >= plan->n_cases) return fail(JR_EINVAL, "bad plan or case");
+  if (U_host)
+    cudaMemcpyAsync(U_host, plan->host[c].U, (size_t)plan->host[c].n_vec * sizeof(double), cudaMemcpyDeviceToHost,
+                    plan->st);
+  Scalars s;
+  cudaMemcpyAsync(&s, plan->sc + c, sizeof(Scalars), cudaMemcpyDeviceToHost, plan->st);
+  if (cudaStreamSynchronize(plan->st) != cudaSuccess) return cuda_check("jr_case_state_get");
+  if (cfl) *cfl = s.cfl;
+  if (residual_norm) *residual_norm = s.res_prev;
+  if (status) *status = s.status;
+  return cuda_check("jr_case_state_get");
 }
 
 int jr_state_set(jr_plan* plan, const double* U_host, double cfl, double residual_norm) {
   if (!plan) return fail(JR_EINVAL, "null plan");
-  if (U_host)
-    cudaMemcpyAsync(plan->U, U_host, (size_t)plan->n_vec * sizeof(double), cudaMemcpyHostToDevice, plan->st);
-  Scalars s{};
-  s.cfl = cfl;
-  s.res_prev = residual_norm;
-  cudaMemcpyAsync(plan->sc, &s, sizeof(Scalars), cudaMemcpyHostToDevice, plan->st);
+  if (U_host) cudaMemcpyAsync(plan->U, U_host, plan->total_vec * sizeof(double), cudaMemcpyHostToDevice, plan->st);
+  std::vector<Scalars> s(plan->n_cases);
+  for (Scalars& x : s) {
+    memset(&x, 0, sizeof(Scalars));
+    x.cfl = cfl;
+    x.res_prev = residual_norm;
+  }
+  cudaMemcpyAsync(plan->sc, s.data(), s.size() * sizeof(Scalars), cudaMemcpyHostToDevice, plan->st);
   if (cudaStreamSynchronize(plan->st) != cudaSuccess) return cuda_check("jr_state_set");
   return cuda_check("jr_state_set");
 }
 
 int jr_state_get(jr_plan* plan, double* U_host, double* cfl, double* residual_norm, int32_t* status) {
   if (!plan) return fail(JR_EINVAL, "null plan");
-  if (U_host)
-    cudaMemcpyAsync(U_host, plan->U, (size_t)plan->n_vec * sizeof(double), cudaMemcpyDeviceToHost, plan->st);
-  Scalars s;
-  cudaMemcpyAsync(&s, plan->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, plan->st);
+  if (U_host) cudaMemcpyAsync(U_host, plan->U, plan->total_vec * sizeof(double), cudaMemcpyDeviceToHost, plan->st);
+  std::vector<Scalars> s(plan->n_cases);
+  cudaMemcpyAsync(s.data(), plan->sc, s.size() * sizeof(Scalars), cudaMemcpyDeviceToHost, plan->st);
   if (cudaStreamSynchronize(plan->st) != cudaSuccess) return cuda_check("jr_state_get");
-  if (cfl) *cfl = s.cfl;
-  if (residual_norm) *residual_norm = s.res_prev;
-  if (status) *status = s.status;
+  for (int k = 0; k < plan->n_cases; ++k) {
+    if (cfl) cfl[k] = s[k].cfl;
+    if (residual_norm) residual_norm[k] = s[k].res_prev;
+    if (status) status[k] = s[k].status;
+  }
   return cuda_check("jr_state_get");
 }
 
@@ -502,26 +639,42 @@ double* jr_state_device(jr_plan* plan) { return plan ? plan->U : nullptr; }
 
 int jr_state_set_device(jr_plan* plan, const double* U_device, double cfl, double residual_norm) {
   if (!plan || !U_device) return fail(JR_EINVAL, "null argument");
-  cudaMemcpyAsync(plan->U, U_device, (size_t)plan->n_vec * sizeof(double), cudaMemcpyDeviceToDevice, plan->st);
-  Scalars s{};
-  s.cfl = cfl;
-  s.res_prev = residual_norm;
-  static thread_local Scalars staged;
-  staged = s;
-  cudaMemcpyAsync(plan->sc, &staged, sizeof(Scalars), cudaMemcpyHostToDevice, plan->st);
-  if (cudaStreamSynchronize(plan->st) != cudaSuccess) return cuda_check("jr_state_set_device");
-  return cuda_check("jr_state_set_device");
+  cudaMemcpyAsync(plan->U, U_device, plan->total_vec * sizeof(double), cudaMemcpyDeviceToDevice, plan->st);
+  return jr_state_set(plan, nullptr, cfl, residual_norm);
 }
 
-static int ensure_graph(jr_plan* plan);
+int jr_case_enable(jr_plan* plan, int32_t c, int32_t enabled) {
+  if (!plan || c < 0 || c >= plan->n_cases) return fail(JR_EINVAL, "bad plan or case");
+  plan->host[c].enabled = enabled != 0;
+  return upload_table(plan);
+}
+
+int jr_case_set_inflow(jr_plan* plan, int32_t c, const double* q_inf) {
+  if (!plan || !q_inf || c < 0 || c >= plan->n_cases) return fail(JR_EINVAL, "bad argument");
+  Physics& P = plan->host[c].P;
+  for (int k = 0; k < 5; ++k) P.q_inf[k] = k < plan->nvar ? q_inf[k] : 0.0;
+  const double g = P.gamma, rho = P.q_inf[0], u = P.q_inf[1], v = P.q_inf[2], p = P.q_inf[3];
+  P.U_inf[0] = rho;
+  P.U_inf[1] = rho * u;
+  P.U_inf[2] = rho * v;
+  P.U_inf[3] = p / (g - 1.0) + 0.5 * rho * (u * u + v * v);
+  P.U_inf[4] = rho * P.q_inf[4];
+  return upload_table(plan);
+}
+
+static int capture_step(jr_plan* plan, cudaGraph_t* g) {
+  if (cudaStreamBeginCapture(plan->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    return cuda_check("begin capture");
+  enqueue_step(plan);
+  if (cudaStreamEndCapture(plan->st, g) != cudaSuccess) return cuda_check("end capture");
+  return JR_OK;
+}
 
 int jr_graph_kernels(jr_plan* plan, int64_t* kernels_per_step) {
   if (!plan || !kernels_per_step) return fail(JR_EINVAL, "null argument");
   cudaGraph_t g;
-  if (cudaStreamBeginCapture(plan->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-    return cuda_check("begin capture");
-  enqueue_step(plan);
-  if (cudaStreamEndCapture(plan->st, &g) != cudaSuccess) return cuda_check("end capture");
+  int rc = capture_step(plan, &g);
+  if (rc) return rc;
   size_t n = 0;
   cudaGraphGetNodes(g, nullptr, &n);
   std::vector<cudaGraphNode_t> nodes(n);
@@ -540,10 +693,8 @@ int jr_graph_kernels(jr_plan* plan, int64_t* kernels_per_step) {
 static int ensure_graph(jr_plan* plan) {
   if (plan->graph) return JR_OK;
   cudaGraph_t g;
-  if (cudaStreamBeginCapture(plan->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-    return cuda_check("begin capture");
-  enqueue_step(plan);
-  if (cudaStreamEndCapture(plan->st, &g) != cudaSuccess) return cuda_check("end capture");
+  int rc = capture_step(plan, &g);
+  if (rc) return rc;
   if (cudaGraphInstantiate(&plan->graph, g, 0) != cudaSuccess) {
     cudaGraphDestroy(g);
     return cuda_check("graph instantiate");
@@ -554,16 +705,16 @@ static int ensure_graph(jr_plan* plan) {
 
 int jr_newton_steps_async(jr_plan* plan, int32_t n_steps, double* history_device) {
   if (!plan || n_steps < 0) return fail(JR_EINVAL, "bad argument");
-  if (n_steps > plan->hist_cap) return fail(JR_EINVAL, "at most 4096 steps per call");
+  if (n_steps > HIST_STEPS) return fail(JR_EINVAL, "at most 4096 steps per call");
   int rc = ensure_graph(plan);
   if (rc) return rc;
-  // the history position restarts at 0 for this call
-  cudaMemsetAsync(&plan->sc->hpos, 0, sizeof(int), plan->st);
+  // the history position of every case restarts at 0 for this call
+  for (int k = 0; k < plan->n_cases; ++k) cudaMemsetAsync(&plan->sc[k].hpos, 0, sizeof(int), plan->st);
   for (int k = 0; k < n_steps; ++k)
     if (cudaGraphLaunch(plan->graph, plan->st) != cudaSuccess) return cuda_check("graph launch");
   if (history_device && n_steps > 0)
-    cudaMemcpyAsync(history_device, plan->history, (size_t)n_steps * sizeof(double), cudaMemcpyDeviceToDevice,
-                    plan->st);
+    cudaMemcpyAsync(history_device, plan->history, (size_t)n_steps * plan->n_cases * sizeof(double),
+                    cudaMemcpyDeviceToDevice, plan->st);
   return cuda_check("jr_newton_steps");
 }
 
@@ -571,7 +722,8 @@ int jr_newton_steps(jr_plan* plan, int32_t n_steps, double* history) {
   int rc = jr_newton_steps_async(plan, n_steps, nullptr);
   if (rc) return rc;
   if (history && n_steps > 0)
-    cudaMemcpyAsync(history, plan->history, (size_t)n_steps * sizeof(double), cudaMemcpyDeviceToHost, plan->st);
+    cudaMemcpyAsync(history, plan->history, (size_t)n_steps * plan->n_cases * sizeof(double), cudaMemcpyDeviceToHost,
+                    plan->st);
   if (cudaStreamSynchronize(plan->st) != cudaSuccess) return cuda_check("jr_newton_steps");
   return cuda_check("jr_newton_steps");
 }
@@ -579,45 +731,46 @@ int jr_newton_steps(jr_plan* plan, int32_t n_steps, double* history) {
 int jr_time_kernels(jr_plan* plan, int32_t reps, double* ms) {
   if (!plan || !ms || reps < 1) return fail(JR_EINVAL, "bad argument");
   jr_plan* p = plan;
-  const Canvas& c = p->cv;
-  const bool sa = c.nvar == 5;
+  const CaseDev* t = p->cases;
+  const BatchDims& d = p->dims;
+  const bool sa = p->nvar == 5;
+  cudaStream_t st = p->st;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   // a consistent state for every kernel: base ghosts, wave speeds, the factor, an
   // active Krylov cycle with z = the residual
-  launch_ghosts(c, p->P, false, p->U, nullptr, p->qg, nullptr, nullptr, p->st);
-  launch_residual(c, p->P, p->visc, true, p->U, p->qg, p->R, p->tile_partial, p->st);
-  launch_faces(c, p->P, p->visc, p->U, p->lam, p->mflux, p->dflux, p->st);
-  launch_cells(c, p->P, p->visc, p->U, p->lam, p->mflux, p->dflux, p->sc, p->vdt, p->dflow, p->dsa, p->st);
-  launch_chain_factor(c, p->P, sa, p->mixed, p->U, p->lam, p->mflux, p->dflux, p->dflow, p->dsa, p->fflow, p->fsa,
-                      p->scratch, p->st);
-  cudaMemcpyAsync(p->z, p->R, (size_t)p->n_vec * sizeof(double), cudaMemcpyDeviceToDevice, p->st);
-  int one = 1;
-  cudaMemcpyAsync(&p->sc->active, &one, sizeof(int), cudaMemcpyHostToDevice, p->st);
-  cudaStreamSynchronize(p->st);
+  launch_ghosts(t, d, -1, 0, st);
+  launch_residual(t, d, p->visc, true, B_R, st);
+  launch_faces(t, d, p->visc, st);
+  launch_cells(t, d, p->visc, st);
+  launch_chain_factor(t, d, sa, p->mixed, st);
+  for (int k = 0; k < p->n_cases; ++k) {
+    const CaseDev& cd = p->host[k];
+    cudaMemcpyAsync(cd.z, cd.R, (size_t)cd.n_vec * sizeof(double), cudaMemcpyDeviceToDevice, st);
+  }
+  std::vector<Scalars> s(p->n_cases);
+  cudaMemcpyAsync(s.data(), p->sc, s.size() * sizeof(Scalars), cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+  for (Scalars& x : s) x.active = 1;
+  cudaMemcpyAsync(p->sc, s.data(), s.size() * sizeof(Scalars), cudaMemcpyHostToDevice, st);
+  cudaStreamSynchronize(st);
   auto timed = [&](int k, auto&& launch) {
     launch();
-    cudaEventRecord(e0, p->st);
+    cudaEventRecord(e0, st);
     for (int r = 0; r < reps; ++r) launch();
-    cudaEventRecord(e1, p->st);
+    cudaEventRecord(e1, st);
     cudaEventSynchronize(e1);
-    float t = 0.f;
-    cudaEventElapsedTime(&t, e0, e1);
-    ms[k] = (double)t / reps;
+    float ms1 = 0.f;
+    cudaEventElapsedTime(&ms1, e0, e1);
+    ms[k] = (double)ms1 / reps;
   };
-  timed(0, [&] { launch_residual(c, p->P, p->visc, true, p->U, p->qg, p->R, p->tile_partial, p->st); });
-  timed(1, [&] { launch_jvp(c, p->P, p->visc, p->U, p->qg, p->z, p->dqg, p->vdt, p->w, nullptr, p->st); });
-  timed(2, [&] { launch_ghosts(c, p->P, true, p->U, p->z, p->qg, p->dqg, nullptr, p->st); });
-  timed(3, [&] {
-    launch_chain_apply(c, sa, p->mixed, p->fflow, p->fsa, p->R, nullptr, nullptr, nullptr, false, p->tmp, p->st);
-  });
-  timed(4, [&] {
-    launch_chain_factor(c, p->P, sa, p->mixed, p->U, p->lam, p->mflux, p->dflux, p->dflow, p->dsa, p->fflow, p->fsa,
-                        p->scratch, p->st);
-  });
-  timed(5, [&] { launch_arnoldi_orth(p->sc, p->V, p->mixed, (size_t)p->n_vec, p->m - 1, p->m, p->w, p->n_vec,
-                                     p->red, p->st); });
+  timed(0, [&] { launch_residual(t, d, p->visc, true, B_R, st); });
+  timed(1, [&] { launch_jvp(t, d, p->visc, B_Z, B_VDT, B_W, 0, st); });
+  timed(2, [&] { launch_ghosts(t, d, B_Z, 0, st); });
+  timed(3, [&] { launch_chain_apply(t, d, sa, p->mixed, B_R, 0, -1, B_TMP, 0, st); });
+  timed(4, [&] { launch_chain_factor(t, d, sa, p->mixed, st); });
+  timed(5, [&] { launch_arnoldi_orth(t, d, p->mixed, p->m - 1, st); });
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return cuda_check("jr_time_kernels");
@@ -625,11 +778,16 @@ int jr_time_kernels(jr_plan* plan, int32_t reps, double* ms) {
 
 int jr_forces(jr_plan* plan, const double* U, double* out) {
   if (!plan || !out) return fail(JR_EINVAL, "null argument");
-  const double* u = U ? U : plan->U;
-  launch_ghosts(plan->cv, plan->P, false, u, nullptr, plan->qg, nullptr, nullptr, plan->st);
-  launch_forces(plan->cv, plan->P, u, plan->qg, plan->force_length, plan->cx0, plan->cy0, plan->force_out, plan->st);
-  cudaMemcpyAsync(out, plan->force_out, 6 * sizeof(double), cudaMemcpyDeviceToHost, plan->st);
+  Adhoc a(plan);
+  if (U) a.vec(&CaseDev::U, U);
+  const CaseDev* t = a.upload();
+  launch_ghosts(t, plan->dims, -1, 0, plan->st);
+  launch_forces(t, plan->dims, plan->st);
+  std::vector<double> f((size_t)8 * plan->n_cases);
+  cudaMemcpyAsync(f.data(), plan->force_out, f.size() * sizeof(double), cudaMemcpyDeviceToHost, plan->st);
   if (cudaStreamSynchronize(plan->st) != cudaSuccess) return cuda_check("jr_forces");
+  for (int k = 0; k < plan->n_cases; ++k)
+    for (int i = 0; i < 6; ++i) out[6 * k + i] = f[8 * k + i];
   return cuda_check("jr_forces");
 }
 

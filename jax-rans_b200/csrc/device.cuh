@@ -92,4 +92,70 @@ struct Reduce {
   int blocks;
 };
 
+// One case of a batch on the device: its canvas, physics, solver settings, buffers and
+// scalars.  Kernels take a table of these and read their case from a grid dimension, so
+// one launch advances every case of a batch; a single case is a batch of one.
+struct CaseDev {
+  Canvas c;
+  Physics P;
+  Config cfg;
+  double *U, *qg, *dqg, *R, *b, *x, *action, *r, *w, *z, *tmp, *vdt, *dflow, *dsa, *lam, *mflux, *dflux;
+  double *tile_partial, *history, *force_out;
+  void *V, *fflow, *fsa, *scratch;
+  Scalars* sc;
+  double* partial;          // reduction partials of this case
+  unsigned int* ticket;     // its last-block ticket
+  double force_length, moment_centre[2];   // force coefficients' reference length and moment centre
+  int n_vec, m, visc, mixed, n_tiles, tiles_x, tiles_y;
+  int enabled;              // 0: a free slot, every kernel returns at once
+};
+
+// Buffers a kernel may be told to read or write (resolved per case)
+enum Buf { B_U = 0, B_QG, B_DQG, B_R, B_B, B_X, B_ACTION, B_RR, B_W, B_Z, B_TMP, B_VDT, B_ZERO, B_NONE };
+
+__device__ __forceinline__ double* buf(const CaseDev& cd, int id) {
+  switch (id) {
+    case B_U: return cd.U;
+    case B_QG: return cd.qg;
+    case B_DQG: return cd.dqg;
+    case B_R: return cd.R;
+    case B_B: return cd.b;
+    case B_X: return cd.x;
+    case B_ACTION: return cd.action;
+    case B_RR: return cd.r;
+    case B_W: return cd.w;
+    case B_Z: return cd.z;
+    case B_TMP: return cd.tmp;
+    case B_VDT: return cd.vdt;
+    default: return nullptr;
+  }
+}
+
+// Copy a case's descriptor into shared memory (every thread of the block calls it).
+__device__ __forceinline__ const CaseDev& stage_case(const CaseDev* cases, int ci, CaseDev* smem) {
+  static_assert(sizeof(CaseDev) % 8 == 0, "CaseDev is copied in 8-byte words");
+  const unsigned long long* src = reinterpret_cast<const unsigned long long*>(cases + ci);
+  unsigned long long* dst = reinterpret_cast<unsigned long long*>(smem);
+  for (int k = threadIdx.x; k < (int)(sizeof(CaseDev) / 8); k += blockDim.x) dst[k] = src[k];
+  __syncthreads();
+  return *smem;
+}
+
+// Grid extents of a batch's launches: the largest of each per-case count.
+struct BatchDims {
+  int n_cases;
+  int tiles_x, tiles_y;     // residual tiles
+  int ghost_records;        // both stages
+  int faces, cells;         // canvas faces, canvas cells
+  int n_vec;                // nvar * cells
+  int chain_blocks;         // chains + off-chain blocks of the line solve
+  int max_L;                // longest chain
+};
+
+// the number of blocks a per-case reduction over n elements uses (<= the grid's x)
+__host__ __device__ __forceinline__ int chunk_blocks(int n) {
+  int b = (n + 1023) / 1024;
+  return b < 1 ? 1 : (b > 2 * 148 ? 2 * 148 : b);
+}
+
 }  // namespace jr

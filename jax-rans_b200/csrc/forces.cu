@@ -71,9 +71,16 @@ __device__ void wall_viscous(const Canvas& c, const Physics& P, const double* U,
   fy = t01 * sx + t11 * sy;
 }
 
-// out: cl, cd, cm, cd_friction, fx, fy
-__global__ void __launch_bounds__(256) k_forces(Canvas c, Physics P, const double* U, const double* qg, double length, double cx0,
-                         double cy0, double* out) {
+// force_out of each case: cl, cd, cm, cd_friction, fx, fy.  One CTA per case.
+__global__ void __launch_bounds__(256) k_forces(const CaseDev* __restrict__ cases) {
+  const CaseDev& cd = cases[blockIdx.y];
+  if (!cd.enabled) return;
+  const Canvas& c = cd.c;
+  const Physics& P = cd.P;
+  const double* U = cd.U;
+  const double* qg = cd.qg;
+  const double length = cd.force_length, cx0 = cd.moment_centre[0], cy0 = cd.moment_centre[1];
+  double* out = cd.force_out;
   __shared__ double red[6][32];
   double acc[6] = {0, 0, 0, 0, 0, 0};
   const double rho = P.q_inf[0], u = P.q_inf[1], v = P.q_inf[2];
@@ -133,9 +140,8 @@ __global__ void __launch_bounds__(256) k_forces(Canvas c, Physics P, const doubl
   }
 }
 
-void launch_forces(const Canvas& c, const Physics& P, const double* U, const double* qg, double length, double cx0,
-                   double cy0, double* out, cudaStream_t st) {
-  k_forces<<<1, 256, 0, st>>>(c, P, U, qg, length, cx0, cy0, out);
+void launch_forces(const CaseDev* cases, const BatchDims& d, cudaStream_t st) {
+  k_forces<<<dim3(1, d.n_cases), 256, 0, st>>>(cases);
 }
 
 }  // namespace jr

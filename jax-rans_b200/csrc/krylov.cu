@@ -31,7 +31,7 @@ __device__ __forceinline__ double warp_max(double x) {
 // Block-sums `vals` into partial[block * W + k]; true in thread 0 of the last block to
 // finish, whose `vals` then hold the fixed-order totals over blocks.
 template <int W, bool MAX = false>
-__device__ bool reduce_last(double (&vals)[W], double* partial, unsigned* ticket) {
+__device__ bool reduce_last(double (&vals)[W], double* partial, unsigned* ticket, int nb) {
   __shared__ double sm[RED_THREADS / 32][W];
   __shared__ bool last;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -50,7 +50,7 @@ __device__ bool reduce_last(double (&vals)[W], double* partial, unsigned* ticket
     }
     __threadfence();
     unsigned prev = atomicAdd(ticket, 1u);
-    last = prev == gridDim.x - 1;
+    last = prev == (unsigned)nb - 1;
   }
   __syncthreads();
   if (!last || threadIdx.x != 0) return false;
@@ -59,31 +59,43 @@ __device__ bool reduce_last(double (&vals)[W], double* partial, unsigned* ticket
   for (int k = 0; k < W; ++k) {
     const volatile double* p = partial;
     double t = p[k];
-    for (int b = 1; b < (int)gridDim.x; ++b) t = MAX ? nmax(t, p[b * W + k]) : t + p[b * W + k];
+    for (int b = 1; b < nb; ++b) t = MAX ? nmax(t, p[b * W + k]) : t + p[b * W + k];
     vals[k] = t;
   }
   *ticket = 0u;
   return true;
 }
 
-// The range of elements block b owns
-__device__ __forceinline__ void chunk(int n, int& lo, int& hi) {
-  int per = (n + gridDim.x - 1) / gridDim.x;
+// The range of elements block b of nb owns
+__device__ __forceinline__ void chunk(int n, int nb, int& lo, int& hi) {
+  int per = (n + nb - 1) / nb;
   lo = blockIdx.x * per;
   hi = min(n, lo + per);
 }
 
 // ---- GMRES ---------------------------------------------------------------------------
+// Every kernel takes the batch's case table and reads its case from blockIdx.y.  The
+// per-case block count of a reduction depends on that case's size alone, so a case's
+// scalars are bitwise the same alone and in a batch; the blocks past it return at once.
+
+// blocks of a chunked per-case reduction over n elements (<= the grid's x)
+__device__ __forceinline__ bool chunk_owner(int n, int& nb, int& lo, int& hi) {
+  nb = chunk_blocks(n);
+  if ((int)blockIdx.x >= nb) return false;
+  chunk(n, nb, lo, hi);
+  return true;
+}
 
 // Start of a Newton step: b = -R, x = action = 0, r = b; |b|; the residual norm of the
 // density row from the tile partials; the history entry.
-__global__ void __launch_bounds__(RED_THREADS) k_gmres_init(Scalars* sc, const double* R, double* b, double* x,
-                                                            double* action, double* r, int n,
-                                                            const double* tile_partial, int n_tiles,
-                                                            double volume_sum, double* history, double* partial,
-                                                            unsigned* ticket) {
-  int lo, hi;
-  chunk(n, lo, hi);
+__global__ void __launch_bounds__(RED_THREADS) k_gmres_init(const CaseDev* __restrict__ cases, int n_cases_hist) {
+  const CaseDev& cd = cases[blockIdx.y];
+  if (!cd.enabled) return;
+  const int n = cd.n_vec;
+  int nb, lo, hi;
+  if (!chunk_owner(n, nb, lo, hi)) return;
+  const double* __restrict__ R = cd.R;
+  double *b = cd.b, *r = cd.r, *x = cd.x, *action = cd.action;
   double acc[1] = {0.0};
   for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
     double v = -R[i];
@@ -93,12 +105,14 @@ __global__ void __launch_bounds__(RED_THREADS) k_gmres_init(Scalars* sc, const d
     action[i] = 0.0;
     acc[0] += v * v;
   }
-  if (reduce_last<1>(acc, partial, ticket)) {
+  if (reduce_last<1>(acc, cd.partial, cd.ticket, nb)) {
+    Scalars* sc = cd.sc;
     double s = 0.0;
-    for (int t = 0; t < n_tiles; ++t) s += tile_partial[t];
-    double nrm = sqrt(s / volume_sum);
+    for (int t = 0; t < cd.n_tiles; ++t) s += cd.tile_partial[t];
+    double nrm = sqrt(s / cd.c.volume_sum);
     sc->norm = nrm;
-    if (history != nullptr) history[sc->hpos] = nrm;
+    // history: [step][case] over the cases of the batch
+    if (cd.history != nullptr) cd.history[(size_t)sc->hpos * n_cases_hist + blockIdx.y] = nrm;
     sc->hpos += 1;
     sc->bnorm = sqrt(acc[0]);
     sc->rnorm = sc->bnorm;
@@ -108,13 +122,18 @@ __global__ void __launch_bounds__(RED_THREADS) k_gmres_init(Scalars* sc, const d
   }
 }
 
-// Cycle start: the restart test between cycles, beta = |r|
-__global__ void k_cycle_start(Scalars* sc, Config cfg) {
+// Cycle start: the restart test between cycles, beta = |r|; H = 0
+__global__ void k_cycle_start(const CaseDev* __restrict__ cases) {
+  const CaseDev& cd = cases[blockIdx.y];
+  if (!cd.enabled) return;
+  Scalars* sc = cd.sc;
+  const Config& cfg = cd.cfg;
+  for (int k = threadIdx.x; k < (cfg.restart + 1) * cfg.restart; k += blockDim.x) sc->H[k] = 0.0;
+  if (threadIdx.x != 0) return;
   bool go = sc->active != 0 && sc->cycle < cfg.maxiter && sc->rnorm > cfg.krylov_tol * sc->bnorm;
   sc->active = go ? 1 : 0;
   sc->beta = sc->rnorm;
   sc->inv_nrm = 1.0 / fmax(sc->beta, 2.2250738585072014e-308);
-  for (int k = 0; k < (cfg.restart + 1) * cfg.restart; ++k) sc->H[k] = 0.0;
 }
 
 // The three passes of CGS2 over the basis, one kernel: MODE 0 h = V^T w; MODE 1
@@ -122,11 +141,21 @@ __global__ void k_cycle_start(Scalars* sc, Config cfg) {
 // thread owns MD_E elements and keeps NK accumulators in registers; all loads of a
 // pass are independent of one another.
 template <class TV, int NK, int MODE>
-__global__ void __launch_bounds__(RED_THREADS) k_mdot(Scalars* sc, const TV* __restrict__ V, size_t ldv, int nk,
-                                                      double* __restrict__ w, int n, const double* __restrict__ hin,
-                                                      double* __restrict__ partial, unsigned* __restrict__ ticket,
-                                                      double* __restrict__ hout, int j, int m) {
+__global__ void __launch_bounds__(RED_THREADS) k_mdot(const CaseDev* __restrict__ cases, int nk, int j) {
+  const CaseDev& cd = cases[blockIdx.y];
+  if (!cd.enabled) return;
+  Scalars* sc = cd.sc;
   if (sc->active == 0) return;
+  const int n = cd.n_vec, m = cd.m;
+  const int nb = (n + RED_THREADS * MD_E - 1) / (RED_THREADS * MD_E);
+  if ((int)blockIdx.x >= nb) return;
+  const TV* __restrict__ V = (const TV*)cd.V;
+  const size_t ldv = (size_t)n;
+  double* __restrict__ w = cd.w;
+  double* __restrict__ partial = cd.partial;
+  unsigned* ticket = cd.ticket;
+  const double* hin = MODE == 1 ? sc->h1 : sc->h2;
+  double* hout = MODE == 0 ? sc->h1 : sc->h2;
   constexpr int NA = MODE == 2 ? 1 : NK;
   __shared__ double sm[RED_THREADS / 32][NA];
   __shared__ bool last;
@@ -178,14 +207,14 @@ __global__ void __launch_bounds__(RED_THREADS) k_mdot(Scalars* sc, const TV* __r
   }
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == (unsigned)nb - 1;
   __syncthreads();
   if (!last) return;
   __threadfence();
   if ((int)threadIdx.x < width) {
     const volatile double* p = partial;
     double t = 0.0;
-    for (int b = 0; b < (int)gridDim.x; ++b) t += p[b * (MAX_KRYLOV + 1) + threadIdx.x];
+    for (int b = 0; b < nb; ++b) t += p[b * (MAX_KRYLOV + 1) + threadIdx.x];
     if constexpr (MODE == 2) {
       double nrm = sqrt(t);
       for (int k = 0; k < nk; ++k) sc->H[k + (m + 1) * j] = sc->h1[k] + sc->h2[k];
@@ -202,11 +231,15 @@ __global__ void __launch_bounds__(RED_THREADS) k_mdot(Scalars* sc, const TV* __r
 }
 
 // argmin |beta e1 - H y| by Givens rotations, pivots below rcond * the largest dropped
-// (krylov.py:100-137); hy = H y.  One CTA: rotation j, once formed, is applied to rows
-// j, j+1 of every later column at once -- each entry sees the same rotations in the
-// same order as column-by-column elimination.
-__global__ void __launch_bounds__(64) k_lstsq(Scalars* sc, int m) {
+// (krylov.py:100-137); hy = H y.  One CTA per case: rotation j, once formed, is applied
+// to rows j, j+1 of every later column at once -- each entry sees the same rotations in
+// the same order as column-by-column elimination.
+__global__ void __launch_bounds__(64) k_lstsq(const CaseDev* __restrict__ cases) {
+  const CaseDev& cd = cases[blockIdx.y];
+  if (!cd.enabled) return;
+  Scalars* sc = cd.sc;
   if (sc->active == 0) return;
+  const int m = cd.m;
   __shared__ double h[MAX_KRYLOV + 1][MAX_KRYLOV + 1];
   __shared__ double g[MAX_KRYLOV + 1], cs[MAX_KRYLOV], sn[MAX_KRYLOV], y[MAX_KRYLOV];
   __shared__ double largest;
@@ -269,9 +302,17 @@ __global__ void __launch_bounds__(64) k_lstsq(Scalars* sc, int m) {
 
 // tmp = V_{0..m-1} y; action += V_{0..m} (H y), V_m = w / |w|
 template <class TV>
-__global__ void k_combine(const Scalars* sc, const TV* V, size_t ldv, int m, const double* w, double* tmp,
-                          double* action, int n) {
+__global__ void k_combine(const CaseDev* __restrict__ cases) {
+  const CaseDev& cd = cases[blockIdx.y];
+  if (!cd.enabled) return;
+  const Scalars* sc = cd.sc;
   if (sc->active == 0) return;
+  const int m = cd.m, n = cd.n_vec;
+  const TV* __restrict__ V = (const TV*)cd.V;
+  const size_t ldv = (size_t)n;
+  const double* __restrict__ w = cd.w;
+  double* __restrict__ tmp = cd.tmp;
+  double* __restrict__ action = cd.action;
   __shared__ double y[MAX_KRYLOV], hy[MAX_KRYLOV + 1];
   if ((int)threadIdx.x < m) y[threadIdx.x] = sc->y[threadIdx.x];
   if ((int)threadIdx.x <= m) hy[threadIdx.x] = sc->hy[threadIdx.x];
@@ -291,12 +332,15 @@ __global__ void k_combine(const Scalars* sc, const TV* V, size_t ldv, int m, con
 }
 
 // x += z; r = b - action; |r|; the cycle count
-__global__ void __launch_bounds__(RED_THREADS) k_cycle_end(Scalars* sc, double* x, const double* z, const double* b,
-                                                           const double* action, double* r, int n, double* partial,
-                                                           unsigned* ticket) {
+__global__ void __launch_bounds__(RED_THREADS) k_cycle_end(const CaseDev* __restrict__ cases) {
+  const CaseDev& cd = cases[blockIdx.y];
+  if (!cd.enabled) return;
+  Scalars* sc = cd.sc;
   if (sc->active == 0) return;
-  int lo, hi;
-  chunk(n, lo, hi);
+  int nb, lo, hi;
+  if (!chunk_owner(cd.n_vec, nb, lo, hi)) return;
+  double *x = cd.x, *r = cd.r;
+  const double *z = cd.z, *b = cd.b, *action = cd.action;
   double acc[1] = {0.0};
   for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
     x[i] += z[i];
@@ -304,7 +348,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_cycle_end(Scalars* sc, double* 
     r[i] = ri;
     acc[0] += ri * ri;
   }
-  if (reduce_last<1>(acc, partial, ticket)) {
+  if (reduce_last<1>(acc, cd.partial, cd.ticket, nb)) {
     sc->rnorm = sqrt(acc[0]);
     sc->cycle += 1;
   }
@@ -313,14 +357,19 @@ __global__ void __launch_bounds__(RED_THREADS) k_cycle_end(Scalars* sc, double* 
 // ---- the Newton update -------------------------------------------------------------
 
 // omega = min(1, fraction / max relative change of rho, p, nu_hat)  (implicit.py:54-81)
-__global__ void __launch_bounds__(RED_THREADS) k_relax(Scalars* sc, Canvas c, Physics P, Config cfg, const double* U,
-                                                       const double* dU, double* partial, unsigned* ticket) {
+__global__ void __launch_bounds__(RED_THREADS) k_relax(const CaseDev* __restrict__ cases) {
+  const CaseDev& cd = cases[blockIdx.y];
+  if (!cd.enabled) return;
+  const Canvas& c = cd.c;
+  const Config& cfg = cd.cfg;
   const int N = c.ncanvas(), nv = c.nvar;
-  const double g = P.gamma;
+  int nb, lo, hi;
+  if (!chunk_owner(N, nb, lo, hi)) return;
+  const double g = cd.P.gamma;
+  const double* __restrict__ U = cd.U;
+  const double* __restrict__ dU = cd.x;
   double worst[1] = {0.0};
   if (cfg.max_relative_update > 0.0) {
-    int lo, hi;
-    chunk(N, lo, hi);
     for (int idx = lo + threadIdx.x; idx < hi; idx += blockDim.x) {
       double rho = U[idx], u = U[N + idx] / rho, v = U[2 * N + idx] / rho;
       double p = (g - 1.0) * (U[3 * N + idx] - 0.5 * rho * (u * u + v * v));
@@ -335,7 +384,8 @@ __global__ void __launch_bounds__(RED_THREADS) k_relax(Scalars* sc, Canvas c, Ph
       worst[0] = nmax(worst[0], w);
     }
   }
-  if (reduce_last<1, true>(worst, partial, ticket)) {
+  if (reduce_last<1, true>(worst, cd.partial, cd.ticket, nb)) {
+    Scalars* sc = cd.sc;
     sc->worst = worst[0];
     if (cfg.max_relative_update > 0.0) {
       double q = cfg.max_relative_update / (worst[0] != worst[0] ? NAN : fmax(worst[0], 1e-300));
@@ -347,13 +397,20 @@ __global__ void __launch_bounds__(RED_THREADS) k_relax(Scalars* sc, Canvas c, Ph
 }
 
 // the linear reduction, physicality of the candidate, accept, the SER CFL ramp
-__global__ void __launch_bounds__(RED_THREADS) k_accept(Scalars* sc, Canvas c, Physics P, Config cfg, const double* U,
-                                                        const double* dU, const double* action, const double* R,
-                                                        double* partial, unsigned* ticket) {
+__global__ void __launch_bounds__(RED_THREADS) k_accept(const CaseDev* __restrict__ cases) {
+  const CaseDev& cd = cases[blockIdx.y];
+  if (!cd.enabled) return;
+  const Canvas& c = cd.c;
+  const Config& cfg = cd.cfg;
+  Scalars* sc = cd.sc;
   const int N = c.ncanvas(), nv = c.nvar, n = nv * N;
-  const double g = P.gamma, om = sc->omega;
-  int lo, hi;
-  chunk(n, lo, hi);
+  int nb, lo, hi;
+  if (!chunk_owner(n, nb, lo, hi)) return;
+  const double g = cd.P.gamma, om = sc->omega;
+  const double* __restrict__ U = cd.U;
+  const double* __restrict__ dU = cd.x;
+  const double* __restrict__ action = cd.action;
+  const double* __restrict__ R = cd.R;
   double acc[3] = {0.0, 0.0, 0.0};  // |omega action + R|^2, |R|^2, bad cells
   for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
     double t = om * action[i] + R[i];
@@ -370,7 +427,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_accept(Scalars* sc, Canvas c, P
       if (!ok) acc[2] += 1.0;
     }
   }
-  if (reduce_last<3>(acc, partial, ticket)) {
+  if (reduce_last<3>(acc, cd.partial, cd.ticket, nb)) {
     double lin = sqrt(acc[0]) / fmax(sqrt(acc[1]), 1e-300);
     bool physical = acc[2] == 0.0;
     bool accept = physical && lin < 1.0;
@@ -395,76 +452,106 @@ __global__ void __launch_bounds__(RED_THREADS) k_accept(Scalars* sc, Canvas c, P
   }
 }
 
-__global__ void k_update(const Scalars* sc, double* U, const double* dU, int n) {
+__global__ void k_update(const CaseDev* __restrict__ cases) {
+  const CaseDev& cd = cases[blockIdx.y];
+  if (!cd.enabled) return;
+  const Scalars* sc = cd.sc;
   if (sc->accept == 0) return;
   const double om = sc->omega;
+  double* __restrict__ U = cd.U;
+  const double* __restrict__ dU = cd.x;
+  const int n = cd.n_vec;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) U[i] = U[i] + om * dU[i];
+}
+
+// z = scale * src, optionally V_j = z rounded to the basis type: the Arnoldi step
+// without a preconditioner (scale_on: by 1/|w| of the case)
+template <class TV>
+__global__ void k_scale_copy(const CaseDev* __restrict__ cases, int src_id, int scale_on, int vout_j, int out_id,
+                             int check_active) {
+  const CaseDev& cd = cases[blockIdx.y];
+  if (!cd.enabled || (check_active && cd.sc->active == 0)) return;
+  const int n = cd.n_vec;
+  const double* __restrict__ src = buf(cd, src_id);
+  double* __restrict__ z = buf(cd, out_id);
+  TV* vout = vout_j >= 0 ? (TV*)cd.V + (size_t)vout_j * n : nullptr;
+  const double s = scale_on ? cd.sc->inv_nrm : 1.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double x = s * src[i];
+    if (vout != nullptr) {
+      TV xv = TV(x);
+      vout[i] = xv;
+      x = double(xv);
+    }
+    z[i] = x;
+  }
 }
 
 // ---- launch wrappers ------------------------------------------------------------------
 
-// blocks of the basis passes (and the largest block count any reduction uses)
+// blocks of the basis passes of a case of n elements (and the largest block count any
+// reduction uses: the size of a case's partial array)
 int reduce_blocks(int n) { return max(2 * 148, (n + RED_THREADS * MD_E - 1) / (RED_THREADS * MD_E)); }
 
-static int chunk_blocks(int n) { return max(1, min(2 * 148, (n + 1023) / 1024)); }
+static dim3 chunk_grid(const BatchDims& d) { return dim3(chunk_blocks(d.n_vec), d.n_cases); }
+static dim3 stride_grid(const BatchDims& d) { return dim3(min((d.n_vec + 255) / 256, 148 * 4), d.n_cases); }
 
-void launch_gmres_init(Scalars* sc, const double* R, double* b, double* x, double* action, double* r, int n,
-                       const double* tile_partial, int n_tiles, double volume_sum, double* history, Reduce red,
-                       cudaStream_t st) {
-  k_gmres_init<<<chunk_blocks(n), RED_THREADS, 0, st>>>(sc, R, b, x, action, r, n, tile_partial, n_tiles, volume_sum,
-                                                        history, red.partial, red.ticket);
+void launch_gmres_init(const CaseDev* cases, const BatchDims& d, cudaStream_t st) {
+  k_gmres_init<<<chunk_grid(d), RED_THREADS, 0, st>>>(cases, d.n_cases);
 }
 
-void launch_cycle_start(Scalars* sc, Config cfg, cudaStream_t st) { k_cycle_start<<<1, 1, 0, st>>>(sc, cfg); }
+void launch_cycle_start(const CaseDev* cases, const BatchDims& d, cudaStream_t st) {
+  k_cycle_start<<<dim3(1, d.n_cases), 128, 0, st>>>(cases);
+}
 
 template <class TV, int NK>
-static void arnoldi_nk(Scalars* sc, const TV* V, size_t ldv, int j, int m, double* w, int n, Reduce red,
-                       cudaStream_t st) {
-  int blocks = (n + RED_THREADS * MD_E - 1) / (RED_THREADS * MD_E);
-  k_mdot<TV, NK, 0><<<blocks, RED_THREADS, 0, st>>>(sc, V, ldv, j + 1, w, n, nullptr, red.partial, red.ticket,
-                                                     sc->h1, j, m);
-  k_mdot<TV, NK, 1><<<blocks, RED_THREADS, 0, st>>>(sc, V, ldv, j + 1, w, n, sc->h1, red.partial, red.ticket,
-                                                     sc->h2, j, m);
-  k_mdot<TV, NK, 2><<<blocks, RED_THREADS, 0, st>>>(sc, V, ldv, j + 1, w, n, sc->h2, red.partial, red.ticket,
-                                                     nullptr, j, m);
+static void arnoldi_nk(const CaseDev* cases, const BatchDims& d, int j, cudaStream_t st) {
+  dim3 grid((d.n_vec + RED_THREADS * MD_E - 1) / (RED_THREADS * MD_E), d.n_cases);
+  k_mdot<TV, NK, 0><<<grid, RED_THREADS, 0, st>>>(cases, j + 1, j);
+  k_mdot<TV, NK, 1><<<grid, RED_THREADS, 0, st>>>(cases, j + 1, j);
+  k_mdot<TV, NK, 2><<<grid, RED_THREADS, 0, st>>>(cases, j + 1, j);
 }
 
 template <class TV>
-static void arnoldi_t(Scalars* sc, const TV* V, size_t ldv, int j, int m, double* w, int n, Reduce red,
-                      cudaStream_t st) {
+static void arnoldi_t(const CaseDev* cases, const BatchDims& d, int j, cudaStream_t st) {
   const int nk = j + 1;
-  if (nk <= 8) arnoldi_nk<TV, 8>(sc, V, ldv, j, m, w, n, red, st);
-  else if (nk <= 16) arnoldi_nk<TV, 16>(sc, V, ldv, j, m, w, n, red, st);
-  else if (nk <= 32) arnoldi_nk<TV, 32>(sc, V, ldv, j, m, w, n, red, st);
-  else arnoldi_nk<TV, 64>(sc, V, ldv, j, m, w, n, red, st);
+  if (nk <= 8) arnoldi_nk<TV, 8>(cases, d, j, st);
+  else if (nk <= 16) arnoldi_nk<TV, 16>(cases, d, j, st);
+  else if (nk <= 32) arnoldi_nk<TV, 32>(cases, d, j, st);
+  else arnoldi_nk<TV, 64>(cases, d, j, st);
 }
 
-void launch_arnoldi_orth(Scalars* sc, const void* V, bool fp32, size_t ldv, int j, int m, double* w, int n,
-                         Reduce red, cudaStream_t st) {
-  if (fp32) arnoldi_t<float>(sc, (const float*)V, ldv, j, m, w, n, red, st);
-  else arnoldi_t<double>(sc, (const double*)V, ldv, j, m, w, n, red, st);
+// orthogonalise w against V_0..V_j (CGS2) and append column j of H
+void launch_arnoldi_orth(const CaseDev* cases, const BatchDims& d, bool fp32, int j, cudaStream_t st) {
+  if (fp32) arnoldi_t<float>(cases, d, j, st);
+  else arnoldi_t<double>(cases, d, j, st);
 }
 
-void launch_lstsq(Scalars* sc, int m, cudaStream_t st) { k_lstsq<<<1, 64, 0, st>>>(sc, m); }
-
-void launch_combine(const Scalars* sc, const void* V, bool fp32, size_t ldv, int m, const double* w, double* tmp,
-                    double* action, int n, cudaStream_t st) {
-  int blocks = min((n + 255) / 256, 148 * 4);
-  if (fp32) k_combine<float><<<blocks, 256, 0, st>>>(sc, (const float*)V, ldv, m, w, tmp, action, n);
-  else k_combine<double><<<blocks, 256, 0, st>>>(sc, (const double*)V, ldv, m, w, tmp, action, n);
+void launch_lstsq(const CaseDev* cases, const BatchDims& d, cudaStream_t st) {
+  k_lstsq<<<dim3(1, d.n_cases), 64, 0, st>>>(cases);
 }
 
-void launch_cycle_end(Scalars* sc, double* x, const double* z, const double* b, const double* action, double* r,
-                      int n, Reduce red, cudaStream_t st) {
-  k_cycle_end<<<chunk_blocks(n), RED_THREADS, 0, st>>>(sc, x, z, b, action, r, n, red.partial, red.ticket);
+void launch_combine(const CaseDev* cases, const BatchDims& d, bool fp32, cudaStream_t st) {
+  if (fp32) k_combine<float><<<stride_grid(d), 256, 0, st>>>(cases);
+  else k_combine<double><<<stride_grid(d), 256, 0, st>>>(cases);
 }
 
-void launch_newton_update(Scalars* sc, const Canvas& c, const Physics& P, Config cfg, double* U, const double* dU,
-                          const double* action, const double* R, Reduce red, cudaStream_t st) {
-  int N = c.NI * c.NJ, n = c.nvar * N;
-  k_relax<<<chunk_blocks(N), RED_THREADS, 0, st>>>(sc, c, P, cfg, U, dU, red.partial, red.ticket);
-  k_accept<<<chunk_blocks(n), RED_THREADS, 0, st>>>(sc, c, P, cfg, U, dU, action, R, red.partial, red.ticket);
-  k_update<<<min((n + 255) / 256, 148 * 4), 256, 0, st>>>(sc, U, dU, n);
+void launch_cycle_end(const CaseDev* cases, const BatchDims& d, cudaStream_t st) {
+  k_cycle_end<<<chunk_grid(d), RED_THREADS, 0, st>>>(cases);
+}
+
+void launch_scale_copy(const CaseDev* cases, const BatchDims& d, bool fp32, int src_id, int scale_on, int vout_j,
+                       int out_id, int check_active, cudaStream_t st) {
+  if (fp32 && vout_j >= 0)
+    k_scale_copy<float><<<stride_grid(d), 256, 0, st>>>(cases, src_id, scale_on, vout_j, out_id, check_active);
+  else
+    k_scale_copy<double><<<stride_grid(d), 256, 0, st>>>(cases, src_id, scale_on, vout_j, out_id, check_active);
+}
+
+void launch_newton_update(const CaseDev* cases, const BatchDims& d, cudaStream_t st) {
+  k_relax<<<dim3(chunk_blocks(d.cells), d.n_cases), RED_THREADS, 0, st>>>(cases);
+  k_accept<<<chunk_grid(d), RED_THREADS, 0, st>>>(cases);
+  k_update<<<stride_grid(d), 256, 0, st>>>(cases);
 }
 
 }  // namespace jr

@@ -157,13 +157,21 @@ __device__ __forceinline__ int level_rows(int L, int level) {
 // scratch holds the level's reduced system (a, d, c: 3 x 16 x rows) and the next one's.
 // ------------------------------------------------------------------------------------
 template <class TF, bool SA>
-__global__ void __launch_bounds__(LS_THREADS) k_cr_factor(Canvas cv, Physics P, const double* __restrict__ U,
-                                                          const double* __restrict__ lam,
-                                                          const double* __restrict__ mflux,
-                                                          const double* __restrict__ dflux,
-                                                          const double* __restrict__ dflow,
-                                                          const double* __restrict__ dsa, TF* __restrict__ fflow,
-                                                          TF* __restrict__ fsa, TF* __restrict__ scratch) {
+__global__ void __launch_bounds__(LS_THREADS) k_cr_factor(const CaseDev* __restrict__ cases) {
+  __shared__ CaseDev scase;
+  const CaseDev& cd = stage_case(cases, blockIdx.y, &scase);
+  if (!cd.enabled || (int)blockIdx.x >= cd.c.n_chains) return;
+  const Canvas& cv = cd.c;
+  const Physics& P = cd.P;
+  const double* __restrict__ U = cd.U;
+  const double* __restrict__ lam = cd.lam;
+  const double* __restrict__ mflux = cd.mflux;
+  const double* __restrict__ dflux = cd.dflux;
+  const double* __restrict__ dflow = cd.dflow;
+  const double* __restrict__ dsa = cd.dsa;
+  TF* __restrict__ fflow = (TF*)cd.fflow;
+  TF* __restrict__ fsa = (TF*)cd.fsa;
+  TF* __restrict__ scratch = (TF*)cd.scratch;
   const int c = blockIdx.x, n = cv.n_chains;
   const int L = cv.ch_len[c];
   TF* F = fflow + (size_t)cv.ch_fbase[c] * 80;   // flow factor: <= 80 entries per row
@@ -316,18 +324,32 @@ __global__ void __launch_bounds__(LS_THREADS) k_cr_factor(Canvas cv, Physics P, 
 // also written there (the normalised Arnoldi vector).  The right-hand side of every
 // level is kept in shared memory for the back substitution.
 // ------------------------------------------------------------------------------------
+// off-chain blocks of a case: enough to cover its cells on no chain, at most 64
+__host__ __device__ __forceinline__ int offchain_blocks(int n_offchain) {
+  int b = (n_offchain + LS_THREADS - 1) / LS_THREADS;
+  return b < 1 ? 1 : (b > 64 ? 64 : b);
+}
+
+// src_id: the right-hand side buffer; scale_on: multiply it by the case's 1/|w|;
+// vout_j >= 0: also write the scaled input to basis vector j; out_id: the result.
 template <class TF, class TV, bool SA>
-__global__ void __launch_bounds__(LS_THREADS) k_cr_apply(Canvas cv, const TF* __restrict__ fflow,
-                                                         const TF* __restrict__ fsa, const double* __restrict__ r,
-                                                         const double* __restrict__ scale_ptr,
-                                                         const int* __restrict__ skip, TV* __restrict__ vout,
-                                                         double* __restrict__ z) {
-  if (skip != nullptr && *skip == 0) return;
+__global__ void __launch_bounds__(LS_THREADS) k_cr_apply(const CaseDev* __restrict__ cases, int src_id, int scale_on,
+                                                         int vout_j, int out_id, int check_active) {
+  __shared__ CaseDev scase;
+  const CaseDev& cd = stage_case(cases, blockIdx.y, &scase);
+  if (!cd.enabled || (check_active && cd.sc->active == 0)) return;
+  const Canvas& cv = cd.c;
+  const TF* __restrict__ fflow = (const TF*)cd.fflow;
+  const TF* __restrict__ fsa = (const TF*)cd.fsa;
+  const double* __restrict__ r = buf(cd, src_id);
+  double* __restrict__ z = buf(cd, out_id);
+  TV* __restrict__ vout = vout_j >= 0 ? (TV*)cd.V + (size_t)vout_j * cd.n_vec : nullptr;
   const int N = cv.ncanvas(), nv = cv.nvar, n = cv.n_chains;
-  const double scale = scale_ptr != nullptr ? *scale_ptr : 1.0;
+  const double scale = scale_on ? cd.sc->inv_nrm : 1.0;
+  if ((int)blockIdx.x >= n + offchain_blocks(cv.n_offchain)) return;
   if ((int)blockIdx.x >= n) {
     // the cells on no chain: z = scale * r
-    const int stride = (gridDim.x - n) * blockDim.x;
+    const int stride = offchain_blocks(cv.n_offchain) * blockDim.x;
     for (int e = (blockIdx.x - n) * blockDim.x + threadIdx.x; e < cv.n_offchain; e += stride) {
       int idx = cv.offchain[e];
       for (int v = 0; v < nv; ++v) {
@@ -476,61 +498,46 @@ __global__ void __launch_bounds__(LS_THREADS) k_cr_apply(Canvas cv, const TF* __
   }
 }
 
-size_t cr_apply_smem(const Canvas& c, bool fp32) { return (size_t)2 * c.L * 5 * (fp32 ? 4 : 8) + 64; }
+size_t cr_apply_smem(int max_L, bool fp32) { return (size_t)2 * max_L * 5 * (fp32 ? 4 : 8) + 64; }
 
-template <class TF>
-void launch_chain_factor_t(const Canvas& c, const Physics& P, bool sa, const double* U, const double* lam,
-                           const double* mflux, const double* dflux, const double* dflow, const double* dsa,
-                           void* fflow, void* fsa, void* scratch, cudaStream_t st) {
-  if (sa)
-    k_cr_factor<TF, true><<<c.n_chains, LS_THREADS, 0, st>>>(c, P, U, lam, mflux, dflux, dflow, dsa, (TF*)fflow,
-                                                            (TF*)fsa, (TF*)scratch);
-  else
-    k_cr_factor<TF, false><<<c.n_chains, LS_THREADS, 0, st>>>(c, P, U, lam, mflux, dflux, dflow, dsa, (TF*)fflow,
-                                                             (TF*)fsa, (TF*)scratch);
-}
-
-void launch_chain_factor(const Canvas& c, const Physics& P, bool sa, bool fp32, const double* U, const double* lam,
-                         const double* mflux, const double* dflux, const double* dflow, const double* dsa,
-                         void* fflow, void* fsa, void* scratch, cudaStream_t st) {
-  if (fp32) launch_chain_factor_t<float>(c, P, sa, U, lam, mflux, dflux, dflow, dsa, fflow, fsa, scratch, st);
-  else launch_chain_factor_t<double>(c, P, sa, U, lam, mflux, dflux, dflow, dsa, fflow, fsa, scratch, st);
-}
-
-template <class TF, class TV>
-static void apply_t(const Canvas& c, bool sa, const void* fflow, const void* fsa, const double* r, const double* scale,
-                    const int* skip, TV* vout, double* z, cudaStream_t st) {
-  int extra = max(1, min(64, (c.n_offchain + LS_THREADS - 1) / LS_THREADS));
-  size_t smem = cr_apply_smem(c, sizeof(TF) == 4);
-  if (sa)
-    k_cr_apply<TF, TV, true><<<c.n_chains + extra, LS_THREADS, smem, st>>>(c, (const TF*)fflow, (const TF*)fsa, r,
-                                                                           scale, skip, vout, z);
-  else
-    k_cr_apply<TF, TV, false><<<c.n_chains + extra, LS_THREADS, smem, st>>>(c, (const TF*)fflow, (const TF*)fsa, r,
-                                                                            scale, skip, vout, z);
-}
-
-void launch_chain_apply(const Canvas& c, bool sa, bool fp32, const void* fflow, const void* fsa, const double* r,
-                        const double* scale, const int* skip, void* vout, bool vout_fp32, double* z, cudaStream_t st) {
+void launch_chain_factor(const CaseDev* cases, const BatchDims& d, bool sa, bool fp32, cudaStream_t st) {
+  dim3 grid(d.chain_blocks, d.n_cases);
   if (fp32) {
-    if (vout_fp32) apply_t<float, float>(c, sa, fflow, fsa, r, scale, skip, (float*)vout, z, st);
-    else apply_t<float, double>(c, sa, fflow, fsa, r, scale, skip, (double*)vout, z, st);
+    if (sa) k_cr_factor<float, true><<<grid, LS_THREADS, 0, st>>>(cases);
+    else k_cr_factor<float, false><<<grid, LS_THREADS, 0, st>>>(cases);
   } else {
-    if (vout_fp32) apply_t<double, float>(c, sa, fflow, fsa, r, scale, skip, (float*)vout, z, st);
-    else apply_t<double, double>(c, sa, fflow, fsa, r, scale, skip, (double*)vout, z, st);
+    if (sa) k_cr_factor<double, true><<<grid, LS_THREADS, 0, st>>>(cases);
+    else k_cr_factor<double, false><<<grid, LS_THREADS, 0, st>>>(cases);
   }
 }
 
-void configure_line_kernels(const Canvas& c) {
-  size_t s8 = cr_apply_smem(c, false), s4 = cr_apply_smem(c, true);
+template <class TF, class TV>
+static void apply_t(const CaseDev* cases, const BatchDims& d, bool sa, int src_id, int scale_on, int vout_j, int out_id,
+                    int check_active, cudaStream_t st) {
+  dim3 grid(d.chain_blocks, d.n_cases);
+  size_t smem = cr_apply_smem(d.max_L, sizeof(TF) == 4);
+  if (sa)
+    k_cr_apply<TF, TV, true><<<grid, LS_THREADS, smem, st>>>(cases, src_id, scale_on, vout_j, out_id, check_active);
+  else
+    k_cr_apply<TF, TV, false><<<grid, LS_THREADS, smem, st>>>(cases, src_id, scale_on, vout_j, out_id, check_active);
+}
+
+// z = M^-1 (scale * src) for every case; vout_j >= 0 writes the scaled input to basis
+// vector j (FP32 when the basis is)
+void launch_chain_apply(const CaseDev* cases, const BatchDims& d, bool sa, bool fp32, int src_id, int scale_on,
+                        int vout_j, int out_id, int check_active, cudaStream_t st) {
+  if (fp32) apply_t<float, float>(cases, d, sa, src_id, scale_on, vout_j, out_id, check_active, st);
+  else apply_t<double, double>(cases, d, sa, src_id, scale_on, vout_j, out_id, check_active, st);
+}
+
+int chain_grid_blocks(int n_chains, int n_offchain) { return n_chains + offchain_blocks(n_offchain); }
+
+void configure_line_kernels(int max_L) {
+  size_t s8 = cr_apply_smem(max_L, false), s4 = cr_apply_smem(max_L, true);
   cudaFuncSetAttribute(k_cr_apply<double, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s8);
   cudaFuncSetAttribute(k_cr_apply<double, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s8);
-  cudaFuncSetAttribute(k_cr_apply<double, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s8);
-  cudaFuncSetAttribute(k_cr_apply<double, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s8);
   cudaFuncSetAttribute(k_cr_apply<float, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s4);
   cudaFuncSetAttribute(k_cr_apply<float, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s4);
-  cudaFuncSetAttribute(k_cr_apply<float, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s4);
-  cudaFuncSetAttribute(k_cr_apply<float, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s4);
 }
 
 }  // namespace jr

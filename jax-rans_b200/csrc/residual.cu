@@ -156,10 +156,19 @@ __device__ __forceinline__ void eval_record(const Canvas& c, const Physics& P, i
 // corner) evaluates that stage-1 record itself rather than reading it, so no record
 // waits on another and every CTA works independently.
 template <class T>
-__global__ void __launch_bounds__(GHOST_THREADS) k_ghosts(Canvas c, Physics P, const double* U, const double* V,
-                                                          double* qg, double* dqg, const int* active) {
-  if (active != nullptr && *active == 0) return;
+__global__ void __launch_bounds__(GHOST_THREADS) k_ghosts(const CaseDev* __restrict__ cases, int tangent_id,
+                                                          int check_active) {
+  __shared__ CaseDev scase;
+  const CaseDev& cd = stage_case(cases, blockIdx.y, &scase);
+  if (!cd.enabled || (check_active && cd.sc->active == 0)) return;
+  const Canvas& c = cd.c;
+  const Physics& P = cd.P;
+  const double* U = cd.U;
+  const double* V = tangent_id >= 0 ? buf(cd, tangent_id) : nullptr;
+  double* qg = cd.qg;
+  double* dqg = cd.dqg;
   const int N = c.ncanvas();
+  if ((int)blockIdx.x * (int)blockDim.x >= c.n_ghost[0] + c.n_ghost[1]) return;
   __shared__ double red_v[GHOST_THREADS / 32][2], red_d[GHOST_THREADS / 32][2];
   __shared__ T circ_s;
   T circ = cst<T>(0.0);
@@ -418,12 +427,22 @@ template <> __device__ __forceinline__ double tangent_or_value<Dual>(const Dual&
 // T = double: out = R(U) (second or first order); partial[block] = sum vol R0^2.
 // T = Dual:   out = vdt * V + dR1/dU . V.
 template <class T, int NV, bool SECOND, int VISC>
-__global__ void __launch_bounds__(TILE_THREADS, TILE_MIN_BLOCKS) k_residual(Canvas c, Physics P, const double* __restrict__ U,
-                                                          const double* __restrict__ qg, const double* __restrict__ V,
-                                                          const double* __restrict__ dqg,
-                                                          const double* __restrict__ vdt, double* __restrict__ out,
-                                                          double* __restrict__ partial, const int* active) {
-  if (active != nullptr && *active == 0) return;
+__global__ void __launch_bounds__(TILE_THREADS, TILE_MIN_BLOCKS)
+    k_residual(const CaseDev* __restrict__ cases, int out_id, int tangent_id, int vdt_id, int with_partial,
+               int check_active) {
+  __shared__ CaseDev scase;
+  const CaseDev& cd = stage_case(cases, blockIdx.z, &scase);
+  if (!cd.enabled || (check_active && cd.sc->active == 0)) return;
+  if ((int)blockIdx.x >= cd.tiles_x || (int)blockIdx.y >= cd.tiles_y) return;
+  const Canvas& c = cd.c;
+  const Physics& P = cd.P;
+  const double* __restrict__ U = cd.U;
+  const double* __restrict__ qg = cd.qg;
+  const double* __restrict__ V = tangent_id >= 0 ? buf(cd, tangent_id) : nullptr;
+  const double* __restrict__ dqg = cd.dqg;
+  const double* __restrict__ vdt = vdt_id >= 0 ? buf(cd, vdt_id) : nullptr;
+  double* __restrict__ out = buf(cd, out_id);
+  double* __restrict__ partial = with_partial ? cd.tile_partial : nullptr;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TileSmem<T, NV>& s = *reinterpret_cast<TileSmem<T, NV>*>(smem_raw);
   const int NI = c.NI, NJ = c.NJ, N = c.ncanvas();
@@ -515,7 +534,7 @@ __global__ void __launch_bounds__(TILE_THREADS, TILE_MIN_BLOCKS) k_residual(Canv
           R[4] = R[4] - tangent_or_value(src) * vol;
         }
         if constexpr (sizeof(T) == sizeof(Dual)) {
-          double w = vdt[idx];
+          double w = vdt != nullptr ? vdt[idx] : 0.0;
           for (int v = 0; v < NV; ++v) out[v * N + idx] = w * V[v * N + idx] + R[v];
         } else {
           for (int v = 0; v < NV; ++v) out[v * N + idx] = R[v];
@@ -523,7 +542,7 @@ __global__ void __launch_bounds__(TILE_THREADS, TILE_MIN_BLOCKS) k_residual(Canv
         }
       } else {
         if constexpr (sizeof(T) == sizeof(Dual)) {
-          double w = vdt[idx];
+          double w = vdt != nullptr ? vdt[idx] : 0.0;
           for (int v = 0; v < NV; ++v) out[v * N + idx] = w * V[v * N + idx] + V[v * N + idx];
         } else {
           for (int v = 0; v < NV; ++v) out[v * N + idx] = U[v * N + idx] - P.U_inf[v];
@@ -539,7 +558,7 @@ __global__ void __launch_bounds__(TILE_THREADS, TILE_MIN_BLOCKS) k_residual(Canv
       if (tid == 0) {
         double t = 0.0;
         for (int k = 0; k < TILE_THREADS / 32; ++k) t += s.red[k];
-        partial[blockIdx.y * gridDim.x + blockIdx.x] = t;
+        partial[blockIdx.y * cd.tiles_x + blockIdx.x] = t;
       }
     }
   }
@@ -559,8 +578,16 @@ __device__ __forceinline__ void prim_raw(const Canvas& c, const Physics& P, cons
 }
 
 template <int VISC>
-__global__ void k_faces(Canvas c, Physics P, const double* __restrict__ U, double* __restrict__ lam,
-                        double* __restrict__ mflux, double* __restrict__ dflux) {
+__global__ void k_faces(const CaseDev* __restrict__ cases) {
+  __shared__ CaseDev scase;
+  const CaseDev& cd = stage_case(cases, blockIdx.y, &scase);
+  if (!cd.enabled) return;
+  const Canvas& c = cd.c;
+  const Physics& P = cd.P;
+  const double* __restrict__ U = cd.U;
+  double* __restrict__ lam = cd.lam;
+  double* __restrict__ mflux = cd.mflux;
+  double* __restrict__ dflux = cd.dflux;
   const int nfi = c.nfi(), nf = nfi + c.nfj();
   const int NI = c.NI, NJ = c.NJ;
   const double g = P.gamma;
@@ -610,10 +637,20 @@ __global__ void k_faces(Canvas c, Physics P, const double* __restrict__ U, doubl
 // Per cell: V/dt = sum lambda / CFL; the flow chains' diagonal scalar sum lambda (1/CFL + 1/2);
 // the SA chains' diagonal (preconditioners.py:564-578).
 template <int VISC>
-__global__ void k_cells(Canvas c, Physics P, const double* __restrict__ U, const double* __restrict__ lam,
-                        const double* __restrict__ mflux, const double* __restrict__ dflux,
-                        const Scalars* __restrict__ sc, double* __restrict__ vdt, double* __restrict__ dflow,
-                        double* __restrict__ dsa) {
+__global__ void k_cells(const CaseDev* __restrict__ cases) {
+  __shared__ CaseDev scase;
+  const CaseDev& cd = stage_case(cases, blockIdx.y, &scase);
+  if (!cd.enabled) return;
+  const Canvas& c = cd.c;
+  const Physics& P = cd.P;
+  const double* __restrict__ U = cd.U;
+  const double* __restrict__ lam = cd.lam;
+  const double* __restrict__ mflux = cd.mflux;
+  const double* __restrict__ dflux = cd.dflux;
+  const Scalars* __restrict__ sc = cd.sc;
+  double* __restrict__ vdt = cd.vdt;
+  double* __restrict__ dflow = cd.dflow;
+  double* __restrict__ dsa = cd.dsa;
   const int NI = c.NI, NJ = c.NJ, N = c.ncanvas(), nfi = c.nfi();
   const double cfl = sc->cfl, g = P.gamma;
   // every canvas cell: V/dt enters the Krylov operator on ghost cells too (there the
@@ -696,61 +733,57 @@ void configure_kernels() {
   done = true;
 }
 
+// One launch over every case of a batch: grid z = the case, x/y = the tiles (a case
+// with fewer tiles returns at once from the excess ones).
 template <class T, int NV, bool SECOND, int VISC>
-static void launch_tile(const Canvas& c, const Physics& P, const double* U, const double* qg, const double* V,
-                        const double* dqg, const double* vdt, double* out, double* partial, const int* active,
-                        cudaStream_t st) {
-  k_residual<T, NV, SECOND, VISC><<<tile_grid(c), TILE_THREADS, sizeof(TileSmem<T, NV>), st>>>(
-      c, P, U, qg, V, dqg, vdt, out, partial, active);
+static void launch_tile(const CaseDev* cases, const BatchDims& d, int out_id, int tangent_id, int vdt_id,
+                        int with_partial, int check_active, cudaStream_t st) {
+  dim3 grid(d.tiles_x, d.tiles_y, d.n_cases);
+  k_residual<T, NV, SECOND, VISC><<<grid, TILE_THREADS, sizeof(TileSmem<T, NV>), st>>>(
+      cases, out_id, tangent_id, vdt_id, with_partial, check_active);
 }
 
-// R(U): second (or first) order, double
-void launch_residual(const Canvas& c, const Physics& P, int visc, bool second, const double* U, const double* qg,
-                     double* R, double* partial, cudaStream_t st) {
+// R(U) of every case into `out_id` (second or first order), with the norm partials
+void launch_residual(const CaseDev* cases, const BatchDims& d, int visc, bool second, int out_id, cudaStream_t st) {
   if (visc == 2) {
-    if (second) launch_tile<double, 5, true, 2>(c, P, U, qg, nullptr, nullptr, nullptr, R, partial, nullptr, st);
-    else launch_tile<double, 5, false, 2>(c, P, U, qg, nullptr, nullptr, nullptr, R, partial, nullptr, st);
+    if (second) launch_tile<double, 5, true, 2>(cases, d, out_id, -1, -1, 1, 0, st);
+    else launch_tile<double, 5, false, 2>(cases, d, out_id, -1, -1, 1, 0, st);
   } else if (visc == 1) {
-    if (second) launch_tile<double, 4, true, 1>(c, P, U, qg, nullptr, nullptr, nullptr, R, partial, nullptr, st);
-    else launch_tile<double, 4, false, 1>(c, P, U, qg, nullptr, nullptr, nullptr, R, partial, nullptr, st);
+    if (second) launch_tile<double, 4, true, 1>(cases, d, out_id, -1, -1, 1, 0, st);
+    else launch_tile<double, 4, false, 1>(cases, d, out_id, -1, -1, 1, 0, st);
   } else {
-    if (second) launch_tile<double, 4, true, 0>(c, P, U, qg, nullptr, nullptr, nullptr, R, partial, nullptr, st);
-    else launch_tile<double, 4, false, 0>(c, P, U, qg, nullptr, nullptr, nullptr, R, partial, nullptr, st);
+    if (second) launch_tile<double, 4, true, 0>(cases, d, out_id, -1, -1, 1, 0, st);
+    else launch_tile<double, 4, false, 0>(cases, d, out_id, -1, -1, 1, 0, st);
   }
 }
 
-// w = vdt * V + dR1/dU . V (the first-order residual's exact tangent)
-void launch_jvp(const Canvas& c, const Physics& P, int visc, const double* U, const double* qg, const double* V,
-                const double* dqg, const double* vdt, double* w, const int* active, cudaStream_t st) {
-  if (visc == 2) launch_tile<Dual, 5, false, 2>(c, P, U, qg, V, dqg, vdt, w, nullptr, active, st);
-  else if (visc == 1) launch_tile<Dual, 4, false, 1>(c, P, U, qg, V, dqg, vdt, w, nullptr, active, st);
-  else launch_tile<Dual, 4, false, 0>(c, P, U, qg, V, dqg, vdt, w, nullptr, active, st);
+// out = vdt * v + dR1/dU . v with v = buffer `tangent_id` (vdt_id < 0: the bare J.v)
+void launch_jvp(const CaseDev* cases, const BatchDims& d, int visc, int tangent_id, int vdt_id, int out_id,
+                int check_active, cudaStream_t st) {
+  if (visc == 2) launch_tile<Dual, 5, false, 2>(cases, d, out_id, tangent_id, vdt_id, 0, check_active, st);
+  else if (visc == 1) launch_tile<Dual, 4, false, 1>(cases, d, out_id, tangent_id, vdt_id, 0, check_active, st);
+  else launch_tile<Dual, 4, false, 0>(cases, d, out_id, tangent_id, vdt_id, 0, check_active, st);
 }
 
-void launch_ghosts(const Canvas& c, const Physics& P, bool dual, const double* U, const double* V, double* qg,
-                   double* dqg, const int* active, cudaStream_t st) {
-  int blocks = max(1, (c.n_ghost[0] + c.n_ghost[1] + GHOST_THREADS - 1) / GHOST_THREADS);
-  if (dual) k_ghosts<Dual><<<blocks, GHOST_THREADS, 0, st>>>(c, P, U, V, qg, dqg, active);
-  else k_ghosts<double><<<blocks, GHOST_THREADS, 0, st>>>(c, P, U, V, qg, dqg, active);
+// the ghosts of U (tangent_id < 0) or of the tangent in buffer `tangent_id`
+void launch_ghosts(const CaseDev* cases, const BatchDims& d, int tangent_id, int check_active, cudaStream_t st) {
+  dim3 grid(max(1, (d.ghost_records + GHOST_THREADS - 1) / GHOST_THREADS), d.n_cases);
+  if (tangent_id >= 0) k_ghosts<Dual><<<grid, GHOST_THREADS, 0, st>>>(cases, tangent_id, check_active);
+  else k_ghosts<double><<<grid, GHOST_THREADS, 0, st>>>(cases, -1, check_active);
 }
 
-void launch_faces(const Canvas& c, const Physics& P, int visc, const double* U, double* lam, double* mflux,
-                  double* dflux, cudaStream_t st) {
-  int n = c.NI * (c.NJ + 1) + (c.NI + 1) * c.NJ;
-  int blocks = min((n + 255) / 256, 148 * 8);
-  if (visc == 2) k_faces<2><<<blocks, 256, 0, st>>>(c, P, U, lam, mflux, dflux);
-  else if (visc == 1) k_faces<1><<<blocks, 256, 0, st>>>(c, P, U, lam, mflux, dflux);
-  else k_faces<0><<<blocks, 256, 0, st>>>(c, P, U, lam, mflux, dflux);
+void launch_faces(const CaseDev* cases, const BatchDims& d, int visc, cudaStream_t st) {
+  dim3 grid(max(1, min((d.faces + 255) / 256, 148 * 8)), d.n_cases);
+  if (visc == 2) k_faces<2><<<grid, 256, 0, st>>>(cases);
+  else if (visc == 1) k_faces<1><<<grid, 256, 0, st>>>(cases);
+  else k_faces<0><<<grid, 256, 0, st>>>(cases);
 }
 
-void launch_cells(const Canvas& c, const Physics& P, int visc, const double* U, const double* lam,
-                  const double* mflux, const double* dflux, const Scalars* sc, double* vdt, double* dflow,
-                  double* dsa, cudaStream_t st) {
-  int n = c.NI * c.NJ;
-  int blocks = min((n + 255) / 256, 148 * 8);
-  if (visc == 2) k_cells<2><<<blocks, 256, 0, st>>>(c, P, U, lam, mflux, dflux, sc, vdt, dflow, dsa);
-  else if (visc == 1) k_cells<1><<<blocks, 256, 0, st>>>(c, P, U, lam, mflux, dflux, sc, vdt, dflow, dsa);
-  else k_cells<0><<<blocks, 256, 0, st>>>(c, P, U, lam, mflux, dflux, sc, vdt, dflow, dsa);
+void launch_cells(const CaseDev* cases, const BatchDims& d, int visc, cudaStream_t st) {
+  dim3 grid(max(1, min((d.cells + 255) / 256, 148 * 8)), d.n_cases);
+  if (visc == 2) k_cells<2><<<grid, 256, 0, st>>>(cases);
+  else if (visc == 1) k_cells<1><<<grid, 256, 0, st>>>(cases);
+  else k_cells<0><<<grid, 256, 0, st>>>(cases);
 }
 
 }  // namespace jr

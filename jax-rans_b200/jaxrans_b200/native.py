@@ -59,7 +59,9 @@ class PlanDesc(C.Structure):
 EXPORTS = ("jr_plan_create", "jr_plan_destroy", "jr_last_error", "jr_plan_sizes", "jr_plan_stream",
            "jr_synchronize", "jr_residual", "jr_jvp", "jr_wave_speeds", "jr_precond_factor", "jr_precond_apply",
            "jr_state_set", "jr_state_get", "jr_state_device", "jr_newton_steps", "jr_newton_steps_async",
-           "jr_forces", "jr_state_set_device", "jr_graph_kernels", "jr_time_kernels", "jr_plan_set_stream")
+           "jr_forces", "jr_state_set_device", "jr_graph_kernels", "jr_time_kernels", "jr_plan_set_stream",
+           "jr_batch_create", "jr_plan_cases", "jr_case_sizes", "jr_case_enable", "jr_case_set_inflow",
+           "jr_case_state_set", "jr_case_state_get")
 
 TIMED_KERNELS = ("residual_tile", "jvp_tile", "ghosts_tangent", "line_apply", "line_factor", "cgs2_full_basis")
 
@@ -103,6 +105,13 @@ def load_library(path: Path | None = None) -> C.CDLL:
         "jr_graph_kernels": (C.c_int, [vp, C.POINTER(C.c_int64)]),
         "jr_time_kernels": (C.c_int, [vp, C.c_int32, _f64p]),
         "jr_plan_set_stream": (C.c_int, [vp, vp]),
+        "jr_batch_create": (C.c_int, [C.POINTER(PlanDesc), C.c_int32, C.POINTER(vp)]),
+        "jr_plan_cases": (C.c_int, [vp]),
+        "jr_case_sizes": (C.c_int, [vp, C.c_int32] + [C.POINTER(C.c_int64)] * 4),
+        "jr_case_enable": (C.c_int, [vp, C.c_int32, C.c_int32]),
+        "jr_case_set_inflow": (C.c_int, [vp, C.c_int32, _f64p]),
+        "jr_case_state_set": (C.c_int, [vp, C.c_int32, vp, C.c_double, C.c_double]),
+        "jr_case_state_get": (C.c_int, [vp, C.c_int32, vp, _f64p, _f64p, _i32p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -122,84 +131,124 @@ def _ptr(a: np.ndarray, kind):
     return a.ctypes.data_as(kind)
 
 
+def fill_desc(d: PlanDesc, plan: Plan, flow: FlowConditions, numerics: NumericsConfig, implicit: ImplicitConfig,
+              force_length: float, moment_centre, keep: list) -> None:
+    """``d`` for one case; the arrays it points into are appended to ``keep``."""
+    nvar = flow.nvar
+    if nvar == 5 and plan.distance is None:
+        raise ValueError("the SA model needs the plan's wall distance (build_plan(..., with_distance=True))")
+
+    def arr(a, dtype):
+        a = np.ascontiguousarray(a, dtype=dtype)
+        keep.append(a)
+        return a
+
+    d.NI, d.NJ, d.nvar = plan.NI, plan.NJ, nvar
+    d.interior = _ptr(arr(plan.interior, np.uint8), _u8p)
+    d.volume = _ptr(arr(plan.volume, np.float64), _f64p)
+    d.faces_i = _ptr(arr(plan.faces_i, np.float64), _f64p)
+    d.faces_j = _ptr(arr(plan.faces_j, np.float64), _f64p)
+    d.centres = _ptr(arr(plan.centres, np.float64), _f64p)
+    d.distance = _ptr(arr(plan.distance, np.float64), _f64p) if (nvar == 5) else _f64p()
+    d.neighbours = _ptr(arr(plan.neighbours, np.int32), _i32p)
+    for s, st in enumerate(plan.stages):
+        d.n_ghost[s] = len(st.ghost)
+        d.ghost[s] = _ptr(arr(st.ghost, np.int32), _i32p)
+        d.source[s] = _ptr(arr(st.source, np.int32), _i32p)
+        d.kind[s] = _ptr(arr(st.kind, np.int32), _i32p)
+        d.geom[s] = _ptr(arr(np.stack([st.normal[0], st.normal[1], st.midpoint[0], st.midpoint[1]], axis=1),
+                             np.float64), _f64p)
+    W = plan.walls
+    d.n_walls = len(W.cell)
+    d.wall_cell = _ptr(arr(W.cell, np.int32), _i32p)
+    d.wall_family = _ptr(arr(W.family, np.int32), _i32p)
+    d.wall_face = _ptr(arr(W.face, np.int32), _i32p)
+    d.wall_into = _ptr(arr(W.into_fluid, np.float64), _f64p)
+    d.wall_mid = _ptr(arr(W.mid if len(W.cell) else np.zeros((0, 2)), np.float64), _f64p)
+    ch = plan.chains
+    d.n_chains, d.chain_L = ch.cells.shape
+    d.chain_cells = _ptr(arr(ch.cells.T, np.int32), _i32p)
+    d.chain_len = _ptr(arr(ch.lengths, np.int32), _i32p)
+    d.chain_up_face = _ptr(arr(ch.up_face.T, np.int32), _i32p)
+    d.chain_up_sign = _ptr(arr(ch.up_sign.T, np.int32), _i32p)
+    d.chain_down_face = _ptr(arr(ch.down_face.T, np.int32), _i32p)
+    d.chain_down_sign = _ptr(arr(ch.down_sign.T, np.int32), _i32p)
+    d.gamma = flow.gamma
+    d.mu_inf = 0.0 if flow.inviscid else flow.mu_inf
+    d.sutherland = -1.0 if flow.sutherland_ratio is None else flow.sutherland_ratio
+    d.c_cr1 = 0.3 if flow.turbulence == "sa_noft2_qcr" else 0.0
+    d.kappa = numerics.kappa
+    d.flux = FLUX_CODES[numerics.flux]
+    d.limiter = 4 if numerics.kappa != 0.0 else LIMITER_CODES[numerics.limiter]
+    d.far_field = FAR_FIELD_CODES[numerics.far_field]
+    for k, v in enumerate(freestream_primitive(flow)):
+        d.q_inf[k] = v
+    d.quarter_chord[0], d.quarter_chord[1] = plan.quarter_chord
+    imp = implicit
+    d.cfl, d.cfl_max, d.cfl_growth = imp.cfl, imp.cfl_max, imp.cfl_growth
+    d.cfl_cutback, d.cfl_min = imp.cfl_cutback, imp.cfl_min
+    d.krylov_tol, d.krylov_success = imp.krylov_tol, imp.krylov_success
+    d.max_relative_update = -1.0 if imp.max_relative_update is None else imp.max_relative_update
+    d.krylov_subspace, d.krylov_restarts = imp.krylov_subspace, imp.krylov_restarts
+    d.preconditioner = 1 if imp.preconditioner == "line_j" else 0
+    d.precision = 1 if imp.precision == "mixed" else 0
+    d.force_length = force_length
+    d.moment_centre[0], d.moment_centre[1] = moment_centre[0], moment_centre[1]
+
+
 class DevicePlan:
-    """One case on the device: ``jr_plan`` with its tables, buffers and state."""
+    """Cases on the device: ``jr_plan`` with their tables, buffers and state.
+
+    ``DevicePlan(plan, flow, ...)`` is one case; ``DevicePlan.batch(plans, flows, ...)``
+    advances several at once (a polar: one grid, one flow per angle).  For a single case
+    fields have the case's shape ``(nvar, NI, NJ)``; for a batch, arrays that span the
+    batch are flat, the cases back to back (``offsets``), and the ``case_*`` methods
+    read or write one case."""
 
     def __init__(self, plan: Plan, flow: FlowConditions, numerics: NumericsConfig,
                  implicit: ImplicitConfig | None = None, force_length: float = 1.0,
                  moment_centre=(0.25, 0.0), library: Path | None = None):
+        self._create([plan], [flow], numerics, implicit, force_length, moment_centre, library)
+
+    @classmethod
+    def batch(cls, plans, flows, numerics: NumericsConfig, implicit: ImplicitConfig | None = None,
+              force_length: float = 1.0, moment_centre=(0.25, 0.0), library: Path | None = None) -> "DevicePlan":
+        if isinstance(plans, Plan):
+            plans = [plans] * len(flows)
+        if len(plans) != len(flows) or not flows:
+            raise ValueError("a batch needs one plan per flow, and at least one case")
+        self = cls.__new__(cls)
+        self._create(list(plans), list(flows), numerics, implicit, force_length, moment_centre, library)
+        return self
+
+    def _create(self, plans, flows, numerics, implicit, force_length, moment_centre, library):
         self.lib = load_library(library)
-        self.plan, self.flow, self.numerics = plan, flow, numerics
+        self.plans, self.flows, self.numerics = plans, flows, numerics
+        self.plan, self.flow = plans[0], flows[0]
         self.implicit = implicit or ImplicitConfig()
-        nvar = flow.nvar
-        if nvar == 5 and plan.distance is None:
-            raise ValueError("the SA model needs the plan's wall distance (build_plan(..., with_distance=True))")
-        keep = []
-
-        def arr(a, dtype):
-            a = np.ascontiguousarray(a, dtype=dtype)
-            keep.append(a)
-            return a
-
-        d = PlanDesc()
-        d.NI, d.NJ, d.nvar = plan.NI, plan.NJ, nvar
-        d.interior = _ptr(arr(plan.interior, np.uint8), _u8p)
-        d.volume = _ptr(arr(plan.volume, np.float64), _f64p)
-        d.faces_i = _ptr(arr(plan.faces_i, np.float64), _f64p)
-        d.faces_j = _ptr(arr(plan.faces_j, np.float64), _f64p)
-        d.centres = _ptr(arr(plan.centres, np.float64), _f64p)
-        d.distance = _ptr(arr(plan.distance, np.float64), _f64p) if (nvar == 5) else _f64p()
-        d.neighbours = _ptr(arr(plan.neighbours, np.int32), _i32p)
-        for s, st in enumerate(plan.stages):
-            d.n_ghost[s] = len(st.ghost)
-            d.ghost[s] = _ptr(arr(st.ghost, np.int32), _i32p)
-            d.source[s] = _ptr(arr(st.source, np.int32), _i32p)
-            d.kind[s] = _ptr(arr(st.kind, np.int32), _i32p)
-            d.geom[s] = _ptr(arr(np.stack([st.normal[0], st.normal[1], st.midpoint[0], st.midpoint[1]], axis=1),
-                                 np.float64), _f64p)
-        W = plan.walls
-        d.n_walls = len(W.cell)
-        d.wall_cell = _ptr(arr(W.cell, np.int32), _i32p)
-        d.wall_family = _ptr(arr(W.family, np.int32), _i32p)
-        d.wall_face = _ptr(arr(W.face, np.int32), _i32p)
-        d.wall_into = _ptr(arr(W.into_fluid, np.float64), _f64p)
-        d.wall_mid = _ptr(arr(W.mid if len(W.cell) else np.zeros((0, 2)), np.float64), _f64p)
-        ch = plan.chains
-        d.n_chains, d.chain_L = ch.cells.shape
-        d.chain_cells = _ptr(arr(ch.cells.T, np.int32), _i32p)
-        d.chain_len = _ptr(arr(ch.lengths, np.int32), _i32p)
-        d.chain_up_face = _ptr(arr(ch.up_face.T, np.int32), _i32p)
-        d.chain_up_sign = _ptr(arr(ch.up_sign.T, np.int32), _i32p)
-        d.chain_down_face = _ptr(arr(ch.down_face.T, np.int32), _i32p)
-        d.chain_down_sign = _ptr(arr(ch.down_sign.T, np.int32), _i32p)
-        d.gamma = flow.gamma
-        d.mu_inf = 0.0 if flow.inviscid else flow.mu_inf
-        d.sutherland = -1.0 if flow.sutherland_ratio is None else flow.sutherland_ratio
-        d.c_cr1 = 0.3 if flow.turbulence == "sa_noft2_qcr" else 0.0
-        d.kappa = numerics.kappa
-        d.flux = FLUX_CODES[numerics.flux]
-        d.limiter = 4 if numerics.kappa != 0.0 else LIMITER_CODES[numerics.limiter]
-        d.far_field = FAR_FIELD_CODES[numerics.far_field]
-        q = freestream_primitive(flow)
-        for k, v in enumerate(q):
-            d.q_inf[k] = v
-        d.quarter_chord[0], d.quarter_chord[1] = plan.quarter_chord
-        imp = self.implicit
-        d.cfl, d.cfl_max, d.cfl_growth = imp.cfl, imp.cfl_max, imp.cfl_growth
-        d.cfl_cutback, d.cfl_min = imp.cfl_cutback, imp.cfl_min
-        d.krylov_tol, d.krylov_success = imp.krylov_tol, imp.krylov_success
-        d.max_relative_update = -1.0 if imp.max_relative_update is None else imp.max_relative_update
-        d.krylov_subspace, d.krylov_restarts = imp.krylov_subspace, imp.krylov_restarts
-        d.preconditioner = 1 if imp.preconditioner == "line_j" else 0
-        d.precision = 1 if imp.precision == "mixed" else 0
-        d.force_length = force_length
-        d.moment_centre[0], d.moment_centre[1] = moment_centre[0], moment_centre[1]
+        keep: list = []
+        descs = (PlanDesc * len(plans))()
+        for k, (plan, flow) in enumerate(zip(plans, flows)):
+            fill_desc(descs[k], plan, flow, numerics, self.implicit, force_length, moment_centre, keep)
         handle = C.c_void_p()
-        _check(self.lib, self.lib.jr_plan_create(C.byref(d), C.byref(handle)), "jr_plan_create")
+        if len(plans) == 1:
+            _check(self.lib, self.lib.jr_plan_create(descs, C.byref(handle)), "jr_plan_create")
+        else:
+            _check(self.lib, self.lib.jr_batch_create(descs, len(plans), C.byref(handle)), "jr_batch_create")
         self.handle = handle
-        self.nvar = nvar
-        self.shape = (nvar, plan.NI, plan.NJ)
-        self.n_faces = (plan.NI + 1) * plan.NJ + plan.NI * (plan.NJ + 1)
+        self.n_cases = len(plans)
+        self.nvar = flows[0].nvar
+        self.shapes = [(self.nvar, p.NI, p.NJ) for p in plans]
+        self.shape = self.shapes[0]
+        sizes = [self.nvar * p.NI * p.NJ for p in plans]
+        self.offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+        self.n_vec = int(self.offsets[-1])
+        faces = [(p.NI + 1) * p.NJ + p.NI * (p.NJ + 1) for p in plans]
+        self.face_offsets = np.concatenate([[0], np.cumsum(faces)]).astype(np.int64)
+        self.n_faces = int(self.face_offsets[-1])
+
+    def _field_shape(self):
+        return self.shape if self.n_cases == 1 else (self.n_vec,)
 
     # -- lifetime ---------------------------------------------------------------------
     def close(self) -> None:
@@ -243,7 +292,7 @@ class DevicePlan:
     # -- entry points --------------------------------------------------------------------
     def residual(self, U, first_order: bool = False):
         u = self._device(U)
-        out = self._empty(self.shape)
+        out = self._empty(self._field_shape())
         _check(self.lib, self.lib.jr_residual(self.handle, u.data_ptr(), out.data_ptr(), int(first_order)),
                "jr_residual")
         self.sync()
@@ -251,7 +300,7 @@ class DevicePlan:
 
     def jvp(self, U, v):
         u, t = self._device(U), self._device(v)
-        out = self._empty(self.shape)
+        out = self._empty(self._field_shape())
         _check(self.lib, self.lib.jr_jvp(self.handle, u.data_ptr(), t.data_ptr(), out.data_ptr()), "jr_jvp")
         self.sync()
         return self._like_input(U, out)
@@ -262,37 +311,75 @@ class DevicePlan:
         _check(self.lib, self.lib.jr_wave_speeds(self.handle, u.data_ptr(), out.data_ptr()), "jr_wave_speeds")
         self.sync()
         lam = self._like_input(U, out)
+        if self.n_cases > 1:
+            return lam
         nfi = (self.plan.NI + 1) * self.plan.NJ
         return (lam[:nfi].reshape(self.plan.NI + 1, self.plan.NJ),
                 lam[nfi:].reshape(self.plan.NI, self.plan.NJ + 1))
 
     def precondition(self, U, cfl: float, r):
         u, rr = self._device(U), self._device(r)
-        out = self._empty(self.shape)
+        out = self._empty(self._field_shape())
         _check(self.lib, self.lib.jr_precond_factor(self.handle, u.data_ptr(), float(cfl)), "jr_precond_factor")
         _check(self.lib, self.lib.jr_precond_apply(self.handle, rr.data_ptr(), out.data_ptr()), "jr_precond_apply")
         self.sync()
         return self._like_input(r, out)
 
     def set_state(self, U=None, cfl: float | None = None, residual_norm: float = float("inf")) -> None:
+        """Every case's state (``U``: the case's shape, or the batch back to back) with one
+        CFL and previous |R|."""
         cfl = self.implicit.cfl if cfl is None else cfl
         ptr = None
         if U is not None:
             U = np.ascontiguousarray(U, dtype=np.float64)
-            if U.shape != self.shape:
-                raise ValueError(f"state must be {self.shape}, got {U.shape}")
+            if U.size != self.n_vec or (self.n_cases == 1 and U.shape != self.shape):
+                raise ValueError(f"state must be {self._field_shape()}, got {U.shape}")
             ptr = U.ctypes.data
         _check(self.lib, self.lib.jr_state_set(self.handle, ptr, float(cfl), float(residual_norm)), "jr_state_set")
 
     def get_state(self):
-        U = np.empty(self.shape)
+        """``(U, cfl, |R| before the last accepted step, status)``; for a batch U is flat
+        and the scalars are arrays over the cases."""
+        U = np.empty(self._field_shape())
+        cfl, res = np.empty(self.n_cases), np.empty(self.n_cases)
+        status = np.empty(self.n_cases, dtype=np.int32)
+        _check(self.lib, self.lib.jr_state_get(self.handle, U.ctypes.data, _ptr(cfl, _f64p), _ptr(res, _f64p),
+                                                _ptr(status, _i32p)), "jr_state_get")
+        if self.n_cases == 1:
+            return U, float(cfl[0]), float(res[0]), int(status[0])
+        return U, cfl, res, status
+
+    def case_state(self, k: int):
+        """Case k: ``(U (nvar, NI, NJ), cfl, |R|, status)``."""
+        U = np.empty(self.shapes[k])
         cfl, res, status = C.c_double(), C.c_double(), C.c_int32()
-        _check(self.lib, self.lib.jr_state_get(self.handle, U.ctypes.data, C.byref(cfl), C.byref(res),
-                                                C.byref(status)), "jr_state_get")
+        _check(self.lib, self.lib.jr_case_state_get(self.handle, int(k), U.ctypes.data, C.byref(cfl), C.byref(res),
+                                                     C.byref(status)), "jr_case_state_get")
         return U, cfl.value, res.value, status.value
 
+    def set_case_state(self, k: int, U=None, cfl: float | None = None, residual_norm: float = float("inf")) -> None:
+        cfl = self.implicit.cfl if cfl is None else cfl
+        ptr = None
+        if U is not None:
+            U = np.ascontiguousarray(U, dtype=np.float64)
+            if U.shape != self.shapes[k]:
+                raise ValueError(f"case {k} state must be {self.shapes[k]}, got {U.shape}")
+            ptr = U.ctypes.data
+        _check(self.lib, self.lib.jr_case_state_set(self.handle, int(k), ptr, float(cfl), float(residual_norm)),
+               "jr_case_state_set")
+
+    def enable(self, k: int, enabled: bool = True) -> None:
+        _check(self.lib, self.lib.jr_case_enable(self.handle, int(k), int(bool(enabled))), "jr_case_enable")
+
+    def set_inflow(self, k: int, q_inf) -> None:
+        """Case k's freestream primitives (rho, u, v, p[, nu_hat])."""
+        q = np.zeros(5)
+        q[: self.nvar] = np.asarray(q_inf, dtype=np.float64)[: self.nvar]
+        _check(self.lib, self.lib.jr_case_set_inflow(self.handle, int(k), _ptr(q, _f64p)), "jr_case_set_inflow")
+
     def newton_steps(self, n: int) -> np.ndarray:
-        hist = np.empty(n)
+        """|R| before each step: ``(n,)``, or ``(n, n_cases)`` for a batch."""
+        hist = np.empty(n if self.n_cases == 1 else (n, self.n_cases))
         _check(self.lib, self.lib.jr_newton_steps(self.handle, int(n), hist.ctypes.data), "jr_newton_steps")
         return hist
 
@@ -325,7 +412,8 @@ class DevicePlan:
         return int(self.lib.jr_state_device(self.handle))
 
     def forces(self, U=None) -> np.ndarray:
-        out = np.empty(6)
+        """cl, cd, cm, cd_friction, fx, fy: ``(6,)``, or ``(n_cases, 6)`` for a batch."""
+        out = np.empty(6 if self.n_cases == 1 else (self.n_cases, 6))
         ptr = None
         keep = None
         if U is not None:

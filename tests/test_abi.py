@@ -41,3 +41,21 @@ def test_errors_without_a_device_are_reported_not_crashed():
     lib = load_library()
     assert lib.jr_plan_create(None, None) == 1          # JR_EINVAL on a null descriptor
     assert b"null" in lib.jr_last_error()
+
+
+def test_batch_rejects_cases_of_different_models_on_the_host():
+    """The batch check runs before any device call: an inviscid and a viscous case
+    cannot share a plan (their launches differ)."""
+    import ctypes as C
+    from goldens import load
+    from jaxrans_b200.native import PlanDesc, fill_desc, load_library
+    lib = load_library()
+    keep = []
+    descs = (PlanDesc * 2)()
+    for k, name in enumerate(["o_euler", "c_laminar"]):
+        z, case, plan = load(name)
+        fill_desc(descs[k], plan, case.flow, case.numerics, case.implicit, 1.0, (0.25, 0.0), keep)
+    handle = C.c_void_p()
+    assert lib.jr_batch_create(descs, 2, C.byref(handle)) == 1
+    assert b"must share" in lib.jr_last_error()
+    assert lib.jr_batch_create(descs, 0, C.byref(handle)) == 1

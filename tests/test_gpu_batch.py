@@ -1,0 +1,115 @@
+"""Batches through the C ABI: several cases advanced by the same launches.
+
+The reference batches a polar by ``jax.vmap`` of one Newton step over the freestreams
+(src/jaxrans/polar.py:80-121); its cases never interact.  Here a batch is one plan
+whose every kernel takes all cases, with each case's reductions split exactly as when
+it runs alone, so a case's history and state in a batch are bitwise those of the same
+case alone.
+"""
+
+from __future__ import annotations
+
+import copy
+from dataclasses import replace
+
+import numpy as np
+import pytest
+
+from goldens import load
+from jaxrans_b200.case import parse_case
+from jaxrans_b200.config import freestream_primitive
+from jaxrans_b200.solver import freestream_state
+
+pytestmark = pytest.mark.gpu
+
+ALPHAS = (-1.0, 2.5)
+
+
+def flows_of(case, alphas):
+    return [replace(case.flow, alpha_deg=float(a)) for a in alphas]
+
+
+def alone(case, plan, flow, steps):
+    from jaxrans_b200.native import DevicePlan
+    dev = DevicePlan(plan, flow, case.numerics, case.implicit)
+    dev.set_state(freestream_state(replace(case, flow=flow), plan), case.implicit.cfl)
+    hist = dev.newton_steps(steps)
+    U, cfl, res, status = dev.get_state()
+    return hist, U, cfl, dev.forces()
+
+
+@pytest.mark.parametrize("name", ["o_euler", "c_sa"])
+def test_batch_is_bitwise_the_cases_alone(cuda, name):
+    from jaxrans_b200.native import DevicePlan
+    z, case, plan = load(name)
+    flows = flows_of(case, ALPHAS)
+    dev = DevicePlan.batch(plan, flows, case.numerics, case.implicit)
+    U0 = np.concatenate([freestream_state(replace(case, flow=f), plan).ravel() for f in flows])
+    dev.set_state(U0, case.implicit.cfl)
+    steps = 12
+    hist = dev.newton_steps(steps)
+    assert hist.shape == (steps, len(flows))
+    forces = dev.forces()
+    for k, flow in enumerate(flows):
+        h1, U1, cfl1, f1 = alone(case, plan, flow, steps)
+        Uk, cflk, _, _ = dev.case_state(k)
+        assert np.array_equal(hist[:, k], h1)
+        assert np.array_equal(Uk, U1)
+        assert cflk == cfl1
+        assert np.array_equal(forces[k], f1)
+
+
+def test_batch_of_two_grids(cuda):
+    """Cases of different canvas sizes in one batch (the launches span the largest)."""
+    from jaxrans_b200.native import DevicePlan
+    z, case, plan = load("o_euler")
+    import json
+    doc = json.loads(str(z["case_json"]))
+    small_doc = copy.deepcopy(doc)
+    small_doc["case"]["domain"]["cells_airfoil"] = 40
+    small_doc["case"]["domain"]["cells_normal"] = 24
+    small = parse_case(small_doc["case"], small_doc["numerical"])
+    small_plan = small.grid()
+    assert small_plan.NI * small_plan.NJ < plan.NI * plan.NJ
+    dev = DevicePlan.batch([plan, small_plan], [case.flow, small.flow], case.numerics, case.implicit)
+    U0 = np.concatenate([freestream_state(case, plan).ravel(), freestream_state(small, small_plan).ravel()])
+    dev.set_state(U0, case.implicit.cfl)
+    hist = dev.newton_steps(8)
+    for k, (c, p) in enumerate([(case, plan), (small, small_plan)]):
+        h1, U1, _, _ = alone(c, p, c.flow, 8)
+        assert np.array_equal(hist[:, k], h1)
+        assert np.array_equal(dev.case_state(k)[0], U1)
+
+
+def test_disabled_case_is_untouched(cuda):
+    from jaxrans_b200.native import DevicePlan
+    z, case, plan = load("o_euler")
+    flows = flows_of(case, ALPHAS)
+    dev = DevicePlan.batch(plan, flows, case.numerics, case.implicit)
+    U0 = np.concatenate([freestream_state(replace(case, flow=f), plan).ravel() for f in flows])
+    dev.set_state(U0, case.implicit.cfl)
+    dev.enable(1, False)
+    dev.newton_steps(5)
+    U1, _, _, _ = dev.case_state(1)
+    assert np.array_equal(U1, freestream_state(replace(case, flow=flows[1]), plan))
+    h0, U0k, _, _ = alone(case, plan, flows[0], 5)
+    assert np.array_equal(dev.case_state(0)[0], U0k)
+    dev.enable(1, True)
+    hist = dev.newton_steps(5)
+    h1, U1k, _, _ = alone(case, plan, flows[1], 5)
+    assert np.array_equal(hist[:, 1], h1)
+
+
+def test_new_inflow_equals_a_new_case(cuda):
+    """Changing a case's freestream in place gives the case built at that angle."""
+    from jaxrans_b200.native import DevicePlan
+    z, case, plan = load("c_sa")
+    flows = flows_of(case, ALPHAS)
+    dev = DevicePlan.batch(plan, [flows[0], flows[0]], case.numerics, case.implicit)
+    dev.set_inflow(1, freestream_primitive(flows[1]))
+    U0 = np.concatenate([freestream_state(replace(case, flow=f), plan).ravel() for f in flows])
+    dev.set_state(U0, case.implicit.cfl)
+    hist = dev.newton_steps(6)
+    h1, U1, _, f1 = alone(case, plan, flows[1], 6)
+    assert np.array_equal(hist[:, 1], h1)
+    assert np.array_equal(dev.forces()[1], f1)
