@@ -143,12 +143,14 @@ def run_reference(args) -> int:
     rank, _, world = rank_info()
     if rank != 0:
         return 0
-    from jaxrans_b200.workloads import workload
-    case = workload(args.workload, **{"implicit.precision": args.precision})
+    from jaxrans_b200.workloads import BATCHES, workload
+    # a batch is timed on its first case (the oracle runs one case at a time)
+    name = BATCHES[args.workload][0][0] if args.workload in BATCHES else args.workload
+    case = workload(name, **{"implicit.precision": args.precision})
     plan = case.grid()
     times = reference_sample(case, plan, args.steps, args.warmup, args.precision)
     per_step = statistics.mean(times)
-    n = STEPS_PER_SOLVE[args.workload]
+    n = STEPS_PER_SOLVE[name]
     value = 3600.0 / (per_step * n)
     sample = (f"{args.steps} Newton steps of the oracle (NumPy FP64, complex-step J.v) from the freestream on "
               f"the {args.workload} case after {args.warmup} warm-up steps, {per_step:.2f} s each, scaled by "
@@ -164,6 +166,29 @@ def run_reference(args) -> int:
     return 0
 
 
+def load_job(args):
+    """The cases of the workload (one, or a named batch), their grids (one per distinct
+    workload) and the device plan."""
+    from jaxrans_b200.batch import batch_device
+    from jaxrans_b200.solver import device_for
+    from jaxrans_b200.workloads import BATCHES, batch_workload, workload
+    prec = {"implicit.precision": args.precision}
+    if args.workload in BATCHES:
+        cases = batch_workload(args.workload, **prec)
+        names = [w for w, _ in BATCHES[args.workload]]
+    else:
+        cases = [workload(args.workload, **prec)]
+        names = [args.workload]
+    made = {}
+    grids = []
+    for name, case in zip(names, cases):
+        if name not in made:
+            made[name] = case.grid()
+        grids.append(made[name])
+    dev = batch_device(cases, grids) if len(cases) > 1 else device_for(cases[0], grids[0])
+    return cases, grids, dev
+
+
 def run_device(args) -> int:
     import torch
     rank, local, world = rank_info()
@@ -173,14 +198,14 @@ def run_device(args) -> int:
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from jaxrans_b200.batch import run_batch_blocks
     from jaxrans_b200.build import build
-    from jaxrans_b200.solver import device_for, freestream_state, run_blocks
-    from jaxrans_b200.workloads import workload
+    from jaxrans_b200.solver import freestream_state
     build()
-    case = workload(args.workload, **{"implicit.precision": args.precision})
-    plan = case.grid()
-    dev = device_for(case, plan)
-    U0 = freestream_state(case, plan)
+    cases, grids, dev = load_job(args)
+    n_cases = len(cases)
+    cfl = cases[0].implicit.cfl
+    U0 = np.concatenate([freestream_state(c, g).ravel() for c, g in zip(cases, grids)])
     U0_pinned = torch.from_numpy(U0).pin_memory()
     U0_dev = U0_pinned.to("cuda")
     stream = torch.cuda.ExternalStream(dev.stream_handle())
@@ -192,13 +217,20 @@ def run_device(args) -> int:
         if dist is not None:
             dist.barrier()
 
+    def enable_all():
+        if n_cases > 1:
+            for k in range(n_cases):
+                dev.enable(k, True)
+
     def device_solve():
-        dev.set_state_device(U0_dev, case.implicit.cfl)
-        return run_blocks(case, dev)
+        dev.set_state_device(U0_dev, cfl)
+        enable_all()
+        return run_batch_blocks(cases, dev)[0]
 
     def host_solve():
-        dev.set_state(U0_pinned.numpy(), case.implicit.cfl)
-        out = run_blocks(case, dev)
+        dev.set_state(U0_pinned.numpy() if n_cases > 1 else U0_pinned.numpy().reshape(dev.shape), cfl)
+        enable_all()
+        out = run_batch_blocks(cases, dev)[0]
         U, _, _, _ = dev.get_state()
         return out, U
 
@@ -219,8 +251,8 @@ def run_device(args) -> int:
             torch.cuda.synchronize()
             starts.append(s)
             ends.append(e)
-    per_solve = [s.elapsed_time(e) / 1e3 for s, e in zip(starts, ends)]
-    total = sum(per_solve)
+    per_step = [s.elapsed_time(e) / 1e3 for s, e in zip(starts, ends)]
+    total = sum(per_step)
     # e2e: host state in, state and forces out, through the C ABI
     e2e_times = []
     for _ in range(args.steps):
@@ -239,51 +271,63 @@ def run_device(args) -> int:
         t = torch.tensor([total, e2e_total], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total, e2e_total = float(t[0]), float(t[1])
-    value = 3600.0 * args.steps * world / total
-    e2e_value = 3600.0 * args.steps * world / e2e_total
-    iters = [int(b.residual.size) for b in solves]
-    blocks = [int(b.blocks) for b in solves]
-    launches = sum(i * kps + b * 2 for i, b in zip(iters, blocks))
+    value = 3600.0 * args.steps * n_cases * world / total
+    e2e_value = 3600.0 * args.steps * n_cases * world / e2e_total
+    # every case's latency: its exit within its batch, on the device clock of the batch
+    latencies = [m.seconds * (step_t / max(mm.seconds for mm in mons))
+                 for mons, step_t in zip(solves, per_step) for m in mons]
+    iters = [m.iterations for mons in solves for m in mons]
+    blocks = [max(len(m.blocks) for m in mons) for mons in solves]
+    steps_run = [max(m.iterations for m in mons) for mons in solves]
+    launches = sum(i * kps + b * 2 for i, b in zip(steps_run, blocks))
     kern = dev.time_kernels(20)
     peaks = measured_peaks()
-    nvar = case.flow.nvar
+    nvar = cases[0].flow.nvar
     bpc = jvp_bytes_per_cell(nvar)
-    achieved = bpc * plan.cells / (kern["jvp_tile"] * 1e-3) / 1e9
+    cells = sum(g.cells for g in grids)
+    achieved = bpc * cells / (kern["jvp_tile"] * 1e-3) / 1e9
     traffic = profiled_traffic(args.workload)
+    last = solves[-1]
+    config = {"workload": args.workload, "cases": n_cases, "cells": cells, "nvar": nvar,
+              "precision": args.precision, "newton_steps_per_solve": int(np.median(iters)),
+              "exit_reasons": sorted({m.reason for mons in solves for m in mons}),
+              "l2": "flushed (256 MB write) per step", "parallelism": f"replicas x{world}"}
+    if n_cases == 1:
+        config["canvas"] = list(grids[0].shape)
+        f = last[0].forces
+        config["forces"] = {"cl": f.cl, "cd": f.cd, "cm": f.cm}
+    else:
+        config["batch"] = "every case in one device plan: one captured graph per Newton step for all"
+        config["newton_steps_per_batch"] = int(max(steps_run))
+    block_iters = cases[0].block_iters
     result = {
         "metric": METRIC, "value": value, "unit": "solves/hr", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32",
-        "data": "synthetic (generated NACA section and grid, freestream start)",
-        "config": {"workload": args.workload, "cells": plan.cells, "canvas": list(plan.shape), "nvar": nvar,
-                   "precision": args.precision, "newton_steps_per_solve": int(np.median(iters)),
-                   "exit_reasons": sorted({b.reason for b in solves}), "l2": "flushed (256 MB write) per step",
-                   "parallelism": f"replicas x{world}",
-                   "forces": {"cl": solves[-1].last_forces.cl, "cd": solves[-1].last_forces.cd,
-                              "cm": solves[-1].last_forces.cm}},
-        "latency_s": {"p50": float(np.percentile(per_solve, 50)), "p99": float(np.percentile(per_solve, 99))},
+        "data": "synthetic (generated NACA sections and grids, freestream start)",
+        "config": config,
+        "latency_s": {"p50": float(np.percentile(latencies, 50)), "p99": float(np.percentile(latencies, 99))},
         "e2e": {"value": e2e_value, "unit": "solves/hr", "h2d_bytes_per_step": int(U0.nbytes),
-                "d2h_bytes_per_step": int(U0.nbytes + sum(b.blocks for b in [out]) * 8 * (case.block_iters + 6))},
+                "d2h_bytes_per_step": int(U0.nbytes + max(len(m.blocks) for m in out) * 8 * n_cases
+                                          * (block_iters + 6))},
         "gpu_launches": launches,
         "roofline": {"kernel": "jvp_tile", "bound": "hbm", "achieved": achieved,
                      "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
                      "traffic": None if traffic is None else traffic,
-                     "algorithmic_bytes_per_launch": bpc * plan.cells, "launch_ms": kern["jvp_tile"],
+                     "algorithmic_bytes_per_launch": bpc * cells, "launch_ms": kern["jvp_tile"],
                      "peak_source": peaks.get("source", "measured")},
         "kernel_ms": kern,
     }
     if rank == 0:
-        with Clocks(local) as _:
-            pass
         result["clocks"] = clocks.summary()
         if world == 1 and not args.no_cpu_baseline:
-            times = reference_sample(case, plan, 1, 0, args.precision)
-            per_step = times[0]
+            times = reference_sample(cases[0], grids[0], 1, 0, args.precision)
+            per = times[0]
             n = int(np.median(iters))
             result["cpu_baseline"] = {
-                "value": 3600.0 / (per_step * n), "unit": "solves/hr", "cores": 1, "kind": "port",
-                "sample": (f"one Newton step of the oracle (NumPy FP64, complex-step J.v) from the freestream, "
-                           f"{per_step:.2f} s, scaled by the {n} Newton steps of a converged solve")}
+                "value": 3600.0 / (per * n), "unit": "solves/hr", "cores": 1, "kind": "port",
+                "sample": (f"one Newton step of the oracle (NumPy FP64, complex-step J.v) from the freestream on "
+                           f"{cases[0].name}, {per:.2f} s, scaled by the {n} Newton steps of a converged solve")}
         print(json.dumps(result), flush=True)
     if dist is not None:
         dist.barrier()
@@ -298,7 +342,7 @@ def main(argv=None) -> int:
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=("b200", "reference"))
-    p.add_argument("--workload", default="c_sa_385", choices=sorted(STEPS_PER_SOLVE))
+    p.add_argument("--workload", default="c_sa_385", choices=sorted(STEPS_PER_SOLVE) + ["polar64_uneven"])
     p.add_argument("--precision", default="fp64", choices=("fp64", "mixed"))
     p.add_argument("--no-cpu-baseline", action="store_true")
     args = p.parse_args(argv)

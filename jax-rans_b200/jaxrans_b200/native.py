@@ -222,14 +222,25 @@ class DevicePlan:
         return self
 
     def _create(self, plans, flows, numerics, implicit, force_length, moment_centre, library):
+        """``numerics``, ``implicit``, ``force_length`` and ``moment_centre`` are one for
+        every case or a list with one per case."""
+        n = len(plans)
+
+        def per_case(x, single=lambda x: False):
+            return list(x) if isinstance(x, (list, tuple)) and not single(x) else [x] * n
+
+        nums = per_case(numerics)
+        imps = [i or ImplicitConfig() for i in per_case(implicit)]
+        lengths = per_case(force_length)
+        centres = per_case(moment_centre, lambda x: len(x) in (2, 3) and np.isscalar(x[0]))
         self.lib = load_library(library)
-        self.plans, self.flows, self.numerics = plans, flows, numerics
+        self.plans, self.flows, self.numerics = plans, flows, nums[0]
         self.plan, self.flow = plans[0], flows[0]
-        self.implicit = implicit or ImplicitConfig()
+        self.implicit = imps[0]
         keep: list = []
-        descs = (PlanDesc * len(plans))()
+        descs = (PlanDesc * n)()
         for k, (plan, flow) in enumerate(zip(plans, flows)):
-            fill_desc(descs[k], plan, flow, numerics, self.implicit, force_length, moment_centre, keep)
+            fill_desc(descs[k], plan, flow, nums[k], imps[k], lengths[k], centres[k], keep)
         handle = C.c_void_p()
         if len(plans) == 1:
             _check(self.lib, self.lib.jr_plan_create(descs, C.byref(handle)), "jr_plan_create")

@@ -160,103 +160,96 @@ class Blocks:
     blocks: int
 
 
-def run_blocks(case: Case, dev, max_iters=None, progress=None) -> Blocks:
-    """Blocks of ``block_iters`` Newton steps from the device's current state until the
-    exit test of ``src/jaxrans/solvers/driver.py:123-201`` stops the case."""
-    num = case.numerics
-    block_iters = case.block_iters
-    max_iters = num.max_iters if max_iters is None else max_iters
-    n_blocks = max(1, -(-max_iters // block_iters))
-    blocks, cl_history, coefficients = [], [], []
-    peak, reason = 0.0, ExitReason.MAX_ITERS
-    started = time.perf_counter()
-    first_block = float("nan")
-    f = None
-    for b in range(n_blocks):
-        hist = dev.newton_steps(block_iters)
-        if b == 0:
-            first_block = time.perf_counter() - started
-        blocks.append(hist)
-        f = forces_of(dev.forces())
-        cl_history.append(f.cl)
-        coefficients.append((f.cl, f.cd, f.cm))
+class CaseMonitor:
+    """The exit test of one case, fed one block of residual norms and the forces after it
+    at a time: ``src/jaxrans/solvers/driver.py:161-190`` for one case, with the force
+    settling of ``src/jaxrans/simulation.py:243-284``.  A single run and every case of a
+    batch go through this same code."""
+
+    def __init__(self, case: Case, max_iters=None):
+        num = case.numerics
+        self.tol, self.forces_tol = num.tol, num.forces_tol
+        self.block_iters = case.block_iters
+        max_iters = num.max_iters if max_iters is None else max_iters
+        self.n_blocks = max(1, -(-max_iters // self.block_iters))
+        self.blocks: list[np.ndarray] = []
+        self.cl_history: list[float] = []
+        self.coefficients: list[tuple] = []
+        self.peak, self.reason, self.forces = 0.0, ExitReason.MAX_ITERS, None
+        self.seconds = float("nan")   # set by a batch driver when the case stops
+
+    @property
+    def done(self) -> bool:
+        return self.reason != ExitReason.MAX_ITERS or len(self.blocks) >= self.n_blocks
+
+    @property
+    def iterations(self) -> int:
+        return len(self.blocks) * self.block_iters
+
+    def orders(self) -> float:
+        last = float(self.blocks[-1][-1])
+        return float(np.log10(self.peak / last)) if self.peak > 0 and last > 0 else 0.0
+
+    def feed(self, hist: np.ndarray, forces) -> bool:
+        """One block; true once the case has stopped."""
+        hist = np.asarray(hist, dtype=np.float64)
+        f = forces_of(forces)
+        self.forces = f
+        self.blocks.append(hist)
+        self.cl_history.append(f.cl)
+        self.coefficients.append((f.cl, f.cd, f.cm))
         finite = hist[np.isfinite(hist)]
         if finite.size:
-            peak = max(peak, float(finite.max()))
-        if progress is not None:
-            last = float(hist[-1])
-            orders = float(np.log10(peak / last)) if peak > 0 and last > 0 else 0.0
-            progress((b + 1) * block_iters, last, orders, f)
-        stop = num.forces_tol is not None and all(cl_spread(h) < num.forces_tol
-                                                  for h in np.transpose(coefficients))
+            self.peak = max(self.peak, float(finite.max()))
+        stop = self.forces_tol is not None and all(cl_spread(h) < self.forces_tol
+                                                   for h in np.transpose(self.coefficients))
         last = hist[-1]
         failed = not np.all(np.isfinite(hist)) or not np.all(np.isfinite([f.cl, f.cd, f.cm]))
         if failed:
-            reason = ExitReason.NON_FINITE
-        elif peak > 0 and last <= num.tol * peak:
-            reason = ExitReason.CONVERGED
+            self.reason = ExitReason.NON_FINITE
+        elif self.peak > 0 and last <= self.tol * self.peak:
+            self.reason = ExitReason.CONVERGED
         elif len(hist) > 1 and np.all(hist == hist[0]):
-            reason = ExitReason.STALLED
+            self.reason = ExitReason.STALLED
         elif stop:
-            reason = ExitReason.SETTLED
-        if reason != ExitReason.MAX_ITERS:
-            break
-    return Blocks(np.concatenate(blocks), reason, np.asarray(cl_history), np.asarray(coefficients), f,
-                  time.perf_counter() - started, first_block, len(blocks))
+            self.reason = ExitReason.SETTLED
+        return self.done
+
+    def residual(self) -> np.ndarray:
+        return np.concatenate(self.blocks) if self.blocks else np.zeros(0)
+
+
+def run_blocks(case: Case, dev, max_iters=None, progress=None) -> Blocks:
+    """Blocks of ``block_iters`` Newton steps from the device's current state until the
+    exit test of ``src/jaxrans/solvers/driver.py:123-201`` stops the case."""
+    mon = CaseMonitor(case, max_iters)
+    started = time.perf_counter()
+    first_block = float("nan")
+    while not mon.done:
+        hist = dev.newton_steps(mon.block_iters)
+        if not mon.blocks:
+            first_block = time.perf_counter() - started
+        mon.feed(hist, dev.forces())
+        if progress is not None:
+            progress(mon.iterations, float(hist[-1]), mon.orders(), mon.forces)
+    return Blocks(mon.residual(), mon.reason, np.asarray(mon.cl_history), np.asarray(mon.coefficients),
+                  mon.forces, time.perf_counter() - started, first_block, len(mon.blocks))
 
 
 def march(case: Case, plan: Plan, progress=None, initial=None, device=None, max_iters=None) -> Result:
     """One grid to steady state from the freestream, or from ``initial`` on the block cells."""
-    num = case.numerics
     dev = device if device is not None else device_for(case, plan)
     U0 = freestream_state(case, plan)
     if initial is not None:
         U0 = np.where(plan.interior, np.asarray(initial), U0)
     dev.set_state(U0, case.implicit.cfl, float("inf"))
-    block_iters = case.block_iters
-    max_iters = num.max_iters if max_iters is None else max_iters
-    n_blocks = max(1, -(-max_iters // block_iters))
-    blocks, cl_history, coefficients = [], [], []
-    peak, reason = 0.0, ExitReason.MAX_ITERS
-    started = time.perf_counter()
-    first_block = float("nan")
-    for b in range(n_blocks):
-        hist = dev.newton_steps(block_iters)
-        if b == 0:
-            first_block = time.perf_counter() - started
-        blocks.append(hist)
-        f = forces_of(dev.forces())
-        cl_history.append(f.cl)
-        coefficients.append((f.cl, f.cd, f.cm))
-        finite = hist[np.isfinite(hist)]
-        if finite.size:
-            peak = max(peak, float(finite.max()))
-        if progress is not None:
-            last = float(hist[-1])
-            orders = float(np.log10(peak / last)) if peak > 0 and last > 0 else 0.0
-            progress((b + 1) * block_iters, last, orders, f)
-        stop = num.forces_tol is not None and all(cl_spread(h) < num.forces_tol
-                                                  for h in np.transpose(coefficients))
-        last = hist[-1]
-        failed = not np.all(np.isfinite(hist)) or not np.all(np.isfinite([f.cl, f.cd, f.cm]))
-        if failed:
-            reason = ExitReason.NON_FINITE
-        elif peak > 0 and last <= num.tol * peak:
-            reason = ExitReason.CONVERGED
-        elif len(hist) > 1 and np.all(hist == hist[0]):
-            reason = ExitReason.STALLED
-        elif stop:
-            reason = ExitReason.SETTLED
-        if reason != ExitReason.MAX_ITERS:
-            break
-    seconds = time.perf_counter() - started
-    residual = np.concatenate(blocks)
+    blk = run_blocks(case, dev, max_iters, progress)
     U, _, _, _ = dev.get_state()
-    history = ConvergenceHistory(residual, reason, int(residual.size), seconds, first_block)
+    history = ConvergenceHistory(blk.residual, blk.reason, int(blk.residual.size), blk.seconds, blk.first_block)
     return Result(case=case, grid=plan, U=U, forces=forces_of(dev.forces()), history=history,
-                  cl_history=np.asarray(cl_history),
-                  timing=Timing(seconds, first_block, int(residual.size), block_iters, plan.cells),
-                  coefficients=np.asarray(coefficients))
+                  cl_history=blk.cl_history,
+                  timing=Timing(blk.seconds, blk.first_block, int(blk.residual.size), case.block_iters, plan.cells),
+                  coefficients=blk.coefficients)
 
 
 def run(case: Case, grid: Plan | None = None, progress=None, on_level=None, devices=None, *, initial=None) -> Result:

@@ -20,6 +20,13 @@ on a GPU box and in the oracle.
   stalls 3.5 orders below its peak.  A solve therefore ends by the reference's own exit
   test: converged at 1e-12 of the peak, or settled once CL, CD and CM each vary by less
   than 1e-6 over the last quarter of the run (a hundredth of a drag count).
+* ``c_sa_257`` / ``c_sa_513`` / ``c_sa_769`` -- the uneven grids of the batched polar:
+  SA-noft2 on C-grids of 257 x 65 (NACA 0012, M 0.15, Re 3e6), 513 x 129 (NACA 2412,
+  M 0.2, Re 6e6) and 769 x 193 nodes (NACA 4415, M 0.3, Re 9e6), two thirds of the
+  cells round the airfoil and a sixth along each wake side, the numerics of
+  ``c_sa_385``.
+* batch ``polar64_uneven`` -- 64 angles uniform on [-4, 16] deg on the ``c_sa_385``
+  grid together with the three uneven cases, all in one device batch.
 """
 
 from __future__ import annotations
@@ -52,6 +59,41 @@ WORKLOADS = {
          "convergence": {"max_iters": 4000, "tol": 1e-12, "forces_tol": 1e-6, "block_iters": 20}},
     ),
 }
+
+
+def _c_sa(name: str, airfoil: str, around: int, wake: int, normal: int, mach: float, reynolds: float):
+    case_doc, num_doc = copy.deepcopy(WORKLOADS["c_sa_385"])
+    case_doc["general"]["case_name"] = name
+    case_doc["domain"].update({"airfoil": airfoil, "cells_airfoil": around, "cells_wake": wake,
+                               "cells_normal": normal})
+    case_doc["freestream"].update({"mach": mach, "reynolds": reynolds})
+    return case_doc, num_doc
+
+
+WORKLOADS["c_sa_257"] = _c_sa("c_sa_257", "naca0012", 172, 42, 64, 0.15, 3e6)
+WORKLOADS["c_sa_513"] = _c_sa("c_sa_513", "naca2412", 344, 84, 128, 0.2, 6e6)
+WORKLOADS["c_sa_769"] = _c_sa("c_sa_769", "naca4415", 512, 128, 192, 0.3, 9e6)
+
+# batches: (workload, alpha or None for the workload's own) per case
+BATCHES = {
+    "polar64_uneven": [("c_sa_385", float(a)) for a in
+                       [-4.0 + 20.0 * k / 63 for k in range(64)]] + [("c_sa_257", None), ("c_sa_513", None),
+                                                                      ("c_sa_769", None)],
+}
+
+
+def batch_workload(name: str, **numerical) -> list[Case]:
+    """The cases of a named batch; ``numerical`` overrides apply to every case."""
+    import dataclasses
+    cases = []
+    for work, alpha in BATCHES[name]:
+        case = workload(work, **numerical)
+        if alpha is not None:
+            flow = dataclasses.replace(case.flow, alpha_deg=alpha)
+            case = dataclasses.replace(case, flow=flow, name=f"{case.name}_a{alpha:+.2f}")
+        cases.append(case)
+    return cases
+
 
 
 def workload(name: str, **numerical) -> Case:

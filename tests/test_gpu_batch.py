@@ -113,3 +113,41 @@ def test_new_inflow_equals_a_new_case(cuda):
     h1, U1, _, f1 = alone(case, plan, flows[1], 6)
     assert np.array_equal(hist[:, 1], h1)
     assert np.array_equal(dev.forces()[1], f1)
+
+
+def test_polar_angles_equal_their_runs_alone(cuda):
+    """run_polar (src/jaxrans/polar.py:80-121) on the device batch: each angle's history,
+    exit and forces are bitwise those of ``march`` of that angle alone."""
+    from jaxrans_b200.polar import at_alpha, run_polar
+    from jaxrans_b200.solver import march
+    z, case, plan = load("c_sa")
+    case = replace(case, numerics=replace(case.numerics, max_iters=80))
+    polar = run_polar(case, [-2.0, 3.0, 7.5], grid=plan)
+    assert polar.table().shape == (3, 9)
+    for a, r in zip(polar.alphas, polar.results):
+        alone = march(at_alpha(case, a), plan)
+        assert r.history.reason == alone.history.reason
+        assert np.array_equal(r.history.residual, alone.history.residual)
+        assert np.array_equal(r.U, alone.U)
+        assert r.forces == alone.forces
+
+
+def test_uneven_batch_equals_runs_alone(cuda):
+    """Cases on grids of different sizes and different flows in one batch."""
+    import json
+    from jaxrans_b200.batch import run_batch
+    from jaxrans_b200.solver import march
+    z, case, plan = load("o_euler")
+    doc = json.loads(str(z["case_json"]))
+    other_doc = copy.deepcopy(doc)
+    other_doc["case"]["domain"]["cells_airfoil"] = 64
+    other_doc["case"]["domain"]["cells_normal"] = 24
+    other_doc["case"]["freestream"]["mach"] = 0.5
+    other = parse_case(other_doc["case"], other_doc["numerical"])
+    cases = [replace(c, numerics=replace(c.numerics, max_iters=60)) for c in (case, other)]
+    grids = [plan, other.grid()]
+    results = run_batch(cases, grids)
+    for c, g, r in zip(cases, grids, results):
+        alone = march(c, g)
+        assert np.array_equal(r.history.residual, alone.history.residual)
+        assert np.array_equal(r.U, alone.U)
