@@ -214,7 +214,20 @@ def march(line: np.ndarray, steps: np.ndarray, closed: bool, outflow: np.ndarray
         C[:, 1, 0] = (ty * ex + tx * ey) / t2
         C[:, 1, 1] = (ty * ey - tx * ex) / t2
         rhs = r + eta + np.einsum("nab,nb->na", C, t) - smoothing * _d2(r, closed)
-        rows, cols, vals = [], [], []
+        # the entries row by row, each row's three 2x2 blocks left to right, zeros
+        # dropped: the sparse matrix the solver sees is the same entry for entry
+        i = np.arange(n) if closed else np.arange(1, n - 1)
+        Ci = C[i]
+        blocks = np.stack([-0.5 * Ci - smoothing * eye, np.broadcast_to((1.0 + 2.0 * smoothing) * eye, Ci.shape),
+                           0.5 * Ci - smoothing * eye], axis=1)                    # (m, 3, 2, 2)
+        j = np.stack([(i - 1) % n, i, (i + 1) % n], axis=1)                         # (m, 3)
+        ab = np.arange(2)
+        r_idx = np.broadcast_to(2 * i[:, None, None, None] + ab[None, None, :, None], blocks.shape)
+        c_idx = np.broadcast_to(2 * j[:, :, None, None] + ab[None, None, None, :], blocks.shape)
+        keep = blocks.ravel() != 0.0
+        rows = list(r_idx.ravel()[keep])
+        cols = list(c_idx.ravel()[keep])
+        vals = list(blocks.ravel()[keep])
 
         def put(i, j, block):
             for a in range(2):
@@ -224,10 +237,6 @@ def march(line: np.ndarray, steps: np.ndarray, closed: bool, outflow: np.ndarray
                         cols.append(2 * j + b)
                         vals.append(block[a, b])
 
-        for i in (range(n) if closed else range(1, n - 1)):
-            put(i, (i - 1) % n, -0.5 * C[i] - smoothing * eye)
-            put(i, i, (1.0 + 2.0 * smoothing) * eye)
-            put(i, (i + 1) % n, 0.5 * C[i] - smoothing * eye)
         if not closed:
             w = outflow / np.linalg.norm(outflow)
             m = np.array([-w[1], w[0]])
