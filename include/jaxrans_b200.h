@@ -113,6 +113,21 @@ int jr_synchronize(jr_plan* plan);
  * (src/jaxrans/numerics/residual.py:273-334, residual() at :324-327).  Device pointers. */
 int jr_residual(jr_plan* plan, const double* U, double* R, int first_order);
 
+/* R(U) as jr_residual computes it, for callers that cannot allocate device memory when
+ * they call: a handler running inside another framework's step, whose allocator owns the
+ * device's memory and where a cudaMalloc or cudaFree would also synchronise the device.
+ * The call's scratch (its case table, the ghost-filled canvas, the tile partial sums) is
+ * a static device array of 8 MiB (8388608 bytes) inside the library, held by every GPU
+ * that loads it, so the call allocates nothing and writes no work buffer of the plan; a
+ * plan that needs more scratch is refused with JR_EINVAL.  The first call on a device
+ * looks up the array's address there (set-up): make it with the plan's device current
+ * and before any stream capture.  Every call on a device shares the one array, which
+ * keeps the last call's contents (the canvas part is cleared by each call): calls whose
+ * work overlaps on the GPU -- on other streams, or for other plans -- race on it.  No
+ * counterpart in the reference, which has no FFI and allocates through XLA.  Device
+ * pointers. */
+int jr_residual_noalloc(jr_plan* plan, const double* U, double* R, int first_order);
+
 /* dR1/dU . v: the exact tangent of the first-order residual at U (forward-mode duals).
  * Replaces jax.linearize(jacobian_source.residual, U)'s jvp
  * (src/jaxrans/solvers/implicit.py:104-108).  Device pointers. */

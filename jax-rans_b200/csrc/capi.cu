@@ -66,6 +66,7 @@ struct jr_plan {
   double* force_out = nullptr;           // 8 per case
   Scalars* sc = nullptr;                 // one per case
   cudaGraphExec_t graph = nullptr;
+  int device = 0;                        // the device current when the plan was made
 };
 
 static int fail(int code, const std::string& msg) {
@@ -437,6 +438,7 @@ int jr_batch_create(const jr_plan_desc* descs, int32_t n_cases, jr_plan** out) {
   }
   jr_plan* plan = new jr_plan();
   plan->n_cases = n_cases;
+  cudaGetDevice(&plan->device);
   plan->host.resize(n_cases);
   if (cudaStreamCreateWithFlags(&plan->owned_stream, cudaStreamNonBlocking) == cudaSuccess)
     plan->st = plan->owned_stream;
@@ -792,3 +794,81 @@ int jr_forces(jr_plan* plan, const double* U, double* out) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------
+// The residual without allocation.  Some callers cannot allocate device memory when they
+// evaluate a residual: a handler running inside another framework's step (an XLA custom
+// call, a serving loop on a caching allocator), where the framework owns the device's
+// memory and a cudaMalloc or cudaFree would also synchronise the whole device.
+// jr_residual_noalloc serves them: its scratch (the call's case table, the ghost-filled
+// primitive canvas and the per-tile partial sums) lives in the file-scope array below,
+// which every GPU that loads this library holds until exit, so a call allocates nothing
+// and writes no work buffer of the plan; it reads the plan's static tables, U, and
+// writes R.
+// ------------------------------------------------------------------------------------
+
+constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(8) << 20;   // 8 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+// the array's device address on each device; the name g_noalloc_scratch in host code is
+// only a host-side stand-in, never a device address
+static unsigned char* g_noalloc_ptr[NOALLOC_MAX_DEVICES];
+
+static size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// The call's table in the scratch: the plan's cases with U and R moved to the caller's
+// arrays and qg, tile_partial into the scratch.  One thread walks the cases, in case
+// order, so the offsets are the plan's own.
+__global__ void k_noalloc_table(const CaseDev* __restrict__ src, CaseDev* __restrict__ dst, int n_cases,
+                                const double* U, double* R, double* qg, double* tile_partial) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  size_t vec = 0, tiles = 0;
+  for (int k = 0; k < n_cases; ++k) {
+    CaseDev cd = src[k];
+    cd.U = const_cast<double*>(U) + vec;
+    cd.R = R + vec;
+    cd.qg = qg + vec;
+    cd.tile_partial = tile_partial + tiles;
+    dst[k] = cd;
+    vec += (size_t)cd.n_vec;
+    tiles += (size_t)cd.n_tiles;
+  }
+}
+
+extern "C" int jr_residual_noalloc(jr_plan* plan, const double* U, double* R, int first_order) {
+  if (!plan || !U || !R) return fail(JR_EINVAL, "null argument");
+  size_t tiles = 0;
+  for (const CaseDev& cd : plan->host) tiles += (size_t)cd.n_tiles;
+  const size_t table_bytes = round256((size_t)plan->n_cases * sizeof(CaseDev));
+  const size_t qg_bytes = round256(plan->total_vec * sizeof(double));
+  const size_t need = table_bytes + qg_bytes + tiles * sizeof(double);
+  if (need > NOALLOC_SCRATCH_BYTES)
+    return fail(JR_EINVAL, "jr_residual_noalloc: the plan needs " + std::to_string(need) +
+                               " bytes of scratch, more than the 8 MiB (8388608 bytes) this entry point has; "
+                               "use jr_residual");
+  if (plan->device < 0 || plan->device >= NOALLOC_MAX_DEVICES)
+    return fail(JR_EINVAL, "jr_residual_noalloc: device ordinal beyond 63");
+  int current = 0;
+  if (cudaGetDevice(&current) != cudaSuccess) return cuda_check("jr_residual_noalloc: cudaGetDevice");
+  if (current != plan->device) return fail(JR_EINVAL, "jr_residual_noalloc: make the plan's device current first");
+  // set-up, once per device (the first call on it): the array's device address
+  unsigned char* base = g_noalloc_ptr[current];
+  if (base == nullptr) {
+    cudaError_t e = cudaGetSymbolAddress((void**)&base, g_noalloc_scratch);
+    if (e != cudaSuccess || base == nullptr)
+      return fail(JR_ECUDA, std::string("jr_residual_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    g_noalloc_ptr[current] = base;
+  }
+  CaseDev* table = reinterpret_cast<CaseDev*>(base);
+  double* qg = reinterpret_cast<double*>(base + table_bytes);
+  double* tile_partial = reinterpret_cast<double*>(base + table_bytes + qg_bytes);
+  // the array keeps the last call's contents: the ghost canvas starts at zero, as the
+  // plan's own does, so canvas cells that no ghost record fills read the same values
+  if (cudaMemsetAsync(qg, 0, plan->total_vec * sizeof(double), plan->st) != cudaSuccess)
+    return cuda_check("jr_residual_noalloc: clear");
+  k_noalloc_table<<<1, 32, 0, plan->st>>>(plan->cases, table, plan->n_cases, U, R, qg, tile_partial);
+  launch_ghosts(table, plan->dims, -1, 0, plan->st);
+  launch_residual(table, plan->dims, plan->visc, first_order == 0, B_R, plan->st);
+  return cuda_check("jr_residual_noalloc");
+}

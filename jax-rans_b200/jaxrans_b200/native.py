@@ -61,7 +61,7 @@ EXPORTS = ("jr_plan_create", "jr_plan_destroy", "jr_last_error", "jr_plan_sizes"
            "jr_state_set", "jr_state_get", "jr_state_device", "jr_newton_steps", "jr_newton_steps_async",
            "jr_forces", "jr_state_set_device", "jr_graph_kernels", "jr_time_kernels", "jr_plan_set_stream",
            "jr_batch_create", "jr_plan_cases", "jr_case_sizes", "jr_case_enable", "jr_case_set_inflow",
-           "jr_case_state_set", "jr_case_state_get")
+           "jr_case_state_set", "jr_case_state_get", "jr_residual_noalloc")
 
 TIMED_KERNELS = ("residual_tile", "jvp_tile", "ghosts_tangent", "line_apply", "line_factor", "cgs2_full_basis")
 
@@ -91,6 +91,7 @@ def load_library(path: Path | None = None) -> C.CDLL:
         "jr_plan_stream": (vp, [vp]),
         "jr_synchronize": (C.c_int, [vp]),
         "jr_residual": (C.c_int, [vp, vp, vp, C.c_int]),
+        "jr_residual_noalloc": (C.c_int, [vp, vp, vp, C.c_int]),
         "jr_jvp": (C.c_int, [vp, vp, vp, vp]),
         "jr_wave_speeds": (C.c_int, [vp, vp, vp]),
         "jr_precond_factor": (C.c_int, [vp, vp, C.c_double]),
