@@ -96,6 +96,14 @@ int jr_case_enable(jr_plan* plan, int32_t c, int32_t enabled);
  * freestream_primitive (src/jaxrans/polar.py:75-77, src/jaxrans/core/state.py:107-121):
  * the angle of attack or Mach number enters the solver only through this vector. */
 int jr_case_set_inflow(jr_plan* plan, int32_t c, const double* q_inf);
+/* Overwrite case c (a slot) with a new case of the same shape: same canvas, ghost, wall
+ * and chain tables' sizes (a grid of the same size and topology, another section or
+ * flow) and the plan's shared solver settings.  Static tables, physics and settings are
+ * replaced in place -- nothing is allocated -- and the slot's state is left for
+ * jr_case_state_set; JR_EMISMATCH when the shapes differ.  Replaces building a new case
+ * and its residual operator (src/jaxrans/case/loader.py:349-373,
+ * src/jaxrans/numerics/residual.py:273-334) for every request a server admits. */
+int jr_case_load(jr_plan* plan, int32_t c, const jr_plan_desc* desc);
 int jr_plan_destroy(jr_plan* plan);
 const char* jr_last_error(void);
 /* Number of canvas cells NI*NJ and of face entries (NI+1)*NJ + NI*(NJ+1), summed over

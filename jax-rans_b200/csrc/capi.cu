@@ -67,6 +67,7 @@ struct jr_plan {
   Scalars* sc = nullptr;                 // one per case
   cudaGraphExec_t graph = nullptr;
   int device = 0;                        // the device current when the plan was made
+  std::vector<std::vector<int>> chain_len;   // each case's chain lengths (host copy)
 };
 
 static int fail(int code, const std::string& msg) {
@@ -106,8 +107,20 @@ static int dev_alloc(jr_plan* p, void** dst, size_t bytes) {
     if (_rc != JR_OK) return _rc; \
   } while (0)
 
+// A table of a case: allocated and filled for a new case, or overwritten in place when a
+// slot takes a new case of the same shape (`reload`).
+template <class T> static int put(jr_plan* p, T** dst, const T* src, size_t n, bool reload) {
+  if (!reload) return dev_copy(p, dst, src, n);
+  if (n == 0) return JR_OK;
+  if (*dst == nullptr) return fail(JR_EMISMATCH, "the slot has no such table");
+  if (cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(JR_ECUDA, "cudaMemcpy to the device failed");
+  return JR_OK;
+}
+
 // Static tables, physics and solver settings of one case (the work buffers come later).
-static int build_case(jr_plan* plan, const jr_plan_desc* d, CaseDev& cd, size_t& factor_rows) {
+static int build_case(jr_plan* plan, const jr_plan_desc* d, CaseDev& cd, size_t& factor_rows,
+                      bool reload = false) {
   if (d->NI < 5 || d->NJ < 5 || (d->nvar != 4 && d->nvar != 5))
     return fail(JR_EINVAL, "canvas must be at least 5 x 5 with nvar 4 or 5");
   if (d->krylov_subspace < 1 || d->krylov_subspace > MAX_KRYLOV)
@@ -119,13 +132,13 @@ static int build_case(jr_plan* plan, const jr_plan_desc* d, CaseDev& cd, size_t&
   c.NI = NI;
   c.NJ = NJ;
   c.nvar = nv;
-  TRY(dev_copy(plan, (uint8_t**)&c.interior, d->interior, (size_t)N));
-  TRY(dev_copy(plan, (double**)&c.volume, d->volume, (size_t)N));
-  TRY(dev_copy(plan, (double**)&c.fi, d->faces_i, 2 * nfi));
-  TRY(dev_copy(plan, (double**)&c.fj, d->faces_j, 2 * nfj));
-  TRY(dev_copy(plan, (double**)&c.centres, d->centres, (size_t)2 * (NI + 2) * (NJ + 2)));
-  if (d->distance) TRY(dev_copy(plan, (double**)&c.distance, d->distance, (size_t)N));
-  TRY(dev_copy(plan, (int**)&c.neighbours, d->neighbours, (size_t)N));
+  TRY(put(plan, (uint8_t**)&c.interior, d->interior, (size_t)N, reload));
+  TRY(put(plan, (double**)&c.volume, d->volume, (size_t)N, reload));
+  TRY(put(plan, (double**)&c.fi, d->faces_i, 2 * nfi, reload));
+  TRY(put(plan, (double**)&c.fj, d->faces_j, 2 * nfj, reload));
+  TRY(put(plan, (double**)&c.centres, d->centres, (size_t)2 * (NI + 2) * (NJ + 2), reload));
+  if (d->distance) TRY(put(plan, (double**)&c.distance, d->distance, (size_t)N, reload));
+  TRY(put(plan, (int**)&c.neighbours, d->neighbours, (size_t)N, reload));
   int cells = 0;
   double vsum = 0.0;
   for (int k = 0; k < N; ++k)
@@ -142,10 +155,10 @@ static int build_case(jr_plan* plan, const jr_plan_desc* d, CaseDev& cd, size_t&
       if (d->ghost[s][k] < 0 || d->ghost[s][k] >= N || d->source[s][k] < 0 || d->source[s][k] >= N ||
           d->kind[s][k] < 0 || d->kind[s][k] > 6)
         return fail(JR_EINVAL, "a ghost record out of range");
-    TRY(dev_copy(plan, (int**)&c.g_ghost[s], d->ghost[s], (size_t)n));
-    TRY(dev_copy(plan, (int**)&c.g_source[s], d->source[s], (size_t)n));
-    TRY(dev_copy(plan, (int**)&c.g_kind[s], d->kind[s], (size_t)n));
-    TRY(dev_copy(plan, (double**)&c.g_geom[s], d->geom[s], (size_t)4 * n));
+    TRY(put(plan, (int**)&c.g_ghost[s], d->ghost[s], (size_t)n, reload));
+    TRY(put(plan, (int**)&c.g_source[s], d->source[s], (size_t)n, reload));
+    TRY(put(plan, (int**)&c.g_kind[s], d->kind[s], (size_t)n, reload));
+    TRY(put(plan, (double**)&c.g_geom[s], d->geom[s], (size_t)4 * n, reload));
   }
   {
     // stage 2 reads stage-1 ghosts at the corners: which stage-1 record fills each source
@@ -153,14 +166,14 @@ static int build_case(jr_plan* plan, const jr_plan_desc* d, CaseDev& cd, size_t&
     for (int k = 0; k < d->n_ghost[0]; ++k) rec_of[d->ghost[0][k]] = k;
     for (int k = 0; k < d->n_ghost[1]; ++k)
       if (!d->interior[d->source[1][k]]) src_rec[k] = rec_of[d->source[1][k]];
-    TRY(dev_copy(plan, (int**)&c.g_src_rec, src_rec.data(), src_rec.size()));
+    TRY(put(plan, (int**)&c.g_src_rec, src_rec.data(), src_rec.size(), reload));
   }
   c.n_walls = d->n_walls;
-  TRY(dev_copy(plan, (int**)&c.w_cell, d->wall_cell, (size_t)d->n_walls));
-  TRY(dev_copy(plan, (int**)&c.w_family, d->wall_family, (size_t)d->n_walls));
-  TRY(dev_copy(plan, (int**)&c.w_face, d->wall_face, (size_t)d->n_walls));
-  TRY(dev_copy(plan, (double**)&c.w_into, d->wall_into, (size_t)d->n_walls));
-  TRY(dev_copy(plan, (double**)&c.w_mid, d->wall_mid, (size_t)2 * d->n_walls));
+  TRY(put(plan, (int**)&c.w_cell, d->wall_cell, (size_t)d->n_walls, reload));
+  TRY(put(plan, (int**)&c.w_family, d->wall_family, (size_t)d->n_walls, reload));
+  TRY(put(plan, (int**)&c.w_face, d->wall_face, (size_t)d->n_walls, reload));
+  TRY(put(plan, (double**)&c.w_into, d->wall_into, (size_t)d->n_walls, reload));
+  TRY(put(plan, (double**)&c.w_mid, d->wall_mid, (size_t)2 * d->n_walls, reload));
   const int nc = d->n_chains, L = d->chain_L;
   if (L > MAX_CHAIN) return fail(JR_EINVAL, "line chains longer than 1024 cells are not supported");
   c.n_chains = nc;
@@ -175,13 +188,13 @@ static int build_case(jr_plan* plan, const jr_plan_desc* d, CaseDev& cd, size_t&
   for (int k = 0; k < N; ++k)
     if (!on_chain[k]) off.push_back(k);
   c.n_offchain = (int)off.size();
-  TRY(dev_copy(plan, (int**)&c.offchain, off.data(), off.size()));
-  TRY(dev_copy(plan, (int**)&c.ch_cells, d->chain_cells, (size_t)nc * L));
-  TRY(dev_copy(plan, (int**)&c.ch_len, d->chain_len, (size_t)nc));
-  TRY(dev_copy(plan, (int**)&c.ch_up_face, d->chain_up_face, (size_t)nc * L));
-  TRY(dev_copy(plan, (int**)&c.ch_up_sign, d->chain_up_sign, (size_t)nc * L));
-  TRY(dev_copy(plan, (int**)&c.ch_down_face, d->chain_down_face, (size_t)nc * L));
-  TRY(dev_copy(plan, (int**)&c.ch_down_sign, d->chain_down_sign, (size_t)nc * L));
+  TRY(put(plan, (int**)&c.offchain, off.data(), off.size(), reload));
+  TRY(put(plan, (int**)&c.ch_cells, d->chain_cells, (size_t)nc * L, reload));
+  TRY(put(plan, (int**)&c.ch_len, d->chain_len, (size_t)nc, reload));
+  TRY(put(plan, (int**)&c.ch_up_face, d->chain_up_face, (size_t)nc * L, reload));
+  TRY(put(plan, (int**)&c.ch_up_sign, d->chain_up_sign, (size_t)nc * L, reload));
+  TRY(put(plan, (int**)&c.ch_down_face, d->chain_down_face, (size_t)nc * L, reload));
+  TRY(put(plan, (int**)&c.ch_down_sign, d->chain_down_sign, (size_t)nc * L, reload));
   std::vector<int> fbase(nc);
   size_t fbase_total = 0;
   for (int k = 0; k < nc; ++k) {
@@ -189,7 +202,7 @@ static int build_case(jr_plan* plan, const jr_plan_desc* d, CaseDev& cd, size_t&
     fbase_total += (size_t)d->chain_len[k] + 16;
   }
   factor_rows = fbase_total;
-  TRY(dev_copy(plan, (int**)&c.ch_fbase, fbase.data(), (size_t)nc));
+  TRY(put(plan, (int**)&c.ch_fbase, fbase.data(), (size_t)nc, reload));
 
   Physics& P = cd.P;
   P.gamma = d->gamma;
@@ -252,7 +265,7 @@ static int build_case(jr_plan* plan, const jr_plan_desc* d, CaseDev& cd, size_t&
   cd.tiles_x = (int)tg.x;
   cd.tiles_y = (int)tg.y;
   cd.n_tiles = (int)(tg.x * tg.y);
-  cd.enabled = 1;
+  if (!reload) cd.enabled = 1;
   return JR_OK;
 }
 
@@ -449,6 +462,8 @@ int jr_batch_create(const jr_plan_desc* descs, int32_t n_cases, jr_plan** out) {
   std::vector<size_t> rows(n_cases);
   int rc = JR_OK;
   for (int k = 0; k < n_cases && rc == JR_OK; ++k) rc = build_case(plan, &descs[k], plan->host[k], rows[k]);
+  for (int k = 0; k < n_cases && rc == JR_OK; ++k)
+    plan->chain_len.emplace_back(descs[k].chain_len, descs[k].chain_len + descs[k].n_chains);
   if (rc == JR_OK) {
     plan->nvar = d0.nvar;
     plan->visc = plan->host[0].visc;
@@ -661,6 +676,43 @@ int jr_case_set_inflow(jr_plan* plan, int32_t c, const double* q_inf) {
   P.U_inf[2] = rho * v;
   P.U_inf[3] = p / (g - 1.0) + 0.5 * rho * (u * u + v * v);
   P.U_inf[4] = rho * P.q_inf[4];
+  return upload_table(plan);
+}
+
+int jr_case_load(jr_plan* plan, int32_t c, const jr_plan_desc* d) {
+  if (!plan || !d || c < 0 || c >= plan->n_cases) return fail(JR_EINVAL, "bad argument");
+  CaseDev& cd = plan->host[c];
+  const Canvas& cv = cd.c;
+  bool same = d->NI == cv.NI && d->NJ == cv.NJ && d->nvar == cv.nvar && d->n_ghost[0] == cv.n_ghost[0] &&
+              d->n_ghost[1] == cv.n_ghost[1] && d->n_walls == cv.n_walls && d->n_chains == cv.n_chains &&
+              d->chain_L == cv.L && (d->distance != nullptr) == (cv.distance != nullptr) &&
+              (d->mu_inf > 0.0) == (cd.visc > 0) && d->precision == (plan->mixed ? 1 : 0) &&
+              d->krylov_subspace == plan->m && d->krylov_restarts == plan->cfg.maxiter &&
+              d->preconditioner == plan->cfg.preconditioner;
+  for (int k = 0; same && k < d->n_chains; ++k) same = d->chain_len[k] == plan->chain_len[c][k];
+  if (same) {
+    const int N = d->NI * d->NJ;
+    std::vector<char> on(N, 0);
+    for (size_t k = 0; k < (size_t)d->n_chains * d->chain_L; ++k) {
+      const int cell = d->chain_cells[k];
+      if (cell >= N) return fail(JR_EINVAL, "a chain cell out of range");
+      if (cell >= 0) on[cell] = 1;
+    }
+    int off = 0;
+    for (int k = 0; k < N; ++k) off += on[k] == 0;
+    same = off == cv.n_offchain;
+  }
+  if (!same)
+    return fail(JR_EMISMATCH,
+                "jr_case_load: the new case's canvas, tables or solver settings differ from the slot's");
+  if (cudaStreamSynchronize(plan->st) != cudaSuccess) return cuda_check("jr_case_load");
+  size_t rows = 0;
+  int rc = build_case(plan, d, cd, rows, true);
+  if (rc != JR_OK) {
+    cd.enabled = 0;   // half overwritten: keep the slot out of every launch
+    upload_table(plan);
+    return rc;
+  }
   return upload_table(plan);
 }
 

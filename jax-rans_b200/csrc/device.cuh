@@ -141,6 +141,14 @@ __device__ __forceinline__ const CaseDev& stage_case(const CaseDev* cases, int c
   return *smem;
 }
 
+// True when a block has nothing to do for its case: a free slot, a block beyond the
+// case's extent (`beyond`), or a Krylov cycle that has stopped.  Read from the table in
+// global memory before the descriptor is staged, so the idle blocks of a batch whose
+// cases differ in size return at once.
+__device__ __forceinline__ bool idle_block(const CaseDev& g, bool beyond, int check_active) {
+  return !g.enabled || beyond || (check_active && g.sc->active == 0);
+}
+
 // Grid extents of a batch's launches: the largest of each per-case count.
 struct BatchDims {
   int n_cases;

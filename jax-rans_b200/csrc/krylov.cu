@@ -28,6 +28,41 @@ __device__ __forceinline__ double warp_max(double x) {
   return x;
 }
 
+// In the last block of a reduction: out[k] = the sum (or NaN-propagating max) over the
+// nb rows of partial[b * stride + k], k < W, by all the block's threads in a fixed order
+// -- thread (k, r) takes the rows b = r, r + R, ... (R = blockDim.x / W groups), with its
+// loads issued four at a time, then thread k adds the R group totals in order.  Loads go
+// to L2 (ld.global.cg), where the other blocks' partials are.
+template <bool MAX>
+__device__ void reduce_rows(const double* partial, int stride, int W, int nb, double* out) {
+  __shared__ double group[RED_THREADS];
+  const int R = max(1, (int)blockDim.x / W);
+  const int t = threadIdx.x, k = t % W, r = t / W;
+  if (r < R) {
+    double acc = MAX ? -INFINITY : 0.0;
+    int b = r;
+    for (; b + 3 * R < nb; b += 4 * R) {
+      const double x0 = __ldcg(partial + (size_t)b * stride + k);
+      const double x1 = __ldcg(partial + (size_t)(b + R) * stride + k);
+      const double x2 = __ldcg(partial + (size_t)(b + 2 * R) * stride + k);
+      const double x3 = __ldcg(partial + (size_t)(b + 3 * R) * stride + k);
+      acc = MAX ? nmax(nmax(nmax(nmax(acc, x0), x1), x2), x3) : (((acc + x0) + x1) + x2) + x3;
+    }
+    for (; b < nb; b += R) {
+      const double x = __ldcg(partial + (size_t)b * stride + k);
+      acc = MAX ? nmax(acc, x) : acc + x;
+    }
+    group[t] = acc;
+  }
+  __syncthreads();
+  if (t < W) {
+    double v = group[t];
+    for (int g = 1; g < R; ++g) v = MAX ? nmax(v, group[g * W + t]) : v + group[g * W + t];
+    out[t] = v;
+  }
+  __syncthreads();
+}
+
 // Block-sums `vals` into partial[block * W + k]; true in thread 0 of the last block to
 // finish, whose `vals` then hold the fixed-order totals over blocks.
 template <int W, bool MAX = false>
@@ -53,17 +88,42 @@ __device__ bool reduce_last(double (&vals)[W], double* partial, unsigned* ticket
     last = prev == (unsigned)nb - 1;
   }
   __syncthreads();
-  if (!last || threadIdx.x != 0) return false;
+  if (!last) return false;
   __threadfence();
+  __shared__ double total[W];
+  reduce_rows<MAX>(partial, W, W, nb, total);
+  if (threadIdx.x != 0) return false;
 #pragma unroll
-  for (int k = 0; k < W; ++k) {
-    const volatile double* p = partial;
-    double t = p[k];
-    for (int b = 1; b < nb; ++b) t = MAX ? nmax(t, p[b * W + k]) : t + p[b * W + k];
-    vals[k] = t;
-  }
+  for (int k = 0; k < W; ++k) vals[k] = total[k];
   *ticket = 0u;
   return true;
+}
+
+// The NK accumulators of every lane summed over the warp by a butterfly that halves the
+// values a lane holds at each of the five exchanges: at the end lane l holds the sums of
+// accumulators l*(NK/32) .. l*(NK/32) + NK/32 - 1 (NK >= 32), or of l / (32/NK) in
+// acc[0] (NK < 32).  The additions follow a fixed tree, so a rerun is bitwise the same.
+template <int NK>
+__device__ __forceinline__ void warp_transpose_sum(double (&acc)[NK], int lane) {
+  int held = NK;
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) {
+    if (held >= 2) {
+      const int half = held / 2;
+      const bool upper = (lane & o) != 0;
+#pragma unroll
+      for (int k = 0; k < NK / 2; ++k) {
+        if (k < half) {
+          const double send = upper ? acc[k] : acc[k + half];
+          const double keep = upper ? acc[k + half] : acc[k];
+          acc[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+      }
+      held = half;
+    } else {
+      acc[0] += __shfl_xor_sync(0xffffffffu, acc[0], o);
+    }
+  }
 }
 
 // The range of elements block b of nb owns
@@ -141,7 +201,7 @@ __global__ void k_cycle_start(const CaseDev* __restrict__ cases) {
 // thread owns MD_E elements and keeps NK accumulators in registers; all loads of a
 // pass are independent of one another.
 template <class TV, int NK, int MODE>
-__global__ void __launch_bounds__(RED_THREADS) k_mdot(const CaseDev* __restrict__ cases, int nk, int j) {
+__global__ void __launch_bounds__(RED_THREADS, 2) k_mdot(const CaseDev* __restrict__ cases, int nk, int j) {
   const CaseDev& cd = cases[blockIdx.y];
   if (!cd.enabled) return;
   Scalars* sc = cd.sc;
@@ -162,13 +222,16 @@ __global__ void __launch_bounds__(RED_THREADS) k_mdot(const CaseDev* __restrict_
   double acc[NA];
 #pragma unroll
   for (int k = 0; k < NA; ++k) acc[k] = 0.0;
-  double h[MODE == 0 ? 1 : NK];
+  // the coefficients of the update, shared by the block (broadcast reads)
+  __shared__ double h[MODE == 0 ? 1 : NK];
   if constexpr (MODE != 0) {
-#pragma unroll
-    for (int k = 0; k < NK; ++k) h[k] = k < nk ? hin[k] : 0.0;
+    if ((int)threadIdx.x < NK) h[threadIdx.x] = (int)threadIdx.x < nk ? hin[threadIdx.x] : 0.0;
+    __syncthreads();
   }
   const int base = blockIdx.x * blockDim.x * MD_E + threadIdx.x;
-#pragma unroll
+  // one element at a time: its NK loads are independent of one another, and the
+  // registers stay within two blocks per SM
+#pragma unroll 1
   for (int t = 0; t < MD_E; ++t) {
     const int i = base + t * blockDim.x;
     if (i < n) {
@@ -192,11 +255,17 @@ __global__ void __launch_bounds__(RED_THREADS) k_mdot(const CaseDev* __restrict_
   }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int width = MODE == 2 ? 1 : nk;
+  if constexpr (MODE == 2) {
+    double x = warp_sum(acc[0]);
+    if (lane == 0) sm[warp][0] = x;
+  } else {
+    // all NK sums of the warp at once: about NK shuffles instead of 5 NK
+    warp_transpose_sum<NK>(acc, lane);
+    constexpr int HOLD = NK >= 32 ? NK / 32 : 1;      // sums a lane ends with
+    constexpr int SHARE = NK >= 32 ? 1 : 32 / NK;     // lanes holding the same sum
+    if (lane % SHARE == 0) {
 #pragma unroll
-  for (int k = 0; k < NA; ++k) {
-    if (k < width) {
-      double x = warp_sum(acc[k]);
-      if (lane == 0) sm[warp][k] = x;
+      for (int r = 0; r < HOLD; ++r) sm[warp][(lane / SHARE) * HOLD + r] = acc[r];
     }
   }
   __syncthreads();
@@ -211,10 +280,10 @@ __global__ void __launch_bounds__(RED_THREADS) k_mdot(const CaseDev* __restrict_
   __syncthreads();
   if (!last) return;
   __threadfence();
+  __shared__ double total[MAX_KRYLOV + 1];
+  reduce_rows<false>(partial, MAX_KRYLOV + 1, width, nb, total);
   if ((int)threadIdx.x < width) {
-    const volatile double* p = partial;
-    double t = 0.0;
-    for (int b = 0; b < nb; ++b) t += p[b * (MAX_KRYLOV + 1) + threadIdx.x];
+    const double t = total[threadIdx.x];
     if constexpr (MODE == 2) {
       double nrm = sqrt(t);
       for (int k = 0; k < nk; ++k) sc->H[k + (m + 1) * j] = sc->h1[k] + sc->h2[k];

@@ -159,6 +159,7 @@ __device__ __forceinline__ int level_rows(int L, int level) {
 template <class TF, bool SA>
 __global__ void __launch_bounds__(LS_THREADS) k_cr_factor(const CaseDev* __restrict__ cases) {
   __shared__ CaseDev scase;
+  if (idle_block(cases[blockIdx.y], (int)blockIdx.x >= cases[blockIdx.y].c.n_chains, 0)) return;
   const CaseDev& cd = stage_case(cases, blockIdx.y, &scase);
   if (!cd.enabled || (int)blockIdx.x >= cd.c.n_chains) return;
   const Canvas& cv = cd.c;
@@ -336,6 +337,11 @@ template <class TF, class TV, bool SA>
 __global__ void __launch_bounds__(LS_THREADS) k_cr_apply(const CaseDev* __restrict__ cases, int src_id, int scale_on,
                                                          int vout_j, int out_id, int check_active) {
   __shared__ CaseDev scase;
+  {
+    const Canvas& g = cases[blockIdx.y].c;
+    if (idle_block(cases[blockIdx.y], (int)blockIdx.x >= g.n_chains + offchain_blocks(g.n_offchain), check_active))
+      return;
+  }
   const CaseDev& cd = stage_case(cases, blockIdx.y, &scase);
   if (!cd.enabled || (check_active && cd.sc->active == 0)) return;
   const Canvas& cv = cd.c;

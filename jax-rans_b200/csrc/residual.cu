@@ -159,6 +159,11 @@ template <class T>
 __global__ void __launch_bounds__(GHOST_THREADS) k_ghosts(const CaseDev* __restrict__ cases, int tangent_id,
                                                           int check_active) {
   __shared__ CaseDev scase;
+  {
+    const Canvas& g = cases[blockIdx.y].c;
+    if (idle_block(cases[blockIdx.y], (int)(blockIdx.x * blockDim.x) >= g.n_ghost[0] + g.n_ghost[1], check_active))
+      return;
+  }
   const CaseDev& cd = stage_case(cases, blockIdx.y, &scase);
   if (!cd.enabled || (check_active && cd.sc->active == 0)) return;
   const Canvas& c = cd.c;
@@ -431,6 +436,10 @@ __global__ void __launch_bounds__(TILE_THREADS, TILE_MIN_BLOCKS)
     k_residual(const CaseDev* __restrict__ cases, int out_id, int tangent_id, int vdt_id, int with_partial,
                int check_active) {
   __shared__ CaseDev scase;
+  if (idle_block(cases[blockIdx.z],
+                 (int)blockIdx.x >= cases[blockIdx.z].tiles_x || (int)blockIdx.y >= cases[blockIdx.z].tiles_y,
+                 check_active))
+    return;
   const CaseDev& cd = stage_case(cases, blockIdx.z, &scase);
   if (!cd.enabled || (check_active && cd.sc->active == 0)) return;
   if ((int)blockIdx.x >= cd.tiles_x || (int)blockIdx.y >= cd.tiles_y) return;
@@ -580,6 +589,11 @@ __device__ __forceinline__ void prim_raw(const Canvas& c, const Physics& P, cons
 template <int VISC>
 __global__ void k_faces(const CaseDev* __restrict__ cases) {
   __shared__ CaseDev scase;
+  {
+    const Canvas& g = cases[blockIdx.y].c;
+    const int nf = (g.NI + 1) * g.NJ + g.NI * (g.NJ + 1);
+    if (idle_block(cases[blockIdx.y], (int)(blockIdx.x * blockDim.x) >= nf, 0)) return;
+  }
   const CaseDev& cd = stage_case(cases, blockIdx.y, &scase);
   if (!cd.enabled) return;
   const Canvas& c = cd.c;
@@ -639,6 +653,10 @@ __global__ void k_faces(const CaseDev* __restrict__ cases) {
 template <int VISC>
 __global__ void k_cells(const CaseDev* __restrict__ cases) {
   __shared__ CaseDev scase;
+  {
+    const Canvas& g = cases[blockIdx.y].c;
+    if (idle_block(cases[blockIdx.y], (int)(blockIdx.x * blockDim.x) >= g.NI * g.NJ, 0)) return;
+  }
   const CaseDev& cd = stage_case(cases, blockIdx.y, &scase);
   if (!cd.enabled) return;
   const Canvas& c = cd.c;

@@ -61,7 +61,7 @@ EXPORTS = ("jr_plan_create", "jr_plan_destroy", "jr_last_error", "jr_plan_sizes"
            "jr_state_set", "jr_state_get", "jr_state_device", "jr_newton_steps", "jr_newton_steps_async",
            "jr_forces", "jr_state_set_device", "jr_graph_kernels", "jr_time_kernels", "jr_plan_set_stream",
            "jr_batch_create", "jr_plan_cases", "jr_case_sizes", "jr_case_enable", "jr_case_set_inflow",
-           "jr_case_state_set", "jr_case_state_get", "jr_residual_noalloc")
+           "jr_case_state_set", "jr_case_state_get", "jr_residual_noalloc", "jr_case_load")
 
 TIMED_KERNELS = ("residual_tile", "jvp_tile", "ghosts_tangent", "line_apply", "line_factor", "cgs2_full_basis")
 
@@ -111,6 +111,7 @@ def load_library(path: Path | None = None) -> C.CDLL:
         "jr_case_sizes": (C.c_int, [vp, C.c_int32] + [C.POINTER(C.c_int64)] * 4),
         "jr_case_enable": (C.c_int, [vp, C.c_int32, C.c_int32]),
         "jr_case_set_inflow": (C.c_int, [vp, C.c_int32, _f64p]),
+        "jr_case_load": (C.c_int, [vp, C.c_int32, C.POINTER(PlanDesc)]),
         "jr_case_state_set": (C.c_int, [vp, C.c_int32, vp, C.c_double, C.c_double]),
         "jr_case_state_get": (C.c_int, [vp, C.c_int32, vp, _f64p, _f64p, _i32p]),
     }
@@ -382,6 +383,19 @@ class DevicePlan:
 
     def enable(self, k: int, enabled: bool = True) -> None:
         _check(self.lib, self.lib.jr_case_enable(self.handle, int(k), int(bool(enabled))), "jr_case_enable")
+
+    def load_case(self, k: int, plan: Plan, flow: FlowConditions, numerics: NumericsConfig,
+                  implicit: ImplicitConfig | None = None, force_length: float = 1.0,
+                  moment_centre=(0.25, 0.0)) -> None:
+        """Slot k takes a new case of the same shape (grid size and topology); its state
+        is set afterwards (``set_case_state``)."""
+        keep: list = []
+        d = PlanDesc()
+        fill_desc(d, plan, flow, numerics, implicit or self.implicit, force_length, moment_centre, keep)
+        _check(self.lib, self.lib.jr_case_load(self.handle, int(k), C.byref(d)), "jr_case_load")
+        self.plans[k], self.flows[k] = plan, flow
+        if k == 0:
+            self.plan, self.flow = plan, flow
 
     def set_inflow(self, k: int, q_inf) -> None:
         """Case k's freestream primitives (rho, u, v, p[, nu_hat])."""

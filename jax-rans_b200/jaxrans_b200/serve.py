@@ -1,0 +1,298 @@
+"""Serving: a request loop with continuous batching.
+
+Requests (2D cases, each with its own section, grid size and flow) arrive over time.
+A pool per grid size holds a device batch of slots (``jr_batch_create``); its slot count
+is set by the free device memory when the pool is first needed.  A request is admitted
+as soon as it has arrived and a slot of its grid size is free: the slot's static tables
+are overwritten with the request's grid (``jr_case_load``), its state reset to the
+request's freestream, and it joins the next block of Newton steps.  Every pool steps all
+its live slots with one captured graph per Newton step, on its own stream, so the pools'
+work overlaps on the device.  After each block the host runs each live request's exit
+test (``jaxrans_b200.solver.CaseMonitor``, the exit test of a single run); a finished
+request frees its slot at once.  States and preconditioner factors stay resident on the
+device for the whole life of a request.
+
+A request's result is the same as the same case run alone: slots never interact, and
+each slot's reductions are split as for a single case.
+"""
+
+from __future__ import annotations
+
+import copy
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .case import Case
+from .plan import Plan
+from .solver import CaseMonitor, ConvergenceHistory, Forces, freestream_state
+
+# C-grid sizes (nodes) of the served requests: cells round the airfoil, along each wake
+# side, normal to the wall
+GRID_CLASSES = {
+    (193, 49): (128, 32, 48),
+    (385, 97): (256, 64, 96),
+    (513, 129): (344, 84, 128),
+    (769, 193): (512, 128, 192),
+}
+
+
+@dataclass
+class Request:
+    """A case and its arrival time (seconds from the start of the stream)."""
+
+    id: int
+    case: Case
+    arrival: float
+    grid_key: tuple = ()
+
+
+@dataclass
+class Served:
+    """A finished request: its exit, forces, history, and its times on the server."""
+
+    request: Request
+    reason: str
+    forces: Forces
+    history: ConvergenceHistory
+    U: np.ndarray
+    admitted: float
+    finished: float
+
+    @property
+    def latency(self) -> float:
+        """Seconds from arrival to result."""
+        return self.finished - self.request.arrival
+
+
+def request_case(template: Case, airfoil: str, size: tuple, mach: float, alpha: float, reynolds: float,
+                 name: str, classes: dict = GRID_CLASSES) -> Case:
+    """``template`` (its numerics, model and boundary conditions) on a C-grid of ``size``
+    nodes round ``airfoil`` at the given flow."""
+    from .case import parse_case
+    around, wake, normal = classes[size]
+    doc = copy.deepcopy(template.raw["case"])
+    num = copy.deepcopy(template.raw["numerical"])
+    doc["general"] = {"case_name": name}
+    doc["domain"] = dict(doc["domain"], airfoil=airfoil, cells_airfoil=around, cells_wake=wake,
+                         cells_normal=normal)
+    doc["freestream"] = dict(doc["freestream"], mach=float(mach), alpha_deg=float(alpha), reynolds=float(reynolds))
+    return parse_case(doc, num)
+
+
+def poisson_requests(n: int, template: Case, rate: float = 20.0, seed: int = 0,
+                     classes: dict = GRID_CLASSES) -> list[Request]:
+    """``n`` requests with Poisson arrivals of mean ``rate`` per second: NACA 4-digit
+    sections of max camber 0-6 %, camber position 20-50 %, thickness 6-24 %, a C-grid
+    size from ``sizes``, M uniform on [0.15, 0.78], alpha uniform on [-5, 15] deg, Re
+    log-uniform on [1e6, 2e7]; all from ``seed``."""
+    rng = np.random.default_rng(seed)
+    sizes = tuple(classes)
+    t = 0.0
+    out = []
+    for i in range(n):
+        t += rng.exponential(1.0 / rate)
+        camber = int(rng.integers(0, 7))
+        position = int(rng.integers(2, 6)) if camber else 0
+        thickness = int(rng.integers(6, 25))
+        airfoil = f"naca{camber}{position}{thickness:02d}"
+        size = sizes[int(rng.integers(0, len(sizes)))]
+        mach = float(rng.uniform(0.15, 0.78))
+        alpha = float(rng.uniform(-5.0, 15.0))
+        reynolds = float(10.0 ** rng.uniform(6.0, np.log10(2e7)))
+        case = request_case(template, airfoil, size, mach, alpha, reynolds, f"req{i:04d}", classes)
+        out.append(Request(i, case, t, size))
+    return out
+
+
+def case_bytes(plan: Plan, nvar: int, m: int, mixed: bool) -> int:
+    """Device bytes one slot of this grid takes (work vectors, basis, line factor)."""
+    n_vec = nvar * plan.NI * plan.NJ
+    tb = 4 if mixed else 8
+    rows = int(plan.chains.lengths.sum()) + 16 * plan.chains.cells.shape[0]
+    return 11 * n_vec * 8 + (m + 1) * n_vec * tb + rows * (80 + 5 + 104) * tb + 32 * plan.NI * plan.NJ * 8
+
+
+@dataclass
+class Pool:
+    """The slots of one grid size: a device batch and who holds each slot."""
+
+    key: tuple
+    dev: object
+    slots: int
+    holder: list = field(default_factory=list)     # Request or None per slot
+    monitor: list = field(default_factory=list)    # CaseMonitor or None per slot
+    admitted: list = field(default_factory=list)
+
+    def free_slot(self):
+        for k, h in enumerate(self.holder):
+            if h is None:
+                return k
+        return None
+
+    @property
+    def live(self) -> bool:
+        return any(h is not None for h in self.holder)
+
+
+def build_grid(case: Case) -> Plan:
+    """A request's grid and plan tables (run in a worker process)."""
+    return case.grid()
+
+
+class Server:
+    """Continuous batching of requests over pools of device slots, one pool per grid size.
+
+    ``max_slots`` caps a pool; ``memory_fraction`` of the free device memory, shared by
+    the grid sizes still without a pool, bounds it when the pool is made.  Each request's
+    grid is generated on the host by a pool of ``workers`` processes from the moment it
+    arrives, while the device steps the admitted ones."""
+
+    def __init__(self, max_slots: int = 64, memory_fraction: float = 0.8, block_iters: int | None = None,
+                 n_classes: int = len(GRID_CLASSES), workers: int = 4):
+        self.max_slots, self.memory_fraction = max_slots, memory_fraction
+        self.n_classes, self.workers = n_classes, workers
+        self.block_iters = block_iters
+        self.pools: dict = {}
+
+    def pool_for(self, req: Request, plan: Plan) -> Pool:
+        if req.grid_key in self.pools:
+            return self.pools[req.grid_key]
+        import torch
+        from .batch import batch_device
+        imp = req.case.implicit
+        per = case_bytes(plan, req.case.flow.nvar, imp.krylov_subspace, imp.precision == "mixed")
+        free, _ = torch.cuda.mem_get_info()
+        left = max(1, self.n_classes - len(self.pools))
+        slots = int(max(1, min(self.max_slots, self.memory_fraction * free / left // per)))
+        dev = batch_device([req.case] * slots, [plan] * slots)
+        for k in range(slots):
+            dev.enable(k, False)
+        pool = Pool(req.grid_key, dev, slots, [None] * slots, [None] * slots, [0.0] * slots)
+        self.pools[req.grid_key] = pool
+        return pool
+
+    def admit(self, pool: Pool, slot: int, req: Request, plan: Plan, now: float) -> None:
+        c = req.case
+        pool.dev.load_case(slot, plan, c.flow, c.numerics, c.implicit, c.grid_spec.reference_length,
+                           tuple(c.grid_spec.moment_centre[:2]))
+        pool.dev.set_case_state(slot, freestream_state(c, plan), c.implicit.cfl, float("inf"))
+        pool.dev.enable(slot, True)
+        pool.holder[slot] = req
+        pool.monitor[slot] = CaseMonitor(c)
+        pool.admitted[slot] = now
+
+    def serve(self, requests: list[Request], realtime: bool = True) -> list[Served]:
+        """Run the stream to its end; ``realtime`` releases each request at its arrival on
+        the wall clock, otherwise every request is there at the start."""
+        import multiprocessing
+        from concurrent.futures import ProcessPoolExecutor
+        with ProcessPoolExecutor(self.workers, mp_context=multiprocessing.get_context("spawn")) as workers:
+            return self._serve(requests, realtime, workers)
+
+    def _serve(self, requests, realtime, workers) -> list[Served]:
+        import torch
+        block = self.block_iters or requests[0].case.block_iters
+        pending = deque(sorted(requests, key=lambda r: r.arrival))
+        grids: dict = {}
+        done: list[Served] = []
+        hist_buf: dict = {}
+        t0 = time.perf_counter()
+
+        def clock():
+            return time.perf_counter() - t0
+
+        while pending or any(p.live for p in self.pools.values()):
+            t = clock() if realtime else float("inf")
+            for req in pending:
+                if req.arrival > t:
+                    break
+                if req.id not in grids:
+                    grids[req.id] = workers.submit(build_grid, req.case)
+            # admit, in arrival order, every arrived request whose grid is ready and that
+            # has a free slot of its size
+            for req in [r for r in pending if r.id in grids and grids[r.id].done()]:
+                plan = grids[req.id].result()
+                pool = self.pool_for(req, plan)
+                slot = pool.free_slot()
+                if slot is None:
+                    continue
+                self.admit(pool, slot, req, plan, clock())
+                pending.remove(req)
+                del grids[req.id]
+            live = [p for p in self.pools.values() if p.live]
+            if not live:
+                time.sleep(0.01)
+                continue
+            # one block of every live pool, each on its own stream: the pools overlap
+            for p in live:
+                buf = hist_buf.get(p.key)
+                if buf is None:
+                    buf = hist_buf[p.key] = torch.empty((block, p.slots), dtype=torch.float64, device="cuda")
+                p.dev.newton_steps_async(block, buf)
+            for p in live:
+                p.dev.sync()
+                hist = hist_buf[p.key].cpu().numpy()
+                forces = np.atleast_2d(p.dev.forces())
+                finished_at = clock()
+                for k, req in enumerate(p.holder):
+                    if req is None:
+                        continue
+                    mon = p.monitor[k]
+                    if mon.feed(hist[:, k], forces[k]):
+                        U = p.dev.case_state(k)[0]
+                        res = mon.residual()
+                        history = ConvergenceHistory(res, mon.reason, int(res.size))
+                        done.append(Served(req, mon.reason, mon.forces, history, U, p.admitted[k], finished_at))
+                        p.dev.enable(k, False)
+                        p.holder[k] = None
+                        p.monitor[k] = None
+        return sorted(done, key=lambda s: s.request.id)
+
+    def close(self) -> None:
+        for p in self.pools.values():
+            p.dev.close()
+        self.pools.clear()
+
+
+def summary(served: list[Served], wall: float) -> dict:
+    lat = np.array([s.latency for s in served])
+    return {"requests": len(served), "solves_per_hr": 3600.0 * len(served) / wall,
+            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "exits": {r: int(sum(s.reason == r for s in served)) for r in sorted({s.reason for s in served})}}
+
+
+def main(argv=None) -> int:
+    """Serve a seeded Poisson stream of SA requests and print a JSON summary."""
+    import argparse
+    import json
+    from .workloads import workload
+    ap = argparse.ArgumentParser(prog="python -m jaxrans_b200.serve", description=main.__doc__)
+    ap.add_argument("--requests", type=int, default=64)
+    ap.add_argument("--rate", type=float, default=20.0)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--precision", default="mixed", choices=("fp64", "mixed"))
+    ap.add_argument("--max-slots", type=int, default=64)
+    ap.add_argument("--workers", type=int, default=8)
+    args = ap.parse_args(argv)
+    template = workload("c_sa_385", **{"implicit.precision": args.precision})
+    requests = poisson_requests(args.requests, template, args.rate, args.seed)
+    server = Server(max_slots=args.max_slots, workers=args.workers)
+    t = time.perf_counter()
+    served = server.serve(requests)
+    wall = time.perf_counter() - t
+    out = summary(served, wall)
+    out.update({"rate_per_s": args.rate, "seed": args.seed, "precision": args.precision, "wall_s": wall,
+                "slots": {f"{k[0]}x{k[1]}": p.slots for k, p in server.pools.items()},
+                "per_class": {f"{k[0]}x{k[1]}": summary([x for x in served if x.request.grid_key == k], wall)
+                              for k in server.pools}})
+    print(json.dumps(out), flush=True)
+    server.close()
+    return 0
+
+
+if __name__ == "__main__":
+    import sys
+    sys.exit(main())

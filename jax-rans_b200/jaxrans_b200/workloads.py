@@ -26,7 +26,8 @@ on a GPU box and in the oracle.
   cells round the airfoil and a sixth along each wake side, the numerics of
   ``c_sa_385``.
 * batch ``polar64_uneven`` -- 64 angles uniform on [-4, 16] deg on the ``c_sa_385``
-  grid together with the three uneven cases, all in one device batch.
+  grid together with the three uneven cases, all in one device batch; ``polar8_769``,
+  8 angles with the 769 x 193 case, is the same mix small enough to profile.
 """
 
 from __future__ import annotations
@@ -79,6 +80,8 @@ BATCHES = {
     "polar64_uneven": [("c_sa_385", float(a)) for a in
                        [-4.0 + 20.0 * k / 63 for k in range(64)]] + [("c_sa_257", None), ("c_sa_513", None),
                                                                       ("c_sa_769", None)],
+    # a small batch of the same kinds, for profiling captures (about 1.5 GB on the device)
+    "polar8_769": [("c_sa_385", float(a)) for a in [-4.0 + 20.0 * k / 7 for k in range(8)]] + [("c_sa_769", None)],
 }
 
 
