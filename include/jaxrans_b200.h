@@ -164,8 +164,13 @@ int jr_case_state_get(jr_plan* plan, int32_t c, double* U_host, double* cfl, dou
 double* jr_state_device(jr_plan* plan);
 /* The state from a device buffer (a restart with the inputs already in HBM). */
 int jr_state_set_device(jr_plan* plan, const double* U_device, double cfl, double residual_norm);
-/* Kernels launched by one captured Newton step (the graph's kernel nodes). */
+/* Kernels one captured Newton step launches when every Krylov cycle runs (each cycle is a
+ * conditional node of the graph, skipped on the device once no case needs it). */
 int jr_graph_kernels(jr_plan* plan, int64_t* kernels_per_step);
+/* Kernels the Newton steps of this plan have launched so far, the skipped cycles not
+ * counted (the device counts the cycles it ran).  Synchronises.  Instrumentation with no
+ * counterpart in the reference. */
+int jr_launch_count(jr_plan* plan, int64_t* kernels);
 /* Average device time (ms, CUDA events on the plan's stream, reps launches each, after one
  * untimed launch) of the hot kernels at the plan's state, out[0..5]: the residual tile, the
  * J.v tile, the tangent ghost fill, the line-solve apply, the line factor, and one CGS2

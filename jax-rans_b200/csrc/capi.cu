@@ -28,6 +28,8 @@ void configure_line_kernels(int max_L);
 // krylov.cu
 void launch_gmres_init(const CaseDev*, const BatchDims&, cudaStream_t);
 void launch_cycle_start(const CaseDev*, const BatchDims&, cudaStream_t);
+void launch_cycle_gate(const CaseDev*, const BatchDims&, cudaGraphConditionalHandle, unsigned long long*,
+                       cudaStream_t);
 void launch_arnoldi_orth(const CaseDev*, const BatchDims&, bool fp32, int j, cudaStream_t);
 void launch_lstsq(const CaseDev*, const BatchDims&, cudaStream_t);
 void launch_combine(const CaseDev*, const BatchDims&, bool fp32, cudaStream_t);
@@ -67,6 +69,21 @@ struct jr_plan {
   Scalars* sc = nullptr;                 // one per case
   cudaGraphExec_t graph = nullptr;
   int device = 0;                        // the device current when the plan was made
+  // the step graph runs over the enabled cases only: their descriptors packed in slot
+  // order (`live`) and the launch extents over them; rebuilt, with the graph, whenever
+  // a case is enabled, disabled or changed
+  CaseDev* live = nullptr;
+  BatchDims live_dims{};
+  cudaStream_t body_st = nullptr;        // captures the bodies of the conditional cycles
+  unsigned long long* cycles = nullptr;  // Krylov cycle bodies run (device counter)
+  int64_t steps_run = 0;                 // Newton steps launched
+  int64_t kernels_outside = 0;           // kernels of a step outside the cycle bodies
+  int64_t kernels_per_cycle = 0;         // kernels of one cycle body
+  int64_t launched = 0;                  // kernels launched by steps of earlier graphs
+  int64_t steps_since = 0;               // steps of the current graph
+  unsigned long long cycles_base = 0;    // the cycle counter when the current graph was made
+  int n_live = 0;
+  bool live_dirty = true;
   std::vector<std::vector<int>> chain_len;   // each case's chain lengths (host copy)
 };
 
@@ -338,21 +355,26 @@ static int build_buffers(jr_plan* p, const std::vector<size_t>& factor_rows) {
     cd.fsa = (char*)fsa + fb_off[k] * 5 * tb;
     cd.scratch = (char*)scratch + fb_off[k] * 104 * tb;
     cd.sc = p->sc + k;
+    cd.slot = k;
     cd.history = p->history;
     cd.force_out = p->force_out + 8 * k;
   }
   TRY(dev_alloc(p, (void**)&p->cases, (size_t)nc * sizeof(CaseDev)));
   TRY(dev_alloc(p, (void**)&p->adhoc, (size_t)nc * sizeof(CaseDev)));
+  TRY(dev_alloc(p, (void**)&p->live, (size_t)nc * sizeof(CaseDev)));
+  TRY(dev_alloc(p, (void**)&p->cycles, sizeof(unsigned long long)));
+  if (cudaStreamCreateWithFlags(&p->body_st, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(JR_ECUDA, "cudaStreamCreate failed");
   if (cudaMemcpy(p->cases, p->host.data(), (size_t)nc * sizeof(CaseDev), cudaMemcpyHostToDevice) != cudaSuccess)
     return cuda_check("case table");
   return JR_OK;
 }
 
-static void compute_dims(jr_plan* p) {
-  BatchDims& d = p->dims;
-  d = BatchDims{};
-  d.n_cases = p->n_cases;
-  for (const CaseDev& cd : p->host) {
+static BatchDims dims_of(const std::vector<CaseDev>& cases, int n_slots) {
+  BatchDims d{};
+  d.n_cases = (int)cases.size();
+  d.n_slots = n_slots;
+  for (const CaseDev& cd : cases) {
     const Canvas& c = cd.c;
     d.tiles_x = std::max(d.tiles_x, cd.tiles_x);
     d.tiles_y = std::max(d.tiles_y, cd.tiles_y);
@@ -362,9 +384,13 @@ static void compute_dims(jr_plan* p) {
     d.n_vec = std::max(d.n_vec, cd.n_vec);
     d.chain_blocks = std::max(d.chain_blocks, chain_grid_blocks(c.n_chains, c.n_offchain));
     d.max_L = std::max(d.max_L, c.L);
+    d.cgs_blocks = std::max(d.cgs_blocks, cgs_blocks(cd.n_vec));
   }
   d.chain_blocks = std::max(d.chain_blocks, 1);
+  return d;
 }
+
+static void compute_dims(jr_plan* p) { p->dims = dims_of(p->host, p->n_cases); }
 
 // The table of a call on caller buffers: the resident table with the named buffers of
 // every case moved to its part of the caller's batch-long arrays.
@@ -386,15 +412,49 @@ struct Adhoc {
 };
 
 static int upload_table(jr_plan* p) {
+  p->live_dirty = true;
   cudaMemcpyAsync(p->cases, p->host.data(), p->host.size() * sizeof(CaseDev), cudaMemcpyHostToDevice, p->st);
   if (cudaStreamSynchronize(p->st) != cudaSuccess) return cuda_check("case table");
   return cuda_check("case table");
 }
 
-// The launch sequence of one Newton step of every case (captured as a graph).
-static void enqueue_step(jr_plan* p) {
-  const CaseDev* t = p->cases;
-  const BatchDims& d = p->dims;
+// The kernels of one Krylov cycle after its start: m Arnoldi steps, the least squares,
+// the correction and the end-of-cycle residual.
+static void enqueue_cycle(jr_plan* p, cudaStream_t st) {
+  const CaseDev* t = p->live;
+  const BatchDims& d = p->live_dims;
+  const bool sa = p->nvar == 5, pre = p->cfg.preconditioner == 1;
+  for (int j = 0; j < p->m; ++j) {
+    const int src = j == 0 ? B_RR : B_W;
+    if (pre) launch_chain_apply(t, d, sa, p->mixed, src, 1, j, B_Z, 1, st);
+    else launch_scale_copy(t, d, p->mixed, src, 1, j, B_Z, 1, st);
+    launch_ghosts(t, d, B_Z, 1, st);
+    launch_jvp(t, d, p->visc, B_Z, B_VDT, B_W, 1, st);
+    launch_arnoldi_orth(t, d, p->mixed, j, st);
+  }
+  launch_lstsq(t, d, st);
+  launch_combine(t, d, p->mixed, st);
+  if (pre) launch_chain_apply(t, d, sa, p->mixed, B_TMP, 0, -1, B_Z, 1, st);
+  else launch_scale_copy(t, d, false, B_TMP, 0, -1, B_Z, 1, st);
+  launch_cycle_end(t, d, st);
+}
+
+// Nodes of a captured graph: every node the step captures is a kernel, but for the
+// conditional nodes of the cycles (whose type this runtime does not report back).
+static int64_t graph_nodes(cudaGraph_t g) {
+  size_t n = 0;
+  cudaGraphGetNodes(g, nullptr, &n);
+  return (int64_t)n;
+}
+
+// The launch sequence of one Newton step of every enabled case, captured on the plan's
+// stream.  Each Krylov cycle is an IF node of the graph: a gate kernel after the cycle's
+// start sets its condition to "some case is still active", so a cycle no case needs is
+// skipped on the device without launching its kernels.
+static int enqueue_step(jr_plan* p) {
+  const CaseDev* t = p->live;
+  const BatchDims& d = p->live_dims;
+  if (d.n_cases == 0) return JR_OK;   // no enabled case: an empty step
   const bool sa = p->nvar == 5, pre = p->cfg.preconditioner == 1;
   cudaStream_t st = p->st;
   launch_ghosts(t, d, -1, 0, st);
@@ -405,21 +465,38 @@ static void enqueue_step(jr_plan* p) {
   if (pre) launch_chain_factor(t, d, sa, p->mixed, st);
   for (int cyc = 0; cyc < p->cfg.maxiter; ++cyc) {
     launch_cycle_start(t, d, st);
-    for (int j = 0; j < p->m; ++j) {
-      const int src = j == 0 ? B_RR : B_W;
-      if (pre) launch_chain_apply(t, d, sa, p->mixed, src, 1, j, B_Z, 1, st);
-      else launch_scale_copy(t, d, p->mixed, src, 1, j, B_Z, 1, st);
-      launch_ghosts(t, d, B_Z, 1, st);
-      launch_jvp(t, d, p->visc, B_Z, B_VDT, B_W, 1, st);
-      launch_arnoldi_orth(t, d, p->mixed, j, st);
-    }
-    launch_lstsq(t, d, st);
-    launch_combine(t, d, p->mixed, st);
-    if (pre) launch_chain_apply(t, d, sa, p->mixed, B_TMP, 0, -1, B_Z, 1, st);
-    else launch_scale_copy(t, d, false, B_TMP, 0, -1, B_Z, 1, st);
-    launch_cycle_end(t, d, st);
+    cudaStreamCaptureStatus status;
+    cudaGraph_t graph;
+    const cudaGraphNode_t* deps;
+    size_t n_deps;
+    if (cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &n_deps) != cudaSuccess ||
+        status != cudaStreamCaptureStatusActive)
+      return fail(JR_ECUDA, "the step is not being captured");
+    cudaGraphConditionalHandle gate;
+    if (cudaGraphConditionalHandleCreate(&gate, graph, 0, 0) != cudaSuccess) return cuda_check("conditional handle");
+    launch_cycle_gate(t, d, gate, p->cycles, st);
+    if (cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &n_deps) != cudaSuccess)
+      return cuda_check("capture info");
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = gate;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (cudaGraphAddNode(&node, graph, deps, n_deps, &cp) != cudaSuccess) return cuda_check("conditional node");
+    if (cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies) != cudaSuccess)
+      return cuda_check("capture dependencies");
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    if (cudaStreamBeginCaptureToGraph(p->body_st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+        cudaSuccess)
+      return cuda_check("body capture");
+    enqueue_cycle(p, p->body_st);
+    cudaGraph_t body_out;
+    if (cudaStreamEndCapture(p->body_st, &body_out) != cudaSuccess) return cuda_check("body capture end");
+    if (cyc == 0) p->kernels_per_cycle = graph_nodes(body);
   }
   launch_newton_update(t, d, st);
+  return JR_OK;
 }
 
 extern "C" {
@@ -432,6 +509,7 @@ int jr_plan_destroy(jr_plan* plan) {
   if (plan->st) cudaStreamSynchronize(plan->st);
   for (void* a : plan->allocs) cudaFree(a);
   if (plan->owned_stream) cudaStreamDestroy(plan->owned_stream);
+  if (plan->body_st) cudaStreamDestroy(plan->body_st);
   delete plan;
   return JR_OK;
 }
@@ -716,35 +794,83 @@ int jr_case_load(jr_plan* plan, int32_t c, const jr_plan_desc* d) {
   return upload_table(plan);
 }
 
+// The packed table of the enabled cases (slot order) and its extents; the step graph
+// is dropped so that the next launch captures one over them.
+static int refresh_live(jr_plan* p) {
+  if (!p->live_dirty) return JR_OK;
+  std::vector<CaseDev> on;
+  for (const CaseDev& cd : p->host)
+    if (cd.enabled) on.push_back(cd);
+  p->n_live = (int)on.size();
+  p->live_dims = dims_of(on, p->n_cases);
+  if (!on.empty()) {
+    cudaMemcpyAsync(p->live, on.data(), on.size() * sizeof(CaseDev), cudaMemcpyHostToDevice, p->st);
+    if (cudaStreamSynchronize(p->st) != cudaSuccess) return cuda_check("live table");
+  }
+  if (p->graph) {
+    cudaGraphExecDestroy(p->graph);
+    p->graph = nullptr;
+  }
+  p->live_dirty = false;
+  return cuda_check("live table");
+}
+
 static int capture_step(jr_plan* plan, cudaGraph_t* g) {
+  int rc = refresh_live(plan);
+  if (rc) return rc;
   if (cudaStreamBeginCapture(plan->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
     return cuda_check("begin capture");
-  enqueue_step(plan);
-  if (cudaStreamEndCapture(plan->st, g) != cudaSuccess) return cuda_check("end capture");
+  int rc2 = enqueue_step(plan);
+  cudaGraph_t made = nullptr;
+  cudaError_t e = cudaStreamEndCapture(plan->st, &made);
+  if (rc2 != JR_OK) {
+    if (made) cudaGraphDestroy(made);
+    return rc2;
+  }
+  if (e != cudaSuccess) return cuda_check("end capture");
+  *g = made;
+  plan->kernels_outside = graph_nodes(made) - (plan->live_dims.n_cases > 0 ? plan->cfg.maxiter : 0);
+  return JR_OK;
+}
+
+// Folds the kernels launched by the current graph's steps into `launched`.
+static int fold_launches(jr_plan* p) {
+  unsigned long long cycles = 0;
+  cudaMemcpyAsync(&cycles, p->cycles, sizeof(cycles), cudaMemcpyDeviceToHost, p->st);
+  if (cudaStreamSynchronize(p->st) != cudaSuccess) return cuda_check("launch count");
+  p->launched += p->steps_since * p->kernels_outside + (int64_t)(cycles - p->cycles_base) * p->kernels_per_cycle;
+  p->cycles_base = cycles;
+  p->steps_since = 0;
   return JR_OK;
 }
 
 int jr_graph_kernels(jr_plan* plan, int64_t* kernels_per_step) {
   if (!plan || !kernels_per_step) return fail(JR_EINVAL, "null argument");
-  cudaGraph_t g;
-  int rc = capture_step(plan, &g);
+  int rc = fold_launches(plan);
   if (rc) return rc;
-  size_t n = 0;
-  cudaGraphGetNodes(g, nullptr, &n);
-  std::vector<cudaGraphNode_t> nodes(n);
-  cudaGraphGetNodes(g, nodes.data(), &n);
-  int64_t kernels = 0;
-  for (auto node : nodes) {
-    cudaGraphNodeType t;
-    cudaGraphNodeGetType(node, &t);
-    if (t == cudaGraphNodeTypeKernel) ++kernels;
-  }
+  cudaGraph_t g;
+  rc = capture_step(plan, &g);
+  if (rc) return rc;
   cudaGraphDestroy(g);
-  *kernels_per_step = kernels;
+  *kernels_per_step = plan->kernels_outside + plan->cfg.maxiter * plan->kernels_per_cycle;
   return cuda_check("jr_graph_kernels");
 }
 
+int jr_launch_count(jr_plan* plan, int64_t* kernels) {
+  if (!plan || !kernels) return fail(JR_EINVAL, "null argument");
+  int rc = fold_launches(plan);
+  if (rc) return rc;
+  *kernels = plan->launched;
+  return JR_OK;
+}
+
 static int ensure_graph(jr_plan* plan) {
+  if (plan->live_dirty && plan->graph) {
+    int rcf = fold_launches(plan);
+    if (rcf) return rcf;
+  }
+  int rc0 = refresh_live(plan);
+  if (rc0) return rc0;
   if (plan->graph) return JR_OK;
   cudaGraph_t g;
   int rc = capture_step(plan, &g);
@@ -764,8 +890,11 @@ int jr_newton_steps_async(jr_plan* plan, int32_t n_steps, double* history_device
   if (rc) return rc;
   // the history position of every case restarts at 0 for this call
   for (int k = 0; k < plan->n_cases; ++k) cudaMemsetAsync(&plan->sc[k].hpos, 0, sizeof(int), plan->st);
-  for (int k = 0; k < n_steps; ++k)
-    if (cudaGraphLaunch(plan->graph, plan->st) != cudaSuccess) return cuda_check("graph launch");
+  if (plan->n_live > 0) {
+    for (int k = 0; k < n_steps; ++k)
+      if (cudaGraphLaunch(plan->graph, plan->st) != cudaSuccess) return cuda_check("graph launch");
+    plan->steps_since += n_steps;
+  }
   if (history_device && n_steps > 0)
     cudaMemcpyAsync(history_device, plan->history, (size_t)n_steps * plan->n_cases * sizeof(double),
                     cudaMemcpyDeviceToDevice, plan->st);

@@ -108,6 +108,7 @@ struct CaseDev {
   double force_length, moment_centre[2];   // force coefficients' reference length and moment centre
   int n_vec, m, visc, mixed, n_tiles, tiles_x, tiles_y;
   int enabled;              // 0: a free slot, every kernel returns at once
+  int slot;                 // the case's index in its plan (its history column)
 };
 
 // Buffers a kernel may be told to read or write (resolved per case)
@@ -151,14 +152,23 @@ __device__ __forceinline__ bool idle_block(const CaseDev& g, bool beyond, int ch
 
 // Grid extents of a batch's launches: the largest of each per-case count.
 struct BatchDims {
-  int n_cases;
+  int n_cases;              // cases in the launch's table
+  int n_slots;              // cases of the plan (the history's row length)
   int tiles_x, tiles_y;     // residual tiles
   int ghost_records;        // both stages
   int faces, cells;         // canvas faces, canvas cells
   int n_vec;                // nvar * cells
   int chain_blocks;         // chains + off-chain blocks of the line solve
   int max_L;                // longest chain
+  int cgs_blocks;           // blocks of the basis passes
 };
+
+// The basis passes: a block owns a chunk of cgs_chunk(n) elements of a case of n, set by
+// the case's size alone (so its sums are the same in any batch): small cases keep two
+// blocks per SM, large ones use longer chunks.
+constexpr int CGS_MAX_CHUNK = 2048;
+__host__ __device__ __forceinline__ int cgs_chunk(int n) { return n >= 2 * 148 * 2048 ? 2048 : 1024; }
+__host__ __device__ __forceinline__ int cgs_blocks(int n) { return (n + cgs_chunk(n) - 1) / cgs_chunk(n); }
 
 // the number of blocks a per-case reduction over n elements uses (<= the grid's x)
 __host__ __device__ __forceinline__ int chunk_blocks(int n) {

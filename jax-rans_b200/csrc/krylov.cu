@@ -13,7 +13,6 @@
 namespace jr {
 
 constexpr int RED_THREADS = 256;
-constexpr int MD_E = 4;   // elements per thread in the basis passes
 
 __device__ __forceinline__ double warp_sum(double x) {
   for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
@@ -172,7 +171,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_gmres_init(const CaseDev* __res
     double nrm = sqrt(s / cd.c.volume_sum);
     sc->norm = nrm;
     // history: [step][case] over the cases of the batch
-    if (cd.history != nullptr) cd.history[(size_t)sc->hpos * n_cases_hist + blockIdx.y] = nrm;
+    if (cd.history != nullptr) cd.history[(size_t)sc->hpos * n_cases_hist + cd.slot] = nrm;
     sc->hpos += 1;
     sc->bnorm = sqrt(acc[0]);
     sc->rnorm = sc->bnorm;
@@ -196,18 +195,34 @@ __global__ void k_cycle_start(const CaseDev* __restrict__ cases) {
   sc->inv_nrm = 1.0 / fmax(sc->beta, 2.2250738585072014e-308);
 }
 
+// The gate of a Krylov cycle in the step graph: the cycle's body (an IF node) runs only
+// when some case of the launch is still active; `cycles` counts the bodies run.
+__global__ void k_cycle_gate(const CaseDev* __restrict__ cases, int n_cases, cudaGraphConditionalHandle gate,
+                             unsigned long long* cycles) {
+  int any = 0;
+  for (int k = threadIdx.x; k < n_cases; k += blockDim.x) any |= cases[k].enabled && cases[k].sc->active != 0;
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) {
+    cudaGraphSetConditional(gate, any ? 1u : 0u);
+    if (any) *cycles += 1ull;
+  }
+}
+
 // The three passes of CGS2 over the basis, one kernel: MODE 0 h = V^T w; MODE 1
-// w -= V hin, then h = V^T w; MODE 2 w -= V hin, then |w| and column j of H.  Each
-// thread owns MD_E elements and keeps NK accumulators in registers; all loads of a
-// pass are independent of one another.
+// w -= V hin, then h = V^T w; MODE 2 w -= V hin, then |w| and column j of H.  A block
+// owns a chunk of cgs_chunk(n) elements.  The update runs thread per element (the nk
+// loads of an element independent of one another); the dot products run warp per basis
+// vector against the block's w held in shared memory, each lane with 16 loads in
+// flight, so the registers stay few and many blocks share an SM.  In MODE 1 the second
+// read of the chunk's basis rows is served by L2.
 template <class TV, int NK, int MODE>
-__global__ void __launch_bounds__(RED_THREADS, 2) k_mdot(const CaseDev* __restrict__ cases, int nk, int j) {
+__global__ void __launch_bounds__(RED_THREADS) k_mdot(const CaseDev* __restrict__ cases, int nk, int j) {
   const CaseDev& cd = cases[blockIdx.y];
   if (!cd.enabled) return;
   Scalars* sc = cd.sc;
   if (sc->active == 0) return;
   const int n = cd.n_vec, m = cd.m;
-  const int nb = (n + RED_THREADS * MD_E - 1) / (RED_THREADS * MD_E);
+  const int nb = cgs_blocks(n), C = cgs_chunk(n);
   if ((int)blockIdx.x >= nb) return;
   const TV* __restrict__ V = (const TV*)cd.V;
   const size_t ldv = (size_t)n;
@@ -216,63 +231,61 @@ __global__ void __launch_bounds__(RED_THREADS, 2) k_mdot(const CaseDev* __restri
   unsigned* ticket = cd.ticket;
   const double* hin = MODE == 1 ? sc->h1 : sc->h2;
   double* hout = MODE == 0 ? sc->h1 : sc->h2;
-  constexpr int NA = MODE == 2 ? 1 : NK;
-  __shared__ double sm[RED_THREADS / 32][NA];
-  __shared__ bool last;
-  double acc[NA];
-#pragma unroll
-  for (int k = 0; k < NA; ++k) acc[k] = 0.0;
-  // the coefficients of the update, shared by the block (broadcast reads)
+  __shared__ double ws[MODE == 2 ? 1 : CGS_MAX_CHUNK];
   __shared__ double h[MODE == 0 ? 1 : NK];
+  __shared__ double sm[RED_THREADS / 32];
+  __shared__ bool last;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   if constexpr (MODE != 0) {
     if ((int)threadIdx.x < NK) h[threadIdx.x] = (int)threadIdx.x < nk ? hin[threadIdx.x] : 0.0;
     __syncthreads();
   }
-  const int base = blockIdx.x * blockDim.x * MD_E + threadIdx.x;
-  // one element at a time: its NK loads are independent of one another, and the
-  // registers stay within two blocks per SM
-#pragma unroll 1
-  for (int t = 0; t < MD_E; ++t) {
-    const int i = base + t * blockDim.x;
-    if (i < n) {
-      double wi = w[i];
-      if constexpr (MODE != 0) {
-        double s = 0.0;
+  const int i0 = blockIdx.x * C;
+  const int cn = min(C, n - i0);
+  // 1. the update (MODE 1, 2), or the copy of w (MODE 0), element by element
+  double acc = 0.0;
+  for (int e = threadIdx.x; e < cn; e += blockDim.x) {
+    const int i = i0 + e;
+    double wi = w[i];
+    if constexpr (MODE != 0) {
+      double s = 0.0;
 #pragma unroll
-        for (int k = 0; k < NK; ++k)
-          if (k < nk) s += h[k] * double(V[k * ldv + i]);
-        wi = wi - s;
-        w[i] = wi;
-      }
-      if constexpr (MODE == 2) {
-        acc[0] += wi * wi;
-      } else {
-#pragma unroll
-        for (int k = 0; k < NK; ++k)
-          if (k < nk) acc[k] += double(V[k * ldv + i]) * wi;
-      }
+      for (int k = 0; k < NK; ++k)
+        if (k < nk) s += h[k] * double(V[k * ldv + i]);
+      wi = wi - s;
+      w[i] = wi;
     }
+    if constexpr (MODE == 2) acc += wi * wi;
+    else ws[e] = wi;
   }
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int width = MODE == 2 ? 1 : nk;
   if constexpr (MODE == 2) {
-    double x = warp_sum(acc[0]);
-    if (lane == 0) sm[warp][0] = x;
-  } else {
-    // all NK sums of the warp at once: about NK shuffles instead of 5 NK
-    warp_transpose_sum<NK>(acc, lane);
-    constexpr int HOLD = NK >= 32 ? NK / 32 : 1;      // sums a lane ends with
-    constexpr int SHARE = NK >= 32 ? 1 : 32 / NK;     // lanes holding the same sum
-    if (lane % SHARE == 0) {
-#pragma unroll
-      for (int r = 0; r < HOLD; ++r) sm[warp][(lane / SHARE) * HOLD + r] = acc[r];
+    double x = warp_sum(acc);
+    if (lane == 0) sm[warp] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = sm[0];
+      for (int ww = 1; ww < nw; ++ww) t += sm[ww];
+      partial[blockIdx.x * (MAX_KRYLOV + 1)] = t;
     }
-  }
-  __syncthreads();
-  if ((int)threadIdx.x < width) {
-    double t = 0.0;
-    for (int ww = 0; ww < nw; ++ww) t += sm[ww][threadIdx.x];
-    partial[blockIdx.x * (MAX_KRYLOV + 1) + threadIdx.x] = t;
+  } else {
+    __syncthreads();
+    // 2. the dot products, warp per basis vector
+    for (int k = warp; k < nk; k += nw) {
+      const TV* __restrict__ vk = V + k * ldv + i0;
+      double a = 0.0;
+      int e = lane;
+      for (; e + 32 * 15 < cn; e += 32 * 16) {
+        double x[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) x[u] = double(vk[e + 32 * u]);
+#pragma unroll
+        for (int u = 0; u < 16; ++u) a += x[u] * ws[e + 32 * u];
+      }
+      for (; e < cn; e += 32) a += double(vk[e]) * ws[e];
+      a = warp_sum(a);
+      if (lane == 0) partial[blockIdx.x * (MAX_KRYLOV + 1) + k] = a;
+    }
   }
   __threadfence();
   __syncthreads();
@@ -560,22 +573,27 @@ __global__ void k_scale_copy(const CaseDev* __restrict__ cases, int src_id, int 
 
 // blocks of the basis passes of a case of n elements (and the largest block count any
 // reduction uses: the size of a case's partial array)
-int reduce_blocks(int n) { return max(2 * 148, (n + RED_THREADS * MD_E - 1) / (RED_THREADS * MD_E)); }
+int reduce_blocks(int n) { return max(2 * 148, (n + 1023) / 1024); }
 
 static dim3 chunk_grid(const BatchDims& d) { return dim3(chunk_blocks(d.n_vec), d.n_cases); }
 static dim3 stride_grid(const BatchDims& d) { return dim3(min((d.n_vec + 255) / 256, 148 * 4), d.n_cases); }
 
 void launch_gmres_init(const CaseDev* cases, const BatchDims& d, cudaStream_t st) {
-  k_gmres_init<<<chunk_grid(d), RED_THREADS, 0, st>>>(cases, d.n_cases);
+  k_gmres_init<<<chunk_grid(d), RED_THREADS, 0, st>>>(cases, d.n_slots);
 }
 
 void launch_cycle_start(const CaseDev* cases, const BatchDims& d, cudaStream_t st) {
   k_cycle_start<<<dim3(1, d.n_cases), 128, 0, st>>>(cases);
 }
 
+void launch_cycle_gate(const CaseDev* cases, const BatchDims& d, cudaGraphConditionalHandle gate,
+                       unsigned long long* cycles, cudaStream_t st) {
+  k_cycle_gate<<<1, 256, 0, st>>>(cases, d.n_cases, gate, cycles);
+}
+
 template <class TV, int NK>
 static void arnoldi_nk(const CaseDev* cases, const BatchDims& d, int j, cudaStream_t st) {
-  dim3 grid((d.n_vec + RED_THREADS * MD_E - 1) / (RED_THREADS * MD_E), d.n_cases);
+  dim3 grid(d.cgs_blocks, d.n_cases);
   k_mdot<TV, NK, 0><<<grid, RED_THREADS, 0, st>>>(cases, j + 1, j);
   k_mdot<TV, NK, 1><<<grid, RED_THREADS, 0, st>>>(cases, j + 1, j);
   k_mdot<TV, NK, 2><<<grid, RED_THREADS, 0, st>>>(cases, j + 1, j);

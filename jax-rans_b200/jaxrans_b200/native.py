@@ -61,7 +61,8 @@ EXPORTS = ("jr_plan_create", "jr_plan_destroy", "jr_last_error", "jr_plan_sizes"
            "jr_state_set", "jr_state_get", "jr_state_device", "jr_newton_steps", "jr_newton_steps_async",
            "jr_forces", "jr_state_set_device", "jr_graph_kernels", "jr_time_kernels", "jr_plan_set_stream",
            "jr_batch_create", "jr_plan_cases", "jr_case_sizes", "jr_case_enable", "jr_case_set_inflow",
-           "jr_case_state_set", "jr_case_state_get", "jr_residual_noalloc", "jr_case_load")
+           "jr_case_state_set", "jr_case_state_get", "jr_residual_noalloc", "jr_case_load",
+           "jr_launch_count")
 
 TIMED_KERNELS = ("residual_tile", "jvp_tile", "ghosts_tangent", "line_apply", "line_factor", "cgs2_full_basis")
 
@@ -104,6 +105,7 @@ def load_library(path: Path | None = None) -> C.CDLL:
         "jr_forces": (C.c_int, [vp, vp, vp]),
         "jr_state_set_device": (C.c_int, [vp, vp, C.c_double, C.c_double]),
         "jr_graph_kernels": (C.c_int, [vp, C.POINTER(C.c_int64)]),
+        "jr_launch_count": (C.c_int, [vp, C.POINTER(C.c_int64)]),
         "jr_time_kernels": (C.c_int, [vp, C.c_int32, _f64p]),
         "jr_plan_set_stream": (C.c_int, [vp, vp]),
         "jr_batch_create": (C.c_int, [C.POINTER(PlanDesc), C.c_int32, C.POINTER(vp)]),
@@ -422,6 +424,12 @@ class DevicePlan:
     def kernels_per_step(self) -> int:
         n = C.c_int64()
         _check(self.lib, self.lib.jr_graph_kernels(self.handle, C.byref(n)), "jr_graph_kernels")
+        return int(n.value)
+
+    def launch_count(self) -> int:
+        """Kernels launched by this plan's Newton steps so far (skipped cycles not counted)."""
+        n = C.c_int64()
+        _check(self.lib, self.lib.jr_launch_count(self.handle, C.byref(n)), "jr_launch_count")
         return int(n.value)
 
     def time_kernels(self, reps: int = 20) -> dict:

@@ -265,31 +265,55 @@ def summary(served: list[Served], wall: float) -> dict:
 
 
 def main(argv=None) -> int:
-    """Serve a seeded Poisson stream of SA requests and print a JSON summary."""
+    """Serve a seeded Poisson stream of SA requests and print a JSON summary; with
+    ``--plain`` also solve the first requests one at a time on the plain FP64 path and
+    compare rates and forces."""
     import argparse
+    import dataclasses
     import json
+    from .solver import march
     from .workloads import workload
     ap = argparse.ArgumentParser(prog="python -m jaxrans_b200.serve", description=main.__doc__)
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--rate", type=float, default=20.0)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--precision", default="mixed", choices=("fp64", "mixed"))
+    ap.add_argument("--limiter", default="van_albada", help="the requests' MUSCL limiter")
     ap.add_argument("--max-slots", type=int, default=64)
     ap.add_argument("--workers", type=int, default=8)
+    ap.add_argument("--plain", type=int, default=0, metavar="N",
+                    help="also solve the first N requests alone on the plain FP64 path")
     args = ap.parse_args(argv)
-    template = workload("c_sa_385", **{"implicit.precision": args.precision})
+    template = workload("c_sa_385", **{"implicit.precision": args.precision,
+                                       "convective_fluxes.limiter": args.limiter})
     requests = poisson_requests(args.requests, template, args.rate, args.seed)
     server = Server(max_slots=args.max_slots, workers=args.workers)
     t = time.perf_counter()
     served = server.serve(requests)
     wall = time.perf_counter() - t
     out = summary(served, wall)
-    out.update({"rate_per_s": args.rate, "seed": args.seed, "precision": args.precision, "wall_s": wall,
-                "slots": {f"{k[0]}x{k[1]}": p.slots for k, p in server.pools.items()},
+    out.update({"rate_per_s": args.rate, "seed": args.seed, "precision": args.precision, "limiter": args.limiter,
+                "wall_s": wall, "slots": {f"{k[0]}x{k[1]}": p.slots for k, p in server.pools.items()},
                 "per_class": {f"{k[0]}x{k[1]}": summary([x for x in served if x.request.grid_key == k], wall)
                               for k in server.pools}})
-    print(json.dumps(out), flush=True)
     server.close()
+    if args.plain:
+        seconds, dcl, dcd, rows = 0.0, [], [], []
+        for x in served[: args.plain]:
+            c = x.request.case
+            plain = dataclasses.replace(c, implicit=dataclasses.replace(c.implicit, precision="fp64"))
+            grid = plain.grid()
+            t = time.perf_counter()
+            r = march(plain, grid)
+            seconds += time.perf_counter() - t
+            dcl.append(abs(x.forces.cl - r.forces.cl))
+            dcd.append(abs(x.forces.cd - r.forces.cd))
+            rows.append({"id": x.request.id, "served": x.reason, "plain": r.history.reason,
+                         "dcl": dcl[-1], "dcd_counts": 1e4 * dcd[-1]})
+        out["plain_fp64"] = {"requests": args.plain, "solves_per_hr": 3600.0 * args.plain / seconds,
+                             "seconds": seconds, "max_dcl": max(dcl), "max_dcd_counts": 1e4 * max(dcd),
+                             "rows": rows}
+    print(json.dumps(out), flush=True)
     return 0
 
 

@@ -151,3 +151,17 @@ def test_uneven_batch_equals_runs_alone(cuda):
         alone = march(c, g)
         assert np.array_equal(r.history.residual, alone.history.residual)
         assert np.array_equal(r.U, alone.U)
+
+
+def test_skipped_krylov_cycles_launch_nothing(cuda):
+    """A Krylov cycle no case needs is skipped on the device (a conditional graph node):
+    the launch count stays below steps x the kernels of a step with every cycle run."""
+    from jaxrans_b200.native import DevicePlan
+    z, case, plan = load("o_euler")
+    dev = DevicePlan(plan, case.flow, case.numerics, replace(case.implicit, krylov_restarts=3))
+    dev.set_state(freestream_state(case, plan), case.implicit.cfl)
+    full = dev.kernels_per_step()
+    before = dev.launch_count()
+    dev.newton_steps(10)
+    launched = dev.launch_count() - before
+    assert 0 < launched < 10 * full
