@@ -13,7 +13,7 @@ namespace jr {
 // residual.cu
 void launch_residual(const CaseDev*, const BatchDims&, int visc, bool second, int out_id, cudaStream_t);
 void launch_jvp(const CaseDev*, const BatchDims&, int visc, int tangent_id, int vdt_id, int out_id, int check_active,
-                cudaStream_t);
+                int own_ghosts, cudaStream_t);
 void launch_ghosts(const CaseDev*, const BatchDims&, int tangent_id, int check_active, cudaStream_t);
 void launch_faces(const CaseDev*, const BatchDims&, int visc, cudaStream_t);
 void launch_cells(const CaseDev*, const BatchDims&, int visc, cudaStream_t);
@@ -84,6 +84,7 @@ struct jr_plan {
   unsigned long long cycles_base = 0;    // the cycle counter when the current graph was made
   int n_live = 0;
   bool live_dirty = true;
+  bool live_vortex = false;              // an enabled case uses the point-vortex far field
   std::vector<std::vector<int>> chain_len;   // each case's chain lengths (host copy)
 };
 
@@ -184,6 +185,11 @@ static int build_case(jr_plan* plan, const jr_plan_desc* d, CaseDev& cd, size_t&
     for (int k = 0; k < d->n_ghost[1]; ++k)
       if (!d->interior[d->source[1][k]]) src_rec[k] = rec_of[d->source[1][k]];
     TRY(put(plan, (int**)&c.g_src_rec, src_rec.data(), src_rec.size(), reload));
+    // which record fills each canvas cell (stage 2 after stage 1, as the fill order)
+    std::vector<int> ghost_rec(N, -1);
+    for (int k = 0; k < d->n_ghost[0]; ++k) ghost_rec[d->ghost[0][k]] = k;
+    for (int k = 0; k < d->n_ghost[1]; ++k) ghost_rec[d->ghost[1][k]] = d->n_ghost[0] + k;
+    TRY(put(plan, (int**)&c.ghost_rec, ghost_rec.data(), ghost_rec.size(), reload));
   }
   c.n_walls = d->n_walls;
   TRY(put(plan, (int**)&c.w_cell, d->wall_cell, (size_t)d->n_walls, reload));
@@ -428,8 +434,10 @@ static void enqueue_cycle(jr_plan* p, cudaStream_t st) {
     const int src = j == 0 ? B_RR : B_W;
     if (pre) launch_chain_apply(t, d, sa, p->mixed, src, 1, j, B_Z, 1, st);
     else launch_scale_copy(t, d, p->mixed, src, 1, j, B_Z, 1, st);
-    launch_ghosts(t, d, B_Z, 1, st);
-    launch_jvp(t, d, p->visc, B_Z, B_VDT, B_W, 1, st);
+    // the tangent ghosts: filled first when a case needs the point-vortex circulation,
+    // else evaluated by the J.v tiles themselves
+    if (p->live_vortex) launch_ghosts(t, d, B_Z, 1, st);
+    launch_jvp(t, d, p->visc, B_Z, B_VDT, B_W, 1, p->live_vortex ? 0 : 1, st);
     launch_arnoldi_orth(t, d, p->mixed, j, st);
   }
   launch_lstsq(t, d, st);
@@ -636,9 +644,13 @@ int jr_jvp(jr_plan* plan, const double* U, const double* v, double* Jv) {
   a.vec(&CaseDev::z, v);
   a.vec(&CaseDev::w, Jv);
   const CaseDev* t = a.upload();
+  // as in the Newton step: the tiles evaluate the tangent ghosts themselves unless a case
+  // uses the point-vortex far field
+  bool vortex = false;
+  for (const CaseDev& cd : plan->host) vortex = vortex || cd.P.far_field == 1;
   launch_ghosts(t, plan->dims, -1, 0, plan->st);
-  launch_ghosts(t, plan->dims, B_Z, 0, plan->st);
-  launch_jvp(t, plan->dims, plan->visc, B_Z, -1, B_W, 0, plan->st);
+  if (vortex) launch_ghosts(t, plan->dims, B_Z, 0, plan->st);
+  launch_jvp(t, plan->dims, plan->visc, B_Z, -1, B_W, 0, vortex ? 0 : 1, plan->st);
   return cuda_check("jr_jvp");
 }
 
@@ -802,6 +814,8 @@ static int refresh_live(jr_plan* p) {
   for (const CaseDev& cd : p->host)
     if (cd.enabled) on.push_back(cd);
   p->n_live = (int)on.size();
+  p->live_vortex = false;
+  for (const CaseDev& cd : on) p->live_vortex = p->live_vortex || cd.P.far_field == 1;
   p->live_dims = dims_of(on, p->n_cases);
   if (!on.empty()) {
     cudaMemcpyAsync(p->live, on.data(), on.size() * sizeof(CaseDev), cudaMemcpyHostToDevice, p->st);
@@ -949,7 +963,7 @@ int jr_time_kernels(jr_plan* plan, int32_t reps, double* ms) {
     ms[k] = (double)ms1 / reps;
   };
   timed(0, [&] { launch_residual(t, d, p->visc, true, B_R, st); });
-  timed(1, [&] { launch_jvp(t, d, p->visc, B_Z, B_VDT, B_W, 0, st); });
+  timed(1, [&] { launch_jvp(t, d, p->visc, B_Z, B_VDT, B_W, 0, 0, st); });
   timed(2, [&] { launch_ghosts(t, d, B_Z, 0, st); });
   timed(3, [&] { launch_chain_apply(t, d, sa, p->mixed, B_R, 0, -1, B_TMP, 0, st); });
   timed(4, [&] { launch_chain_factor(t, d, sa, p->mixed, st); });

@@ -43,6 +43,8 @@ struct Canvas {
   const int* g_kind[2];
   const double* g_geom[2];     // 4 per record: nx, ny, mx, my
   const int* g_src_rec;        // stage 2: the stage-1 record that fills its source, or -1
+  const int* ghost_rec;        // NI*NJ: the record (stage-1 index, or n_ghost[0] + stage-2 index)
+                               // that fills a canvas cell, or -1
   int n_walls;
   const int* w_cell;
   const int* w_family;

@@ -573,7 +573,7 @@ __global__ void k_scale_copy(const CaseDev* __restrict__ cases, int src_id, int 
 
 // blocks of the basis passes of a case of n elements (and the largest block count any
 // reduction uses: the size of a case's partial array)
-int reduce_blocks(int n) { return max(2 * 148, (n + 1023) / 1024); }
+int reduce_blocks(int n) { return max(max(2 * 148, chunk_blocks(n)), cgs_blocks(n)); }
 
 static dim3 chunk_grid(const BatchDims& d) { return dim3(chunk_blocks(d.n_vec), d.n_cases); }
 static dim3 stride_grid(const BatchDims& d) { return dim3(min((d.n_vec + 255) / 256, 148 * 4), d.n_cases); }

@@ -152,6 +152,26 @@ __device__ __forceinline__ void eval_record(const Canvas& c, const Physics& P, i
   }
 }
 
+// The tangent ghost value of record t (both stages numbered as in k_ghosts) from the
+// state and tangent of its source, evaluated where it is needed: the J.v tile computes
+// its halo's ghosts itself when no case uses the point-vortex far field (whose
+// circulation is a reduction over the wall).  Out of line: only boundary tiles call it.
+__device__ __noinline__ void ghost_tangent(const Canvas& c, const Physics& P, int t, const double* U,
+                                           const double* V, const double* qg, const double* dqg, Dual* out) {
+  const int n0 = c.n_ghost[0];
+  const int s = t < n0 ? 0 : 1, r = t < n0 ? t : t - n0;
+  Dual q[5];
+  const int r1 = s == 1 ? c.g_src_rec[r] : -1;
+  if (r1 >= 0) {
+    Dual q1[5];
+    load_prim<Dual>(c, P, c.g_source[0][r1], U, V, qg, dqg, q1);
+    eval_record<Dual>(c, P, 0, r1, q1, cst<Dual>(0.0), q);
+  } else {
+    load_prim<Dual>(c, P, c.g_source[s][r], U, V, qg, dqg, q);
+  }
+  eval_record<Dual>(c, P, s, r, q, cst<Dual>(0.0), out);
+}
+
 // Both stages in one launch: a stage-2 record whose source is a stage-1 ghost (a
 // corner) evaluates that stage-1 record itself rather than reading it, so no record
 // waits on another and every CTA works independently.
@@ -434,7 +454,7 @@ template <> __device__ __forceinline__ double tangent_or_value<Dual>(const Dual&
 template <class T, int NV, bool SECOND, int VISC>
 __global__ void __launch_bounds__(TILE_THREADS, TILE_MIN_BLOCKS)
     k_residual(const CaseDev* __restrict__ cases, int out_id, int tangent_id, int vdt_id, int with_partial,
-               int check_active) {
+               int check_active, int own_ghosts) {
   __shared__ CaseDev scase;
   if (idle_block(cases[blockIdx.z],
                  (int)blockIdx.x >= cases[blockIdx.z].tiles_x || (int)blockIdx.y >= cases[blockIdx.z].tiles_y,
@@ -463,7 +483,17 @@ __global__ void __launch_bounds__(TILE_THREADS, TILE_MIN_BLOCKS)
     int i = i0 - 2 + li, j = j0 - 2 + lj;
     T q[5];
     if (i >= 0 && i < NI && j >= 0 && j < NJ) {
-      load_prim<T>(c, P, i * NJ + j, U, V, qg, dqg, q);
+      const int idx = i * NJ + j;
+      int t = -1;
+      if constexpr (sizeof(T) == sizeof(Dual)) {
+        if (own_ghosts && !c.interior[idx]) t = c.ghost_rec[idx];
+      }
+      if constexpr (sizeof(T) == sizeof(Dual)) {
+        if (t >= 0) ghost_tangent(c, P, t, U, V, qg, dqg, q);
+        else load_prim<T>(c, P, idx, U, V, qg, dqg, q);
+      } else {
+        load_prim<T>(c, P, idx, U, V, qg, dqg, q);
+      }
     } else {
       for (int v = 0; v < NV; ++v) q[v] = cst<T>(1.0);
     }
@@ -755,10 +785,10 @@ void configure_kernels() {
 // with fewer tiles returns at once from the excess ones).
 template <class T, int NV, bool SECOND, int VISC>
 static void launch_tile(const CaseDev* cases, const BatchDims& d, int out_id, int tangent_id, int vdt_id,
-                        int with_partial, int check_active, cudaStream_t st) {
+                        int with_partial, int check_active, cudaStream_t st, int own_ghosts = 0) {
   dim3 grid(d.tiles_x, d.tiles_y, d.n_cases);
   k_residual<T, NV, SECOND, VISC><<<grid, TILE_THREADS, sizeof(TileSmem<T, NV>), st>>>(
-      cases, out_id, tangent_id, vdt_id, with_partial, check_active);
+      cases, out_id, tangent_id, vdt_id, with_partial, check_active, own_ghosts);
 }
 
 // R(U) of every case into `out_id` (second or first order), with the norm partials
@@ -775,12 +805,16 @@ void launch_residual(const CaseDev* cases, const BatchDims& d, int visc, bool se
   }
 }
 
-// out = vdt * v + dR1/dU . v with v = buffer `tangent_id` (vdt_id < 0: the bare J.v)
+// out = vdt * v + dR1/dU . v with v = buffer `tangent_id` (vdt_id < 0: the bare J.v);
+// own_ghosts: the tile evaluates its halo's tangent ghosts (no tangent ghost fill needed)
 void launch_jvp(const CaseDev* cases, const BatchDims& d, int visc, int tangent_id, int vdt_id, int out_id,
-                int check_active, cudaStream_t st) {
-  if (visc == 2) launch_tile<Dual, 5, false, 2>(cases, d, out_id, tangent_id, vdt_id, 0, check_active, st);
-  else if (visc == 1) launch_tile<Dual, 4, false, 1>(cases, d, out_id, tangent_id, vdt_id, 0, check_active, st);
-  else launch_tile<Dual, 4, false, 0>(cases, d, out_id, tangent_id, vdt_id, 0, check_active, st);
+                int check_active, int own_ghosts, cudaStream_t st) {
+  if (visc == 2)
+    launch_tile<Dual, 5, false, 2>(cases, d, out_id, tangent_id, vdt_id, 0, check_active, st, own_ghosts);
+  else if (visc == 1)
+    launch_tile<Dual, 4, false, 1>(cases, d, out_id, tangent_id, vdt_id, 0, check_active, st, own_ghosts);
+  else
+    launch_tile<Dual, 4, false, 0>(cases, d, out_id, tangent_id, vdt_id, 0, check_active, st, own_ghosts);
 }
 
 // the ghosts of U (tangent_id < 0) or of the tangent in buffer `tangent_id`
