@@ -434,10 +434,13 @@ static void enqueue_cycle(jr_plan* p, cudaStream_t st) {
     const int src = j == 0 ? B_RR : B_W;
     if (pre) launch_chain_apply(t, d, sa, p->mixed, src, 1, j, B_Z, 1, st);
     else launch_scale_copy(t, d, p->mixed, src, 1, j, B_Z, 1, st);
-    // the tangent ghosts: filled first when a case needs the point-vortex circulation,
-    // else evaluated by the J.v tiles themselves
-    if (p->live_vortex) launch_ghosts(t, d, B_Z, 1, st);
-    launch_jvp(t, d, p->visc, B_Z, B_VDT, B_W, 1, p->live_vortex ? 0 : 1, st);
+    // the tangent ghosts: a single case's J.v tiles evaluate their halo's ghosts
+    // themselves (one launch fewer on a latency-bound step); a batch, whose tiles run in
+    // many waves, fills them in one launch, as does any case that needs the point-vortex
+    // circulation
+    const bool own = !p->live_vortex && d.n_cases == 1;
+    if (!own) launch_ghosts(t, d, B_Z, 1, st);
+    launch_jvp(t, d, p->visc, B_Z, B_VDT, B_W, 1, own ? 1 : 0, st);
     launch_arnoldi_orth(t, d, p->mixed, j, st);
   }
   launch_lstsq(t, d, st);
