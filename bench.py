@@ -166,6 +166,23 @@ def run_reference(args) -> int:
     return 0
 
 
+def max_over_ranks(values, dist, device):
+    """Each value's maximum over the ranks (the slowest replica times the job); the
+    values themselves without a process group."""
+    if dist is None:
+        return list(values)
+    import torch
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def whole_job_rate(steps: int, n_cases: int, world: int, seconds: float) -> float:
+    """Solves per hour of the whole job: every rank solved steps x n_cases cases in at
+    most `seconds` (independent replicas, no collective on the data path)."""
+    return 3600.0 * steps * n_cases * world / seconds
+
+
 def load_job(args):
     """The cases of the workload (one, or a named batch), their grids (one per distinct
     workload) and the device plan."""
@@ -269,12 +286,9 @@ def run_device(args) -> int:
         torch.cuda.synchronize()
         e2e_times.append(s.elapsed_time(e) / 1e3)
     e2e_total = sum(e2e_times)
-    if dist is not None:
-        t = torch.tensor([total, e2e_total], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total, e2e_total = float(t[0]), float(t[1])
-    value = 3600.0 * args.steps * n_cases * world / total
-    e2e_value = 3600.0 * args.steps * n_cases * world / e2e_total
+    total, e2e_total = max_over_ranks([total, e2e_total], dist, "cuda")
+    value = whole_job_rate(args.steps, n_cases, world, total)
+    e2e_value = whole_job_rate(args.steps, n_cases, world, e2e_total)
     # every case's latency: its exit within its batch, on the device clock of the batch
     latencies = [m.seconds * (step_t / max(mm.seconds for mm in mons))
                  for mons, step_t in zip(solves, per_step) for m in mons]

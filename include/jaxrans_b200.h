@@ -189,10 +189,27 @@ int jr_newton_steps(jr_plan* plan, int32_t n_steps, double* history);
  * on the device) receives the norms.  For timing with events on the plan's stream. */
 int jr_newton_steps_async(jr_plan* plan, int32_t n_steps, double* history_device);
 
+/* The plan's autotuner: times the line factor and the line solve with each block size the
+ * longest chain allows (64, 128, 256 threads per chain, reps launches each, at the plan's
+ * state) and keeps the fastest; chosen (2 values, may be NULL) receives the factor's and
+ * the solve's.  Results do not depend on the schedule (each row's arithmetic is the same).
+ * The tile shape of the residual is not tuned: it sets the order of the residual norm's
+ * partial sums.  Overwrites the plan's preconditioner factor (the next Newton step makes
+ * its own).  Replaces the reference's reliance on XLA's own kernel choices; no
+ * counterpart function. */
+int jr_autotune(jr_plan* plan, int32_t reps, int32_t* chosen);
+
 /* Force coefficients at the plan's state (or at U if not NULL, a device pointer): out
  * (host, 6 per case) = cl, cd, cm, cd_friction, fx, fy.  Replaces force_coefficients
  * (src/jaxrans/post/forces.py:108-161).  Synchronises. */
 int jr_forces(jr_plan* plan, const double* U, double* out);
+
+/* Wall loads per wall face, every case's faces back to back in the plan's wall order, 5
+ * values a face (host out): gauge pressure, the area vector into the fluid (x, y), the
+ * viscous force on the body (x, y) -- the inputs of the surface distributions (cp, cf).
+ * At the plan's state, or at U (device) if not NULL.  Replaces wall_loads
+ * (src/jaxrans/post/forces.py:48-68).  Synchronises. */
+int jr_wall_loads(jr_plan* plan, const double* U, double* out);
 
 #ifdef __cplusplus
 }

@@ -2,6 +2,7 @@
 // buffers and solver state, one stream), the per-call entry points, and the Newton step
 // of every case of the batch as one CUDA graph.  A single case is a batch of one.
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -24,6 +25,7 @@ void launch_chain_factor(const CaseDev*, const BatchDims&, bool sa, bool fp32, c
 void launch_chain_apply(const CaseDev*, const BatchDims&, bool sa, bool fp32, int src_id, int scale_on, int vout_j,
                         int out_id, int check_active, cudaStream_t);
 int chain_grid_blocks(int n_chains, int n_offchain);
+bool apply_threads_valid(int threads, int max_L);
 void configure_line_kernels(int max_L);
 // krylov.cu
 void launch_gmres_init(const CaseDev*, const BatchDims&, cudaStream_t);
@@ -58,8 +60,9 @@ struct jr_plan {
   std::vector<CaseDev> host;             // the resident case table (host copy)
   CaseDev* cases = nullptr;              // ... on the device: the graph's table
   CaseDev* adhoc = nullptr;              // the table of a call on caller buffers
-  std::vector<size_t> vec_off, can_off, face_off;   // offsets of each case in batch-long arrays
-  size_t total_vec = 0, total_can = 0, total_faces = 0;
+  std::vector<size_t> vec_off, can_off, face_off, wall_off;   // offsets of each case in batch-long arrays
+  size_t total_vec = 0, total_can = 0, total_faces = 0, total_walls = 0;
+  double* wall_out = nullptr;            // 5 per wall face, every case
   cudaStream_t st = nullptr;             // the stream work is issued on
   cudaStream_t owned_stream = nullptr;   // the plan's own stream
   std::vector<void*> allocs;
@@ -86,6 +89,7 @@ struct jr_plan {
   bool live_dirty = true;
   bool live_vortex = false;              // an enabled case uses the point-vortex far field
   std::vector<std::vector<int>> chain_len;   // each case's chain lengths (host copy)
+  int ls_factor_threads = 128, ls_apply_threads = 128;   // the line-solve schedule in use
 };
 
 static int fail(int code, const std::string& msg) {
@@ -300,12 +304,15 @@ static int build_buffers(jr_plan* p, const std::vector<size_t>& factor_rows) {
   p->vec_off.assign(nc, 0);
   p->can_off.assign(nc, 0);
   p->face_off.assign(nc, 0);
+  p->wall_off.assign(nc, 0);
   for (int k = 0; k < nc; ++k) {
     const Canvas& c = p->host[k].c;
     const size_t N = (size_t)c.NI * c.NJ, nf = (size_t)(c.NI + 1) * c.NJ + (size_t)c.NI * (c.NJ + 1);
     p->vec_off[k] = p->total_vec;
     p->can_off[k] = p->total_can;
     p->face_off[k] = p->total_faces;
+    p->wall_off[k] = p->total_walls;
+    p->total_walls += (size_t)c.n_walls;
     tile_off[k] = tiles;
     fb_off[k] = fb;
     part_off[k] = part;
@@ -341,6 +348,7 @@ static int build_buffers(jr_plan* p, const std::vector<size_t>& factor_rows) {
   TRY(dev_alloc(p, (void**)&p->sc, (size_t)nc * sizeof(Scalars)));
   TRY(dev_alloc(p, (void**)&p->history, (size_t)HIST_STEPS * nc * sizeof(double)));
   TRY(dev_alloc(p, (void**)&p->force_out, (size_t)8 * nc * sizeof(double)));
+  TRY(dev_alloc(p, (void**)&p->wall_out, std::max<size_t>(1, p->total_walls) * 5 * sizeof(double)));
   p->U = vec[0];
   for (int k = 0; k < nc; ++k) {
     CaseDev& cd = p->host[k];
@@ -364,6 +372,7 @@ static int build_buffers(jr_plan* p, const std::vector<size_t>& factor_rows) {
     cd.slot = k;
     cd.history = p->history;
     cd.force_out = p->force_out + 8 * k;
+    cd.wall_out = p->wall_out + 5 * p->wall_off[k];
   }
   TRY(dev_alloc(p, (void**)&p->cases, (size_t)nc * sizeof(CaseDev)));
   TRY(dev_alloc(p, (void**)&p->adhoc, (size_t)nc * sizeof(CaseDev)));
@@ -393,10 +402,16 @@ static BatchDims dims_of(const std::vector<CaseDev>& cases, int n_slots) {
     d.cgs_blocks = std::max(d.cgs_blocks, cgs_blocks(cd.n_vec));
   }
   d.chain_blocks = std::max(d.chain_blocks, 1);
+  d.ls_factor_threads = 128;
+  d.ls_apply_threads = 128;
   return d;
 }
 
-static void compute_dims(jr_plan* p) { p->dims = dims_of(p->host, p->n_cases); }
+static void compute_dims(jr_plan* p) {
+  p->dims = dims_of(p->host, p->n_cases);
+  p->dims.ls_factor_threads = p->ls_factor_threads;
+  p->dims.ls_apply_threads = p->ls_apply_threads;
+}
 
 // The table of a call on caller buffers: the resident table with the named buffers of
 // every case moved to its part of the caller's batch-long arrays.
@@ -474,8 +489,18 @@ static int enqueue_step(jr_plan* p) {
   launch_faces(t, d, p->visc, st);
   launch_cells(t, d, p->visc, st);
   if (pre) launch_chain_factor(t, d, sa, p->mixed, st);
+  // JR_GRAPH_CONDITIONALS=0 captures every cycle unconditionally (its kernels return at
+  // once when no case is active): for profilers that cannot see the kernels of a graph
+  // with conditional nodes.  The results are the same either way.
+  const char* env = getenv("JR_GRAPH_CONDITIONALS");
+  const bool conditional = env == nullptr || strcmp(env, "0") != 0;
   for (int cyc = 0; cyc < p->cfg.maxiter; ++cyc) {
     launch_cycle_start(t, d, st);
+    if (!conditional) {
+      enqueue_cycle(p, st);
+      p->kernels_per_cycle = 0;
+      continue;
+    }
     cudaStreamCaptureStatus status;
     cudaGraph_t graph;
     const cudaGraphNode_t* deps;
@@ -820,6 +845,8 @@ static int refresh_live(jr_plan* p) {
   p->live_vortex = false;
   for (const CaseDev& cd : on) p->live_vortex = p->live_vortex || cd.P.far_field == 1;
   p->live_dims = dims_of(on, p->n_cases);
+  p->live_dims.ls_factor_threads = p->ls_factor_threads;
+  p->live_dims.ls_apply_threads = p->ls_apply_threads;
   if (!on.empty()) {
     cudaMemcpyAsync(p->live, on.data(), on.size() * sizeof(CaseDev), cudaMemcpyHostToDevice, p->st);
     if (cudaStreamSynchronize(p->st) != cudaSuccess) return cuda_check("live table");
@@ -846,7 +873,8 @@ static int capture_step(jr_plan* plan, cudaGraph_t* g) {
   }
   if (e != cudaSuccess) return cuda_check("end capture");
   *g = made;
-  plan->kernels_outside = graph_nodes(made) - (plan->live_dims.n_cases > 0 ? plan->cfg.maxiter : 0);
+  // every node is a kernel but the cycles' conditional nodes (none without them)
+  plan->kernels_outside = graph_nodes(made) - (plan->kernels_per_cycle > 0 ? plan->cfg.maxiter : 0);
   return JR_OK;
 }
 
@@ -974,6 +1002,78 @@ int jr_time_kernels(jr_plan* plan, int32_t reps, double* ms) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return cuda_check("jr_time_kernels");
+}
+
+// The autotuner: for the line factor and the line solve, time every block size the
+// plan's longest chain allows (64, 128, 256 threads per chain) at the plan's state and
+// keep the fastest.  Only the schedule changes -- each row's arithmetic is the same -- so
+// results do not depend on the choice.  The step graph is captured anew.
+int jr_autotune(jr_plan* plan, int32_t reps, int32_t* chosen) {
+  if (!plan || reps < 1) return fail(JR_EINVAL, "bad argument");
+  jr_plan* p = plan;
+  const CaseDev* t = p->cases;
+  const bool sa = p->nvar == 5;
+  cudaStream_t st = p->st;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  launch_faces(t, p->dims, p->visc, st);
+  launch_cells(t, p->dims, p->visc, st);
+  const int cands[3] = {64, 128, 256};
+  float best_f = 1e30f, best_a = 1e30f;
+  int pick_f = p->ls_factor_threads, pick_a = p->ls_apply_threads;
+  for (int c : cands) {
+    BatchDims d = p->dims;
+    d.ls_factor_threads = c;
+    d.ls_apply_threads = c;
+    auto timed = [&](auto&& launch) {
+      launch();
+      cudaEventRecord(e0, st);
+      for (int r = 0; r < reps; ++r) launch();
+      cudaEventRecord(e1, st);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      return ms;
+    };
+    float tf = timed([&] { launch_chain_factor(t, d, sa, p->mixed, st); });
+    if (tf < best_f) {
+      best_f = tf;
+      pick_f = c;
+    }
+    if (apply_threads_valid(c, p->dims.max_L)) {
+      float ta = timed([&] { launch_chain_apply(t, d, sa, p->mixed, B_R, 0, -1, B_TMP, 0, st); });
+      if (ta < best_a) {
+        best_a = ta;
+        pick_a = c;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  int rc = cuda_check("jr_autotune");
+  if (rc) return rc;
+  p->ls_factor_threads = pick_f;
+  p->ls_apply_threads = pick_a;
+  compute_dims(p);
+  p->live_dirty = true;
+  if (chosen) {
+    chosen[0] = pick_f;
+    chosen[1] = pick_a;
+  }
+  return JR_OK;
+}
+
+int jr_wall_loads(jr_plan* plan, const double* U, double* out) {
+  if (!plan || !out) return fail(JR_EINVAL, "null argument");
+  std::vector<double> f((size_t)6 * plan->n_cases);
+  int rc = jr_forces(plan, U, f.data());   // the same launch writes the per-face loads
+  if (rc) return rc;
+  if (plan->total_walls > 0) {
+    cudaMemcpyAsync(out, plan->wall_out, plan->total_walls * 5 * sizeof(double), cudaMemcpyDeviceToHost, plan->st);
+    if (cudaStreamSynchronize(plan->st) != cudaSuccess) return cuda_check("jr_wall_loads");
+  }
+  return cuda_check("jr_wall_loads");
 }
 
 int jr_forces(jr_plan* plan, const double* U, double* out) {

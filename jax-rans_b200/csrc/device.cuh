@@ -103,6 +103,7 @@ struct CaseDev {
   Config cfg;
   double *U, *qg, *dqg, *R, *b, *x, *action, *r, *w, *z, *tmp, *vdt, *dflow, *dsa, *lam, *mflux, *dflux;
   double *tile_partial, *history, *force_out;
+  double* wall_out;         // per wall face: gauge pressure, area vector into the fluid (2), viscous force (2)
   void *V, *fflow, *fsa, *scratch;
   Scalars* sc;
   double* partial;          // reduction partials of this case
@@ -163,7 +164,11 @@ struct BatchDims {
   int chain_blocks;         // chains + off-chain blocks of the line solve
   int max_L;                // longest chain
   int cgs_blocks;           // blocks of the basis passes
+  int ls_factor_threads;    // threads per chain of the line factor and of the line solve:
+  int ls_apply_threads;     // the schedule the plan's autotuner picked (results do not depend on it)
 };
+
+constexpr int LS_MAX_THREADS = 256;   // the largest line-solve block
 
 // The basis passes: a block owns a chunk of cgs_chunk(n) elements of a case of n, set by
 // the case's size alone (so its sums are the same in any batch): small cases keep two

@@ -109,6 +109,14 @@ __global__ void __launch_bounds__(256) k_forces(const CaseDev* __restrict__ case
       shx = into * fx;
       shy = into * fy;
     }
+    if (cd.wall_out != nullptr) {
+      double* o = cd.wall_out + 5 * w;
+      o[0] = p;
+      o[1] = Sx;
+      o[2] = Sy;
+      o[3] = shx;
+      o[4] = shy;
+    }
     double Lx = px + shx, Ly = py + shy;
     double rx = c.w_mid[2 * w] - cx0, ry = c.w_mid[2 * w + 1] - cy0;
     double moment = ry * px - rx * py;

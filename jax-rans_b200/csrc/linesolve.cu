@@ -157,7 +157,7 @@ __device__ __forceinline__ int level_rows(int L, int level) {
 // scratch holds the level's reduced system (a, d, c: 3 x 16 x rows) and the next one's.
 // ------------------------------------------------------------------------------------
 template <class TF, bool SA>
-__global__ void __launch_bounds__(LS_THREADS) k_cr_factor(const CaseDev* __restrict__ cases) {
+__global__ void __launch_bounds__(LS_MAX_THREADS) k_cr_factor(const CaseDev* __restrict__ cases) {
   __shared__ CaseDev scase;
   if (idle_block(cases[blockIdx.y], (int)blockIdx.x >= cases[blockIdx.y].c.n_chains, 0)) return;
   const CaseDev& cd = stage_case(cases, blockIdx.y, &scase);
@@ -334,7 +334,7 @@ __host__ __device__ __forceinline__ int offchain_blocks(int n_offchain) {
 // src_id: the right-hand side buffer; scale_on: multiply it by the case's 1/|w|;
 // vout_j >= 0: also write the scaled input to basis vector j; out_id: the result.
 template <class TF, class TV, bool SA>
-__global__ void __launch_bounds__(LS_THREADS) k_cr_apply(const CaseDev* __restrict__ cases, int src_id, int scale_on,
+__global__ void __launch_bounds__(LS_MAX_THREADS) k_cr_apply(const CaseDev* __restrict__ cases, int src_id, int scale_on,
                                                          int vout_j, int out_id, int check_active) {
   __shared__ CaseDev scase;
   {
@@ -508,12 +508,13 @@ size_t cr_apply_smem(int max_L, bool fp32) { return (size_t)2 * max_L * 5 * (fp3
 
 void launch_chain_factor(const CaseDev* cases, const BatchDims& d, bool sa, bool fp32, cudaStream_t st) {
   dim3 grid(d.chain_blocks, d.n_cases);
+  const int th = d.ls_factor_threads > 0 ? d.ls_factor_threads : LS_THREADS;
   if (fp32) {
-    if (sa) k_cr_factor<float, true><<<grid, LS_THREADS, 0, st>>>(cases);
-    else k_cr_factor<float, false><<<grid, LS_THREADS, 0, st>>>(cases);
+    if (sa) k_cr_factor<float, true><<<grid, th, 0, st>>>(cases);
+    else k_cr_factor<float, false><<<grid, th, 0, st>>>(cases);
   } else {
-    if (sa) k_cr_factor<double, true><<<grid, LS_THREADS, 0, st>>>(cases);
-    else k_cr_factor<double, false><<<grid, LS_THREADS, 0, st>>>(cases);
+    if (sa) k_cr_factor<double, true><<<grid, th, 0, st>>>(cases);
+    else k_cr_factor<double, false><<<grid, th, 0, st>>>(cases);
   }
 }
 
@@ -522,10 +523,11 @@ static void apply_t(const CaseDev* cases, const BatchDims& d, bool sa, int src_i
                     int check_active, cudaStream_t st) {
   dim3 grid(d.chain_blocks, d.n_cases);
   size_t smem = cr_apply_smem(d.max_L, sizeof(TF) == 4);
+  const int th = d.ls_apply_threads > 0 ? d.ls_apply_threads : LS_THREADS;
   if (sa)
-    k_cr_apply<TF, TV, true><<<grid, LS_THREADS, smem, st>>>(cases, src_id, scale_on, vout_j, out_id, check_active);
+    k_cr_apply<TF, TV, true><<<grid, th, smem, st>>>(cases, src_id, scale_on, vout_j, out_id, check_active);
   else
-    k_cr_apply<TF, TV, false><<<grid, LS_THREADS, smem, st>>>(cases, src_id, scale_on, vout_j, out_id, check_active);
+    k_cr_apply<TF, TV, false><<<grid, th, smem, st>>>(cases, src_id, scale_on, vout_j, out_id, check_active);
 }
 
 // z = M^-1 (scale * src) for every case; vout_j >= 0 writes the scaled input to basis
@@ -537,6 +539,10 @@ void launch_chain_apply(const CaseDev* cases, const BatchDims& d, bool sa, bool 
 }
 
 int chain_grid_blocks(int n_chains, int n_offchain) { return n_chains + offchain_blocks(n_offchain); }
+
+// A thread of the solve keeps up to four even rows of a level in registers, so a block
+// must have at least a quarter as many threads as the longest chain has even rows.
+bool apply_threads_valid(int threads, int max_L) { return 4 * threads >= (max_L + 1) / 2 && threads <= LS_MAX_THREADS; }
 
 void configure_line_kernels(int max_L) {
   size_t s8 = cr_apply_smem(max_L, false), s4 = cr_apply_smem(max_L, true);

@@ -31,9 +31,11 @@ def batch_device(cases: list[Case], grids: list[Plan]):
     and force reference; the model, precision and Krylov settings must agree)."""
     from .native import DevicePlan
     specs = [c.grid_spec for c in cases]
-    return DevicePlan.batch(list(grids), [c.flow for c in cases], [c.numerics for c in cases],
-                            [c.implicit for c in cases], [s.reference_length for s in specs],
-                            [tuple(s.moment_centre[:2]) for s in specs])
+    dev = DevicePlan.batch(list(grids), [c.flow for c in cases], [c.numerics for c in cases],
+                           [c.implicit for c in cases], [s.reference_length for s in specs],
+                           [tuple(s.moment_centre[:2]) for s in specs])
+    dev.autotune()
+    return dev
 
 
 def start_batch(dev, cases: list[Case], grids: list[Plan], initial=None) -> None:
@@ -98,6 +100,9 @@ def run_batch(cases: list[Case], grids: list[Plan] | None = None, progress=None,
     cells = sum(g.cells for g in grids)
     timing = Timing(seconds, first_block, iterations, cases[0].block_iters, cells, cases=len(cases))
     results = []
+    walls = dev.wall_loads()
+    if dev.n_cases == 1:
+        walls = [walls]
     for k, (case, grid, mon) in enumerate(zip(cases, grids, monitors)):
         U = dev.case_state(k)[0]
         residual = mon.residual()
@@ -105,5 +110,5 @@ def run_batch(cases: list[Case], grids: list[Plan] | None = None, progress=None,
         forces = mon.forces if release else forces_of(np.atleast_2d(dev.forces())[k])
         results.append(Result(case=case, grid=grid, U=U, forces=forces, history=history,
                               cl_history=np.asarray(mon.cl_history), timing=timing,
-                              coefficients=np.asarray(mon.coefficients)))
+                              coefficients=np.asarray(mon.coefficients), wall=walls[k]))
     return results

@@ -62,7 +62,7 @@ EXPORTS = ("jr_plan_create", "jr_plan_destroy", "jr_last_error", "jr_plan_sizes"
            "jr_forces", "jr_state_set_device", "jr_graph_kernels", "jr_time_kernels", "jr_plan_set_stream",
            "jr_batch_create", "jr_plan_cases", "jr_case_sizes", "jr_case_enable", "jr_case_set_inflow",
            "jr_case_state_set", "jr_case_state_get", "jr_residual_noalloc", "jr_case_load",
-           "jr_launch_count")
+           "jr_launch_count", "jr_autotune", "jr_wall_loads")
 
 TIMED_KERNELS = ("residual_tile", "jvp_tile", "ghosts_tangent", "line_apply", "line_factor", "cgs2_full_basis")
 
@@ -106,6 +106,8 @@ def load_library(path: Path | None = None) -> C.CDLL:
         "jr_state_set_device": (C.c_int, [vp, vp, C.c_double, C.c_double]),
         "jr_graph_kernels": (C.c_int, [vp, C.POINTER(C.c_int64)]),
         "jr_launch_count": (C.c_int, [vp, C.POINTER(C.c_int64)]),
+        "jr_autotune": (C.c_int, [vp, C.c_int32, _i32p]),
+        "jr_wall_loads": (C.c_int, [vp, vp, vp]),
         "jr_time_kernels": (C.c_int, [vp, C.c_int32, _f64p]),
         "jr_plan_set_stream": (C.c_int, [vp, vp]),
         "jr_batch_create": (C.c_int, [C.POINTER(PlanDesc), C.c_int32, C.POINTER(vp)]),
@@ -426,6 +428,13 @@ class DevicePlan:
         _check(self.lib, self.lib.jr_graph_kernels(self.handle, C.byref(n)), "jr_graph_kernels")
         return int(n.value)
 
+    def autotune(self, reps: int = 10) -> dict:
+        """Pick the line factor's and line solve's block sizes by timing them (results do
+        not depend on the choice)."""
+        out = np.zeros(2, dtype=np.int32)
+        _check(self.lib, self.lib.jr_autotune(self.handle, int(reps), _ptr(out, _i32p)), "jr_autotune")
+        return {"line_factor_threads": int(out[0]), "line_apply_threads": int(out[1])}
+
     def launch_count(self) -> int:
         """Kernels launched by this plan's Newton steps so far (skipped cycles not counted)."""
         n = C.c_int64()
@@ -444,6 +453,17 @@ class DevicePlan:
 
     def state_device_ptr(self) -> int:
         return int(self.lib.jr_state_device(self.handle))
+
+    def wall_loads(self, U=None):
+        """Per wall face (n_walls, 5): gauge pressure, area vector into the fluid (x, y),
+        viscous force (x, y); a list with one array per case for a batch."""
+        n = [len(p.walls.cell) for p in self.plans]
+        out = np.empty((max(1, sum(n)), 5))
+        keep = self._device(U) if U is not None else None
+        ptr = None if keep is None else keep.data_ptr()
+        _check(self.lib, self.lib.jr_wall_loads(self.handle, ptr, out.ctypes.data), "jr_wall_loads")
+        parts = np.split(out[: sum(n)], np.cumsum(n)[:-1])
+        return parts[0] if self.n_cases == 1 else parts
 
     def forces(self, U=None) -> np.ndarray:
         """cl, cd, cm, cd_friction, fx, fy: ``(6,)``, or ``(n_cases, 6)`` for a batch."""

@@ -112,10 +112,38 @@ class Result:
     cl_history: np.ndarray
     timing: Timing
     coefficients: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))
+    wall: np.ndarray | None = None   # per wall face: gauge p, area into the fluid (2), viscous force (2)
 
     @property
     def cells(self) -> int:
         return self.grid.cells
+
+    @property
+    def seconds(self) -> float:
+        return self.timing.total
+
+    def surface(self) -> dict:
+        """Wall distributions per face: ``x``, ``y``, ``body``, ``cp`` and, viscous, ``cf``
+        along the downstream-pointing tangent (``src/jaxrans/post/forces.py:203-226``)."""
+        if self.wall is None:
+            raise ValueError("this result carries no wall loads")
+        p, sx, sy, fx, fy = (np.asarray(self.wall)[:, k] for k in range(5))
+        q = 0.5 * self.case.flow.mach ** 2
+        walls = self.grid.walls
+        out = {"x": walls.mid[:, 0], "y": walls.mid[:, 1], "body": walls.body.astype(float), "cp": p / q}
+        if not self.case.flow.inviscid:
+            length = np.hypot(sx, sy)
+            tx, ty = sy / length, -sx / length
+            sign = np.where(tx >= 0.0, 1.0, -1.0)
+            out["cf"] = sign * (fx * tx + fy * ty) / length / q
+        return out
+
+    def write(self, directory=None, extra: dict | None = None):
+        """The run's files in the reference's layout (``src/jaxrans/simulation.py:135-169``,
+        ``src/jaxrans/io/output.py:70-128``): ``<name>_metadata.json``, ``_residual.dat``,
+        ``_lift.dat``, ``_surface.dat`` and ``_fields.npz`` (U and nodes per block)."""
+        from .output import write_result
+        return write_result(self, directory, extra)
 
     @property
     def cl_spread(self) -> float:
@@ -142,8 +170,10 @@ def freestream_state(case: Case, plan: Plan) -> np.ndarray:
 def device_for(case: Case, plan: Plan):
     from .native import DevicePlan
     spec = case.grid_spec
-    return DevicePlan(plan, case.flow, case.numerics, case.implicit, spec.reference_length,
-                      tuple(spec.moment_centre[:2]))
+    dev = DevicePlan(plan, case.flow, case.numerics, case.implicit, spec.reference_length,
+                     tuple(spec.moment_centre[:2]))
+    dev.autotune()
+    return dev
 
 
 @dataclass
@@ -249,7 +279,7 @@ def march(case: Case, plan: Plan, progress=None, initial=None, device=None, max_
     return Result(case=case, grid=plan, U=U, forces=forces_of(dev.forces()), history=history,
                   cl_history=blk.cl_history,
                   timing=Timing(blk.seconds, blk.first_block, int(blk.residual.size), case.block_iters, plan.cells),
-                  coefficients=blk.coefficients)
+                  coefficients=blk.coefficients, wall=dev.wall_loads())
 
 
 def run(case: Case, grid: Plan | None = None, progress=None, on_level=None, devices=None, *, initial=None) -> Result:

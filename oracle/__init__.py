@@ -23,4 +23,4 @@ from .implicit import (  # noqa: F401
     chain_blocks_flow, chain_blocks_sa, cr_factor, cr_solve, thomas_factor, thomas_solve,
     precondition, gmres_right, hessenberg_lstsq, newton_step, NewtonState, relax,
 )
-from .forces import forces  # noqa: F401
+from .forces import forces, wall_loads  # noqa: F401

@@ -14,8 +14,9 @@ import numpy as np
 from . import numerics as nm
 
 
-def forces(U, model, length: float = 1.0, centre=(0.25, 0.0)):
-    """``(cl, cd, cm, cd_friction, fx, fy)``."""
+def wall_loads(U, model):
+    """Per wall face: gauge pressure ``(n,)``, the area vector into the fluid ``(2, n)``
+    and the viscous force on the body ``(2, n)`` (``src/jaxrans/post/forces.py:48-68``)."""
     plan, g = model.plan, model.gamma
     q = nm.prim(U[:4], g)
     p = q[3].reshape(-1)[plan.walls.cell] - 1.0 / g
@@ -27,6 +28,13 @@ def forces(U, model, length: float = 1.0, centre=(0.25, 0.0)):
         filled = np.pad(nm.fill_ghosts(q, flow_model, "characteristic"), ((0, 0), (1, 1), (1, 1)), mode="edge")
         visc = nm.viscous_fluxes(filled, plan.centres, [plan.faces_i, plan.faces_j], flow_model)
         shear = plan.walls.into_fluid * nm.wall_values(plan, tuple(v[1:3] for v in visc))
+    return p, S, shear
+
+
+def forces(U, model, length: float = 1.0, centre=(0.25, 0.0)):
+    """``(cl, cd, cm, cd_friction, fx, fy)``."""
+    plan = model.plan
+    p, S, shear = wall_loads(U, model)
     rho, u, v = model.q_inf[0], model.q_inf[1], model.q_inf[2]
     speed = np.hypot(u, v)
     pressure = -p * S

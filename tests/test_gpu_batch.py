@@ -165,3 +165,21 @@ def test_skipped_krylov_cycles_launch_nothing(cuda):
     dev.newton_steps(10)
     launched = dev.launch_count() - before
     assert 0 < launched < 10 * full
+
+
+def test_autotuned_schedule_gives_the_same_steps(cuda):
+    """The autotuner only changes the line solve's block sizes: the steps are bitwise the
+    same whatever it picks."""
+    from jaxrans_b200.native import DevicePlan
+    z, case, plan = load("c_sa")
+    runs = []
+    for tune in (False, True):
+        dev = DevicePlan(plan, case.flow, case.numerics, case.implicit)
+        if tune:
+            chosen = dev.autotune(3)
+            assert chosen["line_factor_threads"] in (64, 128, 256)
+            assert chosen["line_apply_threads"] in (64, 128, 256)
+        dev.set_state(freestream_state(case, plan), case.implicit.cfl)
+        runs.append((dev.newton_steps(8), dev.get_state()[0]))
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert np.array_equal(runs[0][1], runs[1][1])

@@ -128,3 +128,19 @@ def test_converged_forces_match_reference(cuda, name):
     assert abs(f.cl - ref["forces"][0]) < 1e-6
     assert abs(f.cd - ref["forces"][1]) < 1e-6
     assert abs(f.cm - ref["forces"][2]) < 1e-6
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_wall_loads_match_oracle(cuda, name):
+    """Per wall face: gauge pressure, area vector into the fluid and viscous force against
+    the oracle's wall loads (the arithmetic the golden forces pin), 1e-12 of each column's
+    largest entry."""
+    import oracle
+    z, case, plan, dev = device_plan(name)
+    U = z["rand0_U"]
+    got = dev.wall_loads(U)
+    p, S, shear = oracle.wall_loads(U, oracle_model(case, plan))
+    ref = np.column_stack([p, S[0], S[1], shear[0], shear[1]])
+    for k in range(5):
+        scale = max(np.abs(ref[:, k]).max(), 1e-300)
+        assert np.abs(got[:, k] - ref[:, k]).max() <= 1e-12 * scale
