@@ -69,7 +69,9 @@ typedef struct jr_plan_desc {
   /* implicit solver */
   double cfl, cfl_max, cfl_growth, cfl_cutback, cfl_min;
   double krylov_tol, krylov_success, max_relative_update;   /* max_relative_update <= 0: none */
-  int32_t krylov_subspace, krylov_restarts, preconditioner; /* preconditioner 0 none, 1 line_j */
+  int32_t krylov_subspace, krylov_restarts, preconditioner; /* preconditioner 0 none, 1 line_j (the reference's
+                                                               split 4x4 + scalar SA chains), 2 line_j_coupled
+                                                               (the SA row coupled to the mean flow: 5x5 blocks) */
   int32_t precision;                                        /* 0 fp64, 1 mixed (fp32 line factor and Krylov basis) */
   double force_length, moment_centre[2];
 } jr_plan_desc;
@@ -145,7 +147,8 @@ int jr_jvp(jr_plan* plan, const double* U, const double* v, double* Jv);
  * ResidualOperator.wave_speeds / face_wave_speeds (src/jaxrans/numerics/residual.py:169-192). */
 int jr_wave_speeds(jr_plan* plan, const double* U, double* lam);
 
-/* Factor the line_j preconditioner at (U, cfl) and apply it: z = M^-1 r.  Replaces
+/* Factor the line_j preconditioner at (U, cfl) and apply it: z = M^-1 r (the coupled
+ * form takes its SA coupling at the same U, which must stay valid until the apply).  Replaces
  * get_preconditioner("line_j")(...)(U, lambdas, cfl) and its solve
  * (src/jaxrans/solvers/preconditioners.py:291-306).  Device pointers. */
 int jr_precond_factor(jr_plan* plan, const double* U, double cfl);

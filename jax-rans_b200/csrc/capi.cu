@@ -27,6 +27,7 @@ void launch_chain_apply(const CaseDev*, const BatchDims&, bool sa, bool fp32, in
 int chain_grid_blocks(int n_chains, int n_offchain);
 bool apply_threads_valid(int threads, int max_L);
 void configure_line_kernels(int max_L);
+void launch_chain_couple(const CaseDev*, const BatchDims&, bool fp32, int out_id, int check_active, cudaStream_t);
 // krylov.cu
 void launch_gmres_init(const CaseDev*, const BatchDims&, cudaStream_t);
 void launch_cycle_start(const CaseDev*, const BatchDims&, cudaStream_t);
@@ -90,6 +91,7 @@ struct jr_plan {
   bool live_vortex = false;              // an enabled case uses the point-vortex far field
   std::vector<std::vector<int>> chain_len;   // each case's chain lengths (host copy)
   int ls_factor_threads = 128, ls_apply_threads = 128;   // the line-solve schedule in use
+  const double* factor_U = nullptr;      // the state of the last jr_precond_factor (the coupled form's)
 };
 
 static int fail(int code, const std::string& msg) {
@@ -444,11 +446,13 @@ static int upload_table(jr_plan* p) {
 static void enqueue_cycle(jr_plan* p, cudaStream_t st) {
   const CaseDev* t = p->live;
   const BatchDims& d = p->live_dims;
-  const bool sa = p->nvar == 5, pre = p->cfg.preconditioner == 1;
+  const bool sa = p->nvar == 5, pre = p->cfg.preconditioner >= 1;
+  const bool coupled = sa && p->cfg.preconditioner == 2;   // the 5x5 form: one more SA chain solve
   for (int j = 0; j < p->m; ++j) {
     const int src = j == 0 ? B_RR : B_W;
     if (pre) launch_chain_apply(t, d, sa, p->mixed, src, 1, j, B_Z, 1, st);
     else launch_scale_copy(t, d, p->mixed, src, 1, j, B_Z, 1, st);
+    if (coupled) launch_chain_couple(t, d, p->mixed, B_Z, 1, st);
     // the tangent ghosts: a single case's J.v tiles evaluate their halo's ghosts
     // themselves (one launch fewer on a latency-bound step); a batch, whose tiles run in
     // many waves, fills them in one launch, as does any case that needs the point-vortex
@@ -462,6 +466,7 @@ static void enqueue_cycle(jr_plan* p, cudaStream_t st) {
   launch_combine(t, d, p->mixed, st);
   if (pre) launch_chain_apply(t, d, sa, p->mixed, B_TMP, 0, -1, B_Z, 1, st);
   else launch_scale_copy(t, d, false, B_TMP, 0, -1, B_Z, 1, st);
+  if (coupled) launch_chain_couple(t, d, p->mixed, B_Z, 1, st);
   launch_cycle_end(t, d, st);
 }
 
@@ -481,7 +486,7 @@ static int enqueue_step(jr_plan* p) {
   const CaseDev* t = p->live;
   const BatchDims& d = p->live_dims;
   if (d.n_cases == 0) return JR_OK;   // no enabled case: an empty step
-  const bool sa = p->nvar == 5, pre = p->cfg.preconditioner == 1;
+  const bool sa = p->nvar == 5, pre = p->cfg.preconditioner >= 1;
   cudaStream_t st = p->st;
   launch_ghosts(t, d, -1, 0, st);
   launch_residual(t, d, p->visc, true, B_R, st);
@@ -696,6 +701,7 @@ int jr_precond_factor(jr_plan* plan, const double* U, double cfl) {
   if (!(cfl > 0.0)) return fail(JR_EINVAL, "cfl must be positive");
   for (int k = 0; k < plan->n_cases; ++k)
     cudaMemcpyAsync(&plan->sc[k].cfl, &cfl, sizeof(double), cudaMemcpyHostToDevice, plan->st);
+  plan->factor_U = U;
   Adhoc a(plan);
   a.vec(&CaseDev::U, U);
   const CaseDev* t = a.upload();
@@ -711,7 +717,10 @@ int jr_precond_apply(jr_plan* plan, const double* r, double* z) {
   Adhoc a(plan);
   a.vec(&CaseDev::r, r);
   a.vec(&CaseDev::z, z);
-  launch_chain_apply(a.upload(), plan->dims, plan->nvar == 5, plan->mixed, B_RR, 0, -1, B_Z, 0, plan->st);
+  if (plan->factor_U) a.vec(&CaseDev::U, plan->factor_U);   // the coupling is taken at the factor's state
+  const CaseDev* t = a.upload();
+  launch_chain_apply(t, plan->dims, plan->nvar == 5, plan->mixed, B_RR, 0, -1, B_Z, 0, plan->st);
+  if (plan->nvar == 5 && plan->cfg.preconditioner == 2) launch_chain_couple(t, plan->dims, plan->mixed, B_Z, 0, plan->st);
   return cuda_check("jr_precond_apply");
 }
 

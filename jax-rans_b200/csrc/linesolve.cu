@@ -504,6 +504,123 @@ __global__ void __launch_bounds__(LS_MAX_THREADS) k_cr_apply(const CaseDev* __re
   }
 }
 
+// ------------------------------------------------------------------------------------
+// The coupled (5x5) form of the line blocks: the SA row also depends on the neighbours'
+// mean flow, through half the Jacobian of its convective flux rho nu_hat V.S,
+// [-nu_hat vn, nu_hat Sx, nu_hat Sy, 0] at the neighbour's state (the mean-flow rows do
+// not depend on rho nu_hat).  The blocks are block lower triangular, so the solve is the
+// split solve followed by one more SA chain solve: z_sa -= M_sa^-1 (C z_flow), C the
+// coupling along the chain.  This kernel does that second step, one CTA per chain, with
+// the SA factor of the split form and the same cyclic-reduction formulas.
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ double sa_coupling_dot(const Canvas& cv, const Physics& P, const double* U,
+                                                  const double* z, int sign, int face, int nb) {
+  if (sign == 0) return 0.0;
+  double sx, sy, q[5];
+  face_vector(cv, face, sx, sy);
+  sx *= sign;
+  sy *= sign;
+  prim_at(cv, P, U, nb, q);
+  const int N = cv.ncanvas();
+  const double nu = q[4], vn = q[1] * sx + q[2] * sy;
+  return 0.5 * ((-nu * vn) * z[nb] + (nu * sx) * z[N + nb] + (nu * sy) * z[2 * N + nb]);
+}
+
+template <class TF>
+__global__ void __launch_bounds__(LS_MAX_THREADS) k_cr_sa_couple(const CaseDev* __restrict__ cases, int out_id,
+                                                                 int check_active) {
+  __shared__ CaseDev scase;
+  if (idle_block(cases[blockIdx.y], (int)blockIdx.x >= cases[blockIdx.y].c.n_chains, check_active)) return;
+  const CaseDev& cd = stage_case(cases, blockIdx.y, &scase);
+  const Canvas& cv = cd.c;
+  const Physics& P = cd.P;
+  const double* __restrict__ U = cd.U;
+  double* __restrict__ z = buf(cd, out_id);
+  const TF* __restrict__ fsa = (const TF*)cd.fsa;
+  const int N = cv.ncanvas(), n = cv.n_chains, c = blockIdx.x;
+  const int L = cv.ch_len[c];
+  const TF* Fs = fsa + (size_t)cv.ch_fbase[c] * 5;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TF* bs = reinterpret_cast<TF*>(smem_raw);   // level-concatenated rows, one scalar each
+  // 1. the right-hand side C z_flow along the chain
+  for (int k = threadIdx.x; k < L; k += blockDim.x) {
+    double t = 0.0;
+    if (k > 0)
+      t += sa_coupling_dot(cv, P, U, z, cv.ch_down_sign[(k - 1) * n + c], cv.ch_down_face[(k - 1) * n + c],
+                           cv.ch_cells[(k - 1) * n + c]);
+    if (k + 1 < L)
+      t += sa_coupling_dot(cv, P, U, z, cv.ch_up_sign[k * n + c], cv.ch_up_face[k * n + c],
+                           cv.ch_cells[(k + 1) * n + c]);
+    bs[k] = TF(t);
+  }
+  __syncthreads();
+  // 2. the SA chain solve (the split apply's scalar formulas)
+  int rows = L;
+  size_t offs = 0, boff = 0;
+  while (rows > 1) {
+    const int ne = (rows + 1) / 2, no = rows / 2;
+    const TF* sal = Fs + offs + 3 * ne;
+    const TF* sga = sal + no;
+    TF* b = bs + boff;
+    TF* bn = bs + boff + rows;
+    for (int o = threadIdx.x; o < no; o += blockDim.x) {
+      TF bx = 2 * o + 2 < rows ? b[2 * o + 2] : TF(0);
+      bn[o] = b[2 * o + 1] - sal[o] * b[2 * o] - sga[o] * bx;
+    }
+    __syncthreads();
+    offs += (size_t)3 * ne + (size_t)2 * no;
+    boff += rows;
+    rows = no;
+  }
+  if (threadIdx.x == 0) bs[boff] = Fs[offs] * bs[boff];
+  __syncthreads();
+  int depth = 0;
+  for (int m = L; m > 1; m >>= 1) ++depth;
+  for (int lev = depth - 1; lev >= 0; --lev) {
+    int rws = L;
+    size_t ofs = 0, bo_ = 0;
+    for (int k = 0; k < lev; ++k) {
+      int ne_ = (rws + 1) / 2, no_ = rws / 2;
+      ofs += (size_t)3 * ne_ + (size_t)2 * no_;
+      bo_ += rws;
+      rws = no_;
+    }
+    const int ne = (rws + 1) / 2, no = rws / 2;
+    const TF* si = Fs + ofs;
+    TF* b = bs + bo_;
+    const TF* x = bs + bo_ + rws;   // the next level's solution (the odd rows)
+    TF xe[4];
+    int cnt = 0;
+    for (int e = threadIdx.x; e < ne; e += blockDim.x, ++cnt) {
+      TF xps = e >= 1 ? x[e - 1] : TF(0);
+      TF xns = e < no ? x[e] : TF(0);
+      xe[cnt] = si[e] * (b[2 * e] - si[ne + e] * xps - si[2 * ne + e] * xns);
+    }
+    __syncthreads();
+    cnt = 0;
+    for (int e = threadIdx.x; e < ne; e += blockDim.x, ++cnt) b[2 * e] = xe[cnt];
+    for (int o = threadIdx.x; o < no; o += blockDim.x) b[2 * o + 1] = x[o];
+    __syncthreads();
+  }
+  // 3. z_sa -= the solution
+  for (int k = threadIdx.x; k < L; k += blockDim.x) {
+    const int cell = cv.ch_cells[k * n + c];
+    z[4 * N + cell] -= double(bs[k]);
+  }
+}
+
+size_t cr_couple_smem(int max_L, bool fp32) { return (size_t)2 * max_L * (fp32 ? 4 : 8) + 64; }
+
+// z_sa -= M_sa^-1 (C z_flow) on every chain: the coupled form's second SA solve
+void launch_chain_couple(const CaseDev* cases, const BatchDims& d, bool fp32, int out_id, int check_active,
+                         cudaStream_t st) {
+  dim3 grid(d.chain_blocks, d.n_cases);
+  const int th = d.ls_apply_threads > 0 ? d.ls_apply_threads : LS_THREADS;
+  const size_t smem = cr_couple_smem(d.max_L, fp32);
+  if (fp32) k_cr_sa_couple<float><<<grid, th, smem, st>>>(cases, out_id, check_active);
+  else k_cr_sa_couple<double><<<grid, th, smem, st>>>(cases, out_id, check_active);
+}
+
 size_t cr_apply_smem(int max_L, bool fp32) { return (size_t)2 * max_L * 5 * (fp32 ? 4 : 8) + 64; }
 
 void launch_chain_factor(const CaseDev* cases, const BatchDims& d, bool sa, bool fp32, cudaStream_t st) {
@@ -545,6 +662,10 @@ int chain_grid_blocks(int n_chains, int n_offchain) { return n_chains + offchain
 bool apply_threads_valid(int threads, int max_L) { return 4 * threads >= (max_L + 1) / 2 && threads <= LS_MAX_THREADS; }
 
 void configure_line_kernels(int max_L) {
+  cudaFuncSetAttribute(k_cr_sa_couple<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)cr_couple_smem(max_L, false));
+  cudaFuncSetAttribute(k_cr_sa_couple<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)cr_couple_smem(max_L, true));
   size_t s8 = cr_apply_smem(max_L, false), s4 = cr_apply_smem(max_L, true);
   cudaFuncSetAttribute(k_cr_apply<double, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s8);
   cudaFuncSetAttribute(k_cr_apply<double, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s8);

@@ -23,7 +23,7 @@ TURBULENCE_MODELS = ("sa_noft2", "sa_noft2_qcr")
 SOLVERS = ("explicit", "implicit")
 FLUXES = ("hllc", "roe")
 LIMITERS = ("minmod", "none", "van_albada", "van_albada_smooth")
-PRECONDITIONERS = ("line_j", "none")
+PRECONDITIONERS = ("line_j", "line_j_coupled", "none")
 FAR_FIELDS = ("characteristic", "characteristic_point_vortex")
 PRECISIONS = ("fp64", "mixed")
 

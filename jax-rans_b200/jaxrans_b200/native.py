@@ -196,7 +196,7 @@ def fill_desc(d: PlanDesc, plan: Plan, flow: FlowConditions, numerics: NumericsC
     d.krylov_tol, d.krylov_success = imp.krylov_tol, imp.krylov_success
     d.max_relative_update = -1.0 if imp.max_relative_update is None else imp.max_relative_update
     d.krylov_subspace, d.krylov_restarts = imp.krylov_subspace, imp.krylov_restarts
-    d.preconditioner = 1 if imp.preconditioner == "line_j" else 0
+    d.preconditioner = {"none": 0, "line_j": 1, "line_j_coupled": 2}[imp.preconditioner]
     d.precision = 1 if imp.precision == "mixed" else 0
     d.force_length = force_length
     d.moment_centre[0], d.moment_centre[1] = moment_centre[0], moment_centre[1]

@@ -241,6 +241,66 @@ def precondition(U, lam, cfl, model, solver: str = "cr"):
     return apply
 
 
+def chain_coupling_sa(U, model):
+    """The SA row's coupling to the mean flow in the coupled (5x5) line blocks:
+    ``(lower, upper)`` ``(L, n_lines, 4)``, half the Jacobian of the SA convective flux
+    ``rho nu_hat V.S`` with respect to the neighbour's (rho, rho u, rho v, rho E) at the
+    neighbour's state, ``[-nu_hat vn, nu_hat Sx, nu_hat Sy, 0]``, with the link's face
+    vector and sign exactly as the mean-flow blocks use them (``chain_blocks_flow``).
+    The mean-flow rows do not depend on rho nu_hat, so the 5x5 blocks are block lower
+    triangular.  This coupled form is the north-star variant of ``line_j``; the
+    reference has only the split form (``preconditioners.py:291-306``)."""
+    plan, g = model.plan, model.gamma
+    ch = plan.chains
+    q = nm.prim(U, g)
+    S = (plan.faces_i, plan.faces_j)
+
+    def coupling(side, sign, nb):
+        s = _faces(S, ch, side)
+        sx, sy = sign * s[0], sign * s[1]
+        nu = nb[4]
+        vn = nb[1] * sx + nb[2] * sy
+        row = 0.5 * np.stack([-nu * vn, nu * sx, nu * sy, np.zeros_like(vn)])
+        return np.transpose(np.where(sign != 0, row, 0.0), (2, 1, 0))
+
+    chains = _gather(q, ch)
+    above = np.concatenate([chains[:, :, 1:], chains[:, :, -1:]], axis=2)
+    upper = coupling("up", ch.up_sign, above)
+    below = coupling("down", ch.down_sign, chains)
+    lower = np.concatenate([np.zeros_like(below[:1]), below[:-1]], axis=0)
+    return lower, upper
+
+
+def precondition_coupled(U, lam, cfl, model):
+    """``r -> M^-1 r`` with the coupled 5x5 line blocks: the mean flow solved first, then
+    the SA chains with the right-hand side ``r_sa - C z_flow`` (block forward
+    substitution of the block lower-triangular blocks)."""
+    split = precondition(U, lam, cfl, model)
+    ch = model.plan.chains
+    valid = ch.cells >= 0
+    found = np.full(model.plan.n_canvas, -1, dtype=np.int64)
+    found[ch.cells[valid]] = np.flatnonzero(valid)
+    lower, upper = chain_coupling_sa(U, model)
+    sa_factor = cr_factor(*chain_blocks_sa(U, lam, cfl, model))
+
+    def apply(r):
+        z = split(r)
+        zf = np.where(valid, _gather(z[:4], ch), 0.0)                       # (4, n_lines, L)
+        zf = np.transpose(zf, (2, 1, 0))                                     # (L, n_lines, 4)
+        below = np.concatenate([np.zeros_like(zf[:1]), zf[:-1]], axis=0)
+        above = np.concatenate([zf[1:], np.zeros_like(zf[:1])], axis=0)
+        cz = np.sum(lower * below, axis=-1) + np.sum(upper * above, axis=-1)   # (L, n_lines)
+        rhs = np.where(valid, _gather(r[4:5], ch), 0.0)[0].T - cz
+        x = cr_solve(sa_factor, rhs[:, :, None])[:, :, 0].T                # (n_lines, L)
+        out = z.copy()
+        flat = out[4].reshape(-1)
+        flat[ch.cells[valid]] = x[valid]
+        out[4] = flat.reshape(out[4].shape)
+        return out
+
+    return apply
+
+
 # --- GMRES (krylov.py:34-137) ---------------------------------------------------------
 
 

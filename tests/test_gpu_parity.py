@@ -144,3 +144,31 @@ def test_wall_loads_match_oracle(cuda, name):
     for k in range(5):
         scale = max(np.abs(ref[:, k]).max(), 1e-300)
         assert np.abs(got[:, k] - ref[:, k]).max() <= 1e-12 * scale
+
+
+@pytest.mark.parametrize("name", ["c_sa", "o_sa_qcr"])
+def test_coupled_line_preconditioner_matches_oracle(cuda, name):
+    """The coupled (5x5) line blocks -- the north-star form; the reference has the split
+    form only -- against the oracle's coupled solve (itself checked against dense block
+    solves), 1e-10 as the split solve."""
+    from oracle import implicit as im
+    z, case, plan, dev = device_plan(name, preconditioner="line_j_coupled")
+    U, r = z["rand0_U"], z["rand0_prec_r"]
+    model = oracle_model(case, plan)
+    ref = im.precondition_coupled(U, nm.wave_speeds(U, model), 25.0, model)(r)
+    out = dev.precondition(U, 25.0, r)
+    assert rel(out, ref) < 1e-10
+
+
+def test_coupled_form_converges_to_the_same_forces(cuda):
+    """A preconditioner does not move the fixed point: the coupled form's converged
+    forces are the split form's (the reference's converged run) to 1e-6."""
+    from jaxrans_b200.solver import march
+    ref = converged("c_sa")
+    if ref is None:
+        pytest.skip("no converged golden")
+    z, case, plan, dev = device_plan("c_sa", preconditioner="line_j_coupled")
+    result = march(case, plan, device=dev)
+    assert result.history.reason in ("converged", "settled")
+    assert abs(result.forces.cl - ref["forces"][0]) < 1e-6
+    assert abs(result.forces.cd - ref["forces"][1]) < 1e-6
