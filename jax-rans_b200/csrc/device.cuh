@@ -25,6 +25,7 @@ enum Status : int {
   ST_NONFINITE = 1,       // a non-finite value met in a reduction
   ST_REJECTED = 2,        // the last Newton step was rejected
   ST_GMRES_BREAKDOWN = 4, // an Arnoldi vector of zero norm
+  ST_STAGE_FAILED = 8,    // the line solve's staged copy of a factor failed (sticky: kept across steps)
 };
 
 struct Canvas {
@@ -166,6 +167,7 @@ struct BatchDims {
   int cgs_blocks;           // blocks of the basis passes
   int ls_factor_threads;    // threads per chain of the line factor and of the line solve:
   int ls_apply_threads;     // the schedule the plan's autotuner picked (results do not depend on it)
+  int ls_apply_stage;       // 1: the line solve first copies its chain's factor into shared memory
 };
 
 constexpr int LS_MAX_THREADS = 256;   // the largest line-solve block

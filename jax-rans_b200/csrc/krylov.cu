@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_gmres_init(const CaseDev* __res
     sc->rnorm = sc->bnorm;
     sc->cycle = 0;
     sc->active = 1;
-    sc->status = 0;
+    sc->status &= ST_STAGE_FAILED;
   }
 }
 

@@ -331,11 +331,112 @@ __host__ __device__ __forceinline__ int offchain_blocks(int n_offchain) {
   return b < 1 ? 1 : (b > 64 ? 64 : b);
 }
 
+// ------------------------------------------------------------------------------------
+// Staging a chain's factor.  A solve reads every entry of its chain's factor once, level
+// by level, and each level waits on its loads before the next barrier: at one chain per
+// CTA the solve is a chain of L2 round trips.  The staged form instead copies the chain's
+// flow factor (contiguous, 16-byte aligned, a multiple of 64 bytes) into shared memory
+// with one bulk asynchronous copy issued at the start, completed on an mbarrier while
+// the threads gather the right-hand side, and its SA scalars with plain loads; the
+// levels then read shared memory.  It costs the factor's size in shared memory per CTA
+// (fewer CTAs per SM), so the plan's autotuner times both forms.
+// ------------------------------------------------------------------------------------
+// entries of a chain's flow factor: every level's even-row blocks (inverse, lower, upper)
+// and odd-row multipliers (alpha, gamma), then the last row's inverse
+__host__ __device__ __forceinline__ int cr_chain_entries(int L) {
+  int e = 16, rows = L;
+  while (rows > 1) {
+    const int ne = (rows + 1) / 2, no = rows / 2;
+    e += 48 * ne + 32 * no;
+    rows = no;
+  }
+  return e;
+}
+
+// entries of a chain's SA factor (three scalars per even row, two per odd row, the last)
+__host__ __device__ __forceinline__ int cr_chain_sa_entries(int L) {
+  int e = 1, rows = L;
+  while (rows > 1) {
+    const int ne = (rows + 1) / 2, no = rows / 2;
+    e += 3 * ne + 2 * no;
+    rows = no;
+  }
+  return e;
+}
+
+constexpr int STAGE_WAIT_TRIES = 1 << 20;      // x a suspend hint of 1 us: about a second
+constexpr unsigned STAGE_WAIT_HINT_NS = 1000;
+// dynamic shared memory of the staged solve at most: the opt-in limit of one CTA (227 KB,
+// static and dynamic together) less room for the kernel's static shared memory
+constexpr size_t SMEM_PER_BLOCK_MAX = 232448 - 2048;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// One thread: arm the barrier for `bytes` and start the bulk copy src (global) -> dst
+// (this CTA's shared memory).  Both addresses 16-byte aligned, bytes a multiple of 16
+// and below 2^20 (the barrier's transaction count).
+__device__ __forceinline__ void stage_issue(unsigned long long* bar, void* dst, const void* src, unsigned bytes) {
+  const unsigned b = smem_u32(bar);
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(b)
+               : "memory");
+}
+
+// Wait for the barrier's first phase, a bounded number of tries; false if it gave up.
+__device__ __forceinline__ bool stage_wait(unsigned long long* bar) {
+  const unsigned b = smem_u32(bar);
+  for (int i = 0; i < STAGE_WAIT_TRIES; ++i) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(b), "r"(0u), "r"(STAGE_WAIT_HINT_NS)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// Shared memory of the line solve: [flow factor | SA factor] when staged, then the
+// level-concatenated right-hand sides (at most 2 L rows of 5).  The staged space is
+// the largest footprint of any chain up to max_L cells.
+struct ApplyLayout {
+  int ent_f, ent_s;       // staged entries (0 unstaged)
+  size_t off_s, off_b;    // byte offsets of the SA factor and of the right-hand sides
+  size_t bytes;           // dynamic shared memory of a CTA
+};
+
+static ApplyLayout apply_layout(int max_L, bool fp32, bool stage) {
+  const size_t tb = fp32 ? 4 : 8;
+  ApplyLayout a{0, 0, 0, 0, 0};
+  if (stage) {
+    for (int l = 1; l <= max_L; ++l) {
+      a.ent_f = cr_chain_entries(l) > a.ent_f ? cr_chain_entries(l) : a.ent_f;
+      a.ent_s = cr_chain_sa_entries(l) > a.ent_s ? cr_chain_sa_entries(l) : a.ent_s;
+    }
+    a.off_s = ((size_t)a.ent_f * tb + 127) / 128 * 128;
+    a.off_b = a.off_s + ((size_t)a.ent_s * tb + 15) / 16 * 16;
+  }
+  a.bytes = a.off_b + (size_t)2 * max_L * 5 * tb + 64;
+  return a;
+}
+
+// whether the staged line solve fits one CTA's shared memory for chains up to max_L
+bool apply_stage_fits(int max_L, bool fp32) { return apply_layout(max_L, fp32, true).bytes <= SMEM_PER_BLOCK_MAX; }
+
 // src_id: the right-hand side buffer; scale_on: multiply it by the case's 1/|w|;
 // vout_j >= 0: also write the scaled input to basis vector j; out_id: the result.
-template <class TF, class TV, bool SA>
+// STAGE: the chain's factor is first copied into shared memory (ent_f, ent_s entries
+// reserved at byte offsets 0 and off_s; the right-hand sides at off_b).
+template <class TF, class TV, bool SA, bool STAGE>
 __global__ void __launch_bounds__(LS_MAX_THREADS) k_cr_apply(const CaseDev* __restrict__ cases, int src_id, int scale_on,
-                                                         int vout_j, int out_id, int check_active) {
+                                                         int vout_j, int out_id, int check_active, int ent_f,
+                                                         int ent_s, int off_s, int off_b) {
   __shared__ CaseDev scase;
   {
     const Canvas& g = cases[blockIdx.y].c;
@@ -370,12 +471,28 @@ __global__ void __launch_bounds__(LS_MAX_THREADS) k_cr_apply(const CaseDev* __re
     }
     return;
   }
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) unsigned long long stage_bar;
   const int c = blockIdx.x;
   const int L = cv.ch_len[c];
-  TF* bs = reinterpret_cast<TF*>(smem_raw);   // [level-concatenated rows][5]
-  const TF* F = fflow + (size_t)cv.ch_fbase[c] * 80;
-  const TF* Fs = fsa + (size_t)cv.ch_fbase[c] * 5;
+  TF* bs = reinterpret_cast<TF*>(smem_raw + off_b);   // [level-concatenated rows][5]
+  const TF* Fg = fflow + (size_t)cv.ch_fbase[c] * 80;
+  const TF* Fsg = fsa + (size_t)cv.ch_fbase[c] * 5;
+  TF* const sf = reinterpret_cast<TF*>(smem_raw);
+  TF* const ss = reinterpret_cast<TF*>(smem_raw + off_s);
+  const TF* F = STAGE ? sf : Fg;
+  const TF* Fs = STAGE ? ss : Fsg;
+  if constexpr (STAGE) {
+    const int ef = cr_chain_entries(L), es = cr_chain_sa_entries(L);
+    const bool aligned = ((smem_u32(sf) | (unsigned)reinterpret_cast<uintptr_t>(Fg)) & 15u) == 0;
+    if (ef > ent_f || (SA && es > ent_s) || !aligned) {   // not reached: sized for max_L, 16-byte rows
+      if (threadIdx.x == 0) atomicOr(&cd.sc->status, (int)ST_STAGE_FAILED);
+      return;
+    }
+    if (threadIdx.x == 0) stage_issue(&stage_bar, sf, Fg, (unsigned)(ef * sizeof(TF)));
+    if constexpr (SA)
+      for (int k = threadIdx.x; k < es; k += blockDim.x) ss[k] = Fsg[k];
+  }
   // gather the right-hand side
   for (int k = threadIdx.x; k < L; k += blockDim.x) {
     const int cell = cv.ch_cells[k * n + c];
@@ -390,6 +507,14 @@ __global__ void __launch_bounds__(LS_MAX_THREADS) k_cr_apply(const CaseDev* __re
     }
   }
   __syncthreads();
+  if constexpr (STAGE) {
+    const bool ok = stage_wait(&stage_bar);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) atomicOr(&cd.sc->status, (int)ST_STAGE_FAILED);
+      stage_wait(&stage_bar);   // a copy still in flight lands in this CTA's shared memory
+      return;
+    }
+  }
   // reduce: b_odd <- b_odd - alpha b_even - gamma b_next_even, level by level
   int rows = L;
   size_t off = 0, offs = 0, boff = 0;
@@ -540,7 +665,7 @@ __global__ void __launch_bounds__(LS_MAX_THREADS) k_cr_sa_couple(const CaseDev* 
   const int N = cv.ncanvas(), n = cv.n_chains, c = blockIdx.x;
   const int L = cv.ch_len[c];
   const TF* Fs = fsa + (size_t)cv.ch_fbase[c] * 5;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   TF* bs = reinterpret_cast<TF*>(smem_raw);   // level-concatenated rows, one scalar each
   // 1. the right-hand side C z_flow along the chain
   for (int k = threadIdx.x; k < L; k += blockDim.x) {
@@ -621,7 +746,6 @@ void launch_chain_couple(const CaseDev* cases, const BatchDims& d, bool fp32, in
   else k_cr_sa_couple<double><<<grid, th, smem, st>>>(cases, out_id, check_active);
 }
 
-size_t cr_apply_smem(int max_L, bool fp32) { return (size_t)2 * max_L * 5 * (fp32 ? 4 : 8) + 64; }
 
 void launch_chain_factor(const CaseDev* cases, const BatchDims& d, bool sa, bool fp32, cudaStream_t st) {
   dim3 grid(d.chain_blocks, d.n_cases);
@@ -639,12 +763,26 @@ template <class TF, class TV>
 static void apply_t(const CaseDev* cases, const BatchDims& d, bool sa, int src_id, int scale_on, int vout_j, int out_id,
                     int check_active, cudaStream_t st) {
   dim3 grid(d.chain_blocks, d.n_cases);
-  size_t smem = cr_apply_smem(d.max_L, sizeof(TF) == 4);
+  const bool fp32 = sizeof(TF) == 4;
+  const bool stage = d.ls_apply_stage && apply_stage_fits(d.max_L, fp32);
+  const ApplyLayout a = apply_layout(d.max_L, fp32, stage);
   const int th = d.ls_apply_threads > 0 ? d.ls_apply_threads : LS_THREADS;
-  if (sa)
-    k_cr_apply<TF, TV, true><<<grid, th, smem, st>>>(cases, src_id, scale_on, vout_j, out_id, check_active);
-  else
-    k_cr_apply<TF, TV, false><<<grid, th, smem, st>>>(cases, src_id, scale_on, vout_j, out_id, check_active);
+  const int os = (int)a.off_s, ob = (int)a.off_b;
+  if (stage) {
+    if (sa)
+      k_cr_apply<TF, TV, true, true><<<grid, th, a.bytes, st>>>(cases, src_id, scale_on, vout_j, out_id, check_active,
+                                                                a.ent_f, a.ent_s, os, ob);
+    else
+      k_cr_apply<TF, TV, false, true><<<grid, th, a.bytes, st>>>(cases, src_id, scale_on, vout_j, out_id, check_active,
+                                                                 a.ent_f, a.ent_s, os, ob);
+  } else {
+    if (sa)
+      k_cr_apply<TF, TV, true, false><<<grid, th, a.bytes, st>>>(cases, src_id, scale_on, vout_j, out_id, check_active,
+                                                                 0, 0, 0, 0);
+    else
+      k_cr_apply<TF, TV, false, false><<<grid, th, a.bytes, st>>>(cases, src_id, scale_on, vout_j, out_id,
+                                                                  check_active, 0, 0, 0, 0);
+  }
 }
 
 // z = M^-1 (scale * src) for every case; vout_j >= 0 writes the scaled input to basis
@@ -666,11 +804,16 @@ void configure_line_kernels(int max_L) {
                        (int)cr_couple_smem(max_L, false));
   cudaFuncSetAttribute(k_cr_sa_couple<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)cr_couple_smem(max_L, true));
-  size_t s8 = cr_apply_smem(max_L, false), s4 = cr_apply_smem(max_L, true);
-  cudaFuncSetAttribute(k_cr_apply<double, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s8);
-  cudaFuncSetAttribute(k_cr_apply<double, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s8);
-  cudaFuncSetAttribute(k_cr_apply<float, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s4);
-  cudaFuncSetAttribute(k_cr_apply<float, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s4);
+  const int s8 = (int)apply_layout(max_L, false, false).bytes, s4 = (int)apply_layout(max_L, true, false).bytes;
+  const int most = (int)SMEM_PER_BLOCK_MAX;
+  cudaFuncSetAttribute(k_cr_apply<double, double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8);
+  cudaFuncSetAttribute(k_cr_apply<double, double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8);
+  cudaFuncSetAttribute(k_cr_apply<float, float, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s4);
+  cudaFuncSetAttribute(k_cr_apply<float, float, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s4);
+  cudaFuncSetAttribute(k_cr_apply<double, double, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+  cudaFuncSetAttribute(k_cr_apply<double, double, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+  cudaFuncSetAttribute(k_cr_apply<float, float, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+  cudaFuncSetAttribute(k_cr_apply<float, float, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
 }
 
 }  // namespace jr

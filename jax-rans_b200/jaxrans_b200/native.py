@@ -62,7 +62,7 @@ EXPORTS = ("jr_plan_create", "jr_plan_destroy", "jr_last_error", "jr_plan_sizes"
            "jr_forces", "jr_state_set_device", "jr_graph_kernels", "jr_time_kernels", "jr_plan_set_stream",
            "jr_batch_create", "jr_plan_cases", "jr_case_sizes", "jr_case_enable", "jr_case_set_inflow",
            "jr_case_state_set", "jr_case_state_get", "jr_residual_noalloc", "jr_case_load",
-           "jr_launch_count", "jr_autotune", "jr_wall_loads")
+           "jr_launch_count", "jr_autotune", "jr_line_schedule", "jr_wall_loads")
 
 TIMED_KERNELS = ("residual_tile", "jvp_tile", "ghosts_tangent", "line_apply", "line_factor", "cgs2_full_basis")
 
@@ -107,6 +107,7 @@ def load_library(path: Path | None = None) -> C.CDLL:
         "jr_graph_kernels": (C.c_int, [vp, C.POINTER(C.c_int64)]),
         "jr_launch_count": (C.c_int, [vp, C.POINTER(C.c_int64)]),
         "jr_autotune": (C.c_int, [vp, C.c_int32, _i32p]),
+        "jr_line_schedule": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32]),
         "jr_wall_loads": (C.c_int, [vp, vp, vp]),
         "jr_time_kernels": (C.c_int, [vp, C.c_int32, _f64p]),
         "jr_plan_set_stream": (C.c_int, [vp, vp]),
@@ -429,11 +430,18 @@ class DevicePlan:
         return int(n.value)
 
     def autotune(self, reps: int = 10) -> dict:
-        """Pick the line factor's and line solve's block sizes by timing them (results do
-        not depend on the choice)."""
-        out = np.zeros(2, dtype=np.int32)
+        """Pick the line factor's and line solve's block sizes, and whether the solve
+        stages its factor in shared memory, by timing them (results do not depend on the
+        choice)."""
+        out = np.zeros(3, dtype=np.int32)
         _check(self.lib, self.lib.jr_autotune(self.handle, int(reps), _ptr(out, _i32p)), "jr_autotune")
-        return {"line_factor_threads": int(out[0]), "line_apply_threads": int(out[1])}
+        return {"line_factor_threads": int(out[0]), "line_apply_threads": int(out[1]),
+                "line_apply_staged": bool(out[2])}
+
+    def line_schedule(self, factor_threads: int = 128, apply_threads: int = 128, staged: bool = False) -> None:
+        """Set the line-solve schedule by hand (``jr_line_schedule``)."""
+        _check(self.lib, self.lib.jr_line_schedule(self.handle, int(factor_threads), int(apply_threads),
+                                                   int(bool(staged))), "jr_line_schedule")
 
     def launch_count(self) -> int:
         """Kernels launched by this plan's Newton steps so far (skipped cycles not counted)."""

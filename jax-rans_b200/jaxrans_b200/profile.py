@@ -2,10 +2,12 @@
 to run under a profiler.
 
     python -m jaxrans_b200.profile [WORKLOAD] [--precision fp64|mixed] [--steps N]
-                                   [--time]
+                                   [--time] [--line-schedule F,A,S]
 
 Prints the residual norms of the steps; ``--time`` also prints the live CUDA-event times
-of the hot kernels (``jr_time_kernels``).
+of the hot kernels (``jr_time_kernels``); ``--line-schedule`` replaces the autotuner's
+choice by the line factor's and line solve's threads per chain and the solve's form
+(``jr_line_schedule``: S = 1 staged).
 """
 
 from __future__ import annotations
@@ -24,6 +26,7 @@ def main(argv=None) -> int:
     p.add_argument("--precision", default="fp64", choices=("fp64", "mixed"))
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--time", action="store_true")
+    p.add_argument("--line-schedule", default=None, metavar="F,A,S")
     args = p.parse_args(argv)
     prec = {"implicit.precision": args.precision}
     if args.workload in BATCHES:
@@ -42,6 +45,9 @@ def main(argv=None) -> int:
         plan = case.grid()
         dev = device_for(case, plan)
         dev.set_state(freestream_state(case, plan), case.implicit.cfl)
+    if args.line_schedule:
+        f, a, s = (int(x) for x in args.line_schedule.split(","))
+        dev.line_schedule(f, a, bool(s))
     first = min(3, args.steps)
     print(dev.newton_steps(first))
     if args.steps > first:
