@@ -194,10 +194,10 @@ int jr_newton_steps_async(jr_plan* plan, int32_t n_steps, double* history_device
 
 /* The plan's autotuner: times the line factor and the line solve with each block size the
  * longest chain allows (64, 128, 256 threads per chain, reps launches each, at the plan's
- * state), and the solve in both forms (its factor read level by level from global memory,
- * or staged into shared memory by one bulk asynchronous copy where it fits), and keeps the
- * fastest; chosen (3 values, may be NULL) receives the factor's threads, the solve's
- * threads and the solve's form (1 staged).  Results do not depend on the schedule (each
+ * state), and the solve in each form (its factor read level by level from global memory,
+ * or, forms s = 1..4, staged into shared memory by one bulk asynchronous copy from level
+ * s-1 of the longest chain, where that fits), and keeps the fastest; chosen (3 values,
+ * may be NULL) receives the factor's threads, the solve's threads and the solve's form.  Results do not depend on the schedule (each
  * row's arithmetic is the same).  The tile shape of the residual is not tuned: it sets
  * the order of the residual norm's partial sums.  Overwrites the plan's preconditioner
  * factor (the next Newton step makes its own).  Replaces the reference's reliance on
@@ -206,8 +206,8 @@ int jr_autotune(jr_plan* plan, int32_t reps, int32_t* chosen);
 
 /* Sets the line-solve schedule the autotuner would pick: factor_threads and apply_threads
  * in {64, 128, 256} (4 x apply_threads at least the longest chain's even rows), and
- * apply_stage 1 for the staged solve (JR_EINVAL where the longest chain's factor does
- * not fit one block's shared memory).  Results do not depend on it.  A staged copy that
+ * apply_stage the solve's form, 0 to 4 (JR_EINVAL where the staged part does not fit
+ * one block's shared memory).  Results do not depend on it.  A staged copy that
  * fails sets status bit 8 of its case (kept until the plan's state is set again); it is
  * not expected.  No counterpart in the reference. */
 int jr_line_schedule(jr_plan* plan, int32_t factor_threads, int32_t apply_threads, int32_t apply_stage);

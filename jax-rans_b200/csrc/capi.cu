@@ -26,7 +26,7 @@ void launch_chain_apply(const CaseDev*, const BatchDims&, bool sa, bool fp32, in
                         int out_id, int check_active, cudaStream_t);
 int chain_grid_blocks(int n_chains, int n_offchain);
 bool apply_threads_valid(int threads, int max_L);
-bool apply_stage_fits(int max_L, bool fp32);
+bool apply_stage_fits(int max_L, bool fp32, int stage);
 void configure_line_kernels(int max_L);
 void launch_chain_couple(const CaseDev*, const BatchDims&, bool fp32, int out_id, int check_active, cudaStream_t);
 // krylov.cu
@@ -92,7 +92,7 @@ struct jr_plan {
   bool live_vortex = false;              // an enabled case uses the point-vortex far field
   std::vector<std::vector<int>> chain_len;   // each case's chain lengths (host copy)
   int ls_factor_threads = 128, ls_apply_threads = 128;   // the line-solve schedule in use
-  int ls_apply_stage = 0;                                // 1: the solve stages its factor
+  int ls_apply_stage = 0;                                // s >= 1: the solve stages its factor
   const double* factor_U = nullptr;      // the state of the last jr_precond_factor (the coupled form's)
 };
 
@@ -1019,9 +1019,10 @@ int jr_time_kernels(jr_plan* plan, int32_t reps, double* ms) {
 }
 
 // The autotuner: for the line factor and the line solve, time every block size the
-// plan's longest chain allows (64, 128, 256 threads per chain), and for the solve both
-// forms (factor read from global memory level by level, or staged into shared memory
-// first, where it fits), at the plan's state, and keep the fastest.  Only the schedule
+// plan's longest chain allows (64, 128, 256 threads per chain), and for the solve each
+// form (factor read from global memory level by level, or staged into shared memory
+// from level s-1 of the longest chain, s = 1..4, where it fits), at the plan's state,
+// and keep the fastest.  Only the schedule
 // changes -- each row's arithmetic is the same -- so results do not depend on the
 // choice.  The step graph is captured anew.
 int jr_autotune(jr_plan* plan, int32_t reps, int32_t* chosen) {
@@ -1036,7 +1037,6 @@ int jr_autotune(jr_plan* plan, int32_t reps, int32_t* chosen) {
   launch_faces(t, p->dims, p->visc, st);
   launch_cells(t, p->dims, p->visc, st);
   const int cands[3] = {64, 128, 256};
-  const int stages = apply_stage_fits(p->dims.max_L, p->mixed) ? 2 : 1;
   float best_f = 1e30f, best_a = 1e30f;
   int pick_f = p->ls_factor_threads, pick_a = p->ls_apply_threads, pick_s = p->ls_apply_stage;
   auto timed = [&](auto&& launch) {
@@ -1059,7 +1059,8 @@ int jr_autotune(jr_plan* plan, int32_t reps, int32_t* chosen) {
       pick_f = c;
     }
     if (!apply_threads_valid(c, p->dims.max_L)) continue;
-    for (int s = 0; s < stages; ++s) {
+    for (int s = 0; s <= APPLY_STAGES; ++s) {
+      if (!apply_stage_fits(p->dims.max_L, p->mixed, s)) continue;
       d.ls_apply_stage = s;
       float ta = timed([&] { launch_chain_apply(t, d, sa, p->mixed, B_R, 0, -1, B_TMP, 0, st); });
       if (ta < best_a) {
@@ -1087,8 +1088,9 @@ int jr_autotune(jr_plan* plan, int32_t reps, int32_t* chosen) {
 }
 
 // A line-solve schedule set by the caller: the block sizes of the factor and of the
-// solve (64, 128 or 256 threads per chain) and the solve's form (1: factor staged into
-// shared memory).  Results do not depend on it.
+// solve (64, 128 or 256 threads per chain) and the solve's form (0: factor read from
+// global memory; s = 1..4: staged into shared memory from level s-1 of the longest
+// chain).  Results do not depend on it.
 int jr_line_schedule(jr_plan* plan, int32_t factor_threads, int32_t apply_threads, int32_t apply_stage) {
   if (!plan) return fail(JR_EINVAL, "bad argument");
   auto ok = [](int th) { return th == 64 || th == 128 || th == 256; };
@@ -1096,9 +1098,9 @@ int jr_line_schedule(jr_plan* plan, int32_t factor_threads, int32_t apply_thread
     return fail(JR_EINVAL, "line-solve blocks must have 64, 128 or 256 threads");
   if (!apply_threads_valid(apply_threads, plan->dims.max_L))
     return fail(JR_EINVAL, "too few line-solve threads for the longest chain (4 x threads >= its even rows)");
-  if (apply_stage != 0 && apply_stage != 1) return fail(JR_EINVAL, "apply_stage must be 0 or 1");
-  if (apply_stage && !apply_stage_fits(plan->dims.max_L, plan->mixed))
-    return fail(JR_EINVAL, "the longest chain's factor does not fit one block's shared memory");
+  if (apply_stage < 0 || apply_stage > APPLY_STAGES) return fail(JR_EINVAL, "apply_stage must be 0 to 4");
+  if (!apply_stage_fits(plan->dims.max_L, plan->mixed, apply_stage))
+    return fail(JR_EINVAL, "the staged factor does not fit one block's shared memory");
   plan->ls_factor_threads = factor_threads;
   plan->ls_apply_threads = apply_threads;
   plan->ls_apply_stage = apply_stage;

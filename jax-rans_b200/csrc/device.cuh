@@ -167,10 +167,11 @@ struct BatchDims {
   int cgs_blocks;           // blocks of the basis passes
   int ls_factor_threads;    // threads per chain of the line factor and of the line solve:
   int ls_apply_threads;     // the schedule the plan's autotuner picked (results do not depend on it)
-  int ls_apply_stage;       // 1: the line solve first copies its chain's factor into shared memory
+  int ls_apply_stage;       // s >= 1: the line solve stages its factor from level s-1 of the longest chain
 };
 
 constexpr int LS_MAX_THREADS = 256;   // the largest line-solve block
+constexpr int APPLY_STAGES = 4;       // staged line-solve forms 1..4 (0: the factor read from global memory)
 
 // The basis passes: a block owns a chunk of cgs_chunk(n) elements of a case of n, set by
 // the case's size alone (so its sums are the same in any batch): small cases keep two

@@ -403,19 +403,22 @@ __device__ __forceinline__ bool stage_wait(unsigned long long* bar) {
 }
 
 // Shared memory of the line solve: [flow factor | SA factor] when staged, then the
-// level-concatenated right-hand sides (at most 2 L rows of 5).  The staged space is
-// the largest footprint of any chain up to max_L cells.
+// level-concatenated right-hand sides (at most 2 L rows of 5).  Stage s >= 1 reserves
+// the largest footprint of any chain of up to max_L >> (s - 1) cells: a chain stages
+// its levels from the first whose remaining rows fit (the longest chain from level s-1)
+// and reads the levels above from global memory, while the copy is in flight.
 struct ApplyLayout {
   int ent_f, ent_s;       // staged entries (0 unstaged)
   size_t off_s, off_b;    // byte offsets of the SA factor and of the right-hand sides
   size_t bytes;           // dynamic shared memory of a CTA
 };
 
-static ApplyLayout apply_layout(int max_L, bool fp32, bool stage) {
+static ApplyLayout apply_layout(int max_L, bool fp32, int stage) {
   const size_t tb = fp32 ? 4 : 8;
   ApplyLayout a{0, 0, 0, 0, 0};
-  if (stage) {
-    for (int l = 1; l <= max_L; ++l) {
+  if (stage > 0) {
+    const int Lb = (max_L >> (stage - 1)) > 1 ? (max_L >> (stage - 1)) : 1;
+    for (int l = 1; l <= Lb; ++l) {
       a.ent_f = cr_chain_entries(l) > a.ent_f ? cr_chain_entries(l) : a.ent_f;
       a.ent_s = cr_chain_sa_entries(l) > a.ent_s ? cr_chain_sa_entries(l) : a.ent_s;
     }
@@ -426,13 +429,80 @@ static ApplyLayout apply_layout(int max_L, bool fp32, bool stage) {
   return a;
 }
 
-// whether the staged line solve fits one CTA's shared memory for chains up to max_L
-bool apply_stage_fits(int max_L, bool fp32) { return apply_layout(max_L, fp32, true).bytes <= SMEM_PER_BLOCK_MAX; }
+// whether the line solve's stage form fits one CTA's shared memory for chains up to max_L
+bool apply_stage_fits(int max_L, bool fp32, int stage) {
+  return stage == 0 || (stage >= 1 && stage <= APPLY_STAGES && apply_layout(max_L, fp32, stage).bytes <= SMEM_PER_BLOCK_MAX);
+}
+
+// One level of the reduction: the odd rows' right-hand sides of the next level,
+// bn[o] = b[2o+1] - alpha_o b[2o] - gamma_o b[2o+2] (4x4 blocks; scalars for SA).
+template <class TF, bool SA>
+__device__ __forceinline__ void cr_reduce_level(const TF* alp, const TF* gam, const TF* sal, const TF* sga, const TF* b,
+                                                TF* bn, int rows) {
+  const int no = rows / 2;
+  for (int o = threadIdx.x; o < no; o += blockDim.x) {
+    TF al[4][4], ga[4][4], t[4], u[4];
+    load4(alp, no, o, al);
+    load4(gam, no, o, ga);
+    TF be[4], bo[4], bx[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      be[v] = b[(2 * o) * 5 + v];
+      bo[v] = b[(2 * o + 1) * 5 + v];
+      bx[v] = 2 * o + 2 < rows ? b[(2 * o + 2) * 5 + v] : TF(0);
+    }
+    mv4(al, be, t);
+    mv4(ga, bx, u);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) bn[o * 5 + v] = bo[v] - t[v] - u[v];
+    if constexpr (SA) {
+      TF bx4 = 2 * o + 2 < rows ? b[(2 * o + 2) * 5 + 4] : TF(0);
+      bn[o * 5 + 4] = b[(2 * o + 1) * 5 + 4] - sal[o] * b[(2 * o) * 5 + 4] - sga[o] * bx4;
+    }
+  }
+}
+
+// One level of the back substitution: the even rows' solution from the odd rows' x,
+// x_e = D_e^-1 (b[2e] - lower_e x[e-1] - upper_e x[e]), kept in registers (xe, xs: up
+// to 4 rows per thread) until every thread has read b.
+template <class TF, bool SA>
+__device__ __forceinline__ void cr_back_level(const TF* inv, const TF* si, const TF* b, const TF* x, int rows, TF* xe,
+                                              TF* xs) {
+  const int ne = (rows + 1) / 2, no = rows / 2;
+  const TF* low = inv + (size_t)16 * ne;
+  const TF* upp = low + (size_t)16 * ne;
+  int cnt = 0;
+  for (int e = threadIdx.x; e < ne; e += blockDim.x, ++cnt) {
+    TF I[4][4], lw[4][4], up[4][4], t[4], u[4], w[4], res[4];
+    load4(inv, ne, e, I);
+    load4(low, ne, e, lw);
+    load4(upp, ne, e, up);
+    TF xp[4], xn[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      xp[v] = e >= 1 ? x[(e - 1) * 5 + v] : TF(0);
+      xn[v] = e < no ? x[e * 5 + v] : TF(0);
+    }
+    mv4(lw, xp, t);
+    mv4(up, xn, u);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) w[v] = b[(2 * e) * 5 + v] - t[v] - u[v];
+    mv4(I, w, res);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) xe[cnt * 4 + v] = res[v];
+    if constexpr (SA) {
+      TF xps = e >= 1 ? x[(e - 1) * 5 + 4] : TF(0);
+      TF xns = e < no ? x[e * 5 + 4] : TF(0);
+      xs[cnt] = si[e] * (b[(2 * e) * 5 + 4] - si[ne + e] * xps - si[2 * ne + e] * xns);
+    }
+  }
+}
 
 // src_id: the right-hand side buffer; scale_on: multiply it by the case's 1/|w|;
 // vout_j >= 0: also write the scaled input to basis vector j; out_id: the result.
-// STAGE: the chain's factor is first copied into shared memory (ent_f, ent_s entries
-// reserved at byte offsets 0 and off_s; the right-hand sides at off_b).
+// STAGE: the chain's factor from its first level whose remaining rows fit ent_f flow
+// entries (and ent_s SA entries) is copied into shared memory (byte offsets 0 and off_s)
+// at the start; the right-hand sides at off_b.
 template <class TF, class TV, bool SA, bool STAGE>
 __global__ void __launch_bounds__(LS_MAX_THREADS) k_cr_apply(const CaseDev* __restrict__ cases, int src_id, int scale_on,
                                                          int vout_j, int out_id, int check_active, int ent_f,
@@ -480,18 +550,29 @@ __global__ void __launch_bounds__(LS_MAX_THREADS) k_cr_apply(const CaseDev* __re
   const TF* Fsg = fsa + (size_t)cv.ch_fbase[c] * 5;
   TF* const sf = reinterpret_cast<TF*>(smem_raw);
   TF* const ss = reinterpret_cast<TF*>(smem_raw + off_s);
-  const TF* F = STAGE ? sf : Fg;
-  const TF* Fs = STAGE ? ss : Fsg;
+  // levels [0, k0) read the factor from global memory, the rest (from entry off0, SA
+  // entry offs0) from the staged copy
+  int k0 = 1 << 30;
+  size_t off0 = 0, offs0 = 0;
   if constexpr (STAGE) {
-    const int ef = cr_chain_entries(L), es = cr_chain_sa_entries(L);
-    const bool aligned = ((smem_u32(sf) | (unsigned)reinterpret_cast<uintptr_t>(Fg)) & 15u) == 0;
-    if (ef > ent_f || (SA && es > ent_s) || !aligned) {   // not reached: sized for max_L, 16-byte rows
+    int rows0 = L;
+    k0 = 0;
+    while (cr_chain_entries(rows0) > ent_f || (SA && cr_chain_sa_entries(rows0) > ent_s)) {
+      const int ne = (rows0 + 1) / 2, no = rows0 / 2;
+      off0 += (size_t)48 * ne + (size_t)32 * no;
+      offs0 += (size_t)3 * ne + (size_t)2 * no;
+      rows0 = no;
+      ++k0;
+    }
+    const int ef = cr_chain_entries(rows0), es = cr_chain_sa_entries(rows0);
+    const bool aligned = ((smem_u32(sf) | (unsigned)reinterpret_cast<uintptr_t>(Fg + off0)) & 15u) == 0;
+    if (ef > ent_f || !aligned) {   // not reached: ent_f >= 16 (one row) and 64-byte levels
       if (threadIdx.x == 0) atomicOr(&cd.sc->status, (int)ST_STAGE_FAILED);
       return;
     }
-    if (threadIdx.x == 0) stage_issue(&stage_bar, sf, Fg, (unsigned)(ef * sizeof(TF)));
+    if (threadIdx.x == 0) stage_issue(&stage_bar, sf, Fg + off0, (unsigned)(ef * sizeof(TF)));
     if constexpr (SA)
-      for (int k = threadIdx.x; k < es; k += blockDim.x) ss[k] = Fsg[k];
+      for (int k = threadIdx.x; k < es; k += blockDim.x) ss[k] = Fsg[offs0 + k];
   }
   // gather the right-hand side
   for (int k = threadIdx.x; k < L; k += blockDim.x) {
@@ -507,66 +588,56 @@ __global__ void __launch_bounds__(LS_MAX_THREADS) k_cr_apply(const CaseDev* __re
     }
   }
   __syncthreads();
-  if constexpr (STAGE) {
+  // before the first staged level: wait for the copy (uniform in the CTA)
+  auto staged_ready = [&]() {
     const bool ok = stage_wait(&stage_bar);
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) atomicOr(&cd.sc->status, (int)ST_STAGE_FAILED);
       stage_wait(&stage_bar);   // a copy still in flight lands in this CTA's shared memory
-      return;
+      return false;
     }
-  }
+    return true;
+  };
   // reduce: b_odd <- b_odd - alpha b_even - gamma b_next_even, level by level
-  int rows = L;
+  int rows = L, lev = 0;
   size_t off = 0, offs = 0, boff = 0;
   while (rows > 1) {
     const int ne = (rows + 1) / 2, no = rows / 2;
-    const TF* alp = F + off + (size_t)48 * ne;
-    const TF* gam = alp + (size_t)16 * no;
     TF* b = bs + boff * 5;
     TF* bn = bs + (boff + rows) * 5;
-    for (int o = threadIdx.x; o < no; o += blockDim.x) {
-      TF al[4][4], ga[4][4], t[4], u[4];
-      load4(alp, no, o, al);
-      load4(gam, no, o, ga);
-      TF be[4], bo[4], bx[4];
-#pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        be[v] = b[(2 * o) * 5 + v];
-        bo[v] = b[(2 * o + 1) * 5 + v];
-        bx[v] = 2 * o + 2 < rows ? b[(2 * o + 2) * 5 + v] : TF(0);
-      }
-      mv4(al, be, t);
-      mv4(ga, bx, u);
-#pragma unroll
-      for (int v = 0; v < 4; ++v) bn[o * 5 + v] = bo[v] - t[v] - u[v];
-      if constexpr (SA) {
-        const TF* sal = Fs + offs + 3 * ne;
-        const TF* sga = sal + no;
-        TF bx4 = 2 * o + 2 < rows ? b[(2 * o + 2) * 5 + 4] : TF(0);
-        bn[o * 5 + 4] = b[(2 * o + 1) * 5 + 4] - sal[o] * b[(2 * o) * 5 + 4] - sga[o] * bx4;
-      }
+    if (!STAGE || lev < k0) {
+      const TF* alp = Fg + off + (size_t)48 * ne;
+      const TF* sal = Fsg + offs + 3 * ne;
+      cr_reduce_level<TF, SA>(alp, alp + (size_t)16 * no, sal, sal + no, b, bn, rows);
+    } else {
+      if (lev == k0 && !staged_ready()) return;
+      const TF* alp = sf + (off - off0) + (size_t)48 * ne;
+      const TF* sal = ss + (offs - offs0) + 3 * ne;
+      cr_reduce_level<TF, SA>(alp, alp + (size_t)16 * no, sal, sal + no, b, bn, rows);
     }
     __syncthreads();
     off += (size_t)48 * ne + (size_t)32 * no;
     offs += (size_t)3 * ne + (size_t)2 * no;
     boff += rows;
     rows = no;
+    ++lev;
   }
+  if (STAGE && lev == k0 && !staged_ready()) return;   // only the last row staged
   // the last row, then substitute back level by level; x of a level overwrites its b
   if (threadIdx.x == 0) {
     TF* b = bs + boff * 5;
     TF I[4][4], x[4];
-    load4(F + off, 1, 0, I);
+    if constexpr (STAGE) load4(sf + (off - off0), 1, 0, I);
+    else load4(Fg + off, 1, 0, I);
     mv4(I, b, x);
 #pragma unroll
     for (int v = 0; v < 4; ++v) b[v] = x[v];
-    if constexpr (SA) b[4] = Fs[offs] * b[4];
+    if constexpr (SA) b[4] = (STAGE ? ss[offs - offs0] : Fsg[offs]) * b[4];
   }
   __syncthreads();
   // walk the levels back: recompute their offsets from the top
-  int depth = 0;
-  for (int m = L; m > 1; m >>= 1) ++depth;
-  for (int lev = depth - 1; lev >= 0; --lev) {
+  const int depth = lev;
+  for (lev = depth - 1; lev >= 0; --lev) {
     int rws = L;
     size_t of = 0, ofs = 0, bo_ = 0;
     for (int k = 0; k < lev; ++k) {
@@ -577,42 +648,15 @@ __global__ void __launch_bounds__(LS_MAX_THREADS) k_cr_apply(const CaseDev* __re
       rws = no_;
     }
     const int ne = (rws + 1) / 2, no = rws / 2;
-    const TF* inv = F + of;
-    const TF* low = inv + (size_t)16 * ne;
-    const TF* upp = low + (size_t)16 * ne;
     TF* b = bs + bo_ * 5;           // this level's right-hand side; becomes its solution
     const TF* x = bs + (bo_ + rws) * 5;   // the next level's solution (the odd rows)
     // evens from the odd solution; the odds copied into place after a barrier
     TF xe[4 * 4];   // up to 4 even rows per thread kept in registers when rows <= 4*threads
     TF xs[4];
-    int cnt = 0;
-    for (int e = threadIdx.x; e < ne; e += blockDim.x, ++cnt) {
-      TF I[4][4], lw[4][4], up[4][4], t[4], u[4], w[4], res[4];
-      load4(inv, ne, e, I);
-      load4(low, ne, e, lw);
-      load4(upp, ne, e, up);
-      TF xp[4], xn[4];
-#pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        xp[v] = e >= 1 ? x[(e - 1) * 5 + v] : TF(0);
-        xn[v] = e < no ? x[e * 5 + v] : TF(0);
-      }
-      mv4(lw, xp, t);
-      mv4(up, xn, u);
-#pragma unroll
-      for (int v = 0; v < 4; ++v) w[v] = b[(2 * e) * 5 + v] - t[v] - u[v];
-      mv4(I, w, res);
-#pragma unroll
-      for (int v = 0; v < 4; ++v) xe[cnt * 4 + v] = res[v];
-      if constexpr (SA) {
-        const TF* si = Fs + ofs;
-        TF xps = e >= 1 ? x[(e - 1) * 5 + 4] : TF(0);
-        TF xns = e < no ? x[e * 5 + 4] : TF(0);
-        xs[cnt] = si[e] * (b[(2 * e) * 5 + 4] - si[ne + e] * xps - si[2 * ne + e] * xns);
-      }
-    }
+    if (!STAGE || lev < k0) cr_back_level<TF, SA>(Fg + of, Fsg + ofs, b, x, rws, xe, xs);
+    else cr_back_level<TF, SA>(sf + (of - off0), ss + (ofs - offs0), b, x, rws, xe, xs);
     __syncthreads();
-    cnt = 0;
+    int cnt = 0;
     for (int e = threadIdx.x; e < ne; e += blockDim.x, ++cnt) {
 #pragma unroll
       for (int v = 0; v < 4; ++v) b[(2 * e) * 5 + v] = xe[cnt * 4 + v];
@@ -764,11 +808,11 @@ static void apply_t(const CaseDev* cases, const BatchDims& d, bool sa, int src_i
                     int check_active, cudaStream_t st) {
   dim3 grid(d.chain_blocks, d.n_cases);
   const bool fp32 = sizeof(TF) == 4;
-  const bool stage = d.ls_apply_stage && apply_stage_fits(d.max_L, fp32);
+  const int stage = apply_stage_fits(d.max_L, fp32, d.ls_apply_stage) ? d.ls_apply_stage : 0;
   const ApplyLayout a = apply_layout(d.max_L, fp32, stage);
   const int th = d.ls_apply_threads > 0 ? d.ls_apply_threads : LS_THREADS;
   const int os = (int)a.off_s, ob = (int)a.off_b;
-  if (stage) {
+  if (stage > 0) {
     if (sa)
       k_cr_apply<TF, TV, true, true><<<grid, th, a.bytes, st>>>(cases, src_id, scale_on, vout_j, out_id, check_active,
                                                                 a.ent_f, a.ent_s, os, ob);
@@ -804,7 +848,7 @@ void configure_line_kernels(int max_L) {
                        (int)cr_couple_smem(max_L, false));
   cudaFuncSetAttribute(k_cr_sa_couple<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)cr_couple_smem(max_L, true));
-  const int s8 = (int)apply_layout(max_L, false, false).bytes, s4 = (int)apply_layout(max_L, true, false).bytes;
+  const int s8 = (int)apply_layout(max_L, false, 0).bytes, s4 = (int)apply_layout(max_L, true, 0).bytes;
   const int most = (int)SMEM_PER_BLOCK_MAX;
   cudaFuncSetAttribute(k_cr_apply<double, double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8);
   cudaFuncSetAttribute(k_cr_apply<double, double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8);

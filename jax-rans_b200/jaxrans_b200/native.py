@@ -436,12 +436,14 @@ class DevicePlan:
         out = np.zeros(3, dtype=np.int32)
         _check(self.lib, self.lib.jr_autotune(self.handle, int(reps), _ptr(out, _i32p)), "jr_autotune")
         return {"line_factor_threads": int(out[0]), "line_apply_threads": int(out[1]),
-                "line_apply_staged": bool(out[2])}
+                "line_apply_stage": int(out[2])}
 
-    def line_schedule(self, factor_threads: int = 128, apply_threads: int = 128, staged: bool = False) -> None:
-        """Set the line-solve schedule by hand (``jr_line_schedule``)."""
+    def line_schedule(self, factor_threads: int = 128, apply_threads: int = 128, stage: int = 0) -> None:
+        """Set the line-solve schedule by hand (``jr_line_schedule``): ``stage`` 0 reads
+        the factor from global memory, 1..4 stage it in shared memory from level
+        ``stage - 1`` of the longest chain."""
         _check(self.lib, self.lib.jr_line_schedule(self.handle, int(factor_threads), int(apply_threads),
-                                                   int(bool(staged))), "jr_line_schedule")
+                                                   int(stage)), "jr_line_schedule")
 
     def launch_count(self) -> int:
         """Kernels launched by this plan's Newton steps so far (skipped cycles not counted)."""

@@ -7,7 +7,7 @@ to run under a profiler.
 Prints the residual norms of the steps; ``--time`` also prints the live CUDA-event times
 of the hot kernels (``jr_time_kernels``); ``--line-schedule`` replaces the autotuner's
 choice by the line factor's and line solve's threads per chain and the solve's form
-(``jr_line_schedule``: S = 1 staged).
+(``jr_line_schedule``: S = 0 global, 1..4 staged).
 """
 
 from __future__ import annotations
@@ -47,7 +47,7 @@ def main(argv=None) -> int:
         dev.set_state(freestream_state(case, plan), case.implicit.cfl)
     if args.line_schedule:
         f, a, s = (int(x) for x in args.line_schedule.split(","))
-        dev.line_schedule(f, a, bool(s))
+        dev.line_schedule(f, a, s)
     first = min(3, args.steps)
     print(dev.newton_steps(first))
     if args.steps > first:

@@ -187,19 +187,22 @@ def test_autotuned_schedule_gives_the_same_steps(cuda):
 
 @pytest.mark.parametrize("name,precision", [("c_sa", "fp64"), ("c_sa", "mixed"), ("o_euler", "fp64")])
 def test_staged_line_solve_gives_the_same_steps(cuda, name, precision):
-    """The line solve with its chain's factor staged in shared memory by one bulk
-    asynchronous copy steps bitwise as the one reading the factor level by level."""
+    """The line solve with its chains' factor staged in shared memory by one bulk
+    asynchronous copy (all levels, or from the first, second or third level down) steps
+    bitwise as the one reading the factor level by level from global memory."""
     from jaxrans_b200.native import DevicePlan
     z, case, plan = load(name)
     implicit = replace(case.implicit, precision=precision)
     runs = []
-    for staged in (False, True):
+    for stage in (0, 1, 2, 3, 4):
         dev = DevicePlan(plan, case.flow, case.numerics, implicit)
-        dev.line_schedule(128, 64, staged)
+        dev.line_schedule(128, 64, stage)
         dev.set_state(freestream_state(case, plan), case.implicit.cfl)
         hist = dev.newton_steps(8)
         U, cfl, res, status = dev.get_state()
         assert status & 8 == 0
         runs.append((hist, U))
-    assert np.array_equal(runs[0][0], runs[1][0])
-    assert np.array_equal(runs[0][1], runs[1][1])
+        dev.close()
+    for hist, U in runs[1:]:
+        assert np.array_equal(runs[0][0], hist)
+        assert np.array_equal(runs[0][1], U)
