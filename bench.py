@@ -2,7 +2,7 @@
 """Benchmark: converged RANS solves per hour on one B200 (or N replicas).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload c_sa_385] [--precision fp64|mixed]
+                    [--workload c_sa_385] [--precision fp64|mixed] [--line-schedule F,A,S]
 
 A step is one converged solve of the workload (``jaxrans_b200.workloads``; by default
 the 2D SA-noft2 NACA 4412 C-grid 385 x 97, Roe + MUSCL minmod, GMRES(30)) from the
@@ -202,7 +202,14 @@ def load_job(args):
         if name not in made:
             made[name] = case.grid()
         grids.append(made[name])
-    dev = batch_device(cases, grids) if len(cases) > 1 else device_for(cases[0], grids[0])
+    dev = (batch_device(cases, grids, autotune=False) if len(cases) > 1
+           else device_for(cases[0], grids[0], autotune=False))
+    if args.line_schedule:
+        f, a, s = (int(x) for x in args.line_schedule.split(","))
+        dev.line_schedule(f, a, s)
+        args.schedule = {"line_factor_threads": f, "line_apply_threads": a, "line_apply_stage": s, "by": "hand"}
+    else:
+        args.schedule = dict(dev.autotune(), by="autotuner")
     return cases, grids, dev
 
 
@@ -310,7 +317,7 @@ def run_device(args) -> int:
               "precision": args.precision, "newton_steps_per_solve": int(np.median(iters)),
               "exit_reasons": sorted({m.reason for mons in solves for m in mons}),
               "l2": "flushed (256 MB write) per step", "parallelism": f"replicas x{world}",
-              "kernels_per_newton_step_max": kps}
+              "kernels_per_newton_step_max": kps, "line_schedule": args.schedule}
     if n_cases == 1:
         config["canvas"] = list(grids[0].shape)
         f = last[0].forces
@@ -364,6 +371,9 @@ def main(argv=None) -> int:
     p.add_argument("--workload", default="c_sa_385", choices=sorted(STEPS_PER_SOLVE) + ["polar64_uneven"])
     p.add_argument("--precision", default="fp64", choices=("fp64", "mixed"))
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--line-schedule", default=None, metavar="F,A,S",
+                   help="line factor threads, line solve threads, solve form (0 global, 1-4 staged) instead of "
+                        "the autotuner's pick (for runs under a profiler, where its timings do not hold)")
     args = p.parse_args(argv)
     if args.warmup < 3:
         raise SystemExit("--warmup must be at least 3")

@@ -26,7 +26,7 @@ from .plan import Plan
 from .solver import CaseMonitor, ConvergenceHistory, Result, Timing, forces_of, freestream_state
 
 
-def batch_device(cases: list[Case], grids: list[Plan]):
+def batch_device(cases: list[Case], grids: list[Plan], autotune: bool = True):
     """One device plan for ``cases`` on ``grids`` (each case's own numerics, CFL settings
     and force reference; the model, precision and Krylov settings must agree)."""
     from .native import DevicePlan
@@ -34,7 +34,8 @@ def batch_device(cases: list[Case], grids: list[Plan]):
     dev = DevicePlan.batch(list(grids), [c.flow for c in cases], [c.numerics for c in cases],
                            [c.implicit for c in cases], [s.reference_length for s in specs],
                            [tuple(s.moment_centre[:2]) for s in specs])
-    dev.autotune()
+    if autotune:
+        dev.autotune()
     return dev
 
 

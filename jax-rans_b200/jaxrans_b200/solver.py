@@ -167,12 +167,13 @@ def freestream_state(case: Case, plan: Plan) -> np.ndarray:
     return np.broadcast_to(np.array(rows)[:, None, None], (len(rows),) + plan.shape).copy()
 
 
-def device_for(case: Case, plan: Plan):
+def device_for(case: Case, plan: Plan, autotune: bool = True):
     from .native import DevicePlan
     spec = case.grid_spec
     dev = DevicePlan(plan, case.flow, case.numerics, case.implicit, spec.reference_length,
                      tuple(spec.moment_centre[:2]))
-    dev.autotune()
+    if autotune:
+        dev.autotune()
     return dev
 
 
