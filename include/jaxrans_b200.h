@@ -29,6 +29,14 @@ extern "C" {
 #define JR_ENOMEM 2      /* a device allocation failed */
 #define JR_ECUDA 3       /* a CUDA error (message in jr_last_error) */
 #define JR_EMISMATCH 4   /* buffers that do not fit the plan */
+#define JR_ETIMEOUT 5    /* a device-side wait gave up (a case's status has JR_STATUS_WAIT_LIMIT) */
+
+/* Bits of a case's status word (jr_state_get, jr_case_state_get): the last Newton step's
+ * outcome.  JR_STATUS_WAIT_LIMIT stays set until the case's state is set again. */
+#define JR_STATUS_NONFINITE 1         /* a non-finite value met in a reduction */
+#define JR_STATUS_REJECTED 2          /* the last Newton step was rejected */
+#define JR_STATUS_GMRES_BREAKDOWN 4   /* an Arnoldi vector of zero norm */
+#define JR_STATUS_WAIT_LIMIT 8        /* the line solve's staged copy was not seen to land in time */
 
 typedef struct jr_plan jr_plan;
 
@@ -183,7 +191,8 @@ int jr_time_kernels(jr_plan* plan, int32_t reps, double* ms_out);
 
 /* n_steps pseudo-transient Newton steps on the plan's state, one captured CUDA graph per
  * step for the whole batch; history (host, n_steps x n_cases, step-major) receives each
- * case's |R| before each step.  Synchronises once.
+ * case's |R| before each step.  Synchronises once; JR_ETIMEOUT if a case's status has
+ * JR_STATUS_WAIT_LIMIT (the steps ran; that case's last solves are not to be trusted).
  * Replaces make_newton_step (src/jaxrans/solvers/implicit.py:84-168) run as the
  * driver's block (src/jaxrans/solvers/driver.py:87-104). */
 int jr_newton_steps(jr_plan* plan, int32_t n_steps, double* history);
@@ -208,9 +217,16 @@ int jr_autotune(jr_plan* plan, int32_t reps, int32_t* chosen);
  * in {64, 128, 256} (4 x apply_threads at least the longest chain's even rows), and
  * apply_stage the solve's form, 0 to 4 (JR_EINVAL where the staged part does not fit
  * one block's shared memory).  Results do not depend on it.  A staged copy that
- * fails sets status bit 8 of its case (kept until the plan's state is set again); it is
+ * fails sets JR_STATUS_WAIT_LIMIT in its case's status (kept until the case's state is set again); it is
  * not expected.  No counterpart in the reference. */
 int jr_line_schedule(jr_plan* plan, int32_t factor_threads, int32_t apply_threads, int32_t apply_stage);
+
+/* A check of the device's bounded waits, with no plan: one block waits, tries times (each
+ * up to about 1 us), on an mbarrier that no copy completes.  The wait must run out:
+ * returns JR_ETIMEOUT with status (may be NULL) = JR_STATUS_WAIT_LIMIT, and the context
+ * stays usable.  Device 0's current context, default stream.  No counterpart in the
+ * reference. */
+int jr_wait_limit_check(int32_t tries, int32_t* status);
 
 /* Force coefficients at the plan's state (or at U if not NULL, a device pointer): out
  * (host, 6 per case) = cl, cd, cm, cd_friction, fx, fy.  Replaces force_coefficients

@@ -11,6 +11,9 @@
 #include "device.cuh"
 
 namespace jr {
+static_assert(JR_STATUS_NONFINITE == ST_NONFINITE && JR_STATUS_REJECTED == ST_REJECTED &&
+                  JR_STATUS_GMRES_BREAKDOWN == ST_GMRES_BREAKDOWN && JR_STATUS_WAIT_LIMIT == ST_STAGE_FAILED,
+              "the status bits of the C ABI are the device's");
 // residual.cu
 void launch_residual(const CaseDev*, const BatchDims&, int visc, bool second, int out_id, cudaStream_t);
 void launch_jvp(const CaseDev*, const BatchDims&, int visc, int tangent_id, int vdt_id, int out_id, int check_active,
@@ -27,6 +30,7 @@ void launch_chain_apply(const CaseDev*, const BatchDims&, bool sa, bool fp32, in
 int chain_grid_blocks(int n_chains, int n_offchain);
 bool apply_threads_valid(int threads, int max_L);
 bool apply_stage_fits(int max_L, bool fp32, int stage);
+int wait_limit_check(int tries, int* status, cudaStream_t st);
 void configure_line_kernels(int max_L);
 void launch_chain_couple(const CaseDev*, const BatchDims&, bool fp32, int out_id, int check_active, cudaStream_t);
 // krylov.cu
@@ -966,8 +970,17 @@ int jr_newton_steps(jr_plan* plan, int32_t n_steps, double* history) {
   if (history && n_steps > 0)
     cudaMemcpyAsync(history, plan->history, (size_t)n_steps * plan->n_cases * sizeof(double), cudaMemcpyDeviceToHost,
                     plan->st);
+  // every case's status word, one strided copy
+  std::vector<int> status(plan->n_cases, 0);
+  cudaMemcpy2DAsync(status.data(), sizeof(int), &plan->sc[0].status, sizeof(Scalars), sizeof(int), plan->n_cases,
+                    cudaMemcpyDeviceToHost, plan->st);
   if (cudaStreamSynchronize(plan->st) != cudaSuccess) return cuda_check("jr_newton_steps");
-  return cuda_check("jr_newton_steps");
+  rc = cuda_check("jr_newton_steps");
+  if (rc) return rc;
+  for (int k = 0; k < plan->n_cases; ++k)
+    if (status[k] & ST_STAGE_FAILED)
+      return fail(JR_ETIMEOUT, "a line solve's staged copy did not land within its wait limit");
+  return JR_OK;
 }
 
 int jr_time_kernels(jr_plan* plan, int32_t reps, double* ms) {
@@ -1084,6 +1097,19 @@ int jr_autotune(jr_plan* plan, int32_t reps, int32_t* chosen) {
     chosen[1] = pick_a;
     chosen[2] = pick_s;
   }
+  return JR_OK;
+}
+
+// The bounded device wait checked on its own: a barrier no copy completes, waited on
+// for `tries` tries (each up to 1 us), must give up and say so.
+int jr_wait_limit_check(int32_t tries, int32_t* status) {
+  if (tries < 1 || tries > (1 << 20)) return fail(JR_EINVAL, "tries must be in 1 .. 2^20");
+  int s = -1;
+  if (wait_limit_check(tries, &s, 0)) return cuda_check("jr_wait_limit_check");
+  int rc = cuda_check("jr_wait_limit_check");
+  if (rc) return rc;
+  if (status) *status = s;
+  if (s & ST_STAGE_FAILED) return fail(JR_ETIMEOUT, "the wait ran out (as it must: nothing completes its barrier)");
   return JR_OK;
 }
 

@@ -388,9 +388,9 @@ __device__ __forceinline__ void stage_issue(unsigned long long* bar, void* dst, 
 }
 
 // Wait for the barrier's first phase, a bounded number of tries; false if it gave up.
-__device__ __forceinline__ bool stage_wait(unsigned long long* bar) {
+__device__ __forceinline__ bool stage_wait(unsigned long long* bar, int tries = STAGE_WAIT_TRIES) {
   const unsigned b = smem_u32(bar);
-  for (int i = 0; i < STAGE_WAIT_TRIES; ++i) {
+  for (int i = 0; i < tries; ++i) {
     unsigned done;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, 1, 0, p;\n\t}"
@@ -400,6 +400,34 @@ __device__ __forceinline__ bool stage_wait(unsigned long long* bar) {
     if (done) return true;
   }
   return false;
+}
+
+// The bounded wait's own check: a barrier armed for 16 bytes that no copy delivers, so the
+// wait runs out after `tries` tries and the block reports it -- the path a staged solve
+// takes if its copy does not land.  Nothing is in flight when the block exits.
+__device__ int g_wait_check;
+
+__global__ void k_wait_limit_check(int tries) {
+  __shared__ __align__(8) unsigned long long bar;
+  if (threadIdx.x == 0) {
+    const unsigned b = smem_u32(&bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(16u) : "memory");
+  }
+  __syncthreads();
+  const bool ok = stage_wait(&bar, tries);
+  const bool gave_up = __syncthreads_or(!ok);
+  if (threadIdx.x == 0) g_wait_check = gave_up ? (int)ST_STAGE_FAILED : 0;
+}
+
+// status <- the check's status word (ST_STAGE_FAILED when the wait ran out, as it must)
+int wait_limit_check(int tries, int* status, cudaStream_t st) {
+  const int zero = -1;
+  cudaMemcpyToSymbolAsync(g_wait_check, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, st);
+  k_wait_limit_check<<<1, 64, 0, st>>>(tries);
+  cudaMemcpyFromSymbolAsync(status, g_wait_check, sizeof(int), 0, cudaMemcpyDeviceToHost, st);
+  return cudaStreamSynchronize(st) == cudaSuccess ? 0 : 1;
 }
 
 // Shared memory of the line solve: [flow factor | SA factor] when staged, then the

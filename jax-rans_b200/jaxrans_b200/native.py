@@ -62,15 +62,29 @@ EXPORTS = ("jr_plan_create", "jr_plan_destroy", "jr_last_error", "jr_plan_sizes"
            "jr_forces", "jr_state_set_device", "jr_graph_kernels", "jr_time_kernels", "jr_plan_set_stream",
            "jr_batch_create", "jr_plan_cases", "jr_case_sizes", "jr_case_enable", "jr_case_set_inflow",
            "jr_case_state_set", "jr_case_state_get", "jr_residual_noalloc", "jr_case_load",
-           "jr_launch_count", "jr_autotune", "jr_line_schedule", "jr_wall_loads")
+           "jr_launch_count", "jr_autotune", "jr_line_schedule", "jr_wait_limit_check", "jr_wall_loads")
 
 TIMED_KERNELS = ("residual_tile", "jvp_tile", "ghosts_tangent", "line_apply", "line_factor", "cgs2_full_basis")
 
 _LIB = None
 
 
+# return codes and status bits of the C ABI (include/jaxrans_b200.h)
+JR_OK, JR_EINVAL, JR_ENOMEM, JR_ECUDA, JR_EMISMATCH, JR_ETIMEOUT = 0, 1, 2, 3, 4, 5
+JR_STATUS_NONFINITE, JR_STATUS_REJECTED, JR_STATUS_GMRES_BREAKDOWN, JR_STATUS_WAIT_LIMIT = 1, 2, 4, 8
+
+
 class NativeError(RuntimeError):
-    """A failure reported by the C-ABI library."""
+    """A failure reported by the C-ABI library (``code``: its return code)."""
+
+    def __init__(self, message: str, code: int = JR_ECUDA):
+        super().__init__(message)
+        self.code = code
+
+
+class DeviceTimeout(NativeError):
+    """A device-side wait gave up (``JR_ETIMEOUT``): a case's status has
+    ``JR_STATUS_WAIT_LIMIT``; its last steps are not to be trusted."""
 
 
 def load_library(path: Path | None = None) -> C.CDLL:
@@ -108,6 +122,7 @@ def load_library(path: Path | None = None) -> C.CDLL:
         "jr_launch_count": (C.c_int, [vp, C.POINTER(C.c_int64)]),
         "jr_autotune": (C.c_int, [vp, C.c_int32, _i32p]),
         "jr_line_schedule": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32]),
+        "jr_wait_limit_check": (C.c_int, [C.c_int32, _i32p]),
         "jr_wall_loads": (C.c_int, [vp, vp, vp]),
         "jr_time_kernels": (C.c_int, [vp, C.c_int32, _f64p]),
         "jr_plan_set_stream": (C.c_int, [vp, vp]),
@@ -131,7 +146,8 @@ def load_library(path: Path | None = None) -> C.CDLL:
 def _check(lib, rc: int, what: str) -> None:
     if rc != 0:
         msg = lib.jr_last_error().decode(errors="replace")
-        raise NativeError(f"{what} failed (code {rc}): {msg}")
+        cls = DeviceTimeout if rc == JR_ETIMEOUT else NativeError
+        raise cls(f"{what} failed (code {rc}): {msg}", rc)
 
 
 def _ptr(a: np.ndarray, kind):

@@ -59,3 +59,16 @@ def test_batch_rejects_cases_of_different_models_on_the_host():
     assert lib.jr_batch_create(descs, 2, C.byref(handle)) == 1
     assert b"must share" in lib.jr_last_error()
     assert lib.jr_batch_create(descs, 0, C.byref(handle)) == 1
+
+
+def test_codes_and_status_bits_match_the_header():
+    """The binding's return codes and status bits are the header's."""
+    from jaxrans_b200 import native
+    text = HEADER.read_text()
+    defines = {k: int(v) for k, v in re.findall(r"^#define (JR_\w+) (\d+)", text, re.M)}
+    names = [n for n in dir(native) if n.startswith("JR_")]
+    assert sorted(names) == sorted(defines)
+    for name in names:
+        assert getattr(native, name) == defines[name], name
+    err = native.DeviceTimeout("x", native.JR_ETIMEOUT)
+    assert isinstance(err, native.NativeError) and err.code == 5
