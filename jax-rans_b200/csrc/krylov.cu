@@ -30,7 +30,7 @@ __device__ __forceinline__ double warp_max(double x) {
 // In the last block of a reduction: out[k] = the sum (or NaN-propagating max) over the
 // nb rows of partial[b * stride + k], k < W, by all the block's threads in a fixed order
 // -- thread (k, r) takes the rows b = r, r + R, ... (R = blockDim.x / W groups), with its
-// loads issued four at a time, then thread k adds the R group totals in order.  Loads go
+// loads issued eight at a time, then thread k adds the R group totals in order.  Loads go
 // to L2 (ld.global.cg), where the other blocks' partials are.
 template <bool MAX>
 __device__ void reduce_rows(const double* partial, int stride, int W, int nb, double* out) {
@@ -40,12 +40,12 @@ __device__ void reduce_rows(const double* partial, int stride, int W, int nb, do
   if (r < R) {
     double acc = MAX ? -INFINITY : 0.0;
     int b = r;
-    for (; b + 3 * R < nb; b += 4 * R) {
-      const double x0 = __ldcg(partial + (size_t)b * stride + k);
-      const double x1 = __ldcg(partial + (size_t)(b + R) * stride + k);
-      const double x2 = __ldcg(partial + (size_t)(b + 2 * R) * stride + k);
-      const double x3 = __ldcg(partial + (size_t)(b + 3 * R) * stride + k);
-      acc = MAX ? nmax(nmax(nmax(nmax(acc, x0), x1), x2), x3) : (((acc + x0) + x1) + x2) + x3;
+    for (; b + 7 * R < nb; b += 8 * R) {
+      double x[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) x[u] = __ldcg(partial + (size_t)(b + u * R) * stride + k);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) acc = MAX ? nmax(acc, x[u]) : acc + x[u];
     }
     for (; b < nb; b += R) {
       const double x = __ldcg(partial + (size_t)b * stride + k);
@@ -210,11 +210,13 @@ __global__ void k_cycle_gate(const CaseDev* __restrict__ cases, int n_cases, cud
 
 // The three passes of CGS2 over the basis, one kernel: MODE 0 h = V^T w; MODE 1
 // w -= V hin, then h = V^T w; MODE 2 w -= V hin, then |w| and column j of H.  A block
-// owns a chunk of cgs_chunk(n) elements.  The update runs thread per element (the nk
-// loads of an element independent of one another); the dot products run warp per basis
-// vector against the block's w held in shared memory, each lane with 16 loads in
-// flight, so the registers stay few and many blocks share an SM.  In MODE 1 the second
-// read of the chunk's basis rows is served by L2.
+// owns a chunk of cgs_chunk(n) elements.  The update runs thread per element (for an FP64
+// basis the nk loads of an element issued together, up to 32 in flight, before they are
+// added in order); the dot products run warp per basis vector against the block's w held
+// in shared memory, each lane with 32 loads in flight (16 for an FP32 basis).  With one
+// or two blocks per SM the passes are bound by the bytes in flight, hence the batches;
+// the order of every sum is that of one load at a time.  In MODE 1 the second read of
+// the chunk's basis rows is served by L2.
 template <class TV, int NK, int MODE>
 __global__ void __launch_bounds__(RED_THREADS) k_mdot(const CaseDev* __restrict__ cases, int nk, int j) {
   const CaseDev& cd = cases[blockIdx.y];
@@ -248,10 +250,19 @@ __global__ void __launch_bounds__(RED_THREADS) k_mdot(const CaseDev* __restrict_
     const int i = i0 + e;
     double wi = w[i];
     if constexpr (MODE != 0) {
+      // an FP64 basis: the element's nk entries loaded together, then added in order (an
+      // FP32 basis keeps one load per entry: measured faster there)
+      constexpr int KB = sizeof(TV) == 4 ? 1 : (NK < 32 ? NK : 32);
       double s = 0.0;
 #pragma unroll
-      for (int k = 0; k < NK; ++k)
-        if (k < nk) s += h[k] * double(V[k * ldv + i]);
+      for (int k0 = 0; k0 < NK; k0 += KB) {
+        double vk[KB];
+#pragma unroll
+        for (int u = 0; u < KB; ++u) vk[u] = k0 + u < nk ? double(V[(size_t)(k0 + u) * ldv + i]) : 0.0;
+#pragma unroll
+        for (int u = 0; u < KB; ++u)
+          if (k0 + u < nk) s += h[k0 + u] * vk[u];
+      }
       wi = wi - s;
       w[i] = wi;
     }
@@ -275,6 +286,15 @@ __global__ void __launch_bounds__(RED_THREADS) k_mdot(const CaseDev* __restrict_
       const TV* __restrict__ vk = V + k * ldv + i0;
       double a = 0.0;
       int e = lane;
+      if constexpr (sizeof(TV) == 8) {   // an FP64 basis: 32 loads in flight per lane
+        for (; e + 32 * 31 < cn; e += 32 * 32) {
+          double x[32];
+#pragma unroll
+          for (int u = 0; u < 32; ++u) x[u] = double(vk[e + 32 * u]);
+#pragma unroll
+          for (int u = 0; u < 32; ++u) a += x[u] * ws[e + 32 * u];
+        }
+      }
       for (; e + 32 * 15 < cn; e += 32 * 16) {
         double x[16];
 #pragma unroll
