@@ -1,0 +1,76 @@
+"""The 3D oracle (oracle.numerics3d) against the reference's own 3D residual, exact
+first-order JVP, wave speeds and norm on the C-H wing fixture (tests/golden/ch_sa3d.npz,
+made by tests/golden/make_golden3d.py from the reference's sources)."""
+
+from __future__ import annotations
+
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from jaxrans_b200.case import _flow
+from jaxrans_b200.geometry import section_source
+from jaxrans_b200.grid3d import wing_block
+from jaxrans_b200.plan3d import build_plan3d
+from oracle import numerics3d as n3
+
+GOLDEN = Path(__file__).resolve().parent / "golden" / "ch_sa3d.npz"
+KINDS = {"wall": "no_slip_wall", "farfield": "far_field", "root": "symmetry", "tip": "symmetry"}
+
+
+@pytest.fixture(scope="module")
+def setup():
+    z = np.load(GOLDEN)
+    w = json.loads(str(z["wing_json"]))
+    doc = json.loads(str(z["case_json"]))
+    plan = build_plan3d([wing_block(section_source(w.pop("section")), **w).with_kinds(KINDS)])
+    flow = _flow(doc["case"])
+    a = flow.alpha_rad
+    # x-z incidence, y along the span (core/state.py:107-140)
+    q_inf = np.array([1.0, flow.mach * np.cos(a), 0.0, flow.mach * np.sin(a), 1.0 / flow.gamma,
+                      flow.nu_tilde_ratio])
+    cv = doc["numerical"]["convective_fluxes"]
+    model = n3.Model3(plan, q_inf, flow.gamma, cv["riemann_solver"], cv["limiter"], 0.0, flow.mu_inf,
+                      flow.sutherland_ratio, True, plan.distance)
+    return z, model
+
+
+def rows_rel(a, b):
+    return max(float(np.abs(a[k] - b[k]).max() / max(np.abs(b[k]).max(), 1e-300)) for k in range(a.shape[0]))
+
+
+def test_freestream_canvas(setup):
+    z, model = setup
+    assert np.array_equal(n3.initial_state(model), z["U0"])
+
+
+@pytest.mark.parametrize("state", ["sin", "rand0"])
+def test_residuals_and_jvp_match_the_reference(setup, state):
+    z, model = setup
+    U = z[f"{state}_U"]
+    R2 = n3.residual(U, model)
+    assert rows_rel(R2, z[f"{state}_R2"]) < 1e-14
+    assert rows_rel(n3.residual(U, model, first_order=True), z[f"{state}_R1"]) < 1e-14
+    assert rows_rel(n3.jvp(U, z[f"{state}_v"], model), z[f"{state}_Jv"]) < 1e-13
+    assert np.isclose(n3.norm(R2, model), float(z[f"{state}_norm"]), rtol=1e-14, atol=0.0)
+
+
+@pytest.mark.parametrize("state", ["sin", "rand0"])
+def test_wave_speeds_match_the_reference(setup, state):
+    z, model = setup
+    lam = n3.wave_speeds(z[f"{state}_U"], model)
+    for a in range(3):
+        assert np.allclose(lam[a], z[f"{state}_lam{a}"], rtol=1e-14, atol=0.0)
+    assert np.allclose(n3.cell_sum(lam) / 25.0, z[f"{state}_vdt"], rtol=1e-14, atol=0.0)
+
+
+def test_freestream_is_preserved_off_the_wall(setup):
+    """A uniform state leaves no residual away from the wall and its ghosts (the face
+    vectors of every cell close)."""
+    z, model = setup
+    R = n3.residual(n3.initial_state(model), model)
+    plan = model.plan
+    off = plan.interior & (plan.distance > 0.5)
+    assert np.abs(R[:5][:, off]).max() < 1e-12
