@@ -1,0 +1,139 @@
+"""The 3D line preconditioner restated in NumPy (oracle; TEST INFRASTRUCTURE).
+
+Follows ``src/jaxrans/solvers/preconditioners.py:209-306`` on a 3D plan: the mean-flow
+chains carry 5x5 blocks (``diag = sum_f lambda_f (1/CFL + 1/2) I``, ``off = 1/2 A(U_nb,
+S_out) - 1/2 lambda_f I``), the SA row its own scalar chains (upwind mass flux, thin
+layer diffusion, the destruction derivative, V/dt).  The chains are solved by the
+block cyclic reduction of ``oracle.implicit`` (``src/jaxrans/core/linalg.py:159-200``),
+which is written for any block size.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import numerics as nm
+from . import numerics3d as n3
+from .implicit import cr_factor, cr_solve, thomas_factor, thomas_solve
+
+
+def _families(fields):
+    return np.concatenate([f.reshape(f.shape[:-3] + (-1,)) for f in fields], axis=-1)
+
+
+def _gather(field, lines):
+    cells = np.where(lines.cells >= 0, lines.cells, 0)
+    return field.reshape(field.shape[:-3] + (-1,))[..., cells]
+
+
+def _faces(fields, lines, side):
+    idx = lines.up_face if side == "up" else lines.down_face
+    return _families(fields)[..., idx]
+
+
+def normal_flux_jacobian(q, s, g):
+    """``A = d(F . S)/dU`` ``(5, 5, ...)`` [row, variable] by the complex step on the flux
+    of the conservative state (``physics/euler.py:55-71``)."""
+    U = n3.conservative(q[:5], g)
+    cols = []
+    for k in range(5):
+        Uc = U.astype(np.complex128)
+        Uc[k] = Uc[k] + 1j * nm.STEP
+        cols.append(np.imag(n3.normal_flux(n3.prim(Uc, g), s, g)) / nm.STEP)
+    return np.stack(cols, axis=1)
+
+
+def chain_blocks_flow(U, lam, cfl, model):
+    """``(lower, diag, upper)`` ``(L, n_lines, 5, 5)`` of the mean-flow chains."""
+    plan, g = model.plan, model.gamma
+    lines = plan.lines
+    valid = lines.cells >= 0
+    q = n3.prim(U[:5], g)
+    eye = np.eye(5)
+    d = np.where(valid, _gather(n3.cell_sum(lam) * (1.0 / cfl + 0.5), lines), 1.0)
+    diag = d.T[:, :, None, None] * eye
+
+    def coupling(side, sign, nb):
+        s = _faces(plan.faces, lines, side)
+        block = 0.5 * normal_flux_jacobian(nb, sign * s, g) - 0.5 * _faces(lam, lines, side) * eye.reshape(5, 5, 1, 1)
+        return np.transpose(np.where(sign != 0, block, 0.0), (3, 2, 0, 1))
+
+    chains = _gather(q, lines)
+    above = np.concatenate([chains[:, :, 1:], chains[:, :, -1:]], axis=2)
+    upper = coupling("up", lines.up_sign, above)
+    below = coupling("down", lines.down_sign, chains)
+    lower = np.concatenate([np.zeros_like(below[:1]), below[:-1]], axis=0)
+    return lower, diag, upper
+
+
+def chain_blocks_sa(U, lam, cfl, model):
+    """Scalar SA chain blocks ``(L, n_lines, 1, 1)``."""
+    plan, g, nu_inf = model.plan, model.gamma, model.mu_inf
+    lines = plan.lines
+    valid = lines.cells >= 0
+    q = n3.prim(U, g)
+    qf = n3.face_averages(plan, q)
+    vols = n3.face_averages(plan, plan.volume)
+    terms = []
+    for a in range(3):
+        f, s = qf[a], plan.faces[a]
+        mu = model.mu(n3.temperature(f, g))
+        kap = nm.diffusion(f[0], f[5] * nu_inf, mu)
+        terms.append((f[0] * n3.dot(f[1:4], s), kap * n3.dot(s, s) / vols[a]))
+    rho = q[0]
+    diag = None
+    for a, (m_f, d_f) in enumerate(terms):
+        lo, hi = [slice(None)] * 3, [slice(None)] * 3
+        lo[a], hi[a] = slice(0, -1), slice(1, None)
+        out_f = np.maximum(m_f, 0.0) + d_f
+        in_f = np.maximum(-m_f, 0.0) + d_f
+        diag = out_f[tuple(hi)] + in_f[tuple(lo)] if diag is None else diag + out_f[tuple(hi)] + in_f[tuple(lo)]
+    diag = diag / rho
+    nu_hat = q[5]
+    gx = n3.green_gauss([f[1:4] for f in qf], plan.faces, plan.volume)
+    nu = model.mu(n3.temperature(q, g)) / rho
+    d = model.distance
+    s_t = nm.s_tilde(n3.vorticity_magnitude(gx), nu_hat * nu_inf, nu, d)
+    fw = nm.f_w(nm.r_of(nu_hat * nu_inf, s_t, d))
+    dest = np.where(nu_hat > 0.0, 2.0 * nm.SA.c_w1 * fw * nu_inf * nu_hat / d ** 2, 0.0)
+    diag = diag + dest * plan.volume + n3.cell_sum(lam) / cfl
+    d_chain = np.where(valid, _gather(diag, lines), 1.0)
+    rho_chain = _gather(rho, lines)
+    m, dj = tuple(t[0] for t in terms), tuple(t[1] for t in terms)
+
+    def coupling(side, sign, rho_nb):
+        block = -(np.maximum(-sign * _faces(m, lines, side), 0.0) + _faces(dj, lines, side)) / rho_nb
+        return np.where(sign != 0, block, 0.0).T[:, :, None, None]
+
+    above = np.concatenate([rho_chain[:, 1:], rho_chain[:, -1:]], axis=1)
+    upper = coupling("up", lines.up_sign, above)
+    below = coupling("down", lines.down_sign, rho_chain)
+    lower = np.concatenate([np.zeros_like(below[:1]), below[:-1]], axis=0)
+    return lower, d_chain.T[:, :, None, None], upper
+
+
+def precondition(U, lam, cfl, model, solver: str = "cr"):
+    """``r -> M^-1 r`` of ``line_j`` on a 3D plan: exact solves along the chains, the SA
+    row on its own scalar chains."""
+    lines = model.plan.lines
+    valid = lines.cells >= 0
+    found = np.full(model.plan.n_canvas, -1, dtype=np.int64)
+    found[lines.cells[valid]] = np.flatnonzero(valid)
+    fac = cr_factor if solver == "cr" else thomas_factor
+    sol = cr_solve if solver == "cr" else thomas_solve
+    parts = [(slice(0, 5), fac(*chain_blocks_flow(U, lam, cfl, model)))]
+    if model.sa:
+        parts.append((slice(5, 6), fac(*chain_blocks_sa(U, lam, cfl, model))))
+
+    def apply(r):
+        out = []
+        for rows, factor in parts:
+            rr = r[rows]
+            rhs = np.where(valid, _gather(rr, lines), 0.0)
+            x = np.transpose(sol(factor, np.transpose(rhs, (2, 1, 0))), (2, 1, 0))
+            flat = rr.reshape(rr.shape[0], -1)
+            vals = x.reshape(x.shape[0], -1)[:, np.where(found >= 0, found, 0)]
+            out.append(np.where(found >= 0, vals, flat).reshape(rr.shape))
+        return np.concatenate(out)
+
+    return apply

@@ -74,3 +74,31 @@ def test_freestream_is_preserved_off_the_wall(setup):
     plan = model.plan
     off = plan.interior & (plan.distance > 0.5)
     assert np.abs(R[:5][:, off]).max() < 1e-12
+
+
+@pytest.mark.parametrize("state", ["sin", "rand0"])
+def test_chain_blocks_and_preconditioner_match_the_reference(setup, state):
+    """5x5 mean-flow chain blocks, scalar SA chain blocks and the line_j solve at CFL
+    25 (src/jaxrans/solvers/preconditioners.py:209-306)."""
+    from oracle import implicit3d as i3
+    z, model = setup
+    U = z[f"{state}_U"]
+    lam = n3.wave_speeds(U, model)
+    for name, blocks in (("flow", i3.chain_blocks_flow(U, lam, 25.0, model)),
+                         ("sa", i3.chain_blocks_sa(U, lam, 25.0, model))):
+        for part, ref in zip(blocks, ("lower", "diag", "upper")):
+            assert np.allclose(part, z[f"{state}_{name}_{ref}"], rtol=1e-13, atol=0.0), (name, ref)
+    zz = i3.precondition(U, lam, 25.0, model)(z[f"{state}_prec_r"])
+    assert rows_rel(zz, z[f"{state}_prec_z"]) < 1e-13
+    # cyclic reduction and block Thomas agree
+    zt = i3.precondition(U, lam, 25.0, model, solver="thomas")(z[f"{state}_prec_r"])
+    assert rows_rel(zt, zz) < 1e-10
+
+
+@pytest.mark.parametrize("state", ["sin", "rand0"])
+def test_forces_match_the_reference(setup, state):
+    from oracle import forces3d as f3
+    z, model = setup
+    area = json.loads(str(z["case_json"]))["case"]["domain"]["reference_area"]
+    f = f3.forces(z[f"{state}_U"], model, area, 0.8, (0.25, 0.0, 0.0))
+    assert np.allclose(f, z[f"{state}_forces"], rtol=1e-12, atol=1e-17)
