@@ -137,3 +137,62 @@ def precondition(U, lam, cfl, model, solver: str = "cr"):
         return np.concatenate(out)
 
     return apply
+
+
+# --- the Newton step (src/jaxrans/solvers/implicit.py:54-168, core/state.py:142-150) ------
+
+
+def relax(dU, U, g, fraction):
+    """One global factor so no cell's density or (linearized) pressure moves by more than
+    ``fraction`` of itself, nor ``nu~`` by more than ``fraction`` of ``max(|nu~|, 1)``."""
+    if fraction is None:
+        return dU, 1.0
+    q = n3.prim(U[:5], g)
+    rho, vel, p = q[0], q[1:4], q[4]
+    d_e = dU[4]
+    for k in range(3):
+        d_e = d_e - vel[k] * dU[1 + k]
+    d_p = (g - 1.0) * (d_e + 0.5 * n3.dot(vel, vel) * dU[0])
+    ratios = [np.abs(dU[0]) / rho, np.abs(d_p) / p]
+    if U.shape[0] > 5:
+        nh = U[5] / rho
+        ratios.append(np.abs((dU[5] - nh * dU[0]) / rho) / np.maximum(np.abs(nh), 1.0))
+    worst = max(float(np.max(r)) for r in ratios)
+    omega = min(1.0, fraction / max(worst, 1e-300))
+    return omega * dU, omega
+
+
+def is_physical(U, g):
+    q = n3.prim(U[:5], g)
+    return (q[0] > 1e-10) & (q[4] > 1e-10) & np.isfinite(q[0]) & np.isfinite(q[4])
+
+
+def newton_step(state, model, config, solver: str = "cr"):
+    """One pseudo-transient Newton step on a 3D plan (the 2D step of ``oracle.implicit``
+    with the 3D residual, JVP, wave speeds and preconditioner)."""
+    from .implicit import NewtonState, gmres_right
+    U, cfl = state.U, state.cfl
+    R = n3.residual(U, model)
+    norm = n3.norm(R, model)
+    lam = n3.wave_speeds(U, model)
+    vdt = n3.cell_sum(lam) / cfl
+    prec = precondition(U, lam, cfl, model, solver) if config.preconditioner == "line_j" else (lambda r: r)
+
+    def matvec(d):
+        return vdt[None] * d + n3.jvp(U, d, model)
+
+    dU, action = gmres_right(matvec, -R, prec, config.krylov_subspace, config.krylov_restarts, config.krylov_tol)
+    dU, omega = relax(dU, U, model.gamma, config.max_relative_update)
+    lin = np.linalg.norm(omega * action + R) / max(np.linalg.norm(R), 1e-300)
+    cand = U + dU
+    physical = bool(np.all(is_physical(cand, model.gamma)) and np.all(np.isfinite(dU)))
+    accept = physical and lin < 1.0
+    reduction = state.residual_norm / max(norm, 1e-300)
+    if accept and lin < config.krylov_success and omega >= 1.0:
+        cfl_next = cfl * min(max(reduction, 1.0), config.cfl_growth)
+    elif accept:
+        cfl_next = cfl
+    else:
+        cfl_next = cfl / config.cfl_cutback
+    return NewtonState(cand if accept else U, min(max(cfl_next, config.cfl_min), config.cfl_max),
+                       norm if accept else state.residual_norm), norm

@@ -37,7 +37,9 @@ from jaxrans.case.loader import load_case  # noqa: E402
 from jaxrans.mesh.block3d import SIDES_3D, InterfaceRect  # noqa: E402
 from jaxrans.numerics.residual import cell_wave_speed_sum, make_residual  # noqa: E402
 from jaxrans.post.forces import integrate_forces  # noqa: E402
+from jaxrans.solvers import implicit  # noqa: E402
 from jaxrans.solvers import preconditioners as pre  # noqa: E402
+from jaxrans.solvers.krylov import gmres_right  # noqa: E402
 
 from jaxrans_b200.geometry import section_source  # noqa: E402
 from jaxrans_b200.grid3d import wing_block, write_plot3d  # noqa: E402
@@ -154,6 +156,23 @@ def main() -> int:
         out[f"{label}_prec_z"] = np.asarray(prepare(U, lam, cfl)(jnp.asarray(r)))
         f = integrate_forces(U, atlas, flow, reference)
         out[f"{label}_forces"] = np.array([f.cl, f.cd, f.cm, f.cd_friction])
+    # One GMRES solve of the Newton system, and three Newton steps, at "rand0"
+    config = case.implicit
+    U = jnp.asarray(states["rand0"])
+    residual = op.residual(U)
+    _, jvp = jax.linearize(jop.residual, U)
+    lam = op.wave_speeds(U)
+    vdt = cell_wave_speed_sum(lam) / cfl
+    dU, action = gmres_right(lambda d: vdt[None] * d + jvp(d), -residual, prepare(U, lam, cfl),
+                             restart=config.krylov_subspace, maxiter=config.krylov_restarts,
+                             tol=config.krylov_tol, return_action=True, action_from_arnoldi=True)
+    out["gmres_dU"], out["gmres_action"] = np.asarray(dU), np.asarray(action)
+    step = implicit.make_newton_step(op, config, jop)
+    state = implicit.ImplicitState(U=U, cfl=cfl, residual_norm=jnp.asarray(np.inf))
+    for k in range(3):
+        state, norm = step(state)
+        out[f"newton{k}_U"], out[f"newton{k}_cfl"] = np.asarray(state.U), np.asarray(state.cfl)
+        out[f"newton{k}_norm"] = np.asarray(norm)
     np.savez_compressed(HERE / "ch_sa3d.npz", **out)
     print(f"ch_sa3d: {atlas.shape} canvas, {atlas.cells} cells -> ch_sa3d.npz")
     return 0

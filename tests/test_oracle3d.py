@@ -102,3 +102,34 @@ def test_forces_match_the_reference(setup, state):
     area = json.loads(str(z["case_json"]))["case"]["domain"]["reference_area"]
     f = f3.forces(z[f"{state}_U"], model, area, 0.8, (0.25, 0.0, 0.0))
     assert np.allclose(f, z[f"{state}_forces"], rtol=1e-12, atol=1e-17)
+
+
+def _implicit_config(doc):
+    from jaxrans_b200.case import NUMERICAL_FILE, _section, _values
+    from jaxrans_b200.config import ImplicitConfig
+    return ImplicitConfig(**_values(_section(doc["numerical"], NUMERICAL_FILE, "implicit"), NUMERICAL_FILE,
+                                    "implicit"))
+
+
+def test_gmres_and_newton_steps_match_the_reference(setup):
+    """One right-preconditioned GMRES solve of the Newton system and three Newton steps
+    from the 'rand0' state at CFL 25 (src/jaxrans/solvers/implicit.py:84-168)."""
+    from oracle import implicit3d as i3
+    from oracle.implicit import NewtonState, gmres_right
+    z, model = setup
+    config = _implicit_config(json.loads(str(z["case_json"])))
+    U = z["rand0_U"]
+    R = n3.residual(U, model)
+    lam = n3.wave_speeds(U, model)
+    vdt = n3.cell_sum(lam) / 25.0
+    dU, action = gmres_right(lambda d: vdt[None] * d + n3.jvp(U, d, model), -R,
+                             i3.precondition(U, lam, 25.0, model), config.krylov_subspace,
+                             config.krylov_restarts, config.krylov_tol)
+    assert rows_rel(dU, z["gmres_dU"]) < 1e-9
+    assert rows_rel(action, z["gmres_action"]) < 1e-9
+    state = NewtonState(U, 25.0, np.inf)
+    for k in range(3):
+        state, norm = i3.newton_step(state, model, config)
+        assert np.isclose(norm, float(z[f"newton{k}_norm"]), rtol=1e-12, atol=0.0)
+        assert rows_rel(state.U, z[f"newton{k}_U"]) < 1e-13
+        assert np.isclose(state.cfl, float(z[f"newton{k}_cfl"]), rtol=1e-12)
