@@ -240,6 +240,46 @@ int jr_forces(jr_plan* plan, const double* U, double* out);
  * (src/jaxrans/post/forces.py:48-68).  Synchronises. */
 int jr_wall_loads(jr_plan* plan, const double* U, double* out);
 
+/* ---- 3D (a wing's C-H block: config 5's path) -------------------------------------- */
+
+typedef struct jr_plan3d jr_plan3d;
+
+/* One 3D case: its canvas (NI x NJ x NK, k fastest; the block's cells with a ring of 2
+ * ghost cells, as src/jaxrans/mesh/atlas3d.py:119-210 lays it out) and physics.  Fields
+ * are variable-major, nvar = 5 (rho, rho u, rho v, rho w, E) or 6 (+ rho nu~, SA-noft2). */
+typedef struct jr_plan3d_desc {
+  int32_t NI, NJ, NK, nvar;
+  const uint8_t* interior;      /* NI*NJ*NK */
+  const double* volume;         /* NI*NJ*NK */
+  const double* faces[3];       /* family a: 3 planes (x, y, z) of (NI+(a==0)) (NJ+(a==1)) (NK+(a==2)) */
+  const double* centres;        /* 3 planes of (NI+2)(NJ+2)(NK+2): centres with one ring beyond the canvas */
+  const double* distance;       /* NI*NJ*NK wall distance (SA), or NULL */
+  int32_t n_stages;             /* the ghost fill's gather stages, in order (every pass), at most 12 */
+  const int32_t* stage_records; /* n_stages counts; the records below are stage after stage */
+  const int32_t* ghost;         /* per record: the ghost cell, its source cell, the kind */
+  const int32_t* source;
+  const int32_t* kind;          /* 0 copy, 1 slip wall, 2 no-slip wall, 3 symmetry, 4 far field */
+  const double* normal;         /* 3 per record: the outward unit normal of the boundary face */
+  double gamma, mu_inf, sutherland, kappa;   /* mu_inf 0: inviscid; sutherland < 0: constant viscosity */
+  int32_t flux, limiter;        /* as jr_plan_desc */
+  double q_inf[6];              /* primitive freestream (rho, u, v, w, p[, nu~ / nu_inf]) */
+} jr_plan3d_desc;
+
+/* Build a 3D plan (device copies of the tables, work buffers, a stream).  Every record
+ * index is checked against the canvas.  No counterpart function in the reference (its
+ * atlas is built in build_atlas_3d, src/jaxrans/mesh/atlas3d.py:119). */
+int jr_plan3d_create(const jr_plan3d_desc* desc, jr_plan3d** out);
+int jr_plan3d_destroy(jr_plan3d* plan);
+/* R(U) on the canvas (device pointers, nvar x canvas): the net flux on block cells,
+ * U - U_inf elsewhere; first_order 1: the first-order residual.  Replaces
+ * make_residual(...).residual (src/jaxrans/numerics/residual.py:273-334) for a 3D atlas.
+ * Synchronises. */
+int jr_residual3d(jr_plan3d* plan, const double* U, double* R, int32_t first_order);
+/* Jv = dR1/dU . v, exact (forward-mode tangents; device pointers).  Replaces
+ * jax.linearize of the first-order residual (src/jaxrans/solvers/implicit.py:104-116).
+ * Synchronises. */
+int jr_jvp3d(jr_plan3d* plan, const double* U, const double* v, double* Jv);
+
 #ifdef __cplusplus
 }
 #endif

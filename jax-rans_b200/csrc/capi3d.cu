@@ -1,0 +1,164 @@
+// The C ABI of the 3D path: a plan of one 3D case (device copies of its canvas tables
+// and ghost records, two work buffers, a stream), its residual and its J.v.
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/jaxrans_b200.h"
+#include "device3d.cuh"
+
+namespace jr {
+int report_error(int code, const std::string& msg);
+void sa_constants(SAConst& s);
+}  // namespace jr
+
+using namespace jr;
+
+struct jr_plan3d {
+  Plan3Dev dev{};
+  std::vector<void*> allocs;
+  void* A = nullptr;   // primitive canvases (Dual-sized: the J.v needs value and tangent)
+  void* B = nullptr;
+  size_t n_canvas = 0;
+  cudaStream_t st = nullptr;
+};
+
+static int check3(const char* where) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return report_error(JR_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
+  return JR_OK;
+}
+
+template <class T> static int copy3(jr_plan3d* p, const T** dst, const T* src, size_t n) {
+  *dst = nullptr;
+  if (n == 0 || src == nullptr) return JR_OK;
+  void* d = nullptr;
+  if (cudaMalloc(&d, n * sizeof(T)) != cudaSuccess) return report_error(JR_ENOMEM, "cudaMalloc failed");
+  p->allocs.push_back(d);
+  if (cudaMemcpy(d, src, n * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+    return report_error(JR_ECUDA, "cudaMemcpy to the device failed");
+  *dst = static_cast<const T*>(d);
+  return JR_OK;
+}
+
+#define TRY3(x)              \
+  do {                       \
+    int rc_ = (x);           \
+    if (rc_ != JR_OK) {      \
+      jr_plan3d_destroy(p);  \
+      return rc_;            \
+    }                        \
+  } while (0)
+
+extern "C" {
+
+int jr_plan3d_destroy(jr_plan3d* plan) {
+  if (!plan) return JR_OK;
+  for (void* a : plan->allocs) cudaFree(a);
+  if (plan->st) cudaStreamDestroy(plan->st);
+  delete plan;
+  return JR_OK;
+}
+
+int jr_plan3d_create(const jr_plan3d_desc* d, jr_plan3d** out) {
+  if (!d || !out) return report_error(JR_EINVAL, "null argument");
+  *out = nullptr;
+  if (d->NI < 5 || d->NJ < 5 || d->NK < 5) return report_error(JR_EINVAL, "a 3D canvas needs at least 5 cells a side");
+  if (d->nvar != 5 && d->nvar != 6) return report_error(JR_EINVAL, "nvar must be 5 or 6");
+  if (d->nvar == 6 && !(d->mu_inf > 0.0)) return report_error(JR_EINVAL, "the SA model needs a viscous flow");
+  if (d->nvar == 6 && !d->distance) return report_error(JR_EINVAL, "the SA model needs the wall distance");
+  if (d->n_stages < 1 || d->n_stages > MAX_STAGES3) return report_error(JR_EINVAL, "1 to 12 ghost stages");
+  if (!d->interior || !d->volume || !d->centres || !d->faces[0] || !d->faces[1] || !d->faces[2] ||
+      !d->stage_records)
+    return report_error(JR_EINVAL, "null table");
+  if (d->flux < 0 || d->flux > 1 || d->limiter < 0 || d->limiter > 4)
+    return report_error(JR_EINVAL, "unknown flux or limiter code");
+  const size_t n = (size_t)d->NI * d->NJ * d->NK;
+  if (n > (size_t)(1u << 30)) return report_error(JR_EINVAL, "canvas too large");
+  // the records: every index inside the canvas, every kind known
+  size_t n_rec = 0;
+  for (int s = 0; s < d->n_stages; ++s) {
+    if (d->stage_records[s] < 0) return report_error(JR_EINVAL, "negative record count");
+    n_rec += (size_t)d->stage_records[s];
+  }
+  if (n_rec > 0 && (!d->ghost || !d->source || !d->kind || !d->normal))
+    return report_error(JR_EINVAL, "null ghost records");
+  for (size_t r = 0; r < n_rec; ++r) {
+    if (d->ghost[r] < 0 || (size_t)d->ghost[r] >= n || d->source[r] < 0 || (size_t)d->source[r] >= n)
+      return report_error(JR_EINVAL, "a ghost record outside the canvas");
+    if (d->kind[r] < 0 || d->kind[r] > 4) return report_error(JR_EINVAL, "unknown ghost record kind");
+  }
+  jr_plan3d* p = new jr_plan3d();
+  p->n_canvas = n;
+  Plan3Dev& dv = p->dev;
+  dv.NI = d->NI;
+  dv.NJ = d->NJ;
+  dv.NK = d->NK;
+  dv.nvar = d->nvar;
+  TRY3(copy3(p, &dv.interior, d->interior, n));
+  TRY3(copy3(p, &dv.volume, d->volume, n));
+  for (int a = 0; a < 3; ++a) {
+    const size_t nf = (size_t)(d->NI + (a == 0)) * (d->NJ + (a == 1)) * (d->NK + (a == 2));
+    TRY3(copy3(p, &dv.faces[a], d->faces[a], 3 * nf));
+  }
+  TRY3(copy3(p, &dv.centres, d->centres, 3 * (size_t)(d->NI + 2) * (d->NJ + 2) * (d->NK + 2)));
+  TRY3(copy3(p, &dv.distance, d->nvar == 6 ? d->distance : nullptr, n));
+  dv.n_stages = d->n_stages;
+  dv.stage_off[0] = 0;
+  for (int s = 0; s < d->n_stages; ++s) dv.stage_off[s + 1] = dv.stage_off[s] + d->stage_records[s];
+  TRY3(copy3(p, &dv.g_ghost, d->ghost, n_rec));
+  TRY3(copy3(p, &dv.g_source, d->source, n_rec));
+  TRY3(copy3(p, &dv.g_kind, d->kind, n_rec));
+  TRY3(copy3(p, &dv.g_normal, d->normal, 3 * n_rec));
+  Physics3& P = dv.P;
+  P.gamma = d->gamma;
+  P.mu_inf = d->mu_inf > 0.0 ? d->mu_inf : 0.0;
+  P.sutherland = d->sutherland;
+  P.kappa = d->kappa;
+  P.flux = d->flux;
+  P.limiter = d->limiter;
+  for (int v = 0; v < NV3_MAX; ++v) P.q_inf[v] = v < d->nvar ? d->q_inf[v] : 0.0;
+  {
+    const double g = d->gamma, rho = P.q_inf[0], u = P.q_inf[1], v = P.q_inf[2], w = P.q_inf[3], pr = P.q_inf[4];
+    P.U_inf[0] = rho;
+    P.U_inf[1] = rho * u;
+    P.U_inf[2] = rho * v;
+    P.U_inf[3] = rho * w;
+    P.U_inf[4] = pr / (g - 1.0) + 0.5 * rho * ((u * u + v * v) + w * w);
+    P.U_inf[5] = rho * P.q_inf[5];
+  }
+  sa_constants(P.sa);
+  const size_t work = (size_t)d->nvar * n * sizeof(Dual);
+  if (cudaMalloc(&p->A, work) != cudaSuccess || (p->allocs.push_back(p->A), cudaMalloc(&p->B, work)) != cudaSuccess) {
+    jr_plan3d_destroy(p);
+    return report_error(JR_ENOMEM, "cudaMalloc failed");
+  }
+  p->allocs.push_back(p->B);
+  if (cudaStreamCreateWithFlags(&p->st, cudaStreamNonBlocking) != cudaSuccess) {
+    jr_plan3d_destroy(p);
+    return report_error(JR_ECUDA, "stream");
+  }
+  int rc = check3("jr_plan3d_create");
+  if (rc) {
+    jr_plan3d_destroy(p);
+    return rc;
+  }
+  *out = p;
+  return JR_OK;
+}
+
+int jr_residual3d(jr_plan3d* plan, const double* U, double* R, int32_t first_order) {
+  if (!plan || !U || !R) return report_error(JR_EINVAL, "null argument");
+  launch_residual3(plan->dev, U, R, plan->A, plan->B, first_order != 0, plan->st);
+  if (cudaStreamSynchronize(plan->st) != cudaSuccess) return check3("jr_residual3d");
+  return check3("jr_residual3d");
+}
+
+int jr_jvp3d(jr_plan3d* plan, const double* U, const double* v, double* Jv) {
+  if (!plan || !U || !v || !Jv) return report_error(JR_EINVAL, "null argument");
+  launch_jvp3(plan->dev, U, v, Jv, plan->A, plan->B, plan->st);
+  if (cudaStreamSynchronize(plan->st) != cudaSuccess) return check3("jr_jvp3d");
+  return check3("jr_jvp3d");
+}
+
+}  // extern "C"

@@ -1,0 +1,168 @@
+"""The 3D path through the C ABI: a 3D plan's descriptor, its ghost records, and a plan
+object with the residual and J.v of one 3D case (``jr_plan3d_*``, ``jr_residual3d``,
+``jr_jvp3d``).
+
+The plan (``jaxrans_b200.plan3d``) keeps the reference's ghost stages in gather form
+(``src/jaxrans/mesh/atlas3d.py:166-210``: per canvas cell the cell itself, a cell to
+copy, or a condition row); the device runs them as records, one per ghost the stage
+writes (a later write of the same ghost wins, as in the gather form).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from .native import FLUX_CODES, LIMITER_CODES, NativeError, _check, _f64p, _i32p, _u8p, load_library
+from .plan3d import Plan3
+
+KIND3 = {"slip_wall": 1, "no_slip_wall": 2, "symmetry": 3, "far_field": 4}
+
+
+class Plan3Desc(C.Structure):
+    """``jr_plan3d_desc`` (include/jaxrans_b200.h)."""
+
+    _fields_ = [
+        ("NI", C.c_int32), ("NJ", C.c_int32), ("NK", C.c_int32), ("nvar", C.c_int32),
+        ("interior", _u8p), ("volume", _f64p), ("faces", _f64p * 3), ("centres", _f64p), ("distance", _f64p),
+        ("n_stages", C.c_int32), ("stage_records", _i32p),
+        ("ghost", _i32p), ("source", _i32p), ("kind", _i32p), ("normal", _f64p),
+        ("gamma", C.c_double), ("mu_inf", C.c_double), ("sutherland", C.c_double), ("kappa", C.c_double),
+        ("flux", C.c_int32), ("limiter", C.c_int32),
+        ("q_inf", C.c_double * 6),
+    ]
+
+
+@dataclass
+class Records:
+    """Every stage's ghost records, stage after stage."""
+
+    counts: np.ndarray      # (n_stages,)
+    ghost: np.ndarray
+    source: np.ndarray
+    kind: np.ndarray
+    normal: np.ndarray      # (n, 3)
+
+
+def records_of(plan: Plan3) -> Records:
+    """The stages of ``plan`` as records: for each ghost a stage writes, a copy of the cell
+    it gathers, or the condition row it gathers (its kind, source cell and normal)."""
+    n = plan.n_canvas
+    counts, ghost, source, kind, normal = [], [], [], [], []
+    for st in plan.stages:
+        written = np.flatnonzero(st.index != np.arange(n))
+        target = st.index[written]
+        copy = target < n
+        row = target - n
+        kinds = np.zeros(len(written), dtype=np.int32)
+        src = np.where(copy, target, 0).astype(np.int64)
+        nrm = np.zeros((len(written), 3))
+        offset = 0
+        for name, cond_source, cond_normal, _ in st.conditions:
+            m = (~copy) & (row >= offset) & (row < offset + len(cond_source))
+            kinds[m] = KIND3[name]
+            src[m] = cond_source[row[m] - offset]
+            nrm[m] = cond_normal[:, row[m] - offset].T
+            offset += len(cond_source)
+        if np.any((~copy) & (row >= offset)):
+            raise ValueError("a stage gathers a condition row it does not have")
+        counts.append(len(written))
+        ghost.append(written)
+        source.append(src)
+        kind.append(kinds)
+        normal.append(nrm)
+    return Records(np.array(counts, dtype=np.int32), np.concatenate(ghost).astype(np.int32),
+                   np.concatenate(source).astype(np.int32), np.concatenate(kind).astype(np.int32),
+                   np.concatenate(normal))
+
+
+def apply_records(records: Records, q: np.ndarray) -> np.ndarray:
+    """The records run on the host as the device runs them (every read of a stage before
+    its writes), with copies only: the fill's index logic, for checking ``records_of``."""
+    flat = q.reshape(q.shape[0], -1).copy()
+    at = 0
+    for count in records.counts:
+        g, s = records.ghost[at:at + count], records.source[at:at + count]
+        new = flat.copy()
+        new[:, g] = flat[:, s]
+        flat = new
+        at += count
+    return flat.reshape(q.shape)
+
+
+class DevicePlan3:
+    """One 3D case on the device: residual and J.v of canvas fields (``(nvar, NI, NJ,
+    NK)`` float64 NumPy arrays in and out)."""
+
+    def __init__(self, plan: Plan3, q_inf, gamma: float, flux: str, limiter: str, kappa: float = 0.0,
+                 mu_inf: float | None = None, sutherland: float | None = None, library=None):
+        self.lib = load_library(library)
+        self.plan = plan
+        self.nvar = len(q_inf)
+        self.shape = (self.nvar,) + plan.shape
+        rec = records_of(plan)
+        keep = []
+
+        def arr(a, dtype):
+            a = np.ascontiguousarray(a, dtype=dtype)
+            keep.append(a)
+            return a
+
+        def ptr(a, t):
+            return a.ctypes.data_as(t)
+
+        d = Plan3Desc()
+        d.NI, d.NJ, d.NK = plan.shape
+        d.nvar = self.nvar
+        d.interior = ptr(arr(plan.interior, np.uint8), _u8p)
+        d.volume = ptr(arr(plan.volume, np.float64), _f64p)
+        for a in range(3):
+            d.faces[a] = ptr(arr(plan.faces[a], np.float64), _f64p)
+        d.centres = ptr(arr(plan.centres, np.float64), _f64p)
+        d.distance = ptr(arr(plan.distance, np.float64), _f64p) if plan.distance is not None else None
+        d.n_stages = len(rec.counts)
+        d.stage_records = ptr(arr(rec.counts, np.int32), _i32p)
+        d.ghost = ptr(arr(rec.ghost, np.int32), _i32p)
+        d.source = ptr(arr(rec.source, np.int32), _i32p)
+        d.kind = ptr(arr(rec.kind, np.int32), _i32p)
+        d.normal = ptr(arr(rec.normal, np.float64), _f64p)
+        d.gamma = gamma
+        d.mu_inf = 0.0 if mu_inf is None else mu_inf
+        d.sutherland = -1.0 if sutherland is None else sutherland
+        d.kappa = kappa
+        d.flux = FLUX_CODES[flux]
+        d.limiter = 4 if kappa != 0.0 else LIMITER_CODES[limiter]
+        for v in range(6):
+            d.q_inf[v] = float(q_inf[v]) if v < self.nvar else 0.0
+        handle = C.c_void_p()
+        _check(self.lib, self.lib.jr_plan3d_create(C.byref(d), C.byref(handle)), "jr_plan3d_create")
+        self.handle = handle
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.jr_plan3d_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+    def _run(self, name, *arrays):
+        import torch
+        if not torch.cuda.is_available():
+            raise NativeError("the 3D path runs on a CUDA device (there is no CPU fallback)")
+        ins = [torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device="cuda") for a in arrays]
+        out = torch.empty(self.shape, dtype=torch.float64, device="cuda")
+        return ins, out
+
+    def residual(self, U, first_order: bool = False) -> np.ndarray:
+        (u,), out = self._run("jr_residual3d", U)
+        _check(self.lib, self.lib.jr_residual3d(self.handle, u.data_ptr(), out.data_ptr(), int(first_order)),
+               "jr_residual3d")
+        return out.cpu().numpy()
+
+    def jvp(self, U, v) -> np.ndarray:
+        (u, t), out = self._run("jr_jvp3d", U, v)
+        _check(self.lib, self.lib.jr_jvp3d(self.handle, u.data_ptr(), t.data_ptr(), out.data_ptr()), "jr_jvp3d")
+        return out.cpu().numpy()

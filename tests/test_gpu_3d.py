@@ -1,0 +1,64 @@
+"""The 3D device path (jr_residual3d, jr_jvp3d) against the 3D oracle and the
+reference's own 3D outputs on the C-H wing fixture (tests/golden/ch_sa3d.npz).
+
+The 3D kernels are new and have not yet run on a B200; these tests are enabled with
+JR_RUN_3D=1 until they have (a failure must not stop the rest of the device suite)."""
+
+from __future__ import annotations
+
+import json
+import os
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from jaxrans_b200.case import _flow
+from jaxrans_b200.geometry import section_source
+from jaxrans_b200.grid3d import wing_block
+from jaxrans_b200.plan3d import build_plan3d
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(os.environ.get("JR_RUN_3D") != "1",
+                                 reason="the 3D device path has not run on a B200 yet (JR_RUN_3D=1 runs it)")]
+
+GOLDEN = Path(__file__).resolve().parent / "golden" / "ch_sa3d.npz"
+KINDS = {"wall": "no_slip_wall", "farfield": "far_field", "root": "symmetry", "tip": "symmetry"}
+
+
+@pytest.fixture(scope="module")
+def device3d():
+    from jaxrans_b200.native3d import DevicePlan3
+    z = np.load(GOLDEN)
+    w = json.loads(str(z["wing_json"]))
+    doc = json.loads(str(z["case_json"]))
+    plan = build_plan3d([wing_block(section_source(w.pop("section")), **w).with_kinds(KINDS)])
+    flow = _flow(doc["case"])
+    a = flow.alpha_rad
+    q_inf = np.array([1.0, flow.mach * np.cos(a), 0.0, flow.mach * np.sin(a), 1.0 / flow.gamma,
+                      flow.nu_tilde_ratio])
+    cv = doc["numerical"]["convective_fluxes"]
+    dev = DevicePlan3(plan, q_inf, flow.gamma, cv["riemann_solver"], cv["limiter"], 0.0, flow.mu_inf,
+                      flow.sutherland_ratio)
+    yield z, dev
+    dev.close()
+
+
+def rows_rel(a, b):
+    return max(float(np.abs(a[k] - b[k]).max() / max(np.abs(b[k]).max(), 1e-300)) for k in range(a.shape[0]))
+
+
+@pytest.mark.parametrize("state", ["sin", "rand0"])
+def test_residual3d_matches_the_reference(cuda, device3d, state):
+    z, dev = device3d
+    U = z[f"{state}_U"]
+    assert rows_rel(dev.residual(U), z[f"{state}_R2"]) < 1e-12
+    assert rows_rel(dev.residual(U, first_order=True), z[f"{state}_R1"]) < 1e-12
+
+
+@pytest.mark.parametrize("state", ["sin", "rand0"])
+def test_jvp3d_matches_the_reference(cuda, device3d, state):
+    z, dev = device3d
+    Jv, ref = dev.jvp(z[f"{state}_U"], z[f"{state}_v"]), z[f"{state}_Jv"]
+    assert rows_rel(Jv[:5], ref[:5]) < 1e-12
+    assert rows_rel(Jv[5:], ref[5:]) < 1e-10

@@ -94,3 +94,33 @@ def test_chains_walls_and_distance_match_the_reference(golden, plan):
     assert np.array_equal(plan.walls.face, golden["walls_face"])
     assert np.array_equal(plan.walls.into_fluid, golden["walls_into_fluid"])
     assert np.allclose(plan.distance, golden["distance"], rtol=1e-14, atol=0.0)
+
+
+def test_ghost_records_reproduce_the_gather_fill(golden, plan):
+    """The device runs each ghost stage as records (one per ghost the stage writes); run
+    on the host with the oracle's conditions, they give the reference's gather fill."""
+    import json as _json
+    from jaxrans_b200.case import _flow
+    from jaxrans_b200.native3d import KIND3, records_of
+    from oracle import numerics3d as n3
+    flow = _flow(_json.loads(str(golden["case_json"]))["case"])
+    a = flow.alpha_rad
+    q_inf = np.array([1.0, flow.mach * np.cos(a), 0.0, flow.mach * np.sin(a), 1.0 / flow.gamma, flow.nu_tilde_ratio])
+    model = n3.Model3(plan, q_inf, flow.gamma, "hllc", "van_albada_smooth", 0.0, flow.mu_inf,
+                      flow.sutherland_ratio, True, plan.distance)
+    q = n3.prim(golden["rand0_U"], flow.gamma)
+    rec = records_of(plan)
+    assert rec.counts.sum() == len(rec.ghost) and np.all(rec.ghost < plan.n_canvas)
+    names = {code: name for name, code in KIND3.items()}
+    flat = q.reshape(q.shape[0], -1).copy()
+    at = 0
+    for count in rec.counts:
+        g, s, k, nrm = (x[at:at + count] for x in (rec.ghost, rec.source, rec.kind, rec.normal))
+        new = flat.copy()
+        for code in np.unique(k):
+            m = k == code
+            vals = flat[:, s[m]]
+            new[:, g[m]] = vals if code == 0 else n3._condition(names[int(code)], vals, nrm[m].T, model)
+        flat = new
+        at += count
+    assert np.array_equal(flat.reshape(q.shape), n3.fill_ghosts(q, model))
