@@ -61,7 +61,7 @@ GENERATED = ("o_grid", "c_grid")
 SECTION = ("multi_element",)
 MADE = GENERATED + SECTION
 GRIDS = ("c_grid", "file", "multi_element", "o_grid")
-BUILT_GRIDS = ("c_grid", "o_grid")
+BUILT_GRIDS = ("c_grid", "file", "o_grid")
 
 CASE = {
     "general": (Key("case_name", "string", REQUIRED), Key("description", "string", None),
@@ -154,11 +154,41 @@ class GridSpec:
     reference_length: float = 1.0
     reference_area: float | None = None
     moment_centre: tuple = (0.25, 0.0, 0.0)
+    file: str | None = None
+    format: str = "auto"
+    coordinate_scale: float = 1.0
+    patches: tuple = ()
+
+    def resolve(self, base: Path) -> Path:
+        """The grid file, relative to the case directory or the working directory
+        (``src/jaxrans/case/domain.py:122-129``)."""
+        for root in (Path(base), Path.cwd()):
+            path = Path(self.file) if Path(self.file).is_absolute() else root / self.file
+            if path.is_file():
+                return path
+        raise CaseError(f"'domain.file' {self.file!r} not found in {base} or {Path.cwd()}")
 
     def build(self, base: Path) -> list[Block]:
         if self.grid not in BUILT_GRIDS:
             raise CaseError(f"'domain.grid' = {self.grid!r} is not implemented in this build; "
                             f"choose from {sorted(BUILT_GRIDS)}")
+        if self.grid == "file":
+            from .gridfile import PatchRule, load_grid, read_plot3d_2d
+            path = self.resolve(base)
+            if self.format == "cgns" or path.suffix.lower() == ".cgns":
+                raise CaseError("a CGNS grid file is not implemented in this build; use Plot3D")
+            try:
+                read_plot3d_2d(path)
+            except ValueError as error:
+                if "not a 2D plane" in str(error):
+                    raise CaseError("a 3D grid file is not implemented in this build's case loader "
+                                    "(the 3D plan is built from jaxrans_b200.grid3d blocks)") from None
+                raise CaseError(str(error)) from None
+            try:
+                rules = tuple(PatchRule(**rule) for rule in self.patches)
+            except TypeError as error:
+                raise CaseError(f"'domain.patches': {error}") from None
+            return load_grid(path, self.coordinate_scale, rules)
         section = section_source(self.airfoil, base).normalised()
         if self.trailing_edge == "close" and not section.sharp:
             raise CaseError("'domain.trailing_edge' = 'close' on a blunt section is not implemented in this build")
@@ -254,7 +284,8 @@ def _grid_spec(case_doc: dict) -> GridSpec:
                     wall_spacing=domain["wall_spacing"], far_field=domain["far_field"],
                     trailing_edge=domain["trailing_edge"], normal_stretching=domain["normal_stretching"],
                     reference_length=domain["reference_length"], reference_area=domain["reference_area"],
-                    moment_centre=tuple(domain["moment_centre"]))
+                    moment_centre=tuple(domain["moment_centre"]), file=domain["file"], format=domain["format"],
+                    coordinate_scale=domain["coordinate_scale"], patches=tuple(domain["patches"] or ()))
 
 
 def _flow(case_doc: dict) -> FlowConditions:
