@@ -109,24 +109,6 @@ namespace jr {
 // shared with the 3D entry points (capi3d.cu)
 int report_error(int code, const std::string& msg) { return fail(code, msg); }
 
-// SA-noft2 constants (src/jaxrans/physics/spalart_allmaras.py:66-89) and the derived ones
-void sa_constants(SAConst& s) {
-  s.c_b1 = 0.1355;
-  s.sigma = 2.0 / 3.0;
-  s.c_b2 = 0.622;
-  s.kappa = 0.41;
-  s.c_w2 = 0.3;
-  s.c_w3 = 2.0;
-  s.c_v1 = 7.1;
-  s.c_2 = 0.7;
-  s.c_3 = 0.9;
-  s.c_n1 = 16.0;
-  s.r_max = 10.0;
-  s.c_w1 = s.c_b1 / (s.kappa * s.kappa) + (1.0 + s.c_b2) / s.sigma;
-  s.c_v1_3 = s.c_v1 * s.c_v1 * s.c_v1;
-  s.c_w3_6 = s.c_w3 * s.c_w3 * s.c_w3 * s.c_w3 * s.c_w3 * s.c_w3;
-  s.c_2_2 = s.c_2 * s.c_2;
-}
 }  // namespace jr
 
 static int cuda_check(const char* where) {

@@ -5,11 +5,10 @@
 #include <vector>
 
 #include "../../include/jaxrans_b200.h"
-#include "device3d.cuh"
+#include "plan3d_desc.cuh"
 
 namespace jr {
 int report_error(int code, const std::string& msg);
-void sa_constants(SAConst& s);
 }  // namespace jr
 
 using namespace jr;
@@ -110,24 +109,7 @@ int jr_plan3d_create(const jr_plan3d_desc* d, jr_plan3d** out) {
   TRY3(copy3(p, &dv.g_source, d->source, n_rec));
   TRY3(copy3(p, &dv.g_kind, d->kind, n_rec));
   TRY3(copy3(p, &dv.g_normal, d->normal, 3 * n_rec));
-  Physics3& P = dv.P;
-  P.gamma = d->gamma;
-  P.mu_inf = d->mu_inf > 0.0 ? d->mu_inf : 0.0;
-  P.sutherland = d->sutherland;
-  P.kappa = d->kappa;
-  P.flux = d->flux;
-  P.limiter = d->limiter;
-  for (int v = 0; v < NV3_MAX; ++v) P.q_inf[v] = v < d->nvar ? d->q_inf[v] : 0.0;
-  {
-    const double g = d->gamma, rho = P.q_inf[0], u = P.q_inf[1], v = P.q_inf[2], w = P.q_inf[3], pr = P.q_inf[4];
-    P.U_inf[0] = rho;
-    P.U_inf[1] = rho * u;
-    P.U_inf[2] = rho * v;
-    P.U_inf[3] = rho * w;
-    P.U_inf[4] = pr / (g - 1.0) + 0.5 * rho * ((u * u + v * v) + w * w);
-    P.U_inf[5] = rho * P.q_inf[5];
-  }
-  sa_constants(P.sa);
+  physics3_from_desc(dv.P, d);
   const size_t work = (size_t)d->nvar * n * sizeof(Dual);
   if (cudaMalloc(&p->A, work) != cudaSuccess || (p->allocs.push_back(p->A), cudaMalloc(&p->B, work)) != cudaSuccess) {
     jr_plan3d_destroy(p);

@@ -43,21 +43,21 @@ struct Plan3Dev {
   Physics3 P;
 };
 
-template <class T> __device__ __forceinline__ T mk(double v, double d);
-template <> __device__ __forceinline__ double mk<double>(double v, double) { return v; }
-template <> __device__ __forceinline__ Dual mk<Dual>(double v, double d) { return Dual{v, d}; }
+template <class T> __host__ __device__ __forceinline__ T mk(double v, double d);
+template <> __host__ __device__ __forceinline__ double mk<double>(double v, double) { return v; }
+template <> __host__ __device__ __forceinline__ Dual mk<Dual>(double v, double d) { return Dual{v, d}; }
 
-__device__ __forceinline__ double tangent_or_value(double x) { return x; }
-__device__ __forceinline__ double tangent_or_value(const Dual& x) { return x.d; }
+__host__ __device__ __forceinline__ double tangent_or_value(double x) { return x; }
+__host__ __device__ __forceinline__ double tangent_or_value(const Dual& x) { return x.d; }
 
-template <class T> __device__ __forceinline__ T viscosity3(const Physics3& P, T Tt) {
+template <class T> __host__ __device__ __forceinline__ T viscosity3(const Physics3& P, T Tt) {
   if (P.sutherland < 0.0) return cst<T>(P.mu_inf);
   double s = P.sutherland;
   return P.mu_inf * Tt * dsqrt(Tt) * (1.0 + s) / (Tt + s);
 }
 
 // (rho, u, v, w, p[, nu~]) from (rho, rho u, rho v, rho w, E[, rho nu~])
-template <class T> __device__ __forceinline__ void to_prim3(const T* U, T* q, int nvar, double g) {
+template <class T> __host__ __device__ __forceinline__ void to_prim3(const T* U, T* q, int nvar, double g) {
   T rho = U[0];
   T u = U[1] / rho, v = U[2] / rho, w = U[3] / rho;
   q[0] = rho;
@@ -68,13 +68,13 @@ template <class T> __device__ __forceinline__ void to_prim3(const T* U, T* q, in
   if (nvar > 5) q[5] = U[5] / rho;
 }
 
-template <class T> __device__ __forceinline__ T dot3(const T* a, const double* n) {
+template <class T> __host__ __device__ __forceinline__ T dot3(const T* a, const double* n) {
   return (a[0] * n[0] + a[1] * n[1]) + a[2] * n[2];
 }
 
-template <class T> __device__ __forceinline__ T sq3(const T* a) { return (a[0] * a[0] + a[1] * a[1]) + a[2] * a[2]; }
+template <class T> __host__ __device__ __forceinline__ T sq3(const T* a) { return (a[0] * a[0] + a[1] * a[1]) + a[2] * a[2]; }
 
-template <class T> __device__ __forceinline__ void normal_flux3(const T* q, const double* n, double g, T* F) {
+template <class T> __host__ __device__ __forceinline__ void normal_flux3(const T* q, const double* n, double g, T* F) {
   T vn = dot3(q + 1, n);
   T E = q[4] / (g - 1.0) + 0.5 * q[0] * sq3(q + 1);
   F[0] = q[0] * vn;
@@ -83,7 +83,7 @@ template <class T> __device__ __forceinline__ void normal_flux3(const T* q, cons
 }
 
 template <class T>
-__device__ __forceinline__ void roe_average3(const T* qL, const T* qR, double g, T& rho, T* vel, T& H, T& a) {
+__host__ __device__ __forceinline__ void roe_average3(const T* qL, const T* qR, double g, T& rho, T* vel, T& H, T& a) {
   T hl = g / (g - 1.0) * qL[4] / qL[0] + 0.5 * sq3(qL + 1);
   T hr = g / (g - 1.0) * qR[4] / qR[0] + 0.5 * sq3(qR + 1);
   T w = dsqrt(qR[0] / qL[0]);
@@ -95,14 +95,14 @@ __device__ __forceinline__ void roe_average3(const T* qL, const T* qR, double g,
   a = dsqrt(dmax(a2, 1e-30));
 }
 
-__device__ __forceinline__ double unit3(const double* s, double* n) {
+__host__ __device__ __forceinline__ double unit3(const double* s, double* n) {
   const double len = sqrt((s[0] * s[0] + s[1] * s[1]) + s[2] * s[2]);
   const double safe = fmax(len, 1e-300);
   for (int m = 0; m < 3; ++m) n[m] = s[m] / safe;
   return len;
 }
 
-template <class T> __device__ __forceinline__ void hllc3(const T* qL, const T* qR, const double* s, double g, T* F) {
+template <class T> __host__ __device__ __forceinline__ void hllc3(const T* qL, const T* qR, const double* s, double g, T* F) {
   double n[3];
   const double len = unit3(s, n);
   T vnl = dot3(qL + 1, n), vnr = dot3(qR + 1, n);
@@ -139,7 +139,7 @@ template <class T> __device__ __forceinline__ void hllc3(const T* qL, const T* q
   for (int k = 0; k < 5; ++k) F[k] = len * f[k];
 }
 
-template <class T> __device__ __forceinline__ void roe3(const T* qL, const T* qR, const double* s, double g, T* F) {
+template <class T> __host__ __device__ __forceinline__ void roe3(const T* qL, const T* qR, const double* s, double g, T* F) {
   double n[3];
   const double len = unit3(s, n);
   T rho, vel[3], H, a;
@@ -170,7 +170,7 @@ template <class T> __device__ __forceinline__ void roe3(const T* qL, const T* qR
   }
 }
 
-template <class T> __device__ __forceinline__ void riemann3(int kind, const T* qL, const T* qR, const double* s,
+template <class T> __host__ __device__ __forceinline__ void riemann3(int kind, const T* qL, const T* qR, const double* s,
                                                              double g, T* F) {
   if (kind == 0)
     hllc3(qL, qR, s, g, F);
@@ -180,7 +180,7 @@ template <class T> __device__ __forceinline__ void riemann3(int kind, const T* q
 
 // a ghost's primitive state from its source cell's (src/jaxrans/numerics/boundary.py:54-130)
 template <class T>
-__device__ __forceinline__ void condition3(int kind, const T* q, double nx, double ny, double nz, const Physics3& P,
+__host__ __device__ __forceinline__ void condition3(int kind, const T* q, double nx, double ny, double nz, const Physics3& P,
                                            int nvar, T* o) {
   const double n[3] = {nx, ny, nz};
   for (int v = 0; v < nvar; ++v) o[v] = q[v];

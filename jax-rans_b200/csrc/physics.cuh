@@ -17,61 +17,61 @@ struct Dual {
   double v, d;
 };
 
-__device__ __forceinline__ double val(double x) { return x; }
-__device__ __forceinline__ double val(const Dual& x) { return x.v; }
+__host__ __device__ __forceinline__ double val(double x) { return x; }
+__host__ __device__ __forceinline__ double val(const Dual& x) { return x.v; }
 
-template <class T> __device__ __forceinline__ T cst(double x);
-template <> __device__ __forceinline__ double cst<double>(double x) { return x; }
-template <> __device__ __forceinline__ Dual cst<Dual>(double x) { return Dual{x, 0.0}; }
+template <class T> __host__ __device__ __forceinline__ T cst(double x);
+template <> __host__ __device__ __forceinline__ double cst<double>(double x) { return x; }
+template <> __host__ __device__ __forceinline__ Dual cst<Dual>(double x) { return Dual{x, 0.0}; }
 
-__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
-__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
-__device__ __forceinline__ Dual operator-(Dual a) { return {-a.v, -a.d}; }
-__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
-__device__ __forceinline__ Dual operator/(Dual a, Dual b) {
+__host__ __device__ __forceinline__ Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+__host__ __device__ __forceinline__ Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+__host__ __device__ __forceinline__ Dual operator-(Dual a) { return {-a.v, -a.d}; }
+__host__ __device__ __forceinline__ Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+__host__ __device__ __forceinline__ Dual operator/(Dual a, Dual b) {
   double q = a.v / b.v;
   return {q, (a.d - q * b.d) / b.v};
 }
-__device__ __forceinline__ Dual operator+(Dual a, double b) { return {a.v + b, a.d}; }
-__device__ __forceinline__ Dual operator+(double a, Dual b) { return {a + b.v, b.d}; }
-__device__ __forceinline__ Dual operator-(Dual a, double b) { return {a.v - b, a.d}; }
-__device__ __forceinline__ Dual operator-(double a, Dual b) { return {a - b.v, -b.d}; }
-__device__ __forceinline__ Dual operator*(Dual a, double b) { return {a.v * b, a.d * b}; }
-__device__ __forceinline__ Dual operator*(double a, Dual b) { return {a * b.v, a * b.d}; }
-__device__ __forceinline__ Dual operator/(Dual a, double b) { return {a.v / b, a.d / b}; }
-__device__ __forceinline__ Dual operator/(double a, Dual b) {
+__host__ __device__ __forceinline__ Dual operator+(Dual a, double b) { return {a.v + b, a.d}; }
+__host__ __device__ __forceinline__ Dual operator+(double a, Dual b) { return {a + b.v, b.d}; }
+__host__ __device__ __forceinline__ Dual operator-(Dual a, double b) { return {a.v - b, a.d}; }
+__host__ __device__ __forceinline__ Dual operator-(double a, Dual b) { return {a - b.v, -b.d}; }
+__host__ __device__ __forceinline__ Dual operator*(Dual a, double b) { return {a.v * b, a.d * b}; }
+__host__ __device__ __forceinline__ Dual operator*(double a, Dual b) { return {a * b.v, a * b.d}; }
+__host__ __device__ __forceinline__ Dual operator/(Dual a, double b) { return {a.v / b, a.d / b}; }
+__host__ __device__ __forceinline__ Dual operator/(double a, Dual b) {
   double q = a / b.v;
   return {q, -q * b.d / b.v};
 }
 
-__device__ __forceinline__ double dsqrt(double x) { return sqrt(x); }
-__device__ __forceinline__ Dual dsqrt(Dual x) {
+__host__ __device__ __forceinline__ double dsqrt(double x) { return sqrt(x); }
+__host__ __device__ __forceinline__ Dual dsqrt(Dual x) {
   double s = sqrt(x.v);
   return {s, x.d * (0.5 / s)};
 }
 // x**c for a constant exponent (pow's JVP: c x^(c-1) t)
-__device__ __forceinline__ double dpow(double x, double c) { return pow(x, c); }
-__device__ __forceinline__ Dual dpow(Dual x, double c) {
+__host__ __device__ __forceinline__ double dpow(double x, double c) { return pow(x, c); }
+__host__ __device__ __forceinline__ Dual dpow(Dual x, double c) {
   return {pow(x.v, c), x.d * (c * pow(x.v, c - 1.0))};
 }
-__device__ __forceinline__ double dabs(double x) { return x >= 0.0 ? x : -x; }
-__device__ __forceinline__ Dual dabs(Dual x) { return x.v >= 0.0 ? x : -x; }
-__device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : (b > a ? b : a); }
-__device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : (b < a ? b : a); }
-__device__ __forceinline__ Dual dmax(Dual a, Dual b) {
+__host__ __device__ __forceinline__ double dabs(double x) { return x >= 0.0 ? x : -x; }
+__host__ __device__ __forceinline__ Dual dabs(Dual x) { return x.v >= 0.0 ? x : -x; }
+__host__ __device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : (b > a ? b : a); }
+__host__ __device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : (b < a ? b : a); }
+__host__ __device__ __forceinline__ Dual dmax(Dual a, Dual b) {
   return a.v > b.v ? a : (b.v > a.v ? b : Dual{a.v, 0.5 * (a.d + b.d)});
 }
-__device__ __forceinline__ Dual dmin(Dual a, Dual b) {
+__host__ __device__ __forceinline__ Dual dmin(Dual a, Dual b) {
   return a.v < b.v ? a : (b.v < a.v ? b : Dual{a.v, 0.5 * (a.d + b.d)});
 }
-__device__ __forceinline__ Dual dmax(Dual a, double b) { return dmax(a, Dual{b, 0.0}); }
-__device__ __forceinline__ Dual dmin(Dual a, double b) { return dmin(a, Dual{b, 0.0}); }
-template <class T> __device__ __forceinline__ T sel(bool c, const T& a, const T& b) { return c ? a : b; }
-__device__ __forceinline__ Dual sel(bool c, const Dual& a, double b) { return c ? a : Dual{b, 0.0}; }
-__device__ __forceinline__ Dual sel(bool c, double a, const Dual& b) { return c ? Dual{a, 0.0} : b; }
-__device__ __forceinline__ double sel(bool c, double a, double b) { return c ? a : b; }
-template <class T> __device__ __forceinline__ T ipow3(T x) { return x * (x * x); }
-template <class T> __device__ __forceinline__ T ipow6(T x) {
+__host__ __device__ __forceinline__ Dual dmax(Dual a, double b) { return dmax(a, Dual{b, 0.0}); }
+__host__ __device__ __forceinline__ Dual dmin(Dual a, double b) { return dmin(a, Dual{b, 0.0}); }
+template <class T> __host__ __device__ __forceinline__ T sel(bool c, const T& a, const T& b) { return c ? a : b; }
+__host__ __device__ __forceinline__ Dual sel(bool c, const Dual& a, double b) { return c ? a : Dual{b, 0.0}; }
+__host__ __device__ __forceinline__ Dual sel(bool c, double a, const Dual& b) { return c ? Dual{a, 0.0} : b; }
+__host__ __device__ __forceinline__ double sel(bool c, double a, double b) { return c ? a : b; }
+template <class T> __host__ __device__ __forceinline__ T ipow3(T x) { return x * (x * x); }
+template <class T> __host__ __device__ __forceinline__ T ipow6(T x) {
   T x2 = x * x;
   return x2 * (x2 * x2);
 }
@@ -81,6 +81,25 @@ struct SAConst {
   double c_b1, sigma, c_b2, kappa, c_w2, c_w3, c_v1, c_2, c_3, c_n1, r_max;
   double c_w1, c_v1_3, c_w3_6, c_2_2;  // derived, evaluated on the host
 };
+
+// SA-noft2 constants (src/jaxrans/physics/spalart_allmaras.py:66-89) and the derived ones
+inline void sa_constants(SAConst& s) {
+  s.c_b1 = 0.1355;
+  s.sigma = 2.0 / 3.0;
+  s.c_b2 = 0.622;
+  s.kappa = 0.41;
+  s.c_w2 = 0.3;
+  s.c_w3 = 2.0;
+  s.c_v1 = 7.1;
+  s.c_2 = 0.7;
+  s.c_3 = 0.9;
+  s.c_n1 = 16.0;
+  s.r_max = 10.0;
+  s.c_w1 = s.c_b1 / (s.kappa * s.kappa) + (1.0 + s.c_b2) / s.sigma;
+  s.c_v1_3 = s.c_v1 * s.c_v1 * s.c_v1;
+  s.c_w3_6 = s.c_w3 * s.c_w3 * s.c_w3 * s.c_w3 * s.c_w3 * s.c_w3;
+  s.c_2_2 = s.c_2 * s.c_2;
+}
 
 // Everything a residual evaluation needs that is not per cell.
 struct Physics {
@@ -99,14 +118,14 @@ struct Physics {
   SAConst sa;
 };
 
-template <class T> __device__ __forceinline__ T viscosity(const Physics& P, T Tt) {
+template <class T> __host__ __device__ __forceinline__ T viscosity(const Physics& P, T Tt) {
   if (P.sutherland < 0.0) return cst<T>(P.mu_inf);
   double s = P.sutherland;
   return P.mu_inf * Tt * dsqrt(Tt) * (1.0 + s) / (Tt + s);
 }
 
 // primitive (rho, u, v, p[, nu_hat]) from conservative
-template <class T> __device__ __forceinline__ void to_prim(const T* U, T* q, int nvar, double g) {
+template <class T> __host__ __device__ __forceinline__ void to_prim(const T* U, T* q, int nvar, double g) {
   T rho = U[0];
   T u = U[1] / rho, v = U[2] / rho;
   q[0] = rho;
@@ -117,7 +136,7 @@ template <class T> __device__ __forceinline__ void to_prim(const T* U, T* q, int
 }
 
 // ---- limiters on differences (src/jaxrans/numerics/limiters.py:61-116)
-template <class T> __device__ __forceinline__ T limit(const T& a, const T& b, int kind) {
+template <class T> __host__ __device__ __forceinline__ T limit(const T& a, const T& b, int kind) {
   if (kind == 1) {  // minmod
     double ab = val(a * b);
     if (!(ab > 0.0)) return cst<T>(0.0);
@@ -138,7 +157,7 @@ template <class T> __device__ __forceinline__ T limit(const T& a, const T& b, in
 
 // ---- Euler flux and Riemann solvers (src/jaxrans/numerics/riemann.py:47-198)
 template <class T>
-__device__ __forceinline__ void normal_flux(const T* q, double nx, double ny, double g, T* F) {
+__host__ __device__ __forceinline__ void normal_flux(const T* q, double nx, double ny, double g, T* F) {
   T vn = q[1] * nx + q[2] * ny;
   T E = q[3] / (g - 1.0) + 0.5 * q[0] * (q[1] * q[1] + q[2] * q[2]);
   F[0] = q[0] * vn;
@@ -148,7 +167,7 @@ __device__ __forceinline__ void normal_flux(const T* q, double nx, double ny, do
 }
 
 template <class T>
-__device__ __forceinline__ void roe_average(const T* qL, const T* qR, double g, T& rho, T& u, T& v, T& H, T& a) {
+__host__ __device__ __forceinline__ void roe_average(const T* qL, const T* qR, double g, T& rho, T& u, T& v, T& H, T& a) {
   T hl = g / (g - 1.0) * qL[3] / qL[0] + 0.5 * (qL[1] * qL[1] + qL[2] * qL[2]);
   T hr = g / (g - 1.0) * qR[3] / qR[0] + 0.5 * (qR[1] * qR[1] + qR[2] * qR[2]);
   T w = dsqrt(qR[0] / qL[0]);
@@ -162,7 +181,7 @@ __device__ __forceinline__ void roe_average(const T* qL, const T* qR, double g, 
 }
 
 template <class T>
-__device__ __forceinline__ void hllc_flux(const T* qL, const T* qR, double sx, double sy, double g, T* F) {
+__host__ __device__ __forceinline__ void hllc_flux(const T* qL, const T* qR, double sx, double sy, double g, T* F) {
   double len = hypot(sx, sy);
   double safe = fmax(len, 1e-300);
   double nx = sx / safe, ny = sy / safe;
@@ -204,7 +223,7 @@ __device__ __forceinline__ void hllc_flux(const T* qL, const T* qR, double sx, d
 }
 
 template <class T>
-__device__ __forceinline__ void roe_flux(const T* qL, const T* qR, double sx, double sy, double g, T* F) {
+__host__ __device__ __forceinline__ void roe_flux(const T* qL, const T* qR, double sx, double sy, double g, T* F) {
   double len = hypot(sx, sy);
   double safe = fmax(len, 1e-300);
   double nx = sx / safe, ny = sy / safe;
@@ -237,7 +256,7 @@ __device__ __forceinline__ void roe_flux(const T* qL, const T* qR, double sx, do
 }
 
 template <class T>
-__device__ __forceinline__ void riemann(int kind, const T* qL, const T* qR, double sx, double sy, double g, T* F) {
+__host__ __device__ __forceinline__ void riemann(int kind, const T* qL, const T* qR, double sx, double sy, double g, T* F) {
   if (kind == 0)
     hllc_flux(qL, qR, sx, sy, g, F);
   else
@@ -245,25 +264,25 @@ __device__ __forceinline__ void riemann(int kind, const T* qL, const T* qR, doub
 }
 
 // ---- Spalart-Allmaras pieces (src/jaxrans/physics/spalart_allmaras.py:119-195)
-template <class T> __device__ __forceinline__ T eddy_viscosity(const SAConst& c, T rho, T nut, T nu) {
+template <class T> __host__ __device__ __forceinline__ T eddy_viscosity(const SAConst& c, T rho, T nut, T nu) {
   if (!(val(nut) > 0.0)) return cst<T>(0.0);
   T chi = nut / nu;
   T chi3 = ipow3(chi);
   return rho * nut * (chi3 / (chi3 + c.c_v1_3));
 }
 
-template <class T> __device__ __forceinline__ T f_n(const SAConst& c, T nut, T nu) {
+template <class T> __host__ __device__ __forceinline__ T f_n(const SAConst& c, T nut, T nu) {
   if (val(nut) >= 0.0) return cst<T>(1.0);
   T chi3 = ipow3(nut / nu);
   return (c.c_n1 + chi3) / (c.c_n1 - chi3);
 }
 
-template <class T> __device__ __forceinline__ T diffusion_coefficient(const SAConst& c, T rho, T nut, T mu) {
+template <class T> __host__ __device__ __forceinline__ T diffusion_coefficient(const SAConst& c, T rho, T nut, T mu) {
   T nu = mu / rho;
   return (mu + rho * nut * f_n(c, nut, nu)) / c.sigma;
 }
 
-template <class T> __device__ __forceinline__ T s_tilde(const SAConst& c, T omega, T nut, T nu, double d) {
+template <class T> __host__ __device__ __forceinline__ T s_tilde(const SAConst& c, T omega, T nut, T nu, double d) {
   T chi = nut / nu;
   T chi3 = ipow3(chi);
   T fv1 = chi3 / (chi3 + c.c_v1_3);
@@ -276,12 +295,12 @@ template <class T> __device__ __forceinline__ T s_tilde(const SAConst& c, T omeg
   return omega + omega * (c.c_2_2 * omega + c.c_3 * sbar) / den;
 }
 
-template <class T> __device__ __forceinline__ T f_w(const SAConst& c, T r) {
+template <class T> __host__ __device__ __forceinline__ T f_w(const SAConst& c, T r) {
   T gg = r + c.c_w2 * (ipow6(r) - r);
   return gg * dpow((1.0 + c.c_w3_6) / (ipow6(gg) + c.c_w3_6), 1.0 / 6.0);
 }
 
-template <class T> __device__ __forceinline__ T r_of(const SAConst& c, T nut, T st, double d) {
+template <class T> __host__ __device__ __forceinline__ T r_of(const SAConst& c, T nut, T st, double d) {
   double kd = c.kappa * d;
   T den = st * (kd * kd);
   if (!(val(den) > 0.0)) return cst<T>(c.r_max);
@@ -290,7 +309,7 @@ template <class T> __device__ __forceinline__ T r_of(const SAConst& c, T nut, T 
 
 // (production, destruction) per unit mass (src/jaxrans/physics/spalart_allmaras.py:165-177)
 template <class T>
-__device__ __forceinline__ void sa_source(const SAConst& c, T nut, T nu, T omega, double d, T& P, T& D) {
+__host__ __device__ __forceinline__ void sa_source(const SAConst& c, T nut, T nu, T omega, double d, T& P, T& D) {
   bool pos = val(nut) >= 0.0;
   T st = s_tilde(c, omega, pos ? nut : cst<T>(0.0), nu, d);
   T w = nut / d;
@@ -301,7 +320,7 @@ __device__ __forceinline__ void sa_source(const SAConst& c, T nut, T nu, T omega
 
 // ---- boundary conditions on primitives (src/jaxrans/numerics/boundary.py:67-158)
 template <class T>
-__device__ __forceinline__ void characteristic(const T* e, double nx, double ny, const T* qf, int nvar, double g,
+__host__ __device__ __forceinline__ void characteristic(const T* e, double nx, double ny, const T* qf, int nvar, double g,
                                                T* out) {
   T ai = dsqrt(g * e[3] / e[0]);
   T af = dsqrt(g * qf[3] / qf[0]);

@@ -92,6 +92,48 @@ def apply_records(records: Records, q: np.ndarray) -> np.ndarray:
     return flat.reshape(q.shape)
 
 
+def describe(plan: Plan3, q_inf, gamma: float, flux: str, limiter: str, kappa: float = 0.0,
+             mu_inf: float | None = None, sutherland: float | None = None):
+    """``(jr_plan3d_desc, arrays it points into)`` for ``plan`` and the physics; keep the
+    arrays alive while the descriptor is used."""
+    rec = records_of(plan)
+    keep = []
+
+    def arr(a, dtype):
+        a = np.ascontiguousarray(a, dtype=dtype)
+        keep.append(a)
+        return a
+
+    def ptr(a, t):
+        return a.ctypes.data_as(t)
+
+    nvar = len(q_inf)
+    d = Plan3Desc()
+    d.NI, d.NJ, d.NK = plan.shape
+    d.nvar = nvar
+    d.interior = ptr(arr(plan.interior, np.uint8), _u8p)
+    d.volume = ptr(arr(plan.volume, np.float64), _f64p)
+    for a in range(3):
+        d.faces[a] = ptr(arr(plan.faces[a], np.float64), _f64p)
+    d.centres = ptr(arr(plan.centres, np.float64), _f64p)
+    d.distance = ptr(arr(plan.distance, np.float64), _f64p) if plan.distance is not None else None
+    d.n_stages = len(rec.counts)
+    d.stage_records = ptr(arr(rec.counts, np.int32), _i32p)
+    d.ghost = ptr(arr(rec.ghost, np.int32), _i32p)
+    d.source = ptr(arr(rec.source, np.int32), _i32p)
+    d.kind = ptr(arr(rec.kind, np.int32), _i32p)
+    d.normal = ptr(arr(rec.normal, np.float64), _f64p)
+    d.gamma = gamma
+    d.mu_inf = 0.0 if mu_inf is None else mu_inf
+    d.sutherland = -1.0 if sutherland is None else sutherland
+    d.kappa = kappa
+    d.flux = FLUX_CODES[flux]
+    d.limiter = 4 if kappa != 0.0 else LIMITER_CODES[limiter]
+    for v in range(6):
+        d.q_inf[v] = float(q_inf[v]) if v < nvar else 0.0
+    return d, keep
+
+
 class DevicePlan3:
     """One 3D case on the device: residual and J.v of canvas fields (``(nvar, NI, NJ,
     NK)`` float64 NumPy arrays in and out)."""
@@ -102,40 +144,7 @@ class DevicePlan3:
         self.plan = plan
         self.nvar = len(q_inf)
         self.shape = (self.nvar,) + plan.shape
-        rec = records_of(plan)
-        keep = []
-
-        def arr(a, dtype):
-            a = np.ascontiguousarray(a, dtype=dtype)
-            keep.append(a)
-            return a
-
-        def ptr(a, t):
-            return a.ctypes.data_as(t)
-
-        d = Plan3Desc()
-        d.NI, d.NJ, d.NK = plan.shape
-        d.nvar = self.nvar
-        d.interior = ptr(arr(plan.interior, np.uint8), _u8p)
-        d.volume = ptr(arr(plan.volume, np.float64), _f64p)
-        for a in range(3):
-            d.faces[a] = ptr(arr(plan.faces[a], np.float64), _f64p)
-        d.centres = ptr(arr(plan.centres, np.float64), _f64p)
-        d.distance = ptr(arr(plan.distance, np.float64), _f64p) if plan.distance is not None else None
-        d.n_stages = len(rec.counts)
-        d.stage_records = ptr(arr(rec.counts, np.int32), _i32p)
-        d.ghost = ptr(arr(rec.ghost, np.int32), _i32p)
-        d.source = ptr(arr(rec.source, np.int32), _i32p)
-        d.kind = ptr(arr(rec.kind, np.int32), _i32p)
-        d.normal = ptr(arr(rec.normal, np.float64), _f64p)
-        d.gamma = gamma
-        d.mu_inf = 0.0 if mu_inf is None else mu_inf
-        d.sutherland = -1.0 if sutherland is None else sutherland
-        d.kappa = kappa
-        d.flux = FLUX_CODES[flux]
-        d.limiter = 4 if kappa != 0.0 else LIMITER_CODES[limiter]
-        for v in range(6):
-            d.q_inf[v] = float(q_inf[v]) if v < self.nvar else 0.0
+        d, keep = describe(plan, q_inf, gamma, flux, limiter, kappa, mu_inf, sutherland)
         handle = C.c_void_p()
         _check(self.lib, self.lib.jr_plan3d_create(C.byref(d), C.byref(handle)), "jr_plan3d_create")
         self.handle = handle
