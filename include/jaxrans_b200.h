@@ -263,6 +263,11 @@ typedef struct jr_plan3d_desc {
   double gamma, mu_inf, sutherland, kappa;   /* mu_inf 0: inviscid; sutherland < 0: constant viscosity */
   int32_t flux, limiter;        /* as jr_plan_desc */
   double q_inf[6];              /* primitive freestream (rho, u, v, w, p[, nu~ / nu_inf]) */
+  const int32_t* neighbours;    /* NI*NJ*NK: the partner across a block face, or the cell itself */
+  int32_t n_chains, chain_L;    /* line chains along each block's wall-normal index */
+  const int32_t* chain_cells;   /* [chain * chain_L + k], -1 past the chain's end */
+  const int32_t* chain_up_face; /* link k -> k+1: flat index into the three face families, concatenated */
+  const int32_t* chain_up_sign; /* +1 / -1 the link face vector out of / into cell k, 0 no link */
 } jr_plan3d_desc;
 
 /* Build a 3D plan (device copies of the tables, work buffers, a stream).  Every record
@@ -279,6 +284,16 @@ int jr_residual3d(jr_plan3d* plan, const double* U, double* R, int32_t first_ord
  * jax.linearize of the first-order residual (src/jaxrans/solvers/implicit.py:104-116).
  * Synchronises. */
 int jr_jvp3d(jr_plan3d* plan, const double* U, const double* v, double* Jv);
+/* lambda on every canvas face (device pointers), the three families back to
+ * back (family a: (NI+(a==0)) (NJ+(a==1)) (NK+(a==2)) faces): |V.S| + a|S| at the face-averaged
+ * state plus the thin-layer viscous term.  Replaces face_wave_speeds
+ * (src/jaxrans/numerics/residual.py:169-192) on a 3D atlas.  Synchronises. */
+int jr_wave_speeds3d(jr_plan3d* plan, const double* U, double* lam);
+/* z = M^-1 r of line_j at (U, cfl) (device pointers): the 5x5 mean-flow chains and the
+ * scalar SA chains along each block's wall-normal index, solved by block Thomas; cells
+ * on no chain copied.  Replaces get_preconditioner("line_j")(...)(U, lambdas, cfl) and
+ * its solve (src/jaxrans/solvers/preconditioners.py:209-306) on a 3D atlas.  Synchronises. */
+int jr_precondition3d(jr_plan3d* plan, const double* U, double cfl, const double* r, double* z);
 
 #ifdef __cplusplus
 }

@@ -18,6 +18,7 @@ struct jr_plan3d {
   std::vector<void*> allocs;
   void* A = nullptr;   // primitive canvases (Dual-sized: the J.v needs value and tangent)
   void* B = nullptr;
+  double* scratch = nullptr;   // the line solve's eliminated blocks: n_chains * chain_L * 30
   size_t n_canvas = 0;
   cudaStream_t st = nullptr;
 };
@@ -87,6 +88,22 @@ int jr_plan3d_create(const jr_plan3d_desc* d, jr_plan3d** out) {
       return report_error(JR_EINVAL, "a ghost record outside the canvas");
     if (d->kind[r] < 0 || d->kind[r] > 4) return report_error(JR_EINVAL, "unknown ghost record kind");
   }
+  // the neighbour map and the chains: every cell and face inside the canvas
+  if (!d->neighbours) return report_error(JR_EINVAL, "null neighbour map");
+  for (size_t c = 0; c < n; ++c)
+    if (d->neighbours[c] < 0 || (size_t)d->neighbours[c] >= n) return report_error(JR_EINVAL, "a neighbour outside the canvas");
+  const size_t n_faces = (size_t)(d->NI + 1) * d->NJ * d->NK + (size_t)d->NI * (d->NJ + 1) * d->NK +
+                         (size_t)d->NI * d->NJ * (d->NK + 1);
+  if (d->n_chains < 0 || d->chain_L < 0 || (d->n_chains > 0 && (d->chain_L < 1 || !d->chain_cells ||
+                                                                 !d->chain_up_face || !d->chain_up_sign)))
+    return report_error(JR_EINVAL, "bad chains");
+  const size_t n_links = (size_t)d->n_chains * d->chain_L;
+  for (size_t e = 0; e < n_links; ++e) {
+    if (d->chain_cells[e] < -1 || d->chain_cells[e] >= (int64_t)n) return report_error(JR_EINVAL, "a chain cell outside the canvas");
+    if (d->chain_up_face[e] < 0 || (size_t)d->chain_up_face[e] >= n_faces)
+      return report_error(JR_EINVAL, "a chain face outside the canvas");
+    if (d->chain_up_sign[e] < -1 || d->chain_up_sign[e] > 1) return report_error(JR_EINVAL, "a chain sign not in {-1, 0, 1}");
+  }
   jr_plan3d* p = new jr_plan3d();
   p->n_canvas = n;
   Plan3Dev& dv = p->dev;
@@ -109,7 +126,22 @@ int jr_plan3d_create(const jr_plan3d_desc* d, jr_plan3d** out) {
   TRY3(copy3(p, &dv.g_source, d->source, n_rec));
   TRY3(copy3(p, &dv.g_kind, d->kind, n_rec));
   TRY3(copy3(p, &dv.g_normal, d->normal, 3 * n_rec));
+  TRY3(copy3(p, &dv.neighbours, d->neighbours, n));
+  dv.n_chains = d->n_chains;
+  dv.chain_L = d->chain_L;
+  TRY3(copy3(p, &dv.ch_cells, d->chain_cells, n_links));
+  TRY3(copy3(p, &dv.ch_face, d->chain_up_face, n_links));
+  TRY3(copy3(p, &dv.ch_sign, d->chain_up_sign, n_links));
   physics3_from_desc(dv.P, d);
+  if (n_links > 0) {
+    void* sc = nullptr;
+    if (cudaMalloc(&sc, n_links * 30 * sizeof(double)) != cudaSuccess) {
+      jr_plan3d_destroy(p);
+      return report_error(JR_ENOMEM, "cudaMalloc failed");
+    }
+    p->allocs.push_back(sc);
+    p->scratch = static_cast<double*>(sc);
+  }
   const size_t work = (size_t)d->nvar * n * sizeof(Dual);
   if (cudaMalloc(&p->A, work) != cudaSuccess || (p->allocs.push_back(p->A), cudaMalloc(&p->B, work)) != cudaSuccess) {
     jr_plan3d_destroy(p);
@@ -141,6 +173,21 @@ int jr_jvp3d(jr_plan3d* plan, const double* U, const double* v, double* Jv) {
   launch_jvp3(plan->dev, U, v, Jv, plan->A, plan->B, plan->st);
   if (cudaStreamSynchronize(plan->st) != cudaSuccess) return check3("jr_jvp3d");
   return check3("jr_jvp3d");
+}
+
+int jr_wave_speeds3d(jr_plan3d* plan, const double* U, double* lam) {
+  if (!plan || !U || !lam) return report_error(JR_EINVAL, "null argument");
+  launch_wave_speeds3(plan->dev, U, lam, plan->st);
+  if (cudaStreamSynchronize(plan->st) != cudaSuccess) return check3("jr_wave_speeds3d");
+  return check3("jr_wave_speeds3d");
+}
+
+int jr_precondition3d(jr_plan3d* plan, const double* U, double cfl, const double* r, double* z) {
+  if (!plan || !U || !r || !z) return report_error(JR_EINVAL, "null argument");
+  if (!(cfl > 0.0)) return report_error(JR_EINVAL, "cfl must be positive");
+  launch_precondition3(plan->dev, U, cfl, r, z, plan->scratch, plan->st);
+  if (cudaStreamSynchronize(plan->st) != cudaSuccess) return check3("jr_precondition3d");
+  return check3("jr_precondition3d");
 }
 
 }  // extern "C"

@@ -40,6 +40,11 @@ struct Plan3Dev {
   const int* g_source;
   const int* g_kind;           // 0 copy, 1 slip wall, 2 no-slip wall, 3 symmetry, 4 far field
   const double* g_normal;      // 3 per record: the outward unit normal of the face
+  const int* neighbours;       // canvas: the partner across a block face, or the cell itself
+  int n_chains, chain_L;       // line chains along each block's wall-normal index
+  const int* ch_cells;         // [chain * chain_L + k], -1 past the chain's end
+  const int* ch_face;          // link k -> k+1: flat index into the three face families, concatenated
+  const int* ch_sign;          // +1 / -1: the link face's vector points out of / into cell k; 0 none
   Physics3 P;
 };
 
@@ -219,5 +224,8 @@ __host__ __device__ __forceinline__ void condition3(int kind, const T* q, double
 void launch_residual3(const Plan3Dev& p, const double* U, double* R, void* A, void* B, bool first_order,
                       cudaStream_t st);
 void launch_jvp3(const Plan3Dev& p, const double* U, const double* v, double* Jv, void* A, void* B, cudaStream_t st);
+void launch_wave_speeds3(const Plan3Dev& p, const double* U, double* lam, cudaStream_t st);
+void launch_precondition3(const Plan3Dev& p, const double* U, double cfl, const double* r, double* z, double* scratch,
+                          cudaStream_t st);
 
 }  // namespace jr

@@ -1,0 +1,311 @@
+// The 3D wave speeds and line preconditioner, per-face and per-chain bodies (host and
+// device code; linesolve3d.cu launches them, one thread each): the reference's
+// face_wave_speeds (src/jaxrans/numerics/residual.py:169-203) and line_j
+// (src/jaxrans/solvers/preconditioners.py:209-306) on a 3D plan -- 5x5 mean-flow chain
+// blocks, the SA row on its own scalar chains -- solved along each chain by the block
+// Thomas algorithm (src/jaxrans/core/linalg.py:80-132).  A first form: one thread walks
+// a chain, its blocks assembled as it goes, the eliminated blocks kept in scratch.
+#pragma once
+#include "residual3d.cuh"
+
+namespace jr {
+
+__host__ __device__ __forceinline__ int face_count(const Plan3Dev& p, int a) {
+  return (p.NI + (a == 0)) * (p.NJ + (a == 1)) * (p.NK + (a == 2));
+}
+
+// a flat index into the three face families, concatenated, to (family, i, j, k)
+__host__ __device__ __forceinline__ void face_of(const Plan3Dev& p, int flat, int& a, int& i, int& j, int& k) {
+  a = 0;
+  while (a < 2 && flat >= face_count(p, a)) flat -= face_count(p, a++);
+  const int fj = p.NJ + (a == 1), fk = p.NK + (a == 2);
+  i = flat / (fj * fk);
+  j = (flat / fk) % fj;
+  k = flat % fk;
+}
+
+// primitive state of canvas cell c straight from U (no ghost fill)
+__host__ __device__ __forceinline__ void prim_at(const Plan3Dev& p, const double* U, int c, double q[NV3_MAX]) {
+  const int n = p.NI * p.NJ * p.NK;
+  double u[NV3_MAX];
+  for (int v = 0; v < p.nvar; ++v) u[v] = U[(size_t)v * n + c];
+  to_prim3(u, q, p.nvar, p.P.gamma);
+}
+
+// the two cells either side of face (a, i, j, k), each replaced by its partner across a
+// block face (the neighbour map), the canvas edge repeated
+__host__ __device__ __forceinline__ void face_cells(const Plan3Dev& p, int a, int i, int j, int k, int& lo, int& hi) {
+  int l[3] = {i, j, k}, h[3] = {i, j, k};
+  l[a] -= 1;
+  lo = p.neighbours[cell_index(p, l[0], l[1], l[2])];
+  hi = p.neighbours[cell_index(p, h[0], h[1], h[2])];
+}
+
+// face-averaged primitive state and volume (src/jaxrans/mesh/atlas.py:169-183)
+__host__ __device__ __forceinline__ void face_average(const Plan3Dev& p, const double* U, int a, int i, int j, int k,
+                                                      double qf[NV3_MAX], double& vol) {
+  int lo, hi;
+  face_cells(p, a, i, j, k, lo, hi);
+  double ql[NV3_MAX], qh[NV3_MAX];
+  prim_at(p, U, lo, ql);
+  prim_at(p, U, hi, qh);
+  for (int v = 0; v < p.nvar; ++v) qf[v] = 0.5 * (ql[v] + qh[v]);
+  vol = 0.5 * (p.volume[lo] + p.volume[hi]);
+}
+
+// lambda = |V.S| + a|S| at the face-averaged state, plus the thin-layer viscous term
+__host__ __device__ __forceinline__ double wave_speed(const Plan3Dev& p, const double* U, int a, int i, int j, int k) {
+  const Physics3& P = p.P;
+  const double g = P.gamma;
+  double qf[NV3_MAX], vol, s[3];
+  face_average(p, U, a, i, j, k, qf, vol);
+  face_vector(p, a, i, j, k, s);
+  const double ss = (s[0] * s[0] + s[1] * s[1]) + s[2] * s[2];
+  double vn = (qf[1] * s[0] + qf[2] * s[1]) + qf[3] * s[2];
+  double lam = (vn >= 0.0 ? vn : -vn) + sqrt(g * qf[4] / qf[0]) * sqrt(ss);
+  if (P.mu_inf > 0.0) {
+    double mu = viscosity3(P, g * qf[4] / qf[0]);
+    if (p.nvar > 5) mu = mu + eddy_viscosity(P.sa, qf[0], qf[5] * P.mu_inf, mu / qf[0]);
+    lam = lam + 2.0 * g / PR_LAMINAR * mu * ss / (qf[0] * vol);
+  }
+  return lam;
+}
+
+// sum over the cell's six faces of lambda (the order of cell_wave_speed_sum)
+__host__ __device__ __forceinline__ double lambda_sum(const Plan3Dev& p, const double* U, int c) {
+  const int i = c / (p.NJ * p.NK), j = (c / p.NK) % p.NJ, k = c % p.NK;
+  double total = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    int h[3] = {i, j, k};
+    h[a] += 1;
+    const double lo = wave_speed(p, U, a, i, j, k), hi = wave_speed(p, U, a, h[0], h[1], h[2]);
+    total = a == 0 ? lo + hi : total + lo + hi;
+  }
+  return total;
+}
+
+// A = d(F . S)/dU (5x5, [row][variable]) by forward-mode tangents of the flux of the
+// conservative state (src/jaxrans/physics/euler.py:55-71)
+__host__ __device__ __forceinline__ void flux_jacobian3(const double* q, const double* s, double g, double A[5][5]) {
+  double U[5];
+  U[0] = q[0];
+  U[1] = q[0] * q[1];
+  U[2] = q[0] * q[2];
+  U[3] = q[0] * q[3];
+  U[4] = q[4] / (g - 1.0) + 0.5 * q[0] * ((q[1] * q[1] + q[2] * q[2]) + q[3] * q[3]);
+  for (int col = 0; col < 5; ++col) {
+    Dual Ud[5], qd[5], F[5];
+    for (int v = 0; v < 5; ++v) Ud[v] = Dual{U[v], v == col ? 1.0 : 0.0};
+    to_prim3(Ud, qd, 5, g);
+    normal_flux3(qd, s, g, F);
+    for (int r = 0; r < 5; ++r) A[r][col] = F[r].d;
+  }
+}
+
+// unpivoted Gauss-Jordan inverse (src/jaxrans/core/linalg.py:49-77)
+template <int M> __host__ __device__ __forceinline__ void invert_n(const double Mx[M][M], double Inv[M][M]) {
+  double a[M][2 * M];
+  for (int r = 0; r < M; ++r)
+    for (int c = 0; c < M; ++c) {
+      a[r][c] = Mx[r][c];
+      a[r][M + c] = r == c ? 1.0 : 0.0;
+    }
+  for (int k = 0; k < M; ++k) {
+    const double piv = a[k][k];
+    for (int c = 0; c < 2 * M; ++c) a[k][c] = a[k][c] / piv;
+    for (int r = 0; r < M; ++r) {
+      if (r == k) continue;
+      const double f = a[r][k];
+      for (int c = 0; c < 2 * M; ++c) a[r][c] = a[r][c] - f * a[k][c];
+    }
+  }
+  for (int r = 0; r < M; ++r)
+    for (int c = 0; c < M; ++c) Inv[r][c] = a[r][M + c];
+}
+
+// the link k -> k+1 of a chain: its face vector (outward from cell k) and lambda there
+__host__ __device__ __forceinline__ void link_face(const Plan3Dev& p, const double* U, int flat, double s[3],
+                                                   double& lam) {
+  int a, i, j, k;
+  face_of(p, flat, a, i, j, k);
+  face_vector(p, a, i, j, k, s);
+  lam = wave_speed(p, U, a, i, j, k);
+}
+
+// 1/2 A(q_nb, sign S) - 1/2 lambda I
+__host__ __device__ __forceinline__ void coupling5(const double* qnb, const double* s, double sign, double lam,
+                                                   double g, double B[5][5]) {
+  const double ss[3] = {sign * s[0], sign * s[1], sign * s[2]};
+  double A[5][5];
+  flux_jacobian3(qnb, ss, g, A);
+  for (int r = 0; r < 5; ++r)
+    for (int c = 0; c < 5; ++c) B[r][c] = 0.5 * A[r][c] - (r == c ? 0.5 * lam : 0.0);
+}
+
+// z = M^-1 r on the mean-flow rows of chain ch (block Thomas, src/jaxrans/core/linalg.py:80-132);
+// C (L x 25) and D (L x 5) the chain's scratch
+__host__ __device__ void chain_flow(const Plan3Dev& p, const double* U, double cfl, int ch, const double* r, double* z,
+                                    double* Cs, double* Ds) {
+  const int n = p.NI * p.NJ * p.NK, L = p.chain_L;
+  const double g = p.P.gamma;
+  const int* cells = p.ch_cells + (size_t)ch * L;
+  int len = 0;
+  while (len < L && cells[len] >= 0) ++len;
+  double cprev[5][5] = {}, dprev[5] = {};
+  double lower[5][5] = {};   // row k's block toward cell k-1
+  for (int k = 0; k < len; ++k) {
+    const int c = cells[k];
+    const double dg = lambda_sum(p, U, c) * (1.0 / cfl + 0.5);
+    double D[5][5];
+    for (int a = 0; a < 5; ++a)
+      for (int b = 0; b < 5; ++b) D[a][b] = a == b ? dg : 0.0;
+    double upper[5][5] = {}, lower_next[5][5] = {};
+    const int sign = k + 1 < len ? p.ch_sign[(size_t)ch * L + k] : 0;
+    if (sign != 0) {
+      double s[3], lam, qn[NV3_MAX], qc[NV3_MAX];
+      link_face(p, U, p.ch_face[(size_t)ch * L + k], s, lam);
+      prim_at(p, U, cells[k + 1], qn);
+      prim_at(p, U, c, qc);
+      coupling5(qn, s, (double)sign, lam, g, upper);
+      coupling5(qc, s, (double)-sign, lam, g, lower_next);
+    }
+    // piv = inv(D - lower c_prev); chat = piv upper; d = piv (r - lower d_prev)
+    double T[5][5], piv[5][5], rhs[5];
+    for (int a = 0; a < 5; ++a)
+      for (int b = 0; b < 5; ++b) {
+        double m = lower[a][0] * cprev[0][b];
+        for (int t = 1; t < 5; ++t) m = m + lower[a][t] * cprev[t][b];
+        T[a][b] = D[a][b] - m;
+      }
+    invert_n<5>(T, piv);
+    for (int a = 0; a < 5; ++a) {
+      double m = lower[a][0] * dprev[0];
+      for (int t = 1; t < 5; ++t) m = m + lower[a][t] * dprev[t];
+      rhs[a] = r[(size_t)a * n + c] - m;
+    }
+    for (int a = 0; a < 5; ++a) {
+      for (int b = 0; b < 5; ++b) {
+        double m = piv[a][0] * upper[0][b];
+        for (int t = 1; t < 5; ++t) m = m + piv[a][t] * upper[t][b];
+        cprev[a][b] = m;
+        Cs[(size_t)k * 25 + a * 5 + b] = m;
+      }
+      double m = piv[a][0] * rhs[0];
+      for (int t = 1; t < 5; ++t) m = m + piv[a][t] * rhs[t];
+      Ds[(size_t)k * 5 + a] = m;
+    }
+    for (int a = 0; a < 5; ++a) {
+      dprev[a] = Ds[(size_t)k * 5 + a];
+      for (int b = 0; b < 5; ++b) lower[a][b] = lower_next[a][b];
+    }
+  }
+  double nxt[5] = {};
+  for (int k = len - 1; k >= 0; --k) {
+    double x[5];
+    for (int a = 0; a < 5; ++a) {
+      double m = Cs[(size_t)k * 25 + a * 5] * nxt[0];
+      for (int t = 1; t < 5; ++t) m = m + Cs[(size_t)k * 25 + a * 5 + t] * nxt[t];
+      x[a] = Ds[(size_t)k * 5 + a] - m;
+    }
+    for (int a = 0; a < 5; ++a) {
+      nxt[a] = x[a];
+      z[(size_t)a * n + cells[k]] = x[a];
+    }
+  }
+}
+
+// the SA row's face terms at face (a, i, j, k): mass flux rho V.S and diffusion kappa |S|^2 / V
+__host__ __device__ __forceinline__ void sa_face_terms(const Plan3Dev& p, const double* U, int a, int i, int j, int k,
+                                                       double& m, double& d) {
+  const Physics3& P = p.P;
+  double qf[NV3_MAX], vol, s[3];
+  face_average(p, U, a, i, j, k, qf, vol);
+  face_vector(p, a, i, j, k, s);
+  const double mu = viscosity3(P, P.gamma * qf[4] / qf[0]);
+  const double kap = diffusion_coefficient(P.sa, qf[0], qf[5] * P.mu_inf, mu);
+  m = qf[0] * ((qf[1] * s[0] + qf[2] * s[1]) + qf[3] * s[2]);
+  d = kap * ((s[0] * s[0] + s[1] * s[1]) + s[2] * s[2]) / vol;
+}
+
+// the SA chain diagonal of cell c (src/jaxrans/solvers/preconditioners.py:235-270)
+__host__ __device__ double sa_diagonal(const Plan3Dev& p, const double* U, double cfl, int c) {
+  const Physics3& P = p.P;
+  const double g = P.gamma;
+  const int i = c / (p.NJ * p.NK), j = (c / p.NK) % p.NJ, k = c % p.NK;
+  double diag = 0.0;
+  double gv[3][3];   // Green-Gauss of face-averaged velocity: gv[direction][component]
+  for (int dir = 0; dir < 3; ++dir)
+    for (int m = 0; m < 3; ++m) gv[dir][m] = 0.0;
+  double vsum[3][3][3];   // per family: hi*S_hi - lo*S_lo, [family][direction][component]
+  for (int a = 0; a < 3; ++a) {
+    int h[3] = {i, j, k};
+    h[a] += 1;
+    double mlo, dlo, mhi, dhi;
+    sa_face_terms(p, U, a, i, j, k, mlo, dlo);
+    sa_face_terms(p, U, a, h[0], h[1], h[2], mhi, dhi);
+    const double out_hi = (mhi > 0.0 ? mhi : 0.0) + dhi;
+    const double in_lo = (-mlo > 0.0 ? -mlo : 0.0) + dlo;
+    diag = a == 0 ? out_hi + in_lo : diag + out_hi + in_lo;
+    double ql[NV3_MAX], qh[NV3_MAX], vl, vh, sl[3], sh[3];
+    face_average(p, U, a, i, j, k, ql, vl);
+    face_average(p, U, a, h[0], h[1], h[2], qh, vh);
+    face_vector(p, a, i, j, k, sl);
+    face_vector(p, a, h[0], h[1], h[2], sh);
+    for (int dir = 0; dir < 3; ++dir)
+      for (int m = 0; m < 3; ++m) vsum[a][dir][m] = qh[1 + m] * sh[dir] - ql[1 + m] * sl[dir];
+  }
+  const double vol = p.volume[c];
+  for (int dir = 0; dir < 3; ++dir)
+    for (int m = 0; m < 3; ++m) gv[dir][m] = ((vsum[0][dir][m] + vsum[1][dir][m]) + vsum[2][dir][m]) / vol;
+  double q[NV3_MAX];
+  prim_at(p, U, c, q);
+  diag = diag / q[0];
+  const double cx = gv[1][2] - gv[2][1], cy = gv[2][0] - gv[0][2], cz = gv[0][1] - gv[1][0];
+  const double sq = (cx * cx + cy * cy) + cz * cz;
+  const double omega = sq > 0.0 ? sqrt(sq) : 0.0;
+  const double nu = viscosity3(P, g * q[4] / q[0]) / q[0];
+  const double dist = p.distance[c];
+  const double st = s_tilde(P.sa, omega, q[5] * P.mu_inf, nu, dist);
+  const double fw = f_w(P.sa, r_of(P.sa, q[5] * P.mu_inf, st, dist));
+  const double dest = q[5] > 0.0 ? 2.0 * P.sa.c_w1 * fw * P.mu_inf * q[5] / (dist * dist) : 0.0;
+  return diag + dest * vol + lambda_sum(p, U, c) / cfl;
+}
+
+// z = M^-1 r on the SA row of chain ch (scalar Thomas); C, D the chain's scratch (L each)
+__host__ __device__ void chain_sa(const Plan3Dev& p, const double* U, double cfl, int ch, const double* r, double* z,
+                                  double* Cs, double* Ds) {
+  const int n = p.NI * p.NJ * p.NK, L = p.chain_L;
+  const int* cells = p.ch_cells + (size_t)ch * L;
+  int len = 0;
+  while (len < L && cells[len] >= 0) ++len;
+  double cprev = 0.0, dprev = 0.0, lower = 0.0;
+  for (int k = 0; k < len; ++k) {
+    const int c = cells[k];
+    const double dg = sa_diagonal(p, U, cfl, c);
+    double upper = 0.0, lower_next = 0.0;
+    const int sign = k + 1 < len ? p.ch_sign[(size_t)ch * L + k] : 0;
+    if (sign != 0) {
+      int a, i, j, kk;
+      face_of(p, p.ch_face[(size_t)ch * L + k], a, i, j, kk);
+      double m, d;
+      sa_face_terms(p, U, a, i, j, kk, m, d);
+      const double rho_up = U[cells[k + 1]], rho_c = U[c];
+      const double up_m = -(double)sign * m, down_m = (double)sign * m;
+      upper = -((up_m > 0.0 ? up_m : 0.0) + d) / rho_up;
+      lower_next = -((down_m > 0.0 ? down_m : 0.0) + d) / rho_c;
+    }
+    const double piv = 1.0 / (dg - lower * cprev);
+    cprev = piv * upper;
+    Cs[k] = cprev;
+    Ds[k] = piv * (r[(size_t)5 * n + c] - lower * dprev);
+    dprev = Ds[k];
+    lower = lower_next;
+  }
+  double nxt = 0.0;
+  for (int k = len - 1; k >= 0; --k) {
+    nxt = Ds[k] - Cs[k] * nxt;
+    z[(size_t)5 * n + cells[k]] = nxt;
+  }
+}
+
+}  // namespace jr

@@ -32,6 +32,8 @@ class Plan3Desc(C.Structure):
         ("gamma", C.c_double), ("mu_inf", C.c_double), ("sutherland", C.c_double), ("kappa", C.c_double),
         ("flux", C.c_int32), ("limiter", C.c_int32),
         ("q_inf", C.c_double * 6),
+        ("neighbours", _i32p), ("n_chains", C.c_int32), ("chain_L", C.c_int32), ("chain_cells", _i32p),
+        ("chain_up_face", _i32p), ("chain_up_sign", _i32p),
     ]
 
 
@@ -131,6 +133,12 @@ def describe(plan: Plan3, q_inf, gamma: float, flux: str, limiter: str, kappa: f
     d.limiter = 4 if kappa != 0.0 else LIMITER_CODES[limiter]
     for v in range(6):
         d.q_inf[v] = float(q_inf[v]) if v < nvar else 0.0
+    d.neighbours = ptr(arr(plan.neighbours, np.int32), _i32p)
+    lines = plan.lines
+    d.n_chains, d.chain_L = lines.cells.shape
+    d.chain_cells = ptr(arr(lines.cells, np.int32), _i32p)
+    d.chain_up_face = ptr(arr(lines.up_face, np.int32), _i32p)
+    d.chain_up_sign = ptr(arr(lines.up_sign, np.int32), _i32p)
     return d, keep
 
 
@@ -174,4 +182,24 @@ class DevicePlan3:
     def jvp(self, U, v) -> np.ndarray:
         (u, t), out = self._run("jr_jvp3d", U, v)
         _check(self.lib, self.lib.jr_jvp3d(self.handle, u.data_ptr(), t.data_ptr(), out.data_ptr()), "jr_jvp3d")
+        return out.cpu().numpy()
+
+    def wave_speeds(self, U) -> list:
+        """lambda per face family (three arrays of the families' face shapes)."""
+        import torch
+        (u,), _ = self._run("jr_wave_speeds3d", U)
+        shapes = [tuple(n + (a == x) for x, n in enumerate(self.plan.shape)) for a in range(3)]
+        out = torch.empty(sum(int(np.prod(s)) for s in shapes), dtype=torch.float64, device="cuda")
+        _check(self.lib, self.lib.jr_wave_speeds3d(self.handle, u.data_ptr(), out.data_ptr()), "jr_wave_speeds3d")
+        flat, parts, at = out.cpu().numpy(), [], 0
+        for s in shapes:
+            parts.append(flat[at:at + int(np.prod(s))].reshape(s))
+            at += int(np.prod(s))
+        return parts
+
+    def precondition(self, U, cfl: float, r) -> np.ndarray:
+        """z = M^-1 r of line_j at (U, cfl)."""
+        (u, rr), out = self._run("jr_precondition3d", U, r)
+        _check(self.lib, self.lib.jr_precondition3d(self.handle, u.data_ptr(), float(cfl), rr.data_ptr(),
+                                                     out.data_ptr()), "jr_precondition3d")
         return out.cpu().numpy()

@@ -6,7 +6,7 @@
 #include <vector>
 
 #include "../../jax-rans_b200/csrc/plan3d_desc.cuh"
-#include "../../jax-rans_b200/csrc/residual3d.cuh"
+#include "../../jax-rans_b200/csrc/linesolve3d.cuh"
 
 using namespace jr;
 
@@ -23,8 +23,7 @@ static void run(const Plan3Dev& p, const double* U, const double* dU, double* R,
   for (int c = 0; c < n; ++c) residual_cell<T, VISC, SA>(p, A.data(), U, dU, R, first_order, c);
 }
 
-extern "C" int jr3_host_eval(const jr_plan3d_desc* d, const double* U, const double* dU, double* R,
-                             int first_order) {
+static Plan3Dev plan_of(const jr_plan3d_desc* d) {
   Plan3Dev p{};
   p.NI = d->NI;
   p.NJ = d->NJ;
@@ -35,15 +34,27 @@ extern "C" int jr3_host_eval(const jr_plan3d_desc* d, const double* U, const dou
   for (int a = 0; a < 3; ++a) p.faces[a] = d->faces[a];
   p.centres = d->centres;
   p.distance = d->distance;
-  p.n_stages = d->n_stages;
-  if (p.n_stages < 1 || p.n_stages > MAX_STAGES3) return 1;
+  p.n_stages = d->n_stages < MAX_STAGES3 ? d->n_stages : MAX_STAGES3;
   p.stage_off[0] = 0;
-  for (int s = 0; s < d->n_stages; ++s) p.stage_off[s + 1] = p.stage_off[s] + d->stage_records[s];
+  for (int s = 0; s < p.n_stages; ++s) p.stage_off[s + 1] = p.stage_off[s] + d->stage_records[s];
   p.g_ghost = d->ghost;
   p.g_source = d->source;
   p.g_kind = d->kind;
   p.g_normal = d->normal;
+  p.neighbours = d->neighbours;
+  p.n_chains = d->n_chains;
+  p.chain_L = d->chain_L;
+  p.ch_cells = d->chain_cells;
+  p.ch_face = d->chain_up_face;
+  p.ch_sign = d->chain_up_sign;
   physics3_from_desc(p.P, d);
+  return p;
+}
+
+extern "C" int jr3_host_eval(const jr_plan3d_desc* d, const double* U, const double* dU, double* R,
+                             int first_order) {
+  if (d->n_stages < 1 || d->n_stages > MAX_STAGES3) return 1;
+  const Plan3Dev p = plan_of(d);
   const bool visc = p.P.mu_inf > 0.0, sa = p.nvar > 5;
   if (dU) {
     if (sa) run<Dual, true, true>(p, U, dU, R, 1);
@@ -53,6 +64,30 @@ extern "C" int jr3_host_eval(const jr_plan3d_desc* d, const double* U, const dou
     if (sa) run<double, true, true>(p, U, nullptr, R, first_order);
     else if (visc) run<double, true, false>(p, U, nullptr, R, first_order);
     else run<double, false, false>(p, U, nullptr, R, first_order);
+  }
+  return 0;
+}
+
+extern "C" int jr3_host_wave_speeds(const jr_plan3d_desc* d, const double* U, double* lam) {
+  const Plan3Dev p = plan_of(d);
+  const int total = face_count(p, 0) + face_count(p, 1) + face_count(p, 2);
+  for (int f = 0; f < total; ++f) {
+    int a, i, j, k;
+    face_of(p, f, a, i, j, k);
+    lam[f] = wave_speed(p, U, a, i, j, k);
+  }
+  return 0;
+}
+
+extern "C" int jr3_host_precondition(const jr_plan3d_desc* d, const double* U, double cfl, const double* r,
+                                     double* z) {
+  const Plan3Dev p = plan_of(d);
+  const size_t n = (size_t)p.nvar * p.NI * p.NJ * p.NK;
+  for (size_t e = 0; e < n; ++e) z[e] = r[e];
+  std::vector<double> scratch((size_t)p.chain_L * 30);
+  for (int ch = 0; ch < p.n_chains; ++ch) {
+    chain_flow(p, U, cfl, ch, r, z, scratch.data(), scratch.data() + (size_t)p.chain_L * 25);
+    if (p.nvar > 5) chain_sa(p, U, cfl, ch, r, z, scratch.data(), scratch.data() + (size_t)p.chain_L * 25);
   }
   return 0;
 }

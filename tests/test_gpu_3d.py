@@ -62,3 +62,13 @@ def test_jvp3d_matches_the_reference(cuda, device3d, state):
     Jv, ref = dev.jvp(z[f"{state}_U"], z[f"{state}_v"]), z[f"{state}_Jv"]
     assert rows_rel(Jv[:5], ref[:5]) < 1e-12
     assert rows_rel(Jv[5:], ref[5:]) < 1e-10
+
+
+@pytest.mark.parametrize("state", ["sin", "rand0"])
+def test_wave_speeds3d_and_line_solve_match_the_reference(cuda, device3d, state):
+    z, dev = device3d
+    U = z[f"{state}_U"]
+    for a, lam in enumerate(dev.wave_speeds(U)):
+        assert np.allclose(lam, z[f"{state}_lam{a}"], rtol=1e-13, atol=0.0)
+    zz = dev.precondition(U, 25.0, z[f"{state}_prec_r"])
+    assert rows_rel(zz, z[f"{state}_prec_z"]) < 1e-10

@@ -84,3 +84,44 @@ def test_kernel_bodies_give_the_reference_jvp(harness, case3d, state):
     Jv, ref = evaluate(harness, desc, z[f"{state}_U"], z[f"{state}_v"]), z[f"{state}_Jv"]
     assert rows_rel(Jv[:5], ref[:5]) < 1e-12
     assert rows_rel(Jv[5:], ref[5:]) < 1e-10
+
+
+@pytest.mark.parametrize("state", ["sin", "rand0"])
+def test_kernel_bodies_give_the_reference_wave_speeds(harness, case3d, state):
+    z, plan, desc, _ = case3d
+    harness.jr3_host_wave_speeds.restype = C.c_int
+    harness.jr3_host_wave_speeds.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    U = np.ascontiguousarray(z[f"{state}_U"])
+    shapes = [tuple(n + (a == x) for x, n in enumerate(plan.shape)) for a in range(3)]
+    lam = np.zeros(sum(int(np.prod(s)) for s in shapes))
+    assert harness.jr3_host_wave_speeds(C.addressof(desc), U.ctypes.data, lam.ctypes.data) == 0
+    at = 0
+    for a, s in enumerate(shapes):
+        part = lam[at:at + int(np.prod(s))].reshape(s)
+        at += int(np.prod(s))
+        assert np.allclose(part, z[f"{state}_lam{a}"], rtol=1e-14, atol=0.0)
+
+
+@pytest.mark.parametrize("state", ["sin", "rand0"])
+def test_kernel_bodies_give_the_reference_line_solve(harness, case3d, state):
+    """Block Thomas along the chains (the device's order) against the oracle's block Thomas
+    (bitwise order) and the reference's cyclic reduction (to round-off)."""
+    from oracle import implicit3d as i3
+    from oracle import numerics3d as n3
+    import json as _json
+    z, plan, desc, _ = case3d
+    harness.jr3_host_precondition.restype = C.c_int
+    harness.jr3_host_precondition.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]
+    U = np.ascontiguousarray(z[f"{state}_U"])
+    r = np.ascontiguousarray(z[f"{state}_prec_r"])
+    out = np.zeros_like(r)
+    assert harness.jr3_host_precondition(C.addressof(desc), U.ctypes.data, 25.0, r.ctypes.data, out.ctypes.data) == 0
+    assert rows_rel(out, z[f"{state}_prec_z"]) < 1e-10
+    flow = _flow(_json.loads(str(z["case_json"]))["case"])
+    a = flow.alpha_rad
+    q_inf = np.array([1.0, flow.mach * np.cos(a), 0.0, flow.mach * np.sin(a), 1.0 / flow.gamma, flow.nu_tilde_ratio])
+    model = n3.Model3(plan, q_inf, flow.gamma, "hllc", "van_albada_smooth", 0.0, flow.mu_inf,
+                      flow.sutherland_ratio, True, plan.distance)
+    lam = n3.wave_speeds(U, model)
+    thomas = i3.precondition(U, lam, 25.0, model, solver="thomas")(r)
+    assert rows_rel(out, thomas) < 1e-13
