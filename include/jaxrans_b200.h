@@ -268,6 +268,10 @@ typedef struct jr_plan3d_desc {
   const int32_t* chain_cells;   /* [chain * chain_L + k], -1 past the chain's end */
   const int32_t* chain_up_face; /* link k -> k+1: flat index into the three face families, concatenated */
   const int32_t* chain_up_sign; /* +1 / -1 the link face vector out of / into cell k, 0 no link */
+  /* implicit solver (as jr_plan_desc; preconditioner 0 none, 1 line_j) */
+  double cfl_max, cfl_growth, cfl_cutback, cfl_min;
+  double krylov_tol, krylov_success, max_relative_update;   /* max_relative_update <= 0: none */
+  int32_t krylov_subspace, krylov_restarts, preconditioner;
 } jr_plan3d_desc;
 
 /* Build a 3D plan (device copies of the tables, work buffers, a stream).  Every record
@@ -294,6 +298,15 @@ int jr_wave_speeds3d(jr_plan3d* plan, const double* U, double* lam);
  * on no chain copied.  Replaces get_preconditioner("line_j")(...)(U, lambdas, cfl) and
  * its solve (src/jaxrans/solvers/preconditioners.py:209-306) on a 3D atlas.  Synchronises. */
 int jr_precondition3d(jr_plan3d* plan, const double* U, double cfl, const double* r, double* z);
+/* n_steps pseudo-transient Newton steps on U (device, nvar x canvas, updated in place)
+ * from *cfl and the previous |R| *residual_norm (both host, updated); history (host,
+ * n_steps) receives |R| before each step.  GMRES(krylov_subspace) with krylov_restarts
+ * cycles, CGS2, Givens least squares, the relaxation, acceptance test and CFL ramp of
+ * src/jaxrans/solvers/implicit.py:54-168, driven from the host over device kernels (a
+ * first form: it synchronises for each scalar).  Replaces make_newton_step run as the
+ * driver's block on a 3D atlas. */
+int jr_newton_steps3d(jr_plan3d* plan, double* U, int32_t n_steps, double* cfl, double* residual_norm,
+                      double* history);
 
 #ifdef __cplusplus
 }

@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "../../include/jaxrans_b200.h"
+#include "newton3d_ops.cuh"
 #include "plan3d_desc.cuh"
 
 namespace jr {
@@ -20,6 +21,9 @@ struct jr_plan3d {
   void* B = nullptr;
   double* scratch = nullptr;   // the line solve's eliminated blocks: n_chains * chain_L * 30
   size_t n_canvas = 0;
+  Newton3Config cfg{};
+  double* work = nullptr;      // the Newton step's vectors
+  int* flag = nullptr;
   cudaStream_t st = nullptr;
 };
 
@@ -148,6 +152,25 @@ int jr_plan3d_create(const jr_plan3d_desc* d, jr_plan3d** out) {
     return report_error(JR_ENOMEM, "cudaMalloc failed");
   }
   p->allocs.push_back(p->B);
+  // the Newton step's configuration and vectors
+  if (d->krylov_subspace < 1 || d->krylov_subspace > 64 || d->krylov_restarts < 1 || d->preconditioner < 0 ||
+      d->preconditioner > 1) {
+    jr_plan3d_destroy(p);
+    return report_error(JR_EINVAL, "krylov_subspace 1..64, krylov_restarts >= 1, preconditioner 0 or 1");
+  }
+  p->cfg = Newton3Config{d->krylov_subspace, d->krylov_restarts, d->preconditioner, d->krylov_tol, d->krylov_success,
+                         d->max_relative_update, d->cfl_min, d->cfl_max, d->cfl_growth, d->cfl_cutback};
+  {
+    const size_t words = DeviceOps3::work_doubles((size_t)d->nvar * n, n, d->krylov_subspace);
+    void *w = nullptr, *f = nullptr;
+    if (cudaMalloc(&w, words * sizeof(double)) != cudaSuccess || (p->allocs.push_back(w), cudaMalloc(&f, sizeof(int))) != cudaSuccess) {
+      jr_plan3d_destroy(p);
+      return report_error(JR_ENOMEM, "cudaMalloc failed");
+    }
+    p->allocs.push_back(f);
+    p->work = static_cast<double*>(w);
+    p->flag = static_cast<int*>(f);
+  }
   if (cudaStreamCreateWithFlags(&p->st, cudaStreamNonBlocking) != cudaSuccess) {
     jr_plan3d_destroy(p);
     return report_error(JR_ECUDA, "stream");
@@ -188,6 +211,32 @@ int jr_precondition3d(jr_plan3d* plan, const double* U, double cfl, const double
   launch_precondition3(plan->dev, U, cfl, r, z, plan->scratch, plan->st);
   if (cudaStreamSynchronize(plan->st) != cudaSuccess) return check3("jr_precondition3d");
   return check3("jr_precondition3d");
+}
+
+int jr_newton_steps3d(jr_plan3d* plan, double* U, int32_t n_steps, double* cfl, double* residual_norm,
+                      double* history) {
+  if (!plan || !U || !cfl || !residual_norm || n_steps < 0) return report_error(JR_EINVAL, "bad argument");
+  if (!(*cfl > 0.0)) return report_error(JR_EINVAL, "cfl must be positive");
+  DeviceOps3 ops;
+  ops.p = plan->dev;
+  ops.n = plan->n_canvas;
+  ops.N = (size_t)plan->dev.nvar * plan->n_canvas;
+  ops.A = plan->A;
+  ops.B = plan->B;
+  ops.scratch = plan->scratch;
+  ops.st = plan->st;
+  ops.bind(plan->work, plan->flag, plan->cfg.restart);
+  double c = *cfl, r = *residual_norm;
+  for (int s = 0; s < n_steps; ++s) {
+    const double norm = newton_step3_device(ops, U, c, r, plan->cfg);
+    if (history) history[s] = norm;
+    int rc = check3("jr_newton_steps3d");
+    if (rc) return rc;
+  }
+  if (cudaStreamSynchronize(plan->st) != cudaSuccess) return check3("jr_newton_steps3d");
+  *cfl = c;
+  *residual_norm = r;
+  return check3("jr_newton_steps3d");
 }
 
 }  // extern "C"

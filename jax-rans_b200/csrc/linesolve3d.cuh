@@ -144,7 +144,7 @@ __host__ __device__ __forceinline__ void coupling5(const double* qnb, const doub
 
 // z = M^-1 r on the mean-flow rows of chain ch (block Thomas, src/jaxrans/core/linalg.py:80-132);
 // C (L x 25) and D (L x 5) the chain's scratch
-__host__ __device__ void chain_flow(const Plan3Dev& p, const double* U, double cfl, int ch, const double* r, double* z,
+inline __host__ __device__ void chain_flow(const Plan3Dev& p, const double* U, double cfl, int ch, const double* r, double* z,
                                     double* Cs, double* Ds) {
   const int n = p.NI * p.NJ * p.NK, L = p.chain_L;
   const double g = p.P.gamma;
@@ -228,7 +228,7 @@ __host__ __device__ __forceinline__ void sa_face_terms(const Plan3Dev& p, const 
 }
 
 // the SA chain diagonal of cell c (src/jaxrans/solvers/preconditioners.py:235-270)
-__host__ __device__ double sa_diagonal(const Plan3Dev& p, const double* U, double cfl, int c) {
+inline __host__ __device__ double sa_diagonal(const Plan3Dev& p, const double* U, double cfl, int c) {
   const Physics3& P = p.P;
   const double g = P.gamma;
   const int i = c / (p.NJ * p.NK), j = (c / p.NK) % p.NJ, k = c % p.NK;
@@ -272,7 +272,7 @@ __host__ __device__ double sa_diagonal(const Plan3Dev& p, const double* U, doubl
 }
 
 // z = M^-1 r on the SA row of chain ch (scalar Thomas); C, D the chain's scratch (L each)
-__host__ __device__ void chain_sa(const Plan3Dev& p, const double* U, double cfl, int ch, const double* r, double* z,
+inline __host__ __device__ void chain_sa(const Plan3Dev& p, const double* U, double cfl, int ch, const double* r, double* z,
                                   double* Cs, double* Ds) {
   const int n = p.NI * p.NJ * p.NK, L = p.chain_L;
   const int* cells = p.ch_cells + (size_t)ch * L;

@@ -34,6 +34,9 @@ class Plan3Desc(C.Structure):
         ("q_inf", C.c_double * 6),
         ("neighbours", _i32p), ("n_chains", C.c_int32), ("chain_L", C.c_int32), ("chain_cells", _i32p),
         ("chain_up_face", _i32p), ("chain_up_sign", _i32p),
+        ("cfl_max", C.c_double), ("cfl_growth", C.c_double), ("cfl_cutback", C.c_double), ("cfl_min", C.c_double),
+        ("krylov_tol", C.c_double), ("krylov_success", C.c_double), ("max_relative_update", C.c_double),
+        ("krylov_subspace", C.c_int32), ("krylov_restarts", C.c_int32), ("preconditioner", C.c_int32),
     ]
 
 
@@ -95,9 +98,10 @@ def apply_records(records: Records, q: np.ndarray) -> np.ndarray:
 
 
 def describe(plan: Plan3, q_inf, gamma: float, flux: str, limiter: str, kappa: float = 0.0,
-             mu_inf: float | None = None, sutherland: float | None = None):
-    """``(jr_plan3d_desc, arrays it points into)`` for ``plan`` and the physics; keep the
-    arrays alive while the descriptor is used."""
+             mu_inf: float | None = None, sutherland: float | None = None, implicit=None):
+    """``(jr_plan3d_desc, arrays it points into)`` for ``plan``, the physics and the
+    implicit solver's settings (``config.ImplicitConfig``; its defaults if None); keep
+    the arrays alive while the descriptor is used."""
     rec = records_of(plan)
     keep = []
 
@@ -139,6 +143,13 @@ def describe(plan: Plan3, q_inf, gamma: float, flux: str, limiter: str, kappa: f
     d.chain_cells = ptr(arr(lines.cells, np.int32), _i32p)
     d.chain_up_face = ptr(arr(lines.up_face, np.int32), _i32p)
     d.chain_up_sign = ptr(arr(lines.up_sign, np.int32), _i32p)
+    from .config import ImplicitConfig
+    imp = implicit if implicit is not None else ImplicitConfig()
+    d.cfl_max, d.cfl_growth, d.cfl_cutback, d.cfl_min = imp.cfl_max, imp.cfl_growth, imp.cfl_cutback, imp.cfl_min
+    d.krylov_tol, d.krylov_success = imp.krylov_tol, imp.krylov_success
+    d.max_relative_update = -1.0 if imp.max_relative_update is None else imp.max_relative_update
+    d.krylov_subspace, d.krylov_restarts = imp.krylov_subspace, imp.krylov_restarts
+    d.preconditioner = {"none": 0, "line_j": 1}[imp.preconditioner]
     return d, keep
 
 
@@ -147,12 +158,12 @@ class DevicePlan3:
     NK)`` float64 NumPy arrays in and out)."""
 
     def __init__(self, plan: Plan3, q_inf, gamma: float, flux: str, limiter: str, kappa: float = 0.0,
-                 mu_inf: float | None = None, sutherland: float | None = None, library=None):
+                 mu_inf: float | None = None, sutherland: float | None = None, implicit=None, library=None):
         self.lib = load_library(library)
         self.plan = plan
         self.nvar = len(q_inf)
         self.shape = (self.nvar,) + plan.shape
-        d, keep = describe(plan, q_inf, gamma, flux, limiter, kappa, mu_inf, sutherland)
+        d, keep = describe(plan, q_inf, gamma, flux, limiter, kappa, mu_inf, sutherland, implicit)
         handle = C.c_void_p()
         _check(self.lib, self.lib.jr_plan3d_create(C.byref(d), C.byref(handle)), "jr_plan3d_create")
         self.handle = handle
@@ -196,6 +207,16 @@ class DevicePlan3:
             parts.append(flat[at:at + int(np.prod(s))].reshape(s))
             at += int(np.prod(s))
         return parts
+
+    def newton_steps(self, U, n_steps: int, cfl: float, residual_norm: float = float("inf")):
+        """``(U, cfl, |R| before the last accepted step, history)`` after ``n_steps``
+        pseudo-transient Newton steps from ``U`` (``jr_newton_steps3d``)."""
+        (u,), _ = self._run("jr_newton_steps3d", U)
+        c, r = C.c_double(cfl), C.c_double(residual_norm)
+        hist = np.zeros(n_steps)
+        _check(self.lib, self.lib.jr_newton_steps3d(self.handle, u.data_ptr(), int(n_steps), C.byref(c), C.byref(r),
+                                                     hist.ctypes.data), "jr_newton_steps3d")
+        return u.cpu().numpy(), c.value, r.value, hist
 
     def precondition(self, U, cfl: float, r) -> np.ndarray:
         """z = M^-1 r of line_j at (U, cfl)."""

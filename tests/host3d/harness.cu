@@ -7,6 +7,7 @@
 
 #include "../../jax-rans_b200/csrc/plan3d_desc.cuh"
 #include "../../jax-rans_b200/csrc/linesolve3d.cuh"
+#include "../../jax-rans_b200/csrc/newton3d.cuh"
 
 using namespace jr;
 
@@ -89,5 +90,109 @@ extern "C" int jr3_host_precondition(const jr_plan3d_desc* d, const double* U, d
     chain_flow(p, U, cfl, ch, r, z, scratch.data(), scratch.data() + (size_t)p.chain_L * 25);
     if (p.nvar > 5) chain_sa(p, U, cfl, ch, r, z, scratch.data(), scratch.data() + (size_t)p.chain_L * 25);
   }
+  return 0;
+}
+
+// The Newton step's vector operations as host loops (sums in index order).
+struct HostOps {
+  enum { R_ = 0, Z_, W_, T_, RES_, B_, DU_, ACT_, BASE };
+  const Plan3Dev& p;
+  size_t N, n;
+  std::vector<std::vector<double>> vec;
+  std::vector<double> vdt;
+  HostOps(const Plan3Dev& plan, int m) : p(plan) {
+    n = (size_t)p.NI * p.NJ * p.NK;
+    N = (size_t)p.nvar * n;
+    vec.assign(BASE + m + 1, std::vector<double>(N, 0.0));
+    vdt.assign(n, 0.0);
+  }
+  int V(int i) const { return BASE + i; }
+  double* d(int id) { return vec[id].data(); }
+  void prepare(const double* U, double cfl) {
+    for (size_t c = 0; c < n; ++c) vdt[c] = lambda_sum(p, U, (int)c) / cfl;
+  }
+  void residual(const double* U, int out) {
+    const bool visc = p.P.mu_inf > 0.0, sa = p.nvar > 5;
+    if (sa) run<double, true, true>(p, U, nullptr, d(out), 0);
+    else if (visc) run<double, true, false>(p, U, nullptr, d(out), 0);
+    else run<double, false, false>(p, U, nullptr, d(out), 0);
+  }
+  void matvec(const double* U, double, int src, int out) {
+    const bool visc = p.P.mu_inf > 0.0, sa = p.nvar > 5;
+    if (sa) run<Dual, true, true>(p, U, d(src), d(out), 1);
+    else if (visc) run<Dual, true, false>(p, U, d(src), d(out), 1);
+    else run<Dual, false, false>(p, U, d(src), d(out), 1);
+    for (size_t e = 0; e < N; ++e) d(out)[e] = vdt[e % n] * d(src)[e] + d(out)[e];
+  }
+  void precondition(const double* U, double cfl, int src, int dst) {
+    for (size_t e = 0; e < N; ++e) d(dst)[e] = d(src)[e];
+    std::vector<double> scratch((size_t)p.chain_L * 30);
+    for (int ch = 0; ch < p.n_chains; ++ch) {
+      chain_flow(p, U, cfl, ch, d(src), d(dst), scratch.data(), scratch.data() + (size_t)p.chain_L * 25);
+      if (p.nvar > 5) chain_sa(p, U, cfl, ch, d(src), d(dst), scratch.data(), scratch.data() + (size_t)p.chain_L * 25);
+    }
+  }
+  double dot(int a, int b) {
+    double s = 0.0;
+    for (size_t e = 0; e < N; ++e) s += d(a)[e] * d(b)[e];
+    return s;
+  }
+  double nrm2(int a) { return std::sqrt(dot(a, a)); }
+  void axpy(double al, int x, int y) { for (size_t e = 0; e < N; ++e) d(y)[e] = d(y)[e] + al * d(x)[e]; }
+  void scale(double al, int x, int y) { for (size_t e = 0; e < N; ++e) d(y)[e] = al * d(x)[e]; }
+  void copy(int x, int y) { vec[y] = vec[x]; }
+  void zero(int y) { std::fill(vec[y].begin(), vec[y].end(), 0.0); }
+  double density_norm(int r) {
+    double a = 0.0, w = 0.0;
+    for (size_t c = 0; c < n; ++c)
+      if (p.interior[c]) {
+        a += p.volume[c] * d(r)[c] * d(r)[c];
+        w += p.volume[c];
+      }
+    return std::sqrt(a / w);
+  }
+  double worst_ratio(const double* U, int du) {
+    double worst = 0.0;
+    for (size_t c = 0; c < n; ++c) {
+      double q[NV3_MAX];
+      prim_at(p, U, (int)c, q);
+      const double* D = d(du);
+      double de = D[4 * n + c];
+      for (int k = 0; k < 3; ++k) de = de - q[1 + k] * D[(1 + k) * n + c];
+      const double vv = (q[1] * q[1] + q[2] * q[2]) + q[3] * q[3];
+      const double dp = (p.P.gamma - 1.0) * (de + 0.5 * vv * D[c]);
+      worst = std::fmax(worst, std::fabs(D[c]) / q[0]);
+      worst = std::fmax(worst, std::fabs(dp) / q[4]);
+      if (p.nvar > 5) {
+        const double nh = U[5 * n + c] / q[0];
+        const double dnh = (D[5 * n + c] - nh * D[c]) / q[0];
+        worst = std::fmax(worst, std::fabs(dnh) / std::fmax(std::fabs(nh), 1.0));
+      }
+    }
+    return worst;
+  }
+  bool physical_after(const double* U, int du) {
+    std::vector<double> cand(N);
+    for (size_t e = 0; e < N; ++e) {
+      if (!std::isfinite(d(du)[e])) return false;
+      cand[e] = U[e] + d(du)[e];
+    }
+    for (size_t c = 0; c < n; ++c) {
+      double q[NV3_MAX];
+      prim_at(p, cand.data(), (int)c, q);
+      if (!(q[0] > 1e-10) || !(q[4] > 1e-10) || !std::isfinite(q[0]) || !std::isfinite(q[4])) return false;
+    }
+    return true;
+  }
+  void add_to_state(double* U, int du) { for (size_t e = 0; e < N; ++e) U[e] = U[e] + d(du)[e]; }
+};
+
+extern "C" int jr3_host_newton_steps(const jr_plan3d_desc* d, const double* config, const int* iconfig, double* U,
+                                     double* cfl, double* res_prev, int n_steps, double* history) {
+  const Plan3Dev p = plan_of(d);
+  Newton3Config c{iconfig[0], iconfig[1], iconfig[2], config[0], config[1], config[2], config[3], config[4],
+                  config[5], config[6]};
+  HostOps ops(p, c.restart);
+  for (int s = 0; s < n_steps; ++s) history[s] = newton_step3(ops, U, *cfl, *res_prev, c);
   return 0;
 }

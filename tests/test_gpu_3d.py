@@ -38,8 +38,11 @@ def device3d():
     q_inf = np.array([1.0, flow.mach * np.cos(a), 0.0, flow.mach * np.sin(a), 1.0 / flow.gamma,
                       flow.nu_tilde_ratio])
     cv = doc["numerical"]["convective_fluxes"]
+    from jaxrans_b200.case import NUMERICAL_FILE, _section, _values
+    from jaxrans_b200.config import ImplicitConfig
+    imp = ImplicitConfig(**_values(_section(doc["numerical"], NUMERICAL_FILE, "implicit"), NUMERICAL_FILE, "implicit"))
     dev = DevicePlan3(plan, q_inf, flow.gamma, cv["riemann_solver"], cv["limiter"], 0.0, flow.mu_inf,
-                      flow.sutherland_ratio)
+                      flow.sutherland_ratio, imp)
     yield z, dev
     dev.close()
 
@@ -72,3 +75,12 @@ def test_wave_speeds3d_and_line_solve_match_the_reference(cuda, device3d, state)
         assert np.allclose(lam, z[f"{state}_lam{a}"], rtol=1e-13, atol=0.0)
     zz = dev.precondition(U, 25.0, z[f"{state}_prec_r"])
     assert rows_rel(zz, z[f"{state}_prec_z"]) < 1e-10
+
+
+def test_newton_steps3d_match_the_reference(cuda, device3d):
+    z, dev = device3d
+    U, cfl, res, hist = dev.newton_steps(z["rand0_U"], 3, 25.0)
+    for k in range(3):
+        assert np.isclose(hist[k], float(z[f"newton{k}_norm"]), rtol=1e-10, atol=0.0)
+    assert rows_rel(U, z["newton2_U"]) < 1e-8
+    assert np.isclose(cfl, float(z["newton2_cfl"]), rtol=1e-12)

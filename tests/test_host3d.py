@@ -125,3 +125,32 @@ def test_kernel_bodies_give_the_reference_line_solve(harness, case3d, state):
     lam = n3.wave_speeds(U, model)
     thomas = i3.precondition(U, lam, 25.0, model, solver="thomas")(r)
     assert rows_rel(out, thomas) < 1e-13
+
+
+def test_newton_steps_match_the_reference(harness, case3d):
+    """Three pseudo-transient Newton steps (GMRES with the line preconditioner, the
+    relaxation, acceptance and CFL ramp) driven by csrc/newton3d.cuh over host loops,
+    from the 'rand0' state at CFL 25 (src/jaxrans/solvers/implicit.py:84-168)."""
+    import json as _json
+    from jaxrans_b200.case import NUMERICAL_FILE, _section, _values
+    from jaxrans_b200.config import ImplicitConfig
+    z, plan, desc, _ = case3d
+    doc = _json.loads(str(z["case_json"]))
+    cfg = ImplicitConfig(**_values(_section(doc["numerical"], NUMERICAL_FILE, "implicit"), NUMERICAL_FILE, "implicit"))
+    config = np.array([cfg.krylov_tol, cfg.krylov_success,
+                       cfg.max_relative_update if cfg.max_relative_update is not None else -1.0,
+                       cfg.cfl_min, cfg.cfl_max, cfg.cfl_growth, cfg.cfl_cutback])
+    iconfig = np.array([cfg.krylov_subspace, cfg.krylov_restarts, 1], dtype=np.int32)
+    harness.jr3_host_newton_steps.restype = C.c_int
+    harness.jr3_host_newton_steps.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                              C.c_void_p, C.c_int, C.c_void_p]
+    U = np.ascontiguousarray(z["rand0_U"]).copy()
+    cfl, res = C.c_double(25.0), C.c_double(np.inf)
+    hist = np.zeros(3)
+    assert harness.jr3_host_newton_steps(C.addressof(desc), config.ctypes.data, iconfig.ctypes.data, U.ctypes.data,
+                                         C.byref(cfl), C.byref(res), 3, hist.ctypes.data) == 0
+    # per-step |R| before the update; the final state and CFL
+    for k in range(3):
+        assert np.isclose(hist[k], float(z[f"newton{k}_norm"]), rtol=1e-11, atol=0.0)
+    assert rows_rel(U, z["newton2_U"]) < 1e-9
+    assert np.isclose(cfl.value, float(z["newton2_cfl"]), rtol=1e-12)
