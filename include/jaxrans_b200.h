@@ -272,6 +272,13 @@ typedef struct jr_plan3d_desc {
   double cfl_max, cfl_growth, cfl_cutback, cfl_min;
   double krylov_tol, krylov_success, max_relative_update;   /* max_relative_update <= 0: none */
   int32_t krylov_subspace, krylov_restarts, preconditioner;
+  /* wall faces (the forces) */
+  int32_t n_walls;
+  const int32_t* wall_cell;     /* the block cell on the face */
+  const int32_t* wall_family;   /* the face's family (normal index axis) */
+  const int32_t* wall_face;     /* its index within the family's canvas faces */
+  const double* wall_into;      /* +1 where the family's vector points into the fluid, else -1 */
+  const double* wall_mid;       /* 3 per face: the mean of its four nodes */
 } jr_plan3d_desc;
 
 /* Build a 3D plan (device copies of the tables, work buffers, a stream).  Every record
@@ -307,6 +314,12 @@ int jr_precondition3d(jr_plan3d* plan, const double* U, double cfl, const double
  * driver's block on a 3D atlas. */
 int jr_newton_steps3d(jr_plan3d* plan, double* U, int32_t n_steps, double* cfl, double* residual_norm,
                       double* history);
+/* Force coefficients of a 3D case at U (device): out (host, 4) = cl, cd, cm, cd_friction
+ * -- lift and drag in the plane of incidence (x-z) per q_inf * area, the pitching moment
+ * of pressure and friction about centre (3 values) per q_inf * area * length; the
+ * friction from the laminar viscous flux at the wall.  Replaces force_coefficients
+ * (src/jaxrans/post/forces.py:108-161) on a 3D atlas.  Synchronises. */
+int jr_forces3d(jr_plan3d* plan, const double* U, double area, double length, const double* centre, double* out);
 
 #ifdef __cplusplus
 }

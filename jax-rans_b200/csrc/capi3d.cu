@@ -22,6 +22,8 @@ struct jr_plan3d {
   double* scratch = nullptr;   // the line solve's eliminated blocks: n_chains * chain_L * 30
   size_t n_canvas = 0;
   Newton3Config cfg{};
+  double* loads = nullptr;     // 7 per wall face
+  std::vector<double> wall_mid;
   double* work = nullptr;      // the Newton step's vectors
   int* flag = nullptr;
   cudaStream_t st = nullptr;
@@ -136,6 +138,35 @@ int jr_plan3d_create(const jr_plan3d_desc* d, jr_plan3d** out) {
   TRY3(copy3(p, &dv.ch_cells, d->chain_cells, n_links));
   TRY3(copy3(p, &dv.ch_face, d->chain_up_face, n_links));
   TRY3(copy3(p, &dv.ch_sign, d->chain_up_sign, n_links));
+  if (d->n_walls < 0 || (d->n_walls > 0 && (!d->wall_cell || !d->wall_family || !d->wall_face || !d->wall_into ||
+                                            !d->wall_mid))) {
+    jr_plan3d_destroy(p);
+    return report_error(JR_EINVAL, "bad wall tables");
+  }
+  for (int w = 0; w < d->n_walls; ++w) {
+    const int a = d->wall_family[w];
+    const size_t nf = a >= 0 && a < 3 ? (size_t)(d->NI + (a == 0)) * (d->NJ + (a == 1)) * (d->NK + (a == 2)) : 0;
+    if (a < 0 || a > 2 || d->wall_face[w] < 0 || (size_t)d->wall_face[w] >= nf || d->wall_cell[w] < 0 ||
+        (size_t)d->wall_cell[w] >= n) {
+      jr_plan3d_destroy(p);
+      return report_error(JR_EINVAL, "a wall face outside the canvas");
+    }
+  }
+  dv.n_walls = d->n_walls;
+  TRY3(copy3(p, &dv.w_cell, d->wall_cell, (size_t)d->n_walls));
+  TRY3(copy3(p, &dv.w_family, d->wall_family, (size_t)d->n_walls));
+  TRY3(copy3(p, &dv.w_face, d->wall_face, (size_t)d->n_walls));
+  TRY3(copy3(p, &dv.w_into, d->wall_into, (size_t)d->n_walls));
+  p->wall_mid.assign(d->wall_mid, d->wall_mid + 3 * (size_t)d->n_walls);
+  if (d->n_walls > 0) {
+    void* l = nullptr;
+    if (cudaMalloc(&l, (size_t)d->n_walls * 7 * sizeof(double)) != cudaSuccess) {
+      jr_plan3d_destroy(p);
+      return report_error(JR_ENOMEM, "cudaMalloc failed");
+    }
+    p->allocs.push_back(l);
+    p->loads = static_cast<double*>(l);
+  }
   physics3_from_desc(dv.P, d);
   if (n_links > 0) {
     void* sc = nullptr;
@@ -237,6 +268,22 @@ int jr_newton_steps3d(jr_plan3d* plan, double* U, int32_t n_steps, double* cfl, 
   *cfl = c;
   *residual_norm = r;
   return check3("jr_newton_steps3d");
+}
+
+int jr_forces3d(jr_plan3d* plan, const double* U, double area, double length, const double* centre, double* out) {
+  if (!plan || !U || !centre || !out) return report_error(JR_EINVAL, "null argument");
+  if (!(area > 0.0) || !(length > 0.0)) return report_error(JR_EINVAL, "area and length must be positive");
+  const int nw = plan->dev.n_walls;
+  std::vector<double> loads((size_t)nw * 7);
+  if (nw > 0) {
+    launch_wall_loads3(plan->dev, U, plan->loads, plan->A, plan->B, plan->st);
+    cudaMemcpyAsync(loads.data(), plan->loads, loads.size() * sizeof(double), cudaMemcpyDeviceToHost, plan->st);
+  }
+  if (cudaStreamSynchronize(plan->st) != cudaSuccess) return check3("jr_forces3d");
+  int rc = check3("jr_forces3d");
+  if (rc) return rc;
+  force_coefficients3(plan->dev.P, nw, loads.data(), plan->wall_mid.data(), area, length, centre, out);
+  return JR_OK;
 }
 
 }  // extern "C"

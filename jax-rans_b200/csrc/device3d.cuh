@@ -45,6 +45,11 @@ struct Plan3Dev {
   const int* ch_cells;         // [chain * chain_L + k], -1 past the chain's end
   const int* ch_face;          // link k -> k+1: flat index into the three face families, concatenated
   const int* ch_sign;          // +1 / -1: the link face's vector points out of / into cell k; 0 none
+  int n_walls;                 // wall faces: the cell on each, the face's family and index in it,
+  const int* w_cell;           // +1 where its vector points into the fluid
+  const int* w_family;
+  const int* w_face;
+  const double* w_into;
   Physics3 P;
 };
 
@@ -225,6 +230,7 @@ void launch_residual3(const Plan3Dev& p, const double* U, double* R, void* A, vo
                       cudaStream_t st);
 void launch_jvp3(const Plan3Dev& p, const double* U, const double* v, double* Jv, void* A, void* B, cudaStream_t st);
 void launch_wave_speeds3(const Plan3Dev& p, const double* U, double* lam, cudaStream_t st);
+void launch_wall_loads3(const Plan3Dev& p, const double* U, double* loads, void* A, void* B, cudaStream_t st);
 void launch_precondition3(const Plan3Dev& p, const double* U, double cfl, const double* r, double* z, double* scratch,
                           cudaStream_t st);
 

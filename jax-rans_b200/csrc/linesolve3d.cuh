@@ -309,3 +309,49 @@ inline __host__ __device__ void chain_sa(const Plan3Dev& p, const double* U, dou
 }
 
 }  // namespace jr
+
+namespace jr {
+
+// The loads on wall face w (src/jaxrans/post/forces.py:48-68): 7 values -- the gauge
+// pressure, the area vector into the fluid (3), the laminar viscous force on the body
+// (3) -- from the ghost-filled primitive canvas Q.
+inline __host__ __device__ void wall_load(const Plan3Dev& p, const double* Q, int w, double out[7]) {
+  const int n = p.NI * p.NJ * p.NK;
+  const double g = p.P.gamma;
+  const int c = p.w_cell[w], a = p.w_family[w], f = p.w_face[w];
+  const int fj = p.NJ + (a == 1), fk = p.NK + (a == 2);
+  const int i = f / (fj * fk), j = (f / fk) % fj, k = f % fk;
+  double s[3];
+  face_vector(p, a, i, j, k, s);
+  const double into = p.w_into[w];
+  out[0] = Q[(size_t)4 * n + c] - 1.0 / g;
+  for (int m = 0; m < 3; ++m) out[1 + m] = into * s[m];
+  for (int m = 0; m < 3; ++m) out[4 + m] = 0.0;
+  if (p.P.mu_inf > 0.0) {
+    double grad[3][5];
+    face_gradient<double>(p, Q, a, i, j, k, 4, grad);
+    int lo[3] = {i, j, k};
+    lo[a] -= 1;
+    double ql[NV3_MAX], qh[NV3_MAX];
+    load_cell(p, Q, cell_index(p, lo[0], lo[1], lo[2]), ql);
+    load_cell(p, Q, cell_index(p, i, j, k), qh);
+    const double T = 0.5 * (g * ql[4] / ql[0] + g * qh[4] / qh[0]);
+    const double mu = viscosity3(p.P, T);
+    const double div = grad[0][0] + grad[1][1] + grad[2][2];
+    const double ttd = (2.0 / 3.0) * div;
+    for (int comp = 0; comp < 3; ++comp) {
+      double tau[3];
+      for (int d = 0; d < 3; ++d) {
+        if (comp == d) {
+          tau[d] = mu * (2.0 * grad[comp][comp] - ttd);
+        } else {
+          const int lo2 = comp < d ? comp : d, hi2 = comp < d ? d : comp;
+          tau[d] = mu * (grad[hi2][lo2] + grad[lo2][hi2]);
+        }
+      }
+      out[4 + comp] = into * ((tau[0] * s[0] + tau[1] * s[1]) + tau[2] * s[2]);
+    }
+  }
+}
+
+}  // namespace jr

@@ -24,4 +24,32 @@ inline void physics3_from_desc(Physics3& P, const jr_plan3d_desc* d) {
   sa_constants(P.sa);
 }
 
+// cl, cd, cm, cd_friction from the per-face wall loads (7 each) and the faces' midpoints
+// (src/jaxrans/post/forces.py:108-161, 3D: lift and drag in the x-z plane)
+inline void force_coefficients3(const Physics3& P, int n_walls, const double* loads, const double* mid, double area,
+                                double length, const double* centre, double out[4]) {
+  const double* q = P.q_inf;
+  const double speed = sqrt((q[1] * q[1] + q[2] * q[2]) + q[3] * q[3]);
+  const double drag[3] = {q[1] / speed, q[2] / speed, q[3] / speed};
+  const double lift[3] = {-drag[2], 0.0, drag[0]};
+  const double q_area = 0.5 * q[0] * speed * speed * area;
+  double cl = 0.0, cd = 0.0, cm = 0.0, shear[3] = {0.0, 0.0, 0.0};
+  for (int w = 0; w < n_walls; ++w) {
+    const double* L = loads + (size_t)7 * w;
+    double load[3];
+    for (int m = 0; m < 3; ++m) {
+      load[m] = -L[0] * L[1 + m] + L[4 + m];
+      shear[m] = shear[m] + L[4 + m];
+    }
+    cl = cl + ((lift[0] * load[0] + lift[1] * load[1]) + lift[2] * load[2]);
+    cd = cd + ((drag[0] * load[0] + drag[1] * load[1]) + drag[2] * load[2]);
+    const double rx = mid[3 * w] - centre[0], rz = mid[3 * w + 2] - centre[2];
+    cm = cm + (rz * load[0] - rx * load[2]) / length;
+  }
+  out[0] = cl / q_area;
+  out[1] = cd / q_area;
+  out[2] = cm / q_area;
+  out[3] = ((drag[0] * shear[0] + drag[1] * shear[1]) + drag[2] * shear[2]) / q_area;
+}
+
 }  // namespace jr

@@ -12,6 +12,7 @@
 // reference's edge padding.
 #include <cstdint>
 
+#include "linesolve3d.cuh"
 #include "residual3d.cuh"
 
 namespace jr {
@@ -69,6 +70,19 @@ static void residual3_t(const Plan3Dev& p, const double* U, const double* dU, do
     k3_residual<T, true, false><<<blocks, 128, 0, st>>>(p, A, U, dU, R, first_order);
   else
     k3_residual<T, false, false><<<blocks, 128, 0, st>>>(p, A, U, dU, R, first_order);
+}
+
+__global__ void k3_wall_loads(Plan3Dev p, const double* __restrict__ Q, double* __restrict__ loads) {
+  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < p.n_walls; w += gridDim.x * blockDim.x)
+    wall_load(p, Q, w, loads + (size_t)7 * w);
+}
+
+// the loads on every wall face (7 each) at U: the primitive canvas ghost-filled first
+void launch_wall_loads3(const Plan3Dev& p, const double* U, double* loads, void* A, void* B, cudaStream_t st) {
+  const int n = p.NI * p.NJ * p.NK;
+  k3_prim<double><<<(n + 127) / 128, 128, 0, st>>>(p, U, nullptr, (double*)A);
+  fill3(p, (double*)A, (double*)B, st);
+  if (p.n_walls > 0) k3_wall_loads<<<(p.n_walls + 127) / 128, 128, 0, st>>>(p, (const double*)A, loads);
 }
 
 void launch_residual3(const Plan3Dev& p, const double* U, double* R, void* A, void* B, bool first_order,

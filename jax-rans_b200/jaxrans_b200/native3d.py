@@ -37,6 +37,8 @@ class Plan3Desc(C.Structure):
         ("cfl_max", C.c_double), ("cfl_growth", C.c_double), ("cfl_cutback", C.c_double), ("cfl_min", C.c_double),
         ("krylov_tol", C.c_double), ("krylov_success", C.c_double), ("max_relative_update", C.c_double),
         ("krylov_subspace", C.c_int32), ("krylov_restarts", C.c_int32), ("preconditioner", C.c_int32),
+        ("n_walls", C.c_int32), ("wall_cell", _i32p), ("wall_family", _i32p), ("wall_face", _i32p),
+        ("wall_into", _f64p), ("wall_mid", _f64p),
     ]
 
 
@@ -150,6 +152,13 @@ def describe(plan: Plan3, q_inf, gamma: float, flux: str, limiter: str, kappa: f
     d.max_relative_update = -1.0 if imp.max_relative_update is None else imp.max_relative_update
     d.krylov_subspace, d.krylov_restarts = imp.krylov_subspace, imp.krylov_restarts
     d.preconditioner = {"none": 0, "line_j": 1}[imp.preconditioner]
+    W = plan.walls
+    d.n_walls = len(W.cell)
+    d.wall_cell = ptr(arr(W.cell, np.int32), _i32p)
+    d.wall_family = ptr(arr(W.family, np.int32), _i32p)
+    d.wall_face = ptr(arr(W.face, np.int32), _i32p)
+    d.wall_into = ptr(arr(W.into_fluid, np.float64), _f64p)
+    d.wall_mid = ptr(arr(W.quads.corners.mean(axis=1), np.float64), _f64p)
     return d, keep
 
 
@@ -217,6 +226,15 @@ class DevicePlan3:
         _check(self.lib, self.lib.jr_newton_steps3d(self.handle, u.data_ptr(), int(n_steps), C.byref(c), C.byref(r),
                                                      hist.ctypes.data), "jr_newton_steps3d")
         return u.cpu().numpy(), c.value, r.value, hist
+
+    def forces(self, U, area: float, length: float = 1.0, centre=(0.25, 0.0, 0.0)) -> np.ndarray:
+        """``(cl, cd, cm, cd_friction)`` at ``U`` (``jr_forces3d``)."""
+        (u,), _ = self._run("jr_forces3d", U)
+        c = np.ascontiguousarray(centre, dtype=np.float64)
+        out = np.zeros(4)
+        _check(self.lib, self.lib.jr_forces3d(self.handle, u.data_ptr(), float(area), float(length), c.ctypes.data,
+                                               out.ctypes.data), "jr_forces3d")
+        return out
 
     def precondition(self, U, cfl: float, r) -> np.ndarray:
         """z = M^-1 r of line_j at (U, cfl)."""

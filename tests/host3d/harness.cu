@@ -48,6 +48,11 @@ static Plan3Dev plan_of(const jr_plan3d_desc* d) {
   p.ch_cells = d->chain_cells;
   p.ch_face = d->chain_up_face;
   p.ch_sign = d->chain_up_sign;
+  p.n_walls = d->n_walls;
+  p.w_cell = d->wall_cell;
+  p.w_family = d->wall_family;
+  p.w_face = d->wall_face;
+  p.w_into = d->wall_into;
   physics3_from_desc(p.P, d);
   return p;
 }
@@ -194,5 +199,21 @@ extern "C" int jr3_host_newton_steps(const jr_plan3d_desc* d, const double* conf
                   config[5], config[6]};
   HostOps ops(p, c.restart);
   for (int s = 0; s < n_steps; ++s) history[s] = newton_step3(ops, U, *cfl, *res_prev, c);
+  return 0;
+}
+
+extern "C" int jr3_host_forces(const jr_plan3d_desc* d, const double* U, double area, double length,
+                               const double* centre, double* out) {
+  const Plan3Dev p = plan_of(d);
+  const int n = p.NI * p.NJ * p.NK;
+  std::vector<double> A((size_t)p.nvar * n), B((size_t)p.nvar * n), loads((size_t)p.n_walls * 7);
+  for (int c = 0; c < n; ++c) prim_cell(p, U, (const double*)nullptr, A.data(), c);
+  for (int s = 0; s < p.n_stages; ++s) {
+    B = A;
+    for (int r = p.stage_off[s]; r < p.stage_off[s + 1]; ++r) ghost_record(p, A.data(), B.data(), r);
+    std::swap(A, B);
+  }
+  for (int w = 0; w < p.n_walls; ++w) wall_load(p, A.data(), w, loads.data() + (size_t)7 * w);
+  force_coefficients3(p.P, p.n_walls, loads.data(), d->wall_mid, area, length, centre, out);
   return 0;
 }

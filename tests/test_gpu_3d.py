@@ -84,3 +84,11 @@ def test_newton_steps3d_match_the_reference(cuda, device3d):
         assert np.isclose(hist[k], float(z[f"newton{k}_norm"]), rtol=1e-10, atol=0.0)
     assert rows_rel(U, z["newton2_U"]) < 1e-8
     assert np.isclose(cfl, float(z["newton2_cfl"]), rtol=1e-12)
+
+
+@pytest.mark.parametrize("state", ["sin", "rand0"])
+def test_forces3d_match_the_reference(cuda, device3d, state):
+    z, dev = device3d
+    area = json.loads(str(z["case_json"]))["case"]["domain"]["reference_area"]
+    assert np.allclose(dev.forces(z[f"{state}_U"], area, 0.8, (0.25, 0.0, 0.0)), z[f"{state}_forces"],
+                       rtol=1e-11, atol=1e-16)

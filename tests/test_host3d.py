@@ -154,3 +154,18 @@ def test_newton_steps_match_the_reference(harness, case3d):
         assert np.isclose(hist[k], float(z[f"newton{k}_norm"]), rtol=1e-11, atol=0.0)
     assert rows_rel(U, z["newton2_U"]) < 1e-9
     assert np.isclose(cfl.value, float(z["newton2_cfl"]), rtol=1e-12)
+
+
+@pytest.mark.parametrize("state", ["sin", "rand0"])
+def test_kernel_bodies_give_the_reference_forces(harness, case3d, state):
+    import json as _json
+    z, plan, desc, _ = case3d
+    f = harness.jr3_host_forces
+    f.restype = C.c_int
+    f.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_void_p]
+    area = _json.loads(str(z["case_json"]))["case"]["domain"]["reference_area"]
+    U = np.ascontiguousarray(z[f"{state}_U"])
+    centre = np.array([0.25, 0.0, 0.0])
+    out = np.zeros(4)
+    assert f(C.addressof(desc), U.ctypes.data, area, 0.8, centre.ctypes.data, out.ctypes.data) == 0
+    assert np.allclose(out, z[f"{state}_forces"], rtol=1e-11, atol=1e-16)
