@@ -20,6 +20,7 @@ import numpy as np
 from .config import (FLUXES, LIMITERS, PRECONDITIONERS, TURBULENCE_MODELS, FlowConditions, ImplicitConfig,
                      NumericsConfig, PRANDTL_LAMINAR, GAMMA_AIR)
 from .geometry import section_source
+from .grid3d import KINDS_3D, Block3
 from .grids import CONDITION_KINDS, WALL_KINDS, Block, c_grid, o_grid, patch_names
 from .plan import Plan, build_plan
 
@@ -174,21 +175,25 @@ class GridSpec:
                             f"choose from {sorted(BUILT_GRIDS)}")
         if self.grid == "file":
             from .gridfile import PatchRule, load_grid, read_plot3d_2d
+            from .gridfile3d import is_3d, load_grid3d
             path = self.resolve(base)
             if self.format == "cgns" or path.suffix.lower() == ".cgns":
                 raise CaseError("a CGNS grid file is not implemented in this build; use Plot3D")
             try:
-                read_plot3d_2d(path)
-            except ValueError as error:
-                if "not a 2D plane" in str(error):
-                    raise CaseError("a 3D grid file is not implemented in this build's case loader "
-                                    "(the 3D plan is built from jaxrans_b200.grid3d blocks)") from None
-                raise CaseError(str(error)) from None
-            try:
                 rules = tuple(PatchRule(**rule) for rule in self.patches)
             except TypeError as error:
                 raise CaseError(f"'domain.patches': {error}") from None
-            return load_grid(path, self.coordinate_scale, rules)
+            try:
+                if is_3d(path):
+                    if self.reference_area is None:
+                        raise CaseError("a 3D case needs 'domain.reference_area'")
+                    return load_grid3d(path, self.coordinate_scale, rules)
+                read_plot3d_2d(path)
+                return load_grid(path, self.coordinate_scale, rules)
+            except ValueError as error:
+                if isinstance(error, CaseError):
+                    raise
+                raise CaseError(str(error)) from None
         section = section_source(self.airfoil, base).normalised()
         if self.trailing_edge == "close" and not section.sharp:
             raise CaseError("'domain.trailing_edge' = 'close' on a blunt section is not implemented in this build")
@@ -216,12 +221,21 @@ class Case:
     raw: dict = field(compare=False, repr=False)
     sequencing: int = 0
 
-    def grid(self) -> Plan:
-        """The grid, every patch given its condition, packed into a plan."""
+    def grid(self):
+        """The grid, every patch given its condition, packed into a plan: a ``Plan``, or
+        for a 3D grid file a ``plan3d.Plan3``."""
         mesh = self.grid_spec.build(self.directory)
         kinds = resolve_conditions(self.conditions, patch_names(mesh), self.flow)
         mesh = [b.with_kinds(kinds) for b in mesh]
-        return build_plan(mesh, self.numerics.n_ghost, with_distance=self.flow.turbulence is not None)
+        turbulent = self.flow.turbulence is not None
+        if mesh and isinstance(mesh[0], Block3):
+            from .plan3d import build_plan3d
+            unsupported = sorted({k for k in kinds.values() if k not in KINDS_3D})
+            if unsupported:
+                raise CaseError(f"boundary condition(s) {unsupported} are not implemented on the 3D path; "
+                                f"it has {sorted(KINDS_3D)}")
+            return build_plan3d(mesh, with_distance=turbulent)
+        return build_plan(mesh, self.numerics.n_ghost, with_distance=turbulent)
 
 
 def _section(doc: dict, file: str, name: str, required: bool = False) -> dict:

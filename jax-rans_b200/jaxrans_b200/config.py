@@ -189,3 +189,12 @@ def freestream_primitive(flow: FlowConditions) -> tuple[float, ...]:
     a = flow.alpha_rad
     q = (1.0, float(flow.mach * np.cos(a)), float(flow.mach * np.sin(a)), 1.0 / flow.gamma)
     return q + ((flow.nu_tilde_ratio,) if flow.turbulence is not None else ())
+
+
+def freestream_primitive3(flow: FlowConditions) -> tuple[float, ...]:
+    """``(rho, u, v, w, p[, nu_hat])`` of the 3D freestream: the incidence in the x-z
+    plane (x chordwise, y along the span, z up), ``V = M (cos a, 0, sin a)``
+    (``src/jaxrans/core/state.py:96-139``)."""
+    a = flow.alpha_rad
+    q = (1.0, float(flow.mach * np.cos(a)), 0.0, float(flow.mach * np.sin(a)), 1.0 / flow.gamma)
+    return q + ((flow.nu_tilde_ratio,) if flow.turbulence is not None else ())

@@ -29,6 +29,7 @@ from .geometry import Section
 from .grids import CONDITION_KINDS, WALL_KINDS, c_grid
 
 SIDES_3D = ("j_min", "j_max", "i_min", "i_max", "k_min", "k_max")
+KINDS_3D = ("slip_wall", "no_slip_wall", "symmetry", "far_field")   # the 3D path's conditions
 AXIS = {"i": 0, "j": 1, "k": 2}
 
 
@@ -99,6 +100,10 @@ class Block3:
 
     def boundaries(self) -> list:
         return [(s, r) for s in SIDES_3D for r in self.sides[s] if isinstance(r, Rect3)]
+
+    def patches(self) -> list:
+        """``(side, Rect3)`` of every named patch (as ``grids.Block.patches``)."""
+        return self.boundaries()
 
     def with_kinds(self, kinds: dict[str, str]) -> "Block3":
         new = {s: [Rect3(r.name, r.start, r.stop, kinds[r.name]) if isinstance(r, Rect3) else r
@@ -174,40 +179,11 @@ def write_plot3d(path: str | Path, blocks: list[np.ndarray]) -> None:
 
 
 def read_plot3d(path: str | Path) -> list[np.ndarray]:
-    """The node arrays ``(3, ni+1, nj+1, nk+1)`` of an unformatted 3D Plot3D file
-    (Fortran records in either byte order, with or without the block count, FP64 or
-    FP32, with or without iblank)."""
-    raw = Path(path).read_bytes()
-    for order in ("<", ">"):
-        records, at = [], 0
-        while at + 4 <= len(raw):
-            n = int(np.frombuffer(raw, order + "i4", 1, at)[0])
-            if n < 0 or at + 8 + n > len(raw) or int(np.frombuffer(raw, order + "i4", 1, at + 4 + n)[0]) != n:
-                records = None
-                break
-            records.append(raw[at + 4:at + 4 + n])
-            at += n + 8
-        if not records or at != len(raw):
-            continue
-        for counted in (True, False):
-            head = 1 if counted else 0
-            nblocks = int(np.frombuffer(records[0], order + "i4")[0]) if counted and len(records[0]) == 4 else 1
-            if counted and len(records[0]) != 4:
-                continue
-            if len(records) != head + 1 + nblocks:
-                continue
-            dims = np.frombuffer(records[head], order + "i4")
-            if dims.size != 3 * nblocks or np.any(dims < 2):
-                continue
-            blocks = []
-            for shape, rec in zip(dims.reshape(nblocks, 3), records[head + 1:]):
-                n = int(np.prod(shape))
-                for fmt in ("f8", "f4"):
-                    size = np.dtype(fmt).itemsize
-                    if len(rec) in (3 * n * size, 3 * n * size + 4 * n):
-                        v = np.frombuffer(rec, order + fmt, 3 * n).astype(np.float64)
-                        blocks.append(np.stack([v[c * n:(c + 1) * n].reshape(shape, order="F") for c in range(3)]))
-                        break
-            if len(blocks) == nblocks:
-                return blocks
-    raise ValueError(f"{Path(path).name}: not an unformatted 3D Plot3D grid")
+    """The node arrays ``(3, ni+1, nj+1, nk+1)`` of a 3D Plot3D file: formatted, or
+    unformatted (Fortran records in either byte order, FP64 or FP32), with or without
+    the block count, with or without iblank."""
+    from .gridfile import read_plot3d_blocks
+    blocks = read_plot3d_blocks(path)
+    if any(len(b) != 3 for b in blocks):
+        raise ValueError(f"{Path(path).name}: a 2D grid, not a 3D one")
+    return [np.stack(b) for b in blocks]

@@ -41,8 +41,9 @@ class PatchRule:
     z_min: float = -np.inf
     z_max: float = np.inf
 
-    def contains(self, x, y):
-        return (x >= self.x_min) & (x <= self.x_max) & (y >= self.y_min) & (y <= self.y_max)
+    def contains(self, x, y, z=None):
+        inside = (x >= self.x_min) & (x <= self.x_max) & (y >= self.y_min) & (y <= self.y_max)
+        return inside if z is None else inside & (z >= self.z_min) & (z <= self.z_max)
 
 
 # --- Plot3D ---------------------------------------------------------------------------------
@@ -166,15 +167,21 @@ def _plane(coords):
     raise ValueError(f"a 3D block of {shape} nodes is not a 2D plane extruded along a thin index")
 
 
-def read_plot3d_2d(path: str | Path) -> list[tuple[np.ndarray, np.ndarray]]:
-    """Every block of a Plot3D file as 2D node arrays ``(x, y)``, ``(ni+1, nj+1)`` each."""
+def read_plot3d_blocks(path: str | Path) -> list[list[np.ndarray]]:
+    """Every block of a Plot3D file as its coordinate arrays, two (2D) or three (3D),
+    each of the block's node shape."""
     path = Path(path)
     raw = _raw(path)
     blocks = _unformatted(raw) if _binary(raw) else _formatted(raw)
     if blocks is None:
         raise ValueError(f"{path.name}: not a Plot3D grid this reader understands (formatted or unformatted, "
                          f"2D or 3D, single or multi-block, with or without iblank)")
-    return [_plane(b) for b in blocks]
+    return blocks
+
+
+def read_plot3d_2d(path: str | Path) -> list[tuple[np.ndarray, np.ndarray]]:
+    """Every block of a Plot3D file as 2D node arrays ``(x, y)``, ``(ni+1, nj+1)`` each."""
+    return [_plane(b) for b in read_plot3d_blocks(path)]
 
 
 def write_plot3d_2d(path: str | Path, blocks: list[tuple[np.ndarray, np.ndarray]]) -> None:

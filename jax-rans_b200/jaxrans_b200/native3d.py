@@ -16,9 +16,10 @@ from dataclasses import dataclass
 import numpy as np
 
 from .native import FLUX_CODES, LIMITER_CODES, NativeError, _check, _f64p, _i32p, _u8p, load_library
+from .grid3d import KINDS_3D
 from .plan3d import Plan3
 
-KIND3 = {"slip_wall": 1, "no_slip_wall": 2, "symmetry": 3, "far_field": 4}
+KIND3 = {k: n + 1 for n, k in enumerate(KINDS_3D)}   # 0: a copy
 
 
 class Plan3Desc(C.Structure):

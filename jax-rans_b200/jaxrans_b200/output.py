@@ -74,7 +74,64 @@ def write_result(result, directory=None, extra: dict | None = None) -> Path:
     arrays = {"n_blocks": np.asarray(len(blocks))}
     for k, (U, b) in enumerate(zip(blocks, result.grid.mesh)):
         arrays[f"U_{k}"] = U
-        arrays[f"x_node_{k}"] = b.x
-        arrays[f"y_node_{k}"] = b.y
+        for axis, c in zip("xyz", _nodes(b)):
+            arrays[f"{axis}_node_{k}"] = c
     np.savez_compressed(directory / f"{name}_fields.npz", **arrays)
+    if getattr(result.grid, "dim", 2) == 3:
+        for k, (U, b) in enumerate(zip(blocks, result.grid.mesh)):
+            write_vts(directory / f"{name}_block{k}.vts", b.nodes, cell_fields3(U, case.flow.gamma))
     return directory
+
+
+def _nodes(block):
+    return block.nodes if hasattr(block, "nodes") else (block.x, block.y)
+
+
+def cell_fields3(U: np.ndarray, gamma: float) -> dict:
+    """Density, velocity, pressure and Mach number of a 3D block's cells
+    (``src/jaxrans/simulation.py:172-177``)."""
+    rho = U[0]
+    velocity = U[1:4] / rho
+    p = (gamma - 1.0) * (U[4] - 0.5 * rho * np.sum(velocity * velocity, axis=0))
+    mach = np.sqrt(np.sum(velocity * velocity, axis=0)) / np.sqrt(gamma * p / rho)
+    return {"density": rho, "velocity": velocity, "pressure": p, "mach": mach}
+
+
+def write_vts(path: Path, nodes: np.ndarray, cells: dict) -> Path:
+    """One 3D block for ParaView (``src/jaxrans/io/output.py:136-185``): a VTK XML
+    structured grid, little-endian raw appended data with 64-bit length headers; the
+    nodes ``(3, ni+1, nj+1, nk+1)`` as points, every array of ``cells`` (scalars of the
+    cell shape, or 3-vectors ``(3, ...)``) as cell data; VTK's order runs ``i`` fastest."""
+    ni, nj, nk = (n - 1 for n in nodes.shape[1:])
+    extent = f"0 {ni} 0 {nj} 0 {nk}"
+    blobs, tags, offset = [], [], 0
+
+    def add(label: str, values: np.ndarray, components: int, group: list):
+        nonlocal offset
+        if components == 1:
+            data = np.asarray(values, dtype="<f8").ravel(order="F")
+        else:
+            data = np.stack([np.asarray(c, dtype="<f8").ravel(order="F") for c in values], axis=1).ravel()
+        raw = data.tobytes()
+        blobs.append(np.array([len(raw)], dtype="<u8").tobytes() + raw)
+        group.append(f'<DataArray type="Float64" Name="{label}" NumberOfComponents="{components}" '
+                     f'format="appended" offset="{offset}"/>')
+        offset += 8 + len(raw)
+
+    points: list = []
+    cell_tags: list = []
+    add("Points", nodes, 3, points)
+    for label, values in cells.items():
+        values = np.asarray(values)
+        add(label, values, 3 if values.ndim == 4 else 1, cell_tags)
+    head = (f'<?xml version="1.0"?>\n<VTKFile type="StructuredGrid" version="1.0" byte_order="LittleEndian" '
+            f'header_type="UInt64"><StructuredGrid WholeExtent="{extent}"><Piece Extent="{extent}">'
+            f'<Points>{"".join(points)}</Points><CellData>{"".join(cell_tags)}</CellData>'
+            f'</Piece></StructuredGrid><AppendedData encoding="raw">_')
+    path = Path(path)
+    with open(path, "wb") as out:
+        out.write(head.encode())
+        for blob in blobs:
+            out.write(blob)
+        out.write(b"</AppendedData></VTKFile>\n")
+    return path

@@ -174,6 +174,7 @@ class Plan3:
     walls: Walls3
     distance: np.ndarray | None = None
     extras: dict = field(default_factory=dict)
+    dim = 3
 
     @property
     def n_canvas(self) -> int:
@@ -194,14 +195,27 @@ class Plan3:
             out[(Ellipsis,) + w] = value
         return out
 
+    def unpack(self, canvas: np.ndarray) -> list:
+        """Each block's cells of a canvas field ``(..., NI, NJ, NK)``."""
+        return [canvas[(Ellipsis,) + w] for w in self.windows()]
+
 
 def _pack2(shapes):
-    """Tiles side by side along the first axis, the plane as wide as the widest."""
-    origins, x = [], 0
-    for w, _ in shapes:
-        origins.append((x, 0))
-        x += w
-    return origins, (x, max(h for _, h in shapes))
+    """First fit in columns: the plane as tall as the tallest tile; tiles taken tallest
+    first (then widest), each stacked on the first column at least as wide as it with
+    room left, else starting a new column (as wide as that tile) to the right."""
+    height = max(h for _, h in shapes)
+    origins = [None] * len(shapes)
+    columns = []                            # [x, width, height used]
+    for k in sorted(range(len(shapes)), key=lambda k: (-shapes[k][1], -shapes[k][0])):
+        w, h = shapes[k]
+        col = next((c for c in columns if w <= c[1] and c[2] + h <= height), None)
+        if col is None:
+            col = [columns[-1][0] + columns[-1][1] if columns else 0, w, 0]
+            columns.append(col)
+        origins[k] = (col[0], col[2])
+        col[2] += h
+    return origins, (columns[-1][0] + columns[-1][1], height)
 
 
 def pack_tiles(tiles):

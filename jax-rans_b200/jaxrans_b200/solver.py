@@ -224,7 +224,7 @@ class CaseMonitor:
     def feed(self, hist: np.ndarray, forces) -> bool:
         """One block; true once the case has stopped."""
         hist = np.asarray(hist, dtype=np.float64)
-        f = forces_of(forces)
+        f = forces if isinstance(forces, Forces) else forces_of(forces)
         self.forces = f
         self.blocks.append(hist)
         self.cl_history.append(f.cl)
@@ -284,7 +284,8 @@ def march(case: Case, plan: Plan, progress=None, initial=None, device=None, max_
 
 
 def run(case: Case, grid: Plan | None = None, progress=None, on_level=None, devices=None, *, initial=None) -> Result:
-    """March ``case`` to steady state on ``grid`` (default ``case.grid()``) on one GPU
+    """March ``case`` to steady state on ``grid`` (default ``case.grid()``; a 3D grid
+    file gives a 3D plan, marched by ``solver3d.march3d``) on one GPU
     (``src/jaxrans/simulation.py:213-240``).  ``devices`` (slabs over several GPUs) is
     not part of this build."""
     if devices is not None and len(devices) > 1:
@@ -292,4 +293,7 @@ def run(case: Case, grid: Plan | None = None, progress=None, on_level=None, devi
     plan = case.grid() if grid is None else grid
     if on_level is not None:
         on_level(0, plan)
+    if getattr(plan, "dim", 2) == 3:
+        from .solver3d import march3d
+        return march3d(case, plan, progress=progress, initial=initial)
     return march(case, plan, progress=progress, initial=initial)

@@ -39,3 +39,29 @@ def fresh_library(request):
     if any(item.get_closest_marker("gpu") for item in request.session.items) and gpu_available():
         from jaxrans_b200.build import build
         build()
+
+
+@pytest.fixture(scope="session")
+def harness(tmp_path_factory):
+    """The 3D kernels' host-and-device bodies built for the host (tests/host3d/harness.cu,
+    nvcc with no device code): the 3D kernels' arithmetic run without a GPU."""
+    import ctypes as C
+    import shutil
+    import subprocess
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(nvcc).exists():
+        pytest.skip("nvcc is not available")
+    out = tmp_path_factory.mktemp("host3d") / "libjr3host.so"
+    subprocess.run([nvcc, "-std=c++17", "-O2", "-Xcompiler", "-fPIC", "-shared",
+                    "-gencode", "arch=compute_100a,code=compute_100a", f"-I{ROOT / 'include'}",
+                    str(ROOT / "tests" / "host3d" / "harness.cu"), "-o", str(out)], check=True)
+    lib = C.CDLL(str(out))
+    p, i, d = C.c_void_p, C.c_int, C.c_double
+    for name, args in {"jr3_host_eval": [p, p, p, p, i],
+                       "jr3_host_wave_speeds": [p, p, p],
+                       "jr3_host_precondition": [p, p, d, p, p],
+                       "jr3_host_newton_steps": [p, p, p, p, p, p, i, p],
+                       "jr3_host_forces": [p, p, d, d, p, p]}.items():
+        f = getattr(lib, name)
+        f.restype, f.argtypes = C.c_int, args
+    return lib

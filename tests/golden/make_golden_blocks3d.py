@@ -1,0 +1,141 @@
+#!/usr/bin/env python3
+"""Generate the multi-block and pole 3D fixtures by running the reference solver itself.
+
+Two grids, written as unformatted Plot3D files and read by the reference through its own
+3D loader (``grid: file``, box patch rules), under the NumPy stand-in in
+``tests/golden/jaxshim`` (as ``make_golden3d.py`` does):
+
+* ``split``: the C-H wing block of ``ch_sa3d`` (``jaxrans_b200.grid3d.wing_block``) cut at
+  two ``i`` stations into three blocks; the second stored with ``i`` and ``k`` reversed,
+  the third with ``i`` and ``k`` swapped (left-handed as stored, so the loader reverses
+  it).  The wake cut becomes an interface between the first and third blocks; SA RANS.
+* ``pole``: a cylinder of cells round the z axis -- ``i`` the azimuth (an O seam), ``j``
+  the radius from the axis (``j_min`` collapsed to a line: a pole), ``k`` along the
+  axis -- with far field all round; inviscid.
+
+For each: the assembled sides, the canvas, the reference's residual, first-order J.v,
+and for ``split`` the wave speeds, the line preconditioner and the forces.
+
+    python tests/golden/make_golden_blocks3d.py
+
+writes ``tests/golden/blocks3d.npz``.  The reference source tree is read from
+``$JAXRANS_REFERENCE`` (default ``/root/reference``).
+"""
+
+from __future__ import annotations
+
+import json
+import os
+import sys
+import tempfile
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+REFERENCE = Path(os.environ.get("JAXRANS_REFERENCE", "/root/reference"))
+sys.path.insert(0, str(HERE / "jaxshim"))
+sys.path.insert(1, str(REFERENCE / "src"))
+sys.path.insert(2, str(ROOT / "jax-rans_b200"))
+
+import numpy as np  # noqa: E402
+
+import jax  # noqa: E402  (the stand-in)
+import jax.numpy as jnp  # noqa: E402
+from jaxrans.case.loader import load_case  # noqa: E402
+from jaxrans.numerics.residual import make_residual  # noqa: E402
+from jaxrans.post.forces import integrate_forces  # noqa: E402
+from jaxrans.solvers import preconditioners as pre  # noqa: E402
+
+from jaxrans_b200.geometry import section_source  # noqa: E402
+from jaxrans_b200.grid3d import wing_block, write_plot3d  # noqa: E402
+
+sys.path.insert(0, str(HERE))
+from make_golden3d import CASE, NUMERICAL, WING, perturbed, sides_record  # noqa: E402
+
+
+def split_blocks() -> list[np.ndarray]:
+    w = dict(WING)
+    nodes = wing_block(section_source(w.pop("section")), **w).nodes
+    a, b, c = nodes[:, :13], nodes[:, 12:25], nodes[:, 24:]
+    return [a.copy(), b[:, ::-1, :, ::-1].copy(), c.transpose(0, 3, 2, 1).copy()]
+
+
+def pole_blocks() -> list[np.ndarray]:
+    theta = np.linspace(0.0, 2.0 * np.pi, 9)
+    theta[-1] = 0.0
+    r = np.array([0.0, 0.4, 0.9, 1.6, 2.5])
+    z = np.linspace(-1.5, 1.5, 7)
+    T, R, Z = np.meshgrid(theta, r, z, indexing="ij")
+    return [np.stack([R * np.cos(T), R * np.sin(T), Z])]
+
+
+POLE_CASE = {"general": {"case_name": "pole3d"},
+             "domain": {"grid": "file", "file": "grid.x", "patches": [{"name": "farfield"}],
+                        "reference_area": 1.0},
+             "boundary_conditions": {"farfield": {"type": "far_field"}},
+             "freestream": {"mach": 0.5, "alpha_deg": 10.0}}
+POLE_NUMERICAL = {"convective_fluxes": {"riemann_solver": "hllc", "limiter": "van_albada_smooth"},
+                  "time_integration": {"solver": "implicit"}}
+
+
+def split_case() -> dict:
+    doc = json.loads(json.dumps(CASE))
+    doc["general"]["case_name"] = "split3d"
+    doc["domain"]["file"] = "grid.x"
+    return doc
+
+
+GRIDS = {"split": (split_blocks, split_case(), NUMERICAL), "pole": (pole_blocks, POLE_CASE, POLE_NUMERICAL)}
+
+
+def main() -> int:
+    out: dict[str, np.ndarray] = {}
+    rng = np.random.default_rng(11)
+    for name, (make, case_doc, numerical) in GRIDS.items():
+        blocks = make()
+        with tempfile.TemporaryDirectory() as tmp:
+            d = Path(tmp)
+            write_plot3d(d / "grid.x", blocks)
+            (d / "case.json").write_text(json.dumps(case_doc))
+            (d / "numerical.json").write_text(json.dumps(numerical))
+            case = load_case(str(d))
+            atlas = case.grid()
+        flow = case.flow
+        op = make_residual(atlas, flow, case.numerics)
+        jop = make_residual(atlas, flow, case.numerics, first_order=True, distance=op.distance)
+        out[f"{name}_case_json"] = np.array(json.dumps({"case": case_doc, "numerical": numerical}))
+        out[f"{name}_n_blocks"] = np.array(len(blocks))
+        for b, nodes in enumerate(blocks):
+            out[f"{name}_raw{b}"] = nodes
+            out[f"{name}_sides{b}"] = np.array(json.dumps(sides_record(atlas.mesh[b])))
+            out[f"{name}_nodes{b}"] = np.asarray(atlas.mesh[b].nodes)
+        out[f"{name}_interior"] = np.asarray(atlas.interior)
+        out[f"{name}_volume"] = np.asarray(atlas.grid.volume)
+        if op.distance is not None:
+            out[f"{name}_distance"] = np.asarray(op.distance)
+        U = perturbed(op.initial_state(), 5, 1e-2)
+        out[f"{name}_U"] = np.asarray(U)
+        out[f"{name}_R2"] = np.asarray(op.residual(U))
+        R1, jvp = jax.linearize(jop.residual, U)
+        out[f"{name}_R1"] = np.asarray(R1)
+        v = np.where(atlas.interior, rng.standard_normal(U.shape), 0.0)
+        out[f"{name}_v"] = v
+        out[f"{name}_Jv"] = np.asarray(jvp(jnp.asarray(v)))
+        lam = op.wave_speeds(U)
+        for a in range(3):
+            out[f"{name}_lam{a}"] = np.asarray(lam[a])
+        if name == "split":
+            cfl = jnp.asarray(25.0)
+            prepare = pre.get_preconditioner("line_j")(atlas, flow.gamma, op.viscosity, op.model, op.distance)
+            r = np.where(atlas.interior, rng.standard_normal(U.shape), 0.0)
+            out[f"{name}_prec_r"] = r
+            out[f"{name}_prec_z"] = np.asarray(prepare(U, lam, cfl)(jnp.asarray(r)))
+            f = integrate_forces(U, atlas, flow, case.grid_spec.force_reference())
+            out[f"{name}_forces"] = np.array([f.cl, f.cd, f.cm, f.cd_friction])
+        print(f"{name}: {len(blocks)} blocks, {atlas.shape} canvas, {atlas.cells} cells")
+    np.savez_compressed(HERE / "blocks3d.npz", **out)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -1,0 +1,249 @@
+"""3D grid files with several blocks and with a pole, against the reference's own loader
+and solver (tests/golden/blocks3d.npz, made by tests/golden/make_golden_blocks3d.py):
+
+* the assembly (``jaxrans_b200.gridfile3d``) gives the reference's blocks and sides;
+* a case directory on such a file loads (``load_case``) to a 3D plan on the reference's
+  canvas;
+* the 3D kernels' bodies, run on the host by the test harness, give the reference's
+  residual, J.v, wave speeds, line preconditioner and forces across interfaces of every
+  orientation and across a pole;
+* ``solver3d.march3d`` drives blocks of Newton steps and the exit test over a device
+  stand-in built on the same harness."""
+
+from __future__ import annotations
+
+import ctypes as C
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from jaxrans_b200.case import CaseError, load_case
+from jaxrans_b200.grid3d import SIDES_3D, Cut3, write_plot3d
+from jaxrans_b200.gridfile import PatchRule
+from jaxrans_b200.gridfile3d import assemble3d, is_3d
+
+GOLDEN = Path(__file__).resolve().parent / "golden" / "blocks3d.npz"
+NAMES = ("split", "pole")
+
+
+@pytest.fixture(scope="module")
+def z():
+    return np.load(GOLDEN)
+
+
+def raw_blocks(z, name):
+    return [z[f"{name}_raw{b}"] for b in range(int(z[f"{name}_n_blocks"]))]
+
+
+def docs(z, name):
+    d = json.loads(str(z[f"{name}_case_json"]))
+    return d["case"], d["numerical"]
+
+
+def record(rect) -> list:
+    if isinstance(rect, Cut3):
+        return ["interface", list(rect.start), list(rect.stop), rect.block, rect.side, list(rect.origin),
+                list(rect.axes), [bool(f) for f in rect.flip], list(rect.period)]
+    return ["boundary", list(rect.start), list(rect.stop), rect.name]
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_assembly_matches_the_reference(z, name):
+    case_doc, _ = docs(z, name)
+    asm = assemble3d(raw_blocks(z, name), [PatchRule(**r) for r in case_doc["domain"]["patches"]])
+    assert asm.mismatch < 1e-12
+    for b, block in enumerate(asm.blocks):
+        assert np.array_equal(block.nodes, z[f"{name}_nodes{b}"])     # the left-handed block reversed
+        ref = json.loads(str(z[f"{name}_sides{b}"]))
+        for side in SIDES_3D:
+            mine = sorted(json.dumps(record(r)) for r in block.sides[side])
+            theirs = sorted(json.dumps(r[:4] if r[0] == "boundary" else r) for r in ref[side])
+            assert mine == theirs, (b, side)
+
+
+def test_assembly_errors():
+    theta = np.linspace(0.0, 2.0 * np.pi, 8)              # 7 cells round: a pole needs an even count
+    theta[-1] = 0.0
+    T, R, Zc = np.meshgrid(theta, [0.0, 1.0, 2.0], [0.0, 1.0, 2.0], indexing="ij")
+    odd = np.stack([R * np.cos(T), R * np.sin(T), Zc])
+    with pytest.raises(ValueError, match="collapsed"):
+        assemble3d([odd], [PatchRule("farfield")])
+    box = np.stack(np.meshgrid(*(np.arange(4.0),) * 3, indexing="ij"))
+    with pytest.raises(ValueError, match="no patch rule"):
+        assemble3d([box], [PatchRule("wall", x_max=0.5)])
+    mixed = box.copy()
+    mixed[0, 3] = 1.5                                     # folds the last layer of cells over
+    with pytest.raises(ValueError, match="non-positive"):
+        assemble3d([mixed], [PatchRule("farfield")])
+
+
+def case_dir(tmp_path: Path, z, name) -> Path:
+    case_doc, numerical = docs(z, name)
+    write_plot3d(tmp_path / "grid.x", raw_blocks(z, name))
+    (tmp_path / "case.json").write_text(json.dumps(case_doc))
+    (tmp_path / "numerical.json").write_text(json.dumps(numerical))
+    return tmp_path
+
+
+@pytest.fixture(scope="module")
+def cases(z, tmp_path_factory):
+    out = {}
+    for name in NAMES:
+        case = load_case(case_dir(tmp_path_factory.mktemp(name), z, name))
+        out[name] = (case, case.grid())
+    return out
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_case_loads_the_file_to_the_reference_canvas(z, cases, name):
+    case, plan = cases[name]
+    assert plan.dim == 3 and is_3d(case.directory / "grid.x")
+    assert plan.shape == z[f"{name}_interior"].shape
+    assert np.array_equal(plan.interior, z[f"{name}_interior"])
+    inside = plan.interior
+    assert np.allclose(plan.volume[inside], z[f"{name}_volume"][inside], rtol=1e-13, atol=0.0)
+    if f"{name}_distance" in z:
+        assert np.allclose(plan.distance[inside], z[f"{name}_distance"][inside], rtol=1e-10, atol=1e-14)
+
+
+def test_case_loader_refuses_what_the_3d_path_lacks(z, tmp_path):
+    d = case_dir(tmp_path, z, "pole")
+    doc = json.loads((d / "case.json").read_text())
+    doc["domain"].pop("reference_area")
+    (d / "case.json").write_text(json.dumps(doc))
+    with pytest.raises(CaseError, match="reference_area"):
+        load_case(d).grid()
+    doc["domain"]["reference_area"] = 1.0
+    doc["boundary_conditions"]["farfield"] = {"type": "outflow_static"}
+    (d / "case.json").write_text(json.dumps(doc))
+    with pytest.raises(CaseError, match="3D path"):
+        load_case(d).grid()
+
+
+def rows_rel(a, b, inside):
+    return max(float(np.abs(a[k][inside] - b[k][inside]).max() / max(np.abs(b[k][inside]).max(), 1e-300))
+               for k in range(a.shape[0]))
+
+
+@pytest.fixture(scope="module")
+def described(cases):
+    from jaxrans_b200.solver3d import describe_case
+    return {name: describe_case(case, plan) for name, (case, plan) in cases.items()}
+
+
+def host_eval(harness, desc, U, v=None, first_order=False):
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    R = np.zeros_like(U)
+    dU = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+    assert harness.jr3_host_eval(C.addressof(desc), U.ctypes.data, None if dU is None else dU.ctypes.data,
+                                 R.ctypes.data, int(first_order)) == 0
+    return R
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_kernel_bodies_give_the_reference_residual_and_jvp(harness, z, cases, described, name):
+    _, plan = cases[name]
+    desc, _ = described[name]
+    inside = plan.interior
+    U = z[f"{name}_U"]
+    assert rows_rel(host_eval(harness, desc, U), z[f"{name}_R2"], inside) < 1e-12
+    assert rows_rel(host_eval(harness, desc, U, first_order=True), z[f"{name}_R1"], inside) < 1e-12
+    Jv, ref = host_eval(harness, desc, U, z[f"{name}_v"]), z[f"{name}_Jv"]
+    assert rows_rel(Jv[:5], ref[:5], inside) < 1e-11
+    if Jv.shape[0] > 5:
+        assert rows_rel(Jv[5:], ref[5:], inside) < 1e-10
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_kernel_bodies_give_the_reference_wave_speeds(harness, z, cases, described, name):
+    _, plan = cases[name]
+    desc, _ = described[name]
+    U = np.ascontiguousarray(z[f"{name}_U"])
+    shapes = [tuple(n + (a == x) for x, n in enumerate(plan.shape)) for a in range(3)]
+    lam = np.zeros(sum(int(np.prod(s)) for s in shapes))
+    assert harness.jr3_host_wave_speeds(C.addressof(desc), U.ctypes.data, lam.ctypes.data) == 0
+    at = 0
+    for a, s in enumerate(shapes):
+        part = lam[at:at + int(np.prod(s))].reshape(s)
+        at += int(np.prod(s))
+        # faces of block cells (the rest of the canvas is never read)
+        ref = z[f"{name}_lam{a}"]
+        used = np.zeros(s, dtype=bool)
+        lo = [slice(None)] * 3
+        lo[a] = slice(0, s[a] - 1)
+        hi = [slice(None)] * 3
+        hi[a] = slice(1, s[a])
+        used[tuple(lo)] |= plan.interior
+        used[tuple(hi)] |= plan.interior
+        assert np.allclose(part[used], ref[used], rtol=1e-13, atol=0.0)
+
+
+def test_kernel_bodies_give_the_reference_line_solve_and_forces(harness, z, cases, described):
+    case, plan = cases["split"]
+    desc, _ = described["split"]
+    U = np.ascontiguousarray(z["split_U"])
+    r = np.ascontiguousarray(z["split_prec_r"])
+    out = np.zeros_like(r)
+    assert harness.jr3_host_precondition(C.addressof(desc), U.ctypes.data, 25.0, r.ctypes.data, out.ctypes.data) == 0
+    assert rows_rel(out, z["split_prec_z"], plan.interior) < 1e-10
+    spec = case.grid_spec
+    centre = np.ascontiguousarray(spec.moment_centre, dtype=np.float64)
+    f = np.zeros(4)
+    assert harness.jr3_host_forces(C.addressof(desc), U.ctypes.data, spec.reference_area, spec.reference_length,
+                                   centre.ctypes.data, f.ctypes.data) == 0
+    assert np.allclose(f, z["split_forces"], rtol=1e-11, atol=1e-16)
+
+
+class HostDevice3:
+    """The ``DevicePlan3`` methods ``march3d`` uses, over the host harness."""
+
+    def __init__(self, harness, case, desc):
+        cfg = case.implicit
+        self.lib, self.desc = harness, desc
+        self.config = np.array([cfg.krylov_tol, cfg.krylov_success,
+                                cfg.max_relative_update if cfg.max_relative_update is not None else -1.0,
+                                cfg.cfl_min, cfg.cfl_max, cfg.cfl_growth, cfg.cfl_cutback])
+        self.iconfig = np.array([cfg.krylov_subspace, cfg.krylov_restarts, 1], dtype=np.int32)
+        self.calls = 0
+
+    def newton_steps(self, U, n, cfl, res):
+        U = np.ascontiguousarray(U, dtype=np.float64).copy()
+        c, r = C.c_double(cfl), C.c_double(res)
+        hist = np.zeros(n)
+        assert self.lib.jr3_host_newton_steps(C.addressof(self.desc), self.config.ctypes.data,
+                                              self.iconfig.ctypes.data, U.ctypes.data, C.byref(c), C.byref(r), n,
+                                              hist.ctypes.data) == 0
+        self.calls += 1
+        return U, c.value, r.value, hist
+
+    def forces(self, U, area, length, centre):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        c = np.ascontiguousarray(centre, dtype=np.float64)
+        out = np.zeros(4)
+        assert self.lib.jr3_host_forces(C.addressof(self.desc), U.ctypes.data, area, length, c.ctypes.data,
+                                        out.ctypes.data) == 0
+        return out
+
+
+def test_march3d_runs_blocks_to_the_iteration_limit(harness, z, cases, described, tmp_path):
+    from dataclasses import replace
+    from jaxrans_b200.solver3d import freestream_state3, march3d
+    case, plan = cases["pole"]
+    case = replace(case, block_iters=2)
+    desc, _ = described["pole"]
+    dev = HostDevice3(harness, case, desc)
+    seen = []
+    result = march3d(case, plan, device=dev, max_iters=6, progress=lambda *a: seen.append(a[0]))
+    assert dev.calls == 3 and seen == [2, 4, 6]
+    assert result.history.reason == "max_iters" and result.history.n_iters == 6
+    assert np.all(np.isfinite(result.history.residual)) and result.cl_history.shape == (3,)
+    # the state the blocks left is the one six steps from the freestream give in one call
+    U, _, _, hist = HostDevice3(harness, case, desc).newton_steps(freestream_state3(case, plan), 6,
+                                                                  case.implicit.cfl, float("inf"))
+    assert np.array_equal(result.U, U) and np.array_equal(result.history.residual, hist)
+    out = result.write(tmp_path / "out")
+    fields = np.load(out / f"{case.name}_fields.npz")
+    assert fields["U_0"].shape == (5, 8, 4, 6) and "z_node_0" in fields
+    assert (out / f"{case.name}_block0.vts").read_bytes().startswith(b"<?xml")

@@ -75,14 +75,16 @@ def test_plot3d_formats_round_trip(tmp_path):
     assert np.array_equal(xx, x) and np.array_equal(yy, y)
 
 
-def test_a_3d_grid_file_is_refused_by_name(tmp_path):
+def test_a_tangled_3d_grid_file_is_a_case_error(tmp_path):
+    """A 3D file goes to the 3D assembly; cells of both volume signs are refused."""
     from jaxrans_b200.case import CaseError
     from jaxrans_b200.grid3d import write_plot3d
     nodes = np.random.default_rng(0).random((3, 4, 5, 6))
     write_plot3d(tmp_path / "w.x", [nodes])
-    doc = {"case": {"general": {"case_name": "w"}, "domain": {"grid": "file", "file": "w.x"},
+    doc = {"case": {"general": {"case_name": "w"},
+                    "domain": {"grid": "file", "file": "w.x", "reference_area": 1.0},
                     "freestream": {"mach": 0.5}},
            "numerical": {"time_integration": {"solver": "implicit"}}}
     case = parse_case(doc["case"], doc["numerical"], tmp_path)
-    with pytest.raises(CaseError, match="3D grid file"):
+    with pytest.raises(CaseError, match="non-positive volume"):
         case.grid()

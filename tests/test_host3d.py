@@ -1,5 +1,6 @@
 """The 3D kernels' per-cell and per-record bodies (csrc/residual3d.cuh) run on the host
-by a test-only harness (tests/host3d/harness.cu, built here with nvcc for the host), in
+by a test-only harness (tests/host3d/harness.cu, built with nvcc for the host by the
+``harness`` fixture of conftest.py), in
 the order the device runs them: the kernels' indexing and arithmetic checked against the
 3D oracle and the reference's outputs on the wing fixture, without a GPU."""
 
@@ -7,8 +8,6 @@ from __future__ import annotations
 
 import ctypes as C
 import json
-import shutil
-import subprocess
 from pathlib import Path
 
 import numpy as np
@@ -23,21 +22,6 @@ from jaxrans_b200.plan3d import build_plan3d
 ROOT = Path(__file__).resolve().parents[1]
 GOLDEN = ROOT / "tests" / "golden" / "ch_sa3d.npz"
 KINDS = {"wall": "no_slip_wall", "farfield": "far_field", "root": "symmetry", "tip": "symmetry"}
-
-
-@pytest.fixture(scope="module")
-def harness(tmp_path_factory):
-    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
-    if not Path(nvcc).exists():
-        pytest.skip("nvcc is not available")
-    out = tmp_path_factory.mktemp("host3d") / "libjr3host.so"
-    subprocess.run([nvcc, "-std=c++17", "-O2", "-Xcompiler", "-fPIC", "-shared",
-                    "-gencode", "arch=compute_100a,code=compute_100a", f"-I{ROOT / 'include'}",
-                    str(ROOT / "tests" / "host3d" / "harness.cu"), "-o", str(out)], check=True)
-    lib = C.CDLL(str(out))
-    lib.jr3_host_eval.restype = C.c_int
-    lib.jr3_host_eval.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
-    return lib
 
 
 @pytest.fixture(scope="module")
