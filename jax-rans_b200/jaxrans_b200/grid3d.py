@@ -26,7 +26,7 @@ from pathlib import Path
 import numpy as np
 
 from .geometry import Section
-from .grids import CONDITION_KINDS, WALL_KINDS, c_grid
+from .grids import CONDITION_KINDS, WALL_KINDS, c_grid, normal_steps
 
 SIDES_3D = ("j_min", "j_max", "i_min", "i_max", "k_min", "k_max")
 KINDS_3D = ("slip_wall", "no_slip_wall", "symmetry", "far_field")   # the 3D path's conditions
@@ -159,6 +159,93 @@ def wing_block(section: Section, cells_airfoil: int, cells_wake: int, cells_norm
     block = Block3(nodes, sides)
     block.check()
     return block
+
+
+@dataclass(frozen=True)
+class WingGrid:
+    """A multi-block wing grid as a grid file holds it: node arrays and the box patch
+    rules (``domain.patches`` entries) that name its boundary faces, and the wing's
+    reference area (semispan planform), length (mean aerodynamic chord) and centre."""
+
+    blocks: list
+    patches: list
+    reference_area: float
+    reference_length: float
+    moment_centre: tuple
+
+
+def wing_ch_blocks(section: Section, cells_airfoil: int, cells_wake: int, cells_normal: int, cells_span: int,
+                   cells_tip: int, wall_spacing: float, far_field: float, semispan: float, taper: float = 1.0,
+                   sweep_deg: float = 0.0, cap_cells: int = 4, span_far: float | None = None) -> WingGrid:
+    """The four point-matched blocks of a C-H grid round a straight-tapered, swept wing
+    with its tip, from the root section (chord 1):
+
+    * spanwise, the wing (root symmetry plane ``y = 0`` to the tip ``y = semispan``,
+      ``cells_span`` stations closing in on the tip) and the region beyond the tip out
+      to the far field ``y = semispan + span_far`` (``cells_tip`` stations, default
+      ``span_far`` = ``far_field`` root chords);
+    * round the section, the lower half (lower wake and lower surface up to the
+      leading edge) and the upper half, ``(cells_airfoil / 2 + cells_wake)`` cells each.
+
+    Each spanwise station is the root's 2D C-grid scaled by the local chord about the
+    leading edge and moved aft by the sweep (beyond the tip, the tip's).  Past the tip
+    the section closes over ``cap_cells`` stations (an elliptic tip cap: its thickness
+    times ``sqrt(1 - (m / cap_cells)^2)``) and then continues as a sheet of zero thickness
+    on the chord line, whose two sides face each other like the wake cut -- for a
+    symmetric section, whose C-grid's lower and upper surfaces are mirror images.
+    ``k`` runs from the spanwise far field to the root, which makes every block
+    right-handed.  Patches by box rules: ``symmetry`` (the root plane), ``wall`` (the
+    wing and its cap), ``farfield``."""
+    if cells_airfoil % 2:
+        raise ValueError(f"cells round the airfoil must be even, got {cells_airfoil}")
+    if not 0 < cap_cells < cells_tip:
+        raise ValueError(f"cap_cells must lie in (0, cells_tip), got {cap_cells} of {cells_tip}")
+    base = c_grid(section, cells_airfoil, cells_wake, cells_normal, wall_spacing, far_field)
+    x2, z2 = base.x, base.y
+    ni, nw = base.ni, cells_wake
+    if np.abs(z2[:, 0] + z2[::-1, 0]).max() > 1e-9 or np.abs(x2[:, 0] - x2[::-1, 0]).max() > 1e-9:
+        raise ValueError("the tip region's sheet needs a symmetric section (mirror-image lower and upper surfaces)")
+    # the chord-line section: the surface moved onto z = 0, the move fading out over half a chord
+    reach = np.concatenate([np.zeros((ni + 1, 1)), np.cumsum(np.hypot(np.diff(x2, axis=1), np.diff(z2, axis=1)),
+                                                             axis=1)], axis=1)
+    fade = (1.0 - np.minimum(reach / 0.5, 1.0)) ** 2
+    lift = np.zeros(ni + 1)
+    lift[nw:ni - nw + 1] = z2[nw:ni - nw + 1, 0]
+    move = lift[:, None] * fade                               # z of the sheet = z2 - move
+    tip_chord = 1.0 - (1.0 - taper)
+    half_thickness = 0.5 * float(np.ptp(z2[:, 0])) * tip_chord
+    step = half_thickness / cap_cells                         # spanwise spacing at the tip and in the cap
+    far = far_field if span_far is None else span_far
+    y_wing = semispan - np.concatenate([[0.0], np.cumsum(normal_steps(cells_span, step, semispan))])[::-1]
+    beyond = np.concatenate([np.full(cap_cells, step), normal_steps(cells_tip - cap_cells, step,
+                                                                    far - cap_cells * step)])
+    y_tip = semispan + np.concatenate([[0.0], np.cumsum(beyond)])
+    shift = math.tan(math.radians(sweep_deg))
+
+    def stations(y, thickness):
+        chord = 1.0 - (1.0 - taper) * np.minimum(y, semispan) / semispan
+        dx = np.minimum(y, semispan) * shift
+        nodes = np.empty((3,) + x2.shape + (len(y),))
+        z = z2[..., None] - (1.0 - thickness) * move[..., None]
+        nodes[0] = x2[..., None] * chord + dx
+        nodes[1] = np.broadcast_to(y, x2.shape + (len(y),))
+        nodes[2] = z * chord
+        return nodes[..., ::-1]                               # k from the far side toward the root
+
+    m = np.arange(cells_tip + 1)
+    cap = np.sqrt(np.clip(1.0 - (m / cap_cells) ** 2, 0.0, None))
+    wing = stations(y_wing, np.ones(cells_span + 1))
+    tip = stations(y_tip, cap)
+    lo, hi = slice(0, ni // 2 + 1), slice(ni // 2, ni + 1)
+    blocks = [np.ascontiguousarray(b[:, s]) for b in (wing, tip) for s in (lo, hi)]
+    reach_x = float(x2[nw:ni - nw + 1, 0].max()) + semispan * shift + 1.0
+    patches = [{"name": "symmetry", "y_max": 1e-9 * semispan},
+               {"name": "wall", "x_min": -1.0, "x_max": reach_x, "y_max": semispan + (cap_cells + 0.5) * step,
+                "z_min": -1.0, "z_max": 1.0},
+               {"name": "farfield"}]
+    area = 0.5 * semispan * (1.0 + taper)
+    mac = (2.0 / 3.0) * (1.0 + taper + taper * taper) / (1.0 + taper)
+    return WingGrid(blocks, patches, area, mac, (0.25, 0.0, 0.0))
 
 
 # --- Plot3D ------------------------------------------------------------------------------

@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """Generate the multi-block and pole 3D fixtures by running the reference solver itself.
 
-Two grids, written as unformatted Plot3D files and read by the reference through its own
+Three grids, written as unformatted Plot3D files and read by the reference through its own
 3D loader (``grid: file``, box patch rules), under the NumPy stand-in in
 ``tests/golden/jaxshim`` (as ``make_golden3d.py`` does):
 
@@ -9,12 +9,15 @@ Two grids, written as unformatted Plot3D files and read by the reference through
   two ``i`` stations into three blocks; the second stored with ``i`` and ``k`` reversed,
   the third with ``i`` and ``k`` swapped (left-handed as stored, so the loader reverses
   it).  The wake cut becomes an interface between the first and third blocks; SA RANS.
+* ``wing4``: the four-block C-H grid of the swept, tapered wing with its tip region
+  (``jaxrans_b200.grid3d.wing_ch_blocks``: wing and beyond-tip blocks, lower and upper
+  halves; past the tip an elliptic cap, then a sheet facing itself), coarse; SA RANS.
 * ``pole``: a cylinder of cells round the z axis -- ``i`` the azimuth (an O seam), ``j``
   the radius from the axis (``j_min`` collapsed to a line: a pole), ``k`` along the
   axis -- with far field all round; inviscid.
 
-For each: the assembled sides, the canvas, the reference's residual, first-order J.v,
-and for ``split`` the wave speeds, the line preconditioner and the forces.
+For each: the assembled sides, the canvas, the reference's residual, first-order J.v and
+wave speeds, and for the wings the line preconditioner and the forces.
 
     python tests/golden/make_golden_blocks3d.py
 
@@ -47,7 +50,7 @@ from jaxrans.post.forces import integrate_forces  # noqa: E402
 from jaxrans.solvers import preconditioners as pre  # noqa: E402
 
 from jaxrans_b200.geometry import section_source  # noqa: E402
-from jaxrans_b200.grid3d import wing_block, write_plot3d  # noqa: E402
+from jaxrans_b200.grid3d import wing_block, wing_ch_blocks, write_plot3d  # noqa: E402
 
 sys.path.insert(0, str(HERE))
 from make_golden3d import CASE, NUMERICAL, WING, perturbed, sides_record  # noqa: E402
@@ -85,7 +88,29 @@ def split_case() -> dict:
     return doc
 
 
-GRIDS = {"split": (split_blocks, split_case(), NUMERICAL), "pole": (pole_blocks, POLE_CASE, POLE_NUMERICAL)}
+WING4 = {"section": "naca0012", "cells_airfoil": 24, "cells_wake": 6, "cells_normal": 10, "cells_span": 6,
+         "cells_tip": 6, "wall_spacing": 1e-3, "far_field": 20.0, "semispan": 1.6, "taper": 0.6, "sweep_deg": 25.0,
+         "cap_cells": 2, "span_far": 3.0}
+
+
+def wing4_grid():
+    w = dict(WING4)
+    return wing_ch_blocks(section_source(w.pop("section")), **w)
+
+
+def wing4_case() -> dict:
+    g = wing4_grid()
+    doc = json.loads(json.dumps(CASE))
+    doc["general"]["case_name"] = "wing4"
+    doc["domain"] = {"grid": "file", "file": "grid.x", "patches": g.patches, "reference_area": g.reference_area,
+                     "reference_length": g.reference_length, "moment_centre": list(g.moment_centre)}
+    doc["boundary_conditions"] = {"wall": {"type": "no_slip_wall"}, "farfield": {"type": "far_field"},
+                                  "symmetry": {"type": "symmetry"}}
+    return doc
+
+
+GRIDS = {"split": (split_blocks, split_case(), NUMERICAL), "pole": (pole_blocks, POLE_CASE, POLE_NUMERICAL),
+         "wing4": (lambda: wing4_grid().blocks, wing4_case(), NUMERICAL)}
 
 
 def main() -> int:
@@ -124,7 +149,7 @@ def main() -> int:
         lam = op.wave_speeds(U)
         for a in range(3):
             out[f"{name}_lam{a}"] = np.asarray(lam[a])
-        if name == "split":
+        if name in ("split", "wing4"):
             cfl = jnp.asarray(25.0)
             prepare = pre.get_preconditioner("line_j")(atlas, flow.gamma, op.viscosity, op.model, op.distance)
             r = np.where(atlas.interior, rng.standard_normal(U.shape), 0.0)

@@ -20,12 +20,12 @@ import numpy as np
 import pytest
 
 from jaxrans_b200.case import CaseError, load_case
-from jaxrans_b200.grid3d import SIDES_3D, Cut3, write_plot3d
+from jaxrans_b200.grid3d import SIDES_3D, Cut3, Rect3, write_plot3d
 from jaxrans_b200.gridfile import PatchRule
 from jaxrans_b200.gridfile3d import assemble3d, is_3d
 
 GOLDEN = Path(__file__).resolve().parent / "golden" / "blocks3d.npz"
-NAMES = ("split", "pole")
+NAMES = ("split", "wing4", "pole")
 
 
 @pytest.fixture(scope="module")
@@ -42,11 +42,21 @@ def docs(z, name):
     return d["case"], d["numerical"]
 
 
-def record(rect) -> list:
-    if isinstance(rect, Cut3):
-        return ["interface", list(rect.start), list(rect.stop), rect.block, rect.side, list(rect.origin),
-                list(rect.axes), [bool(f) for f in rect.flip], list(rect.period)]
-    return ["boundary", list(rect.start), list(rect.stop), rect.name]
+def face_labels(rects, extent) -> dict:
+    """Per face of a side: its patch name, or the partner block, side and running position
+    (independent of how the side is cut into rectangles)."""
+    out = {}
+    for r in rects:
+        for a in ((x, y) for x in range(r.start[0], r.stop[0]) for y in range(r.start[1], r.stop[1])):
+            out[a] = r.name if isinstance(r, Rect3) else (r.block, r.side, r.partner(a))
+    assert len(out) == extent[0] * extent[1]
+    return out
+
+
+def from_record(r):
+    if r[0] == "boundary":
+        return Rect3(r[3], tuple(r[1]), tuple(r[2]))
+    return Cut3(tuple(r[1]), tuple(r[2]), r[3], r[4], tuple(r[5]), tuple(r[6]), tuple(r[7]), tuple(r[8]))
 
 
 @pytest.mark.parametrize("name", NAMES)
@@ -58,9 +68,27 @@ def test_assembly_matches_the_reference(z, name):
         assert np.array_equal(block.nodes, z[f"{name}_nodes{b}"])     # the left-handed block reversed
         ref = json.loads(str(z[f"{name}_sides{b}"]))
         for side in SIDES_3D:
-            mine = sorted(json.dumps(record(r)) for r in block.sides[side])
-            theirs = sorted(json.dumps(r[:4] if r[0] == "boundary" else r) for r in ref[side])
-            assert mine == theirs, (b, side)
+            n = block.extent(side)
+            assert face_labels(block.sides[side], n) == face_labels([from_record(r) for r in ref[side]], n), \
+                (b, side)
+
+
+def test_the_four_block_wing_generator(z):
+    """``wing_ch_blocks`` reproduces the fixture's blocks; its tip region closes the wing:
+    past the cap the sheet's two sides face each other, so the wall is the wing and the
+    cap only."""
+    from jaxrans_b200.geometry import section_source
+    from jaxrans_b200.grid3d import wing_ch_blocks
+    w = json.loads(str(z["wing4_case_json"]))["case"]["domain"]
+    g = wing_ch_blocks(section_source("naca0012"), 24, 6, 10, 6, 6, 1e-3, 20.0, 1.6, 0.6, 25.0, cap_cells=2,
+                       span_far=3.0)
+    assert g.patches == w["patches"] and np.isclose(g.reference_area, w["reference_area"])
+    for b, nodes in enumerate(g.blocks):
+        assert np.array_equal(nodes, z[f"wing4_raw{b}"])
+    asm = assemble3d(g.blocks, [PatchRule(**r) for r in g.patches])
+    assert asm.patches["wall"] == 2 * 12 * 6 + 2 * 12 * 2      # both halves of the wing, then of the cap
+    with pytest.raises(ValueError, match="symmetric section"):
+        wing_ch_blocks(section_source("naca4412"), 64, 16, 24, 6, 6, 1e-3, 20.0, 1.6, span_far=3.0)
 
 
 def test_assembly_errors():
@@ -180,20 +208,21 @@ def test_kernel_bodies_give_the_reference_wave_speeds(harness, z, cases, describ
         assert np.allclose(part[used], ref[used], rtol=1e-13, atol=0.0)
 
 
-def test_kernel_bodies_give_the_reference_line_solve_and_forces(harness, z, cases, described):
-    case, plan = cases["split"]
-    desc, _ = described["split"]
-    U = np.ascontiguousarray(z["split_U"])
-    r = np.ascontiguousarray(z["split_prec_r"])
+@pytest.mark.parametrize("name", ["split", "wing4"])
+def test_kernel_bodies_give_the_reference_line_solve_and_forces(harness, z, cases, described, name):
+    case, plan = cases[name]
+    desc, _ = described[name]
+    U = np.ascontiguousarray(z[f"{name}_U"])
+    r = np.ascontiguousarray(z[f"{name}_prec_r"])
     out = np.zeros_like(r)
     assert harness.jr3_host_precondition(C.addressof(desc), U.ctypes.data, 25.0, r.ctypes.data, out.ctypes.data) == 0
-    assert rows_rel(out, z["split_prec_z"], plan.interior) < 1e-10
+    assert rows_rel(out, z[f"{name}_prec_z"], plan.interior) < 1e-10
     spec = case.grid_spec
     centre = np.ascontiguousarray(spec.moment_centre, dtype=np.float64)
     f = np.zeros(4)
     assert harness.jr3_host_forces(C.addressof(desc), U.ctypes.data, spec.reference_area, spec.reference_length,
                                    centre.ctypes.data, f.ctypes.data) == 0
-    assert np.allclose(f, z["split_forces"], rtol=1e-11, atol=1e-16)
+    assert np.allclose(f, z[f"{name}_forces"], rtol=1e-11, atol=1e-16)
 
 
 class HostDevice3:
