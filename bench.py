@@ -15,6 +15,10 @@ independent: no collective on the data path) and the whole-job rate is reported.
 ``--impl reference`` times the CPU restatement of the reference (``oracle``; the
 reference itself is JAX, absent here) on a bounded sample of the same workload: each
 step one Newton step, extrapolated by the number of Newton steps a converged solve takes.
+
+``--workload wing_ch_4blk`` (or ``wing_ch_4blk_small``) prints a separate line: 3D
+pseudo-transient Newton steps per second of the swept, tapered wing on its four-block
+C-H grid (3.93M cells), the state resident on the device.
 """
 
 from __future__ import annotations
@@ -163,6 +167,147 @@ def run_reference(args) -> int:
             "cpu_baseline": {"value": value, "unit": "solves/hr", "cores": 1, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "solves/hr", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+    return 0
+
+
+# --- the 3D wing (a separate line: Newton steps per second of one 3D case) ------------
+
+WING3D_WORKLOADS = ("wing_ch_4blk", "wing_ch_4blk_small")
+METRIC3D = "3D pseudo-transient Newton steps/s"
+
+
+def wing3d_setup(name: str):
+    """The 3D workload's case (grid file written to a scratch directory) and plan; on a
+    CUDA device the plan's wall distance is computed there."""
+    import tempfile
+    from jaxrans_b200.workloads import wing3d_case
+    with tempfile.TemporaryDirectory() as d:
+        case = wing3d_case(name, d)
+        plan = case.grid()
+    return case, plan
+
+
+def oracle3d_step_seconds(steps: int, warmup: int):
+    """Seconds per Newton step of the 3D oracle (NumPy FP64) on the small wing, from the
+    freestream, and that case's cell count: the CPU rate per cell of a bounded sample."""
+    from oracle import implicit3d as i3
+    from oracle import numerics3d as n3
+    from oracle.implicit import NewtonState
+    from jaxrans_b200.solver3d import freestream_state3, physics3
+    case, plan = wing3d_setup("wing_ch_4blk_small")
+    ph = physics3(case)
+    model = n3.Model3(plan, ph["q_inf"], ph["gamma"], ph["flux"], ph["limiter"], ph["kappa"], ph["mu_inf"],
+                      ph["sutherland"], len(ph["q_inf"]) == 6, plan.distance)
+    state = NewtonState(freestream_state3(case, plan), case.implicit.cfl, math.inf)
+    times = []
+    for k in range(warmup + steps):
+        t0 = time.perf_counter()
+        state, _ = i3.newton_step(state, model, case.implicit)
+        if k >= warmup:
+            times.append(time.perf_counter() - t0)
+    return statistics.mean(times), plan.cells
+
+
+def run_wing3d(args) -> int:
+    """``--workload wing_ch_4blk``: K pseudo-transient Newton steps of the 3D wing
+    (``jr_newton_steps3d``, GMRES with the line preconditioner, host-driven: the step
+    synchronises for its scalars, so it is timed by the host clock between device
+    synchronisations) with the state resident; ``e2e`` the same steps through
+    ``DevicePlan3.newton_steps`` from and back to a host state."""
+    rank, local, world = rank_info()
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        per_step, cells = oracle3d_step_seconds(max(1, min(args.steps, 2)), 1)
+        _, plan = wing3d_setup(args.workload)
+        value = cells / (per_step * plan.cells)
+        sample = (f"Newton steps of the 3D oracle (NumPy FP64, complex-step J.v) on the wing_ch_4blk_small grid "
+                  f"({cells} cells), {per_step:.1f} s each, scaled by cells to the {plan.cells}-cell workload")
+        print(json.dumps({"impl": "reference", "metric": METRIC3D, "value": value, "unit": "steps/s",
+                          "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic (generated wing and grid)",
+                          "config": {"workload": args.workload, "cells": plan.cells},
+                          "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "port",
+                                           "sample": sample},
+                          "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return 0
+    import ctypes as C
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from jaxrans_b200.build import build
+    from jaxrans_b200.solver3d import device3_for, freestream_state3
+    build()
+    case, plan = wing3d_setup(args.workload)
+    dev = device3_for(case, plan)
+    U0 = freestream_state3(case, plan)
+    U_dev = torch.from_numpy(U0).to("cuda")
+    cfl, res, hist = C.c_double(case.implicit.cfl), C.c_double(math.inf), np.zeros(1)
+
+    def device_step():
+        rc = dev.lib.jr_newton_steps3d(dev.handle, U_dev.data_ptr(), 1, C.byref(cfl), C.byref(res), hist.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(f"jr_newton_steps3d failed ({rc}): {dev.lib.jr_last_error().decode()}")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        device_step()
+    launches = C.c_int64()
+    dev.lib.jr_launches3d(C.byref(launches))
+    before = launches.value
+    barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clocks:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            device_step()
+        torch.cuda.synchronize()
+        seconds = time.perf_counter() - t0
+    dev.lib.jr_launches3d(C.byref(launches))
+    launched = launches.value - before
+    U_host, c2, r2 = U0.copy(), case.implicit.cfl, math.inf
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        U_host, c2, r2, _ = dev.newton_steps(U_host, 1, c2, r2)
+    torch.cuda.synchronize()
+    e2e_seconds = time.perf_counter() - t0
+    seconds, e2e_seconds = max_over_ranks([seconds, e2e_seconds], dist, "cuda")
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            per_step, cells = oracle3d_step_seconds(1, 1)
+            cpu = {"value": cells / (per_step * plan.cells), "unit": "steps/s", "cores": 1, "kind": "port",
+                   "sample": f"one Newton step of the 3D oracle on the wing_ch_4blk_small grid ({cells} cells), "
+                             f"{per_step:.1f} s, scaled by cells"}
+        value = world * args.steps / seconds
+        bytes_per_step = int(U0.nbytes)
+        print(json.dumps({
+            "metric": METRIC3D, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * seconds / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (generated wing and grid)",
+            "config": {"workload": args.workload, "cells": plan.cells, "canvas": list(plan.shape),
+                       "blocks": len(plan.mesh), "nvar": int(U0.shape[0]),
+                       "krylov_subspace": case.implicit.krylov_subspace,
+                       "l2": "inputs larger than L2" if U0.nbytes > 126e6 else "inputs smaller than L2, no flush",
+                       "timer": "host clock between device synchronisations (the 3D step is host-driven)"},
+            "e2e": {"value": world * args.steps / e2e_seconds, "unit": "steps/s",
+                    "h2d_bytes_per_step": bytes_per_step, "d2h_bytes_per_step": bytes_per_step},
+            "gpu_launches": launched, "roofline": None, "cpu_baseline": cpu, "clocks": clocks.summary()}),
+            flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    dev.close()
     return 0
 
 
@@ -368,7 +513,8 @@ def main(argv=None) -> int:
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=("b200", "reference"))
-    p.add_argument("--workload", default="c_sa_385", choices=sorted(STEPS_PER_SOLVE) + ["polar64_uneven"])
+    p.add_argument("--workload", default="c_sa_385",
+                   choices=sorted(STEPS_PER_SOLVE) + ["polar64_uneven"] + list(WING3D_WORKLOADS))
     p.add_argument("--precision", default="fp64", choices=("fp64", "mixed"))
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--line-schedule", default=None, metavar="F,A,S",
@@ -377,6 +523,8 @@ def main(argv=None) -> int:
     args = p.parse_args(argv)
     if args.warmup < 3:
         raise SystemExit("--warmup must be at least 3")
+    if args.workload in WING3D_WORKLOADS:
+        return run_wing3d(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_device(args)

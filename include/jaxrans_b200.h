@@ -320,6 +320,15 @@ int jr_newton_steps3d(jr_plan3d* plan, double* U, int32_t n_steps, double* cfl, 
  * friction from the laminar viscous flux at the wall.  Replaces force_coefficients
  * (src/jaxrans/post/forces.py:108-161) on a 3D atlas.  Synchronises. */
 int jr_forces3d(jr_plan3d* plan, const double* U, double area, double length, const double* centre, double* out);
+/* The wall distance of points (device, n_points x 3) to the nearest of n_faces wall faces
+ * (device, n_faces x 4 x 3: the corners round each face, taken as a bilinear patch):
+ * out (device, n_points).  Faces ranked by the distance to their two triangles, then the
+ * exact patch distance over the 16 nearest (src/jaxrans/mesh/wall3d.py:131-158,
+ * wall_distance_3d); infinite with no faces.  For the SA model's plan; synchronises. */
+int jr_wall_distance3d(const double* points, int64_t n_points, const double* faces, int32_t n_faces, double* out);
+/* Kernels the 3D plan entry points (residual, J.v, wave speeds, line solve, Newton steps,
+ * forces) have launched since the library was loaded (counted on the host). */
+int jr_launches3d(int64_t* out);
 
 #ifdef __cplusplus
 }

@@ -14,6 +14,11 @@ int report_error(int code, const std::string& msg);
 
 using namespace jr;
 
+long long& jr::launches3() {
+  static long long n = 0;
+  return n;
+}
+
 struct jr_plan3d {
   Plan3Dev dev{};
   std::vector<void*> allocs;
@@ -284,6 +289,32 @@ int jr_forces3d(jr_plan3d* plan, const double* U, double area, double length, co
   if (rc) return rc;
   force_coefficients3(plan->dev.P, nw, loads.data(), plan->wall_mid.data(), area, length, centre, out);
   return JR_OK;
+}
+
+int jr_launches3d(int64_t* out) {
+  if (!out) return report_error(JR_EINVAL, "null argument");
+  *out = launches3();
+  return JR_OK;
+}
+
+int jr_wall_distance3d(const double* points, int64_t n_points, const double* faces, int32_t n_faces, double* out) {
+  if (n_points < 0 || n_faces < 0) return report_error(JR_EINVAL, "negative size");
+  if ((n_points > 0 && (!points || !out)) || (n_faces > 0 && !faces)) return report_error(JR_EINVAL, "null argument");
+  if (n_points == 0) return JR_OK;
+  double* spheres = nullptr;
+  if (n_faces > 0 && cudaMalloc(&spheres, (size_t)n_faces * 4 * sizeof(double)) != cudaSuccess)
+    return report_error(JR_ENOMEM, "cudaMalloc failed");
+  cudaStream_t st;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaFree(spheres);
+    return check3("jr_wall_distance3d");
+  }
+  launch_wall_distance3(points, n_points, faces, n_faces, spheres, out, st);
+  int rc = check3("jr_wall_distance3d");
+  if (cudaStreamSynchronize(st) != cudaSuccess && rc == JR_OK) rc = check3("jr_wall_distance3d");
+  cudaStreamDestroy(st);
+  cudaFree(spheres);
+  return rc;
 }
 
 }  // extern "C"

@@ -233,5 +233,12 @@ void launch_wave_speeds3(const Plan3Dev& p, const double* U, double* lam, cudaSt
 void launch_wall_loads3(const Plan3Dev& p, const double* U, double* loads, void* A, void* B, cudaStream_t st);
 void launch_precondition3(const Plan3Dev& p, const double* U, double cfl, const double* r, double* z, double* scratch,
                           cudaStream_t st);
+// Kernels the 3D path has launched since the library was loaded (counted on the host at
+// each launch site; the benchmark's launch figure).
+long long& launches3();
+inline void counted3(int n = 1) { launches3() += n; }
+
+void launch_wall_distance3(const double* points, long long n_points, const double* quads, int n_faces, double* spheres,
+                           double* out, cudaStream_t st);
 
 }  // namespace jr

@@ -32,6 +32,7 @@ __global__ void __launch_bounds__(64) k3_chain_solve(Plan3Dev p, const double* _
 
 void launch_wave_speeds3(const Plan3Dev& p, const double* U, double* lam, cudaStream_t st) {
   const int total = face_count(p, 0) + face_count(p, 1) + face_count(p, 2);
+  counted3();
   k3_wave_speeds<<<(total + 127) / 128, 128, 0, st>>>(p, U, lam);
 }
 
@@ -39,6 +40,7 @@ void launch_wave_speeds3(const Plan3Dev& p, const double* U, double* lam, cudaSt
 void launch_precondition3(const Plan3Dev& p, const double* U, double cfl, const double* r, double* z, double* scratch,
                           cudaStream_t st) {
   const int n = p.nvar * p.NI * p.NJ * p.NK;
+  counted3(p.n_chains > 0 ? 2 : 1);
   k3_copy_rows<<<(n + 255) / 256, 256, 0, st>>>(n, r, z);
   if (p.n_chains > 0) k3_chain_solve<<<(p.n_chains + 63) / 64, 64, 0, st>>>(p, U, cfl, r, z, scratch);
 }

@@ -140,6 +140,7 @@ double DeviceOps3::host_sum(int count, int halves) {
 }
 
 void DeviceOps3::prepare(const double* U, double cfl) {
+  counted3();
   k3_vdt<<<grid_of(n), 128, 0, st>>>(p, U, cfl, vdt);
 }
 
@@ -147,6 +148,7 @@ void DeviceOps3::residual(const double* U, int out) { launch_residual3(p, U, v(o
 
 void DeviceOps3::matvec(const double* U, double, int src, int out) {
   launch_jvp3(p, U, v(src), v(out), A, B, st);
+  counted3();
   k3_vdt_add<<<grid_of(N), 256, 0, st>>>(N, n, vdt, v(src), v(out));
 }
 
@@ -155,22 +157,31 @@ void DeviceOps3::precondition(const double* U, double cfl, int src, int dst) {
 }
 
 double DeviceOps3::dot(int a, int b) {
+  counted3();
   k3_dot_partial<<<RED3_BLOCKS, RED3_THREADS, 0, st>>>(N, v(a), v(b), partial);
   return host_sum(RED3_BLOCKS, 1);
 }
 
-void DeviceOps3::axpy(double al, int x, int y) { k3_axpy<<<grid_of(N), 256, 0, st>>>(N, al, v(x), v(y)); }
-void DeviceOps3::scale(double al, int x, int y) { k3_scale<<<grid_of(N), 256, 0, st>>>(N, al, v(x), v(y)); }
+void DeviceOps3::axpy(double al, int x, int y) {
+  counted3();
+  k3_axpy<<<grid_of(N), 256, 0, st>>>(N, al, v(x), v(y));
+}
+void DeviceOps3::scale(double al, int x, int y) {
+  counted3();
+  k3_scale<<<grid_of(N), 256, 0, st>>>(N, al, v(x), v(y));
+}
 void DeviceOps3::copy(int x, int y) { cudaMemcpyAsync(v(y), v(x), N * sizeof(double), cudaMemcpyDeviceToDevice, st); }
 void DeviceOps3::zero(int y) { cudaMemsetAsync(v(y), 0, N * sizeof(double), st); }
 
 double DeviceOps3::density_norm(int r) {
+  counted3();
   k3_norm_partial<<<RED3_BLOCKS, RED3_THREADS, 0, st>>>(p, v(r), partial);
   const double a = host_sum(RED3_BLOCKS, 2);
   return sqrt(a / last_second);
 }
 
 double DeviceOps3::worst_ratio(const double* U, int du) {
+  counted3();
   k3_worst_partial<<<RED3_BLOCKS, RED3_THREADS, 0, st>>>(p, U, v(du), partial);
   std::vector<double> h(RED3_BLOCKS);
   cudaMemcpyAsync(h.data(), partial, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st);
@@ -182,6 +193,7 @@ double DeviceOps3::worst_ratio(const double* U, int du) {
 
 bool DeviceOps3::physical_after(const double* U, int du) {
   cudaMemsetAsync(flag, 0, sizeof(int), st);
+  counted3();
   k3_physical<<<grid_of(n), 128, 0, st>>>(p, U, v(du), flag);
   int h = 0;
   cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -189,7 +201,10 @@ bool DeviceOps3::physical_after(const double* U, int du) {
   return h == 0;
 }
 
-void DeviceOps3::add_to_state(double* U, int du) { k3_axpy<<<grid_of(N), 256, 0, st>>>(N, 1.0, v(du), U); }
+void DeviceOps3::add_to_state(double* U, int du) {
+  counted3();
+  k3_axpy<<<grid_of(N), 256, 0, st>>>(N, 1.0, v(du), U);
+}
 
 size_t DeviceOps3::work_doubles(size_t N, size_t n, int m) {
   return (size_t)(BASE + m + 1) * N + n + 2 * RED3_BLOCKS;

@@ -48,7 +48,10 @@ static void fill3(const Plan3Dev& p, T* A, T* B, cudaStream_t st) {
     cudaMemcpyAsync(nxt, cur, bytes, cudaMemcpyDeviceToDevice, st);
     const int r0 = p.stage_off[s], r1 = p.stage_off[s + 1];
     const int blocks = (r1 - r0 + 127) / 128;
-    if (blocks > 0) k3_ghost_stage<T><<<blocks, 128, 0, st>>>(p, cur, nxt, r0, r1);
+    if (blocks > 0) {
+      counted3();
+      k3_ghost_stage<T><<<blocks, 128, 0, st>>>(p, cur, nxt, r0, r1);
+    }
     T* t = cur;
     cur = nxt;
     nxt = t;
@@ -61,6 +64,7 @@ static void residual3_t(const Plan3Dev& p, const double* U, const double* dU, do
                         cudaStream_t st) {
   const int n = p.NI * p.NJ * p.NK;
   const int blocks = (n + 127) / 128;
+  counted3(2);   // the primitive canvas and, below, the residual
   k3_prim<T><<<blocks, 128, 0, st>>>(p, U, dU, A);
   fill3(p, A, B, st);
   const bool visc = p.P.mu_inf > 0.0, sa = p.nvar > 5;
@@ -80,6 +84,7 @@ __global__ void k3_wall_loads(Plan3Dev p, const double* __restrict__ Q, double* 
 // the loads on every wall face (7 each) at U: the primitive canvas ghost-filled first
 void launch_wall_loads3(const Plan3Dev& p, const double* U, double* loads, void* A, void* B, cudaStream_t st) {
   const int n = p.NI * p.NJ * p.NK;
+  counted3(p.n_walls > 0 ? 2 : 1);
   k3_prim<double><<<(n + 127) / 128, 128, 0, st>>>(p, U, nullptr, (double*)A);
   fill3(p, (double*)A, (double*)B, st);
   if (p.n_walls > 0) k3_wall_loads<<<(p.n_walls + 127) / 128, 128, 0, st>>>(p, (const double*)A, loads);

@@ -15,7 +15,7 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 CSRC = PKG.parent / "csrc"
 INCLUDE = PKG.parents[1] / "include"
-SOURCES = ("residual.cu", "linesolve.cu", "krylov.cu", "forces.cu", "capi.cu", "residual3d.cu", "linesolve3d.cu", "newton3d.cu", "capi3d.cu")
+SOURCES = ("residual.cu", "linesolve.cu", "krylov.cu", "forces.cu", "capi.cu", "residual3d.cu", "linesolve3d.cu", "newton3d.cu", "walldist3d.cu", "capi3d.cu")
 LIB = PKG / "lib" / "libjaxrans_b200.so"
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
 

@@ -243,3 +243,18 @@ class DevicePlan3:
         _check(self.lib, self.lib.jr_precondition3d(self.handle, u.data_ptr(), float(cfl), rr.data_ptr(),
                                                      out.data_ptr()), "jr_precondition3d")
         return out.cpu().numpy()
+
+
+def wall_distance_device(points: np.ndarray, faces: np.ndarray, library=None) -> np.ndarray:
+    """The distance of every point ``(..., 3)`` to the nearest wall face ``(m, 4, 3)`` on
+    the device (``jr_wall_distance3d``)."""
+    import torch
+    if not torch.cuda.is_available():
+        raise NativeError("the device wall distance runs on a CUDA device")
+    lib = load_library(library)
+    pts = torch.as_tensor(np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3), device="cuda")
+    q = torch.as_tensor(np.ascontiguousarray(faces, dtype=np.float64).reshape(-1, 4, 3), device="cuda")
+    out = torch.empty(pts.shape[0], dtype=torch.float64, device="cuda")
+    _check(lib, lib.jr_wall_distance3d(pts.data_ptr(), int(pts.shape[0]), q.data_ptr(), int(q.shape[0]),
+                                       out.data_ptr()), "jr_wall_distance3d")
+    return out.cpu().numpy().reshape(np.shape(points)[:-1])

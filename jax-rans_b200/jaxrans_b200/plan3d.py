@@ -237,8 +237,13 @@ def pack_tiles(tiles):
     return best
 
 
-def build_plan3d(mesh, g: int = G, with_distance: bool = True) -> Plan3:
-    """Pack ``mesh`` (3D blocks whose patches carry conditions) and build every table."""
+def build_plan3d(mesh, g: int = G, with_distance: bool = True, distance_on: str = "auto") -> Plan3:
+    """Pack ``mesh`` (3D blocks whose patches carry conditions) and build every table.
+    The wall distance is computed on the device (``jr_wall_distance3d``) when
+    ``distance_on`` is ``"device"``, or ``"auto"`` with a CUDA device present; on the
+    host (NumPy) otherwise."""
+    if distance_on not in ("auto", "device", "host"):
+        raise ValueError(f"distance_on must be auto, device or host, got {distance_on!r}")
     mesh = list(mesh)
     for block in mesh:
         block.check()
@@ -326,9 +331,31 @@ def build_plan3d(mesh, g: int = G, with_distance: bool = True) -> Plan3:
                  _neighbours(mesh, pos, n_canvas), _lines(mesh, origins, g, canvas),
                  _walls(mesh, origins, pos, g, canvas))
     if with_distance:
-        plan.distance = plan.pack([wall_distance3d(b, plan.walls.quads, c) for b, (c, _, _)
-                                   in zip(mesh, block_geometry)], 1.0)
+        centres_of = [c for c, _, _ in block_geometry]
+        if _on_device(distance_on):
+            from .native3d import wall_distance_device
+            points = np.concatenate([np.moveaxis(c, 0, -1).reshape(-1, 3) for c in centres_of])
+            flat = wall_distance_device(points, plan.walls.quads.corners) if len(plan.walls.quads.corners) \
+                else np.full(len(points), np.inf)
+            parts, at = [], 0
+            for b in mesh:
+                n = int(np.prod(b.shape))
+                parts.append(flat[at:at + n].reshape(b.shape))
+                at += n
+        else:
+            parts = [wall_distance3d(b, plan.walls.quads, c) for b, c in zip(mesh, centres_of)]
+        plan.distance = plan.pack(parts, 1.0)
     return plan
+
+
+def _on_device(distance_on: str) -> bool:
+    if distance_on != "auto":
+        return distance_on == "device"
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except ImportError:
+        return False
 
 
 def reflect(stage: Stage3, centres: np.ndarray) -> np.ndarray:

@@ -28,6 +28,14 @@ on a GPU box and in the oracle.
 * batch ``polar64_uneven`` -- 64 angles uniform on [-4, 16] deg on the ``c_sa_385``
   grid together with the three uneven cases, all in one device batch; ``polar8_769``,
   8 angles with the 769 x 193 case, is the same mix small enough to profile.
+* ``wing_ch_4blk`` -- 3D SA-noft2 RANS round a swept, tapered wing: NACA 0012 sections,
+  aspect ratio 4 (semispan 1.6 root chords), taper 0.6, leading-edge sweep 25 deg, on a
+  four-block point-matched C-H grid of 193 x 65 x 81 nodes per block (3.93M cells; the
+  wing and the region past its tip, each in lower and upper halves), first cell 2e-6 root
+  chord, far field at 50 root chords, M 0.8, alpha 2.5 deg, Re 1e7, HLLC with MUSCL and
+  the smooth van Albada limiter, 6 variables.  ``wing_ch_4blk_small`` is the same wing on
+  a grid of 49 x 17 x 17 nodes per block, for profiling and tests.  A 3D case is a grid
+  file plus its documents: ``wing3d_case`` writes them into a directory and loads them.
 """
 
 from __future__ import annotations
@@ -97,6 +105,48 @@ def batch_workload(name: str, **numerical) -> list[Case]:
         cases.append(case)
     return cases
 
+
+
+WING3D = {
+    "wing_ch_4blk": {"cells_airfoil": 256, "cells_wake": 64, "cells_normal": 64, "cells_span": 80,
+                     "cells_tip": 80, "wall_spacing": 2e-6, "far_field": 50.0, "cap_cells": 4},
+    "wing_ch_4blk_small": {"cells_airfoil": 64, "cells_wake": 16, "cells_normal": 16, "cells_span": 16,
+                           "cells_tip": 16, "wall_spacing": 1e-4, "far_field": 20.0, "cap_cells": 3},
+}
+WING3D_PLANFORM = {"semispan": 1.6, "taper": 0.6, "sweep_deg": 25.0}
+WING3D_FLOW = {"freestream": {"mach": 0.8, "alpha_deg": 2.5, "reynolds": 1e7}, "turbulence": {"model": "sa_noft2"}}
+WING3D_NUMERICS = {"convective_fluxes": {"riemann_solver": "hllc", "limiter": "van_albada_smooth"},
+                   "time_integration": {"solver": "implicit"},
+                   "implicit": {"krylov_subspace": 30, "max_relative_update": 0.2},
+                   "convergence": {"max_iters": 6000, "tol": 1e-10, "block_iters": 20}}
+
+
+def wing3d_case(name: str, directory, **numerical) -> Case:
+    """Write the 3D workload ``name`` (its Plot3D grid ``grid.x``, ``case.json`` and
+    ``numerical.json``) into ``directory`` and load it as a case."""
+    import json
+    from pathlib import Path
+    from .case import load_case
+    from .geometry import section_source
+    from .grid3d import wing_ch_blocks, write_plot3d
+    directory = Path(directory)
+    directory.mkdir(parents=True, exist_ok=True)
+    grid = wing_ch_blocks(section_source("naca0012"), **WING3D[name], **WING3D_PLANFORM)
+    write_plot3d(directory / "grid.x", grid.blocks)
+    case_doc = {"general": {"case_name": name},
+                "domain": {"grid": "file", "file": "grid.x", "patches": grid.patches,
+                           "reference_area": grid.reference_area, "reference_length": grid.reference_length,
+                           "moment_centre": list(grid.moment_centre)},
+                "boundary_conditions": {"wall": {"type": "no_slip_wall"}, "farfield": {"type": "far_field"},
+                                        "symmetry": {"type": "symmetry"}},
+                **copy.deepcopy(WING3D_FLOW)}
+    num_doc = copy.deepcopy(WING3D_NUMERICS)
+    for path, value in numerical.items():
+        section, key = path.split(".")
+        num_doc.setdefault(section, {})[key] = value
+    (directory / "case.json").write_text(json.dumps(case_doc, indent=1))
+    (directory / "numerical.json").write_text(json.dumps(num_doc, indent=1))
+    return load_case(directory)
 
 
 def workload(name: str, **numerical) -> Case:

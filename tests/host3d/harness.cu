@@ -8,6 +8,7 @@
 #include "../../jax-rans_b200/csrc/plan3d_desc.cuh"
 #include "../../jax-rans_b200/csrc/linesolve3d.cuh"
 #include "../../jax-rans_b200/csrc/newton3d.cuh"
+#include "../../jax-rans_b200/csrc/walldist3d.cuh"
 
 using namespace jr;
 
@@ -215,5 +216,24 @@ extern "C" int jr3_host_forces(const jr_plan3d_desc* d, const double* U, double 
   }
   for (int w = 0; w < p.n_walls; ++w) wall_load(p, A.data(), w, loads.data() + (size_t)7 * w);
   force_coefficients3(p.P, p.n_walls, loads.data(), d->wall_mid, area, length, centre, out);
+  return 0;
+}
+
+// the wall distance of points (n x 3) to faces (m x 4 x 3), faces offered in order as the
+// kernel offers them (bounded = 1: skipping by the bounding spheres; 0: every face ranked)
+extern "C" int jr3_host_wall_distance(const double* points, long long n, const double* faces, int m, double* out,
+                                      int bounded) {
+  std::vector<double> spheres((size_t)4 * m);
+  for (int f = 0; f < m; ++f) face_sphere(faces + (size_t)12 * f, spheres.data() + (size_t)4 * f);
+  for (long long i = 0; i < n; ++i) {
+    const V3 p = v3(points + 3 * i);
+    Candidates c;
+    c.init(m);
+    for (int f = 0; f < m; ++f) {
+      if (bounded) offer_face(c, p, faces + (size_t)12 * f, spheres.data() + (size_t)4 * f, f);
+      else c.offer(face_rank_distance(p, faces + (size_t)12 * f), f);
+    }
+    out[i] = m > 0 ? candidates_distance(p, c, faces) : INFINITY;
+  }
   return 0;
 }

@@ -276,3 +276,21 @@ def test_march3d_runs_blocks_to_the_iteration_limit(harness, z, cases, described
     fields = np.load(out / f"{case.name}_fields.npz")
     assert fields["U_0"].shape == (5, 8, 4, 6) and "z_node_0" in fields
     assert (out / f"{case.name}_block0.vts").read_bytes().startswith(b"<?xml")
+
+
+@pytest.mark.parametrize("name", ["split", "wing4"])
+def test_wall_distance_kernel_body_gives_the_reference_distance(harness, z, cases, name):
+    """The device wall distance's arithmetic (csrc/walldist3d.cuh: the stable 16-candidate
+    ranking and the patch distance), run on the host, against the reference's distance
+    and the plan's NumPy distance."""
+    _, plan = cases[name]
+    points = np.ascontiguousarray(np.moveaxis(plan.centres[:, 1:-1, 1:-1, 1:-1], 0, -1)[plan.interior])
+    faces = np.ascontiguousarray(plan.walls.quads.corners)
+    out, every = np.zeros(len(points)), np.zeros(len(points))
+    assert harness.jr3_host_wall_distance(points.ctypes.data, len(points), faces.ctypes.data, len(faces),
+                                          out.ctypes.data, 1) == 0
+    assert harness.jr3_host_wall_distance(points.ctypes.data, len(points), faces.ctypes.data, len(faces),
+                                          every.ctypes.data, 0) == 0
+    assert np.array_equal(out, every)          # the sphere bound skips only faces the ranking refuses
+    assert np.allclose(out, z[f"{name}_distance"][plan.interior], rtol=1e-12, atol=1e-15)
+    assert np.allclose(out, plan.distance[plan.interior], rtol=1e-12, atol=1e-15)

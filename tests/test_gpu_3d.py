@@ -104,7 +104,7 @@ def blocks3d(tmp_path_factory):
     from jaxrans_b200.grid3d import write_plot3d
     z = np.load(BLOCKS)
     out = {}
-    for name in ("split", "pole"):
+    for name in ("split", "wing4", "pole"):
         d = tmp_path_factory.mktemp(name)
         doc = json.loads(str(z[f"{name}_case_json"]))
         write_plot3d(d / "grid.x", [z[f"{name}_raw{b}"] for b in range(int(z[f"{name}_n_blocks"]))])
@@ -115,7 +115,7 @@ def blocks3d(tmp_path_factory):
     return z, out
 
 
-@pytest.mark.parametrize("name", ["split", "pole"])
+@pytest.mark.parametrize("name", ["split", "wing4", "pole"])
 def test_blocks3d_residual_and_jvp_on_the_device(cuda, blocks3d, name):
     from jaxrans_b200.solver3d import device3_for
     z, cases = blocks3d
@@ -142,3 +142,14 @@ def test_run_marches_a_3d_grid_file(cuda, blocks3d):
     result = run(replace(case, block_iters=2, numerics=replace(case.numerics, max_iters=4)), plan)
     assert 2 <= result.history.n_iters <= 4 and np.all(np.isfinite(result.history.residual))
     assert result.U.shape == (5,) + plan.shape
+
+
+def test_wall_distance_on_the_device(cuda, blocks3d):
+    """jr_wall_distance3d against the reference's distance and the plan's NumPy distance."""
+    from jaxrans_b200.native3d import wall_distance_device
+    z, cases = blocks3d
+    for name in ("split", "wing4"):
+        _, plan = cases[name]
+        points = np.moveaxis(plan.centres[:, 1:-1, 1:-1, 1:-1], 0, -1)[plan.interior]
+        got = wall_distance_device(points, plan.walls.quads.corners)
+        assert np.allclose(got, z[f"{name}_distance"][plan.interior], rtol=1e-12, atol=1e-15)
