@@ -279,6 +279,9 @@ typedef struct jr_plan3d_desc {
   const int32_t* wall_face;     /* its index within the family's canvas faces */
   const double* wall_into;      /* +1 where the family's vector points into the fluid, else -1 */
   const double* wall_mid;       /* 3 per face: the mean of its four nodes */
+  /* 0: the line factor and apply in FP64; 1: in FP32 (the mixed form; Krylov vectors,
+   * residual, J.v and update stay FP64) */
+  int32_t line_precision;
 } jr_plan3d_desc;
 
 /* Build a 3D plan (device copies of the tables, work buffers, a stream).  Every record

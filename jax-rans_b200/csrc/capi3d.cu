@@ -24,7 +24,7 @@ struct jr_plan3d {
   std::vector<void*> allocs;
   void* A = nullptr;   // primitive canvases (Dual-sized: the J.v needs value and tangent)
   void* B = nullptr;
-  double* scratch = nullptr;   // the line solve's eliminated blocks: n_chains * chain_L * 30
+  void* factor = nullptr;      // the line factor: n_chains * chain_L * FACTOR3 words (FP32 in the mixed form)
   size_t n_canvas = 0;
   Newton3Config cfg{};
   double* loads = nullptr;     // 7 per wall face
@@ -173,14 +173,19 @@ int jr_plan3d_create(const jr_plan3d_desc* d, jr_plan3d** out) {
     p->loads = static_cast<double*>(l);
   }
   physics3_from_desc(dv.P, d);
+  if (d->line_precision != 0 && d->line_precision != 1) {
+    jr_plan3d_destroy(p);
+    return report_error(JR_EINVAL, "line_precision must be 0 (FP64) or 1 (FP32)");
+  }
+  dv.line_fp32 = d->line_precision;
   if (n_links > 0) {
     void* sc = nullptr;
-    if (cudaMalloc(&sc, n_links * 30 * sizeof(double)) != cudaSuccess) {
+    if (cudaMalloc(&sc, n_links * FACTOR3 * (dv.line_fp32 ? sizeof(float) : sizeof(double))) != cudaSuccess) {
       jr_plan3d_destroy(p);
       return report_error(JR_ENOMEM, "cudaMalloc failed");
     }
     p->allocs.push_back(sc);
-    p->scratch = static_cast<double*>(sc);
+    p->factor = sc;
   }
   const size_t work = (size_t)d->nvar * n * sizeof(Dual);
   if (cudaMalloc(&p->A, work) != cudaSuccess || (p->allocs.push_back(p->A), cudaMalloc(&p->B, work)) != cudaSuccess) {
@@ -244,7 +249,7 @@ int jr_wave_speeds3d(jr_plan3d* plan, const double* U, double* lam) {
 int jr_precondition3d(jr_plan3d* plan, const double* U, double cfl, const double* r, double* z) {
   if (!plan || !U || !r || !z) return report_error(JR_EINVAL, "null argument");
   if (!(cfl > 0.0)) return report_error(JR_EINVAL, "cfl must be positive");
-  launch_precondition3(plan->dev, U, cfl, r, z, plan->scratch, plan->st);
+  launch_precondition3(plan->dev, U, cfl, r, z, plan->factor, plan->st);
   if (cudaStreamSynchronize(plan->st) != cudaSuccess) return check3("jr_precondition3d");
   return check3("jr_precondition3d");
 }
@@ -259,7 +264,8 @@ int jr_newton_steps3d(jr_plan3d* plan, double* U, int32_t n_steps, double* cfl, 
   ops.N = (size_t)plan->dev.nvar * plan->n_canvas;
   ops.A = plan->A;
   ops.B = plan->B;
-  ops.scratch = plan->scratch;
+  ops.factor = plan->factor;
+  ops.line = plan->cfg.preconditioner == 1;
   ops.st = plan->st;
   ops.bind(plan->work, plan->flag, plan->cfg.restart);
   double c = *cfl, r = *residual_norm;

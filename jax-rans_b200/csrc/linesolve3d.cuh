@@ -142,23 +142,37 @@ __host__ __device__ __forceinline__ void coupling5(const double* qnb, const doub
     for (int c = 0; c < 5; ++c) B[r][c] = 0.5 * A[r][c] - (r == c ? 0.5 * lam : 0.0);
 }
 
-// z = M^-1 r on the mean-flow rows of chain ch (block Thomas, src/jaxrans/core/linalg.py:80-132);
-// C (L x 25) and D (L x 5) the chain's scratch
-inline __host__ __device__ void chain_flow(const Plan3Dev& p, const double* U, double cfl, int ch, const double* r, double* z,
-                                    double* Cs, double* Ds) {
-  const int n = p.NI * p.NJ * p.NK, L = p.chain_L;
+// The line_j factor of one chain (block Thomas, src/jaxrans/core/linalg.py:80-132, and the
+// scalar SA chain): for element k of the chain, the block toward k-1 (lower_k), the
+// inverse pivot P_k = (D_k - lower_k C_{k-1})^-1 and C_k = P_k upper_k -- 75 entries -- and
+// on the SA row the same three scalars.  Entry e of element k of chain ch is stored at
+// F[(k * FACTOR3 + e) * n_chains + ch]: neighbouring chains' threads read neighbouring
+// words.  The apply is then z_k = P_k (r_k - lower_k d_{k-1}) down the chain and
+// x_k = d_k - C_k x_{k+1} back up, the factor computed once per Newton step.
+constexpr int F3_LOWER = 0, F3_PIV = 25, F3_CHAT = 50, F3_SA = 75;
+
+__host__ __device__ __forceinline__ size_t factor_at(const Plan3Dev& p, int ch, int k, int e) {
+  return ((size_t)k * FACTOR3 + e) * p.n_chains + ch;
+}
+
+__host__ __device__ __forceinline__ int chain_length(const Plan3Dev& p, int ch) {
+  const int* cells = p.ch_cells + (size_t)ch * p.chain_L;
+  int len = 0;
+  while (len < p.chain_L && cells[len] >= 0) ++len;
+  return len;
+}
+
+template <class TF>
+inline __host__ __device__ void chain_factor_flow(const Plan3Dev& p, const double* U, double cfl, int ch, TF* F) {
+  const int L = p.chain_L;
   const double g = p.P.gamma;
   const int* cells = p.ch_cells + (size_t)ch * L;
-  int len = 0;
-  while (len < L && cells[len] >= 0) ++len;
-  double cprev[5][5] = {}, dprev[5] = {};
+  const int len = chain_length(p, ch);
+  double cprev[5][5] = {};
   double lower[5][5] = {};   // row k's block toward cell k-1
   for (int k = 0; k < len; ++k) {
     const int c = cells[k];
     const double dg = lambda_sum(p, U, c) * (1.0 / cfl + 0.5);
-    double D[5][5];
-    for (int a = 0; a < 5; ++a)
-      for (int b = 0; b < 5; ++b) D[a][b] = a == b ? dg : 0.0;
     double upper[5][5] = {}, lower_next[5][5] = {};
     const int sign = k + 1 < len ? p.ch_sign[(size_t)ch * L + k] : 0;
     if (sign != 0) {
@@ -169,47 +183,64 @@ inline __host__ __device__ void chain_flow(const Plan3Dev& p, const double* U, d
       coupling5(qn, s, (double)sign, lam, g, upper);
       coupling5(qc, s, (double)-sign, lam, g, lower_next);
     }
-    // piv = inv(D - lower c_prev); chat = piv upper; d = piv (r - lower d_prev)
-    double T[5][5], piv[5][5], rhs[5];
+    // P = inv(D - lower c_prev); chat = P upper
+    double T[5][5], piv[5][5];
     for (int a = 0; a < 5; ++a)
       for (int b = 0; b < 5; ++b) {
         double m = lower[a][0] * cprev[0][b];
         for (int t = 1; t < 5; ++t) m = m + lower[a][t] * cprev[t][b];
-        T[a][b] = D[a][b] - m;
+        T[a][b] = (a == b ? dg : 0.0) - m;
       }
     invert_n<5>(T, piv);
-    for (int a = 0; a < 5; ++a) {
-      double m = lower[a][0] * dprev[0];
-      for (int t = 1; t < 5; ++t) m = m + lower[a][t] * dprev[t];
-      rhs[a] = r[(size_t)a * n + c] - m;
-    }
-    for (int a = 0; a < 5; ++a) {
+    for (int a = 0; a < 5; ++a)
       for (int b = 0; b < 5; ++b) {
         double m = piv[a][0] * upper[0][b];
         for (int t = 1; t < 5; ++t) m = m + piv[a][t] * upper[t][b];
         cprev[a][b] = m;
-        Cs[(size_t)k * 25 + a * 5 + b] = m;
+        F[factor_at(p, ch, k, F3_LOWER + a * 5 + b)] = (TF)lower[a][b];
+        F[factor_at(p, ch, k, F3_PIV + a * 5 + b)] = (TF)piv[a][b];
+        F[factor_at(p, ch, k, F3_CHAT + a * 5 + b)] = (TF)m;
       }
-      double m = piv[a][0] * rhs[0];
-      for (int t = 1; t < 5; ++t) m = m + piv[a][t] * rhs[t];
-      Ds[(size_t)k * 5 + a] = m;
+    for (int a = 0; a < 5; ++a)
+      for (int b = 0; b < 5; ++b) lower[a][b] = lower_next[a][b];
+  }
+}
+
+// z = M^-1 r on the mean-flow rows of chain ch from its factor; d_k is kept in z between
+// the two sweeps
+template <class TF>
+inline __host__ __device__ void chain_apply_flow(const Plan3Dev& p, int ch, const TF* F, const double* r, double* z) {
+  const int n = p.NI * p.NJ * p.NK;
+  const int* cells = p.ch_cells + (size_t)ch * p.chain_L;
+  const int len = chain_length(p, ch);
+  TF dprev[5] = {};
+  for (int k = 0; k < len; ++k) {
+    const int c = cells[k];
+    TF rhs[5];
+    for (int a = 0; a < 5; ++a) {
+      TF m = F[factor_at(p, ch, k, F3_LOWER + a * 5)] * dprev[0];
+      for (int t = 1; t < 5; ++t) m = m + F[factor_at(p, ch, k, F3_LOWER + a * 5 + t)] * dprev[t];
+      rhs[a] = (TF)r[(size_t)a * n + c] - m;
     }
     for (int a = 0; a < 5; ++a) {
-      dprev[a] = Ds[(size_t)k * 5 + a];
-      for (int b = 0; b < 5; ++b) lower[a][b] = lower_next[a][b];
+      TF m = F[factor_at(p, ch, k, F3_PIV + a * 5)] * rhs[0];
+      for (int t = 1; t < 5; ++t) m = m + F[factor_at(p, ch, k, F3_PIV + a * 5 + t)] * rhs[t];
+      dprev[a] = m;
+      z[(size_t)a * n + c] = (double)m;
     }
   }
-  double nxt[5] = {};
+  TF nxt[5] = {};
   for (int k = len - 1; k >= 0; --k) {
-    double x[5];
+    const int c = cells[k];
+    TF x[5];
     for (int a = 0; a < 5; ++a) {
-      double m = Cs[(size_t)k * 25 + a * 5] * nxt[0];
-      for (int t = 1; t < 5; ++t) m = m + Cs[(size_t)k * 25 + a * 5 + t] * nxt[t];
-      x[a] = Ds[(size_t)k * 5 + a] - m;
+      TF m = F[factor_at(p, ch, k, F3_CHAT + a * 5)] * nxt[0];
+      for (int t = 1; t < 5; ++t) m = m + F[factor_at(p, ch, k, F3_CHAT + a * 5 + t)] * nxt[t];
+      x[a] = (TF)z[(size_t)a * n + c] - m;
     }
     for (int a = 0; a < 5; ++a) {
       nxt[a] = x[a];
-      z[(size_t)a * n + cells[k]] = x[a];
+      z[(size_t)a * n + c] = (double)x[a];
     }
   }
 }
@@ -271,14 +302,13 @@ inline __host__ __device__ double sa_diagonal(const Plan3Dev& p, const double* U
   return diag + dest * vol + lambda_sum(p, U, c) / cfl;
 }
 
-// z = M^-1 r on the SA row of chain ch (scalar Thomas); C, D the chain's scratch (L each)
-inline __host__ __device__ void chain_sa(const Plan3Dev& p, const double* U, double cfl, int ch, const double* r, double* z,
-                                  double* Cs, double* Ds) {
-  const int n = p.NI * p.NJ * p.NK, L = p.chain_L;
+// the SA row's factor of chain ch (scalar Thomas): lower_k, 1 / (d_k - lower_k c_{k-1}), c_k
+template <class TF>
+inline __host__ __device__ void chain_factor_sa(const Plan3Dev& p, const double* U, double cfl, int ch, TF* F) {
+  const int L = p.chain_L;
   const int* cells = p.ch_cells + (size_t)ch * L;
-  int len = 0;
-  while (len < L && cells[len] >= 0) ++len;
-  double cprev = 0.0, dprev = 0.0, lower = 0.0;
+  const int len = chain_length(p, ch);
+  double cprev = 0.0, lower = 0.0;
   for (int k = 0; k < len; ++k) {
     const int c = cells[k];
     const double dg = sa_diagonal(p, U, cfl, c);
@@ -296,15 +326,29 @@ inline __host__ __device__ void chain_sa(const Plan3Dev& p, const double* U, dou
     }
     const double piv = 1.0 / (dg - lower * cprev);
     cprev = piv * upper;
-    Cs[k] = cprev;
-    Ds[k] = piv * (r[(size_t)5 * n + c] - lower * dprev);
-    dprev = Ds[k];
+    F[factor_at(p, ch, k, F3_SA)] = (TF)lower;
+    F[factor_at(p, ch, k, F3_SA + 1)] = (TF)piv;
+    F[factor_at(p, ch, k, F3_SA + 2)] = (TF)cprev;
     lower = lower_next;
   }
-  double nxt = 0.0;
+}
+
+template <class TF>
+inline __host__ __device__ void chain_apply_sa(const Plan3Dev& p, int ch, const TF* F, const double* r, double* z) {
+  const int n = p.NI * p.NJ * p.NK;
+  const int* cells = p.ch_cells + (size_t)ch * p.chain_L;
+  const int len = chain_length(p, ch);
+  TF dprev = 0;
+  for (int k = 0; k < len; ++k) {
+    const int c = cells[k];
+    dprev = F[factor_at(p, ch, k, F3_SA + 1)] * ((TF)r[(size_t)5 * n + c] - F[factor_at(p, ch, k, F3_SA)] * dprev);
+    z[(size_t)5 * n + c] = (double)dprev;
+  }
+  TF nxt = 0;
   for (int k = len - 1; k >= 0; --k) {
-    nxt = Ds[k] - Cs[k] * nxt;
-    z[(size_t)5 * n + cells[k]] = nxt;
+    const int c = cells[k];
+    nxt = (TF)z[(size_t)5 * n + c] - F[factor_at(p, ch, k, F3_SA + 2)] * nxt;
+    z[(size_t)5 * n + c] = (double)nxt;
   }
 }
 

@@ -142,6 +142,7 @@ double DeviceOps3::host_sum(int count, int halves) {
 void DeviceOps3::prepare(const double* U, double cfl) {
   counted3();
   k3_vdt<<<grid_of(n), 128, 0, st>>>(p, U, cfl, vdt);
+  if (line) launch_line_factor3(p, U, cfl, factor, st);
 }
 
 void DeviceOps3::residual(const double* U, int out) { launch_residual3(p, U, v(out), A, B, false, st); }
@@ -152,8 +153,9 @@ void DeviceOps3::matvec(const double* U, double, int src, int out) {
   k3_vdt_add<<<grid_of(N), 256, 0, st>>>(N, n, vdt, v(src), v(out));
 }
 
-void DeviceOps3::precondition(const double* U, double cfl, int src, int dst) {
-  launch_precondition3(p, U, cfl, v(src), v(dst), scratch, st);
+// the factor of this step's (U, cfl), made in prepare
+void DeviceOps3::precondition(const double*, double, int src, int dst) {
+  launch_line_apply3(p, factor, v(src), v(dst), st);
 }
 
 double DeviceOps3::dot(int a, int b) {

@@ -13,7 +13,8 @@ struct DeviceOps3 {
   Plan3Dev p;
   size_t N = 0, n = 0;
   void *A = nullptr, *B = nullptr;   // primitive canvases of the residual / J.v
-  double* scratch = nullptr;         // the line solve's
+  void* factor = nullptr;            // the line factor (computed in prepare when line)
+  bool line = false;
   double* vecs = nullptr;
   double* vdt = nullptr;
   double* partial = nullptr;

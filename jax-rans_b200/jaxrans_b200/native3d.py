@@ -39,7 +39,7 @@ class Plan3Desc(C.Structure):
         ("krylov_tol", C.c_double), ("krylov_success", C.c_double), ("max_relative_update", C.c_double),
         ("krylov_subspace", C.c_int32), ("krylov_restarts", C.c_int32), ("preconditioner", C.c_int32),
         ("n_walls", C.c_int32), ("wall_cell", _i32p), ("wall_family", _i32p), ("wall_face", _i32p),
-        ("wall_into", _f64p), ("wall_mid", _f64p),
+        ("wall_into", _f64p), ("wall_mid", _f64p), ("line_precision", C.c_int32),
     ]
 
 
@@ -153,6 +153,7 @@ def describe(plan: Plan3, q_inf, gamma: float, flux: str, limiter: str, kappa: f
     d.max_relative_update = -1.0 if imp.max_relative_update is None else imp.max_relative_update
     d.krylov_subspace, d.krylov_restarts = imp.krylov_subspace, imp.krylov_restarts
     d.preconditioner = {"none": 0, "line_j": 1}[imp.preconditioner]
+    d.line_precision = 1 if imp.precision == "mixed" else 0
     W = plan.walls
     d.n_walls = len(W.cell)
     d.wall_cell = ptr(arr(W.cell, np.int32), _i32p)
@@ -171,6 +172,10 @@ class DevicePlan3:
                  mu_inf: float | None = None, sutherland: float | None = None, implicit=None, library=None):
         self.lib = load_library(library)
         self.plan = plan
+        self.q_inf, self.gamma, self.flux, self.limiter = np.asarray(q_inf, dtype=np.float64), gamma, flux, limiter
+        self.mu_inf, self.sutherland = mu_inf, sutherland
+        from .config import ImplicitConfig
+        self.implicit = implicit if implicit is not None else ImplicitConfig()
         self.nvar = len(q_inf)
         self.shape = (self.nvar,) + plan.shape
         d, keep = describe(plan, q_inf, gamma, flux, limiter, kappa, mu_inf, sutherland, implicit)

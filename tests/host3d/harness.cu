@@ -45,6 +45,7 @@ static Plan3Dev plan_of(const jr_plan3d_desc* d) {
   p.g_normal = d->normal;
   p.neighbours = d->neighbours;
   p.n_chains = d->n_chains;
+  p.line_fp32 = d->line_precision;
   p.chain_L = d->chain_L;
   p.ch_cells = d->chain_cells;
   p.ch_face = d->chain_up_face;
@@ -86,16 +87,30 @@ extern "C" int jr3_host_wave_speeds(const jr_plan3d_desc* d, const double* U, do
   return 0;
 }
 
-extern "C" int jr3_host_precondition(const jr_plan3d_desc* d, const double* U, double cfl, const double* r,
-                                     double* z) {
-  const Plan3Dev p = plan_of(d);
+// the line factor of every chain, then the apply, in the words the descriptor asks for
+template <class TF>
+static void line_solve(const Plan3Dev& p, const double* U, double cfl, const double* r, double* z) {
   const size_t n = (size_t)p.nvar * p.NI * p.NJ * p.NK;
   for (size_t e = 0; e < n; ++e) z[e] = r[e];
-  std::vector<double> scratch((size_t)p.chain_L * 30);
+  std::vector<TF> F((size_t)p.n_chains * p.chain_L * FACTOR3);
   for (int ch = 0; ch < p.n_chains; ++ch) {
-    chain_flow(p, U, cfl, ch, r, z, scratch.data(), scratch.data() + (size_t)p.chain_L * 25);
-    if (p.nvar > 5) chain_sa(p, U, cfl, ch, r, z, scratch.data(), scratch.data() + (size_t)p.chain_L * 25);
+    chain_factor_flow(p, U, cfl, ch, F.data());
+    if (p.nvar > 5) chain_factor_sa(p, U, cfl, ch, F.data());
   }
+  for (int ch = 0; ch < p.n_chains; ++ch) {
+    chain_apply_flow(p, ch, F.data(), r, z);
+    if (p.nvar > 5) chain_apply_sa(p, ch, F.data(), r, z);
+  }
+}
+
+static void line_solve_as(const Plan3Dev& p, const double* U, double cfl, const double* r, double* z) {
+  if (p.line_fp32) line_solve<float>(p, U, cfl, r, z);
+  else line_solve<double>(p, U, cfl, r, z);
+}
+
+extern "C" int jr3_host_precondition(const jr_plan3d_desc* d, const double* U, double cfl, const double* r,
+                                     double* z) {
+  line_solve_as(plan_of(d), U, cfl, r, z);
   return 0;
 }
 
@@ -130,14 +145,7 @@ struct HostOps {
     else run<Dual, false, false>(p, U, d(src), d(out), 1);
     for (size_t e = 0; e < N; ++e) d(out)[e] = vdt[e % n] * d(src)[e] + d(out)[e];
   }
-  void precondition(const double* U, double cfl, int src, int dst) {
-    for (size_t e = 0; e < N; ++e) d(dst)[e] = d(src)[e];
-    std::vector<double> scratch((size_t)p.chain_L * 30);
-    for (int ch = 0; ch < p.n_chains; ++ch) {
-      chain_flow(p, U, cfl, ch, d(src), d(dst), scratch.data(), scratch.data() + (size_t)p.chain_L * 25);
-      if (p.nvar > 5) chain_sa(p, U, cfl, ch, d(src), d(dst), scratch.data(), scratch.data() + (size_t)p.chain_L * 25);
-    }
-  }
+  void precondition(const double* U, double cfl, int src, int dst) { line_solve_as(p, U, cfl, d(src), d(dst)); }
   double dot(int a, int b) {
     double s = 0.0;
     for (size_t e = 0; e < N; ++e) s += d(a)[e] * d(b)[e];

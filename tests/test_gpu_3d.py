@@ -153,3 +153,21 @@ def test_wall_distance_on_the_device(cuda, blocks3d):
         points = np.moveaxis(plan.centres[:, 1:-1, 1:-1, 1:-1], 0, -1)[plan.interior]
         got = wall_distance_device(points, plan.walls.quads.corners)
         assert np.allclose(got, z[f"{name}_distance"][plan.interior], rtol=1e-12, atol=1e-15)
+
+
+def test_mixed_line_solve3d_on_the_device(cuda, device3d):
+    """The FP32 line factor and apply (implicit.precision = mixed) within FP32 of FP64."""
+    from dataclasses import replace
+    from jaxrans_b200.native3d import DevicePlan3
+    z, dev = device3d
+    imp = replace(dev.implicit, precision="mixed")
+    U, r = z["rand0_U"], z["rand0_prec_r"]
+    exact = dev.precondition(U, 25.0, r)
+    mixed_dev = DevicePlan3(dev.plan, dev.q_inf, dev.gamma, dev.flux, dev.limiter, 0.0, dev.mu_inf, dev.sutherland,
+                            imp)
+    try:
+        mixed = mixed_dev.precondition(U, 25.0, r)
+    finally:
+        mixed_dev.close()
+    err = max(float(np.abs(mixed[k] - exact[k]).max() / np.abs(exact[k]).max()) for k in range(exact.shape[0]))
+    assert 0.0 < err < 1e-4

@@ -153,3 +153,22 @@ def test_kernel_bodies_give_the_reference_forces(harness, case3d, state):
     out = np.zeros(4)
     assert f(C.addressof(desc), U.ctypes.data, area, 0.8, centre.ctypes.data, out.ctypes.data) == 0
     assert np.allclose(out, z[f"{state}_forces"], rtol=1e-11, atol=1e-16)
+
+
+@pytest.mark.parametrize("state", ["sin", "rand0"])
+def test_the_mixed_line_solve_stays_within_fp32_of_fp64(harness, case3d, state):
+    """The mixed form's line factor and apply in FP32 (``line_precision = 1``) against the
+    FP64 solve: FP32 round-off grown through the chain's block eliminations."""
+    z, plan, desc, _ = case3d
+    U = np.ascontiguousarray(z[f"{state}_U"])
+    r = np.ascontiguousarray(z[f"{state}_prec_r"])
+    exact, mixed = np.zeros_like(r), np.zeros_like(r)
+    assert harness.jr3_host_precondition(C.addressof(desc), U.ctypes.data, 25.0, r.ctypes.data, exact.ctypes.data) == 0
+    desc.line_precision = 1
+    try:
+        assert harness.jr3_host_precondition(C.addressof(desc), U.ctypes.data, 25.0, r.ctypes.data,
+                                             mixed.ctypes.data) == 0
+    finally:
+        desc.line_precision = 0
+    err = rows_rel(mixed, exact)
+    assert 0.0 < err < 1e-4
