@@ -312,8 +312,8 @@ int jr_precondition3d(jr_plan3d* plan, const double* U, double cfl, const double
  * from *cfl and the previous |R| *residual_norm (both host, updated); history (host,
  * n_steps) receives |R| before each step.  GMRES(krylov_subspace) with krylov_restarts
  * cycles, CGS2, Givens least squares, the relaxation, acceptance test and CFL ramp of
- * src/jaxrans/solvers/implicit.py:54-168, driven from the host over device kernels (a
- * first form: it synchronises for each scalar).  Replaces make_newton_step run as the
+ * src/jaxrans/solvers/implicit.py:54-168, driven from the host over device kernels (it
+ * synchronises for the scalars: three times per Arnoldi step).  Replaces make_newton_step run as the
  * driver's block on a 3D atlas. */
 int jr_newton_steps3d(jr_plan3d* plan, double* U, int32_t n_steps, double* cfl, double* residual_norm,
                       double* history);

@@ -194,7 +194,7 @@ int jr_plan3d_create(const jr_plan3d_desc* d, jr_plan3d** out) {
   }
   p->allocs.push_back(p->B);
   // the Newton step's configuration and vectors
-  if (d->krylov_subspace < 1 || d->krylov_subspace > 64 || d->krylov_restarts < 1 || d->preconditioner < 0 ||
+  if (d->krylov_subspace < 1 || d->krylov_subspace > MAX_RESTART3 || d->krylov_restarts < 1 || d->preconditioner < 0 ||
       d->preconditioner > 1) {
     jr_plan3d_destroy(p);
     return report_error(JR_EINVAL, "krylov_subspace 1..64, krylov_restarts >= 1, preconditioner 0 or 1");

@@ -1,7 +1,8 @@
 // The 3D Newton step on the device: newton3d.cuh's driver over kernel-backed vector
 // operations (the residual, J.v, wave speeds and line solve of residual3d.cu and
 // linesolve3d.cu; dot products by a fixed-order two-stage reduction, so a step is
-// bitwise reproducible).  A first form: the driver synchronises on each scalar it needs.
+// bitwise reproducible).  The driver synchronises for the scalars it needs: each CGS2
+// pass's dots come back together (k3_mdot_partial), three reads per Arnoldi step.
 #include <cstdio>
 
 #include "linesolve3d.cuh"
@@ -55,6 +56,32 @@ __global__ void k3_dot_partial(size_t N, const double* __restrict__ a, const dou
     acc = acc + a[e] * b[e];
   const double t = block_sum(acc);
   if (threadIdx.x == 0) partial[blockIdx.x] = t;
+}
+
+// the dots of basis vectors 0..count-1 with w in one launch: block (x, i) makes exactly
+// the partial sum k3_dot_partial makes for V_i . w
+__global__ void k3_mdot_partial(size_t N, const double* __restrict__ V, const double* __restrict__ w,
+                                double* __restrict__ partial) {
+  const double* a = V + (size_t)blockIdx.y * N;
+  double acc = 0.0;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < N; e += (size_t)gridDim.x * blockDim.x)
+    acc = acc + a[e] * w[e];
+  const double t = block_sum(acc);
+  if (threadIdx.x == 0) partial[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = t;
+}
+
+struct Coeffs3 {
+  double c[MAX_RESTART3 + 1];
+};
+
+// y += c_0 V_0 + c_1 V_1 + ... + c_{count-1} V_{count-1}, term by term in that order (the
+// arithmetic of count axpys, in one pass)
+__global__ void k3_maxpy(size_t N, int count, Coeffs3 cf, const double* __restrict__ V, double* __restrict__ y) {
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < N; e += (size_t)gridDim.x * blockDim.x) {
+    double acc = y[e];
+    for (int i = 0; i < count; ++i) acc = acc + cf.c[i] * V[(size_t)i * N + e];
+    y[e] = acc;
+  }
 }
 
 __global__ void k3_norm_partial(Plan3Dev p, const double* __restrict__ R, double* __restrict__ partial) {
@@ -158,6 +185,26 @@ void DeviceOps3::precondition(const double*, double, int src, int dst) {
   launch_line_apply3(p, factor, v(src), v(dst), st);
 }
 
+void DeviceOps3::mdot(int count, int w, double* h) {
+  counted3();
+  k3_mdot_partial<<<dim3(RED3_BLOCKS, count), RED3_THREADS, 0, st>>>(N, v(V(0)), v(w), partial);
+  std::vector<double> part((size_t)count * RED3_BLOCKS);
+  cudaMemcpyAsync(part.data(), partial, part.size() * sizeof(double), cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+  for (int i = 0; i < count; ++i) {
+    double s = 0.0;
+    for (int b = 0; b < RED3_BLOCKS; ++b) s = s + part[(size_t)i * RED3_BLOCKS + b];
+    h[i] = s;
+  }
+}
+
+void DeviceOps3::maxpy(int count, const double* coef, int y) {
+  Coeffs3 cf{};
+  for (int i = 0; i < count; ++i) cf.c[i] = coef[i];
+  counted3();
+  k3_maxpy<<<grid_of(N), 256, 0, st>>>(N, count, cf, v(V(0)), v(y));
+}
+
 double DeviceOps3::dot(int a, int b) {
   counted3();
   k3_dot_partial<<<RED3_BLOCKS, RED3_THREADS, 0, st>>>(N, v(a), v(b), partial);
@@ -209,7 +256,7 @@ void DeviceOps3::add_to_state(double* U, int du) {
 }
 
 size_t DeviceOps3::work_doubles(size_t N, size_t n, int m) {
-  return (size_t)(BASE + m + 1) * N + n + 2 * RED3_BLOCKS;
+  return (size_t)(BASE + m + 1) * N + n + (size_t)(m + 1) * RED3_BLOCKS;
 }
 
 void DeviceOps3::bind(double* work, int* flag_word, int m) {

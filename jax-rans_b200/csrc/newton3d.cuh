@@ -10,6 +10,8 @@
 
 namespace jr {
 
+constexpr int MAX_RESTART3 = 64;   // krylov_subspace at most
+
 struct Newton3Config {
   int restart, maxiter, preconditioner;   // preconditioner 0 none, 1 line_j
   double tol, success, max_relative_update;   // max_relative_update <= 0: none
@@ -50,9 +52,10 @@ inline void givens_lstsq(const std::vector<double>& Hc, int m, double beta, doub
 
 // Ops: vectors by index -- R_, Z_, W_, T_ (GMRES work), RES_, B_, DU_, ACT_ (the step's),
 // V(i) the basis -- each of the canvas length N = nvar * cells; the state U is the
-// caller's.  Operations: prepare(U, cfl) (V/dt), residual, matvec (V/dt z + J1 z),
-// precondition, dot, nrm2, axpy, scale, copy, zero, density_norm, worst_ratio,
-// physical_after, add_to_state.
+// caller's.  Operations: prepare(U, cfl) (V/dt, the line factor), residual, matvec
+// (V/dt z + J1 z), precondition, dot, mdot (the dots of V(0..count-1) with a vector, as
+// that many dots), maxpy (y += sum of coef_i V(i), as that many axpys in order), nrm2,
+// axpy, scale, copy, zero, density_norm, worst_ratio, physical_after, add_to_state.
 template <class Ops>
 int gmres3(Ops& ops, const double* U, double cfl, const Newton3Config& c, int B, int X, int ACTION) {
   // solves (V/dt + J) X = B; ACTION = the Arnoldi action A X
@@ -67,7 +70,7 @@ int gmres3(Ops& ops, const double* U, double cfl, const Newton3Config& c, int B,
   ops.zero(X);
   ops.copy(B, Ops::R_);
   ops.zero(ACTION);
-  std::vector<double> H((size_t)(m + 1) * m), h(m + 1), h2(m + 1), y, Hy(m + 1);
+  std::vector<double> H((size_t)(m + 1) * m), h(m + 1), h2(m + 1), neg(m + 1), y, Hy(m + 1);
   for (int k = 0; k < c.maxiter; ++k) {
     const double rn = ops.nrm2(Ops::R_);
     if (!(rn > c.tol * bn)) break;
@@ -77,10 +80,12 @@ int gmres3(Ops& ops, const double* U, double cfl, const Newton3Config& c, int B,
     for (int j = 0; j < m; ++j) {
       prec(ops.V(j), Ops::Z_);
       ops.matvec(U, cfl, Ops::Z_, Ops::W_);
-      for (int i = 0; i <= j; ++i) h[i] = ops.dot(ops.V(i), Ops::W_);
-      for (int i = 0; i <= j; ++i) ops.axpy(-h[i], ops.V(i), Ops::W_);
-      for (int i = 0; i <= j; ++i) h2[i] = ops.dot(ops.V(i), Ops::W_);
-      for (int i = 0; i <= j; ++i) ops.axpy(-h2[i], ops.V(i), Ops::W_);
+      ops.mdot(j + 1, Ops::W_, h.data());
+      for (int i = 0; i <= j; ++i) neg[i] = -h[i];
+      ops.maxpy(j + 1, neg.data(), Ops::W_);
+      ops.mdot(j + 1, Ops::W_, h2.data());
+      for (int i = 0; i <= j; ++i) neg[i] = -h2[i];
+      ops.maxpy(j + 1, neg.data(), Ops::W_);
       const double nrm = ops.nrm2(Ops::W_);
       for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = h[i] + h2[i];
       H[(size_t)(j + 1) * m + j] = nrm;
@@ -88,7 +93,7 @@ int gmres3(Ops& ops, const double* U, double cfl, const Newton3Config& c, int B,
     }
     givens_lstsq(H, m, beta, rcond, y);
     ops.zero(Ops::T_);
-    for (int i = 0; i < m; ++i) ops.axpy(y[i], ops.V(i), Ops::T_);
+    ops.maxpy(m, y.data(), Ops::T_);
     prec(Ops::T_, Ops::Z_);
     ops.axpy(1.0, Ops::Z_, X);
     for (int i = 0; i <= m; ++i) {
@@ -96,7 +101,7 @@ int gmres3(Ops& ops, const double* U, double cfl, const Newton3Config& c, int B,
       for (int j = 0; j < m; ++j) s = s + H[(size_t)i * m + j] * y[j];
       Hy[i] = s;
     }
-    for (int i = 0; i <= m; ++i) ops.axpy(Hy[i], ops.V(i), ACTION);
+    ops.maxpy(m + 1, Hy.data(), ACTION);
     ops.copy(B, Ops::R_);
     ops.axpy(-1.0, ACTION, Ops::R_);
   }

@@ -30,6 +30,8 @@ struct DeviceOps3 {
   void matvec(const double* U, double cfl, int src, int out);
   void precondition(const double* U, double cfl, int src, int dst);
   double dot(int a, int b);
+  void mdot(int count, int w, double* h);                 // h[i] = V(i) . w, i < count
+  void maxpy(int count, const double* coef, int y);       // y += sum_i coef[i] V(i), in order
   double nrm2(int a) { return sqrt(dot(a, a)); }
   void axpy(double al, int x, int y);
   void scale(double al, int x, int y);

@@ -152,6 +152,12 @@ struct HostOps {
     return s;
   }
   double nrm2(int a) { return std::sqrt(dot(a, a)); }
+  void mdot(int count, int w, double* h) {
+    for (int i = 0; i < count; ++i) h[i] = dot(V(i), w);
+  }
+  void maxpy(int count, const double* coef, int y) {
+    for (int i = 0; i < count; ++i) axpy(coef[i], V(i), y);
+  }
   void axpy(double al, int x, int y) { for (size_t e = 0; e < N; ++e) d(y)[e] = d(y)[e] + al * d(x)[e]; }
   void scale(double al, int x, int y) { for (size_t e = 0; e < N; ++e) d(y)[e] = al * d(x)[e]; }
   void copy(int x, int y) { vec[y] = vec[x]; }
