@@ -1,5 +1,5 @@
 """The coupled (5x5) line preconditioner of the oracle against a dense solve of the same
-block-tridiagonal chains (CPU).  The coupled form is the north-star variant of line_j:
+block-tridiagonal chains (CPU).  The coupled form is the 5x5 variant of line_j:
 the SA row gains its coupling to the mean flow; the reference has only the split form."""
 
 from __future__ import annotations
