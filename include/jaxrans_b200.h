@@ -323,6 +323,11 @@ int jr_newton_steps3d(jr_plan3d* plan, double* U, int32_t n_steps, double* cfl, 
  * friction from the laminar viscous flux at the wall.  Replaces force_coefficients
  * (src/jaxrans/post/forces.py:108-161) on a 3D atlas.  Synchronises. */
 int jr_forces3d(jr_plan3d* plan, const double* U, double area, double length, const double* centre, double* out);
+/* The loads on every wall face of a 3D case at U (device): out (host, n_walls x 7) = the
+ * gauge pressure, the face's area vector into the fluid (3), the laminar viscous force on
+ * the body (3) -- wall_loads (src/jaxrans/post/forces.py:48-68), for the surface
+ * distributions (src/jaxrans/post/forces.py:229-246).  Synchronises. */
+int jr_wall_loads3d(jr_plan3d* plan, const double* U, double* out);
 /* The wall distance of points (device, n_points x 3) to the nearest of n_faces wall faces
  * (device, n_faces x 4 x 3: the corners round each face, taken as a bilinear patch):
  * out (device, n_points).  Faces ranked by the distance to their two triangles, then the

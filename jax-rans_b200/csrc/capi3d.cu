@@ -297,6 +297,17 @@ int jr_forces3d(jr_plan3d* plan, const double* U, double area, double length, co
   return JR_OK;
 }
 
+int jr_wall_loads3d(jr_plan3d* plan, const double* U, double* out) {
+  if (!plan || !U || (!out && plan->dev.n_walls > 0)) return report_error(JR_EINVAL, "null argument");
+  const int nw = plan->dev.n_walls;
+  if (nw > 0) {
+    launch_wall_loads3(plan->dev, U, plan->loads, plan->A, plan->B, plan->st);
+    cudaMemcpyAsync(out, plan->loads, (size_t)nw * 7 * sizeof(double), cudaMemcpyDeviceToHost, plan->st);
+  }
+  if (cudaStreamSynchronize(plan->st) != cudaSuccess) return check3("jr_wall_loads3d");
+  return check3("jr_wall_loads3d");
+}
+
 int jr_launches3d(int64_t* out) {
   if (!out) return report_error(JR_EINVAL, "null argument");
   *out = launches3();

@@ -233,9 +233,45 @@ class DevicePlan3:
                                                      hist.ctypes.data), "jr_newton_steps3d")
         return u.cpu().numpy(), c.value, r.value, hist
 
+    # -- a state kept on the device between calls (the march's blocks)
+    def set_state(self, U, cfl: float, residual_norm: float = float("inf")) -> None:
+        """Keep ``U`` on the device with the step's CFL and previous |R|."""
+        (u,), _ = self._run("set_state", U)
+        self._state = [u, float(cfl), float(residual_norm)]
+
+    def get_state(self):
+        """``(U, cfl, residual_norm)`` of the kept state."""
+        u, cfl, res = self._state
+        return u.cpu().numpy(), cfl, res
+
+    def newton_block(self, n_steps: int) -> np.ndarray:
+        """``n_steps`` Newton steps on the kept state; |R| before each."""
+        u, cfl, res = self._state
+        c, r = C.c_double(cfl), C.c_double(res)
+        hist = np.zeros(n_steps)
+        _check(self.lib, self.lib.jr_newton_steps3d(self.handle, u.data_ptr(), int(n_steps), C.byref(c), C.byref(r),
+                                                     hist.ctypes.data), "jr_newton_steps3d")
+        self._state = [u, c.value, r.value]
+        return hist
+
+    def state_wall_loads(self) -> np.ndarray:
+        """Per wall face of the kept state: gauge pressure, area vector into the fluid (3),
+        laminar viscous force (3) (``jr_wall_loads3d``)."""
+        out = np.zeros((len(self.plan.walls.cell), 7))
+        _check(self.lib, self.lib.jr_wall_loads3d(self.handle, self._state[0].data_ptr(), out.ctypes.data),
+               "jr_wall_loads3d")
+        return out
+
+    def state_forces(self, area: float, length: float = 1.0, centre=(0.25, 0.0, 0.0)) -> np.ndarray:
+        """``(cl, cd, cm, cd_friction)`` of the kept state."""
+        return self._forces_at(self._state[0], area, length, centre)
+
     def forces(self, U, area: float, length: float = 1.0, centre=(0.25, 0.0, 0.0)) -> np.ndarray:
         """``(cl, cd, cm, cd_friction)`` at ``U`` (``jr_forces3d``)."""
         (u,), _ = self._run("jr_forces3d", U)
+        return self._forces_at(u, area, length, centre)
+
+    def _forces_at(self, u, area, length, centre) -> np.ndarray:
         c = np.ascontiguousarray(centre, dtype=np.float64)
         out = np.zeros(4)
         _check(self.lib, self.lib.jr_forces3d(self.handle, u.data_ptr(), float(area), float(length), c.ctypes.data,

@@ -67,7 +67,7 @@ def write_result(result, directory=None, extra: dict | None = None) -> Path:
                header="iteration cl", fmt=["%d", "%.12e"])
     if result.wall is not None:
         surface = result.surface()
-        names = {"x": "x_over_c", "y": "y_over_c"}
+        names = {"x": "x_over_c", "y": "y_over_c", "z": "z_over_c", "x_streamwise": "x_streamwise_over_c"}
         np.savetxt(directory / f"{name}_surface.dat", np.column_stack([np.asarray(v) for v in surface.values()]),
                    header=" ".join(names.get(k, k) for k in surface), fmt="%.12e")
     blocks = result.grid.unpack(np.asarray(result.U))

@@ -127,6 +127,9 @@ class Result:
         along the downstream-pointing tangent (``src/jaxrans/post/forces.py:203-226``)."""
         if self.wall is None:
             raise ValueError("this result carries no wall loads")
+        if getattr(self.grid, "dim", 2) == 3:
+            from .solver3d import surface3
+            return surface3(np.asarray(self.wall), self.grid, self.case.flow)
         p, sx, sy, fx, fy = (np.asarray(self.wall)[:, k] for k in range(5))
         q = 0.5 * self.case.flow.mach ** 2
         walls = self.grid.walls

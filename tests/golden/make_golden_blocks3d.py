@@ -17,7 +17,8 @@ Three grids, written as unformatted Plot3D files and read by the reference throu
   axis -- with far field all round; inviscid.
 
 For each: the assembled sides, the canvas, the reference's residual, first-order J.v and
-wave speeds, and for the wings the line preconditioner and the forces.
+wave speeds, and for the wings the line preconditioner, the forces and the surface
+distributions.
 
     python tests/golden/make_golden_blocks3d.py
 
@@ -46,7 +47,7 @@ import jax  # noqa: E402  (the stand-in)
 import jax.numpy as jnp  # noqa: E402
 from jaxrans.case.loader import load_case  # noqa: E402
 from jaxrans.numerics.residual import make_residual  # noqa: E402
-from jaxrans.post.forces import integrate_forces  # noqa: E402
+from jaxrans.post.forces import integrate_forces, surface  # noqa: E402
 from jaxrans.solvers import preconditioners as pre  # noqa: E402
 
 from jaxrans_b200.geometry import section_source  # noqa: E402
@@ -157,6 +158,8 @@ def main() -> int:
             out[f"{name}_prec_z"] = np.asarray(prepare(U, lam, cfl)(jnp.asarray(r)))
             f = integrate_forces(U, atlas, flow, case.grid_spec.force_reference())
             out[f"{name}_forces"] = np.array([f.cl, f.cd, f.cm, f.cd_friction])
+            for key, values in surface(U, atlas, flow).items():
+                out[f"{name}_surface_{key}"] = np.asarray(values)
         print(f"{name}: {len(blocks)} blocks, {atlas.shape} canvas, {atlas.cells} cells")
     np.savez_compressed(HERE / "blocks3d.npz", **out)
     return 0

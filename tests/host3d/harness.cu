@@ -217,19 +217,26 @@ extern "C" int jr3_host_newton_steps(const jr_plan3d_desc* d, const double* conf
   return 0;
 }
 
-extern "C" int jr3_host_forces(const jr_plan3d_desc* d, const double* U, double area, double length,
-                               const double* centre, double* out) {
+// the 7 loads of every wall face (n_walls x 7) from the ghost-filled state
+extern "C" int jr3_host_wall_loads(const jr_plan3d_desc* d, const double* U, double* loads) {
   const Plan3Dev p = plan_of(d);
   const int n = p.NI * p.NJ * p.NK;
-  std::vector<double> A((size_t)p.nvar * n), B((size_t)p.nvar * n), loads((size_t)p.n_walls * 7);
+  std::vector<double> A((size_t)p.nvar * n), B((size_t)p.nvar * n);
   for (int c = 0; c < n; ++c) prim_cell(p, U, (const double*)nullptr, A.data(), c);
   for (int s = 0; s < p.n_stages; ++s) {
     B = A;
     for (int r = p.stage_off[s]; r < p.stage_off[s + 1]; ++r) ghost_record(p, A.data(), B.data(), r);
     std::swap(A, B);
   }
-  for (int w = 0; w < p.n_walls; ++w) wall_load(p, A.data(), w, loads.data() + (size_t)7 * w);
-  force_coefficients3(p.P, p.n_walls, loads.data(), d->wall_mid, area, length, centre, out);
+  for (int w = 0; w < p.n_walls; ++w) wall_load(p, A.data(), w, loads + (size_t)7 * w);
+  return 0;
+}
+
+extern "C" int jr3_host_forces(const jr_plan3d_desc* d, const double* U, double area, double length,
+                               const double* centre, double* out) {
+  std::vector<double> loads((size_t)d->n_walls * 7);
+  jr3_host_wall_loads(d, U, loads.data());
+  force_coefficients3(plan_of(d).P, d->n_walls, loads.data(), d->wall_mid, area, length, centre, out);
   return 0;
 }
 

@@ -226,7 +226,7 @@ def test_kernel_bodies_give_the_reference_line_solve_and_forces(harness, z, case
 
 
 class HostDevice3:
-    """The ``DevicePlan3`` methods ``march3d`` uses, over the host harness."""
+    """The ``DevicePlan3`` state methods ``march3d`` uses, over the host harness."""
 
     def __init__(self, harness, case, desc):
         cfg = case.implicit
@@ -246,6 +246,25 @@ class HostDevice3:
                                               hist.ctypes.data) == 0
         self.calls += 1
         return U, c.value, r.value, hist
+
+    def set_state(self, U, cfl, res):
+        self.state = (np.ascontiguousarray(U, dtype=np.float64).copy(), cfl, res)
+
+    def get_state(self):
+        return self.state
+
+    def newton_block(self, n):
+        U, cfl, res, hist = self.newton_steps(*self.state[:1], n, *self.state[1:])
+        self.state = (U, cfl, res)
+        return hist
+
+    def state_wall_loads(self):
+        out = np.zeros((self.desc.n_walls, 7))
+        assert self.lib.jr3_host_wall_loads(C.addressof(self.desc), self.state[0].ctypes.data, out.ctypes.data) == 0
+        return out
+
+    def state_forces(self, area, length, centre):
+        return self.forces(self.state[0], area, length, centre)
 
     def forces(self, U, area, length, centre):
         U = np.ascontiguousarray(U, dtype=np.float64)
@@ -276,6 +295,7 @@ def test_march3d_runs_blocks_to_the_iteration_limit(harness, z, cases, described
     fields = np.load(out / f"{case.name}_fields.npz")
     assert fields["U_0"].shape == (5, 8, 4, 6) and "z_node_0" in fields
     assert (out / f"{case.name}_block0.vts").read_bytes().startswith(b"<?xml")
+    assert not (out / f"{case.name}_surface.dat").exists()      # the pole case has no wall
 
 
 @pytest.mark.parametrize("name", ["split", "wing4"])
@@ -294,3 +314,22 @@ def test_wall_distance_kernel_body_gives_the_reference_distance(harness, z, case
     assert np.array_equal(out, every)          # the sphere bound skips only faces the ranking refuses
     assert np.allclose(out, z[f"{name}_distance"][plan.interior], rtol=1e-12, atol=1e-15)
     assert np.allclose(out, plan.distance[plan.interior], rtol=1e-12, atol=1e-15)
+
+
+@pytest.mark.parametrize("name", ["split", "wing4"])
+def test_surface_distributions_match_the_reference(harness, z, cases, described, name):
+    """Per wall face: block, running position, centre, cp and the skin-friction vector
+    (``solver3d.surface3`` on the kernels' wall loads), face by face in the reference's order."""
+    from jaxrans_b200.solver3d import surface3
+    case, plan = cases[name]
+    desc, _ = described[name]
+    U = np.ascontiguousarray(z[f"{name}_U"])
+    loads = np.zeros((desc.n_walls, 7))
+    assert harness.jr3_host_wall_loads(C.addressof(desc), U.ctypes.data, loads.ctypes.data) == 0
+    got = surface3(loads, plan, case.flow)
+    keys = sorted(k[len(f"{name}_surface_"):] for k in z.files if k.startswith(f"{name}_surface_"))
+    assert sorted(got) == keys
+    for key in keys:
+        ref = z[f"{name}_surface_{key}"]
+        scale = max(float(np.abs(ref).max()), 1e-300)
+        assert np.allclose(got[key], ref, rtol=0.0, atol=1e-11 * scale), key
