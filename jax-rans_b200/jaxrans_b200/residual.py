@@ -4,7 +4,8 @@ Mirrors ``make_residual(grid, flow, numerics, first_order=False, freestream=None
 distance=None, mu_inf=None) -> ResidualOperator`` (``src/jaxrans/numerics/residual.py:
 207-334``): ``.residual(U)``, ``.wave_speeds(U)``, ``.norm(R)`` and ``.initial_state()``
 on canvas fields ``(nvar, NI, NJ)``.  Fields may be NumPy arrays (copied to the device
-and back) or float64 CUDA tensors (used in place).
+and back) or float64 CUDA tensors (used in place).  On a 3D plan (``plan3d.Plan3``) the
+same operator runs the 3D kernels on fields ``(nvar, NI, NJ, NK)`` (NumPy arrays).
 """
 
 from __future__ import annotations
@@ -49,6 +50,9 @@ class ResidualOperator:
         return float(np.sqrt(np.sum(w * R[variable] ** 2) / np.sum(w)))
 
     def initial_state(self) -> np.ndarray:
+        if getattr(self.plan, "dim", 2) == 3:
+            from .solver3d import freestream_state3
+            return freestream_state3(self, self.plan)
         q = freestream_primitive(self.flow)
         g = self.flow.gamma
         rho, u, v, p = q[:4]
@@ -67,6 +71,15 @@ def make_residual(grid: Plan, flow: FlowConditions, numerics: NumericsConfig, fi
         raise ValueError("freestream / mu_inf overrides are not implemented in this build; set them in flow")
     if distance is not None:
         grid.distance = np.asarray(distance, dtype=np.float64)
+    if getattr(grid, "dim", 2) == 3:
+        from .config import freestream_primitive3
+        from .native3d import DevicePlan3
+        if flow.turbulence is not None and grid.distance is None:
+            raise ValueError("a 3D plan for the SA model needs its wall distance (build_plan3d with_distance)")
+        device = DevicePlan3(grid, np.array(freestream_primitive3(flow)), flow.gamma, numerics.flux, numerics.limiter,
+                             numerics.kappa, None if flow.inviscid else flow.mu_inf, flow.sutherland_ratio,
+                             ImplicitConfig())
+        return ResidualOperator(grid, flow, numerics, first_order, device)
     if flow.turbulence is not None and grid.distance is None:
         from .plan import wall_distance
         grid.distance = grid.pack(wall_distance(grid.mesh, grid.walls), 1.0)

@@ -171,3 +171,18 @@ def test_mixed_line_solve3d_on_the_device(cuda, device3d):
         mixed_dev.close()
     err = max(float(np.abs(mixed[k] - exact[k]).max() / np.abs(exact[k]).max()) for k in range(exact.shape[0]))
     assert 0.0 < err < 1e-4
+
+
+def test_make_residual_on_a_3d_plan(cuda, blocks3d):
+    """``make_residual`` on a 3D plan: the reference's operator surface over the 3D kernels."""
+    from jaxrans_b200.residual import make_residual
+    z, cases = blocks3d
+    case, plan = cases["wing4"]
+    op = make_residual(plan, case.flow, case.numerics)
+    inside = plan.interior
+    R = op.residual(z["wing4_U"])
+    for k in range(R.shape[0]):
+        ref = z["wing4_R2"][k][inside]
+        assert np.abs(R[k][inside] - ref).max() <= 1e-12 * np.abs(ref).max()
+    U0 = op.initial_state()
+    assert U0.shape == (6,) + plan.shape and np.isfinite(op.norm(op.residual(U0)))
