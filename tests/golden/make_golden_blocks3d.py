@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """Generate the multi-block and pole 3D fixtures by running the reference solver itself.
 
-Three grids, written as unformatted Plot3D files and read by the reference through its own
+Three grids (five cases), written as unformatted Plot3D files and read by the reference through its own
 3D loader (``grid: file``, box patch rules), under the NumPy stand-in in
 ``tests/golden/jaxshim`` (as ``make_golden3d.py`` does):
 
@@ -12,6 +12,8 @@ Three grids, written as unformatted Plot3D files and read by the reference throu
 * ``wing4``: the four-block C-H grid of the swept, tapered wing with its tip region
   (``jaxrans_b200.grid3d.wing_ch_blocks``: wing and beyond-tip blocks, lower and upper
   halves; past the tip an elliptic cap, then a sheet facing itself), coarse; SA RANS.
+* ``split_laminar``: the split grid, laminar with Sutherland's law, Roe with minmod;
+  ``wing4_euler``: the four-block wing inviscid, HLLC with unlimited MUSCL, kappa 1/3.
 * ``pole``: a cylinder of cells round the z axis -- ``i`` the azimuth (an O seam), ``j``
   the radius from the axis (``j_min`` collapsed to a line: a pole), ``k`` along the
   axis -- with far field all round; inviscid.
@@ -110,8 +112,38 @@ def wing4_case() -> dict:
     return doc
 
 
+def laminar_case() -> dict:
+    """The split grid, laminar (Re 1e4, Sutherland's law at 540 R): 5 variables, viscous, no SA."""
+    doc = split_case()
+    doc["general"]["case_name"] = "split_laminar"
+    doc.pop("turbulence")
+    doc["freestream"] = {"mach": 0.5, "alpha_deg": 4.0, "reynolds": 1e4, "temperature": 540.0}
+    doc["material_properties"] = {"dynamic_viscosity": "sutherland", "sutherland_temperature": 198.6}
+    return doc
+
+
+LAMINAR_NUMERICAL = {"convective_fluxes": {"riemann_solver": "roe", "limiter": "minmod"},
+                     "time_integration": {"solver": "implicit"}}
+
+
+def euler_case() -> dict:
+    """The four-block wing, inviscid (slip walls), unlimited MUSCL with kappa = 1/3."""
+    doc = wing4_case()
+    doc["general"]["case_name"] = "wing4_euler"
+    doc.pop("turbulence")
+    doc["freestream"] = {"mach": 0.8, "alpha_deg": 2.5}
+    doc["boundary_conditions"]["wall"] = {"type": "slip_wall"}
+    return doc
+
+
+EULER_NUMERICAL = {"convective_fluxes": {"riemann_solver": "hllc", "limiter": "none", "muscl_kappa": 1.0 / 3.0},
+                   "time_integration": {"solver": "implicit"}}
+
 GRIDS = {"split": (split_blocks, split_case(), NUMERICAL), "pole": (pole_blocks, POLE_CASE, POLE_NUMERICAL),
-         "wing4": (lambda: wing4_grid().blocks, wing4_case(), NUMERICAL)}
+         "wing4": (lambda: wing4_grid().blocks, wing4_case(), NUMERICAL),
+         "split_laminar": (split_blocks, laminar_case(), LAMINAR_NUMERICAL),
+         "wing4_euler": (lambda: wing4_grid().blocks, euler_case(), EULER_NUMERICAL)}
+WALLED = ("split", "wing4", "split_laminar", "wing4_euler")
 
 
 def main() -> int:
@@ -140,6 +172,13 @@ def main() -> int:
         if op.distance is not None:
             out[f"{name}_distance"] = np.asarray(op.distance)
         U = perturbed(op.initial_state(), 5, 1e-2)
+        if numerical["convective_fluxes"]["riemann_solver"] == "roe":
+            # a spanwise velocity everywhere: with none, V.n is zero to round-off on the faces
+            # normal to the span, where Roe's |V.n| has its kink, and the tangent there is
+            # decided by the sign of round-off
+            U = np.asarray(U).copy()
+            U[2] = U[2] + 2e-2 * U[0] * np.random.default_rng(9).uniform(-1.0, 1.0, U[0].shape)
+            U = jnp.asarray(U)
         out[f"{name}_U"] = np.asarray(U)
         out[f"{name}_R2"] = np.asarray(op.residual(U))
         R1, jvp = jax.linearize(jop.residual, U)
@@ -150,7 +189,7 @@ def main() -> int:
         lam = op.wave_speeds(U)
         for a in range(3):
             out[f"{name}_lam{a}"] = np.asarray(lam[a])
-        if name in ("split", "wing4"):
+        if name in WALLED:
             cfl = jnp.asarray(25.0)
             prepare = pre.get_preconditioner("line_j")(atlas, flow.gamma, op.viscosity, op.model, op.distance)
             r = np.where(atlas.interior, rng.standard_normal(U.shape), 0.0)

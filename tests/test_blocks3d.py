@@ -5,8 +5,10 @@ and solver (tests/golden/blocks3d.npz, made by tests/golden/make_golden_blocks3d
 * a case directory on such a file loads (``load_case``) to a 3D plan on the reference's
   canvas;
 * the 3D kernels' bodies, run on the host by the test harness, give the reference's
-  residual, J.v, wave speeds, line preconditioner and forces across interfaces of every
-  orientation and across a pole;
+  residual, J.v, wave speeds, line preconditioner, forces and surface distributions
+  across interfaces of every orientation and across a pole, for SA RANS (HLLC, smooth
+  van Albada), laminar flow with Sutherland's law (Roe, minmod) and inviscid flow
+  (HLLC, unlimited MUSCL with kappa 1/3);
 * ``solver3d.march3d`` drives blocks of Newton steps and the exit test over a device
   stand-in built on the same harness."""
 
@@ -25,7 +27,8 @@ from jaxrans_b200.gridfile import PatchRule
 from jaxrans_b200.gridfile3d import assemble3d, is_3d
 
 GOLDEN = Path(__file__).resolve().parent / "golden" / "blocks3d.npz"
-NAMES = ("split", "wing4", "pole")
+NAMES = ("split", "wing4", "pole", "split_laminar", "wing4_euler")
+WALLED = ("split", "wing4", "split_laminar", "wing4_euler")
 
 
 @pytest.fixture(scope="module")
@@ -208,7 +211,7 @@ def test_kernel_bodies_give_the_reference_wave_speeds(harness, z, cases, describ
         assert np.allclose(part[used], ref[used], rtol=1e-13, atol=0.0)
 
 
-@pytest.mark.parametrize("name", ["split", "wing4"])
+@pytest.mark.parametrize("name", WALLED)
 def test_kernel_bodies_give_the_reference_line_solve_and_forces(harness, z, cases, described, name):
     case, plan = cases[name]
     desc, _ = described[name]
@@ -316,7 +319,7 @@ def test_wall_distance_kernel_body_gives_the_reference_distance(harness, z, case
     assert np.allclose(out, plan.distance[plan.interior], rtol=1e-12, atol=1e-15)
 
 
-@pytest.mark.parametrize("name", ["split", "wing4"])
+@pytest.mark.parametrize("name", WALLED)
 def test_surface_distributions_match_the_reference(harness, z, cases, described, name):
     """Per wall face: block, running position, centre, cp and the skin-friction vector
     (``solver3d.surface3`` on the kernels' wall loads), face by face in the reference's order."""
