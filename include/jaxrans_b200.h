@@ -282,6 +282,7 @@ typedef struct jr_plan3d_desc {
   /* 0: the line factor and apply in FP64; 1: in FP32 (the mixed form; Krylov vectors,
    * residual, J.v and update stay FP64) */
   int32_t line_precision;
+  double c_cr1;                 /* QCR2000's c_cr1 on the SA model's stress (0: off; TMR's 0.3) */
 } jr_plan3d_desc;
 
 /* Build a 3D plan (device copies of the tables, work buffers, a stream).  Every record

@@ -19,6 +19,7 @@ struct Physics3 {
   double mu_inf;       // M / Re (<= 0: inviscid)
   double sutherland;   // S / T_inf, < 0: constant viscosity
   double kappa;        // MUSCL kappa (limiter 4)
+  double c_cr1;        // QCR2000 (0: off)
   int flux;            // 0 hllc, 1 roe
   int limiter;         // 0 none, 1 minmod, 2 van_albada, 3 van_albada_smooth, 4 kappa family
   double q_inf[NV3_MAX];   // primitive freestream

@@ -11,6 +11,7 @@ inline void physics3_from_desc(Physics3& P, const jr_plan3d_desc* d) {
   P.mu_inf = d->mu_inf > 0.0 ? d->mu_inf : 0.0;
   P.sutherland = d->sutherland;
   P.kappa = d->kappa;
+  P.c_cr1 = d->c_cr1;
   P.flux = d->flux;
   P.limiter = d->limiter;
   for (int v = 0; v < NV3_MAX; ++v) P.q_inf[v] = v < d->nvar ? d->q_inf[v] : 0.0;

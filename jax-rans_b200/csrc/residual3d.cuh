@@ -179,6 +179,33 @@ __host__ __device__ __forceinline__ void load_cell(const Plan3Dev& p, const T* Q
 
 // The net flux through face (fi, fj, fk) of family a (inviscid minus viscous), and for
 // SA the row's face flux (upwind on the mass flux, minus the diffusion).
+// QCR2000's addition to the stress (src/jaxrans/physics/spalart_allmaras.py:197-216):
+// -c_cr1 (O_ik tau_jk + O_jk tau_ik), O = (grad V - grad V^T) / |grad V| (0 where grad V
+// is 0, and so its tangent), tau = mu_t (grad V + grad V^T - 2/3 div V I); with
+// gv[a][b] = d v_a / d x_b = grad[b][a].
+template <class T>
+__host__ __device__ __forceinline__ void qcr_extra(const T grad[3][5], const T& mut, double c_cr1, T extra[3][3]) {
+  T gv[3][3];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) gv[a][b] = grad[b][a];
+  T square = gv[0][0] * gv[0][0];
+  for (int e = 1; e < 9; ++e) square = square + gv[e / 3][e % 3] * gv[e / 3][e % 3];
+  const bool positive = val(square) > 0.0;
+  const T norm = positive ? dsqrt(square) : cst<T>(1.0);
+  const T div = (gv[0][0] + gv[1][1]) + gv[2][2];
+  T rot[3][3], tau[3][3];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      rot[a][b] = (gv[a][b] - gv[b][a]) / norm;
+      tau[a][b] = mut * (gv[a][b] + gv[b][a] - (a == b ? (2.0 / 3.0) * div : cst<T>(0.0)));
+    }
+  T prod[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) prod[i][j] = (rot[i][0] * tau[j][0] + rot[i][1] * tau[j][1]) + rot[i][2] * tau[j][2];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) extra[a][b] = -c_cr1 * (prod[a][b] + prod[b][a]);
+}
+
 template <class T, bool VISC, bool SA>
 __host__ __device__ void face_flux(const Plan3Dev& p, const T* Q, int a, int fi, int fj, int fk, bool first_order, T F[NV3_MAX]) {
   const Physics3& P = p.P;
@@ -221,6 +248,7 @@ __host__ __device__ void face_flux(const Plan3Dev& p, const T* Q, int a, int fi,
     T grad[3][5];
     face_gradient(p, Q, a, fi, fj, fk, nphi, grad);
     // face means of the two cells either side
+    T extra[3][3];
     T vel[3], Tl = g * qm[4] / qm[0], Th = g * qp[4] / qp[0];
     for (int m = 0; m < 3; ++m) vel[m] = 0.5 * (qm[1 + m] + qp[1 + m]);
     T Tf = 0.5 * (Tl + Th);
@@ -233,8 +261,9 @@ __host__ __device__ void face_flux(const Plan3Dev& p, const T* Q, int a, int fi,
       T mut = eddy_viscosity(P.sa, fa[0], fa[5] * P.mu_inf, mu_f / fa[0]);
       mu = mu + mut;
       k = k + mut / (PR_TURBULENT * (g - 1.0));
+      if (P.c_cr1 != 0.0) qcr_extra(grad, mut, P.c_cr1, extra);
     }
-    // gv[c][d] = d v_c / d x_d
+    // grad[d][c] = d v_c / d x_d (the stress is symmetric in the pair)
     T div = grad[0][0] + grad[1][1] + grad[2][2];
     T ttd = (2.0 / 3.0) * div;
     T force[3];
@@ -247,6 +276,7 @@ __host__ __device__ void face_flux(const Plan3Dev& p, const T* Q, int a, int fi,
           const int lo = c < d ? c : d, hi = c < d ? d : c;
           tau[d] = mu * (grad[hi][lo] + grad[lo][hi]);
         }
+        if (SA && P.c_cr1 != 0.0) tau[d] = tau[d] + extra[c][d];
       }
       force[c] = tau[0] * s[0] + tau[1] * s[1] + tau[2] * s[2];
     }

@@ -39,7 +39,7 @@ class Plan3Desc(C.Structure):
         ("krylov_tol", C.c_double), ("krylov_success", C.c_double), ("max_relative_update", C.c_double),
         ("krylov_subspace", C.c_int32), ("krylov_restarts", C.c_int32), ("preconditioner", C.c_int32),
         ("n_walls", C.c_int32), ("wall_cell", _i32p), ("wall_family", _i32p), ("wall_face", _i32p),
-        ("wall_into", _f64p), ("wall_mid", _f64p), ("line_precision", C.c_int32),
+        ("wall_into", _f64p), ("wall_mid", _f64p), ("line_precision", C.c_int32), ("c_cr1", C.c_double),
     ]
 
 
@@ -101,7 +101,7 @@ def apply_records(records: Records, q: np.ndarray) -> np.ndarray:
 
 
 def describe(plan: Plan3, q_inf, gamma: float, flux: str, limiter: str, kappa: float = 0.0,
-             mu_inf: float | None = None, sutherland: float | None = None, implicit=None):
+             mu_inf: float | None = None, sutherland: float | None = None, implicit=None, c_cr1: float = 0.0):
     """``(jr_plan3d_desc, arrays it points into)`` for ``plan``, the physics and the
     implicit solver's settings (``config.ImplicitConfig``; its defaults if None); keep
     the arrays alive while the descriptor is used."""
@@ -154,6 +154,7 @@ def describe(plan: Plan3, q_inf, gamma: float, flux: str, limiter: str, kappa: f
     d.krylov_subspace, d.krylov_restarts = imp.krylov_subspace, imp.krylov_restarts
     d.preconditioner = {"none": 0, "line_j": 1}[imp.preconditioner]
     d.line_precision = 1 if imp.precision == "mixed" else 0
+    d.c_cr1 = float(c_cr1)
     W = plan.walls
     d.n_walls = len(W.cell)
     d.wall_cell = ptr(arr(W.cell, np.int32), _i32p)
@@ -169,7 +170,8 @@ class DevicePlan3:
     NK)`` float64 NumPy arrays in and out)."""
 
     def __init__(self, plan: Plan3, q_inf, gamma: float, flux: str, limiter: str, kappa: float = 0.0,
-                 mu_inf: float | None = None, sutherland: float | None = None, implicit=None, library=None):
+                 mu_inf: float | None = None, sutherland: float | None = None, implicit=None, library=None,
+                 c_cr1: float = 0.0):
         self.lib = load_library(library)
         self.plan = plan
         self.q_inf, self.gamma, self.flux, self.limiter = np.asarray(q_inf, dtype=np.float64), gamma, flux, limiter
@@ -178,7 +180,7 @@ class DevicePlan3:
         self.implicit = implicit if implicit is not None else ImplicitConfig()
         self.nvar = len(q_inf)
         self.shape = (self.nvar,) + plan.shape
-        d, keep = describe(plan, q_inf, gamma, flux, limiter, kappa, mu_inf, sutherland, implicit)
+        d, keep = describe(plan, q_inf, gamma, flux, limiter, kappa, mu_inf, sutherland, implicit, c_cr1)
         handle = C.c_void_p()
         _check(self.lib, self.lib.jr_plan3d_create(C.byref(d), C.byref(handle)), "jr_plan3d_create")
         self.handle = handle

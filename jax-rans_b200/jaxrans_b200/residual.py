@@ -78,7 +78,7 @@ def make_residual(grid: Plan, flow: FlowConditions, numerics: NumericsConfig, fi
             raise ValueError("a 3D plan for the SA model needs its wall distance (build_plan3d with_distance)")
         device = DevicePlan3(grid, np.array(freestream_primitive3(flow)), flow.gamma, numerics.flux, numerics.limiter,
                              numerics.kappa, None if flow.inviscid else flow.mu_inf, flow.sutherland_ratio,
-                             ImplicitConfig())
+                             ImplicitConfig(), c_cr1=0.3 if flow.turbulence == "sa_noft2_qcr" else 0.0)
         return ResidualOperator(grid, flow, numerics, first_order, device)
     if flow.turbulence is not None and grid.distance is None:
         from .plan import wall_distance

@@ -26,7 +26,7 @@ def physics3(case) -> dict:
     flow, num = case.flow, case.numerics
     return {"q_inf": np.array(freestream_primitive3(flow)), "gamma": flow.gamma, "flux": num.flux,
             "limiter": num.limiter, "kappa": num.kappa, "mu_inf": None if flow.inviscid else flow.mu_inf,
-            "sutherland": flow.sutherland_ratio}
+            "sutherland": flow.sutherland_ratio, "c_cr1": 0.3 if flow.turbulence == "sa_noft2_qcr" else 0.0}
 
 
 def describe_case(case, plan: Plan3):

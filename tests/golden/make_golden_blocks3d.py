@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """Generate the multi-block and pole 3D fixtures by running the reference solver itself.
 
-Three grids (five cases), written as unformatted Plot3D files and read by the reference through its own
+Three grids (six cases), written as unformatted Plot3D files and read by the reference through its own
 3D loader (``grid: file``, box patch rules), under the NumPy stand-in in
 ``tests/golden/jaxshim`` (as ``make_golden3d.py`` does):
 
@@ -13,6 +13,7 @@ Three grids (five cases), written as unformatted Plot3D files and read by the re
   (``jaxrans_b200.grid3d.wing_ch_blocks``: wing and beyond-tip blocks, lower and upper
   halves; past the tip an elliptic cap, then a sheet facing itself), coarse; SA RANS.
 * ``split_laminar``: the split grid, laminar with Sutherland's law, Roe with minmod;
+  ``split_qcr``: the split grid with SA-noft2-QCR2000;
   ``wing4_euler``: the four-block wing inviscid, HLLC with unlimited MUSCL, kappa 1/3.
 * ``pole``: a cylinder of cells round the z axis -- ``i`` the azimuth (an O seam), ``j``
   the radius from the axis (``j_min`` collapsed to a line: a pole), ``k`` along the
@@ -136,14 +137,23 @@ def euler_case() -> dict:
     return doc
 
 
+def qcr_case() -> dict:
+    """The split grid with SA-noft2-QCR2000 (the quadratic constitutive relation)."""
+    doc = split_case()
+    doc["general"]["case_name"] = "split_qcr"
+    doc["turbulence"] = {"model": "sa_noft2_qcr"}
+    return doc
+
+
 EULER_NUMERICAL = {"convective_fluxes": {"riemann_solver": "hllc", "limiter": "none", "muscl_kappa": 1.0 / 3.0},
                    "time_integration": {"solver": "implicit"}}
 
 GRIDS = {"split": (split_blocks, split_case(), NUMERICAL), "pole": (pole_blocks, POLE_CASE, POLE_NUMERICAL),
          "wing4": (lambda: wing4_grid().blocks, wing4_case(), NUMERICAL),
          "split_laminar": (split_blocks, laminar_case(), LAMINAR_NUMERICAL),
-         "wing4_euler": (lambda: wing4_grid().blocks, euler_case(), EULER_NUMERICAL)}
-WALLED = ("split", "wing4", "split_laminar", "wing4_euler")
+         "wing4_euler": (lambda: wing4_grid().blocks, euler_case(), EULER_NUMERICAL),
+         "split_qcr": (split_blocks, qcr_case(), NUMERICAL)}
+WALLED = ("split", "wing4", "split_laminar", "wing4_euler", "split_qcr")
 
 
 def main() -> int:

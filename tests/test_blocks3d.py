@@ -7,7 +7,7 @@ and solver (tests/golden/blocks3d.npz, made by tests/golden/make_golden_blocks3d
 * the 3D kernels' bodies, run on the host by the test harness, give the reference's
   residual, J.v, wave speeds, line preconditioner, forces and surface distributions
   across interfaces of every orientation and across a pole, for SA RANS (HLLC, smooth
-  van Albada), laminar flow with Sutherland's law (Roe, minmod) and inviscid flow
+  van Albada; with and without QCR2000), laminar flow with Sutherland's law (Roe, minmod) and inviscid flow
   (HLLC, unlimited MUSCL with kappa 1/3);
 * ``solver3d.march3d`` drives blocks of Newton steps and the exit test over a device
   stand-in built on the same harness."""
@@ -27,8 +27,8 @@ from jaxrans_b200.gridfile import PatchRule
 from jaxrans_b200.gridfile3d import assemble3d, is_3d
 
 GOLDEN = Path(__file__).resolve().parent / "golden" / "blocks3d.npz"
-NAMES = ("split", "wing4", "pole", "split_laminar", "wing4_euler")
-WALLED = ("split", "wing4", "split_laminar", "wing4_euler")
+NAMES = ("split", "wing4", "pole", "split_laminar", "wing4_euler", "split_qcr")
+WALLED = ("split", "wing4", "split_laminar", "wing4_euler", "split_qcr")
 
 
 @pytest.fixture(scope="module")

@@ -104,7 +104,7 @@ def blocks3d(tmp_path_factory):
     from jaxrans_b200.grid3d import write_plot3d
     z = np.load(BLOCKS)
     out = {}
-    for name in ("split", "wing4", "pole", "split_laminar", "wing4_euler"):
+    for name in ("split", "wing4", "pole", "split_laminar", "wing4_euler", "split_qcr"):
         d = tmp_path_factory.mktemp(name)
         doc = json.loads(str(z[f"{name}_case_json"]))
         write_plot3d(d / "grid.x", [z[f"{name}_raw{b}"] for b in range(int(z[f"{name}_n_blocks"]))])
@@ -115,7 +115,7 @@ def blocks3d(tmp_path_factory):
     return z, out
 
 
-@pytest.mark.parametrize("name", ["split", "wing4", "pole", "split_laminar", "wing4_euler"])
+@pytest.mark.parametrize("name", ["split", "wing4", "pole", "split_laminar", "wing4_euler", "split_qcr"])
 def test_blocks3d_residual_and_jvp_on_the_device(cuda, blocks3d, name):
     from jaxrans_b200.solver3d import device3_for
     z, cases = blocks3d
