@@ -234,6 +234,9 @@ class Case:
             if unsupported:
                 raise CaseError(f"boundary condition(s) {unsupported} are not implemented on the 3D path; "
                                 f"it has {sorted(KINDS_3D)}")
+            if self.numerics.far_field != "characteristic":
+                raise CaseError("the far-field 'model' point_vortex is a 2D model (a vortex in the plane); "
+                                "a 3D case takes the freestream far field")
             return build_plan3d(mesh, with_distance=turbulent)
         return build_plan(mesh, self.numerics.n_ghost, with_distance=turbulent)
 

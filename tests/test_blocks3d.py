@@ -151,6 +151,10 @@ def test_case_loader_refuses_what_the_3d_path_lacks(z, tmp_path):
     (d / "case.json").write_text(json.dumps(doc))
     with pytest.raises(CaseError, match="3D path"):
         load_case(d).grid()
+    doc["boundary_conditions"]["farfield"] = {"type": "far_field", "model": "point_vortex"}
+    (d / "case.json").write_text(json.dumps(doc))
+    with pytest.raises(CaseError, match="2D model"):
+        load_case(d).grid()
 
 
 def rows_rel(a, b, inside):
