@@ -271,7 +271,7 @@ typedef struct jr_plan3d_desc {
   /* implicit solver (as jr_plan_desc; preconditioner 0 none, 1 line_j) */
   double cfl_max, cfl_growth, cfl_cutback, cfl_min;
   double krylov_tol, krylov_success, max_relative_update;   /* max_relative_update <= 0: none */
-  int32_t krylov_subspace, krylov_restarts, preconditioner;
+  int32_t krylov_subspace, krylov_restarts, preconditioner;   /* 0 none, 1 line_j, 2 line_j coupled (6x6) */
   /* wall faces (the forces) */
   int32_t n_walls;
   const int32_t* wall_cell;     /* the block cell on the face */

@@ -178,6 +178,7 @@ int jr_plan3d_create(const jr_plan3d_desc* d, jr_plan3d** out) {
     return report_error(JR_EINVAL, "line_precision must be 0 (FP64) or 1 (FP32)");
   }
   dv.line_fp32 = d->line_precision;
+  dv.line_coupled = d->preconditioner == 2;
   if (n_links > 0) {
     void* sc = nullptr;
     if (cudaMalloc(&sc, n_links * FACTOR3 * (dv.line_fp32 ? sizeof(float) : sizeof(double))) != cudaSuccess) {
@@ -195,9 +196,9 @@ int jr_plan3d_create(const jr_plan3d_desc* d, jr_plan3d** out) {
   p->allocs.push_back(p->B);
   // the Newton step's configuration and vectors
   if (d->krylov_subspace < 1 || d->krylov_subspace > MAX_RESTART3 || d->krylov_restarts < 1 || d->preconditioner < 0 ||
-      d->preconditioner > 1) {
+      d->preconditioner > 2) {
     jr_plan3d_destroy(p);
-    return report_error(JR_EINVAL, "krylov_subspace 1..64, krylov_restarts >= 1, preconditioner 0 or 1");
+    return report_error(JR_EINVAL, "krylov_subspace 1..64, krylov_restarts >= 1, preconditioner 0, 1 or 2");
   }
   p->cfg = Newton3Config{d->krylov_subspace, d->krylov_restarts, d->preconditioner, d->krylov_tol, d->krylov_success,
                          d->max_relative_update, d->cfl_min, d->cfl_max, d->cfl_growth, d->cfl_cutback};
@@ -265,7 +266,7 @@ int jr_newton_steps3d(jr_plan3d* plan, double* U, int32_t n_steps, double* cfl, 
   ops.A = plan->A;
   ops.B = plan->B;
   ops.factor = plan->factor;
-  ops.line = plan->cfg.preconditioner == 1;
+  ops.line = plan->cfg.preconditioner >= 1;
   ops.st = plan->st;
   ops.bind(plan->work, plan->flag, plan->cfg.restart);
   double c = *cfl, r = *residual_norm;

@@ -44,6 +44,7 @@ struct Plan3Dev {
   const int* neighbours;       // canvas: the partner across a block face, or the cell itself
   int n_chains, chain_L;       // line chains along each block's wall-normal index
   int line_fp32;               // the line factor and apply in FP32 (the mixed form)
+  int line_coupled;            // the SA row coupled to the neighbours' mean flow (6x6 blocks)
   const int* ch_cells;         // [chain * chain_L + k], -1 past the chain's end
   const int* ch_face;          // link k -> k+1: flat index into the three face families, concatenated
   const int* ch_sign;          // +1 / -1: the link face's vector points out of / into cell k; 0 none
@@ -237,9 +238,9 @@ void launch_line_factor3(const Plan3Dev& p, const double* U, double cfl, void* F
 void launch_line_apply3(const Plan3Dev& p, const void* F, const double* r, double* z, cudaStream_t st);
 void launch_precondition3(const Plan3Dev& p, const double* U, double cfl, const double* r, double* z, void* F,
                           cudaStream_t st);
-// words per chain element of the line factor (linesolve3d.cuh): three 5x5 blocks and
-// three SA scalars
-constexpr int FACTOR3 = 78;
+// words per chain element of the line factor (linesolve3d.cuh): three 5x5 blocks, three
+// SA scalars and the SA row's two coupling rows to the mean flow (the coupled form)
+constexpr int FACTOR3 = 88;
 
 // Kernels the 3D path has launched since the library was loaded (counted on the host at
 // each launch site; the benchmark's launch figure).

@@ -149,7 +149,22 @@ __host__ __device__ __forceinline__ void coupling5(const double* qnb, const doub
 // F[(k * FACTOR3 + e) * n_chains + ch]: neighbouring chains' threads read neighbouring
 // words.  The apply is then z_k = P_k (r_k - lower_k d_{k-1}) down the chain and
 // x_k = d_k - C_k x_{k+1} back up, the factor computed once per Newton step.
-constexpr int F3_LOWER = 0, F3_PIV = 25, F3_CHAT = 50, F3_SA = 75;
+constexpr int F3_LOWER = 0, F3_PIV = 25, F3_CHAT = 50, F3_SA = 75, F3_CPL_LO = 78, F3_CPL_UP = 83;
+
+// the SA row's coupling to a neighbour's mean flow: half the Jacobian of rho nu_hat V.S'
+// with respect to its (rho, rho u, rho v, rho w, rho E) at its state qnb, S' = sign S:
+// [-nu_hat vn, nu_hat S'x, nu_hat S'y, nu_hat S'z, 0]
+__host__ __device__ __forceinline__ void sa_coupling_row(const double* qnb, const double* s, double sign,
+                                                         double row[5]) {
+  const double sx = sign * s[0], sy = sign * s[1], sz = sign * s[2];
+  const double nu = qnb[5];
+  const double vn = qnb[1] * sx + qnb[2] * sy + qnb[3] * sz;
+  row[0] = 0.5 * (-nu * vn);
+  row[1] = 0.5 * (nu * sx);
+  row[2] = 0.5 * (nu * sy);
+  row[3] = 0.5 * (nu * sz);
+  row[4] = 0.5 * 0.0;
+}
 
 __host__ __device__ __forceinline__ size_t factor_at(const Plan3Dev& p, int ch, int k, int e) {
   return ((size_t)k * FACTOR3 + e) * p.n_chains + ch;
@@ -170,10 +185,12 @@ inline __host__ __device__ void chain_factor_flow(const Plan3Dev& p, const doubl
   const int len = chain_length(p, ch);
   double cprev[5][5] = {};
   double lower[5][5] = {};   // row k's block toward cell k-1
+  double cpl_lower[5] = {};  // the coupled form: the SA row k's coupling to cell k-1's mean flow
   for (int k = 0; k < len; ++k) {
     const int c = cells[k];
     const double dg = lambda_sum(p, U, c) * (1.0 / cfl + 0.5);
     double upper[5][5] = {}, lower_next[5][5] = {};
+    double cpl_upper[5] = {}, cpl_lower_next[5] = {};
     const int sign = k + 1 < len ? p.ch_sign[(size_t)ch * L + k] : 0;
     if (sign != 0) {
       double s[3], lam, qn[NV3_MAX], qc[NV3_MAX];
@@ -182,7 +199,17 @@ inline __host__ __device__ void chain_factor_flow(const Plan3Dev& p, const doubl
       prim_at(p, U, c, qc);
       coupling5(qn, s, (double)sign, lam, g, upper);
       coupling5(qc, s, (double)-sign, lam, g, lower_next);
+      if (p.line_coupled && p.nvar > 5) {
+        sa_coupling_row(qn, s, (double)sign, cpl_upper);
+        sa_coupling_row(qc, s, (double)-sign, cpl_lower_next);
+      }
     }
+    if (p.line_coupled && p.nvar > 5)
+      for (int t = 0; t < 5; ++t) {
+        F[factor_at(p, ch, k, F3_CPL_LO + t)] = (TF)cpl_lower[t];
+        F[factor_at(p, ch, k, F3_CPL_UP + t)] = (TF)cpl_upper[t];
+        cpl_lower[t] = cpl_lower_next[t];
+      }
     // P = inv(D - lower c_prev); chat = P upper
     double T[5][5], piv[5][5];
     for (int a = 0; a < 5; ++a)
@@ -333,6 +360,8 @@ inline __host__ __device__ void chain_factor_sa(const Plan3Dev& p, const double*
   }
 }
 
+// z = M^-1 r on the SA row of chain ch; in the coupled form after the mean flow's apply,
+// the right-hand side less the coupling to the neighbours' z (block forward substitution)
 template <class TF>
 inline __host__ __device__ void chain_apply_sa(const Plan3Dev& p, int ch, const TF* F, const double* r, double* z) {
   const int n = p.NI * p.NJ * p.NK;
@@ -341,7 +370,20 @@ inline __host__ __device__ void chain_apply_sa(const Plan3Dev& p, int ch, const 
   TF dprev = 0;
   for (int k = 0; k < len; ++k) {
     const int c = cells[k];
-    dprev = F[factor_at(p, ch, k, F3_SA + 1)] * ((TF)r[(size_t)5 * n + c] - F[factor_at(p, ch, k, F3_SA)] * dprev);
+    TF rhs = (TF)r[(size_t)5 * n + c];
+    if (p.line_coupled) {
+      TF lo = 0, up = 0;
+      if (k > 0) {
+        lo = F[factor_at(p, ch, k, F3_CPL_LO)] * (TF)z[cells[k - 1]];
+        for (int t = 1; t < 5; ++t) lo = lo + F[factor_at(p, ch, k, F3_CPL_LO + t)] * (TF)z[(size_t)t * n + cells[k - 1]];
+      }
+      if (k + 1 < len) {
+        up = F[factor_at(p, ch, k, F3_CPL_UP)] * (TF)z[cells[k + 1]];
+        for (int t = 1; t < 5; ++t) up = up + F[factor_at(p, ch, k, F3_CPL_UP + t)] * (TF)z[(size_t)t * n + cells[k + 1]];
+      }
+      rhs = rhs - (lo + up);
+    }
+    dprev = F[factor_at(p, ch, k, F3_SA + 1)] * (rhs - F[factor_at(p, ch, k, F3_SA)] * dprev);
     z[(size_t)5 * n + c] = (double)dprev;
   }
   TF nxt = 0;

@@ -13,7 +13,7 @@ namespace jr {
 constexpr int MAX_RESTART3 = 64;   // krylov_subspace at most
 
 struct Newton3Config {
-  int restart, maxiter, preconditioner;   // preconditioner 0 none, 1 line_j
+  int restart, maxiter, preconditioner;   // preconditioner 0 none, 1 line_j, 2 line_j coupled
   double tol, success, max_relative_update;   // max_relative_update <= 0: none
   double cfl_min, cfl_max, cfl_growth, cfl_cutback;
 };
@@ -63,7 +63,7 @@ int gmres3(Ops& ops, const double* U, double cfl, const Newton3Config& c, int B,
   const double rcond = 2.220446049250313e-16 * (c.restart + 1);
   const int m = c.restart;
   auto prec = [&](int src, int dst) {
-    if (c.preconditioner == 1) ops.precondition(U, cfl, src, dst);
+    if (c.preconditioner >= 1) ops.precondition(U, cfl, src, dst);
     else ops.copy(src, dst);
   };
   const double bn = ops.nrm2(B);

@@ -152,7 +152,7 @@ def describe(plan: Plan3, q_inf, gamma: float, flux: str, limiter: str, kappa: f
     d.krylov_tol, d.krylov_success = imp.krylov_tol, imp.krylov_success
     d.max_relative_update = -1.0 if imp.max_relative_update is None else imp.max_relative_update
     d.krylov_subspace, d.krylov_restarts = imp.krylov_subspace, imp.krylov_restarts
-    d.preconditioner = {"none": 0, "line_j": 1}[imp.preconditioner]
+    d.preconditioner = {"none": 0, "line_j": 1, "line_j_coupled": 2}[imp.preconditioner]
     d.line_precision = 1 if imp.precision == "mixed" else 0
     d.c_cr1 = float(c_cr1)
     W = plan.walls

@@ -139,6 +139,65 @@ def precondition(U, lam, cfl, model, solver: str = "cr"):
     return apply
 
 
+def chain_coupling_sa(U, model):
+    """The SA row's coupling to the neighbours' mean flow in the coupled (6x6) line
+    blocks: ``(lower, upper)`` ``(L, n_lines, 5)``, half the Jacobian of the SA convective
+    flux ``rho nu_hat V.S`` with respect to the neighbour's (rho, rho u, rho v, rho w,
+    rho E) at the neighbour's state, ``[-nu_hat vn, nu_hat Sx, nu_hat Sy, nu_hat Sz, 0]``,
+    with the link's face vector and sign as the mean-flow blocks use them
+    (``chain_blocks_flow``).  The mean-flow rows do not depend on rho nu_hat, so the
+    6x6 blocks are block lower triangular.  This build's coupled variant of ``line_j``
+    (the 3D form of ``oracle.implicit.chain_coupling_sa``); the reference has only the
+    split form (``preconditioners.py:291-306``)."""
+    plan, g = model.plan, model.gamma
+    lines = plan.lines
+    q = n3.prim(U, g)
+
+    def coupling(side, sign, nb):
+        s = _faces(plan.faces, lines, side)
+        sx, sy, sz = sign * s[0], sign * s[1], sign * s[2]
+        nu = nb[5]
+        vn = nb[1] * sx + nb[2] * sy + nb[3] * sz
+        row = 0.5 * np.stack([-nu * vn, nu * sx, nu * sy, nu * sz, np.zeros_like(vn)])
+        return np.transpose(np.where(sign != 0, row, 0.0), (2, 1, 0))
+
+    chains = _gather(q, lines)
+    above = np.concatenate([chains[:, :, 1:], chains[:, :, -1:]], axis=2)
+    upper = coupling("up", lines.up_sign, above)
+    below = coupling("down", lines.down_sign, chains)
+    lower = np.concatenate([np.zeros_like(below[:1]), below[:-1]], axis=0)
+    return lower, upper
+
+
+def precondition_coupled(U, lam, cfl, model, solver: str = "cr"):
+    """``r -> M^-1 r`` with the coupled 6x6 line blocks: the mean flow solved first, then
+    the SA chains with the right-hand side ``r_sa - C z_flow`` (block forward
+    substitution of the block lower-triangular blocks)."""
+    split = precondition(U, lam, cfl, model, solver)
+    lines = model.plan.lines
+    valid = lines.cells >= 0
+    lower, upper = chain_coupling_sa(U, model)
+    fac = cr_factor if solver == "cr" else thomas_factor
+    sol = cr_solve if solver == "cr" else thomas_solve
+    sa_factor = fac(*chain_blocks_sa(U, lam, cfl, model))
+
+    def apply(r):
+        z = split(r)
+        zf = np.transpose(np.where(valid, _gather(z[:5], lines), 0.0), (2, 1, 0))   # (L, n_lines, 5)
+        below = np.concatenate([np.zeros_like(zf[:1]), zf[:-1]], axis=0)
+        above = np.concatenate([zf[1:], np.zeros_like(zf[:1])], axis=0)
+        cz = np.sum(lower * below, axis=-1) + np.sum(upper * above, axis=-1)       # (L, n_lines)
+        rhs = np.where(valid, _gather(r[5:6], lines), 0.0)[0].T - cz
+        x = sol(sa_factor, rhs[:, :, None])[:, :, 0].T                              # (n_lines, L)
+        out = z.copy()
+        flat = out[5].reshape(-1)
+        flat[lines.cells[valid]] = x[valid]
+        out[5] = flat.reshape(out[5].shape)
+        return out
+
+    return apply
+
+
 # --- the Newton step (src/jaxrans/solvers/implicit.py:54-168, core/state.py:142-150) ------
 
 

@@ -46,6 +46,7 @@ static Plan3Dev plan_of(const jr_plan3d_desc* d) {
   p.neighbours = d->neighbours;
   p.n_chains = d->n_chains;
   p.line_fp32 = d->line_precision;
+  p.line_coupled = d->preconditioner == 2;
   p.chain_L = d->chain_L;
   p.ch_cells = d->chain_cells;
   p.ch_face = d->chain_up_face;

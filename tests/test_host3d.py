@@ -172,3 +172,34 @@ def test_the_mixed_line_solve_stays_within_fp32_of_fp64(harness, case3d, state):
         desc.line_precision = 0
     err = rows_rel(mixed, exact)
     assert 0.0 < err < 1e-4
+
+
+@pytest.mark.parametrize("state", ["sin", "rand0"])
+def test_kernel_bodies_give_the_coupled_line_solve(harness, case3d, state):
+    """The coupled (6x6) form of the line solve (descriptor preconditioner 2): the factor's
+    SA coupling rows and the apply's forward substitution against the oracle's coupled
+    solve (itself checked against dense block solves)."""
+    import json as _json
+    from oracle import implicit3d as i3
+    from oracle import numerics3d as n3
+    z, plan, desc, _ = case3d
+    U = np.ascontiguousarray(z[f"{state}_U"])
+    r = np.ascontiguousarray(z[f"{state}_prec_r"])
+    out = np.zeros_like(r)
+    desc.preconditioner = 2
+    try:
+        assert harness.jr3_host_precondition(C.addressof(desc), U.ctypes.data, 25.0, r.ctypes.data,
+                                             out.ctypes.data) == 0
+    finally:
+        desc.preconditioner = 1
+    flow = _flow(_json.loads(str(z["case_json"]))["case"])
+    a = flow.alpha_rad
+    q_inf = np.array([1.0, flow.mach * np.cos(a), 0.0, flow.mach * np.sin(a), 1.0 / flow.gamma, flow.nu_tilde_ratio])
+    model = n3.Model3(plan, q_inf, flow.gamma, "hllc", "van_albada_smooth", 0.0, flow.mu_inf,
+                      flow.sutherland_ratio, True, plan.distance)
+    lam = n3.wave_speeds(U, model)
+    ref = i3.precondition_coupled(U, lam, 25.0, model, solver="thomas")(r)
+    assert rows_rel(out, ref) < 1e-12
+    split = i3.precondition(U, lam, 25.0, model, solver="thomas")(r)
+    assert rows_rel(out[5:], split[5:]) > 1e-9          # the coupling changes the SA row
+    assert rows_rel(out[:5], split[:5]) < 1e-13         # and not the mean flow

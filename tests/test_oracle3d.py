@@ -133,3 +133,39 @@ def test_gmres_and_newton_steps_match_the_reference(setup):
         assert np.isclose(norm, float(z[f"newton{k}_norm"]), rtol=1e-12, atol=0.0)
         assert rows_rel(state.U, z[f"newton{k}_U"]) < 1e-13
         assert np.isclose(state.cfl, float(z[f"newton{k}_cfl"]), rtol=1e-12)
+
+
+@pytest.mark.parametrize("state", ["sin", "rand0"])
+def test_coupled_line_solve_is_the_dense_6x6_block_solve(setup, state):
+    """The coupled (6x6) line blocks -- the SA row also coupled to the neighbours' mean
+    flow -- solved by mean flow first, then the SA chains with r_sa - C z_flow, against a
+    dense solve of each chain's assembled block-tridiagonal matrix (CPU)."""
+    from oracle import implicit3d as i3
+    z, model = setup
+    U, r = z[f"{state}_U"], z[f"{state}_prec_r"]
+    lam = n3.wave_speeds(U, model)
+    fl, fd, fu = i3.chain_blocks_flow(U, lam, 25.0, model)
+    sl, sd, su = i3.chain_blocks_sa(U, lam, 25.0, model)
+    cl, cu = i3.chain_coupling_sa(U, model)
+    assert np.abs(cl).max() > 0.0 and np.abs(cu).max() > 0.0
+    got = i3.precondition_coupled(U, lam, 25.0, model)(r)
+    lines = model.plan.lines
+    flat_r = r.reshape(6, -1)
+    flat_got = got.reshape(6, -1)
+    for line in range(lines.cells.shape[0]):
+        cells = lines.cells[line][lines.cells[line] >= 0]
+        L = len(cells)
+        M = np.zeros((6 * L, 6 * L))
+        for k in range(L):
+            def put(col, flow, cpl, sa):
+                M[6 * k:6 * k + 5, 6 * col:6 * col + 5] = flow
+                if cpl is not None:
+                    M[6 * k + 5, 6 * col:6 * col + 5] = cpl
+                M[6 * k + 5, 6 * col + 5] = sa
+            put(k, fd[k, line], None, sd[k, line, 0, 0])
+            if k > 0:
+                put(k - 1, fl[k, line], cl[k, line], sl[k, line, 0, 0])
+            if k + 1 < L:
+                put(k + 1, fu[k, line], cu[k, line], su[k, line, 0, 0])
+        x = np.linalg.solve(M, flat_r[:, cells].T.reshape(-1)).reshape(L, 6).T
+        assert np.allclose(flat_got[:, cells], x, rtol=1e-9, atol=1e-12 * np.abs(x).max())
