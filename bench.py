@@ -299,6 +299,7 @@ def run_wing3d(args) -> int:
             "config": {"workload": args.workload, "cells": plan.cells, "canvas": list(plan.shape),
                        "blocks": len(plan.mesh), "nvar": int(U0.shape[0]),
                        "krylov_subspace": case.implicit.krylov_subspace,
+                       "preconditioner": case.implicit.preconditioner, "precision": case.implicit.precision,
                        "l2": "inputs larger than L2" if U0.nbytes > 126e6 else "inputs smaller than L2, no flush",
                        "timer": "host clock between device synchronisations (the 3D step is host-driven)"},
             "e2e": {"value": world * args.steps / e2e_seconds, "unit": "steps/s",

@@ -33,7 +33,8 @@ on a GPU box and in the oracle.
   four-block point-matched C-H grid of 193 x 65 x 81 nodes per block (3.93M cells; the
   wing and the region past its tip, each in lower and upper halves), first cell 2e-6 root
   chord, far field at 50 root chords, M 0.8, alpha 2.5 deg, Re 1e7, HLLC with MUSCL and
-  the smooth van Albada limiter, 6 variables.  ``wing_ch_4blk_small`` is the same wing on
+  the smooth van Albada limiter, 6 variables; FP64 residual, J.v and Krylov vectors, the
+  coupled 6x6 line preconditioner in FP32.  ``wing_ch_4blk_small`` is the same wing on
   a grid of 49 x 17 x 17 nodes per block, for profiling and tests.  A 3D case is a grid
   file plus its documents: ``wing3d_case`` writes them into a directory and loads them.
 """
@@ -117,7 +118,8 @@ WING3D_PLANFORM = {"semispan": 1.6, "taper": 0.6, "sweep_deg": 25.0}
 WING3D_FLOW = {"freestream": {"mach": 0.8, "alpha_deg": 2.5, "reynolds": 1e7}, "turbulence": {"model": "sa_noft2"}}
 WING3D_NUMERICS = {"convective_fluxes": {"riemann_solver": "hllc", "limiter": "van_albada_smooth"},
                    "time_integration": {"solver": "implicit"},
-                   "implicit": {"krylov_subspace": 30, "max_relative_update": 0.2},
+                   "implicit": {"krylov_subspace": 30, "max_relative_update": 0.2,
+                                "preconditioner": "line_j_coupled", "precision": "mixed"},
                    "convergence": {"max_iters": 6000, "tol": 1e-10, "block_iters": 20}}
 
 
