@@ -203,3 +203,36 @@ def test_kernel_bodies_give_the_coupled_line_solve(harness, case3d, state):
     split = i3.precondition(U, lam, 25.0, model, solver="thomas")(r)
     assert rows_rel(out[5:], split[5:]) > 1e-9          # the coupling changes the SA row
     assert rows_rel(out[:5], split[:5]) < 1e-13         # and not the mean flow
+
+
+def test_newton_steps_with_the_coupled_and_mixed_line_solve(harness, case3d):
+    """The Newton driver over the coupled 6x6 line blocks in FP32 (config 5's
+    preconditioner): the residual falls as with line_j in FP64, step for step within a
+    few per cent."""
+    import json as _json
+    from jaxrans_b200.case import NUMERICAL_FILE, _section, _values
+    from jaxrans_b200.config import ImplicitConfig
+    z, plan, desc, _ = case3d
+    doc = _json.loads(str(z["case_json"]))
+    cfg = ImplicitConfig(**_values(_section(doc["numerical"], NUMERICAL_FILE, "implicit"), NUMERICAL_FILE, "implicit"))
+    config = np.array([cfg.krylov_tol, cfg.krylov_success,
+                       cfg.max_relative_update if cfg.max_relative_update is not None else -1.0,
+                       cfg.cfl_min, cfg.cfl_max, cfg.cfl_growth, cfg.cfl_cutback])
+
+    def steps(preconditioner, precision):
+        iconfig = np.array([cfg.krylov_subspace, cfg.krylov_restarts, preconditioner], dtype=np.int32)
+        U = np.ascontiguousarray(z["rand0_U"]).copy()
+        cfl, res = C.c_double(25.0), C.c_double(np.inf)
+        hist = np.zeros(4)
+        desc.preconditioner, desc.line_precision = preconditioner, precision
+        try:
+            assert harness.jr3_host_newton_steps(C.addressof(desc), config.ctypes.data, iconfig.ctypes.data,
+                                                 U.ctypes.data, C.byref(cfl), C.byref(res), 4, hist.ctypes.data) == 0
+        finally:
+            desc.preconditioner, desc.line_precision = 1, 0
+        return hist
+
+    plain, coupled = steps(1, 0), steps(2, 1)
+    assert plain[0] == coupled[0]                       # the same state before the first step
+    assert np.all(np.isfinite(coupled)) and coupled[-1] < coupled[0]
+    assert np.allclose(coupled, plain, rtol=5e-2)
