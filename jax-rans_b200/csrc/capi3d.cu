@@ -188,6 +188,17 @@ int jr_plan3d_create(const jr_plan3d_desc* d, jr_plan3d** out) {
     p->allocs.push_back(sc);
     p->factor = sc;
   }
+  {
+    const size_t nf = (size_t)(d->NI + 1) * d->NJ * d->NK + (size_t)d->NI * (d->NJ + 1) * d->NK +
+                      (size_t)d->NI * d->NJ * (d->NK + 1);
+    void* fb = nullptr;
+    if (cudaMalloc(&fb, nf * d->nvar * sizeof(double)) != cudaSuccess) {
+      jr_plan3d_destroy(p);
+      return report_error(JR_ENOMEM, "cudaMalloc failed");
+    }
+    p->allocs.push_back(fb);
+    dv.face_buf = static_cast<double*>(fb);
+  }
   const size_t work = (size_t)d->nvar * n * sizeof(Dual);
   if (cudaMalloc(&p->A, work) != cudaSuccess || (p->allocs.push_back(p->A), cudaMalloc(&p->B, work)) != cudaSuccess) {
     jr_plan3d_destroy(p);

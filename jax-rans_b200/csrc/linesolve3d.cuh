@@ -10,19 +10,6 @@
 
 namespace jr {
 
-__host__ __device__ __forceinline__ int face_count(const Plan3Dev& p, int a) {
-  return (p.NI + (a == 0)) * (p.NJ + (a == 1)) * (p.NK + (a == 2));
-}
-
-// a flat index into the three face families, concatenated, to (family, i, j, k)
-__host__ __device__ __forceinline__ void face_of(const Plan3Dev& p, int flat, int& a, int& i, int& j, int& k) {
-  a = 0;
-  while (a < 2 && flat >= face_count(p, a)) flat -= face_count(p, a++);
-  const int fj = p.NJ + (a == 1), fk = p.NK + (a == 2);
-  i = flat / (fj * fk);
-  j = (flat / fk) % fj;
-  k = flat % fk;
-}
 
 // primitive state of canvas cell c straight from U (no ghost fill)
 __host__ __device__ __forceinline__ void prim_at(const Plan3Dev& p, const double* U, int c, double q[NV3_MAX]) {

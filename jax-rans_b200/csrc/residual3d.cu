@@ -2,12 +2,12 @@
 // wing's C-H block; the reference's 3D path, src/jaxrans/numerics/residual.py:54-91,
 // 273-334, on the canvas of src/jaxrans/mesh/atlas3d.py:119-210).
 //
-// The first device form of the 3D path: the ghost fill runs its gather stages as
-// record kernels (one thread per ghost record, double-buffered so every read of a
-// stage precedes its writes), then one thread per canvas cell evaluates its six faces
-// -- MUSCL on the flow rows, HLLC or Roe with a vector normal, the 3D diamond face
-// gradient, the viscous flux, the SA row with |curl V| -- and sums F_hi - F_lo per
-// family.  Templated on the scalar: `double` for R(U), `Dual` (value + tangent) for
+// The ghost fill runs its gather stages as record kernels (one thread per ghost record,
+// double-buffered so every read of a stage precedes its writes); then one thread per
+// face evaluates its flux once -- MUSCL on the flow rows, HLLC or Roe with a vector
+// normal, the 3D diamond face gradient, the viscous flux (with QCR2000), the SA row's
+// convection and diffusion -- into a face buffer, and one thread per cell sums F_hi -
+// F_lo per family and adds the SA source with |curl V|.  Templated on the scalar: `double` for R(U), `Dual` (value + tangent) for
 // the J.v of the first-order residual.  Every canvas index is clamped to the canvas, the
 // reference's edge padding.
 #include <cstdint>
@@ -29,13 +29,20 @@ __global__ void k3_ghost_stage(Plan3Dev p, const T* __restrict__ in, T* __restri
     ghost_record(p, in, out, r);
 }
 
+// phase 1: every face's flux once (one thread per face of the three families)
 template <class T, bool VISC, bool SA>
-__global__ void __launch_bounds__(128) k3_residual(Plan3Dev p, const T* __restrict__ Q, const double* __restrict__ U,
-                                                   const double* __restrict__ dU, double* __restrict__ R,
-                                                   int first_order) {
+__global__ void __launch_bounds__(128) k3_face_flux(Plan3Dev p, const T* __restrict__ Q, int first_order, int nf) {
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += gridDim.x * blockDim.x)
+    store_face_flux<T, VISC, SA>(p, Q, first_order, f, p.face_buf, (size_t)nf);
+}
+
+// phase 2: each cell's sum of its faces' fluxes (and the SA source)
+template <class T, bool SA>
+__global__ void __launch_bounds__(128) k3_cell_sum(Plan3Dev p, const T* __restrict__ Q, const double* __restrict__ U,
+                                                   const double* __restrict__ dU, double* __restrict__ R, int nf) {
   const int n = p.NI * p.NJ * p.NK;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
-    residual_cell<T, VISC, SA>(p, Q, U, dU, R, first_order, c);
+    residual_cell_from_faces<T, SA>(p, Q, p.face_buf, (size_t)nf, U, dU, R, c);
 }
 
 // ---- launchers
@@ -68,12 +75,19 @@ static void residual3_t(const Plan3Dev& p, const double* U, const double* dU, do
   k3_prim<T><<<blocks, 128, 0, st>>>(p, U, dU, A);
   fill3(p, A, B, st);
   const bool visc = p.P.mu_inf > 0.0, sa = p.nvar > 5;
+  const int nf = face_count(p, 0) + face_count(p, 1) + face_count(p, 2);
+  const int fblocks = (nf + 127) / 128;
+  counted3();   // the face phase (the cell phase is counted with the primitive canvas)
   if (sa)
-    k3_residual<T, true, true><<<blocks, 128, 0, st>>>(p, A, U, dU, R, first_order);
+    k3_face_flux<T, true, true><<<fblocks, 128, 0, st>>>(p, A, first_order, nf);
   else if (visc)
-    k3_residual<T, true, false><<<blocks, 128, 0, st>>>(p, A, U, dU, R, first_order);
+    k3_face_flux<T, true, false><<<fblocks, 128, 0, st>>>(p, A, first_order, nf);
   else
-    k3_residual<T, false, false><<<blocks, 128, 0, st>>>(p, A, U, dU, R, first_order);
+    k3_face_flux<T, false, false><<<fblocks, 128, 0, st>>>(p, A, first_order, nf);
+  if (sa)
+    k3_cell_sum<T, true><<<blocks, 128, 0, st>>>(p, A, U, dU, R, nf);
+  else
+    k3_cell_sum<T, false><<<blocks, 128, 0, st>>>(p, A, U, dU, R, nf);
 }
 
 __global__ void k3_wall_loads(Plan3Dev p, const double* __restrict__ Q, double* __restrict__ loads) {

@@ -31,6 +31,28 @@ __host__ __device__ __forceinline__ void ghost_record(const Plan3Dev& p, const T
 }
 
 // ---- geometry access
+// faces of family a on the canvas (one more than the cells along a)
+__host__ __device__ __forceinline__ int face_count(const Plan3Dev& p, int a) {
+  return (p.NI + (a == 0)) * (p.NJ + (a == 1)) * (p.NK + (a == 2));
+}
+
+// a flat index into the three face families, concatenated, to (family, i, j, k)
+__host__ __device__ __forceinline__ void face_of(const Plan3Dev& p, int flat, int& a, int& i, int& j, int& k) {
+  a = 0;
+  while (a < 2 && flat >= face_count(p, a)) flat -= face_count(p, a++);
+  const int fj = p.NJ + (a == 1), fk = p.NK + (a == 2);
+  i = flat / (fj * fk);
+  j = (flat / fk) % fj;
+  k = flat % fk;
+}
+
+// the flat index of face (i, j, k) of family a
+__host__ __device__ __forceinline__ int face_flat(const Plan3Dev& p, int a, int i, int j, int k) {
+  int off = 0;
+  for (int b = 0; b < a; ++b) off += face_count(p, b);
+  return off + (i * (p.NJ + (a == 1)) + j) * (p.NK + (a == 2)) + k;
+}
+
 __host__ __device__ __forceinline__ int clampi(int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi : x); }
 
 struct Cell3 {
@@ -296,7 +318,66 @@ __host__ __device__ void face_flux(const Plan3Dev& p, const T* Q, int a, int fi,
   }
 }
 
-// R of block cell c; R = U - U_inf elsewhere (tangent: v)
+// The SA row's source at block cell c, times the volume: the production and destruction
+// with |curl V| and the c_b2 gradient term, both from Green-Gauss gradients of the face
+// means of (u, v, w, nu~) (src/jaxrans/numerics/turbulence.py).
+template <class T>
+__host__ __device__ T sa_cell_source(const Plan3Dev& p, const T* __restrict__ Q, int c) {
+  const int i = c / (p.NJ * p.NK), j = (c / p.NK) % p.NJ, k = c % p.NK;
+  T lo_s[3][5], hi_s[3][5];   // face means of (u, v, w, nu~) for the cell's Green-Gauss gradients
+  for (int a = 0; a < 3; ++a) {
+    int lo[3] = {i, j, k}, hi[3] = {i, j, k};
+    lo[a] -= 1;
+    hi[a] += 1;
+    T qc[NV3_MAX], ql[NV3_MAX], qh[NV3_MAX];
+    load_cell(p, Q, c, qc);
+    load_cell(p, Q, cell_index(p, lo[0], lo[1], lo[2]), ql);
+    load_cell(p, Q, cell_index(p, hi[0], hi[1], hi[2]), qh);
+    for (int m = 0; m < 3; ++m) {
+      lo_s[a][m] = 0.5 * (ql[1 + m] + qc[1 + m]);
+      hi_s[a][m] = 0.5 * (qc[1 + m] + qh[1 + m]);
+    }
+    lo_s[a][3] = 0.5 * (ql[5] + qc[5]);
+    hi_s[a][3] = 0.5 * (qc[5] + qh[5]);
+  }
+  const Physics3& P = p.P;
+  const double vol = p.volume[c];
+  // Green-Gauss: (1/V) sum_families (phi_hi S_hi - phi_lo S_lo)[component]
+  T gv[3][3], gn[3];
+  for (int comp = 0; comp < 3; ++comp) {
+    T tv[3], tn = cst<T>(0.0);
+    for (int m = 0; m < 3; ++m) tv[m] = cst<T>(0.0);
+    for (int a = 0; a < 3; ++a) {
+      int f0[3] = {i, j, k}, f1[3] = {i, j, k};
+      f1[a] += 1;
+      double s0[3], s1[3];
+      face_vector(p, a, f0[0], f0[1], f0[2], s0);
+      face_vector(p, a, f1[0], f1[1], f1[2], s1);
+      for (int m = 0; m < 3; ++m) {
+        T d = hi_s[a][m] * s1[comp] - lo_s[a][m] * s0[comp];
+        tv[m] = a == 0 ? d : tv[m] + d;
+      }
+      T dn = hi_s[a][3] * s1[comp] - lo_s[a][3] * s0[comp];
+      tn = a == 0 ? dn : tn + dn;
+    }
+    for (int m = 0; m < 3; ++m) gv[comp][m] = tv[m] / vol;   // gv[direction][component]
+    gn[comp] = tn / vol;
+  }
+  T cx = gv[1][2] - gv[2][1], cy = gv[2][0] - gv[0][2], cz = gv[0][1] - gv[1][0];
+  T sq = (cx * cx + cy * cy) + cz * cz;
+  T omega = val(sq) > 0.0 ? dsqrt(sq) : cst<T>(0.0);
+  T qc[NV3_MAX];
+  load_cell(p, Q, c, qc);
+  const double g = P.gamma;
+  T mu = viscosity3(P, g * qc[4] / qc[0]);
+  T Pr, Dd;
+  sa_source(P.sa, qc[5] * P.mu_inf, mu / qc[0], omega, p.distance[c], Pr, Dd);
+  T src = qc[0] * ((Pr - Dd) / P.mu_inf + P.sa.c_b2 / P.sa.sigma * P.mu_inf * ((gn[0] * gn[0] + gn[1] * gn[1]) + gn[2] * gn[2]));
+  return src * vol;
+}
+
+// R of block cell c; R = U - U_inf elsewhere (tangent: v).  Each of the cell's six faces
+// evaluated here (the fused form; the device runs the two phases below).
 template <class T, bool VISC, bool SA>
 __host__ __device__ void residual_cell(const Plan3Dev& p, const T* __restrict__ Q, const double* __restrict__ U,
                                        const double* __restrict__ dU, double* __restrict__ R, int first_order, int c) {
@@ -308,7 +389,6 @@ __host__ __device__ void residual_cell(const Plan3Dev& p, const T* __restrict__ 
   }
   const int i = c / (p.NJ * p.NK), j = (c / p.NK) % p.NJ, k = c % p.NK;
   T acc[NV3_MAX];
-  T lo_s[3][5], hi_s[3][5];   // SA: face means of (u, v, w, nu~) for the cell's Green-Gauss gradients
   for (int v = 0; v < p.nvar; ++v) acc[v] = cst<T>(0.0);
   for (int a = 0; a < 3; ++a) {
     int f0[3] = {i, j, k}, f1[3] = {i, j, k};
@@ -317,59 +397,57 @@ __host__ __device__ void residual_cell(const Plan3Dev& p, const T* __restrict__ 
     face_flux<T, VISC, SA>(p, Q, a, f0[0], f0[1], f0[2], first_order != 0, Flo);
     face_flux<T, VISC, SA>(p, Q, a, f1[0], f1[1], f1[2], first_order != 0, Fhi);
     for (int v = 0; v < p.nvar; ++v) acc[v] = a == 0 ? Fhi[v] - Flo[v] : acc[v] + (Fhi[v] - Flo[v]);
-    if constexpr (SA) {
-      int lo[3] = {i, j, k}, hi[3] = {i, j, k};
-      lo[a] -= 1;
-      hi[a] += 1;
-      T qc[NV3_MAX], ql[NV3_MAX], qh[NV3_MAX];
-      load_cell(p, Q, c, qc);
-      load_cell(p, Q, cell_index(p, lo[0], lo[1], lo[2]), ql);
-      load_cell(p, Q, cell_index(p, hi[0], hi[1], hi[2]), qh);
-      for (int m = 0; m < 3; ++m) {
-        lo_s[a][m] = 0.5 * (ql[1 + m] + qc[1 + m]);
-        hi_s[a][m] = 0.5 * (qc[1 + m] + qh[1 + m]);
-      }
-      lo_s[a][3] = 0.5 * (ql[5] + qc[5]);
-      hi_s[a][3] = 0.5 * (qc[5] + qh[5]);
-    }
   }
-  if constexpr (SA) {
-    const Physics3& P = p.P;
-    const double vol = p.volume[c];
-    // Green-Gauss: (1/V) sum_families (phi_hi S_hi - phi_lo S_lo)[component]
-    T gv[3][3], gn[3];
-    for (int comp = 0; comp < 3; ++comp) {
-      T tv[3], tn = cst<T>(0.0);
-      for (int m = 0; m < 3; ++m) tv[m] = cst<T>(0.0);
-      for (int a = 0; a < 3; ++a) {
-        int f0[3] = {i, j, k}, f1[3] = {i, j, k};
-        f1[a] += 1;
-        double s0[3], s1[3];
-        face_vector(p, a, f0[0], f0[1], f0[2], s0);
-        face_vector(p, a, f1[0], f1[1], f1[2], s1);
-        for (int m = 0; m < 3; ++m) {
-          T d = hi_s[a][m] * s1[comp] - lo_s[a][m] * s0[comp];
-          tv[m] = a == 0 ? d : tv[m] + d;
-        }
-        T dn = hi_s[a][3] * s1[comp] - lo_s[a][3] * s0[comp];
-        tn = a == 0 ? dn : tn + dn;
-      }
-      for (int m = 0; m < 3; ++m) gv[comp][m] = tv[m] / vol;   // gv[direction][component]
-      gn[comp] = tn / vol;
-    }
-    T cx = gv[1][2] - gv[2][1], cy = gv[2][0] - gv[0][2], cz = gv[0][1] - gv[1][0];
-    T sq = (cx * cx + cy * cy) + cz * cz;
-    T omega = val(sq) > 0.0 ? dsqrt(sq) : cst<T>(0.0);
-    T qc[NV3_MAX];
-    load_cell(p, Q, c, qc);
-    const double g = P.gamma;
-    T mu = viscosity3(P, g * qc[4] / qc[0]);
-    T Pr, Dd;
-    sa_source(P.sa, qc[5] * P.mu_inf, mu / qc[0], omega, p.distance[c], Pr, Dd);
-    T src = qc[0] * ((Pr - Dd) / P.mu_inf + P.sa.c_b2 / P.sa.sigma * P.mu_inf * ((gn[0] * gn[0] + gn[1] * gn[1]) + gn[2] * gn[2]));
-    acc[5] = acc[5] - src * vol;
-  }
+  if constexpr (SA) acc[5] = acc[5] - sa_cell_source(p, Q, c);
   for (int v = 0; v < p.nvar; ++v) R[(size_t)v * n + c] = tangent_or_value(acc[v]);
+}
+
+// Phase 1 of the two-phase residual: the flux through face `flat` -- its value, or for
+// Dual its tangent -- stored at Fb[v * nf + flat], for a face with a block cell on
+// either side (no cell reads the others).  Every face is evaluated once instead of once
+// from each side, with the same arithmetic, so phase 2's sums are residual_cell's.
+template <class T, bool VISC, bool SA>
+__host__ __device__ void store_face_flux(const Plan3Dev& p, const T* __restrict__ Q, int first_order, int flat,
+                                         double* __restrict__ Fb, size_t nf) {
+  int a, i, j, k;
+  face_of(p, flat, a, i, j, k);
+  int h[3] = {i, j, k}, l[3] = {i, j, k};
+  l[a] -= 1;
+  const int dims[3] = {p.NI, p.NJ, p.NK};
+  const bool hi_in = h[a] < dims[a] && p.interior[(h[0] * p.NJ + h[1]) * p.NK + h[2]];
+  const bool lo_in = l[a] >= 0 && p.interior[(l[0] * p.NJ + l[1]) * p.NK + l[2]];
+  if (!hi_in && !lo_in) return;
+  T F[NV3_MAX];
+  face_flux<T, VISC, SA>(p, Q, a, i, j, k, first_order != 0, F);
+  for (int v = 0; v < p.nvar; ++v) Fb[(size_t)v * nf + flat] = tangent_or_value(F[v]);
+}
+
+// Phase 2: R of cell c from the stored face fluxes (residual_cell's sums and SA source)
+template <class T, bool SA>
+__host__ __device__ void residual_cell_from_faces(const Plan3Dev& p, const T* __restrict__ Q,
+                                                  const double* __restrict__ Fb, size_t nf,
+                                                  const double* __restrict__ U, const double* __restrict__ dU,
+                                                  double* __restrict__ R, int c) {
+  const int n = p.NI * p.NJ * p.NK;
+  if (!p.interior[c]) {
+    for (int v = 0; v < p.nvar; ++v)
+      R[(size_t)v * n + c] = dU ? dU[(size_t)v * n + c] : U[(size_t)v * n + c] - p.P.U_inf[v];
+    return;
+  }
+  const int i = c / (p.NJ * p.NK), j = (c / p.NK) % p.NJ, k = c % p.NK;
+  double acc[NV3_MAX];
+  for (int v = 0; v < p.nvar; ++v) acc[v] = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    int f1[3] = {i, j, k};
+    f1[a] += 1;
+    const int lo = face_flat(p, a, i, j, k), hi = face_flat(p, a, f1[0], f1[1], f1[2]);
+    for (int v = 0; v < p.nvar; ++v) {
+      const double d = Fb[(size_t)v * nf + hi] - Fb[(size_t)v * nf + lo];
+      acc[v] = a == 0 ? d : acc[v] + d;
+    }
+  }
+  if constexpr (SA) acc[5] = acc[5] - tangent_or_value(sa_cell_source(p, Q, c));
+  for (int v = 0; v < p.nvar; ++v) R[(size_t)v * n + c] = acc[v];
 }
 
 }  // namespace jr

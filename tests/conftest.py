@@ -58,6 +58,7 @@ def harness(tmp_path_factory):
     lib = C.CDLL(str(out))
     p, i, d = C.c_void_p, C.c_int, C.c_double
     for name, args in {"jr3_host_eval": [p, p, p, p, i],
+                       "jr3_host_eval_faces": [p, p, p, p, i],
                        "jr3_host_wave_speeds": [p, p, p],
                        "jr3_host_precondition": [p, p, d, p, p],
                        "jr3_host_newton_steps": [p, p, p, p, p, p, i, p],

@@ -2,6 +2,7 @@
 // residual3d.cuh) run on the host, in the order the device runs them, on a plan given by
 // its C-ABI descriptor -- a check of the kernels' indexing and arithmetic without a GPU.
 // Nothing of the library calls this; it is built by tests/test_host3d.py.
+#include <cmath>
 #include <utility>
 #include <vector>
 
@@ -12,8 +13,11 @@
 
 using namespace jr;
 
+// the residual in the fused form (each cell evaluates its six faces), or in the device's
+// two phases (every face once into a buffer, unwritten entries NaN, then the cell sums)
 template <class T, bool VISC, bool SA>
-static void run(const Plan3Dev& p, const double* U, const double* dU, double* R, int first_order) {
+static void run(const Plan3Dev& p, const double* U, const double* dU, double* R, int first_order,
+                bool two_phase = false) {
   const int n = p.NI * p.NJ * p.NK;
   std::vector<T> A((size_t)p.nvar * n), B((size_t)p.nvar * n);
   for (int c = 0; c < n; ++c) prim_cell(p, U, dU, A.data(), c);
@@ -22,7 +26,14 @@ static void run(const Plan3Dev& p, const double* U, const double* dU, double* R,
     for (int r = p.stage_off[s]; r < p.stage_off[s + 1]; ++r) ghost_record(p, A.data(), B.data(), r);
     std::swap(A, B);
   }
-  for (int c = 0; c < n; ++c) residual_cell<T, VISC, SA>(p, A.data(), U, dU, R, first_order, c);
+  if (!two_phase) {
+    for (int c = 0; c < n; ++c) residual_cell<T, VISC, SA>(p, A.data(), U, dU, R, first_order, c);
+    return;
+  }
+  const int nf = face_count(p, 0) + face_count(p, 1) + face_count(p, 2);
+  std::vector<double> Fb((size_t)p.nvar * nf, std::nan(""));
+  for (int f = 0; f < nf; ++f) store_face_flux<T, VISC, SA>(p, A.data(), first_order, f, Fb.data(), (size_t)nf);
+  for (int c = 0; c < n; ++c) residual_cell_from_faces<T, SA>(p, A.data(), Fb.data(), (size_t)nf, U, dU, R, c);
 }
 
 static Plan3Dev plan_of(const jr_plan3d_desc* d) {
@@ -60,21 +71,32 @@ static Plan3Dev plan_of(const jr_plan3d_desc* d) {
   return p;
 }
 
-extern "C" int jr3_host_eval(const jr_plan3d_desc* d, const double* U, const double* dU, double* R,
-                             int first_order) {
+static int eval(const jr_plan3d_desc* d, const double* U, const double* dU, double* R, int first_order,
+                bool two_phase) {
   if (d->n_stages < 1 || d->n_stages > MAX_STAGES3) return 1;
   const Plan3Dev p = plan_of(d);
   const bool visc = p.P.mu_inf > 0.0, sa = p.nvar > 5;
   if (dU) {
-    if (sa) run<Dual, true, true>(p, U, dU, R, 1);
-    else if (visc) run<Dual, true, false>(p, U, dU, R, 1);
-    else run<Dual, false, false>(p, U, dU, R, 1);
+    if (sa) run<Dual, true, true>(p, U, dU, R, 1, two_phase);
+    else if (visc) run<Dual, true, false>(p, U, dU, R, 1, two_phase);
+    else run<Dual, false, false>(p, U, dU, R, 1, two_phase);
   } else {
-    if (sa) run<double, true, true>(p, U, nullptr, R, first_order);
-    else if (visc) run<double, true, false>(p, U, nullptr, R, first_order);
-    else run<double, false, false>(p, U, nullptr, R, first_order);
+    if (sa) run<double, true, true>(p, U, nullptr, R, first_order, two_phase);
+    else if (visc) run<double, true, false>(p, U, nullptr, R, first_order, two_phase);
+    else run<double, false, false>(p, U, nullptr, R, first_order, two_phase);
   }
   return 0;
+}
+
+// the device's two-phase form of jr3_host_eval
+extern "C" int jr3_host_eval_faces(const jr_plan3d_desc* d, const double* U, const double* dU, double* R,
+                                   int first_order) {
+  return eval(d, U, dU, R, first_order, true);
+}
+
+extern "C" int jr3_host_eval(const jr_plan3d_desc* d, const double* U, const double* dU, double* R,
+                             int first_order) {
+  return eval(d, U, dU, R, first_order, false);
 }
 
 extern "C" int jr3_host_wave_speeds(const jr_plan3d_desc* d, const double* U, double* lam) {
@@ -135,15 +157,15 @@ struct HostOps {
   }
   void residual(const double* U, int out) {
     const bool visc = p.P.mu_inf > 0.0, sa = p.nvar > 5;
-    if (sa) run<double, true, true>(p, U, nullptr, d(out), 0);
-    else if (visc) run<double, true, false>(p, U, nullptr, d(out), 0);
-    else run<double, false, false>(p, U, nullptr, d(out), 0);
+    if (sa) run<double, true, true>(p, U, nullptr, d(out), 0, true);
+    else if (visc) run<double, true, false>(p, U, nullptr, d(out), 0, true);
+    else run<double, false, false>(p, U, nullptr, d(out), 0, true);
   }
   void matvec(const double* U, double, int src, int out) {
     const bool visc = p.P.mu_inf > 0.0, sa = p.nvar > 5;
-    if (sa) run<Dual, true, true>(p, U, d(src), d(out), 1);
-    else if (visc) run<Dual, true, false>(p, U, d(src), d(out), 1);
-    else run<Dual, false, false>(p, U, d(src), d(out), 1);
+    if (sa) run<Dual, true, true>(p, U, d(src), d(out), 1, true);
+    else if (visc) run<Dual, true, false>(p, U, d(src), d(out), 1, true);
+    else run<Dual, false, false>(p, U, d(src), d(out), 1, true);
     for (size_t e = 0; e < N; ++e) d(out)[e] = vdt[e % n] * d(src)[e] + d(out)[e];
   }
   void precondition(const double* U, double cfl, int src, int dst) { line_solve_as(p, U, cfl, d(src), d(dst)); }

@@ -340,3 +340,18 @@ def test_surface_distributions_match_the_reference(harness, z, cases, described,
         ref = z[f"{name}_surface_{key}"]
         scale = max(float(np.abs(ref).max()), 1e-300)
         assert np.allclose(got[key], ref, rtol=0.0, atol=1e-11 * scale), key
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_the_two_phase_residual_is_the_fused_one_bit_for_bit(harness, z, cases, described, name):
+    """The device's two phases -- every face's flux once into a buffer (unwritten entries
+    NaN here, so a read of one would show), then each cell's sums -- give the fused
+    per-cell form's R2, R1 and J.v bit for bit."""
+    desc, _ = described[name]
+    U, v = np.ascontiguousarray(z[f"{name}_U"]), np.ascontiguousarray(z[f"{name}_v"])
+    for dv, fo in ((None, 0), (None, 1), (v, 1)):
+        fused, faces = np.zeros_like(U), np.zeros_like(U)
+        ptr = None if dv is None else dv.ctypes.data
+        assert harness.jr3_host_eval(C.addressof(desc), U.ctypes.data, ptr, fused.ctypes.data, fo) == 0
+        assert harness.jr3_host_eval_faces(C.addressof(desc), U.ctypes.data, ptr, faces.ctypes.data, fo) == 0
+        assert np.array_equal(fused, faces)
