@@ -189,6 +189,17 @@ int jr_plan3d_create(const jr_plan3d_desc* d, jr_plan3d** out) {
     p->factor = sc;
   }
   {
+    size_t most = 1;
+    for (int s = 0; s < d->n_stages; ++s) most = (size_t)d->stage_records[s] > most ? (size_t)d->stage_records[s] : most;
+    void* gb = nullptr;
+    if (cudaMalloc(&gb, most * d->nvar * sizeof(Dual)) != cudaSuccess) {
+      jr_plan3d_destroy(p);
+      return report_error(JR_ENOMEM, "cudaMalloc failed");
+    }
+    p->allocs.push_back(gb);
+    dv.ghost_buf = gb;
+  }
+  {
     const size_t nf = (size_t)(d->NI + 1) * d->NJ * d->NK + (size_t)d->NI * (d->NJ + 1) * d->NK +
                       (size_t)d->NI * d->NJ * (d->NK + 1);
     void* fb = nullptr;

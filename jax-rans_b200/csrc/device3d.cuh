@@ -46,6 +46,7 @@ struct Plan3Dev {
   int line_fp32;               // the line factor and apply in FP32 (the mixed form)
   int line_coupled;            // the SA row coupled to the neighbours' mean flow (6x6 blocks)
   double* face_buf;            // the residual's face fluxes: nvar x (all three families' faces)
+  void* ghost_buf;             // one ghost stage's values: nvar x (the largest stage's records), Dual-sized
   const int* ch_cells;         // [chain * chain_L + k], -1 past the chain's end
   const int* ch_face;          // link k -> k+1: flat index into the three face families, concatenated
   const int* ch_sign;          // +1 / -1: the link face's vector points out of / into cell k; 0 none

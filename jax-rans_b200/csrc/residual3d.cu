@@ -24,9 +24,15 @@ __global__ void k3_prim(Plan3Dev p, const double* __restrict__ U, const double* 
 }
 
 template <class T>
-__global__ void k3_ghost_stage(Plan3Dev p, const T* __restrict__ in, T* __restrict__ out, int r0, int r1) {
+__global__ void k3_ghost_values(Plan3Dev p, const T* __restrict__ Q, int r0, int r1, T* __restrict__ buf) {
   for (int r = r0 + blockIdx.x * blockDim.x + threadIdx.x; r < r1; r += gridDim.x * blockDim.x)
-    ghost_record(p, in, out, r);
+    ghost_value(p, Q, r, r0, r1 - r0, buf);
+}
+
+template <class T>
+__global__ void k3_ghost_store(Plan3Dev p, const T* __restrict__ buf, int r0, int r1, T* __restrict__ Q) {
+  for (int r = r0 + blockIdx.x * blockDim.x + threadIdx.x; r < r1; r += gridDim.x * blockDim.x)
+    ghost_store(p, buf, r, r0, r1 - r0, Q);
 }
 
 // phase 1: every face's flux once (one thread per face of the three families)
@@ -46,34 +52,29 @@ __global__ void __launch_bounds__(128) k3_cell_sum(Plan3Dev p, const T* __restri
 }
 
 // ---- launchers
+// the ghost stages on the canvas A in place, each in two passes through p.ghost_buf
 template <class T>
-static void fill3(const Plan3Dev& p, T* A, T* B, cudaStream_t st) {
-  const size_t bytes = (size_t)p.nvar * p.NI * p.NJ * p.NK * sizeof(T);
-  T* cur = A;
-  T* nxt = B;
+static void fill3(const Plan3Dev& p, T* A, cudaStream_t st) {
+  T* buf = static_cast<T*>(p.ghost_buf);
   for (int s = 0; s < p.n_stages; ++s) {
-    cudaMemcpyAsync(nxt, cur, bytes, cudaMemcpyDeviceToDevice, st);
     const int r0 = p.stage_off[s], r1 = p.stage_off[s + 1];
     const int blocks = (r1 - r0 + 127) / 128;
     if (blocks > 0) {
-      counted3();
-      k3_ghost_stage<T><<<blocks, 128, 0, st>>>(p, cur, nxt, r0, r1);
+      counted3(2);
+      k3_ghost_values<T><<<blocks, 128, 0, st>>>(p, A, r0, r1, buf);
+      k3_ghost_store<T><<<blocks, 128, 0, st>>>(p, buf, r0, r1, A);
     }
-    T* t = cur;
-    cur = nxt;
-    nxt = t;
   }
-  if (cur != A) cudaMemcpyAsync(A, cur, bytes, cudaMemcpyDeviceToDevice, st);
 }
 
 template <class T>
-static void residual3_t(const Plan3Dev& p, const double* U, const double* dU, double* R, T* A, T* B, bool first_order,
-                        cudaStream_t st) {
+static void residual3_t(const Plan3Dev& p, const double* U, const double* dU, double* R, T* A, T* /*B*/,
+                        bool first_order, cudaStream_t st) {
   const int n = p.NI * p.NJ * p.NK;
   const int blocks = (n + 127) / 128;
   counted3(2);   // the primitive canvas and, below, the residual
   k3_prim<T><<<blocks, 128, 0, st>>>(p, U, dU, A);
-  fill3(p, A, B, st);
+  fill3(p, A, st);
   const bool visc = p.P.mu_inf > 0.0, sa = p.nvar > 5;
   const int nf = face_count(p, 0) + face_count(p, 1) + face_count(p, 2);
   const int fblocks = (nf + 127) / 128;
@@ -100,7 +101,7 @@ void launch_wall_loads3(const Plan3Dev& p, const double* U, double* loads, void*
   const int n = p.NI * p.NJ * p.NK;
   counted3(p.n_walls > 0 ? 2 : 1);
   k3_prim<double><<<(n + 127) / 128, 128, 0, st>>>(p, U, nullptr, (double*)A);
-  fill3(p, (double*)A, (double*)B, st);
+  fill3(p, (double*)A, st);
   if (p.n_walls > 0) k3_wall_loads<<<(p.n_walls + 127) / 128, 128, 0, st>>>(p, (const double*)A, loads);
 }
 

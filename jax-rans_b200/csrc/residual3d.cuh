@@ -30,6 +30,29 @@ __host__ __device__ __forceinline__ void ghost_record(const Plan3Dev& p, const T
   for (int v = 0; v < p.nvar; ++v) out[(size_t)v * n + ghost] = o[v];
 }
 
+// The same stage in place, in two passes: every record's value from the canvas as it was
+// before the stage (into buf, slot r - r0 of count), then every value to its ghost.  A
+// stage writes each ghost once, so the two passes give the double-buffered stage's canvas
+// without copying the canvas.
+template <class T>
+__host__ __device__ __forceinline__ void ghost_value(const Plan3Dev& p, const T* Q, int r, int r0, int count, T* buf) {
+  const int n = p.NI * p.NJ * p.NK;
+  const int ghost = p.g_ghost[r], src = p.g_source[r], kind = p.g_kind[r];
+  if (ghost < 0 || ghost >= n || src < 0 || src >= n) return;   // validated on the host
+  T q[NV3_MAX], o[NV3_MAX];
+  for (int v = 0; v < p.nvar; ++v) q[v] = Q[(size_t)v * n + src];
+  condition3(kind, q, p.g_normal[3 * r], p.g_normal[3 * r + 1], p.g_normal[3 * r + 2], p.P, p.nvar, o);
+  for (int v = 0; v < p.nvar; ++v) buf[(size_t)v * count + (r - r0)] = o[v];
+}
+
+template <class T>
+__host__ __device__ __forceinline__ void ghost_store(const Plan3Dev& p, const T* buf, int r, int r0, int count, T* Q) {
+  const int n = p.NI * p.NJ * p.NK;
+  const int ghost = p.g_ghost[r], src = p.g_source[r];
+  if (ghost < 0 || ghost >= n || src < 0 || src >= n) return;
+  for (int v = 0; v < p.nvar; ++v) Q[(size_t)v * n + ghost] = buf[(size_t)v * count + (r - r0)];
+}
+
 // ---- geometry access
 // faces of family a on the canvas (one more than the cells along a)
 __host__ __device__ __forceinline__ int face_count(const Plan3Dev& p, int a) {

@@ -64,6 +64,7 @@ def harness(tmp_path_factory):
                        "jr3_host_newton_steps": [p, p, p, p, p, p, i, p],
                        "jr3_host_forces": [p, p, d, d, p, p],
                        "jr3_host_wall_loads": [p, p, p],
+                       "jr3_host_fill": [p, p, p, i],
                        "jr3_host_wall_distance": [p, C.c_longlong, p, i, p, i]}.items():
         f = getattr(lib, name)
         f.restype, f.argtypes = C.c_int, args

@@ -2,6 +2,7 @@
 // residual3d.cuh) run on the host, in the order the device runs them, on a plan given by
 // its C-ABI descriptor -- a check of the kernels' indexing and arithmetic without a GPU.
 // Nothing of the library calls this; it is built by tests/test_host3d.py.
+#include <algorithm>
 #include <cmath>
 #include <utility>
 #include <vector>
@@ -13,19 +14,39 @@
 
 using namespace jr;
 
+// the ghost stages in place as the device runs them: each stage's values first (from the
+// canvas before the stage), then the stores
+template <class T>
+static void fill_ghosts(const Plan3Dev& p, std::vector<T>& A) {
+  for (int s = 0; s < p.n_stages; ++s) {
+    const int r0 = p.stage_off[s], r1 = p.stage_off[s + 1];
+    std::vector<T> buf((size_t)p.nvar * (r1 - r0 > 0 ? r1 - r0 : 1));
+    for (int r = r0; r < r1; ++r) ghost_value(p, A.data(), r, r0, r1 - r0, buf.data());
+    for (int r = r0; r < r1; ++r) ghost_store(p, buf.data(), r, r0, r1 - r0, A.data());
+  }
+}
+
+// the ghost stages double-buffered (each stage from a copy of the canvas): the gather
+// form's meaning, for checking the in-place passes against it
+template <class T>
+static void fill_ghosts_copying(const Plan3Dev& p, std::vector<T>& A) {
+  std::vector<T> B;
+  for (int s = 0; s < p.n_stages; ++s) {
+    B = A;
+    for (int r = p.stage_off[s]; r < p.stage_off[s + 1]; ++r) ghost_record(p, A.data(), B.data(), r);
+    std::swap(A, B);
+  }
+}
+
 // the residual in the fused form (each cell evaluates its six faces), or in the device's
 // two phases (every face once into a buffer, unwritten entries NaN, then the cell sums)
 template <class T, bool VISC, bool SA>
 static void run(const Plan3Dev& p, const double* U, const double* dU, double* R, int first_order,
                 bool two_phase = false) {
   const int n = p.NI * p.NJ * p.NK;
-  std::vector<T> A((size_t)p.nvar * n), B((size_t)p.nvar * n);
+  std::vector<T> A((size_t)p.nvar * n);
   for (int c = 0; c < n; ++c) prim_cell(p, U, dU, A.data(), c);
-  for (int s = 0; s < p.n_stages; ++s) {
-    B = A;
-    for (int r = p.stage_off[s]; r < p.stage_off[s + 1]; ++r) ghost_record(p, A.data(), B.data(), r);
-    std::swap(A, B);
-  }
+  fill_ghosts(p, A);
   if (!two_phase) {
     for (int c = 0; c < n; ++c) residual_cell<T, VISC, SA>(p, A.data(), U, dU, R, first_order, c);
     return;
@@ -244,13 +265,9 @@ extern "C" int jr3_host_newton_steps(const jr_plan3d_desc* d, const double* conf
 extern "C" int jr3_host_wall_loads(const jr_plan3d_desc* d, const double* U, double* loads) {
   const Plan3Dev p = plan_of(d);
   const int n = p.NI * p.NJ * p.NK;
-  std::vector<double> A((size_t)p.nvar * n), B((size_t)p.nvar * n);
+  std::vector<double> A((size_t)p.nvar * n);
   for (int c = 0; c < n; ++c) prim_cell(p, U, (const double*)nullptr, A.data(), c);
-  for (int s = 0; s < p.n_stages; ++s) {
-    B = A;
-    for (int r = p.stage_off[s]; r < p.stage_off[s + 1]; ++r) ghost_record(p, A.data(), B.data(), r);
-    std::swap(A, B);
-  }
+  fill_ghosts(p, A);
   for (int w = 0; w < p.n_walls; ++w) wall_load(p, A.data(), w, loads + (size_t)7 * w);
   return 0;
 }
@@ -279,5 +296,18 @@ extern "C" int jr3_host_wall_distance(const double* points, long long n, const d
     }
     out[i] = m > 0 ? candidates_distance(p, c, faces) : INFINITY;
   }
+  return 0;
+}
+
+// the ghost-filled primitive canvas (nvar x canvas) at U, in place (mode 0) or
+// double-buffered (mode 1)
+extern "C" int jr3_host_fill(const jr_plan3d_desc* d, const double* U, double* Q, int mode) {
+  const Plan3Dev p = plan_of(d);
+  const int n = p.NI * p.NJ * p.NK;
+  std::vector<double> A((size_t)p.nvar * n);
+  for (int c = 0; c < n; ++c) prim_cell(p, U, (const double*)nullptr, A.data(), c);
+  if (mode == 0) fill_ghosts(p, A);
+  else fill_ghosts_copying(p, A);
+  std::copy(A.begin(), A.end(), Q);
   return 0;
 }

@@ -355,3 +355,23 @@ def test_the_two_phase_residual_is_the_fused_one_bit_for_bit(harness, z, cases, 
         assert harness.jr3_host_eval(C.addressof(desc), U.ctypes.data, ptr, fused.ctypes.data, fo) == 0
         assert harness.jr3_host_eval_faces(C.addressof(desc), U.ctypes.data, ptr, faces.ctypes.data, fo) == 0
         assert np.array_equal(fused, faces)
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_the_in_place_ghost_fill_is_the_double_buffered_one(harness, z, cases, described, name):
+    """The device's ghost stages in place (each stage's values first, then its stores)
+    give the double-buffered stages' canvas bit for bit: a stage writes each ghost once."""
+    desc, _ = described[name]
+    U = np.ascontiguousarray(z[f"{name}_U"])
+    inplace, copying = np.zeros_like(U), np.zeros_like(U)
+    assert harness.jr3_host_fill(C.addressof(desc), U.ctypes.data, inplace.ctypes.data, 0) == 0
+    assert harness.jr3_host_fill(C.addressof(desc), U.ctypes.data, copying.ctypes.data, 1) == 0
+    assert np.array_equal(inplace, copying)
+    _, plan = cases[name]
+    from jaxrans_b200.native3d import records_of
+    rec = records_of(plan)
+    at = 0
+    for count in rec.counts:                       # each stage writes a ghost once
+        ghosts = rec.ghost[at:at + count]
+        assert len(np.unique(ghosts)) == len(ghosts)
+        at += count
