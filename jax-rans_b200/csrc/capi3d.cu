@@ -23,7 +23,6 @@ struct jr_plan3d {
   Plan3Dev dev{};
   std::vector<void*> allocs;
   void* A = nullptr;   // primitive canvases (Dual-sized: the J.v needs value and tangent)
-  void* B = nullptr;
   void* factor = nullptr;      // the line factor: n_chains * chain_L * FACTOR3 words (FP32 in the mixed form)
   size_t n_canvas = 0;
   Newton3Config cfg{};
@@ -211,11 +210,11 @@ int jr_plan3d_create(const jr_plan3d_desc* d, jr_plan3d** out) {
     dv.face_buf = static_cast<double*>(fb);
   }
   const size_t work = (size_t)d->nvar * n * sizeof(Dual);
-  if (cudaMalloc(&p->A, work) != cudaSuccess || (p->allocs.push_back(p->A), cudaMalloc(&p->B, work)) != cudaSuccess) {
+  if (cudaMalloc(&p->A, work) != cudaSuccess) {
     jr_plan3d_destroy(p);
     return report_error(JR_ENOMEM, "cudaMalloc failed");
   }
-  p->allocs.push_back(p->B);
+  p->allocs.push_back(p->A);
   // the Newton step's configuration and vectors
   if (d->krylov_subspace < 1 || d->krylov_subspace > MAX_RESTART3 || d->krylov_restarts < 1 || d->preconditioner < 0 ||
       d->preconditioner > 2) {
@@ -250,14 +249,14 @@ int jr_plan3d_create(const jr_plan3d_desc* d, jr_plan3d** out) {
 
 int jr_residual3d(jr_plan3d* plan, const double* U, double* R, int32_t first_order) {
   if (!plan || !U || !R) return report_error(JR_EINVAL, "null argument");
-  launch_residual3(plan->dev, U, R, plan->A, plan->B, first_order != 0, plan->st);
+  launch_residual3(plan->dev, U, R, plan->A, first_order != 0, plan->st);
   if (cudaStreamSynchronize(plan->st) != cudaSuccess) return check3("jr_residual3d");
   return check3("jr_residual3d");
 }
 
 int jr_jvp3d(jr_plan3d* plan, const double* U, const double* v, double* Jv) {
   if (!plan || !U || !v || !Jv) return report_error(JR_EINVAL, "null argument");
-  launch_jvp3(plan->dev, U, v, Jv, plan->A, plan->B, plan->st);
+  launch_jvp3(plan->dev, U, v, Jv, plan->A, plan->st);
   if (cudaStreamSynchronize(plan->st) != cudaSuccess) return check3("jr_jvp3d");
   return check3("jr_jvp3d");
 }
@@ -286,7 +285,6 @@ int jr_newton_steps3d(jr_plan3d* plan, double* U, int32_t n_steps, double* cfl, 
   ops.n = plan->n_canvas;
   ops.N = (size_t)plan->dev.nvar * plan->n_canvas;
   ops.A = plan->A;
-  ops.B = plan->B;
   ops.factor = plan->factor;
   ops.line = plan->cfg.preconditioner >= 1;
   ops.st = plan->st;
@@ -310,7 +308,7 @@ int jr_forces3d(jr_plan3d* plan, const double* U, double area, double length, co
   const int nw = plan->dev.n_walls;
   std::vector<double> loads((size_t)nw * 7);
   if (nw > 0) {
-    launch_wall_loads3(plan->dev, U, plan->loads, plan->A, plan->B, plan->st);
+    launch_wall_loads3(plan->dev, U, plan->loads, plan->A, plan->st);
     cudaMemcpyAsync(loads.data(), plan->loads, loads.size() * sizeof(double), cudaMemcpyDeviceToHost, plan->st);
   }
   if (cudaStreamSynchronize(plan->st) != cudaSuccess) return check3("jr_forces3d");
@@ -324,7 +322,7 @@ int jr_wall_loads3d(jr_plan3d* plan, const double* U, double* out) {
   if (!plan || !U || (!out && plan->dev.n_walls > 0)) return report_error(JR_EINVAL, "null argument");
   const int nw = plan->dev.n_walls;
   if (nw > 0) {
-    launch_wall_loads3(plan->dev, U, plan->loads, plan->A, plan->B, plan->st);
+    launch_wall_loads3(plan->dev, U, plan->loads, plan->A, plan->st);
     cudaMemcpyAsync(out, plan->loads, (size_t)nw * 7 * sizeof(double), cudaMemcpyDeviceToHost, plan->st);
   }
   if (cudaStreamSynchronize(plan->st) != cudaSuccess) return check3("jr_wall_loads3d");

@@ -231,11 +231,11 @@ __host__ __device__ __forceinline__ void condition3(int kind, const T* q, double
   }
 }
 
-void launch_residual3(const Plan3Dev& p, const double* U, double* R, void* A, void* B, bool first_order,
-                      cudaStream_t st);
-void launch_jvp3(const Plan3Dev& p, const double* U, const double* v, double* Jv, void* A, void* B, cudaStream_t st);
+void launch_residual3(const Plan3Dev& p, const double* U, double* R, void* A, bool first_order, cudaStream_t st);
+// the exact tangent of the first-order residual at U along v (A: a Dual-sized canvas)
+void launch_jvp3(const Plan3Dev& p, const double* U, const double* v, double* Jv, void* A, cudaStream_t st);
 void launch_wave_speeds3(const Plan3Dev& p, const double* U, double* lam, cudaStream_t st);
-void launch_wall_loads3(const Plan3Dev& p, const double* U, double* loads, void* A, void* B, cudaStream_t st);
+void launch_wall_loads3(const Plan3Dev& p, const double* U, double* loads, void* A, cudaStream_t st);
 void launch_line_factor3(const Plan3Dev& p, const double* U, double cfl, void* F, cudaStream_t st);
 void launch_line_apply3(const Plan3Dev& p, const void* F, const double* r, double* z, cudaStream_t st);
 void launch_precondition3(const Plan3Dev& p, const double* U, double cfl, const double* r, double* z, void* F,

@@ -172,10 +172,10 @@ void DeviceOps3::prepare(const double* U, double cfl) {
   if (line) launch_line_factor3(p, U, cfl, factor, st);
 }
 
-void DeviceOps3::residual(const double* U, int out) { launch_residual3(p, U, v(out), A, B, false, st); }
+void DeviceOps3::residual(const double* U, int out) { launch_residual3(p, U, v(out), A, false, st); }
 
 void DeviceOps3::matvec(const double* U, double, int src, int out) {
-  launch_jvp3(p, U, v(src), v(out), A, B, st);
+  launch_jvp3(p, U, v(src), v(out), A, st);
   counted3();
   k3_vdt_add<<<grid_of(N), 256, 0, st>>>(N, n, vdt, v(src), v(out));
 }

@@ -12,7 +12,7 @@ struct DeviceOps3 {
   enum { R_ = 0, Z_, W_, T_, RES_, B_, DU_, ACT_, BASE };
   Plan3Dev p;
   size_t N = 0, n = 0;
-  void *A = nullptr, *B = nullptr;   // primitive canvases of the residual / J.v
+  void* A = nullptr;                 // the primitive canvas of the residual / J.v (Dual-sized)
   void* factor = nullptr;            // the line factor (computed in prepare when line)
   bool line = false;
   double* vecs = nullptr;

@@ -68,8 +68,8 @@ static void fill3(const Plan3Dev& p, T* A, cudaStream_t st) {
 }
 
 template <class T>
-static void residual3_t(const Plan3Dev& p, const double* U, const double* dU, double* R, T* A, T* /*B*/,
-                        bool first_order, cudaStream_t st) {
+static void residual3_t(const Plan3Dev& p, const double* U, const double* dU, double* R, T* A, bool first_order,
+                        cudaStream_t st) {
   const int n = p.NI * p.NJ * p.NK;
   const int blocks = (n + 127) / 128;
   counted3(2);   // the primitive canvas and, below, the residual
@@ -97,7 +97,7 @@ __global__ void k3_wall_loads(Plan3Dev p, const double* __restrict__ Q, double* 
 }
 
 // the loads on every wall face (7 each) at U: the primitive canvas ghost-filled first
-void launch_wall_loads3(const Plan3Dev& p, const double* U, double* loads, void* A, void* B, cudaStream_t st) {
+void launch_wall_loads3(const Plan3Dev& p, const double* U, double* loads, void* A, cudaStream_t st) {
   const int n = p.NI * p.NJ * p.NK;
   counted3(p.n_walls > 0 ? 2 : 1);
   k3_prim<double><<<(n + 127) / 128, 128, 0, st>>>(p, U, nullptr, (double*)A);
@@ -105,13 +105,12 @@ void launch_wall_loads3(const Plan3Dev& p, const double* U, double* loads, void*
   if (p.n_walls > 0) k3_wall_loads<<<(p.n_walls + 127) / 128, 128, 0, st>>>(p, (const double*)A, loads);
 }
 
-void launch_residual3(const Plan3Dev& p, const double* U, double* R, void* A, void* B, bool first_order,
-                      cudaStream_t st) {
-  residual3_t<double>(p, U, nullptr, R, (double*)A, (double*)B, first_order, st);
+void launch_residual3(const Plan3Dev& p, const double* U, double* R, void* A, bool first_order, cudaStream_t st) {
+  residual3_t<double>(p, U, nullptr, R, (double*)A, first_order, st);
 }
 
-void launch_jvp3(const Plan3Dev& p, const double* U, const double* v, double* Jv, void* A, void* B, cudaStream_t st) {
-  residual3_t<Dual>(p, U, v, Jv, (Dual*)A, (Dual*)B, true, st);
+void launch_jvp3(const Plan3Dev& p, const double* U, const double* v, double* Jv, void* A, cudaStream_t st) {
+  residual3_t<Dual>(p, U, v, Jv, (Dual*)A, true, st);
 }
 
 }  // namespace jr
