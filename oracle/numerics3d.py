@@ -42,6 +42,7 @@ class Model3:
     sutherland: float | None = None
     sa: bool = False
     distance: np.ndarray | None = None
+    c_cr1: float = 0.0              # QCR2000 on the SA model's stress (0: off)
 
     @property
     def nvar(self) -> int:
@@ -336,16 +337,34 @@ def temperature(q, g):
     return g * q[4] / q[0]
 
 
-def viscous_flux(vel, gv, gt, s, mu, k):
-    """``F_v . S`` with ``gv[a][b] = d v_a / d x_b``."""
+def qcr_stress(gv, mu_t, c_cr1):
+    """QCR2000's addition to the stress (``spalart_allmaras.py:197-216``): ``-c_cr1 (O_ik
+    tau_jk + O_jk tau_ik)``, ``O = (grad V - grad V^T) / |grad V|`` (1 in place of the norm
+    where grad V is 0), ``tau = mu_t (grad V + grad V^T - 2/3 div V I)``."""
+    square = sum(gv[a][b] * gv[a][b] for a in range(3) for b in range(3))
+    positive = np.real(square) > 0.0
+    norm = np.where(positive, np.sqrt(np.where(positive, square, 1.0)), 1.0)
+    div = gv[0][0] + gv[1][1] + gv[2][2]
+    rot = [[(gv[a][b] - gv[b][a]) / norm for b in range(3)] for a in range(3)]
+    tau = [[mu_t * (gv[a][b] + gv[b][a] - ((2.0 / 3.0) * div if a == b else 0.0)) for b in range(3)]
+           for a in range(3)]
+    prod = [[rot[i][0] * tau[j][0] + rot[i][1] * tau[j][1] + rot[i][2] * tau[j][2] for j in range(3)]
+            for i in range(3)]
+    return [[-c_cr1 * (prod[a][b] + prod[b][a]) for b in range(3)] for a in range(3)]
+
+
+def viscous_flux(vel, gv, gt, s, mu, k, extra=None):
+    """``F_v . S`` with ``gv[a][b] = d v_a / d x_b``; ``extra`` added to the stress."""
     div = gv[0][0] + gv[1][1] + gv[2][2]
     ttd = (2.0 / 3.0) * div
 
     def tau(a, b):
         if a == b:
-            return mu * (2.0 * gv[a][a] - ttd)
-        lo, hi = min(a, b), max(a, b)
-        return mu * (gv[lo][hi] + gv[hi][lo])
+            t = mu * (2.0 * gv[a][a] - ttd)
+        else:
+            lo, hi = min(a, b), max(a, b)
+            t = mu * (gv[lo][hi] + gv[hi][lo])
+        return t if extra is None else t + extra[a][b]
 
     force = np.stack([dot(np.stack([tau(a, b) for b in range(3)]), s) for a in range(3)])
     energy = dot(vel, force) + k * dot(gt, s)
@@ -369,7 +388,8 @@ def viscous_fluxes(p1, centres, faces, model: Model3, mu_t=None, grads=None):
             k = k + mu_t[a] / (PR_TURB * (g - 1.0))
         G = grads[a]
         gv = [[G[b, c] for b in range(3)] for c in range(3)]       # gv[component][direction]
-        out.append(viscous_flux(vel, gv, G[:, 3], faces[a], mu, k))
+        extra = qcr_stress(gv, mu_t[a], model.c_cr1) if mu_t is not None and model.c_cr1 else None
+        out.append(viscous_flux(vel, gv, G[:, 3], faces[a], mu, k, extra))
     return out
 
 
