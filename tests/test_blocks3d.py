@@ -396,3 +396,29 @@ def test_the_3d_oracle_gives_the_reference_residual_and_jvp(z, cases, name):
     assert rows_rel(Jv[:5], ref[:5], inside) < 1e-11
     if Jv.shape[0] > 5:
         assert rows_rel(Jv[5:], ref[5:], inside) < 1e-10
+
+
+@pytest.mark.parametrize("name", WALLED)
+def test_the_3d_oracle_gives_the_reference_forces_and_surface(z, cases, name):
+    """The oracle's wall loads (``oracle.forces3d``) on the multi-block walls: the force
+    coefficients and, face by face, cp and the skin-friction vector of the reference."""
+    from oracle import forces3d as f3
+    from oracle import numerics3d as n3
+    from jaxrans_b200.solver3d import physics3
+    case, plan = cases[name]
+    ph = physics3(case)
+    model = n3.Model3(plan, ph["q_inf"], ph["gamma"], ph["flux"], ph["limiter"], ph["kappa"], ph["mu_inf"],
+                      ph["sutherland"], len(ph["q_inf"]) == 6, plan.distance, ph["c_cr1"])
+    U = z[f"{name}_U"]
+    spec = case.grid_spec
+    f = f3.forces(U, model, spec.reference_area, spec.reference_length, tuple(spec.moment_centre))
+    assert np.allclose(f, z[f"{name}_forces"], rtol=1e-11, atol=1e-16)
+    p, S, shear = f3.wall_loads(U, model)
+    q = 0.5 * case.flow.mach ** 2
+    ref_cp = z[f"{name}_surface_cp"]
+    assert np.allclose(p / q, ref_cp, rtol=0.0, atol=1e-11 * np.abs(ref_cp).max())
+    if not case.flow.inviscid:
+        area = np.linalg.norm(S, axis=0)
+        for c, axis in enumerate("xyz"):
+            ref = z[f"{name}_surface_cf_{axis}"]
+            assert np.allclose(shear[c] / area / q, ref, rtol=0.0, atol=1e-11 * np.abs(ref).max())
