@@ -422,3 +422,21 @@ def test_the_3d_oracle_gives_the_reference_forces_and_surface(z, cases, name):
         for c, axis in enumerate("xyz"):
             ref = z[f"{name}_surface_cf_{axis}"]
             assert np.allclose(shear[c] / area / q, ref, rtol=0.0, atol=1e-11 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("name", WALLED)
+def test_the_3d_oracle_gives_the_reference_line_solve(z, cases, name):
+    """The oracle's line_j (cyclic reduction and block Thomas) across block interfaces:
+    chains along each block's wall-normal index, against the reference's solve."""
+    from oracle import implicit3d as i3
+    from oracle import numerics3d as n3
+    from jaxrans_b200.solver3d import physics3
+    case, plan = cases[name]
+    ph = physics3(case)
+    model = n3.Model3(plan, ph["q_inf"], ph["gamma"], ph["flux"], ph["limiter"], ph["kappa"], ph["mu_inf"],
+                      ph["sutherland"], len(ph["q_inf"]) == 6, plan.distance, ph["c_cr1"])
+    U, r = z[f"{name}_U"], z[f"{name}_prec_r"]
+    lam = n3.wave_speeds(U, model)
+    for solver in ("cr", "thomas"):
+        got = i3.precondition(U, lam, 25.0, model, solver=solver)(r)
+        assert rows_rel(got, z[f"{name}_prec_z"], plan.interior) < 1e-10, solver
