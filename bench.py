@@ -218,16 +218,17 @@ def run_wing3d(args) -> int:
     if args.impl == "reference":
         if rank != 0:
             return 0
+        from jaxrans_b200.workloads import wing3d_cells
         per_step, cells = oracle3d_step_seconds(max(1, min(args.steps, 2)), 1)
-        _, plan = wing3d_setup(args.workload)
-        value = cells / (per_step * plan.cells)
+        total = wing3d_cells(args.workload)
+        value = cells / (per_step * total)
         sample = (f"Newton steps of the 3D oracle (NumPy FP64, complex-step J.v) on the wing_ch_4blk_small grid "
-                  f"({cells} cells), {per_step:.1f} s each, scaled by cells to the {plan.cells}-cell workload")
+                  f"({cells} cells), {per_step:.1f} s each, scaled by cells to the {total}-cell workload")
         print(json.dumps({"impl": "reference", "metric": METRIC3D, "value": value, "unit": "steps/s",
                           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                           "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
                           "vs_baseline": None, "dtype": "f64", "data": "synthetic (generated wing and grid)",
-                          "config": {"workload": args.workload, "cells": plan.cells},
+                          "config": {"workload": args.workload, "cells": total},
                           "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "port",
                                            "sample": sample},
                           "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0,

@@ -123,6 +123,13 @@ WING3D_NUMERICS = {"convective_fluxes": {"riemann_solver": "hllc", "limiter": "v
                    "convergence": {"max_iters": 6000, "tol": 1e-10, "block_iters": 20}}
 
 
+def wing3d_cells(name: str) -> int:
+    """Cells of the 3D workload's grid: four blocks, each half the C round the section by
+    the normal layers by the wing's or the tip region's stations."""
+    w = WING3D[name]
+    return 2 * (w["cells_airfoil"] // 2 + w["cells_wake"]) * w["cells_normal"] * (w["cells_span"] + w["cells_tip"])
+
+
 def wing3d_case(name: str, directory, **numerical) -> Case:
     """Write the 3D workload ``name`` (its Plot3D grid ``grid.x``, ``case.json`` and
     ``numerical.json``) into ``directory`` and load it as a case."""

@@ -440,3 +440,14 @@ def test_the_3d_oracle_gives_the_reference_line_solve(z, cases, name):
     for solver in ("cr", "thomas"):
         got = i3.precondition(U, lam, 25.0, model, solver=solver)(r)
         assert rows_rel(got, z[f"{name}_prec_z"], plan.interior) < 1e-10, solver
+
+
+def test_the_wing_workloads_cell_counts():
+    """``workloads.wing3d_cells`` (the bench's cell count, no plan built) is the generated
+    grid's: config 5's 3.93M cells and the small wing's."""
+    from jaxrans_b200.geometry import section_source
+    from jaxrans_b200.grid3d import wing_ch_blocks
+    from jaxrans_b200.workloads import WING3D, WING3D_PLANFORM, wing3d_cells
+    assert wing3d_cells("wing_ch_4blk") == 3932160
+    g = wing_ch_blocks(section_source("naca0012"), **WING3D["wing_ch_4blk_small"], **WING3D_PLANFORM)
+    assert wing3d_cells("wing_ch_4blk_small") == sum(int(np.prod([n - 1 for n in b.shape[1:]])) for b in g.blocks)
