@@ -287,7 +287,7 @@ def run_wing3d(args) -> int:
     if rank == 0:
         cpu = None
         if not args.no_cpu_baseline and world == 1:
-            per_step, cells = oracle3d_step_seconds(1, 1)
+            per_step, cells = oracle3d_step_seconds(1, 0)   # NumPy: no warm-up to amortise
             cpu = {"value": cells / (per_step * plan.cells), "unit": "steps/s", "cores": 1, "kind": "port",
                    "sample": f"one Newton step of the 3D oracle on the wing_ch_4blk_small grid ({cells} cells), "
                              f"{per_step:.1f} s, scaled by cells"}
