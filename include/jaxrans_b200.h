@@ -139,7 +139,9 @@ int jr_residual(jr_plan* plan, const double* U, double* R, int first_order);
  * that loads it, so the call allocates nothing and writes no work buffer of the plan; a
  * plan that needs more scratch is refused with JR_EINVAL.  The first call on a device
  * looks up the array's address there (set-up): make it with the plan's device current
- * and before any stream capture.  Every call on a device shares the one array, which
+ * and before any stream capture.  The address is kept for the life of the process, so a
+ * cudaDeviceReset (which re-creates the device's context) makes it stale: do not use the
+ * library across a device reset.  Every call on a device shares the one array, which
  * keeps the last call's contents (the canvas part is cleared by each call): calls whose
  * work overlaps on the GPU -- on other streams, or for other plans -- race on it.  No
  * counterpart in the reference, which has no FFI and allocates through XLA.  Device

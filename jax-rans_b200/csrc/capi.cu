@@ -1172,7 +1172,11 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH
 
 constexpr int NOALLOC_MAX_DEVICES = 64;
 // the array's device address on each device; the name g_noalloc_scratch in host code is
-// only a host-side stand-in, never a device address
+// only a host-side stand-in, never a device address.  Looked up once per device and kept
+// for the life of the process: a cudaDeviceReset (or anything else that re-creates the
+// device's primary context) leaves the kept address stale, so the library must not be
+// used across one.  Host threads may race on an entry the first time; the race is benign,
+// as every writer stores the same address.
 static unsigned char* g_noalloc_ptr[NOALLOC_MAX_DEVICES];
 
 static size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
@@ -1223,8 +1227,9 @@ extern "C" int jr_residual_noalloc(jr_plan* plan, const double* U, double* R, in
   CaseDev* table = reinterpret_cast<CaseDev*>(base);
   double* qg = reinterpret_cast<double*>(base + table_bytes);
   double* tile_partial = reinterpret_cast<double*>(base + table_bytes + qg_bytes);
-  // the array keeps the last call's contents: the ghost canvas starts at zero, as the
-  // plan's own does, so canvas cells that no ghost record fills read the same values
+  // the array keeps the last call's contents: clearing the ghost canvas makes the result
+  // independent of earlier calls (the residual reads a canvas entry of this buffer only
+  // where a ghost record has just written it)
   if (cudaMemsetAsync(qg, 0, plan->total_vec * sizeof(double), plan->st) != cudaSuccess)
     return cuda_check("jr_residual_noalloc: clear");
   k_noalloc_table<<<1, 32, 0, plan->st>>>(plan->cases, table, plan->n_cases, U, R, qg, tile_partial);

@@ -1,13 +1,10 @@
-"""The 3D device path (jr_residual3d, jr_jvp3d) against the 3D oracle and the
-reference's own 3D outputs on the C-H wing fixture (tests/golden/ch_sa3d.npz).
-
-The 3D kernels are new and have not yet run on a B200; these tests are enabled with
-JR_RUN_3D=1 until they have (a failure must not stop the rest of the device suite)."""
+"""The 3D device path (jr_residual3d, jr_jvp3d, the line solve, the Newton step, the
+forces and the wall distance) against the reference's own 3D outputs on the C-H wing
+fixture (tests/golden/ch_sa3d.npz) and the multi-block fixtures (tests/golden/blocks3d.npz)."""
 
 from __future__ import annotations
 
 import json
-import os
 from pathlib import Path
 
 import numpy as np
@@ -18,9 +15,7 @@ from jaxrans_b200.geometry import section_source
 from jaxrans_b200.grid3d import wing_block
 from jaxrans_b200.plan3d import build_plan3d
 
-pytestmark = [pytest.mark.gpu,
-              pytest.mark.skipif(os.environ.get("JR_RUN_3D") != "1",
-                                 reason="the 3D device path has not run on a B200 yet (JR_RUN_3D=1 runs it)")]
+pytestmark = pytest.mark.gpu
 
 GOLDEN = Path(__file__).resolve().parent / "golden" / "ch_sa3d.npz"
 KINDS = {"wall": "no_slip_wall", "farfield": "far_field", "root": "symmetry", "tip": "symmetry"}

@@ -77,3 +77,19 @@ def test_noalloc_refuses_a_plan_beyond_its_scratch(cuda):
     assert dev.lib.jr_residual_noalloc(dev.handle, U.data_ptr(), R.data_ptr(), 0) == 1
     assert b"8 MiB" in dev.lib.jr_last_error()
     assert bool((R == 7.0).all())
+
+
+def test_noalloc_residual_after_newton_steps(cuda):
+    """After Newton steps the plan's own ghost canvas holds that march's values, not zeros;
+    the two entry points still agree on the plan's current state."""
+    import torch
+    from jaxrans_b200.native import DevicePlan
+    z, case, plan = load("c_sa")
+    dev = DevicePlan(plan, case.flow, case.numerics, case.implicit)
+    dev.set_state(z["rand0_U"], 25.0, float("inf"))
+    dev.newton_steps(3)
+    U_host = dev.get_state()[0]
+    U = torch.as_tensor(U_host, device="cuda").contiguous()
+    for first in (False, True, False):
+        out, ref = residual_pair(dev, U, first)
+        assert row_rel(out, ref) < 1e-12
