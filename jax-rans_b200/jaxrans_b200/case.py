@@ -32,8 +32,22 @@ class CaseError(ValueError):
     """A case that cannot be run as written."""
 
 
+# what each schema type accepts (a bool is neither a number nor an integer)
+_ACCEPTS = {
+    "number": lambda v: isinstance(v, (int, float)) and not isinstance(v, bool),
+    "integer": lambda v: isinstance(v, int) and not isinstance(v, bool),
+    "string": lambda v: isinstance(v, str),
+    "boolean": lambda v: isinstance(v, bool),
+    "list": lambda v: isinstance(v, list),
+}
+
+
 @dataclass(frozen=True)
 class Key:
+    """One key of a section: its type (``"|null"`` when null is allowed), its default
+    (``REQUIRED`` when it has none), the values implemented, and for domain keys the grid
+    sources that take it and those that require it."""
+
     name: str
     type: str
     default: Any
@@ -41,21 +55,17 @@ class Key:
     grids: tuple | None = None
     required_for: tuple = ()
 
-    def check(self, path: str, value: Any) -> None:
+    def problem(self, path: str, value: Any) -> str | None:
+        """What is wrong with ``value`` at ``path``, worded for the user; None if nothing."""
+        kind, _, null = self.type.partition("|")
         if value is None:
-            if not self.type.endswith("|null"):
-                raise TypeError(f"'{path}' may not be null")
-            return
-        base = self.type.split("|")[0]
-        ok = {"number": lambda v: isinstance(v, (int, float)) and not isinstance(v, bool),
-              "integer": lambda v: isinstance(v, int) and not isinstance(v, bool),
-              "string": lambda v: isinstance(v, str),
-              "boolean": lambda v: isinstance(v, bool),
-              "list": lambda v: isinstance(v, list)}[base](value)
-        if not ok:
-            raise TypeError(f"'{path}' must be {'an' if base[0] in 'aeiou' else 'a'} {base}, got {value!r}")
+            return None if null == "null" else f"'{path}' may not be null"
+        if not _ACCEPTS[kind](value):
+            article = "an" if kind[0] in "aeiou" else "a"
+            return f"'{path}' must be {article} {kind}, got {value!r}"
         if self.choices is not None and value not in self.choices:
-            raise ValueError(f"'{path}' = {value!r} is not implemented; choose from {sorted(self.choices)}")
+            return f"'{path}' = {value!r} is not implemented; choose from {sorted(self.choices)}"
+        return None
 
 
 GENERATED = ("o_grid", "c_grid")
@@ -241,148 +251,200 @@ class Case:
         return build_plan(mesh, self.numerics.n_ghost, with_distance=turbulent)
 
 
-def _section(doc: dict, file: str, name: str, required: bool = False) -> dict:
-    if name not in doc:
+# --- reading a document against its schema ------------------------------------------------
+
+
+def _fields(container: dict, name: str, allowed, where: str, required: bool = False) -> dict:
+    """The object ``container[name]`` without its ``notes``: it must be a JSON object
+    whose keys are all in ``allowed``.  Absent: {} (or ``CaseError`` when required)."""
+    if name not in container:
         if required:
             raise CaseError(f"missing section '{name}'")
         return {}
-    section = doc[name]
-    if not isinstance(section, dict):
-        raise CaseError(f"'{name}' must be an object, got {type(section).__name__}")
-    allowed = keys(file, name)
-    unknown = set(section) - set(allowed) - {"notes"}
-    if unknown:
-        raise CaseError(f"unknown key(s) {sorted(f'{name}.{k}' for k in unknown)}; allowed: {sorted(allowed)}")
-    return {k: v for k, v in section.items() if k != "notes"}
+    obj = container[name]
+    if not isinstance(obj, dict):
+        raise CaseError(f"'{where}' must be an object, got {type(obj).__name__}")
+    stray = sorted(f"{where}.{k}" for k in obj if k not in allowed and k != "notes")
+    if stray:
+        raise CaseError(f"unknown key(s) {stray}; allowed: {sorted(allowed)}")
+    return {k: v for k, v in obj.items() if k != "notes"}
 
 
-def _values(section: dict, file: str, name: str) -> dict:
-    out = {}
-    for key in FILES[file][name]:
-        path = f"{name}.{key.name}"
-        if key.name in section:
-            try:
-                key.check(path, section[key.name])
-            except (TypeError, ValueError) as error:
-                raise CaseError(str(error)) from None
-            out[key.name] = section[key.name]
+def _complete(given: dict, schema: tuple, where: str) -> dict:
+    """Every key of ``schema``: the given value once checked, else the key's default."""
+    values = {}
+    for key in schema:
+        path = f"{where}.{key.name}"
+        if key.name in given:
+            message = key.problem(path, given[key.name])
+            if message:
+                raise CaseError(message)
+            values[key.name] = given[key.name]
         elif key.default is REQUIRED:
             raise CaseError(f"missing '{path}'")
         else:
-            out[key.name] = key.default
-    return out
+            values[key.name] = key.default
+    return values
 
 
-def _top_level(doc: dict, file: str) -> None:
-    unknown = set(doc) - set(FILES[file]) - ({"boundary_conditions"} if file == CASE_FILE else set())
-    if unknown:
-        raise CaseError(f"{file}: unknown section(s) {sorted(unknown)}; allowed: {sorted(FILES[file])}")
+class Document:
+    """One of the two JSON documents read against its schema (``FILES[file]``): an unknown
+    section or key, a value of the wrong type, or an option not implemented is a
+    ``CaseError`` naming it; ``given(name)`` is what the document wrote in a section,
+    ``values(name)`` every key of it with the defaults filled in."""
+
+    def __init__(self, doc: dict, file: str):
+        self.doc, self.file, self.schema = doc, file, FILES[file]
+        extra = {"boundary_conditions"} if file == CASE_FILE else set()
+        stray = sorted(set(doc) - set(self.schema) - extra)
+        if stray:
+            raise CaseError(f"{file}: unknown section(s) {stray}; allowed: {sorted(self.schema)}")
+
+    def given(self, name: str, required: bool = False) -> dict:
+        return _fields(self.doc, name, {k.name for k in self.schema[name]}, name, required)
+
+    def values(self, name: str, required: bool = False) -> dict:
+        return _complete(self.given(name, required), self.schema[name], name)
 
 
-def _grid_spec(case_doc: dict) -> GridSpec:
-    raw = _section(case_doc, CASE_FILE, "domain", required=True)
-    if "grid" not in raw:
-        raise CaseError(f"missing 'domain.grid'; choose from {sorted(GRIDS)}")
-    domain = _values(raw, CASE_FILE, "domain")
+def _raise_first(problems) -> None:
+    """Raise the first message a rule generator yields, if any."""
+    for message in problems:
+        raise CaseError(message)
+
+
+# --- cross-key rules, each a generator of messages in the order they are checked -----------
+
+
+def _domain_problems(written: dict, domain: dict):
     kind = domain["grid"]
-    ks = keys(CASE_FILE, "domain")
-    foreign = sorted(k for k in raw if ks[k].grids is not None and kind not in ks[k].grids)
+    table = keys(CASE_FILE, "domain")
+    foreign = sorted(k for k in written if table[k].grids is not None and kind not in table[k].grids)
     if foreign:
-        takes = sorted(k for k, key in ks.items() if key.grids and kind in key.grids)
-        raise CaseError(f"'domain.{foreign[0]}' does not apply to grid {kind!r}; it takes {takes}")
-    for name, key in ks.items():
+        takes = sorted(k for k, key in table.items() if key.grids and kind in key.grids)
+        yield f"'domain.{foreign[0]}' does not apply to grid {kind!r}; it takes {takes}"
+    for name, key in table.items():
         if kind in key.required_for and domain[name] is None:
-            raise CaseError(f"'domain.{name}' is required for grid {kind!r}")
+            yield f"'domain.{name}' is required for grid {kind!r}"
     if kind not in BUILT_GRIDS:
-        raise CaseError(f"'domain.grid' = {kind!r} is not implemented in this build; choose from "
-                        f"{sorted(BUILT_GRIDS)}")
-    return GridSpec(grid=kind, airfoil=domain["airfoil"], cells_airfoil=domain["cells_airfoil"],
-                    cells_wake=domain["cells_wake"], cells_normal=domain["cells_normal"],
-                    wall_spacing=domain["wall_spacing"], far_field=domain["far_field"],
-                    trailing_edge=domain["trailing_edge"], normal_stretching=domain["normal_stretching"],
-                    reference_length=domain["reference_length"], reference_area=domain["reference_area"],
-                    moment_centre=tuple(domain["moment_centre"]), file=domain["file"], format=domain["format"],
-                    coordinate_scale=domain["coordinate_scale"], patches=tuple(domain["patches"] or ()))
+        yield f"'domain.grid' = {kind!r} is not implemented in this build; choose from {sorted(BUILT_GRIDS)}"
 
 
-def _flow(case_doc: dict) -> FlowConditions:
-    given = {name: _section(case_doc, CASE_FILE, name, required=name == "freestream")
-             for name in ("freestream", "material_properties", "turbulence")}
-    freestream, material, turbulence = (_values(given[n], CASE_FILE, n) for n in given)
-    inviscid = freestream["reynolds"] is None
-    sutherland = None
-    if inviscid:
+def _flow_problems(written_material: dict, written_turbulence: dict, freestream: dict, material: dict,
+                   turbulence: dict):
+    if freestream["reynolds"] is None:
         for key in ("dynamic_viscosity", "prandtl_number", "sutherland_temperature"):
-            if key in given["material_properties"]:
-                raise CaseError(f"'material_properties.{key}' given for an inviscid case "
-                                f"(freestream.reynolds is null)")
+            if key in written_material:
+                yield f"'material_properties.{key}' given for an inviscid case (freestream.reynolds is null)"
     else:
         if material["dynamic_viscosity"] == "sutherland":
             if freestream["temperature"] is None or material["sutherland_temperature"] is None:
-                raise CaseError("Sutherland's law needs 'freestream.temperature' and "
-                                "'material_properties.sutherland_temperature', in one absolute unit")
-            sutherland = material["sutherland_temperature"] / freestream["temperature"]
+                yield ("Sutherland's law needs 'freestream.temperature' and "
+                       "'material_properties.sutherland_temperature', in one absolute unit")
         elif material["sutherland_temperature"] is not None:
-            raise CaseError("'material_properties.sutherland_temperature' given with a constant viscosity")
+            yield "'material_properties.sutherland_temperature' given with a constant viscosity"
         if material["prandtl_number"] != PRANDTL_LAMINAR:
-            raise CaseError(f"'material_properties.prandtl_number' = {material['prandtl_number']} is not "
-                            f"implemented; only {PRANDTL_LAMINAR}")
-    model = turbulence["model"]
-    if model != "none" and inviscid:
-        raise CaseError("'turbulence.model' needs a viscous case (freestream.reynolds)")
-    if model == "none" and "freestream_nu_tilde_ratio" in given["turbulence"]:
-        raise CaseError("'turbulence.freestream_nu_tilde_ratio' given without a model")
+            yield (f"'material_properties.prandtl_number' = {material['prandtl_number']} is not implemented; "
+                   f"only {PRANDTL_LAMINAR}")
+    if turbulence["model"] != "none" and freestream["reynolds"] is None:
+        yield "'turbulence.model' needs a viscous case (freestream.reynolds)"
+    if turbulence["model"] == "none" and "freestream_nu_tilde_ratio" in written_turbulence:
+        yield "'turbulence.freestream_nu_tilde_ratio' given without a model"
     if freestream["sweep_deg"] is not None:
-        raise CaseError("'freestream.sweep_deg' (an infinite swept wing) is not implemented in this build")
+        yield "'freestream.sweep_deg' (an infinite swept wing) is not implemented in this build"
+
+
+def _patch_problems(where: str, entry, inviscid: bool):
+    if not isinstance(entry, dict):
+        yield f"'{where}' must be an object with a 'type', got {entry!r}"
+        return
+    table = {k.name: k for k in BOUNDARY_KEYS}
+    stray = sorted(f"{where}.{k}" for k in entry if k not in table and k != "notes")
+    if stray:
+        yield f"unknown key(s) {stray}; allowed: {sorted(table)}"
+    if "type" not in entry:
+        yield f"missing '{where}.type'"
+    for name in entry:
+        if name != "notes":
+            message = table[name].problem(f"{where}.{name}", entry[name])
+            if message:
+                yield message
+    if "model" in entry and entry["type"] != "far_field":
+        yield f"'{where}.model' applies to a far_field patch only"
+    if entry["type"] == "no_slip_wall" and inviscid:
+        yield f"'{where}.type' = 'no_slip_wall' in an inviscid case (freestream.reynolds is null)"
+
+
+# --- the parts of a case --------------------------------------------------------------------
+
+
+def _grid_spec(case: Document) -> GridSpec:
+    written = case.given("domain", required=True)
+    if "grid" not in written:
+        raise CaseError(f"missing 'domain.grid'; choose from {sorted(GRIDS)}")
+    d = case.values("domain")
+    _raise_first(_domain_problems(written, d))
+    return GridSpec(grid=d["grid"], airfoil=d["airfoil"], cells_airfoil=d["cells_airfoil"],
+                    cells_wake=d["cells_wake"], cells_normal=d["cells_normal"], wall_spacing=d["wall_spacing"],
+                    far_field=d["far_field"], trailing_edge=d["trailing_edge"],
+                    normal_stretching=d["normal_stretching"], reference_length=d["reference_length"],
+                    reference_area=d["reference_area"], moment_centre=tuple(d["moment_centre"]), file=d["file"],
+                    format=d["format"], coordinate_scale=d["coordinate_scale"], patches=tuple(d["patches"] or ()))
+
+
+def _flow_of(case: Document) -> FlowConditions:
+    written = {n: case.given(n, required=n == "freestream") for n in ("freestream", "material_properties",
+                                                                       "turbulence")}
+    fs, mat, turb = (_complete(written[n], case.schema[n], n) for n in written)
+    _raise_first(_flow_problems(written["material_properties"], written["turbulence"], fs, mat, turb))
+    sutherland = None
+    if fs["reynolds"] is not None and mat["dynamic_viscosity"] == "sutherland":
+        sutherland = mat["sutherland_temperature"] / fs["temperature"]
     try:
-        return FlowConditions(mach=freestream["mach"], alpha_deg=freestream["alpha_deg"],
-                              reynolds=freestream["reynolds"], gamma=material["specific_heat_ratio"],
-                              sutherland_ratio=sutherland, turbulence=None if model == "none" else model,
-                              nu_tilde_ratio=turbulence["freestream_nu_tilde_ratio"])
+        return FlowConditions(mach=fs["mach"], alpha_deg=fs["alpha_deg"], reynolds=fs["reynolds"],
+                              gamma=mat["specific_heat_ratio"], sutherland_ratio=sutherland,
+                              turbulence=None if turb["model"] == "none" else turb["model"],
+                              nu_tilde_ratio=turb["freestream_nu_tilde_ratio"])
+    except ValueError as error:
+        raise CaseError(str(error)) from None
+
+
+def flow_conditions(case_doc: dict) -> FlowConditions:
+    """The flow a ``case.json`` document describes (its freestream, material and
+    turbulence sections)."""
+    return _flow_of(Document(case_doc, CASE_FILE))
+
+
+def implicit_config(numerical_doc: dict) -> ImplicitConfig:
+    """The implicit solver's settings a ``numerical.json`` document gives."""
+    try:
+        return ImplicitConfig(**Document(numerical_doc, NUMERICAL_FILE).values("implicit"))
     except ValueError as error:
         raise CaseError(str(error)) from None
 
 
 def default_conditions(flow: FlowConditions) -> dict[str, str]:
+    """The condition of a patch the case does not name, by the patch's name."""
     return {"wall": "slip_wall" if flow.inviscid else "no_slip_wall", "farfield": "far_field",
             "symmetry": "symmetry", "inflow": "inflow_total", "outflow": "outflow_static"}
 
 
 def _boundaries(case_doc: dict, flow: FlowConditions) -> tuple[dict, str]:
+    """The conditions the case names (patch -> kind) and the one far-field model."""
     section = case_doc.get("boundary_conditions", {})
     if not isinstance(section, dict):
         raise CaseError("'boundary_conditions' must be an object")
-    kinds, models = {}, set()
-    allowed = {k.name: k for k in BOUNDARY_KEYS}
-    for patch, entry in section.items():
-        if patch == "notes":
-            continue
-        where = f"boundary_conditions.{patch}"
-        if not isinstance(entry, dict):
-            raise CaseError(f"'{where}' must be an object with a 'type', got {entry!r}")
-        unknown = set(entry) - set(allowed) - {"notes"}
-        if unknown:
-            raise CaseError(f"unknown key(s) {sorted(f'{where}.{k}' for k in unknown)}; allowed: {sorted(allowed)}")
-        if "type" not in entry:
-            raise CaseError(f"missing '{where}.type'")
-        for name in set(entry) - {"notes"}:
-            try:
-                allowed[name].check(f"{where}.{name}", entry[name])
-            except (TypeError, ValueError) as error:
-                raise CaseError(str(error)) from None
-        if "model" in entry and entry["type"] != "far_field":
-            raise CaseError(f"'{where}.model' applies to a far_field patch only")
-        if entry["type"] == "far_field":
-            models.add(entry.get("model", "freestream"))
-        if entry["type"] == "no_slip_wall" and flow.inviscid:
-            raise CaseError(f"'{where}.type' = 'no_slip_wall' in an inviscid case (freestream.reynolds is null)")
-        kinds[patch] = entry["type"]
+    entries = {patch: entry for patch, entry in section.items() if patch != "notes"}
+    for patch, entry in entries.items():
+        _raise_first(_patch_problems(f"boundary_conditions.{patch}", entry, flow.inviscid))
+    models = sorted({e.get("model", "freestream") for e in entries.values() if e["type"] == "far_field"})
     if len(models) > 1:
-        raise CaseError(f"far-field patches name different models {sorted(models)}; one model per case")
-    return kinds, FAR_FIELD_MODELS[models.pop() if models else "freestream"]
+        raise CaseError(f"far-field patches name different models {models}; one model per case")
+    return {p: e["type"] for p, e in entries.items()}, FAR_FIELD_MODELS[models[0] if models else "freestream"]
 
 
 def resolve_conditions(named: dict, grid_patches: list, flow: FlowConditions) -> dict:
+    """Every grid patch's condition: the one the case names, else its name's default."""
     unknown = [p for p in named if p not in grid_patches]
     if unknown:
         raise CaseError(f"'boundary_conditions' names patch(es) {unknown} the grid does not have; "
@@ -390,77 +452,103 @@ def resolve_conditions(named: dict, grid_patches: list, flow: FlowConditions) ->
     defaults = default_conditions(flow)
     missing = [p for p in grid_patches if p not in named and p not in defaults]
     if missing:
-        raise CaseError(f"no boundary condition for patch(es) {missing}")
+        raise CaseError(f"no boundary condition for patch(es) {missing}: give each a 'type' in "
+                        f"'boundary_conditions' (the grid's patches are {grid_patches})")
     return {p: named.get(p, defaults.get(p)) for p in grid_patches}
 
 
+# what this build refuses among the options the schema accepts: (file section, key, accepted
+# value, message)
+_NOT_BUILT = (
+    ("time_integration", "solver", "implicit",
+     "'time_integration.solver' = 'explicit' (multistage Runge-Kutta) is not implemented in this build; set it "
+     "to 'implicit'"),
+    ("implicit", "jacobian", "first_order",
+     "'implicit.jacobian' = 'exact' is not implemented in this build; use 'first_order'"),
+    ("convergence", "grid_sequencing", 0,
+     "'convergence.grid_sequencing' other than 0 is not implemented in this build"),
+)
+
+
 def parse_case(case_doc: dict, numerical_doc: dict, directory: Path = Path(".")) -> Case:
-    _top_level(case_doc, CASE_FILE)
-    _top_level(numerical_doc, NUMERICAL_FILE)
-    general = _values(_section(case_doc, CASE_FILE, "general", required=True), CASE_FILE, "general")
-    spec = _grid_spec(case_doc)
-    flow = _flow(case_doc)
+    """A ``Case`` from the two documents (``src/jaxrans/case/loader.py:273-323``);
+    ``CaseError`` names the offending key."""
+    case, numerical = Document(case_doc, CASE_FILE), Document(numerical_doc, NUMERICAL_FILE)
+    general = case.values("general", required=True)
+    spec = _grid_spec(case)
+    flow = _flow_of(case)
     if "section" in case_doc["domain"]:
         raise CaseError("'domain.section' applies to a swept case only ('freestream.sweep_deg')")
     conditions, far_field = _boundaries(case_doc, flow)
-    fluxes, stepping, implicit, convergence = (
-        _values(_section(numerical_doc, NUMERICAL_FILE, n), NUMERICAL_FILE, n)
-        for n in ("convective_fluxes", "time_integration", "implicit", "convergence"))
-    if stepping["solver"] != "implicit":
-        raise CaseError("'time_integration.solver' = 'explicit' (multistage Runge-Kutta) is not implemented in "
-                        "this build; set it to 'implicit'")
-    if implicit["jacobian"] != "first_order":
-        raise CaseError("'implicit.jacobian' = 'exact' is not implemented in this build; use 'first_order'")
+    sections = {n: numerical.values(n) for n in ("convective_fluxes", "time_integration", "implicit", "convergence")}
+    for section, key, built, message in _NOT_BUILT[:2]:
+        if sections[section][key] != built:
+            raise CaseError(message)
+    fluxes, stepping, conv = sections["convective_fluxes"], sections["time_integration"], sections["convergence"]
     try:
-        imp = ImplicitConfig(**implicit)
+        imp = ImplicitConfig(**sections["implicit"])
         numerics = NumericsConfig(flux=fluxes["riemann_solver"], limiter=fluxes["limiter"],
-                                  kappa=fluxes["muscl_kappa"], cfl=stepping["cfl"],
-                                  max_iters=convergence["max_iters"], tol=convergence["tol"],
-                                  forces_tol=convergence["forces_tol"], solver=stepping["solver"],
+                                  kappa=fluxes["muscl_kappa"], cfl=stepping["cfl"], max_iters=conv["max_iters"],
+                                  tol=conv["tol"], forces_tol=conv["forces_tol"], solver=stepping["solver"],
                                   far_field=far_field)
     except (ValueError, KeyError) as error:
         raise CaseError(str(error)) from None
-    block_iters = convergence["block_iters"] or 20
+    block_iters = conv["block_iters"] or 20
     if block_iters < 1:
         raise CaseError(f"'convergence.block_iters' must be >= 1, got {block_iters}")
-    if convergence["grid_sequencing"] != 0:
-        raise CaseError("'convergence.grid_sequencing' other than 0 is not implemented in this build")
+    section, key, built, message = _NOT_BUILT[2]
+    if sections[section][key] != built:
+        raise CaseError(message)
+    out = Path(general["save_path"])
     directory = Path(directory)
-    output = Path(general["save_path"])
     return Case(name=general["case_name"], description=general["description"] or general["case_name"],
-                output=output if output.is_absolute() else directory / output, grid_spec=spec,
-                conditions=conditions, flow=flow, numerics=numerics, implicit=imp, block_iters=block_iters,
-                directory=directory, raw={"case": case_doc, "numerical": numerical_doc})
+                output=out if out.is_absolute() else directory / out, grid_spec=spec, conditions=conditions,
+                flow=flow, numerics=numerics, implicit=imp, block_iters=block_iters, directory=directory,
+                raw={"case": case_doc, "numerical": numerical_doc})
+
+
+# --- case directories and overrides ----------------------------------------------------------
+
+_OVERRIDE_FILES = ("case", "numerical")
 
 
 def apply_override(docs: dict, assignment: str) -> None:
-    """``file.section.key=value`` (``src/jaxrans/case/loader.py:329-346``)."""
-    if "=" not in assignment:
+    """Set one ``file.section.key=value`` in the raw documents (``file`` is case or
+    numerical; the value is read as JSON, else taken as a bare string), as the
+    reference's ``--set`` does (``src/jaxrans/case/loader.py:329-346``)."""
+    path, eq, text = assignment.partition("=")
+    if not eq:
         raise CaseError(f"override {assignment!r} is not of the form file.section.key=value")
-    path, text = assignment.split("=", 1)
-    parts = path.strip().split(".")
-    if len(parts) != 3 or parts[0] not in docs:
-        raise CaseError(f"override path {path!r} must be case|numerical.section.key")
+    where = path.strip().split(".")
+    if len(where) != 3 or where[0] not in docs:
+        raise CaseError(f"override path {path!r} must be {'|'.join(_OVERRIDE_FILES)}.section.key, "
+                        f"e.g. numerical.convective_fluxes.limiter")
+    file, section, key = where
     try:
         value = json.loads(text)
     except json.JSONDecodeError:
         value = text
-    docs[parts[0]].setdefault(parts[1], {})[parts[2]] = value
+    docs[file].setdefault(section, {})[key] = value
+
+
+def _read_json(path: Path) -> dict:
+    if not path.is_file():
+        return {}
+    try:
+        return json.loads(path.read_text())
+    except json.JSONDecodeError as error:
+        raise CaseError(f"{path}: {error}") from None
 
 
 def load_case(directory: str | Path, overrides: tuple[str, ...] = ()) -> Case:
-    """Read a case directory, apply overrides, parse (``src/jaxrans/case/loader.py:349-373``)."""
+    """A case directory (``case.json`` and, optional, ``numerical.json``) with overrides
+    applied, parsed (``src/jaxrans/case/loader.py:349-373``): ``FileNotFoundError`` when
+    there is no ``case.json``, ``CaseError`` prefixed with the directory otherwise."""
     directory = Path(directory)
     if not (directory / CASE_FILE).is_file():
         raise FileNotFoundError(f"{directory} holds no {CASE_FILE}")
-    docs = {}
-    for label, filename in (("case", CASE_FILE), ("numerical", NUMERICAL_FILE)):
-        path = directory / filename
-        try:
-            docs[label] = json.loads(path.read_text()) if path.is_file() else {}
-        except json.JSONDecodeError as error:
-            raise CaseError(f"{path}: {error}") from None
-    docs = copy.deepcopy(docs)
+    docs = copy.deepcopy({"case": _read_json(directory / CASE_FILE),
+                          "numerical": _read_json(directory / NUMERICAL_FILE)})
     for assignment in overrides:
         apply_override(docs, assignment)
     try:

@@ -10,8 +10,7 @@ generated grids; nothing here is used at run time by the library.
     PYTHONPATH=tests/golden/jaxshim:<reference>/src python tests/golden/make_golden.py [--converge]
 
 writes ``tests/golden/<case>.npz`` (+ ``<case>_converged.npz`` with ``--converge``).
-The reference source tree is read from ``$JAXRANS_REFERENCE`` (default
-``/root/reference``).
+The reference source tree is read from ``$JAXRANS_REFERENCE`` (required).
 """
 
 from __future__ import annotations
@@ -24,7 +23,9 @@ import time
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REFERENCE = Path(os.environ.get("JAXRANS_REFERENCE", "/root/reference"))
+if "JAXRANS_REFERENCE" not in os.environ:
+    raise SystemExit("set JAXRANS_REFERENCE to the reference source checkout (the directory holding src/jaxrans)")
+REFERENCE = Path(os.environ["JAXRANS_REFERENCE"])
 sys.path.insert(0, str(HERE / "jaxshim"))
 sys.path.insert(1, str(REFERENCE / "src"))
 

@@ -11,7 +11,7 @@ all run on the reference's sources, unmodified, on top of the NumPy stand-in in
     python tests/golden/make_golden3d.py
 
 writes ``tests/golden/ch_sa3d.npz``.  The reference source tree is read from
-``$JAXRANS_REFERENCE`` (default ``/root/reference``).
+``$JAXRANS_REFERENCE`` (required).
 """
 
 from __future__ import annotations
@@ -24,7 +24,9 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
-REFERENCE = Path(os.environ.get("JAXRANS_REFERENCE", "/root/reference"))
+if "JAXRANS_REFERENCE" not in os.environ:
+    raise SystemExit("set JAXRANS_REFERENCE to the reference source checkout (the directory holding src/jaxrans)")
+REFERENCE = Path(os.environ["JAXRANS_REFERENCE"])
 sys.path.insert(0, str(HERE / "jaxshim"))
 sys.path.insert(1, str(REFERENCE / "src"))
 sys.path.insert(2, str(ROOT / "jax-rans_b200"))

@@ -26,7 +26,7 @@ distributions.
     python tests/golden/make_golden_blocks3d.py
 
 writes ``tests/golden/blocks3d.npz``.  The reference source tree is read from
-``$JAXRANS_REFERENCE`` (default ``/root/reference``).
+``$JAXRANS_REFERENCE`` (required).
 """
 
 from __future__ import annotations
@@ -39,7 +39,9 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
-REFERENCE = Path(os.environ.get("JAXRANS_REFERENCE", "/root/reference"))
+if "JAXRANS_REFERENCE" not in os.environ:
+    raise SystemExit("set JAXRANS_REFERENCE to the reference source checkout (the directory holding src/jaxrans)")
+REFERENCE = Path(os.environ["JAXRANS_REFERENCE"])
 sys.path.insert(0, str(HERE / "jaxshim"))
 sys.path.insert(1, str(REFERENCE / "src"))
 sys.path.insert(2, str(ROOT / "jax-rans_b200"))

@@ -23,7 +23,9 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
-REFERENCE = Path(os.environ.get("JAXRANS_REFERENCE", "/root/reference"))
+if "JAXRANS_REFERENCE" not in os.environ:
+    raise SystemExit("set JAXRANS_REFERENCE to the reference source checkout (the directory holding src/jaxrans)")
+REFERENCE = Path(os.environ["JAXRANS_REFERENCE"])
 sys.path.insert(0, str(HERE / "jaxshim"))
 sys.path.insert(1, str(REFERENCE / "src"))
 sys.path.insert(2, str(ROOT / "jax-rans_b200"))

@@ -10,7 +10,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from jaxrans_b200.case import _flow
+from jaxrans_b200.case import flow_conditions
 from jaxrans_b200.geometry import section_source
 from jaxrans_b200.grid3d import wing_block
 from jaxrans_b200.plan3d import build_plan3d
@@ -28,14 +28,13 @@ def device3d():
     w = json.loads(str(z["wing_json"]))
     doc = json.loads(str(z["case_json"]))
     plan = build_plan3d([wing_block(section_source(w.pop("section")), **w).with_kinds(KINDS)])
-    flow = _flow(doc["case"])
+    flow = flow_conditions(doc["case"])
     a = flow.alpha_rad
     q_inf = np.array([1.0, flow.mach * np.cos(a), 0.0, flow.mach * np.sin(a), 1.0 / flow.gamma,
                       flow.nu_tilde_ratio])
     cv = doc["numerical"]["convective_fluxes"]
-    from jaxrans_b200.case import NUMERICAL_FILE, _section, _values
-    from jaxrans_b200.config import ImplicitConfig
-    imp = ImplicitConfig(**_values(_section(doc["numerical"], NUMERICAL_FILE, "implicit"), NUMERICAL_FILE, "implicit"))
+    from jaxrans_b200.case import implicit_config
+    imp = implicit_config(doc["numerical"])
     dev = DevicePlan3(plan, q_inf, flow.gamma, cv["riemann_solver"], cv["limiter"], 0.0, flow.mu_inf,
                       flow.sutherland_ratio, imp)
     yield z, dev

@@ -13,7 +13,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from jaxrans_b200.case import _flow
+from jaxrans_b200.case import flow_conditions
 from jaxrans_b200.geometry import section_source
 from jaxrans_b200.grid3d import wing_block
 from jaxrans_b200.native3d import describe
@@ -30,7 +30,7 @@ def case3d():
     w = json.loads(str(z["wing_json"]))
     doc = json.loads(str(z["case_json"]))
     plan = build_plan3d([wing_block(section_source(w.pop("section")), **w).with_kinds(KINDS)])
-    flow = _flow(doc["case"])
+    flow = flow_conditions(doc["case"])
     a = flow.alpha_rad
     q_inf = np.array([1.0, flow.mach * np.cos(a), 0.0, flow.mach * np.sin(a), 1.0 / flow.gamma,
                       flow.nu_tilde_ratio])
@@ -101,7 +101,7 @@ def test_kernel_bodies_give_the_reference_line_solve(harness, case3d, state):
     out = np.zeros_like(r)
     assert harness.jr3_host_precondition(C.addressof(desc), U.ctypes.data, 25.0, r.ctypes.data, out.ctypes.data) == 0
     assert rows_rel(out, z[f"{state}_prec_z"]) < 1e-10
-    flow = _flow(_json.loads(str(z["case_json"]))["case"])
+    flow = flow_conditions(_json.loads(str(z["case_json"]))["case"])
     a = flow.alpha_rad
     q_inf = np.array([1.0, flow.mach * np.cos(a), 0.0, flow.mach * np.sin(a), 1.0 / flow.gamma, flow.nu_tilde_ratio])
     model = n3.Model3(plan, q_inf, flow.gamma, "hllc", "van_albada_smooth", 0.0, flow.mu_inf,
@@ -116,11 +116,10 @@ def test_newton_steps_match_the_reference(harness, case3d):
     relaxation, acceptance and CFL ramp) driven by csrc/newton3d.cuh over host loops,
     from the 'rand0' state at CFL 25 (src/jaxrans/solvers/implicit.py:84-168)."""
     import json as _json
-    from jaxrans_b200.case import NUMERICAL_FILE, _section, _values
-    from jaxrans_b200.config import ImplicitConfig
+    from jaxrans_b200.case import implicit_config
     z, plan, desc, _ = case3d
     doc = _json.loads(str(z["case_json"]))
-    cfg = ImplicitConfig(**_values(_section(doc["numerical"], NUMERICAL_FILE, "implicit"), NUMERICAL_FILE, "implicit"))
+    cfg = implicit_config(doc["numerical"])
     config = np.array([cfg.krylov_tol, cfg.krylov_success,
                        cfg.max_relative_update if cfg.max_relative_update is not None else -1.0,
                        cfg.cfl_min, cfg.cfl_max, cfg.cfl_growth, cfg.cfl_cutback])
@@ -192,7 +191,7 @@ def test_kernel_bodies_give_the_coupled_line_solve(harness, case3d, state):
                                              out.ctypes.data) == 0
     finally:
         desc.preconditioner = 1
-    flow = _flow(_json.loads(str(z["case_json"]))["case"])
+    flow = flow_conditions(_json.loads(str(z["case_json"]))["case"])
     a = flow.alpha_rad
     q_inf = np.array([1.0, flow.mach * np.cos(a), 0.0, flow.mach * np.sin(a), 1.0 / flow.gamma, flow.nu_tilde_ratio])
     model = n3.Model3(plan, q_inf, flow.gamma, "hllc", "van_albada_smooth", 0.0, flow.mu_inf,
@@ -210,11 +209,10 @@ def test_newton_steps_with_the_coupled_and_mixed_line_solve(harness, case3d):
     preconditioner): the residual falls as with line_j in FP64, step for step within a
     few per cent."""
     import json as _json
-    from jaxrans_b200.case import NUMERICAL_FILE, _section, _values
-    from jaxrans_b200.config import ImplicitConfig
+    from jaxrans_b200.case import implicit_config
     z, plan, desc, _ = case3d
     doc = _json.loads(str(z["case_json"]))
-    cfg = ImplicitConfig(**_values(_section(doc["numerical"], NUMERICAL_FILE, "implicit"), NUMERICAL_FILE, "implicit"))
+    cfg = implicit_config(doc["numerical"])
     config = np.array([cfg.krylov_tol, cfg.krylov_success,
                        cfg.max_relative_update if cfg.max_relative_update is not None else -1.0,
                        cfg.cfl_min, cfg.cfl_max, cfg.cfl_growth, cfg.cfl_cutback])

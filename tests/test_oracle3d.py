@@ -10,7 +10,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from jaxrans_b200.case import _flow
+from jaxrans_b200.case import flow_conditions
 from jaxrans_b200.geometry import section_source
 from jaxrans_b200.grid3d import wing_block
 from jaxrans_b200.plan3d import build_plan3d
@@ -26,7 +26,7 @@ def setup():
     w = json.loads(str(z["wing_json"]))
     doc = json.loads(str(z["case_json"]))
     plan = build_plan3d([wing_block(section_source(w.pop("section")), **w).with_kinds(KINDS)])
-    flow = _flow(doc["case"])
+    flow = flow_conditions(doc["case"])
     a = flow.alpha_rad
     # x-z incidence, y along the span (core/state.py:107-140)
     q_inf = np.array([1.0, flow.mach * np.cos(a), 0.0, flow.mach * np.sin(a), 1.0 / flow.gamma,
@@ -105,10 +105,8 @@ def test_forces_match_the_reference(setup, state):
 
 
 def _implicit_config(doc):
-    from jaxrans_b200.case import NUMERICAL_FILE, _section, _values
-    from jaxrans_b200.config import ImplicitConfig
-    return ImplicitConfig(**_values(_section(doc["numerical"], NUMERICAL_FILE, "implicit"), NUMERICAL_FILE,
-                                    "implicit"))
+    from jaxrans_b200.case import implicit_config
+    return implicit_config(doc["numerical"])
 
 
 def test_gmres_and_newton_steps_match_the_reference(setup):

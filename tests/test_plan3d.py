@@ -100,10 +100,10 @@ def test_ghost_records_reproduce_the_gather_fill(golden, plan):
     """The device runs each ghost stage as records (one per ghost the stage writes); run
     on the host with the oracle's conditions, they give the reference's gather fill."""
     import json as _json
-    from jaxrans_b200.case import _flow
+    from jaxrans_b200.case import flow_conditions
     from jaxrans_b200.native3d import KIND3, records_of
     from oracle import numerics3d as n3
-    flow = _flow(_json.loads(str(golden["case_json"]))["case"])
+    flow = flow_conditions(_json.loads(str(golden["case_json"]))["case"])
     a = flow.alpha_rad
     q_inf = np.array([1.0, flow.mach * np.cos(a), 0.0, flow.mach * np.sin(a), 1.0 / flow.gamma, flow.nu_tilde_ratio])
     model = n3.Model3(plan, q_inf, flow.gamma, "hllc", "van_albada_smooth", 0.0, flow.mu_inf,
