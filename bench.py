@@ -41,14 +41,38 @@ for _p in (ROOT, ROOT / "jax-rans_b200"):
 import numpy as np  # noqa: E402
 
 METRIC = "converged RANS solves/hr"
-# Newton steps of one converged solve of each workload, measured on the device path (the
-# bench line's config.newton_steps_per_solve); the reference arm's sample is scaled by it.
-STEPS_PER_SOLVE = {"c_sa_385": 620, "o_euler_257": 3840}
-# algorithmic bytes per cell of one J.v tile launch: U, v and w (nvar each), V/dt, the
-# volume, the two face vectors a cell owns (4 doubles), the centre (2), the wall distance
-# (SA only), all FP64
-def jvp_bytes_per_cell(nvar: int) -> int:
-    return 8 * (3 * nvar + 1 + 1 + 4 + 2 + (1 if nvar == 5 else 0))
+# Newton steps of one converged solve of each workload from the freestream (FP64): the
+# device path's own count (the bench line's config.newton_steps_per_solve, which it
+# measures every run); the CPU samples, a few Newton steps each, are scaled by it.
+STEPS_PER_SOLVE = {"c_sa_385": 640, "o_euler_257": 3840}
+# coefficients of the linearisation the J.v tile reads per face and per cell (the
+# kernel's JacShape and JCELL): inviscid 4 x 4 per side, the SA convection's 3, the
+# viscous tail's rows x intermediates
+LIN_FACE = {"euler": 32, "laminar": 32 + 3 * 9, "sa": 35 + 4 * 14}
+LIN_CELL = {"euler": 0, "laminar": 0, "sa": 7}
+
+
+def model_of(flow) -> str:
+    return "euler" if flow.inviscid else ("sa" if flow.turbulence is not None else "laminar")
+
+
+def jvp_bytes_per_cell(model: str, nvar: int) -> int:
+    """Algorithmic bytes per cell of one J.v tile launch (FP64): the coefficients of the
+    two faces a cell owns and its own, then U (the primitive tangent), v and the output,
+    V/dt; viscous: the centre (2); SA: the volume and the two face vectors the Green-Gauss
+    source reads (4)."""
+    words = 2 * LIN_FACE[model] + LIN_CELL[model] + 3 * nvar + 1
+    if model != "euler":
+        words += 2
+    if model == "sa":
+        words += 1 + 4
+    return 8 * words
+
+
+def residual_bytes_per_cell(model: str, nvar: int) -> int:
+    """Algorithmic bytes per cell of one residual tile launch (FP64): U and R, the volume,
+    the two face vectors a cell owns (4); viscous: the centre (2); SA: the wall distance."""
+    return 8 * (2 * nvar + 1 + 4 + (2 if model != "euler" else 0) + (1 if model == "sa" else 0))
 
 
 def rank_info():
@@ -123,11 +147,16 @@ def profiled_traffic(workload: str):
     return None
 
 
-def reference_sample(case, plan, steps: int, warmup: int, precision: str):
-    """Newton steps of the CPU restatement (the oracle) from the freestream."""
+def reference_sample(name: str, steps: int, warmup: int, precision: str):
+    """Seconds of each of `steps` Newton steps of the CPU restatement (the oracle) of
+    workload `name` from the freestream, after `warmup` untimed ones (one process, one
+    thread: the pool around it gives each host core its own solve)."""
     from jaxrans_b200.config import freestream_primitive
+    from jaxrans_b200.workloads import workload
     from oracle import implicit as im
     from oracle import numerics as nm
+    case = workload(name, **{"implicit.precision": precision})
+    plan = case.grid()
     flow, num = case.flow, case.numerics
     model = nm.Model(plan, np.array(freestream_primitive(flow)), flow.gamma, num.flux, num.limiter, num.kappa,
                      None if flow.inviscid else flow.mu_inf, flow.sutherland_ratio, flow.turbulence is not None,
@@ -143,6 +172,37 @@ def reference_sample(case, plan, steps: int, warmup: int, precision: str):
     return times
 
 
+def _sample_worker(job):
+    return reference_sample(*job)
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_rate(name: str, steps: int, warmup: int, precision: str, steps_per_solve: int) -> dict:
+    """The oracle's whole-host throughput on workload `name`: one independent solve per
+    host core (a process pool started with spawn, one BLAS thread each), each timed over
+    `steps` Newton steps after `warmup`; solves/hr = cores / (mean step x steps per solve)."""
+    import multiprocessing
+    cores = host_cores()
+    for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[var] = "1"
+    with multiprocessing.get_context("spawn").Pool(cores) as pool:
+        times = pool.map(_sample_worker, [(name, steps, warmup, precision)] * cores)
+    per_step = statistics.mean(t for ts in times for t in ts)
+    value = cores * 3600.0 / (per_step * steps_per_solve)
+    sample = (f"{cores} processes (one per host core, one thread each), each one solve of the oracle (NumPy "
+              f"FP64, complex-step J.v) from the freestream on {name}: {warmup} untimed and {steps} timed Newton "
+              f"steps, {per_step:.2f} s per step on average, scaled by {steps_per_solve} Newton steps per "
+              f"converged solve")
+    return {"value": value, "unit": "solves/hr", "cores": cores, "kind": "port", "sample": sample,
+            "seconds_per_step": per_step}
+
+
 def run_reference(args) -> int:
     rank, _, world = rank_info()
     if rank != 0:
@@ -150,21 +210,16 @@ def run_reference(args) -> int:
     from jaxrans_b200.workloads import BATCHES, workload
     # a batch is timed on its first case (the oracle runs one case at a time)
     name = BATCHES[args.workload][0][0] if args.workload in BATCHES else args.workload
-    case = workload(name, **{"implicit.precision": args.precision})
-    plan = case.grid()
-    times = reference_sample(case, plan, args.steps, args.warmup, args.precision)
-    per_step = statistics.mean(times)
     n = STEPS_PER_SOLVE[name]
-    value = 3600.0 / (per_step * n)
-    sample = (f"{args.steps} Newton steps of the oracle (NumPy FP64, complex-step J.v) from the freestream on "
-              f"the {args.workload} case after {args.warmup} warm-up steps, {per_step:.2f} s each, scaled by "
-              f"{n} Newton steps per converged solve")
+    cpu = cpu_rate(name, args.steps, args.warmup, args.precision, n)
+    value, per_step = cpu["value"], cpu.pop("seconds_per_step")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/hr", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * per_step * n,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * per_step * n / cpu["cores"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (generated NACA section and grid)",
-            "config": {"workload": args.workload, "cells": plan.cells, "newton_steps_per_solve": n},
-            "cpu_baseline": {"value": value, "unit": "solves/hr", "cores": 1, "kind": "port", "sample": sample},
+            "config": {"workload": args.workload, "cells": workload(name).grid().cells,
+                       "newton_steps_per_solve": n, "cores": cpu["cores"]},
+            "cpu_baseline": cpu,
             "e2e": {"value": value, "unit": "solves/hr", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -313,6 +368,17 @@ def run_wing3d(args) -> int:
     return 0
 
 
+def roofline_of(kern: dict, model: str, nvar: int, cells: int, peaks: dict, kernel: str = "jvp_tile") -> dict:
+    """A tile kernel's achieved HBM bandwidth: its algorithmic bytes per launch over its
+    CUDA-event launch time, against the measured copy bandwidth."""
+    per_cell = jvp_bytes_per_cell(model, nvar) if kernel == "jvp_tile" else residual_bytes_per_cell(model, nvar)
+    achieved = per_cell * cells / (kern[kernel] * 1e-3) / 1e9
+    return {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / peaks["hbm_gbs"], "traffic": None, "algorithmic_bytes_per_cell": per_cell,
+            "algorithmic_bytes_per_launch": per_cell * cells, "launch_ms": kern[kernel],
+            "peak_source": peaks.get("source", "measured")}
+
+
 def max_over_ranks(values, dist, device):
     """Each value's maximum over the ranks (the slowest replica times the job); the
     values themselves without a process group."""
@@ -450,15 +516,15 @@ def run_device(args) -> int:
     blocks = [max(len(m.blocks) for m in mons) for mons in solves]
     steps_run = [max(m.iterations for m in mons) for mons in solves]
     # the Newton steps' kernels (skipped Krylov cycles not counted) and, per block, the
-    # ghost fill and force kernels of the force monitor
-    launches = launched + 2 * sum(blocks)
+    # ghost fill, force and exit-test kernels of the device monitor: all counted by the plan
+    launches = launched
     kern = dev.time_kernels(20)
     peaks = measured_peaks()
     nvar = cases[0].flow.nvar
-    bpc = jvp_bytes_per_cell(nvar)
+    model = model_of(cases[0].flow)
     cells = sum(g.cells for g in grids)
-    achieved = bpc * cells / (kern["jvp_tile"] * 1e-3) / 1e9
-    traffic = profiled_traffic(args.workload)
+    roofline = roofline_of(kern, model, nvar, cells, peaks)
+    roofline["traffic"] = profiled_traffic(args.workload)
     last = solves[-1]
     config = {"workload": args.workload, "cases": n_cases, "cells": cells, "nvar": nvar,
               "precision": args.precision, "newton_steps_per_solve": int(np.median(iters)),
@@ -481,26 +547,22 @@ def run_device(args) -> int:
         "config": config,
         "latency_s": {"p50": float(np.percentile(latencies, 50)), "p99": float(np.percentile(latencies, 99))},
         "e2e": {"value": e2e_value, "unit": "solves/hr", "h2d_bytes_per_step": int(U0.nbytes),
+                # the state, every step's |R| and every block's force sample of every case
                 "d2h_bytes_per_step": int(U0.nbytes + max(len(m.blocks) for m in out) * 8 * n_cases
-                                          * (block_iters + 6))},
+                                          * (block_iters + 3))},
         "gpu_launches": launches,
-        "roofline": {"kernel": "jvp_tile", "bound": "hbm", "achieved": achieved,
-                     "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-                     "traffic": None if traffic is None else traffic,
-                     "algorithmic_bytes_per_launch": bpc * cells, "launch_ms": kern["jvp_tile"],
-                     "peak_source": peaks.get("source", "measured")},
+        "roofline": roofline,
+        "roofline_residual": roofline_of(kern, model, nvar, cells, peaks, kernel="residual_tile"),
         "kernel_ms": kern,
     }
     if rank == 0:
         result["clocks"] = clocks.summary()
         if world == 1 and not args.no_cpu_baseline:
-            times = reference_sample(cases[0], grids[0], 1, 0, args.precision)
-            per = times[0]
-            n = int(np.median(iters))
-            result["cpu_baseline"] = {
-                "value": 3600.0 / (per * n), "unit": "solves/hr", "cores": 1, "kind": "port",
-                "sample": (f"one Newton step of the oracle (NumPy FP64, complex-step J.v) from the freestream on "
-                           f"{cases[0].name}, {per:.2f} s, scaled by the {n} Newton steps of a converged solve")}
+            from jaxrans_b200.workloads import BATCHES
+            name = BATCHES[args.workload][0][0] if args.workload in BATCHES else args.workload
+            cpu = cpu_rate(name, args.steps, args.warmup, args.precision, STEPS_PER_SOLVE[name])
+            cpu.pop("seconds_per_step")
+            result["cpu_baseline"] = cpu
         print(json.dumps(result), flush=True)
     if dist is not None:
         dist.barrier()

@@ -122,7 +122,8 @@ int jr_plan_sizes(const jr_plan* plan, int64_t* n_canvas, int64_t* n_faces);
 /* The plan's CUDA stream (a cudaStream_t), for callers that order their own work on it. */
 void* jr_plan_stream(jr_plan* plan);
 /* Issue the plan's work on a caller's cudaStream_t (an XLA FFI handler passes XLA's);
- * NULL returns to the plan's own stream.  The stream in use is drained first. */
+ * NULL returns to the plan's own stream.  The stream in use is drained first, unless it
+ * is already the one asked for (then the call does nothing). */
 int jr_plan_set_stream(jr_plan* plan, void* stream);
 int jr_synchronize(jr_plan* plan);
 
@@ -148,8 +149,11 @@ int jr_residual(jr_plan* plan, const double* U, double* R, int first_order);
  * pointers. */
 int jr_residual_noalloc(jr_plan* plan, const double* U, double* R, int first_order);
 
-/* dR1/dU . v: the exact tangent of the first-order residual at U (forward-mode duals).
- * Replaces jax.linearize(jacobian_source.residual, U)'s jvp
+/* dR1/dU . v: the exact tangent of the first-order residual at U.  The call linearises
+ * the residual at U (each face's flux derivatives and each cell's SA source derivatives,
+ * by forward-mode duals, into the plan's linearisation buffer) and applies that
+ * linearisation to v, as a Newton step does once per step and once per Arnoldi step.
+ * Replaces jax.linearize(jacobian_source.residual, U) and its jvp
  * (src/jaxrans/solvers/implicit.py:104-108).  Device pointers. */
 int jr_jvp(jr_plan* plan, const double* U, const double* v, double* Jv);
 
@@ -185,10 +189,11 @@ int jr_graph_kernels(jr_plan* plan, int64_t* kernels_per_step);
  * counterpart in the reference. */
 int jr_launch_count(jr_plan* plan, int64_t* kernels);
 /* Average device time (ms, CUDA events on the plan's stream, reps launches each, after one
- * untimed launch) of the hot kernels at the plan's state, out[0..5]: the residual tile, the
- * J.v tile, the tangent ghost fill, the line-solve apply, the line factor, and one CGS2
- * orthogonalisation against the full basis (three passes).  Replaces the timing loop of
- * the reference's scripts/benchmark.py:40-47,88-108 for these pieces. */
+ * untimed launch) of the hot kernels at the plan's state, out[0..6]: the residual tile, the
+ * J.v tile (the tangent pass over the linearisation), the tangent ghost fill, the
+ * line-solve apply, the line factor, one CGS2 orthogonalisation against the full basis
+ * (three passes), and the linearisation (once per Newton step).  Replaces the timing loop
+ * of the reference's scripts/benchmark.py:40-47,88-108 for these pieces. */
 int jr_time_kernels(jr_plan* plan, int32_t reps, double* ms_out);
 
 /* n_steps pseudo-transient Newton steps on the plan's state, one captured CUDA graph per
@@ -202,6 +207,28 @@ int jr_newton_steps(jr_plan* plan, int32_t n_steps, double* history);
 /* The same step count without synchronising: history_device (n_steps x n_cases doubles
  * on the device) receives the norms.  For timing with events on the plan's stream. */
 int jr_newton_steps_async(jr_plan* plan, int32_t n_steps, double* history_device);
+
+/* The exit test of case c on the device (the driver's per-case test,
+ * src/jaxrans/solvers/driver.py:161-190, with the force settling of
+ * src/jaxrans/simulation.py:259-272), run by jr_monitor_blocks after every block:
+ * non-finite (a NaN or Inf norm or force coefficient), converged (the block's last |R| <=
+ * tol x the running peak), stalled (every |R| of the block equal), settled (CL, CD and CM
+ * each varying by less than forces_tol over the last quarter of the blocks, at least four
+ * there; forces_tol <= 0: no such test), max_iters after max_blocks blocks (1..1024).
+ * release != 0: the case leaves the launches when it stops (a single-case plan is left
+ * enabled for later calls).  Resets the case's monitor and enables the case. */
+int jr_monitor_set(jr_plan* plan, int32_t c, double tol, double forces_tol, int32_t max_blocks, int32_t release);
+/* n_blocks blocks of block_iters Newton steps of every enabled case, each block followed on
+ * the device by the forces and the exit test of every monitored case; one synchronisation
+ * at the end instead of one per block.  history (host, n_blocks * block_iters x n_cases,
+ * step-major, at most 4096 steps) receives each case's |R| before each step; rows after
+ * a case stopped are not its.  JR_ETIMEOUT as jr_newton_steps.  Replaces the driver's
+ * host loop over blocks (src/jaxrans/solvers/driver.py:161-190). */
+int jr_monitor_blocks(jr_plan* plan, int32_t n_blocks, int32_t block_iters, double* history);
+/* Case c's monitor: reason (0 running, 1 converged, 2 settled, 3 max_iters, 4 non_finite,
+ * 5 stalled), blocks run, the running peak of |R|, and (may be NULL) the force samples,
+ * blocks x 3 (CL, CD, CM after each block). */
+int jr_monitor_get(jr_plan* plan, int32_t c, int32_t* reason, int32_t* blocks, double* peak, double* coefficients);
 
 /* The plan's autotuner: times the line factor and the line solve with each block size the
  * longest chain allows (64, 128, 256 threads per chain, reps launches each, at the plan's

@@ -1,6 +1,7 @@
 // The C ABI: plans (a batch of cases: device copies of each case's static tables, work
 // buffers and solver state, one stream), the per-call entry points, and the Newton step
 // of every case of the batch as one CUDA graph.  A single case is a batch of one.
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -19,6 +20,9 @@ void launch_residual(const CaseDev*, const BatchDims&, int visc, bool second, in
 void launch_jvp(const CaseDev*, const BatchDims&, int visc, int tangent_id, int vdt_id, int out_id, int check_active,
                 int own_ghosts, cudaStream_t);
 void launch_ghosts(const CaseDev*, const BatchDims&, int tangent_id, int check_active, cudaStream_t);
+void launch_linearize(const CaseDev*, const BatchDims&, int visc, cudaStream_t);
+int jac_coefficients(int visc);
+int jac_cell_coefficients(int visc);
 void launch_faces(const CaseDev*, const BatchDims&, int visc, cudaStream_t);
 void launch_cells(const CaseDev*, const BatchDims&, int visc, cudaStream_t);
 dim3 tile_grid(const Canvas&);
@@ -48,6 +52,7 @@ void launch_newton_update(const CaseDev*, const BatchDims&, cudaStream_t);
 int reduce_blocks(int n);
 // forces.cu
 void launch_forces(const CaseDev*, const BatchDims&, cudaStream_t);
+void launch_monitor(CaseDev* cases, int n_live, int n_slots, int step0, int block_iters, cudaStream_t st);
 }  // namespace jr
 
 using namespace jr;
@@ -76,6 +81,7 @@ struct jr_plan {
   double* history = nullptr;             // [step][case]
   double* force_out = nullptr;           // 8 per case
   Scalars* sc = nullptr;                 // one per case
+  Monitor* mon = nullptr;                // one per case: the exit test on the device
   cudaGraphExec_t graph = nullptr;
   int device = 0;                        // the device current when the plan was made
   // the step graph runs over the enabled cases only: their descriptors packed in slot
@@ -298,8 +304,9 @@ static int build_case(jr_plan* plan, const jr_plan_desc* d, CaseDev& cd, size_t&
 // Work buffers: each kind is one allocation holding every case's part back to back.
 static int build_buffers(jr_plan* p, const std::vector<size_t>& factor_rows) {
   const int nc = p->n_cases;
-  std::vector<size_t> tile_off(nc), fb_off(nc), part_off(nc);
-  size_t tiles = 0, fb = 0, part = 0;
+  std::vector<size_t> tile_off(nc), fb_off(nc), part_off(nc), jac_off(nc);
+  size_t tiles = 0, fb = 0, part = 0, jac = 0;
+  const int n_coef = jac_coefficients(p->visc), n_cell_coef = jac_cell_coefficients(p->visc);
   p->vec_off.assign(nc, 0);
   p->can_off.assign(nc, 0);
   p->face_off.assign(nc, 0);
@@ -319,6 +326,9 @@ static int build_buffers(jr_plan* p, const std::vector<size_t>& factor_rows) {
     p->total_can += N;
     p->total_faces += nf;
     tiles += (size_t)p->host[k].n_tiles;
+    p->host[k].jstride = (int)((nf + 31) / 32 * 32);
+    jac_off[k] = jac;
+    jac += (size_t)n_coef * p->host[k].jstride + (size_t)n_cell_coef * N;
     fb += factor_rows[k];
     part += (size_t)reduce_blocks(p->host[k].n_vec) * (MAX_KRYLOV + 1);
   }
@@ -326,7 +336,7 @@ static int build_buffers(jr_plan* p, const std::vector<size_t>& factor_rows) {
   const int NVEC = 11;
   double* vec[NVEC];
   for (int v = 0; v < NVEC; ++v) TRY(dev_alloc(p, (void**)&vec[v], p->total_vec * sizeof(double)));
-  double *vdt, *dflow, *dsa, *lam, *mflux, *dflux, *tile_partial, *partial;
+  double *vdt, *dflow, *dsa, *lam, *mflux, *dflux, *tile_partial, *partial, *lin;
   unsigned* ticket;
   void *V, *fflow, *fsa, *scratch;
   TRY(dev_alloc(p, (void**)&vdt, p->total_can * sizeof(double)));
@@ -336,6 +346,7 @@ static int build_buffers(jr_plan* p, const std::vector<size_t>& factor_rows) {
   TRY(dev_alloc(p, (void**)&mflux, p->total_faces * sizeof(double)));
   TRY(dev_alloc(p, (void**)&dflux, p->total_faces * sizeof(double)));
   TRY(dev_alloc(p, (void**)&tile_partial, tiles * sizeof(double)));
+  TRY(dev_alloc(p, (void**)&lin, jac * sizeof(double)));
   TRY(dev_alloc(p, (void**)&partial, part * sizeof(double)));
   TRY(dev_alloc(p, (void**)&ticket, (size_t)nc * sizeof(unsigned)));
   TRY(dev_alloc(p, &V, (size_t)(p->m + 1) * p->total_vec * tb));
@@ -345,6 +356,7 @@ static int build_buffers(jr_plan* p, const std::vector<size_t>& factor_rows) {
   TRY(dev_alloc(p, &fsa, fb * 5 * tb));
   TRY(dev_alloc(p, &scratch, fb * 104 * tb));
   TRY(dev_alloc(p, (void**)&p->sc, (size_t)nc * sizeof(Scalars)));
+  TRY(dev_alloc(p, (void**)&p->mon, (size_t)nc * sizeof(Monitor)));
   TRY(dev_alloc(p, (void**)&p->history, (size_t)HIST_STEPS * nc * sizeof(double)));
   TRY(dev_alloc(p, (void**)&p->force_out, (size_t)8 * nc * sizeof(double)));
   TRY(dev_alloc(p, (void**)&p->wall_out, std::max<size_t>(1, p->total_walls) * 5 * sizeof(double)));
@@ -361,6 +373,8 @@ static int build_buffers(jr_plan* p, const std::vector<size_t>& factor_rows) {
     cd.mflux = mflux + fo;
     cd.dflux = dflux + fo;
     cd.tile_partial = tile_partial + tile_off[k];
+    cd.jac = lin + jac_off[k];
+    cd.jcell = n_cell_coef > 0 ? cd.jac + (size_t)n_coef * cd.jstride : nullptr;
     cd.partial = partial + part_off[k];
     cd.ticket = ticket + k;
     cd.V = (char*)V + (size_t)(p->m + 1) * vo * tb;
@@ -368,6 +382,7 @@ static int build_buffers(jr_plan* p, const std::vector<size_t>& factor_rows) {
     cd.fsa = (char*)fsa + fb_off[k] * 5 * tb;
     cd.scratch = (char*)scratch + fb_off[k] * 104 * tb;
     cd.sc = p->sc + k;
+    cd.mon = p->mon + k;
     cd.slot = k;
     cd.history = p->history;
     cd.force_out = p->force_out + 8 * k;
@@ -489,6 +504,7 @@ static int enqueue_step(jr_plan* p) {
   cudaStream_t st = p->st;
   launch_ghosts(t, d, -1, 0, st);
   launch_residual(t, d, p->visc, true, B_R, st);
+  launch_linearize(t, d, p->visc, st);
   launch_gmres_init(t, d, st);
   launch_faces(t, d, p->visc, st);
   launch_cells(t, d, p->visc, st);
@@ -647,8 +663,10 @@ void* jr_plan_stream(jr_plan* plan) { return plan ? (void*)plan->st : nullptr; }
 
 int jr_plan_set_stream(jr_plan* plan, void* stream) {
   if (!plan) return fail(JR_EINVAL, "null plan");
+  cudaStream_t next = stream != nullptr ? (cudaStream_t)stream : plan->owned_stream;
+  if (next == plan->st) return JR_OK;
   if (cudaStreamSynchronize(plan->st) != cudaSuccess) return cuda_check("jr_plan_set_stream");
-  plan->st = stream != nullptr ? (cudaStream_t)stream : plan->owned_stream;
+  plan->st = next;
   return JR_OK;
 }
 
@@ -681,6 +699,7 @@ int jr_jvp(jr_plan* plan, const double* U, const double* v, double* Jv) {
   bool vortex = false;
   for (const CaseDev& cd : plan->host) vortex = vortex || cd.P.far_field == 1;
   launch_ghosts(t, plan->dims, -1, 0, plan->st);
+  launch_linearize(t, plan->dims, plan->visc, plan->st);
   if (vortex) launch_ghosts(t, plan->dims, B_Z, 0, plan->st);
   launch_jvp(t, plan->dims, plan->visc, B_Z, -1, B_W, 0, vortex ? 0 : 1, plan->st);
   return cuda_check("jr_jvp");
@@ -974,6 +993,100 @@ int jr_newton_steps(jr_plan* plan, int32_t n_steps, double* history) {
   return JR_OK;
 }
 
+int jr_monitor_set(jr_plan* plan, int32_t c, double tol, double forces_tol, int32_t max_blocks, int32_t release) {
+  if (!plan || c < 0 || c >= plan->n_cases) return fail(JR_EINVAL, "bad plan or case");
+  if (max_blocks < 1 || max_blocks > MONITOR_BLOCKS)
+    return fail(JR_EINVAL, "max_blocks must lie in [1, " + std::to_string(MONITOR_BLOCKS) + "]");
+  if (!(tol >= 0.0)) return fail(JR_EINVAL, "tol must be >= 0");
+  Monitor head{};
+  head.tol = tol;
+  head.forces_tol = forces_tol > 0.0 ? forces_tol : -1.0;
+  head.peak = 0.0;
+  head.max_blocks = max_blocks;
+  head.blocks = 0;
+  head.reason = MON_RUNNING;
+  head.release = release != 0;
+  cudaMemcpyAsync(plan->mon + c, &head, offsetof(Monitor, coef), cudaMemcpyHostToDevice, plan->st);
+  if (!plan->host[c].enabled) {
+    plan->host[c].enabled = 1;
+    return upload_table(plan);
+  }
+  if (cudaStreamSynchronize(plan->st) != cudaSuccess) return cuda_check("jr_monitor_set");
+  return cuda_check("jr_monitor_set");
+}
+
+int jr_monitor_blocks(jr_plan* plan, int32_t n_blocks, int32_t block_iters, double* history) {
+  if (!plan || n_blocks < 1 || block_iters < 1) return fail(JR_EINVAL, "bad argument");
+  if ((int64_t)n_blocks * block_iters > HIST_STEPS) return fail(JR_EINVAL, "at most 4096 steps per call");
+  int rc = ensure_graph(plan);
+  if (rc) return rc;
+  cudaStream_t st = plan->st;
+  for (int k = 0; k < plan->n_cases; ++k) cudaMemsetAsync(&plan->sc[k].hpos, 0, sizeof(int), st);
+  if (plan->n_live > 0) {
+    for (int b = 0; b < n_blocks; ++b) {
+      for (int k = 0; k < block_iters; ++k)
+        if (cudaGraphLaunch(plan->graph, st) != cudaSuccess) return cuda_check("graph launch");
+      plan->steps_since += block_iters;
+      launch_ghosts(plan->live, plan->live_dims, -1, 0, st);
+      launch_forces(plan->live, plan->live_dims, st);
+      launch_monitor(plan->live, plan->n_live, plan->n_cases, b * block_iters, block_iters, st);
+      plan->launched += 3;
+    }
+  }
+  if (history)
+    cudaMemcpyAsync(history, plan->history, (size_t)n_blocks * block_iters * plan->n_cases * sizeof(double),
+                    cudaMemcpyDeviceToHost, st);
+  std::vector<int> status(plan->n_cases, 0), reason(plan->n_cases, 0), release(plan->n_cases, 0);
+  cudaMemcpy2DAsync(status.data(), sizeof(int), &plan->sc[0].status, sizeof(Scalars), sizeof(int), plan->n_cases,
+                    cudaMemcpyDeviceToHost, st);
+  cudaMemcpy2DAsync(reason.data(), sizeof(int), &plan->mon[0].reason, sizeof(Monitor), sizeof(int), plan->n_cases,
+                    cudaMemcpyDeviceToHost, st);
+  cudaMemcpy2DAsync(release.data(), sizeof(int), &plan->mon[0].release, sizeof(Monitor), sizeof(int),
+                    plan->n_cases, cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return cuda_check("jr_monitor_blocks");
+  rc = cuda_check("jr_monitor_blocks");
+  if (rc) return rc;
+  // a stopped case the device took out of the launches: a batch's leaves the host's
+  // launch set too; a single case's plan is left enabled, as after jr_newton_steps
+  bool changed = false;
+  for (int k = 0; k < plan->n_cases; ++k) {
+    if (!plan->host[k].enabled || reason[k] == MON_RUNNING || !release[k]) continue;
+    if (plan->n_cases > 1) {
+      plan->host[k].enabled = 0;
+      changed = true;
+    } else {
+      const int on = 1;
+      cudaMemcpyAsync(&plan->live[0].enabled, &on, sizeof(int), cudaMemcpyHostToDevice, st);
+      if (cudaStreamSynchronize(st) != cudaSuccess) return cuda_check("jr_monitor_blocks");
+    }
+  }
+  if (changed) {
+    rc = upload_table(plan);
+    if (rc) return rc;
+  }
+  for (int k = 0; k < plan->n_cases; ++k)
+    if (status[k] & ST_STAGE_FAILED)
+      return fail(JR_ETIMEOUT, "a line solve's staged copy did not land within its wait limit");
+  return JR_OK;
+}
+
+int jr_monitor_get(jr_plan* plan, int32_t c, int32_t* reason, int32_t* blocks, double* peak, double* coefficients) {
+  if (!plan || c < 0 || c >= plan->n_cases) return fail(JR_EINVAL, "bad plan or case");
+  Monitor head{};
+  cudaMemcpyAsync(&head, plan->mon + c, offsetof(Monitor, coef), cudaMemcpyDeviceToHost, plan->st);
+  if (cudaStreamSynchronize(plan->st) != cudaSuccess) return cuda_check("jr_monitor_get");
+  const int n = head.blocks < MONITOR_BLOCKS ? head.blocks : MONITOR_BLOCKS;
+  if (coefficients && n > 0) {
+    const char* coef = reinterpret_cast<const char*>(plan->mon + c) + offsetof(Monitor, coef);
+    cudaMemcpyAsync(coefficients, coef, (size_t)n * 3 * sizeof(double), cudaMemcpyDeviceToHost, plan->st);
+    if (cudaStreamSynchronize(plan->st) != cudaSuccess) return cuda_check("jr_monitor_get");
+  }
+  if (reason) *reason = head.reason;
+  if (blocks) *blocks = head.blocks;
+  if (peak) *peak = head.peak;
+  return cuda_check("jr_monitor_get");
+}
+
 int jr_time_kernels(jr_plan* plan, int32_t reps, double* ms) {
   if (!plan || !ms || reps < 1) return fail(JR_EINVAL, "bad argument");
   jr_plan* p = plan;
@@ -988,6 +1101,7 @@ int jr_time_kernels(jr_plan* plan, int32_t reps, double* ms) {
   // active Krylov cycle with z = the residual
   launch_ghosts(t, d, -1, 0, st);
   launch_residual(t, d, p->visc, true, B_R, st);
+  launch_linearize(t, d, p->visc, st);
   launch_faces(t, d, p->visc, st);
   launch_cells(t, d, p->visc, st);
   launch_chain_factor(t, d, sa, p->mixed, st);
@@ -1017,6 +1131,7 @@ int jr_time_kernels(jr_plan* plan, int32_t reps, double* ms) {
   timed(3, [&] { launch_chain_apply(t, d, sa, p->mixed, B_R, 0, -1, B_TMP, 0, st); });
   timed(4, [&] { launch_chain_factor(t, d, sa, p->mixed, st); });
   timed(5, [&] { launch_arnoldi_orth(t, d, p->mixed, p->m - 1, st); });
+  timed(6, [&] { launch_linearize(t, d, p->visc, st); });
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return cuda_check("jr_time_kernels");

@@ -70,6 +70,24 @@ struct Canvas {
   __device__ __forceinline__ int ncanvas() const { return NI * NJ; }
 };
 
+// The exit test of one case, run on the device after every block of Newton steps
+// (src/jaxrans/solvers/driver.py:161-190 with the force settling of
+// src/jaxrans/simulation.py:259-272): the running peak of |R|, the forces after every
+// block, and why the case stopped.
+constexpr int MONITOR_BLOCKS = 1024;   // blocks (force samples) a monitor holds
+enum MonitorReason { MON_RUNNING = 0, MON_CONVERGED = 1, MON_SETTLED = 2, MON_MAX_ITERS = 3, MON_NON_FINITE = 4,
+                     MON_STALLED = 5 };
+struct Monitor {
+  double tol;          // converged: the block's last |R| <= tol x the running peak
+  double forces_tol;   // settled: CL, CD, CM each vary by less over the last quarter (< 0: no test)
+  double peak;         // the largest finite |R| so far
+  int max_blocks;      // 0: the case is not monitored
+  int blocks;          // blocks seen
+  int reason;          // MonitorReason
+  int release;         // 1: the case leaves the launches when it stops
+  double coef[MONITOR_BLOCKS][3];   // CL, CD, CM after each block
+};
+
 // Per-case solver scalars, resident on the device across a whole block of steps.
 struct Scalars {
   double cfl, res_prev, norm, bnorm, rnorm, beta;
@@ -104,15 +122,19 @@ struct CaseDev {
   Config cfg;
   double *U, *qg, *dqg, *R, *b, *x, *action, *r, *w, *z, *tmp, *vdt, *dflow, *dsa, *lam, *mflux, *dflux;
   double *tile_partial, *history, *force_out;
+  double* jac;              // the linearisation: per face coefficient planes of jstride doubles
+  double* jcell;            // ... and per cell (SA: 7 planes of NI*NJ)
   double* wall_out;         // per wall face: gauge pressure, area vector into the fluid (2), viscous force (2)
   void *V, *fflow, *fsa, *scratch;
   Scalars* sc;
+  Monitor* mon;             // the case's exit test on the device
   double* partial;          // reduction partials of this case
   unsigned int* ticket;     // its last-block ticket
   double force_length, moment_centre[2];   // force coefficients' reference length and moment centre
   int n_vec, m, visc, mixed, n_tiles, tiles_x, tiles_y;
   int enabled;              // 0: a free slot, every kernel returns at once
   int slot;                 // the case's index in its plan (its history column)
+  int jstride, jpad;        // the coefficient planes' stride (faces rounded up to 32)
 };
 
 // Buffers a kernel may be told to read or write (resolved per case)

@@ -152,4 +152,83 @@ void launch_forces(const CaseDev* cases, const BatchDims& d, cudaStream_t st) {
   k_forces<<<dim3(1, d.n_cases), 256, 0, st>>>(cases);
 }
 
+// The exit test of every monitored case after a block of block_iters Newton steps whose
+// norms sit in rows step0.. of the history, and whose forces k_forces has just written
+// (one warp per case).  The decisions are the host driver's, in the same order and with
+// the same arithmetic: non-finite (a NaN or Inf norm or force), converged (last <= tol x
+// running peak), stalled (every norm of the block equal to the first), settled (CL, CD
+// and CM each with a range below forces_tol over the last quarter of the samples, at
+// least four there), and max_iters once max_blocks blocks have run.  A case that stops
+// with `release` set is disabled in `cases` itself, so the launches already queued skip
+// it.
+__global__ void __launch_bounds__(32) k_monitor(CaseDev* __restrict__ cases, int n_slots, int step0,
+                                                int block_iters) {
+  CaseDev& cd = cases[blockIdx.x];
+  if (!cd.enabled || cd.mon == nullptr) return;
+  Monitor& m = *cd.mon;
+  if (m.max_blocks == 0 || m.reason != MON_RUNNING) return;
+  const int lane = threadIdx.x;
+  const double* hist = cd.history + (size_t)step0 * n_slots + cd.slot;
+  const double first = hist[0], last = hist[(size_t)(block_iters - 1) * n_slots];
+  bool finite = true, equal = true;
+  double top = -INFINITY;
+  bool any = false;
+  for (int s = lane; s < block_iters; s += 32) {
+    const double h = hist[(size_t)s * n_slots];
+    const bool ok = isfinite(h);
+    finite = finite && ok;
+    equal = equal && h == first;
+    if (ok) {
+      top = fmax(top, h);
+      any = true;
+    }
+  }
+  finite = __all_sync(0xffffffffu, finite);
+  equal = __all_sync(0xffffffffu, equal);
+  any = __any_sync(0xffffffffu, any);
+  for (int o = 16; o > 0; o >>= 1) top = fmax(top, __shfl_xor_sync(0xffffffffu, top, o));
+  const double cl = cd.force_out[0], cdr = cd.force_out[1], cm = cd.force_out[2];
+  const int n = m.blocks + 1;
+  if (lane == 0 && m.blocks < MONITOR_BLOCKS) {
+    m.coef[m.blocks][0] = cl;
+    m.coef[m.blocks][1] = cdr;
+    m.coef[m.blocks][2] = cm;
+  }
+  __syncwarp();
+  const double peak = any ? fmax(m.peak, top) : m.peak;
+  // the spread of each coefficient over the last quarter of the n samples
+  const int start = 3 * n / 4, tail = n - start;
+  bool settled = false;
+  if (m.forces_tol >= 0.0 && tail >= 4 && n <= MONITOR_BLOCKS) {
+    settled = true;
+    for (int k = 0; k < 3; ++k) {
+      double lo = INFINITY, hi = -INFINITY;
+      for (int b = start + lane; b < n; b += 32) {
+        lo = fmin(lo, m.coef[b][k]);
+        hi = fmax(hi, m.coef[b][k]);
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+      }
+      settled = settled && (hi - lo < m.forces_tol);
+    }
+  }
+  if (lane != 0) return;
+  m.peak = peak;
+  m.blocks = n;
+  int reason = MON_RUNNING;
+  if (!finite || !isfinite(cl) || !isfinite(cdr) || !isfinite(cm)) reason = MON_NON_FINITE;
+  else if (peak > 0.0 && last <= m.tol * peak) reason = MON_CONVERGED;
+  else if (block_iters > 1 && equal) reason = MON_STALLED;
+  else if (settled) reason = MON_SETTLED;
+  else if (n >= m.max_blocks) reason = MON_MAX_ITERS;
+  m.reason = reason;
+  if (reason != MON_RUNNING && m.release) cd.enabled = 0;
+}
+
+void launch_monitor(CaseDev* cases, int n_live, int n_slots, int step0, int block_iters, cudaStream_t st) {
+  if (n_live > 0) k_monitor<<<n_live, 32, 0, st>>>(cases, n_slots, step0, block_iters);
+}
+
 }  // namespace jr

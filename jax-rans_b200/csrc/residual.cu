@@ -296,6 +296,154 @@ template <class T, int NV> struct TileSmem {
   double red[TILE_THREADS / 32];
 };
 
+// The viscous face terms in two parts.  face_intermediates gathers, from the cells
+// either side of a face and the four other cells of its two nodes, what the viscous flux
+// depends on: the diamond gradients of u, v, T (and nu_hat), the two-cell means of u,
+// v and T (and rho, p, nu_hat).  Each is linear in the cells' values of (u, v, T, ...),
+// so the same function maps tangents of those values to tangents of the intermediates.
+// viscous_tail is the nonlinear rest (viscosity, eddy viscosity, QCR, stresses, heat
+// flux, SA diffusion).  x: [0..3] du/dx, du/dy, dv/dx, dv/dy; [4, 5] dT/dx, dT/dy;
+// [6, 7] face u, v; [8] face T; SA: [9, 10] dnu_hat/dx, dnu_hat/dy; [11..13] face rho,
+// p, nu_hat.  (residual.py:94-124, gradients.py:59-95, turbulence.py:78-90,129-135)
+template <int VISC> struct ViscShape {
+  static constexpr int NX = VISC == 2 ? 14 : 9;   // intermediates
+  static constexpr int NR = VISC == 2 ? 4 : 3;    // tail outputs: fx, fy, energy[, SA diffusion]
+};
+
+// q(v, i, j): primitive row v of staged cell (i, j); phi(i, j, k): (u, v, T, nu_hat)[k];
+// cx(i, j), cy(i, j): the cell's centre.  The face lies between A = (ai, aj) and the next
+// cell along `axis`.
+template <class T, int VISC, class Q, class PHI, class CX, class CY>
+__device__ __forceinline__ void face_intermediates(Q q, PHI phi, CX cxv, CY cyv, int axis, int ai, int aj, T* x) {
+  const int di = axis == 0 ? 1 : 0, dj = axis == 0 ? 0 : 1;
+  const int bi = ai + di, bj = aj + dj;
+  // the face's two nodes, each the mean of its four cells
+  int n0i[4], n0j[4], n1i[4], n1j[4];
+  if (axis == 0) {
+    // i-face between (ai, aj) and (ai+1, aj): nodes at (i, j) and (i, j+1)
+    n0i[0] = ai; n0j[0] = aj - 1; n0i[1] = ai + 1; n0j[1] = aj - 1;
+    n0i[2] = ai; n0j[2] = aj;     n0i[3] = ai + 1; n0j[3] = aj;
+    n1i[0] = ai; n1j[0] = aj;     n1i[1] = ai + 1; n1j[1] = aj;
+    n1i[2] = ai; n1j[2] = aj + 1; n1i[3] = ai + 1; n1j[3] = aj + 1;
+  } else {
+    // j-face between (ai, aj) and (ai, aj+1): nodes at (i, j) and (i+1, j)
+    n0i[0] = ai - 1; n0j[0] = aj; n0i[1] = ai;     n0j[1] = aj;
+    n0i[2] = ai - 1; n0j[2] = aj + 1; n0i[3] = ai; n0j[3] = aj + 1;
+    n1i[0] = ai;     n1j[0] = aj; n1i[1] = ai + 1; n1j[1] = aj;
+    n1i[2] = ai;     n1j[2] = aj + 1; n1i[3] = ai + 1; n1j[3] = aj + 1;
+  }
+  double d1x = cxv(bi, bj) - cxv(ai, aj), d1y = cyv(bi, bj) - cyv(ai, aj);
+  double xn0 = 0.25 * (((cxv(n0i[0], n0j[0]) + cxv(n0i[1], n0j[1])) + cxv(n0i[2], n0j[2])) + cxv(n0i[3], n0j[3]));
+  double yn0 = 0.25 * (((cyv(n0i[0], n0j[0]) + cyv(n0i[1], n0j[1])) + cyv(n0i[2], n0j[2])) + cyv(n0i[3], n0j[3]));
+  double xn1 = 0.25 * (((cxv(n1i[0], n1j[0]) + cxv(n1i[1], n1j[1])) + cxv(n1i[2], n1j[2])) + cxv(n1i[3], n1j[3]));
+  double yn1 = 0.25 * (((cyv(n1i[0], n1j[0]) + cyv(n1i[1], n1j[1])) + cyv(n1i[2], n1j[2])) + cyv(n1i[3], n1j[3]));
+  double d2x = xn1 - xn0, d2y = yn1 - yn0;
+  double det = d1x * d2y - d2x * d1y;
+  constexpr int NPHI = VISC == 2 ? 4 : 3;
+  T gx[NPHI], gy[NPHI];
+#pragma unroll
+  for (int k = 0; k < NPHI; ++k) {
+    T dpc = phi(bi, bj, k) - phi(ai, aj, k);
+    T p0 = 0.25 * (((phi(n0i[0], n0j[0], k) + phi(n0i[1], n0j[1], k)) + phi(n0i[2], n0j[2], k)) + phi(n0i[3], n0j[3], k));
+    T p1 = 0.25 * (((phi(n1i[0], n1j[0], k) + phi(n1i[1], n1j[1], k)) + phi(n1i[2], n1j[2], k)) + phi(n1i[3], n1j[3], k));
+    T dpn = p1 - p0;
+    gx[k] = (dpc * d2y - dpn * d1y) / det;
+    gy[k] = (d1x * dpn - d2x * dpc) / det;
+  }
+  x[0] = gx[0];
+  x[1] = gy[0];
+  x[2] = gx[1];
+  x[3] = gy[1];
+  x[4] = gx[2];
+  x[5] = gy[2];
+  x[6] = 0.5 * (q(1, ai, aj) + q(1, bi, bj));
+  x[7] = 0.5 * (q(2, ai, aj) + q(2, bi, bj));
+  x[8] = 0.5 * (phi(ai, aj, 2) + phi(bi, bj, 2));
+  if constexpr (VISC == 2) {
+    x[9] = gx[3];
+    x[10] = gy[3];
+    x[11] = 0.5 * (q(0, ai, aj) + q(0, bi, bj));
+    x[12] = 0.5 * (q(3, ai, aj) + q(3, bi, bj));
+    x[13] = 0.5 * (q(4, ai, aj) + q(4, bi, bj));
+  }
+}
+
+// out: fx, fy, energy (the viscous parts of rows 1-3, subtracted) and, SA, the
+// diffusion of nu_hat through the face (subtracted from row 4)
+template <class T, int VISC>
+__device__ __forceinline__ void viscous_tail(const Physics& P, const T* x, double sx, double sy, T* out) {
+  const double g = P.gamma;
+  T mu = viscosity(P, x[8]);
+  T k = mu / (PR_LAM * (g - 1.0));
+  T g00 = x[0], g01 = x[1], g10 = x[2], g11 = x[3];
+  T mut = cst<T>(0.0);
+  T ex00 = cst<T>(0.0), ex01 = cst<T>(0.0), ex10 = cst<T>(0.0), ex11 = cst<T>(0.0);
+  bool extra = false;
+  T rho_f, nuh_f, Tface;
+  if constexpr (VISC == 2) {
+    rho_f = x[11];
+    T p_f = x[12];
+    nuh_f = x[13];
+    Tface = g * p_f / rho_f;
+    T mu_face = viscosity(P, Tface);
+    mut = eddy_viscosity(P.sa, rho_f, nuh_f * P.mu_inf, mu_face / rho_f);
+    mu = mu + mut;
+    k = k + mut / (PR_TURB * (g - 1.0));
+    if (P.c_cr1 != 0.0) {
+      extra = true;
+      T square = ((g00 * g00 + g01 * g01) + g10 * g10) + g11 * g11;
+      bool pos = val(square) > 0.0;
+      T nrm = pos ? dsqrt(square) : cst<T>(1.0);
+      T r01 = (g01 - g10) / nrm, r10 = (g10 - g01) / nrm;
+      T r00 = (g00 - g00) / nrm, r11 = (g11 - g11) / nrm;
+      T div = g00 + g11;
+      T t00 = mut * (g00 + g00 - (2.0 / 3.0) * div * 1.0);
+      T t01 = mut * (g01 + g10 - (2.0 / 3.0) * div * 0.0);
+      T t10 = mut * (g10 + g01 - (2.0 / 3.0) * div * 0.0);
+      T t11 = mut * (g11 + g11 - (2.0 / 3.0) * div * 1.0);
+      T p00 = r00 * t00 + r01 * t01, p01 = r00 * t10 + r01 * t11;
+      T p10 = r10 * t00 + r11 * t01, p11 = r10 * t10 + r11 * t11;
+      ex00 = -P.c_cr1 * (p00 + p00);
+      ex01 = -P.c_cr1 * (p01 + p10);
+      ex10 = -P.c_cr1 * (p10 + p01);
+      ex11 = -P.c_cr1 * (p11 + p11);
+    }
+  }
+  T div = g00 + g11;
+  T ttd = (2.0 / 3.0) * div;
+  T t00 = mu * (2.0 * g00 - ttd), t11 = mu * (2.0 * g11 - ttd), t01 = mu * (g01 + g10);
+  T t10 = t01;
+  if (extra) {
+    t00 = t00 + ex00;
+    t01 = t01 + ex01;
+    t10 = t10 + ex10;
+    t11 = t11 + ex11;
+  }
+  T fx = t00 * sx + t01 * sy;
+  T fy = t10 * sx + t11 * sy;
+  out[0] = fx;
+  out[1] = fy;
+  out[2] = (x[6] * fx + x[7] * fy) + k * (x[4] * sx + x[5] * sy);
+  if constexpr (VISC == 2) {
+    T mu_face = viscosity(P, Tface);
+    T coef = diffusion_coefficient(P.sa, rho_f, nuh_f * P.mu_inf, mu_face);
+    out[3] = coef * (x[9] * sx + x[10] * sy);
+  }
+}
+
+// The SA source of one cell times nothing (the caller multiplies by the volume):
+// y = (rho, p, nu_hat, dv/dx, du/dy, dnu_hat/dx, dnu_hat/dy), the gradients by
+// Green-Gauss over face-averaged values (turbulence.py:93-103,138-151).
+template <class T>
+__device__ __forceinline__ T sa_cell_source(const Physics& P, const T* y, double d) {
+  T omega = dabs(y[3] - y[4]);
+  T rho = y[0];
+  T mu = viscosity(P, P.gamma * y[1] / rho);
+  T Pr, D;
+  sa_source(P.sa, y[2] * P.mu_inf, mu / rho, omega, d, Pr, D);
+  return rho * ((Pr - D) / P.mu_inf + P.sa.c_b2 / P.sa.sigma * P.mu_inf * (y[5] * y[5] + y[6] * y[6]));
+}
+
 // Flux through one face of the tile: inviscid (MUSCL or first-order faces), minus the
 // viscous flux, plus the SA convection-diffusion flux.  The face lies between the tile
 // cells A (lower) and B (upper) along `axis`; (ai, aj) is A's position in the staged
@@ -330,117 +478,27 @@ __device__ __forceinline__ void face_flux(const Physics& P, TileSmem<T, NV>& s, 
 #pragma unroll
   for (int v = 0; v < 4; ++v) F[v] = Finv[v];
   if constexpr (VISC > 0) {
-    // cells either side and the two nodes of the face (node = mean of 4 cells)
-    const T* qa[NV];
-    // phi = (u, v, T[, nu_hat]) at A and B
+    auto q = [&](int v, int i, int j) -> T { return s.q[v][i][j]; };
     auto phi = [&](int i, int j, int k) -> T {
       if (k < 2) return s.q[1 + k][i][j];
       if (k == 2) return g * s.q[3][i][j] / s.q[0][i][j];
       return s.q[4][i][j];
     };
-    (void)qa;
-    const int bi = ai + di, bj = aj + dj;
-    // node corners in staged-tile coordinates: n0 and n1 (the face's two ends)
-    int n0i[4], n0j[4], n1i[4], n1j[4];
-    if (axis == 0) {
-      // i-face between (ai, aj) and (ai+1, aj): nodes at (i, j) and (i, j+1)
-      n0i[0] = ai; n0j[0] = aj - 1; n0i[1] = ai + 1; n0j[1] = aj - 1;
-      n0i[2] = ai; n0j[2] = aj;     n0i[3] = ai + 1; n0j[3] = aj;
-      n1i[0] = ai; n1j[0] = aj;     n1i[1] = ai + 1; n1j[1] = aj;
-      n1i[2] = ai; n1j[2] = aj + 1; n1i[3] = ai + 1; n1j[3] = aj + 1;
-    } else {
-      // j-face between (ai, aj) and (ai, aj+1): nodes at (i, j) and (i+1, j)
-      n0i[0] = ai - 1; n0j[0] = aj; n0i[1] = ai;     n0j[1] = aj;
-      n0i[2] = ai - 1; n0j[2] = aj + 1; n0i[3] = ai; n0j[3] = aj + 1;
-      n1i[0] = ai;     n1j[0] = aj; n1i[1] = ai + 1; n1j[1] = aj;
-      n1i[2] = ai;     n1j[2] = aj + 1; n1i[3] = ai + 1; n1j[3] = aj + 1;
-    }
     // centres: staged with a 1-cell halo, offset 1 from the q tile's 2-cell halo
     auto cxv = [&](int i, int j) { return s.cx[i - 1][j - 1]; };
     auto cyv = [&](int i, int j) { return s.cy[i - 1][j - 1]; };
-    double d1x = cxv(bi, bj) - cxv(ai, aj), d1y = cyv(bi, bj) - cyv(ai, aj);
-    double xn0 = 0.25 * (((cxv(n0i[0], n0j[0]) + cxv(n0i[1], n0j[1])) + cxv(n0i[2], n0j[2])) + cxv(n0i[3], n0j[3]));
-    double yn0 = 0.25 * (((cyv(n0i[0], n0j[0]) + cyv(n0i[1], n0j[1])) + cyv(n0i[2], n0j[2])) + cyv(n0i[3], n0j[3]));
-    double xn1 = 0.25 * (((cxv(n1i[0], n1j[0]) + cxv(n1i[1], n1j[1])) + cxv(n1i[2], n1j[2])) + cxv(n1i[3], n1j[3]));
-    double yn1 = 0.25 * (((cyv(n1i[0], n1j[0]) + cyv(n1i[1], n1j[1])) + cyv(n1i[2], n1j[2])) + cyv(n1i[3], n1j[3]));
-    double d2x = xn1 - xn0, d2y = yn1 - yn0;
-    double det = d1x * d2y - d2x * d1y;
-    constexpr int NPHI = VISC == 2 ? 4 : 3;
-    T gx[NPHI], gy[NPHI];
-#pragma unroll
-    for (int k = 0; k < NPHI; ++k) {
-      T dpc = phi(bi, bj, k) - phi(ai, aj, k);
-      T p0 = 0.25 * (((phi(n0i[0], n0j[0], k) + phi(n0i[1], n0j[1], k)) + phi(n0i[2], n0j[2], k)) + phi(n0i[3], n0j[3], k));
-      T p1 = 0.25 * (((phi(n1i[0], n1j[0], k) + phi(n1i[1], n1j[1], k)) + phi(n1i[2], n1j[2], k)) + phi(n1i[3], n1j[3], k));
-      T dpn = p1 - p0;
-      gx[k] = (dpc * d2y - dpn * d1y) / det;
-      gy[k] = (d1x * dpn - d2x * dpc) / det;
-    }
-    // face velocity and temperature: two-cell means
-    T vel0 = 0.5 * (s.q[1][ai][aj] + s.q[1][bi][bj]);
-    T vel1 = 0.5 * (s.q[2][ai][aj] + s.q[2][bi][bj]);
-    T Tf = 0.5 * (phi(ai, aj, 2) + phi(bi, bj, 2));
-    T mu = viscosity(P, Tf);
-    T k = mu / (PR_LAM * (g - 1.0));
-    // gv[comp][dir]
-    T g00 = gx[0], g01 = gy[0], g10 = gx[1], g11 = gy[1];
-    T mut = cst<T>(0.0);
-    T ex00 = cst<T>(0.0), ex01 = cst<T>(0.0), ex10 = cst<T>(0.0), ex11 = cst<T>(0.0);
-    bool extra = false;
-    T rho_f, nuh_f, Tface;
-    if constexpr (VISC == 2) {
-      rho_f = 0.5 * (s.q[0][ai][aj] + s.q[0][bi][bj]);
-      T p_f = 0.5 * (s.q[3][ai][aj] + s.q[3][bi][bj]);
-      nuh_f = 0.5 * (s.q[4][ai][aj] + s.q[4][bi][bj]);
-      Tface = g * p_f / rho_f;
-      T mu_face = viscosity(P, Tface);
-      mut = eddy_viscosity(P.sa, rho_f, nuh_f * P.mu_inf, mu_face / rho_f);
-      mu = mu + mut;
-      k = k + mut / (PR_TURB * (g - 1.0));
-      if (P.c_cr1 != 0.0) {
-        extra = true;
-        T square = ((g00 * g00 + g01 * g01) + g10 * g10) + g11 * g11;
-        bool pos = val(square) > 0.0;
-        T nrm = pos ? dsqrt(square) : cst<T>(1.0);
-        T r01 = (g01 - g10) / nrm, r10 = (g10 - g01) / nrm;
-        T r00 = (g00 - g00) / nrm, r11 = (g11 - g11) / nrm;
-        T div = g00 + g11;
-        T t00 = mut * (g00 + g00 - (2.0 / 3.0) * div * 1.0);
-        T t01 = mut * (g01 + g10 - (2.0 / 3.0) * div * 0.0);
-        T t10 = mut * (g10 + g01 - (2.0 / 3.0) * div * 0.0);
-        T t11 = mut * (g11 + g11 - (2.0 / 3.0) * div * 1.0);
-        T p00 = r00 * t00 + r01 * t01, p01 = r00 * t10 + r01 * t11;
-        T p10 = r10 * t00 + r11 * t01, p11 = r10 * t10 + r11 * t11;
-        ex00 = -P.c_cr1 * (p00 + p00);
-        ex01 = -P.c_cr1 * (p01 + p10);
-        ex10 = -P.c_cr1 * (p10 + p01);
-        ex11 = -P.c_cr1 * (p11 + p11);
-      }
-    }
-    T div = g00 + g11;
-    T ttd = (2.0 / 3.0) * div;
-    T t00 = mu * (2.0 * g00 - ttd), t11 = mu * (2.0 * g11 - ttd), t01 = mu * (g01 + g10);
-    T t10 = t01;
-    if (extra) {
-      t00 = t00 + ex00;
-      t01 = t01 + ex01;
-      t10 = t10 + ex10;
-      t11 = t11 + ex11;
-    }
-    T fx = t00 * sx + t01 * sy;
-    T fy = t10 * sx + t11 * sy;
-    T energy = (vel0 * fx + vel1 * fy) + k * (gx[2] * sx + gy[2] * sy);
-    F[1] = F[1] - fx;
-    F[2] = F[2] - fy;
-    F[3] = F[3] - energy;
+    T x[ViscShape<VISC>::NX], out[ViscShape<VISC>::NR];
+    face_intermediates<T, VISC>(q, phi, cxv, cyv, axis, ai, aj, x);
+    viscous_tail<T, VISC>(P, x, sx, sy, out);
+    F[1] = F[1] - out[0];
+    F[2] = F[2] - out[1];
+    F[3] = F[3] - out[2];
     if constexpr (VISC == 2) {
       // SA face flux: upwind nu_hat on the inviscid mass flux, diffusion through the
       // face gradient (turbulence.py:129-135)
       T mass = Finv[0];
-      T up = val(mass) > 0.0 ? s.q[4][ai][aj] : s.q[4][bi][bj];
-      T mu_face = viscosity(P, Tface);
-      T coef = diffusion_coefficient(P.sa, rho_f, nuh_f * P.mu_inf, mu_face);
-      F[4] = mass * up - coef * (gx[3] * sx + gy[3] * sy);
+      T up = val(mass) > 0.0 ? s.q[4][ai][aj] : s.q[4][ai + di][aj + dj];
+      F[4] = mass * up - out[3];
     }
   }
 }
@@ -548,7 +606,7 @@ __global__ void __launch_bounds__(TILE_THREADS, TILE_MIN_BLOCKS)
           R[v] = (s.Fi[v][li + 1][lj] - s.Fi[v][li][lj]) + (s.Fj[v][li][lj + 1] - s.Fj[v][li][lj]);
         if constexpr (VISC == 2) {
           const int si = li + 2, sj = lj + 2;
-          const double g = P.gamma, vol = c.volume[idx];
+          const double vol = c.volume[idx];
           const int fl = i * NJ + j, fh = (i + 1) * NJ + j;
           const int gl = i * (NJ + 1) + j, gh = i * (NJ + 1) + j + 1;
           double sxl = c.fi[fl], syl = c.fi[c.nfi() + fl], sxh = c.fi[fh], syh = c.fi[c.nfi() + fh];
@@ -563,13 +621,8 @@ __global__ void __launch_bounds__(TILE_THREADS, TILE_MIN_BLOCKS)
             gg[0][v] = ((pih * sxh - pil * sxl) + (pjh * txh - pjl * txl)) / vol;
             gg[1][v] = ((pih * syh - pil * syl) + (pjh * tyh - pjl * tyl)) / vol;
           }
-          T omega = dabs(gg[0][1] - gg[1][0]);
-          T rho = s.q[0][si][sj];
-          T mu = viscosity(P, g * s.q[3][si][sj] / rho);
-          T Pr, D;
-          sa_source(P.sa, s.q[4][si][sj] * P.mu_inf, mu / rho, omega, c.distance[idx], Pr, D);
-          T src = rho * ((Pr - D) / P.mu_inf +
-                         P.sa.c_b2 / P.sa.sigma * P.mu_inf * (gg[0][2] * gg[0][2] + gg[1][2] * gg[1][2]));
+          const T y[7] = {s.q[0][si][sj], s.q[3][si][sj], s.q[4][si][sj], gg[0][1], gg[1][0], gg[0][2], gg[1][2]};
+          T src = sa_cell_source(P, y, c.distance[idx]);
           R[4] = R[4] - tangent_or_value(src) * vol;
         }
         if constexpr (sizeof(T) == sizeof(Dual)) {
@@ -603,6 +656,377 @@ __global__ void __launch_bounds__(TILE_THREADS, TILE_MIN_BLOCKS)
   }
 }
 
+// ------------------------------------------------------------------------------------
+// The linearised J.v.  One linearisation serves every J.v of a Newton step, as in the
+// reference, where jax.linearize evaluates the primal once and keeps what the tangent map
+// needs (src/jaxrans/solvers/implicit.py:102-108).  k_linearize runs once per step at U:
+// for every live face of the first-order residual it stores the face flux's derivatives
+// in factored form -- the inviscid flux with respect to the primitive states either side
+// (AL, AR: 4 x 4 each), the SA convection's upwind value and mass flux, the viscous
+// tail with respect to its intermediates -- and for every interior cell the SA source's
+// derivatives.  Each is one forward-mode (dual-number) evaluation per input direction of
+// the same physics code the residual runs.  k_jv applies them to a tangent: it stages
+// the tangents of (rho, u, v, p[, nu_hat], T) of the tile and its 1-cell halo, maps them
+// to the face intermediates' tangents by the (linear) face_intermediates, and sums
+// coefficient times tangent.  The tangent map is linear in the direction, so the result
+// is the dual-number J.v up to rounding order.
+// ------------------------------------------------------------------------------------
+
+template <int VISC> struct JacShape {
+  static constexpr int SA0 = 32;                      // SA convection: up, mass if A is upwind, mass if B is
+  static constexpr int VBASE = VISC == 2 ? 35 : 32;   // the viscous tail's [r][k] at VBASE + r * NX + k
+  static constexpr int NCOEF = VISC == 0 ? 32 : VBASE + ViscShape<VISC>::NR * ViscShape<VISC>::NX;
+};
+constexpr int JCELL = 7;   // the SA source's derivatives per interior cell
+
+int jac_coefficients(int visc) {
+  return visc == 2 ? JacShape<2>::NCOEF : (visc == 1 ? JacShape<1>::NCOEF : JacShape<0>::NCOEF);
+}
+int jac_cell_coefficients(int visc) { return visc == 2 ? JCELL : 0; }
+
+// Coefficients of one face at flat face index f (i-faces first, then j-faces); the face
+// lies between staged cells (ai, aj) and the next along `axis` of a double tile.
+template <int NV, int VISC>
+__device__ __forceinline__ void linearize_face(const Physics& P, TileSmem<double, NV>& s, int axis, int ai, int aj,
+                                               double sx, double sy, double* __restrict__ jac, size_t stride,
+                                               int f) {
+  using J = JacShape<VISC>;
+  const double g = P.gamma;
+  const int bi = ai + (axis == 0 ? 1 : 0), bj = aj + (axis == 0 ? 0 : 1);
+  double qa[4], qb[4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    qa[v] = s.q[v][ai][aj];
+    qb[v] = s.q[v][bi][bj];
+  }
+  double mass = 0.0;
+#pragma unroll 1
+  for (int seed = 0; seed < 8; ++seed) {
+    Dual qL[4], qR[4], F[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      qL[v] = Dual{qa[v], seed == v ? 1.0 : 0.0};
+      qR[v] = Dual{qb[v], seed == 4 + v ? 1.0 : 0.0};
+    }
+    riemann(P.flux, qL, qR, sx, sy, g, F);
+    const int base = seed < 4 ? seed : 12 + seed;   // AL[r][v] at r * 4 + v, AR[r][v] at 16 + r * 4 + v
+#pragma unroll
+    for (int r = 0; r < 4; ++r) jac[(size_t)(base + 4 * r) * stride + f] = F[r].d;
+    mass = F[0].v;
+  }
+  if constexpr (VISC == 2) {
+    const bool a_up = mass > 0.0;
+    jac[(size_t)J::SA0 * stride + f] = a_up ? s.q[4][ai][aj] : s.q[4][bi][bj];
+    jac[(size_t)(J::SA0 + 1) * stride + f] = a_up ? mass : 0.0;
+    jac[(size_t)(J::SA0 + 2) * stride + f] = a_up ? 0.0 : mass;
+  }
+  if constexpr (VISC > 0) {
+    constexpr int NX = ViscShape<VISC>::NX, NR = ViscShape<VISC>::NR;
+    auto q = [&](int v, int i, int j) -> double { return s.q[v][i][j]; };
+    auto phi = [&](int i, int j, int k) -> double {
+      if (k < 2) return s.q[1 + k][i][j];
+      if (k == 2) return g * s.q[3][i][j] / s.q[0][i][j];
+      return s.q[NV == 5 ? 4 : 0][i][j];
+    };
+    auto cxv = [&](int i, int j) { return s.cx[i - 1][j - 1]; };
+    auto cyv = [&](int i, int j) { return s.cy[i - 1][j - 1]; };
+    double x[NX];
+    face_intermediates<double, VISC>(q, phi, cxv, cyv, axis, ai, aj, x);
+#pragma unroll 1
+    for (int k = 0; k < NX; ++k) {
+      Dual xd[NX], out[NR];
+#pragma unroll
+      for (int m = 0; m < NX; ++m) xd[m] = Dual{x[m], m == k ? 1.0 : 0.0};
+      viscous_tail<Dual, VISC>(P, xd, sx, sy, out);
+#pragma unroll
+      for (int r = 0; r < NR; ++r) jac[(size_t)(J::VBASE + r * NX + k) * stride + f] = out[r].d;
+    }
+  }
+}
+
+template <int NV, int VISC>
+__global__ void __launch_bounds__(TILE_THREADS) k_linearize(const CaseDev* __restrict__ cases) {
+  __shared__ CaseDev scase;
+  if (idle_block(cases[blockIdx.z],
+                 (int)blockIdx.x >= cases[blockIdx.z].tiles_x || (int)blockIdx.y >= cases[blockIdx.z].tiles_y, 0))
+    return;
+  const CaseDev& cd = stage_case(cases, blockIdx.z, &scase);
+  if (!cd.enabled) return;
+  const Canvas& c = cd.c;
+  const Physics& P = cd.P;
+  const double* __restrict__ U = cd.U;
+  const double* __restrict__ qg = cd.qg;
+  double* __restrict__ jac = cd.jac;
+  const size_t stride = (size_t)cd.jstride;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TileSmem<double, NV>& s = *reinterpret_cast<TileSmem<double, NV>*>(smem_raw);
+  const int NI = c.NI, NJ = c.NJ, N = c.ncanvas();
+  const int i0 = blockIdx.y * TILE_I, j0 = blockIdx.x * TILE_J;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < HI * HJ; e += TILE_THREADS) {
+    int li = e / HJ, lj = e % HJ;
+    int i = i0 - 2 + li, j = j0 - 2 + lj;
+    double q[5];
+    if (i >= 0 && i < NI && j >= 0 && j < NJ) {
+      load_prim<double>(c, P, i * NJ + j, U, nullptr, qg, nullptr, q);
+    } else {
+      for (int v = 0; v < NV; ++v) q[v] = 1.0;
+    }
+    for (int v = 0; v < NV; ++v) s.q[v][li][lj] = q[v];
+  }
+  if constexpr (VISC > 0) {
+    const int CI = NI + 2, CJ = NJ + 2;
+    for (int e = tid; e < (TILE_I + 2) * (TILE_J + 2); e += TILE_THREADS) {
+      int li = e / (TILE_J + 2), lj = e % (TILE_J + 2);
+      int i = i0 - 1 + li, j = j0 - 1 + lj;
+      int ci = min(max(i + 1, 0), CI - 1), cj = min(max(j + 1, 0), CJ - 1);
+      s.cx[li][lj] = c.centres[ci * CJ + cj];
+      s.cy[li][lj] = c.centres[CI * CJ + ci * CJ + cj];
+    }
+  }
+  __syncthreads();
+  const int nfi = c.nfi();
+  for (int e = tid; e < (TILE_I + 1) * TILE_J; e += TILE_THREADS) {
+    int fi = e / TILE_J, fj = e % TILE_J;
+    int i = i0 + fi, j = j0 + fj;
+    if (j < NJ && (interior_at(c, i - 1, j) || interior_at(c, i, j))) {
+      int f = i * NJ + j;
+      linearize_face<NV, VISC>(P, s, 0, fi + 1, fj + 2, c.fi[f], c.fi[nfi + f], jac, stride, f);
+    }
+  }
+  for (int e = tid; e < TILE_I * (TILE_J + 1); e += TILE_THREADS) {
+    int fi = e / (TILE_J + 1), fj = e % (TILE_J + 1);
+    int i = i0 + fi, j = j0 + fj;
+    if (i < NI && (interior_at(c, i, j - 1) || interior_at(c, i, j))) {
+      int f = i * (NJ + 1) + j;
+      linearize_face<NV, VISC>(P, s, 1, fi + 2, fj + 1, c.fj[f], c.fj[c.nfj() + f], jac, stride, nfi + f);
+    }
+  }
+  if constexpr (VISC == 2) {
+    double* __restrict__ jcell = cd.jcell;
+    if (tid < TILE_I * TILE_J) {
+      int li = tid / TILE_J, lj = tid % TILE_J;
+      int i = i0 + li, j = j0 + lj;
+      if (i < NI && j < NJ && c.interior[i * NJ + j]) {
+        const int idx = i * NJ + j, si = li + 2, sj = lj + 2;
+        const double vol = c.volume[idx];
+        const int fl = i * NJ + j, fh = (i + 1) * NJ + j;
+        const int gl = i * (NJ + 1) + j, gh = i * (NJ + 1) + j + 1;
+        double sxl = c.fi[fl], syl = c.fi[nfi + fl], sxh = c.fi[fh], syh = c.fi[nfi + fh];
+        double txl = c.fj[gl], tyl = c.fj[c.nfj() + gl], txh = c.fj[gh], tyh = c.fj[c.nfj() + gh];
+        auto avg = [&](int v, int a, int b2, int cc, int dd) { return 0.5 * (s.q[v][a][b2] + s.q[v][cc][dd]); };
+        double gg[2][3];
+        for (int v = 0; v < 3; ++v) {
+          int row = v < 2 ? 1 + v : 4;
+          double pil = avg(row, si - 1, sj, si, sj), pih = avg(row, si, sj, si + 1, sj);
+          double pjl = avg(row, si, sj - 1, si, sj), pjh = avg(row, si, sj, si, sj + 1);
+          gg[0][v] = ((pih * sxh - pil * sxl) + (pjh * txh - pjl * txl)) / vol;
+          gg[1][v] = ((pih * syh - pil * syl) + (pjh * tyh - pjl * tyl)) / vol;
+        }
+        const double y[JCELL] = {s.q[0][si][sj], s.q[3][si][sj], s.q[NV == 5 ? 4 : 0][si][sj], gg[0][1], gg[1][0],
+                                 gg[0][2], gg[1][2]};
+        const double d = c.distance[idx];
+#pragma unroll 1
+        for (int k = 0; k < JCELL; ++k) {
+          Dual yd[JCELL];
+#pragma unroll
+          for (int m = 0; m < JCELL; ++m) yd[m] = Dual{y[m], m == k ? 1.0 : 0.0};
+          jcell[(size_t)k * N + idx] = sa_cell_source(P, yd, d).d;
+        }
+      }
+    }
+  }
+}
+
+// The tangent pass: tangents of the tile and a 1-cell halo, face tangent fluxes from the
+// stored coefficients, per-cell sums.
+constexpr int JHI = TILE_I + 2, JHJ = TILE_J + 2;
+
+template <int NV> struct JvSmem {
+  double dq[NV + 1][JHI][JHJ];   // tangents of (rho, u, v, p[, nu_hat]) and of T = gamma p / rho
+  double cx[JHI][JHJ], cy[JHI][JHJ];
+  double Fi[NV][TILE_I + 1][TILE_J];
+  double Fj[NV][TILE_I][TILE_J + 1];
+};
+
+template <int NV, int VISC>
+__device__ __forceinline__ void jv_face(const JvSmem<NV>& s, int axis, int ai, int aj,
+                                        const double* __restrict__ jf, size_t stride, double* dF) {
+  using J = JacShape<VISC>;
+  const int bi = ai + (axis == 0 ? 1 : 0), bj = aj + (axis == 0 ? 0 : 1);
+  double a[4], b[4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    a[v] = s.dq[v][ai][aj];
+    b[v] = s.dq[v][bi][bj];
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    double acc = 0.0;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) acc += jf[(size_t)(4 * r + v) * stride] * a[v];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) acc += jf[(size_t)(16 + 4 * r + v) * stride] * b[v];
+    dF[r] = acc;
+  }
+  if constexpr (VISC == 2) {
+    dF[NV - 1] = (jf[(size_t)J::SA0 * stride] * dF[0] + jf[(size_t)(J::SA0 + 1) * stride] * s.dq[NV - 1][ai][aj]) +
+                 jf[(size_t)(J::SA0 + 2) * stride] * s.dq[NV - 1][bi][bj];
+  }
+  if constexpr (VISC > 0) {
+    constexpr int NX = ViscShape<VISC>::NX, NR = ViscShape<VISC>::NR;
+    auto q = [&](int v, int i, int j) -> double { return s.dq[v][i][j]; };
+    auto phi = [&](int i, int j, int k) -> double {
+      if (k < 2) return s.dq[1 + k][i][j];
+      if (k == 2) return s.dq[NV][i][j];
+      return s.dq[NV - 1][i][j];
+    };
+    auto cxv = [&](int i, int j) { return s.cx[i][j]; };
+    auto cyv = [&](int i, int j) { return s.cy[i][j]; };
+    double x[NX];
+    face_intermediates<double, VISC>(q, phi, cxv, cyv, axis, ai, aj, x);
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      double acc = 0.0;
+#pragma unroll
+      for (int k = 0; k < NX; ++k) acc += jf[(size_t)(J::VBASE + r * NX + k) * stride] * x[k];
+      dF[r < 3 ? 1 + r : NV - 1] -= acc;
+    }
+  }
+}
+
+// out = vdt * v + dR1/dU . v with v = buffer `tangent_id` (vdt_id < 0: the bare J.v),
+// from the case's linearisation; own_ghosts: the tile evaluates its halo's tangent
+// ghosts (no tangent ghost fill needed)
+template <int NV, int VISC>
+__global__ void __launch_bounds__(TILE_THREADS) k_jv(const CaseDev* __restrict__ cases, int out_id, int tangent_id,
+                                                     int vdt_id, int check_active, int own_ghosts) {
+  __shared__ CaseDev scase;
+  if (idle_block(cases[blockIdx.z],
+                 (int)blockIdx.x >= cases[blockIdx.z].tiles_x || (int)blockIdx.y >= cases[blockIdx.z].tiles_y,
+                 check_active))
+    return;
+  const CaseDev& cd = stage_case(cases, blockIdx.z, &scase);
+  if (!cd.enabled || (check_active && cd.sc->active == 0)) return;
+  const Canvas& c = cd.c;
+  const Physics& P = cd.P;
+  const double* __restrict__ U = cd.U;
+  const double* __restrict__ qg = cd.qg;
+  const double* __restrict__ V = buf(cd, tangent_id);
+  const double* __restrict__ dqg = cd.dqg;
+  const double* __restrict__ vdt = vdt_id >= 0 ? buf(cd, vdt_id) : nullptr;
+  const double* __restrict__ jac = cd.jac;
+  const size_t stride = (size_t)cd.jstride;
+  double* __restrict__ out = buf(cd, out_id);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  JvSmem<NV>& s = *reinterpret_cast<JvSmem<NV>*>(smem_raw);
+  const int NI = c.NI, NJ = c.NJ, N = c.ncanvas();
+  const int i0 = blockIdx.y * TILE_I, j0 = blockIdx.x * TILE_J;
+  const int tid = threadIdx.x;
+  // 1. the tangents of the tile and its halo
+  for (int e = tid; e < JHI * JHJ; e += TILE_THREADS) {
+    int li = e / JHJ, lj = e % JHJ;
+    int i = i0 - 1 + li, j = j0 - 1 + lj;
+    double t[NV + 1];
+    if (i >= 0 && i < NI && j >= 0 && j < NJ) {
+      const int idx = i * NJ + j;
+      Dual q[5];
+      const int rec = own_ghosts && !c.interior[idx] ? c.ghost_rec[idx] : -1;
+      if (rec >= 0) ghost_tangent(c, P, rec, U, V, qg, dqg, q);
+      else load_prim<Dual>(c, P, idx, U, V, qg, dqg, q);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) t[v] = q[v].d;
+      t[NV] = (P.gamma * q[3] / q[0]).d;
+    } else {
+#pragma unroll
+      for (int v = 0; v <= NV; ++v) t[v] = 0.0;
+    }
+#pragma unroll
+    for (int v = 0; v <= NV; ++v) s.dq[v][li][lj] = t[v];
+  }
+  if constexpr (VISC > 0) {
+    const int CI = NI + 2, CJ = NJ + 2;
+    for (int e = tid; e < JHI * JHJ; e += TILE_THREADS) {
+      int li = e / JHJ, lj = e % JHJ;
+      int i = i0 - 1 + li, j = j0 - 1 + lj;
+      int ci = min(max(i + 1, 0), CI - 1), cj = min(max(j + 1, 0), CJ - 1);
+      s.cx[li][lj] = c.centres[ci * CJ + cj];
+      s.cy[li][lj] = c.centres[CI * CJ + ci * CJ + cj];
+    }
+  }
+  __syncthreads();
+  const int nfi = c.nfi();
+  // 2. i-faces: face (i, j) lies between canvas cells (i-1, j) and (i, j)
+  for (int e = tid; e < (TILE_I + 1) * TILE_J; e += TILE_THREADS) {
+    int fi = e / TILE_J, fj = e % TILE_J;
+    int i = i0 + fi, j = j0 + fj;
+    double dF[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) dF[v] = 0.0;
+    if (j < NJ && (interior_at(c, i - 1, j) || interior_at(c, i, j)))
+      jv_face<NV, VISC>(s, 0, fi, fj + 1, jac + i * NJ + j, stride, dF);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) s.Fi[v][fi][fj] = dF[v];
+  }
+  // 3. j-faces: face (i, j) lies between (i, j-1) and (i, j)
+  for (int e = tid; e < TILE_I * (TILE_J + 1); e += TILE_THREADS) {
+    int fi = e / (TILE_J + 1), fj = e % (TILE_J + 1);
+    int i = i0 + fi, j = j0 + fj;
+    double dF[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) dF[v] = 0.0;
+    if (i < NI && (interior_at(c, i, j - 1) || interior_at(c, i, j)))
+      jv_face<NV, VISC>(s, 1, fi + 1, fj, jac + nfi + i * (NJ + 1) + j, stride, dF);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) s.Fj[v][fi][fj] = dF[v];
+  }
+  __syncthreads();
+  // 4. cells: the net tangent flux, the SA source's tangent, the output
+  if (tid < TILE_I * TILE_J) {
+    int li = tid / TILE_J, lj = tid % TILE_J;
+    int i = i0 + li, j = j0 + lj;
+    if (i < NI && j < NJ) {
+      const int idx = i * NJ + j;
+      const double w = vdt != nullptr ? vdt[idx] : 0.0;
+      if (c.interior[idx]) {
+        double R[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+          R[v] = (s.Fi[v][li + 1][lj] - s.Fi[v][li][lj]) + (s.Fj[v][li][lj + 1] - s.Fj[v][li][lj]);
+        if constexpr (VISC == 2) {
+          const int si = li + 1, sj = lj + 1;
+          const double vol = c.volume[idx];
+          const int fl = i * NJ + j, fh = (i + 1) * NJ + j;
+          const int gl = i * (NJ + 1) + j, gh = i * (NJ + 1) + j + 1;
+          double sxl = c.fi[fl], syl = c.fi[nfi + fl], sxh = c.fi[fh], syh = c.fi[nfi + fh];
+          double txl = c.fj[gl], tyl = c.fj[c.nfj() + gl], txh = c.fj[gh], tyh = c.fj[c.nfj() + gh];
+          auto avg = [&](int v, int a, int b2, int cc, int dd) { return 0.5 * (s.dq[v][a][b2] + s.dq[v][cc][dd]); };
+          double gg[2][3];
+#pragma unroll
+          for (int v = 0; v < 3; ++v) {
+            int row = v < 2 ? 1 + v : NV - 1;
+            double pil = avg(row, si - 1, sj, si, sj), pih = avg(row, si, sj, si + 1, sj);
+            double pjl = avg(row, si, sj - 1, si, sj), pjh = avg(row, si, sj, si, sj + 1);
+            gg[0][v] = ((pih * sxh - pil * sxl) + (pjh * txh - pjl * txl)) / vol;
+            gg[1][v] = ((pih * syh - pil * syl) + (pjh * tyh - pjl * tyl)) / vol;
+          }
+          const double y[JCELL] = {s.dq[0][si][sj], s.dq[3][si][sj], s.dq[NV - 1][si][sj], gg[0][1], gg[1][0],
+                                   gg[0][2], gg[1][2]};
+          const double* __restrict__ jcell = cd.jcell;
+          double src = 0.0;
+#pragma unroll
+          for (int k = 0; k < JCELL; ++k) src += jcell[(size_t)k * N + idx] * y[k];
+          R[NV - 1] = R[NV - 1] - src * vol;
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) out[v * N + idx] = w * V[v * N + idx] + R[v];
+      } else {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) out[v * N + idx] = w * V[v * N + idx] + V[v * N + idx];
+      }
+    }
+  }
+}
 // ------------------------------------------------------------------------------------
 // Wave speeds and the per-face terms of the preconditioner (residual.py:169-203,
 // preconditioners.py:557-563): lambda from face-averaged states (a block face's
@@ -753,10 +1177,6 @@ __global__ void k_cells(const CaseDev* __restrict__ cases) {
 // Launch wrappers
 // ------------------------------------------------------------------------------------
 
-size_t tile_smem(bool dual, int nv) {
-  if (dual) return nv == 5 ? sizeof(TileSmem<Dual, 5>) : sizeof(TileSmem<Dual, 4>);
-  return nv == 5 ? sizeof(TileSmem<double, 5>) : sizeof(TileSmem<double, 4>);
-}
 
 dim3 tile_grid(const Canvas& c) { return dim3((c.NJ + TILE_J - 1) / TILE_J, (c.NI + TILE_I - 1) / TILE_I); }
 
@@ -775,9 +1195,12 @@ void configure_kernels() {
   configure_one<double, 4, false, 1>();
   configure_one<double, 4, true, 0>();
   configure_one<double, 4, false, 0>();
-  configure_one<Dual, 5, false, 2>();
-  configure_one<Dual, 4, false, 1>();
-  configure_one<Dual, 4, false, 0>();
+  cudaFuncSetAttribute(k_linearize<5, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem<double, 5>));
+  cudaFuncSetAttribute(k_linearize<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem<double, 4>));
+  cudaFuncSetAttribute(k_linearize<4, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem<double, 4>));
+  cudaFuncSetAttribute(k_jv<5, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(JvSmem<5>));
+  cudaFuncSetAttribute(k_jv<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(JvSmem<4>));
+  cudaFuncSetAttribute(k_jv<4, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(JvSmem<4>));
   done = true;
 }
 
@@ -805,16 +1228,29 @@ void launch_residual(const CaseDev* cases, const BatchDims& d, int visc, bool se
   }
 }
 
-// out = vdt * v + dR1/dU . v with v = buffer `tangent_id` (vdt_id < 0: the bare J.v);
-// own_ghosts: the tile evaluates its halo's tangent ghosts (no tangent ghost fill needed)
+// The linearisation of every case's first-order residual at its U (ghosts of U filled)
+void launch_linearize(const CaseDev* cases, const BatchDims& d, int visc, cudaStream_t st) {
+  dim3 grid(d.tiles_x, d.tiles_y, d.n_cases);
+  if (visc == 2) k_linearize<5, 2><<<grid, TILE_THREADS, sizeof(TileSmem<double, 5>), st>>>(cases);
+  else if (visc == 1) k_linearize<4, 1><<<grid, TILE_THREADS, sizeof(TileSmem<double, 4>), st>>>(cases);
+  else k_linearize<4, 0><<<grid, TILE_THREADS, sizeof(TileSmem<double, 4>), st>>>(cases);
+}
+
+// out = vdt * v + dR1/dU . v with v = buffer `tangent_id` (vdt_id < 0: the bare J.v), from
+// the linearisation launch_linearize stored; own_ghosts: the tile evaluates its halo's
+// tangent ghosts (no tangent ghost fill needed)
 void launch_jvp(const CaseDev* cases, const BatchDims& d, int visc, int tangent_id, int vdt_id, int out_id,
                 int check_active, int own_ghosts, cudaStream_t st) {
+  dim3 grid(d.tiles_x, d.tiles_y, d.n_cases);
   if (visc == 2)
-    launch_tile<Dual, 5, false, 2>(cases, d, out_id, tangent_id, vdt_id, 0, check_active, st, own_ghosts);
+    k_jv<5, 2><<<grid, TILE_THREADS, sizeof(JvSmem<5>), st>>>(cases, out_id, tangent_id, vdt_id, check_active,
+                                                              own_ghosts);
   else if (visc == 1)
-    launch_tile<Dual, 4, false, 1>(cases, d, out_id, tangent_id, vdt_id, 0, check_active, st, own_ghosts);
+    k_jv<4, 1><<<grid, TILE_THREADS, sizeof(JvSmem<4>), st>>>(cases, out_id, tangent_id, vdt_id, check_active,
+                                                              own_ghosts);
   else
-    launch_tile<Dual, 4, false, 0>(cases, d, out_id, tangent_id, vdt_id, 0, check_active, st, own_ghosts);
+    k_jv<4, 0><<<grid, TILE_THREADS, sizeof(JvSmem<4>), st>>>(cases, out_id, tangent_id, vdt_id, check_active,
+                                                              own_ghosts);
 }
 
 // the ghosts of U (tangent_id < 0) or of the tangent in buffer `tangent_id`

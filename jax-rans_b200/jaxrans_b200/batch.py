@@ -23,7 +23,8 @@ import numpy as np
 
 from .case import Case
 from .plan import Plan
-from .solver import CaseMonitor, ConvergenceHistory, Result, Timing, forces_of, freestream_state
+from .solver import (CaseMonitor, ConvergenceHistory, Result, Timing, device_monitored, forces_of,
+                     freestream_state)
 
 
 def batch_device(cases: list[Case], grids: list[Plan], autotune: bool = True):
@@ -50,10 +51,22 @@ def start_batch(dev, cases: list[Case], grids: list[Plan], initial=None) -> None
         dev.enable(k, True)
 
 
-def run_batch_blocks(cases: list[Case], dev, max_iters=None, progress=None, release: bool = True):
+def run_batch_blocks(cases: list[Case], dev, max_iters=None, progress=None, release: bool = True,
+                     monitor: str = "device"):
     """Blocks of Newton steps of every case of the device batch until each has stopped by
-    the exit test of a single run.  Returns the monitors (with each case's exit time in
-    ``seconds``), the seconds and the first block's seconds."""
+    the exit test of a single run, run on the device (``monitor="device"``: one host
+    synchronisation every few blocks, each case leaving the launches at its own exit) or
+    on the host after every block (``"host"``).  Returns the monitors (with each case's
+    exit time in ``seconds`` and its forces at the end), the seconds and the first block's
+    seconds."""
+    if monitor == "device":
+        monitors, seconds, first_block = device_monitored(cases, dev, max_iters, release=release)
+        forces = np.atleast_2d(dev.forces())
+        for k, m in enumerate(monitors):
+            m.forces = forces_of(forces[k])
+        if progress is not None:
+            progress(max(m.iterations for m in monitors), np.array([m.cl_history[-1] for m in monitors]))
+        return monitors, seconds, first_block
     block_iters = {c.block_iters for c in cases}
     if len(block_iters) != 1:
         raise ValueError("the cases of a batch must share convergence.block_iters")
@@ -81,9 +94,10 @@ def run_batch_blocks(cases: list[Case], dev, max_iters=None, progress=None, rele
 
 
 def run_batch(cases: list[Case], grids: list[Plan] | None = None, progress=None, release: bool = True,
-              initial=None, device=None) -> list[Result]:
+              initial=None, device=None, monitor: str = "device") -> list[Result]:
     """Each case of ``cases`` to steady state, all advanced together on one GPU; one
-    ``Result`` per case, as ``run`` gives it alone."""
+    ``Result`` per case, as ``run`` gives it alone (``monitor``: where the exit tests run,
+    as in ``run_batch_blocks``)."""
     if not cases:
         return []
     if grids is None:
@@ -96,7 +110,8 @@ def run_batch(cases: list[Case], grids: list[Plan] | None = None, progress=None,
             grids.append(made[key])
     dev = device if device is not None else batch_device(cases, grids)
     start_batch(dev, cases, grids, initial)
-    monitors, seconds, first_block = run_batch_blocks(cases, dev, progress=progress, release=release)
+    monitors, seconds, first_block = run_batch_blocks(cases, dev, progress=progress, release=release,
+                                                      monitor=monitor)
     iterations = max(m.iterations for m in monitors)
     cells = sum(g.cells for g in grids)
     timing = Timing(seconds, first_block, iterations, cases[0].block_iters, cells, cases=len(cases))

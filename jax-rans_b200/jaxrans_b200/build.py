@@ -50,5 +50,38 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     return LIB
 
 
+FFI_SOURCE = CSRC / "ffi" / "jr_ffi.cc"
+FFI_LIB = PKG / "lib" / "libjaxrans_b200_ffi.so"
+
+
+def ffi_include_dir() -> str | None:
+    """JAX's XLA FFI header directory, or None where JAX is not installed."""
+    try:
+        import jax.ffi
+    except ImportError:
+        return None
+    return jax.ffi.include_dir()
+
+
+def build_ffi(force: bool = False) -> Path | None:
+    """Compile the jax.ffi handlers (``csrc/ffi/jr_ffi.cc``) against JAX's FFI headers,
+    linked to the library.  Returns None, building nothing, where JAX is absent."""
+    include = ffi_include_dir()
+    if include is None:
+        return None
+    lib = build()
+    if not force and FFI_LIB.is_file() and FFI_LIB.stat().st_mtime > max(FFI_SOURCE.stat().st_mtime,
+                                                                         lib.stat().st_mtime):
+        return FFI_LIB
+    cuda = Path(nvcc()).resolve().parents[1]
+    cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", f"-I{include}", f"-I{INCLUDE}", f"-I{cuda / 'include'}",
+           str(FFI_SOURCE), f"-L{lib.parent}", "-ljaxrans_b200", f"-Wl,-rpath,{lib.parent}", f"-L{cuda / 'lib64'}",
+           "-lcudart", "-o", str(FFI_LIB)]
+    subprocess.run(cmd, check=True)
+    return FFI_LIB
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
+    if "--ffi" in sys.argv:
+        print(build_ffi(force="--force" in sys.argv) or "JAX is not installed: the jax.ffi handlers are not built")

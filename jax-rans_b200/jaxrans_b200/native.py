@@ -65,9 +65,10 @@ EXPORTS = ("jr_plan_create", "jr_plan_destroy", "jr_last_error", "jr_plan_sizes"
            "jr_launch_count", "jr_autotune", "jr_line_schedule", "jr_wait_limit_check", "jr_wall_loads",
            "jr_plan3d_create", "jr_plan3d_destroy", "jr_residual3d", "jr_jvp3d", "jr_wave_speeds3d",
            "jr_precondition3d", "jr_newton_steps3d", "jr_forces3d", "jr_wall_distance3d",
-           "jr_launches3d", "jr_wall_loads3d")
+           "jr_launches3d", "jr_wall_loads3d", "jr_monitor_set", "jr_monitor_blocks", "jr_monitor_get")
 
-TIMED_KERNELS = ("residual_tile", "jvp_tile", "ghosts_tangent", "line_apply", "line_factor", "cgs2_full_basis")
+TIMED_KERNELS = ("residual_tile", "jvp_tile", "ghosts_tangent", "line_apply", "line_factor", "cgs2_full_basis",
+                 "linearize")
 
 _LIB = None
 
@@ -148,6 +149,9 @@ def load_library(path: Path | None = None) -> C.CDLL:
         "jr_case_load": (C.c_int, [vp, C.c_int32, C.POINTER(PlanDesc)]),
         "jr_case_state_set": (C.c_int, [vp, C.c_int32, vp, C.c_double, C.c_double]),
         "jr_case_state_get": (C.c_int, [vp, C.c_int32, vp, _f64p, _f64p, _i32p]),
+        "jr_monitor_set": (C.c_int, [vp, C.c_int32, C.c_double, C.c_double, C.c_int32, C.c_int32]),
+        "jr_monitor_blocks": (C.c_int, [vp, C.c_int32, C.c_int32, vp]),
+        "jr_monitor_get": (C.c_int, [vp, C.c_int32, _i32p, _i32p, _f64p, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -443,6 +447,33 @@ class DevicePlan:
         hist = np.empty(n if self.n_cases == 1 else (n, self.n_cases))
         _check(self.lib, self.lib.jr_newton_steps(self.handle, int(n), hist.ctypes.data), "jr_newton_steps")
         return hist
+
+    # the exit test on the device (jr_monitor_*): reasons by code
+    MONITOR_REASONS = ("running", "converged", "settled", "max_iters", "non_finite", "stalled")
+    MONITOR_BLOCKS = 1024
+
+    def monitor_set(self, k: int, tol: float, forces_tol, max_blocks: int, release: bool = True) -> None:
+        """Case k's exit test on the device (``jr_monitor_set``); enables the case."""
+        ft = -1.0 if forces_tol is None else float(forces_tol)
+        _check(self.lib, self.lib.jr_monitor_set(self.handle, int(k), float(tol), ft, int(max_blocks),
+                                                 int(bool(release))), "jr_monitor_set")
+
+    def monitor_blocks(self, n_blocks: int, block_iters: int) -> np.ndarray:
+        """n_blocks blocks of Newton steps with the exit tests on the device; |R| before
+        each step, ``(n_blocks * block_iters, n_cases)``."""
+        hist = np.empty((n_blocks * block_iters, self.n_cases))
+        _check(self.lib, self.lib.jr_monitor_blocks(self.handle, int(n_blocks), int(block_iters), hist.ctypes.data),
+               "jr_monitor_blocks")
+        return hist
+
+    def monitor_get(self, k: int):
+        """Case k's monitor: ``(reason, blocks, peak, coefficients (blocks, 3))``."""
+        reason, blocks, peak = C.c_int32(), C.c_int32(), C.c_double()
+        coef = np.empty((self.MONITOR_BLOCKS, 3))
+        _check(self.lib, self.lib.jr_monitor_get(self.handle, int(k), C.byref(reason), C.byref(blocks),
+                                                 C.byref(peak), coef.ctypes.data), "jr_monitor_get")
+        n = min(int(blocks.value), self.MONITOR_BLOCKS)
+        return self.MONITOR_REASONS[reason.value], int(blocks.value), peak.value, coef[:n].copy()
 
     def newton_steps_async(self, n: int, history_device=None) -> None:
         ptr = None if history_device is None else history_device.data_ptr()

@@ -253,11 +253,75 @@ class CaseMonitor:
         return np.concatenate(self.blocks) if self.blocks else np.zeros(0)
 
 
-def run_blocks(case: Case, dev, max_iters=None, progress=None) -> Blocks:
-    """Blocks of ``block_iters`` Newton steps from the device's current state until the
-    exit test of ``src/jaxrans/solvers/driver.py:123-201`` stops the case."""
-    mon = CaseMonitor(case, max_iters)
+_DEVICE_REASONS = {"converged": ExitReason.CONVERGED, "settled": ExitReason.SETTLED,
+                   "max_iters": ExitReason.MAX_ITERS, "non_finite": ExitReason.NON_FINITE,
+                   "stalled": ExitReason.STALLED, "running": ExitReason.MAX_ITERS}
+
+
+def device_monitored(cases, dev, max_iters=None, chunk: int = 4, release: bool = True, on_block=None):
+    """Blocks of Newton steps of every case of ``dev`` with each case's exit test run on
+    the device after every block (``jr_monitor_blocks``): the host synchronises once per
+    ``chunk`` blocks instead of once per block, and a case that stops mid-chunk leaves the
+    launches already queued.  The decisions are the host monitor's (``CaseMonitor``), made
+    on the device with the same arithmetic; the returned monitors hold what the host
+    monitor would -- each case's blocks of |R|, its force samples (CL, CD, CM), its peak
+    and reason -- with ``forces`` left for the caller to read at the end (a stopped case's
+    state, and so its forces, stay as they were at its exit).  ``on_block(k, monitor)``
+    runs for every new block of case k, after its chunk."""
+    block_iters = {c.block_iters for c in cases}
+    if len(block_iters) != 1:
+        raise ValueError("the cases of a batch must share convergence.block_iters")
+    block_iters = block_iters.pop()
+    monitors = [CaseMonitor(c, max_iters) for c in cases]
+    if any(m.n_blocks > dev.MONITOR_BLOCKS for m in monitors):
+        raise ValueError(f"the device monitor holds at most {dev.MONITOR_BLOCKS} blocks")
+    for k, (c, m) in enumerate(zip(cases, monitors)):
+        dev.monitor_set(k, c.numerics.tol, c.numerics.forces_tol, m.n_blocks, release)
     started = time.perf_counter()
+    first_block = float("nan")
+    while not all(m.done for m in monitors):
+        left = max(m.n_blocks - len(m.blocks) for m in monitors if not m.done)
+        n = max(1, min(chunk, left, 4096 // block_iters))
+        hist = dev.monitor_blocks(n, block_iters)
+        if np.isnan(first_block):
+            first_block = time.perf_counter() - started
+        for k, m in enumerate(monitors):
+            if m.done:
+                continue
+            reason, blocks, peak, coef = dev.monitor_get(k)
+            for b in range(blocks - len(m.blocks)):
+                m.blocks.append(hist[b * block_iters:(b + 1) * block_iters, k].copy())
+                cl, cd, cm = (float(x) for x in coef[len(m.blocks) - 1])
+                m.cl_history.append(cl)
+                m.coefficients.append((cl, cd, cm))
+                if on_block is not None:
+                    on_block(k, m)
+            m.peak = peak
+            if reason != "running":
+                m.reason = _DEVICE_REASONS[reason]
+                m.seconds = time.perf_counter() - started
+                if reason == "max_iters":
+                    m.blocks = m.blocks[:m.n_blocks]
+    return monitors, time.perf_counter() - started, first_block
+
+
+def run_blocks(case: Case, dev, max_iters=None, progress=None, monitor: str = "device") -> Blocks:
+    """Blocks of ``block_iters`` Newton steps from the device's current state until the
+    exit test of ``src/jaxrans/solvers/driver.py:123-201`` stops the case: run on the
+    device (``monitor="device"``, a host synchronisation every few blocks), or on the host
+    after every block (``"host"``, the reference's own rhythm).  Both stop on the same
+    block with the same history."""
+    started = time.perf_counter()
+    if monitor == "device":
+        def report(_, m):
+            if progress is not None:
+                progress(m.iterations, float(m.blocks[-1][-1]), m.orders(),
+                         Forces(*m.coefficients[-1], float("nan"), float("nan")))
+        (mon,), seconds, first_block = device_monitored([case], dev, max_iters, on_block=report)
+        mon.forces = forces_of(dev.forces())
+        return Blocks(mon.residual(), mon.reason, np.asarray(mon.cl_history), np.asarray(mon.coefficients),
+                      mon.forces, seconds, first_block, len(mon.blocks))
+    mon = CaseMonitor(case, max_iters)
     first_block = float("nan")
     while not mon.done:
         hist = dev.newton_steps(mon.block_iters)
@@ -270,14 +334,15 @@ def run_blocks(case: Case, dev, max_iters=None, progress=None) -> Blocks:
                   mon.forces, time.perf_counter() - started, first_block, len(mon.blocks))
 
 
-def march(case: Case, plan: Plan, progress=None, initial=None, device=None, max_iters=None) -> Result:
+def march(case: Case, plan: Plan, progress=None, initial=None, device=None, max_iters=None,
+          monitor: str = "device") -> Result:
     """One grid to steady state from the freestream, or from ``initial`` on the block cells."""
     dev = device if device is not None else device_for(case, plan)
     U0 = freestream_state(case, plan)
     if initial is not None:
         U0 = np.where(plan.interior, np.asarray(initial), U0)
     dev.set_state(U0, case.implicit.cfl, float("inf"))
-    blk = run_blocks(case, dev, max_iters, progress)
+    blk = run_blocks(case, dev, max_iters, progress, monitor)
     U, _, _, _ = dev.get_state()
     history = ConvergenceHistory(blk.residual, blk.reason, int(blk.residual.size), blk.seconds, blk.first_block)
     return Result(case=case, grid=plan, U=U, forces=forces_of(dev.forces()), history=history,

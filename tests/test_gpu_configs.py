@@ -1,0 +1,94 @@
+"""Device parity on the benchmark workloads' own grids, through the C ABI, against the
+reference's outputs on those grids (tests/golden/make_golden_configs.py):
+
+* ``o_euler_257``: 2D Euler, NACA 0012, O-grid 257 x 65 nodes, far field at 50 chords,
+  HLLC with van Albada;
+* ``c_sa_385``: SA-noft2, NACA 4412, C-grid 385 x 97 nodes (192-cell wake chains), Roe
+  with minmod;
+* ``c_sa_513``: the uneven 513 x 129 SA C-grid of the batched polar (256-cell chains,
+  many waves of residual tiles).
+
+Tolerances as in test_gpu_parity.py: R 1e-12 relative to each row's largest entry, J.v
+1e-12 on the mean-flow rows and 1e-10 on the SA row, wave speeds 1e-13, the line solve
+1e-10, forces 1e-12."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from goldens import config_state, config_vector, load, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def row_rel(a, b):
+    return max(float(np.abs(a[v] - b[v]).max() / max(np.abs(b[v]).max(), 1e-300)) for v in range(b.shape[0]))
+
+
+@pytest.fixture(scope="module")
+def configs():
+    """One device plan per workload grid, made on first use and kept for the module."""
+    from jaxrans_b200.native import DevicePlan
+    made = {}
+
+    def get(name):
+        if name not in made:
+            z, case, plan = load(name)
+            made[name] = (z, case, plan, DevicePlan(plan, case.flow, case.numerics, case.implicit))
+        return made[name]
+
+    yield get
+    for *_, dev in made.values():
+        dev.close()
+
+
+@pytest.mark.parametrize("name,state", [("o_euler_257", "sin"), ("o_euler_257", "rand0"), ("c_sa_385", "sin"),
+                                        ("c_sa_385", "rand0"), ("c_sa_513", "sin")])
+def test_residual_on_config_grids(cuda, configs, name, state):
+    z, case, plan, dev = configs(name)
+    U = config_state(z, plan, state)
+    assert row_rel(dev.residual(U), z[f"{state}_R2"]) < 1e-12
+    if f"{state}_R1" in z:
+        assert row_rel(dev.residual(U, first_order=True), z[f"{state}_R1"]) < 1e-12
+
+
+@pytest.mark.parametrize("name,state", [("o_euler_257", "sin"), ("o_euler_257", "rand0"), ("c_sa_385", "sin"),
+                                        ("c_sa_385", "rand0")])
+def test_jvp_on_config_grids(cuda, configs, name, state):
+    z, case, plan, dev = configs(name)
+    U = config_state(z, plan, state)
+    ref = z[f"{state}_Jv"]
+    Jv = dev.jvp(U, config_vector(plan, state, "v", ref.shape[0]))
+    assert row_rel(Jv[:4], ref[:4]) < 1e-12
+    if ref.shape[0] > 4:
+        assert row_rel(Jv[4:], ref[4:]) < 1e-10
+
+
+@pytest.mark.parametrize("name", ["o_euler_257", "c_sa_385"])
+def test_wave_speeds_on_config_grids(cuda, configs, name):
+    z, case, plan, dev = configs(name)
+    li, lj = dev.wave_speeds(config_state(z, plan, "sin"))
+    live_i = np.zeros(li.shape, bool)
+    live_i[:-1] |= plan.interior
+    live_i[1:] |= plan.interior
+    live_j = np.zeros(lj.shape, bool)
+    live_j[:, :-1] |= plan.interior
+    live_j[:, 1:] |= plan.interior
+    assert rel(li[live_i], z["sin_lam_i"][live_i]) < 1e-13
+    assert rel(lj[live_j], z["sin_lam_j"][live_j]) < 1e-13
+
+
+@pytest.mark.parametrize("name", ["o_euler_257", "c_sa_385", "c_sa_513"])
+def test_line_solve_on_config_grids(cuda, configs, name):
+    z, case, plan, dev = configs(name)
+    ref = z["sin_prec_z"]
+    out = dev.precondition(config_state(z, plan, "sin"), 25.0, config_vector(plan, "sin", "r", ref.shape[0]))
+    assert rel(out, ref) < 1e-10
+
+
+@pytest.mark.parametrize("name,state", [("o_euler_257", "sin"), ("c_sa_385", "sin"), ("c_sa_385", "rand0")])
+def test_forces_on_config_grids(cuda, configs, name, state):
+    z, case, plan, dev = configs(name)
+    f = dev.forces(config_state(z, plan, state))
+    assert np.abs(f - z[f"{state}_forces"]).max() < 1e-12
