@@ -47,8 +47,8 @@ METRIC = "converged RANS solves/hr"
 STEPS_PER_SOLVE = {"c_sa_385": 640, "o_euler_257": 3840}
 # coefficients of the linearisation the J.v tile reads per face and per cell (the
 # kernel's JacShape and JCELL): inviscid 4 x 4 per side, the SA convection's 3, the
-# viscous tail's rows x intermediates
-LIN_FACE = {"euler": 32, "laminar": 32 + 3 * 9, "sa": 35 + 4 * 14}
+# viscous tail's derivatives its dependences allow (19 laminar, 33 SA)
+LIN_FACE = {"euler": 32, "laminar": 32 + 19, "sa": 35 + 33}
 LIN_CELL = {"euler": 0, "laminar": 0, "sa": 7}
 
 

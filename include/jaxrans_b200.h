@@ -157,6 +157,12 @@ int jr_residual_noalloc(jr_plan* plan, const double* U, double* R, int first_ord
  * (src/jaxrans/solvers/implicit.py:104-108).  Device pointers. */
 int jr_jvp(jr_plan* plan, const double* U, const double* v, double* Jv);
 
+/* The volume-weighted L2 norm of row `variable` of the field R over each case's block
+ * cells, sqrt(sum V R^2 / sum V), computed on the device (a fixed-order sum); out (host)
+ * receives one value per case.  Replaces ResidualOperator.norm
+ * (src/jaxrans/numerics/residual.py:237-240).  R: device pointer; synchronises. */
+int jr_norm(jr_plan* plan, const double* R, int32_t variable, double* out);
+
 /* lambda on every canvas face, i-faces then j-faces (length n_faces).  Replaces
  * ResidualOperator.wave_speeds / face_wave_speeds (src/jaxrans/numerics/residual.py:169-192). */
 int jr_wave_speeds(jr_plan* plan, const double* U, double* lam);

@@ -53,6 +53,7 @@ int reduce_blocks(int n);
 // forces.cu
 void launch_forces(const CaseDev*, const BatchDims&, cudaStream_t);
 void launch_monitor(CaseDev* cases, int n_live, int n_slots, int step0, int block_iters, cudaStream_t st);
+void launch_norm(const CaseDev* cases, int n_cases, int variable, double* out, cudaStream_t st);
 }  // namespace jr
 
 using namespace jr;
@@ -80,6 +81,7 @@ struct jr_plan {
   double* U = nullptr;                   // every case's state, back to back
   double* history = nullptr;             // [step][case]
   double* force_out = nullptr;           // 8 per case
+  double* norm_out = nullptr;            // 1 per case (jr_norm)
   Scalars* sc = nullptr;                 // one per case
   Monitor* mon = nullptr;                // one per case: the exit test on the device
   cudaGraphExec_t graph = nullptr;
@@ -359,6 +361,7 @@ static int build_buffers(jr_plan* p, const std::vector<size_t>& factor_rows) {
   TRY(dev_alloc(p, (void**)&p->mon, (size_t)nc * sizeof(Monitor)));
   TRY(dev_alloc(p, (void**)&p->history, (size_t)HIST_STEPS * nc * sizeof(double)));
   TRY(dev_alloc(p, (void**)&p->force_out, (size_t)8 * nc * sizeof(double)));
+  TRY(dev_alloc(p, (void**)&p->norm_out, (size_t)nc * sizeof(double)));
   TRY(dev_alloc(p, (void**)&p->wall_out, std::max<size_t>(1, p->total_walls) * 5 * sizeof(double)));
   p->U = vec[0];
   for (int k = 0; k < nc; ++k) {
@@ -703,6 +706,18 @@ int jr_jvp(jr_plan* plan, const double* U, const double* v, double* Jv) {
   if (vortex) launch_ghosts(t, plan->dims, B_Z, 0, plan->st);
   launch_jvp(t, plan->dims, plan->visc, B_Z, -1, B_W, 0, vortex ? 0 : 1, plan->st);
   return cuda_check("jr_jvp");
+}
+
+int jr_norm(jr_plan* plan, const double* R, int32_t variable, double* out) {
+  if (!plan || !R || !out) return fail(JR_EINVAL, "null argument");
+  if (variable < 0 || variable >= plan->nvar) return fail(JR_EINVAL, "variable out of range");
+  Adhoc a(plan);
+  a.vec(&CaseDev::R, R);
+  const CaseDev* t = a.upload();
+  launch_norm(t, plan->n_cases, variable, plan->norm_out, plan->st);
+  cudaMemcpyAsync(out, plan->norm_out, (size_t)plan->n_cases * sizeof(double), cudaMemcpyDeviceToHost, plan->st);
+  if (cudaStreamSynchronize(plan->st) != cudaSuccess) return cuda_check("jr_norm");
+  return cuda_check("jr_norm");
 }
 
 int jr_wave_speeds(jr_plan* plan, const double* U, double* lam) {

@@ -227,6 +227,33 @@ __global__ void __launch_bounds__(32) k_monitor(CaseDev* __restrict__ cases, int
   if (reason != MON_RUNNING && m.release) cd.enabled = 0;
 }
 
+// The volume-weighted L2 norm of row `variable` of each case's field R over its block
+// cells (src/jaxrans/numerics/residual.py:237-240): sqrt(sum V R^2 / sum V), one CTA per
+// case, its threads' partial sums added in a fixed order.
+__global__ void __launch_bounds__(256) k_norm(const CaseDev* __restrict__ cases, int variable,
+                                              double* __restrict__ out) {
+  const CaseDev& cd = cases[blockIdx.x];
+  const Canvas& c = cd.c;
+  const int N = c.ncanvas();
+  const double* __restrict__ R = cd.R + (size_t)variable * N;
+  __shared__ double red[8];
+  double acc = 0.0;
+  for (int k = threadIdx.x; k < N; k += blockDim.x)
+    if (c.interior[k]) acc += c.volume[k] * (R[k] * R[k]);
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    out[blockIdx.x] = sqrt(t / c.volume_sum);
+  }
+}
+
+void launch_norm(const CaseDev* cases, int n_cases, int variable, double* out, cudaStream_t st) {
+  k_norm<<<n_cases, 256, 0, st>>>(cases, variable, out);
+}
+
 void launch_monitor(CaseDev* cases, int n_live, int n_slots, int step0, int block_iters, cudaStream_t st) {
   if (n_live > 0) k_monitor<<<n_live, 32, 0, st>>>(cases, n_slots, step0, block_iters);
 }

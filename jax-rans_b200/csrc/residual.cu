@@ -308,6 +308,22 @@ template <class T, int NV> struct TileSmem {
 template <int VISC> struct ViscShape {
   static constexpr int NX = VISC == 2 ? 14 : 9;   // intermediates
   static constexpr int NR = VISC == 2 ? 4 : 3;    // tail outputs: fx, fy, energy[, SA diffusion]
+  // the intermediates each output depends on (bit k: x[k]): fx and fy on the velocity
+  // gradients, the laminar face T and (SA) the face rho, p, nu_hat through the eddy
+  // viscosity; the energy on all of those and the T gradient and face velocity; the SA
+  // diffusion on the nu_hat gradient and the face rho, p, nu_hat
+  __host__ __device__ static constexpr unsigned depends(int r) {
+    return VISC == 2 ? (r < 2 ? 0x390Fu : (r == 2 ? 0x39FFu : 0x3E00u)) : (r < 2 ? 0x10Fu : 0x1FFu);
+  }
+  // the place of d out[r] / d x[k] among the stored derivatives (those a dependence allows)
+  __host__ __device__ static constexpr int slot(int r, int k) {
+    int n = 0;
+    for (int q = 0; q < r; ++q)
+      for (int b = 0; b < NX; ++b) n += (depends(q) >> b) & 1u;
+    for (int b = 0; b < k; ++b) n += (depends(r) >> b) & 1u;
+    return n;
+  }
+  static constexpr int NSTORED = slot(NR - 1, NX);
 };
 
 // q(v, i, j): primitive row v of staged cell (i, j); phi(i, j, k): (u, v, T, nu_hat)[k];
@@ -675,7 +691,7 @@ __global__ void __launch_bounds__(TILE_THREADS, TILE_MIN_BLOCKS)
 template <int VISC> struct JacShape {
   static constexpr int SA0 = 32;                      // SA convection: up, mass if A is upwind, mass if B is
   static constexpr int VBASE = VISC == 2 ? 35 : 32;   // the viscous tail's [r][k] at VBASE + r * NX + k
-  static constexpr int NCOEF = VISC == 0 ? 32 : VBASE + ViscShape<VISC>::NR * ViscShape<VISC>::NX;
+  static constexpr int NCOEF = VISC == 0 ? 32 : VBASE + ViscShape<VISC>::NSTORED;
 };
 constexpr int JCELL = 7;   // the SA source's derivatives per interior cell
 
@@ -732,6 +748,7 @@ __device__ __forceinline__ void linearize_face(const Physics& P, TileSmem<double
     auto cyv = [&](int i, int j) { return s.cy[i - 1][j - 1]; };
     double x[NX];
     face_intermediates<double, VISC>(q, phi, cxv, cyv, axis, ai, aj, x);
+    using S = ViscShape<VISC>;
 #pragma unroll 1
     for (int k = 0; k < NX; ++k) {
       Dual xd[NX], out[NR];
@@ -739,7 +756,8 @@ __device__ __forceinline__ void linearize_face(const Physics& P, TileSmem<double
       for (int m = 0; m < NX; ++m) xd[m] = Dual{x[m], m == k ? 1.0 : 0.0};
       viscous_tail<Dual, VISC>(P, xd, sx, sy, out);
 #pragma unroll
-      for (int r = 0; r < NR; ++r) jac[(size_t)(J::VBASE + r * NX + k) * stride + f] = out[r].d;
+      for (int r = 0; r < NR; ++r)
+        if ((S::depends(r) >> k) & 1u) jac[(size_t)(J::VBASE + S::slot(r, k)) * stride + f] = out[r].d;
     }
   }
 }
@@ -885,11 +903,13 @@ __device__ __forceinline__ void jv_face(const JvSmem<NV>& s, int axis, int ai, i
     auto cyv = [&](int i, int j) { return s.cy[i][j]; };
     double x[NX];
     face_intermediates<double, VISC>(q, phi, cxv, cyv, axis, ai, aj, x);
+    using S = ViscShape<VISC>;
 #pragma unroll
     for (int r = 0; r < NR; ++r) {
       double acc = 0.0;
 #pragma unroll
-      for (int k = 0; k < NX; ++k) acc += jf[(size_t)(J::VBASE + r * NX + k) * stride] * x[k];
+      for (int k = 0; k < NX; ++k)
+        if ((S::depends(r) >> k) & 1u) acc += jf[(size_t)(J::VBASE + S::slot(r, k)) * stride] * x[k];
       dF[r < 3 ? 1 + r : NV - 1] -= acc;
     }
   }

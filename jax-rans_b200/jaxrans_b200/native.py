@@ -65,7 +65,7 @@ EXPORTS = ("jr_plan_create", "jr_plan_destroy", "jr_last_error", "jr_plan_sizes"
            "jr_launch_count", "jr_autotune", "jr_line_schedule", "jr_wait_limit_check", "jr_wall_loads",
            "jr_plan3d_create", "jr_plan3d_destroy", "jr_residual3d", "jr_jvp3d", "jr_wave_speeds3d",
            "jr_precondition3d", "jr_newton_steps3d", "jr_forces3d", "jr_wall_distance3d",
-           "jr_launches3d", "jr_wall_loads3d", "jr_monitor_set", "jr_monitor_blocks", "jr_monitor_get")
+           "jr_launches3d", "jr_wall_loads3d", "jr_monitor_set", "jr_monitor_blocks", "jr_monitor_get", "jr_norm")
 
 TIMED_KERNELS = ("residual_tile", "jvp_tile", "ghosts_tangent", "line_apply", "line_factor", "cgs2_full_basis",
                  "linearize")
@@ -152,6 +152,7 @@ def load_library(path: Path | None = None) -> C.CDLL:
         "jr_monitor_set": (C.c_int, [vp, C.c_int32, C.c_double, C.c_double, C.c_int32, C.c_int32]),
         "jr_monitor_blocks": (C.c_int, [vp, C.c_int32, C.c_int32, vp]),
         "jr_monitor_get": (C.c_int, [vp, C.c_int32, _i32p, _i32p, _f64p, vp]),
+        "jr_norm": (C.c_int, [vp, vp, C.c_int32, _f64p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -356,6 +357,14 @@ class DevicePlan:
         _check(self.lib, self.lib.jr_jvp(self.handle, u.data_ptr(), t.data_ptr(), out.data_ptr()), "jr_jvp")
         self.sync()
         return self._like_input(U, out)
+
+    def norm(self, R, variable: int = 0):
+        """The volume-weighted L2 norm of row ``variable`` over the block cells, on the
+        device: a float, or one per case for a batch."""
+        keep = self._device(R)
+        out = np.empty(self.n_cases)
+        _check(self.lib, self.lib.jr_norm(self.handle, keep.data_ptr(), int(variable), _ptr(out, _f64p)), "jr_norm")
+        return float(out[0]) if self.n_cases == 1 else out
 
     def wave_speeds(self, U):
         u = self._device(U)
