@@ -330,7 +330,8 @@ static int build_buffers(jr_plan* p, const std::vector<size_t>& factor_rows) {
     tiles += (size_t)p->host[k].n_tiles;
     p->host[k].jstride = (int)((nf + 31) / 32 * 32);
     jac_off[k] = jac;
-    jac += (size_t)n_coef * p->host[k].jstride + (size_t)n_cell_coef * N;
+    jac += (size_t)n_coef * p->host[k].jstride + (size_t)n_cell_coef * N +
+           (size_t)(c.n_ghost[0] + c.n_ghost[1]) * c.nvar * c.nvar;
     fb += factor_rows[k];
     part += (size_t)reduce_blocks(p->host[k].n_vec) * (MAX_KRYLOV + 1);
   }
@@ -378,6 +379,7 @@ static int build_buffers(jr_plan* p, const std::vector<size_t>& factor_rows) {
     cd.tile_partial = tile_partial + tile_off[k];
     cd.jac = lin + jac_off[k];
     cd.jcell = n_cell_coef > 0 ? cd.jac + (size_t)n_coef * cd.jstride : nullptr;
+    cd.gmap = cd.jac + (size_t)n_coef * cd.jstride + (size_t)n_cell_coef * cd.c.NI * cd.c.NJ;
     cd.partial = partial + part_off[k];
     cd.ticket = ticket + k;
     cd.V = (char*)V + (size_t)(p->m + 1) * vo * tb;
@@ -470,13 +472,11 @@ static void enqueue_cycle(jr_plan* p, cudaStream_t st) {
     if (pre) launch_chain_apply(t, d, sa, p->mixed, src, 1, j, B_Z, 1, st);
     else launch_scale_copy(t, d, p->mixed, src, 1, j, B_Z, 1, st);
     if (coupled) launch_chain_couple(t, d, p->mixed, B_Z, 1, st);
-    // the tangent ghosts: a single case's J.v tiles evaluate their halo's ghosts
-    // themselves (one launch fewer on a latency-bound step); a batch, whose tiles run in
-    // many waves, fills them in one launch, as does any case that needs the point-vortex
-    // circulation
-    const bool own = !p->live_vortex && d.n_cases == 1;
-    if (!own) launch_ghosts(t, d, B_Z, 1, st);
-    launch_jvp(t, d, p->visc, B_Z, B_VDT, B_W, 1, own ? 1 : 0, st);
+    // the tangent ghosts: the J.v tiles map their halo's ghosts from the source cells'
+    // tangents (the linearisation's ghost maps); a case with the point-vortex far field
+    // (its circulation a sum over the wall) has its tangent ghosts filled by a launch
+    if (p->live_vortex) launch_ghosts(t, d, B_Z, 1, st);
+    launch_jvp(t, d, p->visc, B_Z, B_VDT, B_W, 1, 1, st);
     launch_arnoldi_orth(t, d, p->mixed, j, st);
   }
   launch_lstsq(t, d, st);
@@ -704,7 +704,7 @@ int jr_jvp(jr_plan* plan, const double* U, const double* v, double* Jv) {
   launch_ghosts(t, plan->dims, -1, 0, plan->st);
   launch_linearize(t, plan->dims, plan->visc, plan->st);
   if (vortex) launch_ghosts(t, plan->dims, B_Z, 0, plan->st);
-  launch_jvp(t, plan->dims, plan->visc, B_Z, -1, B_W, 0, vortex ? 0 : 1, plan->st);
+  launch_jvp(t, plan->dims, plan->visc, B_Z, -1, B_W, 0, 1, plan->st);
   return cuda_check("jr_jvp");
 }
 
@@ -1141,7 +1141,7 @@ int jr_time_kernels(jr_plan* plan, int32_t reps, double* ms) {
     ms[k] = (double)ms1 / reps;
   };
   timed(0, [&] { launch_residual(t, d, p->visc, true, B_R, st); });
-  timed(1, [&] { launch_jvp(t, d, p->visc, B_Z, B_VDT, B_W, 0, 0, st); });
+  timed(1, [&] { launch_jvp(t, d, p->visc, B_Z, B_VDT, B_W, 0, 1, st); });
   timed(2, [&] { launch_ghosts(t, d, B_Z, 0, st); });
   timed(3, [&] { launch_chain_apply(t, d, sa, p->mixed, B_R, 0, -1, B_TMP, 0, st); });
   timed(4, [&] { launch_chain_factor(t, d, sa, p->mixed, st); });

@@ -124,6 +124,7 @@ struct CaseDev {
   double *tile_partial, *history, *force_out;
   double* jac;              // the linearisation: per face coefficient planes of jstride doubles
   double* jcell;            // ... and per cell (SA: 7 planes of NI*NJ)
+  double* gmap;             // ... and per ghost record: its nvar x nvar tangent map
   double* wall_out;         // per wall face: gauge pressure, area vector into the fluid (2), viscous force (2)
   void *V, *fflow, *fsa, *scratch;
   Scalars* sc;

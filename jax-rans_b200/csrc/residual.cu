@@ -16,14 +16,6 @@ __device__ __forceinline__ bool interior_at(const Canvas& c, int i, int j) {
   return i >= 0 && i < c.NI && j >= 0 && j < c.NJ && c.interior[i * c.NJ + j];
 }
 
-template <class T> struct Tangent;
-template <> struct Tangent<double> {
-  __device__ static double make(double v, const double*, int) { return v; }
-};
-template <> struct Tangent<Dual> {
-  __device__ static Dual make(double v, const double* dv, int k) { return Dual{v, dv[k]}; }
-};
-
 // primitive state of canvas cell `idx`: prim(U) on block cells, the ghost buffer elsewhere
 template <class T>
 __device__ __forceinline__ void load_prim(const Canvas& c, const Physics& P, int idx, const double* U,
@@ -150,26 +142,6 @@ __device__ __forceinline__ void eval_record(const Canvas& c, const Physics& P, i
   } else {
     condition<T>(P, kind, q, c.g_geom[s] + 4 * r, circ, out);
   }
-}
-
-// The tangent ghost value of record t (both stages numbered as in k_ghosts) from the
-// state and tangent of its source, evaluated where it is needed: the J.v tile computes
-// its halo's ghosts itself when no case uses the point-vortex far field (whose
-// circulation is a reduction over the wall).  Out of line: only boundary tiles call it.
-__device__ __noinline__ void ghost_tangent(const Canvas& c, const Physics& P, int t, const double* U,
-                                           const double* V, const double* qg, const double* dqg, Dual* out) {
-  const int n0 = c.n_ghost[0];
-  const int s = t < n0 ? 0 : 1, r = t < n0 ? t : t - n0;
-  Dual q[5];
-  const int r1 = s == 1 ? c.g_src_rec[r] : -1;
-  if (r1 >= 0) {
-    Dual q1[5];
-    load_prim<Dual>(c, P, c.g_source[0][r1], U, V, qg, dqg, q1);
-    eval_record<Dual>(c, P, 0, r1, q1, cst<Dual>(0.0), q);
-  } else {
-    load_prim<Dual>(c, P, c.g_source[s][r], U, V, qg, dqg, q);
-  }
-  eval_record<Dual>(c, P, s, r, q, cst<Dual>(0.0), out);
 }
 
 // Both stages in one launch: a stage-2 record whose source is a stage-1 ghost (a
@@ -523,12 +495,11 @@ template <class T> __device__ __forceinline__ double tangent_or_value(const T& x
 template <> __device__ __forceinline__ double tangent_or_value<double>(const double& x) { return x; }
 template <> __device__ __forceinline__ double tangent_or_value<Dual>(const Dual& x) { return x.d; }
 
-// T = double: out = R(U) (second or first order); partial[block] = sum vol R0^2.
-// T = Dual:   out = vdt * V + dR1/dU . V.
+// out = R(U) (second or first order); partial[block] = sum vol R0^2.  T is the staged
+// scalar (double).
 template <class T, int NV, bool SECOND, int VISC>
 __global__ void __launch_bounds__(TILE_THREADS, TILE_MIN_BLOCKS)
-    k_residual(const CaseDev* __restrict__ cases, int out_id, int tangent_id, int vdt_id, int with_partial,
-               int check_active, int own_ghosts) {
+    k_residual(const CaseDev* __restrict__ cases, int out_id, int with_partial, int check_active) {
   __shared__ CaseDev scase;
   if (idle_block(cases[blockIdx.z],
                  (int)blockIdx.x >= cases[blockIdx.z].tiles_x || (int)blockIdx.y >= cases[blockIdx.z].tiles_y,
@@ -541,9 +512,6 @@ __global__ void __launch_bounds__(TILE_THREADS, TILE_MIN_BLOCKS)
   const Physics& P = cd.P;
   const double* __restrict__ U = cd.U;
   const double* __restrict__ qg = cd.qg;
-  const double* __restrict__ V = tangent_id >= 0 ? buf(cd, tangent_id) : nullptr;
-  const double* __restrict__ dqg = cd.dqg;
-  const double* __restrict__ vdt = vdt_id >= 0 ? buf(cd, vdt_id) : nullptr;
   double* __restrict__ out = buf(cd, out_id);
   double* __restrict__ partial = with_partial ? cd.tile_partial : nullptr;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -557,17 +525,7 @@ __global__ void __launch_bounds__(TILE_THREADS, TILE_MIN_BLOCKS)
     int i = i0 - 2 + li, j = j0 - 2 + lj;
     T q[5];
     if (i >= 0 && i < NI && j >= 0 && j < NJ) {
-      const int idx = i * NJ + j;
-      int t = -1;
-      if constexpr (sizeof(T) == sizeof(Dual)) {
-        if (own_ghosts && !c.interior[idx]) t = c.ghost_rec[idx];
-      }
-      if constexpr (sizeof(T) == sizeof(Dual)) {
-        if (t >= 0) ghost_tangent(c, P, t, U, V, qg, dqg, q);
-        else load_prim<T>(c, P, idx, U, V, qg, dqg, q);
-      } else {
-        load_prim<T>(c, P, idx, U, V, qg, dqg, q);
-      }
+      load_prim<T>(c, P, i * NJ + j, U, nullptr, qg, nullptr, q);
     } else {
       for (int v = 0; v < NV; ++v) q[v] = cst<T>(1.0);
     }
@@ -641,24 +599,14 @@ __global__ void __launch_bounds__(TILE_THREADS, TILE_MIN_BLOCKS)
           T src = sa_cell_source(P, y, c.distance[idx]);
           R[4] = R[4] - tangent_or_value(src) * vol;
         }
-        if constexpr (sizeof(T) == sizeof(Dual)) {
-          double w = vdt != nullptr ? vdt[idx] : 0.0;
-          for (int v = 0; v < NV; ++v) out[v * N + idx] = w * V[v * N + idx] + R[v];
-        } else {
-          for (int v = 0; v < NV; ++v) out[v * N + idx] = R[v];
-          acc = c.volume[idx] * (R[0] * R[0]);
-        }
+        for (int v = 0; v < NV; ++v) out[v * N + idx] = R[v];
+        acc = c.volume[idx] * (R[0] * R[0]);
       } else {
-        if constexpr (sizeof(T) == sizeof(Dual)) {
-          double w = vdt != nullptr ? vdt[idx] : 0.0;
-          for (int v = 0; v < NV; ++v) out[v * N + idx] = w * V[v * N + idx] + V[v * N + idx];
-        } else {
-          for (int v = 0; v < NV; ++v) out[v * N + idx] = U[v * N + idx] - P.U_inf[v];
-        }
+        for (int v = 0; v < NV; ++v) out[v * N + idx] = U[v * N + idx] - P.U_inf[v];
       }
     }
   }
-  if constexpr (sizeof(T) == sizeof(double)) {
+  {
     if (partial != nullptr) {
       for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
       if ((tid & 31) == 0) s.red[tid >> 5] = acc;
@@ -762,8 +710,10 @@ __device__ __forceinline__ void linearize_face(const Physics& P, TileSmem<double
   }
 }
 
+// Three CTAs per SM (at most 168 registers, some spilled to local memory): a single
+// 385 x 97 case's tiles then run in one wave instead of two; measured 262 against 368 us.
 template <int NV, int VISC>
-__global__ void __launch_bounds__(TILE_THREADS) k_linearize(const CaseDev* __restrict__ cases) {
+__global__ void __launch_bounds__(TILE_THREADS, 3) k_linearize(const CaseDev* __restrict__ cases) {
   __shared__ CaseDev scase;
   if (idle_block(cases[blockIdx.z],
                  (int)blockIdx.x >= cases[blockIdx.z].tiles_x || (int)blockIdx.y >= cases[blockIdx.z].tiles_y, 0))
@@ -852,6 +802,49 @@ __global__ void __launch_bounds__(TILE_THREADS) k_linearize(const CaseDev* __res
           jcell[(size_t)k * N + idx] = sa_cell_source(P, yd, d).d;
         }
       }
+    }
+  }
+}
+
+// The tangent of every ghost record as a map of its source cell's primitive tangent:
+// record t (stage-1 records first) fills its ghost from source cell src(t) -- for a
+// stage-2 record whose source is a stage-1 ghost (a corner), through that record too --
+// so dq_ghost = G_t dq_src, G_t = d(record)/d(q_src), one dual-number evaluation of the
+// condition per source component, at the state of the linearisation.  The uniform
+// far field and the wall, symmetry, inflow, outflow and copy conditions are functions of
+// the source state alone; the point-vortex far field (its circulation a sum over the
+// wall) is not, and its cases fill their tangent ghosts every J.v (k_ghosts) instead.
+__device__ __forceinline__ int ghost_source(const Canvas& c, int t) {
+  const int n0 = c.n_ghost[0];
+  if (t < n0) return c.g_source[0][t];
+  const int r = t - n0, r1 = c.g_src_rec[r];
+  return r1 >= 0 ? c.g_source[0][r1] : c.g_source[1][r];
+}
+
+template <int NV>
+__global__ void k_ghost_maps(const CaseDev* __restrict__ cases) {
+  const CaseDev& cd = cases[blockIdx.y];
+  if (!cd.enabled || cd.P.far_field == 1) return;
+  const Canvas& c = cd.c;
+  const Physics& P = cd.P;
+  const int n0 = c.n_ghost[0], total = n0 + c.n_ghost[1];
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int s = t < n0 ? 0 : 1, r = t < n0 ? t : t - n0;
+    const int r1 = s == 1 ? c.g_src_rec[r] : -1;
+    double qs[5];
+    load_prim<double>(c, P, ghost_source(c, t), cd.U, nullptr, cd.qg, nullptr, qs);
+    double* G = cd.gmap + (size_t)t * NV * NV;
+#pragma unroll 1
+    for (int k = 0; k < NV; ++k) {
+      Dual q[5], q1[5], out[5];
+      for (int v = 0; v < NV; ++v) q[v] = Dual{qs[v], v == k ? 1.0 : 0.0};
+      if (r1 >= 0) {
+        eval_record<Dual>(c, P, 0, r1, q, cst<Dual>(0.0), q1);
+        eval_record<Dual>(c, P, s, r, q1, cst<Dual>(0.0), out);
+      } else {
+        eval_record<Dual>(c, P, s, r, q, cst<Dual>(0.0), out);
+      }
+      for (int v = 0; v < NV; ++v) G[v * NV + k] = out[v].d;
     }
   }
 }
@@ -951,9 +944,23 @@ __global__ void __launch_bounds__(TILE_THREADS) k_jv(const CaseDev* __restrict__
     if (i >= 0 && i < NI && j >= 0 && j < NJ) {
       const int idx = i * NJ + j;
       Dual q[5];
-      const int rec = own_ghosts && !c.interior[idx] ? c.ghost_rec[idx] : -1;
-      if (rec >= 0) ghost_tangent(c, P, rec, U, V, qg, dqg, q);
-      else load_prim<Dual>(c, P, idx, U, V, qg, dqg, q);
+      const int rec = own_ghosts && P.far_field != 1 && !c.interior[idx] ? c.ghost_rec[idx] : -1;
+      if (rec >= 0) {
+        // the ghost's tangent from its source cell's, through the record's map; its
+        // state from the ghost-filled canvas
+        Dual qs[5];
+        load_prim<Dual>(c, P, ghost_source(c, rec), U, V, qg, dqg, qs);
+        const double* G = cd.gmap + (size_t)rec * NV * NV;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          double d = 0.0;
+#pragma unroll
+          for (int k = 0; k < NV; ++k) d += G[v * NV + k] * qs[k].d;
+          q[v] = Dual{qg[v * N + idx], d};
+        }
+      } else {
+        load_prim<Dual>(c, P, idx, U, V, qg, dqg, q);
+      }
 #pragma unroll
       for (int v = 0; v < NV; ++v) t[v] = q[v].d;
       t[NV] = (P.gamma * q[3] / q[0]).d;
@@ -1227,29 +1234,32 @@ void configure_kernels() {
 // One launch over every case of a batch: grid z = the case, x/y = the tiles (a case
 // with fewer tiles returns at once from the excess ones).
 template <class T, int NV, bool SECOND, int VISC>
-static void launch_tile(const CaseDev* cases, const BatchDims& d, int out_id, int tangent_id, int vdt_id,
-                        int with_partial, int check_active, cudaStream_t st, int own_ghosts = 0) {
+static void launch_tile(const CaseDev* cases, const BatchDims& d, int out_id, int with_partial, int check_active,
+                        cudaStream_t st) {
   dim3 grid(d.tiles_x, d.tiles_y, d.n_cases);
-  k_residual<T, NV, SECOND, VISC><<<grid, TILE_THREADS, sizeof(TileSmem<T, NV>), st>>>(
-      cases, out_id, tangent_id, vdt_id, with_partial, check_active, own_ghosts);
+  k_residual<T, NV, SECOND, VISC><<<grid, TILE_THREADS, sizeof(TileSmem<T, NV>), st>>>(cases, out_id, with_partial,
+                                                                                     check_active);
 }
 
 // R(U) of every case into `out_id` (second or first order), with the norm partials
 void launch_residual(const CaseDev* cases, const BatchDims& d, int visc, bool second, int out_id, cudaStream_t st) {
   if (visc == 2) {
-    if (second) launch_tile<double, 5, true, 2>(cases, d, out_id, -1, -1, 1, 0, st);
-    else launch_tile<double, 5, false, 2>(cases, d, out_id, -1, -1, 1, 0, st);
+    if (second) launch_tile<double, 5, true, 2>(cases, d, out_id, 1, 0, st);
+    else launch_tile<double, 5, false, 2>(cases, d, out_id, 1, 0, st);
   } else if (visc == 1) {
-    if (second) launch_tile<double, 4, true, 1>(cases, d, out_id, -1, -1, 1, 0, st);
-    else launch_tile<double, 4, false, 1>(cases, d, out_id, -1, -1, 1, 0, st);
+    if (second) launch_tile<double, 4, true, 1>(cases, d, out_id, 1, 0, st);
+    else launch_tile<double, 4, false, 1>(cases, d, out_id, 1, 0, st);
   } else {
-    if (second) launch_tile<double, 4, true, 0>(cases, d, out_id, -1, -1, 1, 0, st);
-    else launch_tile<double, 4, false, 0>(cases, d, out_id, -1, -1, 1, 0, st);
+    if (second) launch_tile<double, 4, true, 0>(cases, d, out_id, 1, 0, st);
+    else launch_tile<double, 4, false, 0>(cases, d, out_id, 1, 0, st);
   }
 }
 
 // The linearisation of every case's first-order residual at its U (ghosts of U filled)
 void launch_linearize(const CaseDev* cases, const BatchDims& d, int visc, cudaStream_t st) {
+  dim3 ggrid(max(1, (d.ghost_records + GHOST_THREADS - 1) / GHOST_THREADS), d.n_cases);
+  if (visc == 2) k_ghost_maps<5><<<ggrid, GHOST_THREADS, 0, st>>>(cases);
+  else k_ghost_maps<4><<<ggrid, GHOST_THREADS, 0, st>>>(cases);
   dim3 grid(d.tiles_x, d.tiles_y, d.n_cases);
   if (visc == 2) k_linearize<5, 2><<<grid, TILE_THREADS, sizeof(TileSmem<double, 5>), st>>>(cases);
   else if (visc == 1) k_linearize<4, 1><<<grid, TILE_THREADS, sizeof(TileSmem<double, 4>), st>>>(cases);
@@ -1257,8 +1267,9 @@ void launch_linearize(const CaseDev* cases, const BatchDims& d, int visc, cudaSt
 }
 
 // out = vdt * v + dR1/dU . v with v = buffer `tangent_id` (vdt_id < 0: the bare J.v), from
-// the linearisation launch_linearize stored; own_ghosts: the tile evaluates its halo's
-// tangent ghosts (no tangent ghost fill needed)
+// the linearisation launch_linearize stored; own_ghosts: the tiles map their halo's
+// tangent ghosts through the linearisation's ghost maps, but in a case with the
+// point-vortex far field, whose tangent ghosts a ghost fill (launch_ghosts) must provide
 void launch_jvp(const CaseDev* cases, const BatchDims& d, int visc, int tangent_id, int vdt_id, int out_id,
                 int check_active, int own_ghosts, cudaStream_t st) {
   dim3 grid(d.tiles_x, d.tiles_y, d.n_cases);
