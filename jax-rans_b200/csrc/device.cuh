@@ -197,10 +197,13 @@ constexpr int LS_MAX_THREADS = 256;   // the largest line-solve block
 constexpr int APPLY_STAGES = 4;       // staged line-solve forms 1..4 (0: the factor read from global memory)
 
 // The basis passes: a block owns a chunk of cgs_chunk(n) elements of a case of n, set by
-// the case's size alone (so its sums are the same in any batch): small cases keep two
-// blocks per SM, large ones use longer chunks.
+// the case's size alone (so its sums are the same in any batch): small cases (a 385 x 97
+// SA case: 194k unknowns, 380 blocks) take short chunks to keep more blocks per SM,
+// large ones longer chunks.
 constexpr int CGS_MAX_CHUNK = 2048;
-__host__ __device__ __forceinline__ int cgs_chunk(int n) { return n >= 2 * 148 * 2048 ? 2048 : 1024; }
+__host__ __device__ __forceinline__ int cgs_chunk(int n) {
+  return n >= 2 * 148 * 2048 ? 2048 : (n >= 2 * 148 * 1024 ? 1024 : 512);
+}
 __host__ __device__ __forceinline__ int cgs_blocks(int n) { return (n + cgs_chunk(n) - 1) / cgs_chunk(n); }
 
 // the number of blocks a per-case reduction over n elements uses (<= the grid's x)
