@@ -16,6 +16,12 @@ independent: no collective on the data path) and the whole-job rate is reported.
 reference itself is JAX, absent here) on a bounded sample of the same workload: each
 step one Newton step, extrapolated by the number of Newton steps a converged solve takes.
 
+The default line (config 2, FP64) also carries ``forms``: the north-star forms timed
+beside it on bounded samples -- the batched mixed polar ``polar16_uneven`` (19 cases of
+uneven grids in one device plan) and a served Poisson stream of 24 mixed requests with
+continuous batching -- with their solves/hr, p50/p99 and ratios to the plain FP64 path
+(``--no-forms`` skips them).
+
 ``--workload wing_ch_4blk`` (or ``wing_ch_4blk_small``) prints a separate line: 3D
 pseudo-transient Newton steps per second of the swept, tapered wing on its four-block
 C-H grid (3.93M cells), the state resident on the device.
@@ -379,6 +385,87 @@ def roofline_of(kern: dict, model: str, nvar: int, cells: int, peaks: dict, kern
             "peak_source": peaks.get("source", "measured")}
 
 
+def measure_forms(fp64_value: float, fp64_forces, served_requests: int = 24) -> dict:
+    """The north-star forms beside the plain FP64 line, each bounded to a few minutes:
+
+    * batched, mixed: the 19 cases of ``polar16_uneven`` (16 angles on the 385 x 97 grid and
+      the 257, 513 and 769 uneven grids) in one device plan, FP32 line preconditioner and
+      Krylov basis, each case leaving the launches at its own exit; solves/hr of the whole
+      batch (device clock), the cases' exit times (p50, p99), and |dCL|, |dCD| of its 8 deg
+      case against the FP64 line's forces;
+    * served: a seeded Poisson stream (20 requests/s) of ``served_requests`` SA requests of
+      the config-4 distribution (van Albada), mixed, continuous batching with up to
+      ``served_requests`` slots per grid size; solves/hr over the stream's wall time,
+      p50/p99 latency from arrival; the first three requests also solved one at a time on
+      the plain FP64 path (solves/hr, |dCL|, |dCD| against the served results).
+    """
+    import dataclasses
+    import torch
+    from jaxrans_b200.batch import batch_device, run_batch_blocks, start_batch
+    from jaxrans_b200.serve import Server, poisson_requests, summary
+    from jaxrans_b200.solver import march
+    from jaxrans_b200.workloads import BATCHES, batch_workload, workload
+    out = {}
+    # batched, mixed
+    cases = batch_workload("polar16_uneven", **{"implicit.precision": "mixed"})
+    made, grids = {}, []
+    for (w, _), c in zip(BATCHES["polar16_uneven"], cases):
+        if w not in made:
+            made[w] = c.grid()
+        grids.append(made[w])
+    dev = batch_device(cases, grids, autotune=True)
+    start_batch(dev, cases, grids)
+    stream = torch.cuda.ExternalStream(dev.stream_handle())
+    torch.cuda.synchronize()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    monitors, seconds, _ = run_batch_blocks(cases, dev)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    wall = s0.elapsed_time(s1) / 1e3
+    dev.close()
+    lat = [m.seconds * wall / seconds for m in monitors]
+    k8 = [round(c.flow.alpha_deg, 6) for c in cases].index(8.0)
+    f8 = monitors[k8].forces
+    value = 3600.0 * len(cases) / wall
+    out["batched_mixed"] = {
+        "workload": "polar16_uneven", "cases": len(cases), "cells": sum(g.cells for g in grids),
+        "solves_per_hr": value, "ratio_to_fp64_line": value / fp64_value, "seconds": wall,
+        "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+        "newton_steps_slowest": max(m.iterations for m in monitors),
+        "exits": {r: sum(m.reason == r for m in monitors) for r in sorted({m.reason for m in monitors})},
+        "alpha8_vs_fp64_line": {"dcl": abs(f8.cl - fp64_forces["cl"]), "dcd": abs(f8.cd - fp64_forces["cd"]),
+                                "note": "settled (minmod) states: the state the forces settle on depends "
+                                        "on the path, by about 5e-4 in CL between FP64 runs too"}}
+    # served, mixed, continuous batching
+    template = workload("c_sa_385", **{"implicit.precision": "mixed", "convective_fluxes.limiter": "van_albada"})
+    requests = poisson_requests(served_requests, template, 20.0, seed=0)
+    server = Server(max_slots=served_requests, workers=4)
+    t = time.perf_counter()
+    served = server.serve(requests)
+    wall = time.perf_counter() - t
+    server.close()
+    summ = summary(served, wall)
+    plain_s, dcl, dcd = 0.0, [], []
+    for x in served[:3]:
+        c = x.request.case
+        plain = dataclasses.replace(c, implicit=dataclasses.replace(c.implicit, precision="fp64"))
+        grid = plain.grid()
+        t = time.perf_counter()
+        r = march(plain, grid)
+        plain_s += time.perf_counter() - t
+        dcl.append(abs(x.forces.cl - r.forces.cl))
+        dcd.append(abs(x.forces.cd - r.forces.cd))
+    plain_rate = 3600.0 * 3 / plain_s
+    out["served_mixed"] = {
+        "requests": served_requests, "rate_per_s": 20.0, "seed": 0, "limiter": "van_albada",
+        "solves_per_hr": summ["solves_per_hr"], "p50_s": summ["p50_s"], "p99_s": summ["p99_s"],
+        "exits": summ["exits"], "seconds": wall,
+        "plain_fp64_first3": {"solves_per_hr": plain_rate, "max_dcl": max(dcl), "max_dcd": max(dcd)},
+        "ratio_to_plain_fp64_same_requests": summ["solves_per_hr"] / plain_rate}
+    return out
+
+
 def max_over_ranks(values, dist, device):
     """Each value's maximum over the ranks (the slowest replica times the job); the
     values themselves without a process group."""
@@ -557,6 +644,9 @@ def run_device(args) -> int:
     }
     if rank == 0:
         result["clocks"] = clocks.summary()
+        if world == 1 and n_cases == 1 and not args.no_forms and args.workload == "c_sa_385" \
+                and args.precision == "fp64":
+            result["forms"] = measure_forms(value, config["forces"])
         if world == 1 and not args.no_cpu_baseline:
             from jaxrans_b200.workloads import BATCHES
             name = BATCHES[args.workload][0][0] if args.workload in BATCHES else args.workload
@@ -578,9 +668,11 @@ def main(argv=None) -> int:
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=("b200", "reference"))
     p.add_argument("--workload", default="c_sa_385",
-                   choices=sorted(STEPS_PER_SOLVE) + ["polar64_uneven"] + list(WING3D_WORKLOADS))
+                   choices=sorted(STEPS_PER_SOLVE) + ["polar64_uneven", "polar16_uneven"] + list(WING3D_WORKLOADS))
     p.add_argument("--precision", default="fp64", choices=("fp64", "mixed"))
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-forms", action="store_true",
+                   help="skip the batched and served mixed forms timed beside the default FP64 line")
     p.add_argument("--line-schedule", default=None, metavar="F,A,S",
                    help="line factor threads, line solve threads, solve form (0 global, 1-4 staged) instead of "
                         "the autotuner's pick (for runs under a profiler, where its timings do not hold)")

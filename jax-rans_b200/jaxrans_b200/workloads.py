@@ -26,7 +26,9 @@ on a GPU box and in the oracle.
   cells round the airfoil and a sixth along each wake side, the numerics of
   ``c_sa_385``.
 * batch ``polar64_uneven`` -- 64 angles uniform on [-4, 16] deg on the ``c_sa_385``
-  grid together with the three uneven cases, all in one device batch; ``polar8_769``,
+  grid together with the three uneven cases, all in one device batch; ``polar16_uneven``,
+  16 angles with the same three uneven cases, is the bounded form the benchmark times;
+  ``polar8_769``,
   8 angles with the 769 x 193 case, is the same mix small enough to profile.
 * ``wing_ch_4blk`` -- 3D SA-noft2 RANS round a swept, tapered wing: NACA 0012 sections,
   aspect ratio 4 (semispan 1.6 root chords), taper 0.6, leading-edge sweep 25 deg, on a
@@ -88,6 +90,10 @@ WORKLOADS["c_sa_769"] = _c_sa("c_sa_769", "naca4415", 512, 128, 192, 0.3, 9e6)
 BATCHES = {
     "polar64_uneven": [("c_sa_385", float(a)) for a in
                        [-4.0 + 20.0 * k / 63 for k in range(64)]] + [("c_sa_257", None), ("c_sa_513", None),
+                                                                      ("c_sa_769", None)],
+    # a quarter of it, timed beside the plain FP64 line: 16 angles and the three uneven grids
+    "polar16_uneven": [("c_sa_385", float(a)) for a in
+                       [-4.0 + 20.0 * k / 15 for k in range(16)]] + [("c_sa_257", None), ("c_sa_513", None),
                                                                       ("c_sa_769", None)],
     # a small batch of the same kinds, for profiling captures (about 1.5 GB on the device)
     "polar8_769": [("c_sa_385", float(a)) for a in [-4.0 + 20.0 * k / 7 for k in range(8)]] + [("c_sa_769", None)],
