@@ -821,6 +821,7 @@ __device__ __forceinline__ int ghost_source(const Canvas& c, int t) {
   return r1 >= 0 ? c.g_source[0][r1] : c.g_source[1][r];
 }
 
+// One thread per (record, source component): column k of G_t.
 template <int NV>
 __global__ void k_ghost_maps(const CaseDev* __restrict__ cases) {
   const CaseDev& cd = cases[blockIdx.y];
@@ -828,24 +829,22 @@ __global__ void k_ghost_maps(const CaseDev* __restrict__ cases) {
   const Canvas& c = cd.c;
   const Physics& P = cd.P;
   const int n0 = c.n_ghost[0], total = n0 + c.n_ghost[1];
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total * NV; e += gridDim.x * blockDim.x) {
+    const int t = e / NV, k = e % NV;
     const int s = t < n0 ? 0 : 1, r = t < n0 ? t : t - n0;
     const int r1 = s == 1 ? c.g_src_rec[r] : -1;
     double qs[5];
     load_prim<double>(c, P, ghost_source(c, t), cd.U, nullptr, cd.qg, nullptr, qs);
     double* G = cd.gmap + (size_t)t * NV * NV;
-#pragma unroll 1
-    for (int k = 0; k < NV; ++k) {
-      Dual q[5], q1[5], out[5];
-      for (int v = 0; v < NV; ++v) q[v] = Dual{qs[v], v == k ? 1.0 : 0.0};
-      if (r1 >= 0) {
-        eval_record<Dual>(c, P, 0, r1, q, cst<Dual>(0.0), q1);
-        eval_record<Dual>(c, P, s, r, q1, cst<Dual>(0.0), out);
-      } else {
-        eval_record<Dual>(c, P, s, r, q, cst<Dual>(0.0), out);
-      }
-      for (int v = 0; v < NV; ++v) G[v * NV + k] = out[v].d;
+    Dual q[5], q1[5], out[5];
+    for (int v = 0; v < NV; ++v) q[v] = Dual{qs[v], v == k ? 1.0 : 0.0};
+    if (r1 >= 0) {
+      eval_record<Dual>(c, P, 0, r1, q, cst<Dual>(0.0), q1);
+      eval_record<Dual>(c, P, s, r, q1, cst<Dual>(0.0), out);
+    } else {
+      eval_record<Dual>(c, P, s, r, q, cst<Dual>(0.0), out);
     }
+    for (int v = 0; v < NV; ++v) G[v * NV + k] = out[v].d;
   }
 }
 
@@ -1257,7 +1256,7 @@ void launch_residual(const CaseDev* cases, const BatchDims& d, int visc, bool se
 
 // The linearisation of every case's first-order residual at its U (ghosts of U filled)
 void launch_linearize(const CaseDev* cases, const BatchDims& d, int visc, cudaStream_t st) {
-  dim3 ggrid(max(1, (d.ghost_records + GHOST_THREADS - 1) / GHOST_THREADS), d.n_cases);
+  dim3 ggrid(max(1, (d.ghost_records * 5 + GHOST_THREADS - 1) / GHOST_THREADS), d.n_cases);
   if (visc == 2) k_ghost_maps<5><<<ggrid, GHOST_THREADS, 0, st>>>(cases);
   else k_ghost_maps<4><<<ggrid, GHOST_THREADS, 0, st>>>(cases);
   dim3 grid(d.tiles_x, d.tiles_y, d.n_cases);
