@@ -62,17 +62,17 @@ def model_of(flow) -> str:
     return "euler" if flow.inviscid else ("sa" if flow.turbulence is not None else "laminar")
 
 
-def jvp_bytes_per_cell(model: str, nvar: int) -> int:
-    """Algorithmic bytes per cell of one J.v tile launch (FP64): the coefficients of the
-    two faces a cell owns and its own, then U (the primitive tangent), v and the output,
-    V/dt; viscous: the centre (2); SA: the volume and the two face vectors the Green-Gauss
-    source reads (4)."""
-    words = 2 * LIN_FACE[model] + LIN_CELL[model] + 3 * nvar + 1
+def jvp_bytes_per_cell(model: str, nvar: int, fp32_faces: bool = False) -> int:
+    """Algorithmic bytes per cell of one J.v tile launch: the coefficients of the two faces
+    a cell owns (FP64, or FP32 in the mixed form) and its own, then U (the primitive
+    tangent), v and the output, V/dt; viscous: the centre (2); SA: the volume and the two
+    face vectors the Green-Gauss source reads (4), all FP64."""
+    words = LIN_CELL[model] + 3 * nvar + 1
     if model != "euler":
         words += 2
     if model == "sa":
         words += 1 + 4
-    return 8 * words
+    return 8 * words + (4 if fp32_faces else 8) * 2 * LIN_FACE[model]
 
 
 def residual_bytes_per_cell(model: str, nvar: int) -> int:

@@ -17,10 +17,10 @@ static_assert(JR_STATUS_NONFINITE == ST_NONFINITE && JR_STATUS_REJECTED == ST_RE
               "the status bits of the C ABI are the device's");
 // residual.cu
 void launch_residual(const CaseDev*, const BatchDims&, int visc, bool second, int out_id, cudaStream_t);
-void launch_jvp(const CaseDev*, const BatchDims&, int visc, int tangent_id, int vdt_id, int out_id, int check_active,
-                int own_ghosts, cudaStream_t);
+void launch_jvp(const CaseDev*, const BatchDims&, int visc, bool fp32, int tangent_id, int vdt_id, int out_id,
+                int check_active, int own_ghosts, cudaStream_t);
 void launch_ghosts(const CaseDev*, const BatchDims&, int tangent_id, int check_active, cudaStream_t);
-void launch_linearize(const CaseDev*, const BatchDims&, int visc, cudaStream_t);
+void launch_linearize(const CaseDev*, const BatchDims&, int visc, bool fp32, cudaStream_t);
 int jac_coefficients(int visc);
 int jac_cell_coefficients(int visc);
 void launch_faces(const CaseDev*, const BatchDims&, int visc, cudaStream_t);
@@ -330,7 +330,10 @@ static int build_buffers(jr_plan* p, const std::vector<size_t>& factor_rows) {
     tiles += (size_t)p->host[k].n_tiles;
     p->host[k].jstride = (int)((nf + 31) / 32 * 32);
     jac_off[k] = jac;
-    jac += (size_t)n_coef * p->host[k].jstride + (size_t)n_cell_coef * N +
+    // the face coefficients (FP32 in the mixed form: half as many doubles' room), then the
+    // cell coefficients and the ghost maps in FP64
+    const size_t face_words = (size_t)n_coef * p->host[k].jstride;
+    jac += (p->mixed ? face_words / 2 : face_words) + (size_t)n_cell_coef * N +
            (size_t)(c.n_ghost[0] + c.n_ghost[1]) * c.nvar * c.nvar;
     fb += factor_rows[k];
     part += (size_t)reduce_blocks(p->host[k].n_vec) * (MAX_KRYLOV + 1);
@@ -378,8 +381,12 @@ static int build_buffers(jr_plan* p, const std::vector<size_t>& factor_rows) {
     cd.dflux = dflux + fo;
     cd.tile_partial = tile_partial + tile_off[k];
     cd.jac = lin + jac_off[k];
-    cd.jcell = n_cell_coef > 0 ? cd.jac + (size_t)n_coef * cd.jstride : nullptr;
-    cd.gmap = cd.jac + (size_t)n_coef * cd.jstride + (size_t)n_cell_coef * cd.c.NI * cd.c.NJ;
+    {
+      const size_t face_words = (size_t)n_coef * cd.jstride;   // jstride is a multiple of 32
+      double* rest = lin + jac_off[k] + (p->mixed ? face_words / 2 : face_words);
+      cd.jcell = n_cell_coef > 0 ? rest : nullptr;
+      cd.gmap = rest + (size_t)n_cell_coef * cd.c.NI * cd.c.NJ;
+    }
     cd.partial = partial + part_off[k];
     cd.ticket = ticket + k;
     cd.V = (char*)V + (size_t)(p->m + 1) * vo * tb;
@@ -476,7 +483,7 @@ static void enqueue_cycle(jr_plan* p, cudaStream_t st) {
     // tangents (the linearisation's ghost maps); a case with the point-vortex far field
     // (its circulation a sum over the wall) has its tangent ghosts filled by a launch
     if (p->live_vortex) launch_ghosts(t, d, B_Z, 1, st);
-    launch_jvp(t, d, p->visc, B_Z, B_VDT, B_W, 1, 1, st);
+    launch_jvp(t, d, p->visc, p->mixed, B_Z, B_VDT, B_W, 1, 1, st);
     launch_arnoldi_orth(t, d, p->mixed, j, st);
   }
   launch_lstsq(t, d, st);
@@ -507,7 +514,7 @@ static int enqueue_step(jr_plan* p) {
   cudaStream_t st = p->st;
   launch_ghosts(t, d, -1, 0, st);
   launch_residual(t, d, p->visc, true, B_R, st);
-  launch_linearize(t, d, p->visc, st);
+  launch_linearize(t, d, p->visc, p->mixed, st);
   launch_gmres_init(t, d, st);
   launch_faces(t, d, p->visc, st);
   launch_cells(t, d, p->visc, st);
@@ -702,9 +709,9 @@ int jr_jvp(jr_plan* plan, const double* U, const double* v, double* Jv) {
   bool vortex = false;
   for (const CaseDev& cd : plan->host) vortex = vortex || cd.P.far_field == 1;
   launch_ghosts(t, plan->dims, -1, 0, plan->st);
-  launch_linearize(t, plan->dims, plan->visc, plan->st);
+  launch_linearize(t, plan->dims, plan->visc, plan->mixed, plan->st);
   if (vortex) launch_ghosts(t, plan->dims, B_Z, 0, plan->st);
-  launch_jvp(t, plan->dims, plan->visc, B_Z, -1, B_W, 0, 1, plan->st);
+  launch_jvp(t, plan->dims, plan->visc, plan->mixed, B_Z, -1, B_W, 0, 1, plan->st);
   return cuda_check("jr_jvp");
 }
 
@@ -1116,7 +1123,7 @@ int jr_time_kernels(jr_plan* plan, int32_t reps, double* ms) {
   // active Krylov cycle with z = the residual
   launch_ghosts(t, d, -1, 0, st);
   launch_residual(t, d, p->visc, true, B_R, st);
-  launch_linearize(t, d, p->visc, st);
+  launch_linearize(t, d, p->visc, p->mixed, st);
   launch_faces(t, d, p->visc, st);
   launch_cells(t, d, p->visc, st);
   launch_chain_factor(t, d, sa, p->mixed, st);
@@ -1141,12 +1148,12 @@ int jr_time_kernels(jr_plan* plan, int32_t reps, double* ms) {
     ms[k] = (double)ms1 / reps;
   };
   timed(0, [&] { launch_residual(t, d, p->visc, true, B_R, st); });
-  timed(1, [&] { launch_jvp(t, d, p->visc, B_Z, B_VDT, B_W, 0, 1, st); });
+  timed(1, [&] { launch_jvp(t, d, p->visc, p->mixed, B_Z, B_VDT, B_W, 0, 1, st); });
   timed(2, [&] { launch_ghosts(t, d, B_Z, 0, st); });
   timed(3, [&] { launch_chain_apply(t, d, sa, p->mixed, B_R, 0, -1, B_TMP, 0, st); });
   timed(4, [&] { launch_chain_factor(t, d, sa, p->mixed, st); });
   timed(5, [&] { launch_arnoldi_orth(t, d, p->mixed, p->m - 1, st); });
-  timed(6, [&] { launch_linearize(t, d, p->visc, st); });
+  timed(6, [&] { launch_linearize(t, d, p->visc, p->mixed, st); });
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return cuda_check("jr_time_kernels");

@@ -122,7 +122,8 @@ struct CaseDev {
   Config cfg;
   double *U, *qg, *dqg, *R, *b, *x, *action, *r, *w, *z, *tmp, *vdt, *dflow, *dsa, *lam, *mflux, *dflux;
   double *tile_partial, *history, *force_out;
-  double* jac;              // the linearisation: per face coefficient planes of jstride doubles
+  void* jac;                // the linearisation: per face coefficient planes of jstride values
+                            // (double, or float in the mixed form)
   double* jcell;            // ... and per cell (SA: 7 planes of NI*NJ)
   double* gmap;             // ... and per ghost record: its nvar x nvar tangent map
   double* wall_out;         // per wall face: gauge pressure, area vector into the fluid (2), viscous force (2)

@@ -650,9 +650,9 @@ int jac_cell_coefficients(int visc) { return visc == 2 ? JCELL : 0; }
 
 // Coefficients of one face at flat face index f (i-faces first, then j-faces); the face
 // lies between staged cells (ai, aj) and the next along `axis` of a double tile.
-template <int NV, int VISC>
+template <int NV, int VISC, class TJ>
 __device__ __forceinline__ void linearize_face(const Physics& P, TileSmem<double, NV>& s, int axis, int ai, int aj,
-                                               double sx, double sy, double* __restrict__ jac, size_t stride,
+                                               double sx, double sy, TJ* __restrict__ jac, size_t stride,
                                                int f) {
   using J = JacShape<VISC>;
   const double g = P.gamma;
@@ -675,14 +675,14 @@ __device__ __forceinline__ void linearize_face(const Physics& P, TileSmem<double
     riemann(P.flux, qL, qR, sx, sy, g, F);
     const int base = seed < 4 ? seed : 12 + seed;   // AL[r][v] at r * 4 + v, AR[r][v] at 16 + r * 4 + v
 #pragma unroll
-    for (int r = 0; r < 4; ++r) jac[(size_t)(base + 4 * r) * stride + f] = F[r].d;
+    for (int r = 0; r < 4; ++r) jac[(size_t)(base + 4 * r) * stride + f] = TJ(F[r].d);
     mass = F[0].v;
   }
   if constexpr (VISC == 2) {
     const bool a_up = mass > 0.0;
-    jac[(size_t)J::SA0 * stride + f] = a_up ? s.q[4][ai][aj] : s.q[4][bi][bj];
-    jac[(size_t)(J::SA0 + 1) * stride + f] = a_up ? mass : 0.0;
-    jac[(size_t)(J::SA0 + 2) * stride + f] = a_up ? 0.0 : mass;
+    jac[(size_t)J::SA0 * stride + f] = TJ(a_up ? s.q[4][ai][aj] : s.q[4][bi][bj]);
+    jac[(size_t)(J::SA0 + 1) * stride + f] = TJ(a_up ? mass : 0.0);
+    jac[(size_t)(J::SA0 + 2) * stride + f] = TJ(a_up ? 0.0 : mass);
   }
   if constexpr (VISC > 0) {
     constexpr int NX = ViscShape<VISC>::NX, NR = ViscShape<VISC>::NR;
@@ -705,14 +705,14 @@ __device__ __forceinline__ void linearize_face(const Physics& P, TileSmem<double
       viscous_tail<Dual, VISC>(P, xd, sx, sy, out);
 #pragma unroll
       for (int r = 0; r < NR; ++r)
-        if ((S::depends(r) >> k) & 1u) jac[(size_t)(J::VBASE + S::slot(r, k)) * stride + f] = out[r].d;
+        if ((S::depends(r) >> k) & 1u) jac[(size_t)(J::VBASE + S::slot(r, k)) * stride + f] = TJ(out[r].d);
     }
   }
 }
 
 // Three CTAs per SM (at most 168 registers, some spilled to local memory): a single
 // 385 x 97 case's tiles then run in one wave instead of two; measured 262 against 368 us.
-template <int NV, int VISC>
+template <int NV, int VISC, class TJ>
 __global__ void __launch_bounds__(TILE_THREADS, 3) k_linearize(const CaseDev* __restrict__ cases) {
   __shared__ CaseDev scase;
   if (idle_block(cases[blockIdx.z],
@@ -724,7 +724,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 3) k_linearize(const CaseDev* __
   const Physics& P = cd.P;
   const double* __restrict__ U = cd.U;
   const double* __restrict__ qg = cd.qg;
-  double* __restrict__ jac = cd.jac;
+  TJ* __restrict__ jac = static_cast<TJ*>(cd.jac);
   const size_t stride = (size_t)cd.jstride;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TileSmem<double, NV>& s = *reinterpret_cast<TileSmem<double, NV>*>(smem_raw);
@@ -759,7 +759,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 3) k_linearize(const CaseDev* __
     int i = i0 + fi, j = j0 + fj;
     if (j < NJ && (interior_at(c, i - 1, j) || interior_at(c, i, j))) {
       int f = i * NJ + j;
-      linearize_face<NV, VISC>(P, s, 0, fi + 1, fj + 2, c.fi[f], c.fi[nfi + f], jac, stride, f);
+      linearize_face<NV, VISC, TJ>(P, s, 0, fi + 1, fj + 2, c.fi[f], c.fi[nfi + f], jac, stride, f);
     }
   }
   for (int e = tid; e < TILE_I * (TILE_J + 1); e += TILE_THREADS) {
@@ -767,7 +767,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 3) k_linearize(const CaseDev* __
     int i = i0 + fi, j = j0 + fj;
     if (i < NI && (interior_at(c, i, j - 1) || interior_at(c, i, j))) {
       int f = i * (NJ + 1) + j;
-      linearize_face<NV, VISC>(P, s, 1, fi + 2, fj + 1, c.fj[f], c.fj[c.nfj() + f], jac, stride, nfi + f);
+      linearize_face<NV, VISC, TJ>(P, s, 1, fi + 2, fj + 1, c.fj[f], c.fj[c.nfj() + f], jac, stride, nfi + f);
     }
   }
   if constexpr (VISC == 2) {
@@ -859,9 +859,9 @@ template <int NV> struct JvSmem {
   double Fj[NV][TILE_I][TILE_J + 1];
 };
 
-template <int NV, int VISC>
+template <int NV, int VISC, class TJ>
 __device__ __forceinline__ void jv_face(const JvSmem<NV>& s, int axis, int ai, int aj,
-                                        const double* __restrict__ jf, size_t stride, double* dF) {
+                                        const TJ* __restrict__ jf, size_t stride, double* dF) {
   using J = JacShape<VISC>;
   const int bi = ai + (axis == 0 ? 1 : 0), bj = aj + (axis == 0 ? 0 : 1);
   double a[4], b[4];
@@ -874,14 +874,15 @@ __device__ __forceinline__ void jv_face(const JvSmem<NV>& s, int axis, int ai, i
   for (int r = 0; r < 4; ++r) {
     double acc = 0.0;
 #pragma unroll
-    for (int v = 0; v < 4; ++v) acc += jf[(size_t)(4 * r + v) * stride] * a[v];
+    for (int v = 0; v < 4; ++v) acc += double(jf[(size_t)(4 * r + v) * stride]) * a[v];
 #pragma unroll
-    for (int v = 0; v < 4; ++v) acc += jf[(size_t)(16 + 4 * r + v) * stride] * b[v];
+    for (int v = 0; v < 4; ++v) acc += double(jf[(size_t)(16 + 4 * r + v) * stride]) * b[v];
     dF[r] = acc;
   }
   if constexpr (VISC == 2) {
-    dF[NV - 1] = (jf[(size_t)J::SA0 * stride] * dF[0] + jf[(size_t)(J::SA0 + 1) * stride] * s.dq[NV - 1][ai][aj]) +
-                 jf[(size_t)(J::SA0 + 2) * stride] * s.dq[NV - 1][bi][bj];
+    dF[NV - 1] = (double(jf[(size_t)J::SA0 * stride]) * dF[0] +
+                  double(jf[(size_t)(J::SA0 + 1) * stride]) * s.dq[NV - 1][ai][aj]) +
+                 double(jf[(size_t)(J::SA0 + 2) * stride]) * s.dq[NV - 1][bi][bj];
   }
   if constexpr (VISC > 0) {
     constexpr int NX = ViscShape<VISC>::NX, NR = ViscShape<VISC>::NR;
@@ -901,7 +902,7 @@ __device__ __forceinline__ void jv_face(const JvSmem<NV>& s, int axis, int ai, i
       double acc = 0.0;
 #pragma unroll
       for (int k = 0; k < NX; ++k)
-        if ((S::depends(r) >> k) & 1u) acc += jf[(size_t)(J::VBASE + S::slot(r, k)) * stride] * x[k];
+        if ((S::depends(r) >> k) & 1u) acc += double(jf[(size_t)(J::VBASE + S::slot(r, k)) * stride]) * x[k];
       dF[r < 3 ? 1 + r : NV - 1] -= acc;
     }
   }
@@ -910,7 +911,7 @@ __device__ __forceinline__ void jv_face(const JvSmem<NV>& s, int axis, int ai, i
 // out = vdt * v + dR1/dU . v with v = buffer `tangent_id` (vdt_id < 0: the bare J.v),
 // from the case's linearisation; own_ghosts: the tile evaluates its halo's tangent
 // ghosts (no tangent ghost fill needed)
-template <int NV, int VISC>
+template <int NV, int VISC, class TJ>
 __global__ void __launch_bounds__(TILE_THREADS) k_jv(const CaseDev* __restrict__ cases, int out_id, int tangent_id,
                                                      int vdt_id, int check_active, int own_ghosts) {
   __shared__ CaseDev scase;
@@ -927,7 +928,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_jv(const CaseDev* __restrict__
   const double* __restrict__ V = buf(cd, tangent_id);
   const double* __restrict__ dqg = cd.dqg;
   const double* __restrict__ vdt = vdt_id >= 0 ? buf(cd, vdt_id) : nullptr;
-  const double* __restrict__ jac = cd.jac;
+  const TJ* __restrict__ jac = static_cast<const TJ*>(cd.jac);
   const size_t stride = (size_t)cd.jstride;
   double* __restrict__ out = buf(cd, out_id);
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -990,7 +991,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_jv(const CaseDev* __restrict__
 #pragma unroll
     for (int v = 0; v < NV; ++v) dF[v] = 0.0;
     if (j < NJ && (interior_at(c, i - 1, j) || interior_at(c, i, j)))
-      jv_face<NV, VISC>(s, 0, fi, fj + 1, jac + i * NJ + j, stride, dF);
+      jv_face<NV, VISC, TJ>(s, 0, fi, fj + 1, jac + i * NJ + j, stride, dF);
 #pragma unroll
     for (int v = 0; v < NV; ++v) s.Fi[v][fi][fj] = dF[v];
   }
@@ -1002,7 +1003,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_jv(const CaseDev* __restrict__
 #pragma unroll
     for (int v = 0; v < NV; ++v) dF[v] = 0.0;
     if (i < NI && (interior_at(c, i, j - 1) || interior_at(c, i, j)))
-      jv_face<NV, VISC>(s, 1, fi + 1, fj, jac + nfi + i * (NJ + 1) + j, stride, dF);
+      jv_face<NV, VISC, TJ>(s, 1, fi + 1, fj, jac + nfi + i * (NJ + 1) + j, stride, dF);
 #pragma unroll
     for (int v = 0; v < NV; ++v) s.Fj[v][fi][fj] = dF[v];
   }
@@ -1211,6 +1212,18 @@ template <class T, int NV, bool SECOND, int VISC> static void configure_one() {
                        (int)sizeof(TileSmem<T, NV>));
 }
 
+template <class TJ> static void configure_lin() {
+  cudaFuncSetAttribute(k_linearize<5, 2, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(TileSmem<double, 5>));
+  cudaFuncSetAttribute(k_linearize<4, 1, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(TileSmem<double, 4>));
+  cudaFuncSetAttribute(k_linearize<4, 0, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(TileSmem<double, 4>));
+  cudaFuncSetAttribute(k_jv<5, 2, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(JvSmem<5>));
+  cudaFuncSetAttribute(k_jv<4, 1, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(JvSmem<4>));
+  cudaFuncSetAttribute(k_jv<4, 0, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(JvSmem<4>));
+}
+
 // the tile kernels' dynamic shared memory limits, set once before any launch or capture
 void configure_kernels() {
   static bool done = false;
@@ -1221,12 +1234,8 @@ void configure_kernels() {
   configure_one<double, 4, false, 1>();
   configure_one<double, 4, true, 0>();
   configure_one<double, 4, false, 0>();
-  cudaFuncSetAttribute(k_linearize<5, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem<double, 5>));
-  cudaFuncSetAttribute(k_linearize<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem<double, 4>));
-  cudaFuncSetAttribute(k_linearize<4, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem<double, 4>));
-  cudaFuncSetAttribute(k_jv<5, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(JvSmem<5>));
-  cudaFuncSetAttribute(k_jv<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(JvSmem<4>));
-  cudaFuncSetAttribute(k_jv<4, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(JvSmem<4>));
+  configure_lin<double>();
+  configure_lin<float>();
   done = true;
 }
 
@@ -1254,33 +1263,48 @@ void launch_residual(const CaseDev* cases, const BatchDims& d, int visc, bool se
   }
 }
 
-// The linearisation of every case's first-order residual at its U (ghosts of U filled)
-void launch_linearize(const CaseDev* cases, const BatchDims& d, int visc, cudaStream_t st) {
+// The linearisation of every case's first-order residual at its U (ghosts of U filled);
+// fp32: its face coefficients stored in single precision (the mixed form)
+template <class TJ>
+static void linearize_t(const CaseDev* cases, const BatchDims& d, int visc, cudaStream_t st) {
+  dim3 grid(d.tiles_x, d.tiles_y, d.n_cases);
+  if (visc == 2) k_linearize<5, 2, TJ><<<grid, TILE_THREADS, sizeof(TileSmem<double, 5>), st>>>(cases);
+  else if (visc == 1) k_linearize<4, 1, TJ><<<grid, TILE_THREADS, sizeof(TileSmem<double, 4>), st>>>(cases);
+  else k_linearize<4, 0, TJ><<<grid, TILE_THREADS, sizeof(TileSmem<double, 4>), st>>>(cases);
+}
+
+void launch_linearize(const CaseDev* cases, const BatchDims& d, int visc, bool fp32, cudaStream_t st) {
   dim3 ggrid(max(1, (d.ghost_records * 5 + GHOST_THREADS - 1) / GHOST_THREADS), d.n_cases);
   if (visc == 2) k_ghost_maps<5><<<ggrid, GHOST_THREADS, 0, st>>>(cases);
   else k_ghost_maps<4><<<ggrid, GHOST_THREADS, 0, st>>>(cases);
-  dim3 grid(d.tiles_x, d.tiles_y, d.n_cases);
-  if (visc == 2) k_linearize<5, 2><<<grid, TILE_THREADS, sizeof(TileSmem<double, 5>), st>>>(cases);
-  else if (visc == 1) k_linearize<4, 1><<<grid, TILE_THREADS, sizeof(TileSmem<double, 4>), st>>>(cases);
-  else k_linearize<4, 0><<<grid, TILE_THREADS, sizeof(TileSmem<double, 4>), st>>>(cases);
+  if (fp32) linearize_t<float>(cases, d, visc, st);
+  else linearize_t<double>(cases, d, visc, st);
 }
 
 // out = vdt * v + dR1/dU . v with v = buffer `tangent_id` (vdt_id < 0: the bare J.v), from
-// the linearisation launch_linearize stored; own_ghosts: the tiles map their halo's
-// tangent ghosts through the linearisation's ghost maps, but in a case with the
-// point-vortex far field, whose tangent ghosts a ghost fill (launch_ghosts) must provide
-void launch_jvp(const CaseDev* cases, const BatchDims& d, int visc, int tangent_id, int vdt_id, int out_id,
-                int check_active, int own_ghosts, cudaStream_t st) {
+// the linearisation launch_linearize stored (fp32: its coefficients in single precision,
+// every product and sum in double); own_ghosts: the tiles map their halo's tangent ghosts
+// through the linearisation's ghost maps, but in a case with the point-vortex far field,
+// whose tangent ghosts a ghost fill (launch_ghosts) must provide
+template <class TJ>
+static void jvp_t(const CaseDev* cases, const BatchDims& d, int visc, int tangent_id, int vdt_id, int out_id,
+                  int check_active, int own_ghosts, cudaStream_t st) {
   dim3 grid(d.tiles_x, d.tiles_y, d.n_cases);
   if (visc == 2)
-    k_jv<5, 2><<<grid, TILE_THREADS, sizeof(JvSmem<5>), st>>>(cases, out_id, tangent_id, vdt_id, check_active,
-                                                              own_ghosts);
+    k_jv<5, 2, TJ><<<grid, TILE_THREADS, sizeof(JvSmem<5>), st>>>(cases, out_id, tangent_id, vdt_id, check_active,
+                                                                  own_ghosts);
   else if (visc == 1)
-    k_jv<4, 1><<<grid, TILE_THREADS, sizeof(JvSmem<4>), st>>>(cases, out_id, tangent_id, vdt_id, check_active,
-                                                              own_ghosts);
+    k_jv<4, 1, TJ><<<grid, TILE_THREADS, sizeof(JvSmem<4>), st>>>(cases, out_id, tangent_id, vdt_id, check_active,
+                                                                  own_ghosts);
   else
-    k_jv<4, 0><<<grid, TILE_THREADS, sizeof(JvSmem<4>), st>>>(cases, out_id, tangent_id, vdt_id, check_active,
-                                                              own_ghosts);
+    k_jv<4, 0, TJ><<<grid, TILE_THREADS, sizeof(JvSmem<4>), st>>>(cases, out_id, tangent_id, vdt_id, check_active,
+                                                                  own_ghosts);
+}
+
+void launch_jvp(const CaseDev* cases, const BatchDims& d, int visc, bool fp32, int tangent_id, int vdt_id,
+                int out_id, int check_active, int own_ghosts, cudaStream_t st) {
+  if (fp32) jvp_t<float>(cases, d, visc, tangent_id, vdt_id, out_id, check_active, own_ghosts, st);
+  else jvp_t<double>(cases, d, visc, tangent_id, vdt_id, out_id, check_active, own_ghosts, st);
 }
 
 // the ghosts of U (tangent_id < 0) or of the tangent in buffer `tangent_id`
