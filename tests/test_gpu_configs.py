@@ -23,7 +23,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from goldens import config_state, config_vector, load, rel
+from goldens import config_state, config_vector, converged, load, rel
 
 pytestmark = pytest.mark.gpu
 
@@ -98,3 +98,26 @@ def test_forces_on_config_grids(cuda, configs, name, state):
     z, case, plan, dev = configs(name)
     f = dev.forces(config_state(z, plan, state))
     assert np.abs(f - z[f"{state}_forces"]).max() < 1e-12
+
+
+def test_converged_forces_on_config_1_grid(cuda):
+    """Config 1 (o_euler_257: Euler, HLLC with van Albada, residual tolerance 1e-10) run
+    from the freestream to the reference's own exit test on the device: CL, CD and CM
+    against the reference's converged run on the same grid (tests/golden/
+    o_euler_257_converged.npz: converged after 3840 Newton steps, the residual 10.06
+    orders below its peak; CL 0.3453720421, CD 0.0226314963, CM -0.0375774112), 1e-6."""
+    from jaxrans_b200.native import DevicePlan
+    from jaxrans_b200.solver import march
+    ref = converged("o_euler_257")
+    assert ref is not None and str(ref["reason"]) == "converged"
+    z, case, plan = load("o_euler_257")
+    dev = DevicePlan(plan, case.flow, case.numerics, case.implicit)
+    try:
+        result = march(case, plan, device=dev)
+    finally:
+        dev.close()
+    assert result.history.reason in ("converged", "settled")
+    f = result.forces
+    assert abs(f.cl - ref["forces"][0]) < 1e-6
+    assert abs(f.cd - ref["forces"][1]) < 1e-6
+    assert abs(f.cm - ref["forces"][2]) < 1e-6
