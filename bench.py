@@ -269,6 +269,24 @@ def oracle3d_step_seconds(steps: int, warmup: int):
     return statistics.mean(times), plan.cells
 
 
+def jvp3d_bytes_per_cell(nvar: int) -> int:
+    """Algorithmic bytes per cell of one 3D J.v (every launch of jr_jvp3d: primitive canvas,
+    ghost stages, face phase, cell phase): U and v read, J.v written (3 nvar), the volume,
+    the three face vectors a cell owns (9), the centre (3) and the wall distance, FP64."""
+    return 8 * (3 * nvar + 1 + 9 + 3 + 1)
+
+
+def roofline3d(kern: dict, nvar: int, cells: int, peaks: dict) -> dict:
+    """The 3D J.v's achieved HBM bandwidth (its algorithmic bytes over the CUDA-event time of
+    the whole jr_jvp3d sequence) against the measured copy bandwidth."""
+    per_cell = jvp3d_bytes_per_cell(nvar)
+    achieved = per_cell * cells / (kern["jvp3d"] * 1e-3) / 1e9
+    return {"kernel": "jvp3d (primitive canvas, ghost stages, face phase, cell phase)", "bound": "hbm",
+            "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+            "traffic": None, "algorithmic_bytes_per_cell": per_cell, "algorithmic_bytes_per_launch": per_cell * cells,
+            "launch_ms": kern["jvp3d"], "peak_source": peaks.get("source", "measured")}
+
+
 def run_wing3d(args) -> int:
     """``--workload wing_ch_4blk``: K pseudo-transient Newton steps of the 3D wing
     (``jr_newton_steps3d``, GMRES with the line preconditioner, host-driven: the step
@@ -336,6 +354,7 @@ def run_wing3d(args) -> int:
         seconds = time.perf_counter() - t0
     dev.lib.jr_launches3d(C.byref(launches))
     launched = launches.value - before
+    kern3 = dev.time_kernels(U_dev.cpu().numpy(), 5)
     U_host, c2, r2 = U0.copy(), case.implicit.cfl, math.inf
     barrier()
     torch.cuda.synchronize()
@@ -366,7 +385,9 @@ def run_wing3d(args) -> int:
                        "timer": "host clock between device synchronisations (the 3D step is host-driven)"},
             "e2e": {"value": world * args.steps / e2e_seconds, "unit": "steps/s",
                     "h2d_bytes_per_step": bytes_per_step, "d2h_bytes_per_step": bytes_per_step},
-            "gpu_launches": launched, "roofline": None, "cpu_baseline": cpu, "clocks": clocks.summary()}),
+            "gpu_launches": launched, "kernel_ms": kern3,
+            "roofline": roofline3d(kern3, int(U0.shape[0]), plan.cells, measured_peaks()),
+            "cpu_baseline": cpu, "clocks": clocks.summary()}),
             flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -374,10 +395,13 @@ def run_wing3d(args) -> int:
     return 0
 
 
-def roofline_of(kern: dict, model: str, nvar: int, cells: int, peaks: dict, kernel: str = "jvp_tile") -> dict:
+def roofline_of(kern: dict, model: str, nvar: int, cells: int, peaks: dict, kernel: str = "jvp_tile",
+                fp32_faces: bool = False) -> dict:
     """A tile kernel's achieved HBM bandwidth: its algorithmic bytes per launch over its
-    CUDA-event launch time, against the measured copy bandwidth."""
-    per_cell = jvp_bytes_per_cell(model, nvar) if kernel == "jvp_tile" else residual_bytes_per_cell(model, nvar)
+    CUDA-event launch time, against the measured copy bandwidth (fp32_faces: the J.v of
+    the mixed form, its face coefficients in FP32)."""
+    per_cell = (jvp_bytes_per_cell(model, nvar, fp32_faces) if kernel == "jvp_tile"
+                else residual_bytes_per_cell(model, nvar))
     achieved = per_cell * cells / (kern[kernel] * 1e-3) / 1e9
     return {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / peaks["hbm_gbs"], "traffic": None, "algorithmic_bytes_per_cell": per_cell,
@@ -385,14 +409,15 @@ def roofline_of(kern: dict, model: str, nvar: int, cells: int, peaks: dict, kern
             "peak_source": peaks.get("source", "measured")}
 
 
-def measure_forms(fp64_value: float, fp64_forces, served_requests: int = 24) -> dict:
+def measure_forms(fp64_value: float, fp64_forces, peaks: dict, served_requests: int = 24) -> dict:
     """The north-star forms beside the plain FP64 line, each bounded to a few minutes:
 
     * batched, mixed: the 19 cases of ``polar16_uneven`` (16 angles on the 385 x 97 grid and
       the 257, 513 and 769 uneven grids) in one device plan, FP32 line preconditioner and
       Krylov basis, each case leaving the launches at its own exit; solves/hr of the whole
-      batch (device clock), the cases' exit times (p50, p99), and |dCL|, |dCD| of its 8 deg
-      case against the FP64 line's forces;
+      batch (device clock), the cases' exit times (p50, p99), |dCL|, |dCD| of its 8 deg
+      case against the FP64 line's forces, and the J.v and residual tiles' rooflines over
+      the batch's 819k cells (each tile timed live with CUDA events on the batch);
     * served: a seeded Poisson stream (20 requests/s) of ``served_requests`` SA requests of
       the config-4 distribution (van Albada), mixed, continuous batching with up to
       ``served_requests`` slots per grid size; solves/hr over the stream's wall time,
@@ -423,7 +448,11 @@ def measure_forms(fp64_value: float, fp64_forces, served_requests: int = 24) -> 
     s1.record(stream)
     torch.cuda.synchronize()
     wall = s0.elapsed_time(s1) / 1e3
+    for k in range(len(cases)):   # the finished cases back in the launches, for the kernel times
+        dev.enable(k, True)
+    kern = dev.time_kernels(10)
     dev.close()
+    batch_cells = sum(g.cells for g in grids)
     lat = [m.seconds * wall / seconds for m in monitors]
     k8 = [round(c.flow.alpha_deg, 6) for c in cases].index(8.0)
     f8 = monitors[k8].forces
@@ -436,7 +465,10 @@ def measure_forms(fp64_value: float, fp64_forces, served_requests: int = 24) -> 
         "exits": {r: sum(m.reason == r for m in monitors) for r in sorted({m.reason for m in monitors})},
         "alpha8_vs_fp64_line": {"dcl": abs(f8.cl - fp64_forces["cl"]), "dcd": abs(f8.cd - fp64_forces["cd"]),
                                 "note": "settled (minmod) states: the state the forces settle on depends "
-                                        "on the path, by about 5e-4 in CL between FP64 runs too"}}
+                                        "on the path, by about 5e-4 in CL between FP64 runs too"},
+        "kernel_ms": kern,
+        "roofline": roofline_of(kern, "sa", 5, batch_cells, peaks, fp32_faces=True),
+        "roofline_residual": roofline_of(kern, "sa", 5, batch_cells, peaks, kernel="residual_tile")}
     # served, mixed, continuous batching
     template = workload("c_sa_385", **{"implicit.precision": "mixed", "convective_fluxes.limiter": "van_albada"})
     requests = poisson_requests(served_requests, template, 20.0, seed=0)
@@ -462,7 +494,7 @@ def measure_forms(fp64_value: float, fp64_forces, served_requests: int = 24) -> 
         "solves_per_hr": summ["solves_per_hr"], "p50_s": summ["p50_s"], "p99_s": summ["p99_s"],
         "exits": summ["exits"], "seconds": wall,
         "plain_fp64_first3": {"solves_per_hr": plain_rate, "max_dcl": max(dcl), "max_dcd": max(dcd)},
-        "ratio_to_plain_fp64_same_requests": summ["solves_per_hr"] / plain_rate}
+        "ratio_to_plain_fp64_first3": summ["solves_per_hr"] / plain_rate}
     return out
 
 
@@ -646,7 +678,7 @@ def run_device(args) -> int:
         result["clocks"] = clocks.summary()
         if world == 1 and n_cases == 1 and not args.no_forms and args.workload == "c_sa_385" \
                 and args.precision == "fp64":
-            result["forms"] = measure_forms(value, config["forces"])
+            result["forms"] = measure_forms(value, config["forces"], peaks)
         if world == 1 and not args.no_cpu_baseline:
             from jaxrans_b200.workloads import BATCHES
             name = BATCHES[args.workload][0][0] if args.workload in BATCHES else args.workload

@@ -373,6 +373,12 @@ int jr_wall_distance3d(const double* points, int64_t n_points, const double* fac
 /* Kernels the 3D plan entry points (residual, J.v, wave speeds, line solve, Newton steps,
  * forces) have launched since the library was loaded (counted on the host). */
 int jr_launches3d(int64_t* out);
+/* Average milliseconds per call, over `reps` calls after one untimed call, with CUDA events
+ * on the plan's stream, at U (device): ms (host, 3) = the residual R2 (ghost stages,
+ * face phase, cell phase), the J.v of R1 along U itself, and the line preconditioner
+ * (factor and solve) at CFL 25.  Synchronises; allocates two work vectors for the call.
+ * No counterpart in the reference (its scripts/benchmark.py times the jitted calls). */
+int jr_time_kernels3d(jr_plan3d* plan, const double* U, int32_t reps, double* ms);
 
 #ifdef __cplusplus
 }

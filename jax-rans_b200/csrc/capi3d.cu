@@ -329,6 +329,40 @@ int jr_wall_loads3d(jr_plan3d* plan, const double* U, double* out) {
   return check3("jr_wall_loads3d");
 }
 
+int jr_time_kernels3d(jr_plan3d* plan, const double* U, int32_t reps, double* ms) {
+  if (!plan || !U || !ms || reps < 1) return report_error(JR_EINVAL, "bad argument");
+  const size_t N = (size_t)plan->dev.nvar * plan->n_canvas;
+  double *v = nullptr, *out = nullptr;
+  if (cudaMalloc(&v, N * sizeof(double)) != cudaSuccess || cudaMalloc(&out, N * sizeof(double)) != cudaSuccess) {
+    cudaFree(v);
+    return report_error(JR_ENOMEM, "cudaMalloc failed");
+  }
+  cudaMemcpyAsync(v, U, N * sizeof(double), cudaMemcpyDeviceToDevice, plan->st);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  auto timed = [&](int k, auto&& launch) {
+    launch();
+    cudaEventRecord(e0, plan->st);
+    for (int r = 0; r < reps; ++r) launch();
+    cudaEventRecord(e1, plan->st);
+    cudaEventSynchronize(e1);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    ms[k] = (double)t / reps;
+  };
+  const double cfl = 25.0;
+  timed(0, [&] { launch_residual3(plan->dev, U, out, plan->A, false, plan->st); });
+  timed(1, [&] { launch_jvp3(plan->dev, U, v, out, plan->A, plan->st); });
+  timed(2, [&] { launch_precondition3(plan->dev, U, cfl, v, out, plan->factor, plan->st); });
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamSynchronize(plan->st);
+  cudaFree(v);
+  cudaFree(out);
+  return check3("jr_time_kernels3d");
+}
+
 int jr_launches3d(int64_t* out) {
   if (!out) return report_error(JR_EINVAL, "null argument");
   *out = launches3();

@@ -65,7 +65,8 @@ EXPORTS = ("jr_plan_create", "jr_plan_destroy", "jr_last_error", "jr_plan_sizes"
            "jr_launch_count", "jr_autotune", "jr_line_schedule", "jr_wait_limit_check", "jr_wall_loads",
            "jr_plan3d_create", "jr_plan3d_destroy", "jr_residual3d", "jr_jvp3d", "jr_wave_speeds3d",
            "jr_precondition3d", "jr_newton_steps3d", "jr_forces3d", "jr_wall_distance3d",
-           "jr_launches3d", "jr_wall_loads3d", "jr_monitor_set", "jr_monitor_blocks", "jr_monitor_get", "jr_norm")
+           "jr_launches3d", "jr_wall_loads3d", "jr_monitor_set", "jr_monitor_blocks", "jr_monitor_get", "jr_norm",
+           "jr_time_kernels3d")
 
 TIMED_KERNELS = ("residual_tile", "jvp_tile", "ghosts_tangent", "line_apply", "line_factor", "cgs2_full_basis",
                  "linearize")
@@ -137,6 +138,7 @@ def load_library(path: Path | None = None) -> C.CDLL:
         "jr_forces3d": (C.c_int, [vp, vp, C.c_double, C.c_double, vp, vp]),
         "jr_wall_distance3d": (C.c_int, [vp, C.c_int64, vp, C.c_int32, vp]),
         "jr_launches3d": (C.c_int, [vp]),
+        "jr_time_kernels3d": (C.c_int, [vp, vp, C.c_int32, _f64p]),
         "jr_wall_loads3d": (C.c_int, [vp, vp, vp]),
         "jr_wall_loads": (C.c_int, [vp, vp, vp]),
         "jr_time_kernels": (C.c_int, [vp, C.c_int32, _f64p]),

@@ -235,6 +235,15 @@ class DevicePlan3:
                                                      hist.ctypes.data), "jr_newton_steps3d")
         return u.cpu().numpy(), c.value, r.value, hist
 
+    def time_kernels(self, U, reps: int = 5) -> dict:
+        """Average ms per call at ``U`` (``jr_time_kernels3d``, CUDA events on the plan's
+        stream): the residual R2, the J.v of R1 and the line preconditioner."""
+        (u,), _ = self._run("jr_time_kernels3d", U)
+        ms = np.zeros(3)
+        _check(self.lib, self.lib.jr_time_kernels3d(self.handle, u.data_ptr(), int(reps), ms.ctypes.data_as(_f64p)),
+               "jr_time_kernels3d")
+        return dict(zip(("residual3d", "jvp3d", "line_precondition3d"), ms.tolist()))
+
     # -- a state kept on the device between calls (the march's blocks)
     def set_state(self, U, cfl: float, residual_norm: float = float("inf")) -> None:
         """Keep ``U`` on the device with the step's CFL and previous |R|."""

@@ -180,3 +180,15 @@ def test_make_residual_on_a_3d_plan(cuda, blocks3d):
         assert np.abs(R[k][inside] - ref).max() <= 1e-12 * np.abs(ref).max()
     U0 = op.initial_state()
     assert U0.shape == (6,) + plan.shape and np.isfinite(op.norm(op.residual(U0)))
+
+
+def test_time_kernels3d_leaves_the_results_alone(cuda, device3d):
+    """jr_time_kernels3d times the residual, J.v and line preconditioner on its own work
+    vectors: every time is positive, and the residual at the same state is unchanged."""
+    z, dev = device3d
+    U = z["sin_U"]
+    before = dev.residual(U)
+    ms = dev.time_kernels(U, 2)
+    assert set(ms) == {"residual3d", "jvp3d", "line_precondition3d"}
+    assert all(v > 0.0 for v in ms.values())
+    assert np.array_equal(dev.residual(U), before)
