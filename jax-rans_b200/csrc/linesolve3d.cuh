@@ -402,7 +402,7 @@ inline __host__ __device__ void wall_load(const Plan3Dev& p, const double* Q, in
   for (int m = 0; m < 3; ++m) out[4 + m] = 0.0;
   if (p.P.mu_inf > 0.0) {
     double grad[3][5];
-    face_gradient<double>(p, Q, a, i, j, k, 4, grad);
+    face_gradient<double, 4>(p, Q, a, i, j, k, grad);
     int lo[3] = {i, j, k};
     lo[a] -= 1;
     double ql[NV3_MAX], qh[NV3_MAX];

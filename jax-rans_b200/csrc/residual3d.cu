@@ -36,10 +36,32 @@ __global__ void k3_ghost_store(Plan3Dev p, const T* __restrict__ buf, int r0, in
 }
 
 // phase 1: every face's flux once (one thread per face of the three families)
-template <class T, bool VISC, bool SA>
-__global__ void __launch_bounds__(128) k3_face_flux(Plan3Dev p, const T* __restrict__ Q, int first_order, int nf) {
+// (FO 1: the first-order flux, 2: second order; PART 0: the whole flux, 1: its inviscid
+// part, 2: its viscous part added to the stored inviscid part)
+template <class T, bool VISC, bool SA, int FO, int PART>
+__global__ void __launch_bounds__(128) k3_face_flux(Plan3Dev p, const T* __restrict__ Q, int nf) {
   for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += gridDim.x * blockDim.x)
-    store_face_flux<T, VISC, SA>(p, Q, first_order, f, p.face_buf, (size_t)nf);
+    store_face_flux<T, VISC, SA, FO, PART>(p, Q, FO == 1, f, p.face_buf, (size_t)nf);
+}
+
+// A viscous flux in two launches (inviscid, then viscous added): each holds half the
+// live values of the whole, so neither spills the way the fused face did.
+template <class T, bool VISC, bool SA, int FO>
+static void face_parts(const Plan3Dev& p, const T* A, int nf, cudaStream_t st) {
+  const int fblocks = (nf + 127) / 128;
+  if constexpr (VISC) {
+    counted3();
+    k3_face_flux<T, VISC, SA, FO, 1><<<fblocks, 128, 0, st>>>(p, A, nf);
+    k3_face_flux<T, VISC, SA, FO, 2><<<fblocks, 128, 0, st>>>(p, A, nf);
+  } else {
+    k3_face_flux<T, VISC, SA, FO, 0><<<fblocks, 128, 0, st>>>(p, A, nf);
+  }
+}
+
+template <class T, bool VISC, bool SA>
+static void face_phase(const Plan3Dev& p, const T* A, bool first_order, int nf, cudaStream_t st) {
+  if (first_order) face_parts<T, VISC, SA, 1>(p, A, nf, st);
+  else face_parts<T, VISC, SA, 2>(p, A, nf, st);
 }
 
 // phase 2: each cell's sum of its faces' fluxes (and the SA source)
@@ -77,14 +99,13 @@ static void residual3_t(const Plan3Dev& p, const double* U, const double* dU, do
   fill3(p, A, st);
   const bool visc = p.P.mu_inf > 0.0, sa = p.nvar > 5;
   const int nf = face_count(p, 0) + face_count(p, 1) + face_count(p, 2);
-  const int fblocks = (nf + 127) / 128;
   counted3();   // the face phase (the cell phase is counted with the primitive canvas)
   if (sa)
-    k3_face_flux<T, true, true><<<fblocks, 128, 0, st>>>(p, A, first_order, nf);
+    face_phase<T, true, true>(p, A, first_order, nf, st);
   else if (visc)
-    k3_face_flux<T, true, false><<<fblocks, 128, 0, st>>>(p, A, first_order, nf);
+    face_phase<T, true, false>(p, A, first_order, nf, st);
   else
-    k3_face_flux<T, false, false><<<fblocks, 128, 0, st>>>(p, A, first_order, nf);
+    face_phase<T, false, false>(p, A, first_order, nf, st);
   if (sa)
     k3_cell_sum<T, true><<<blocks, 128, 0, st>>>(p, A, U, dU, R, nf);
   else

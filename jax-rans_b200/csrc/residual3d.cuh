@@ -141,6 +141,32 @@ __host__ __device__ __forceinline__ void grad_vars(const Plan3Dev& p, const T* Q
   if (p.nvar > 5) phi[4] = Q[(size_t)5 * n + c];
 }
 
+// component m of grad_vars at cell c (the same arithmetic, one component)
+template <class T>
+__host__ __device__ __forceinline__ T grad_var(const Plan3Dev& p, const T* Q, int c, int m) {
+  const int n = p.NI * p.NJ * p.NK;
+  if (m < 3) return Q[(size_t)(1 + m) * n + c];
+  if (m == 3) return p.P.gamma * Q[(size_t)4 * n + c] / Q[c];
+  return Q[(size_t)5 * n + c];
+}
+
+// component m of node_phi: the same three halvings of the eight cells' values, one
+// component at a time (a face's gradient then never holds all eight cells' values)
+template <class T>
+__host__ __device__ __forceinline__ T node_phi_m(const Plan3Dev& p, const T* Q, int I, int J, int K, int m) {
+  T jk[2][2];
+#pragma unroll
+  for (int b = 0; b < 2; ++b)
+#pragma unroll
+    for (int d = 0; d < 2; ++d)
+      jk[b][d] = 0.5 * (grad_var(p, Q, cell_index(p, I - 1, J - 1 + b, K - 1 + d), m) +
+                        grad_var(p, Q, cell_index(p, I, J - 1 + b, K - 1 + d), m));
+  T kk[2];
+#pragma unroll
+  for (int d = 0; d < 2; ++d) kk[d] = 0.5 * (jk[0][d] + jk[1][d]);
+  return 0.5 * (kk[0] + kk[1]);
+}
+
 template <class T>
 __host__ __device__ __forceinline__ void node_phi(const Plan3Dev& p, const T* Q, int I, int J, int K, int nphi, T out[5]) {
   T c[2][2][2][5];
@@ -165,8 +191,9 @@ __host__ __device__ __forceinline__ void cross3(const double a[3], const double 
 
 // The diamond gradient at face (fi, fj, fk) of family a: grad[d][m] = d phi_m / d x_d
 // (src/jaxrans/numerics/gradients.py:59-95).
-template <class T>
-__host__ __device__ void face_gradient(const Plan3Dev& p, const T* Q, int a, int fi, int fj, int fk, int nphi, T grad[3][5]) {
+template <class T, int NPHI>
+__host__ __device__ __forceinline__ void face_gradient(const Plan3Dev& p, const T* Q, int a, int fi, int fj, int fk,
+                                                       T grad[3][5]) {
   int lo[3] = {fi, fj, fk}, hi[3] = {fi, fj, fk};
   lo[a] -= 1;
   double xl[3], xh[3];
@@ -194,11 +221,6 @@ __host__ __device__ void face_gradient(const Plan3Dev& p, const T* Q, int a, int
   node_centre(p, n11[0], n11[1], n11[2], x11);
   node_centre(p, n10[0], n10[1], n10[2], x10);
   node_centre(p, n01[0], n01[1], n01[2], x01);
-  T f00[5], f11[5], f10[5], f01[5];
-  node_phi(p, Q, n00[0], n00[1], n00[2], nphi, f00);
-  node_phi(p, Q, n11[0], n11[1], n11[2], nphi, f11);
-  node_phi(p, Q, n10[0], n10[1], n10[2], nphi, f10);
-  node_phi(p, Q, n01[0], n01[1], n01[2], nphi, f01);
   double d1[3], d2[3], d3[3];
   for (int m = 0; m < 3; ++m) {
     d1[m] = xh[m] - xl[m];
@@ -210,8 +232,12 @@ __host__ __device__ void face_gradient(const Plan3Dev& p, const T* Q, int a, int
   cross3(d3, d1, c31);
   cross3(d1, d2, c12);
   const double det = d1[0] * c23[0] + d1[1] * c23[1] + d1[2] * c23[2];
-  for (int m = 0; m < nphi; ++m) {
-    T p1 = ph[m] - pl[m], p2 = f11[m] - f00[m], p3 = f01[m] - f10[m];
+#pragma unroll
+  for (int m = 0; m < NPHI; ++m) {
+    const T f00 = node_phi_m(p, Q, n00[0], n00[1], n00[2], m), f11 = node_phi_m(p, Q, n11[0], n11[1], n11[2], m);
+    const T f10 = node_phi_m(p, Q, n10[0], n10[1], n10[2], m), f01 = node_phi_m(p, Q, n01[0], n01[1], n01[2], m);
+    T p1 = ph[m] - pl[m], p2 = f11 - f00, p3 = f01 - f10;
+#pragma unroll
     for (int d = 0; d < 3; ++d) grad[d][m] = (p1 * c23[d] + p2 * c31[d] + p3 * c12[d]) / det;
   }
 }
@@ -220,6 +246,15 @@ template <class T>
 __host__ __device__ __forceinline__ void load_cell(const Plan3Dev& p, const T* Q, int c, T q[NV3_MAX]) {
   const int n = p.NI * p.NJ * p.NK;
   for (int v = 0; v < p.nvar; ++v) q[v] = Q[(size_t)v * n + c];
+}
+
+// the same with the variable count known at compile time (the plan's nvar: 6 with SA,
+// else 5), so the cell's values stay in registers
+template <int NV, class T>
+__host__ __device__ __forceinline__ void load_cell_n(const Plan3Dev& p, const T* Q, int c, T q[NV3_MAX]) {
+  const int n = p.NI * p.NJ * p.NK;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) q[v] = Q[(size_t)v * n + c];
 }
 
 // The net flux through face (fi, fj, fk) of family a (inviscid minus viscous), and for
@@ -251,22 +286,40 @@ __host__ __device__ __forceinline__ void qcr_extra(const T grad[3][5], const T& 
     for (int b = 0; b < 3; ++b) extra[a][b] = -c_cr1 * (prod[a][b] + prod[b][a]);
 }
 
-template <class T, bool VISC, bool SA>
-__host__ __device__ void face_flux(const Plan3Dev& p, const T* Q, int a, int fi, int fj, int fk, bool first_order, T F[NV3_MAX]) {
+// FO: 1 first order, 2 second order, 0 as `first_order` says (the kernels fix it at
+// compile time, so a first-order flux loads only the two cells either side).  PART: 0 the
+// whole flux; 1 its inviscid part (with the SA row's upwind convection); 2 its viscous
+// part alone, the terms the whole flux subtracts, negated (0 - term), so that part 1 plus
+// part 2 is the whole flux bitwise (a + (0 - b) == a - b).
+template <class T, bool VISC, bool SA, int FO = 0, int PART = 0>
+__host__ __device__ void face_flux(const Plan3Dev& p, const T* Q, int a, int fi, int fj, int fk, bool first_order_arg,
+                                   T F[NV3_MAX]) {
+  constexpr int NV = SA ? 6 : 5;
+  const bool first_order = FO == 0 ? first_order_arg : FO == 1;
   const Physics3& P = p.P;
   const double g = P.gamma;
   int idx[4];
+#pragma unroll
   for (int o = 0; o < 4; ++o) {
     int c[3] = {fi, fj, fk};
     c[a] += o - 2;
     idx[o] = cell_index(p, c[0], c[1], c[2]);
   }
   T qmm[NV3_MAX], qm[NV3_MAX], qp[NV3_MAX], qpp[NV3_MAX];
-  load_cell(p, Q, idx[0], qmm);
-  load_cell(p, Q, idx[1], qm);
-  load_cell(p, Q, idx[2], qp);
-  load_cell(p, Q, idx[3], qpp);
+  load_cell_n<NV>(p, Q, idx[1], qm);
+  load_cell_n<NV>(p, Q, idx[2], qp);
+  if (PART != 2 && !first_order) {
+    load_cell_n<NV>(p, Q, idx[0], qmm);
+    load_cell_n<NV>(p, Q, idx[3], qpp);
+  }
+  double s[3];
+  face_vector(p, a, fi, fj, fk, s);
+  if constexpr (PART == 2) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) F[v] = cst<T>(0.0);
+  } else {
   T qL[5], qR[5];
+#pragma unroll
   for (int v = 0; v < 5; ++v) {
     if (first_order) {
       qL[v] = qm[v];
@@ -282,16 +335,18 @@ __host__ __device__ void face_flux(const Plan3Dev& p, const T* Q, int a, int fi,
       qR[v] = qp[v] - 0.5 * limit(dd, dp, P.limiter);
     }
   }
-  double s[3];
-  face_vector(p, a, fi, fj, fk, s);
   T Fi[5];
   riemann3(P.flux, qL, qR, s, g, Fi);
   for (int v = 0; v < 5; ++v) F[v] = Fi[v];
-  if (p.nvar > 5) F[5] = cst<T>(0.0);
-  if constexpr (VISC) {
-    const int nphi = SA ? 5 : 4;
+  if constexpr (NV > 5) F[5] = cst<T>(0.0);
+  if constexpr (SA) {
+    T up = val(Fi[0]) > 0.0 ? qm[5] : qp[5];
+    F[5] = Fi[0] * up;
+  }
+  }
+  if constexpr (VISC && PART != 1) {
     T grad[3][5];
-    face_gradient(p, Q, a, fi, fj, fk, nphi, grad);
+    face_gradient<T, SA ? 5 : 4>(p, Q, a, fi, fj, fk, grad);
     // face means of the two cells either side
     T extra[3][3];
     T vel[3], Tl = g * qm[4] / qm[0], Th = g * qp[4] / qp[0];
@@ -332,11 +387,10 @@ __host__ __device__ void face_flux(const Plan3Dev& p, const T* Q, int a, int fi,
     if constexpr (SA) {
       T fa[NV3_MAX];
       for (int v = 0; v < 6; ++v) fa[v] = 0.5 * (qm[v] + qp[v]);
-      T up = val(Fi[0]) > 0.0 ? qm[5] : qp[5];
       T mu_f = viscosity3(P, g * fa[4] / fa[0]);
       T coef = diffusion_coefficient(P.sa, fa[0], fa[5] * P.mu_inf, mu_f);
       T gn = grad[0][4] * s[0] + grad[1][4] * s[1] + grad[2][4] * s[2];
-      F[5] = Fi[0] * up - coef * gn;
+      F[5] = F[5] - coef * gn;
     }
   }
 }
@@ -353,9 +407,9 @@ __host__ __device__ T sa_cell_source(const Plan3Dev& p, const T* __restrict__ Q,
     lo[a] -= 1;
     hi[a] += 1;
     T qc[NV3_MAX], ql[NV3_MAX], qh[NV3_MAX];
-    load_cell(p, Q, c, qc);
-    load_cell(p, Q, cell_index(p, lo[0], lo[1], lo[2]), ql);
-    load_cell(p, Q, cell_index(p, hi[0], hi[1], hi[2]), qh);
+    load_cell_n<6>(p, Q, c, qc);
+    load_cell_n<6>(p, Q, cell_index(p, lo[0], lo[1], lo[2]), ql);
+    load_cell_n<6>(p, Q, cell_index(p, hi[0], hi[1], hi[2]), qh);
     for (int m = 0; m < 3; ++m) {
       lo_s[a][m] = 0.5 * (ql[1 + m] + qc[1 + m]);
       hi_s[a][m] = 0.5 * (qc[1 + m] + qh[1 + m]);
@@ -429,9 +483,11 @@ __host__ __device__ void residual_cell(const Plan3Dev& p, const T* __restrict__ 
 // Dual its tangent -- stored at Fb[v * nf + flat], for a face with a block cell on
 // either side (no cell reads the others).  Every face is evaluated once instead of once
 // from each side, with the same arithmetic, so phase 2's sums are residual_cell's.
-template <class T, bool VISC, bool SA>
+// (PART 2: the viscous part added to the stored inviscid part; the mass row has none)
+template <class T, bool VISC, bool SA, int FO = 0, int PART = 0>
 __host__ __device__ void store_face_flux(const Plan3Dev& p, const T* __restrict__ Q, int first_order, int flat,
                                          double* __restrict__ Fb, size_t nf) {
+  constexpr int NV = SA ? 6 : 5;
   int a, i, j, k;
   face_of(p, flat, a, i, j, k);
   int h[3] = {i, j, k}, l[3] = {i, j, k};
@@ -441,8 +497,14 @@ __host__ __device__ void store_face_flux(const Plan3Dev& p, const T* __restrict_
   const bool lo_in = l[a] >= 0 && p.interior[(l[0] * p.NJ + l[1]) * p.NK + l[2]];
   if (!hi_in && !lo_in) return;
   T F[NV3_MAX];
-  face_flux<T, VISC, SA>(p, Q, a, i, j, k, first_order != 0, F);
-  for (int v = 0; v < p.nvar; ++v) Fb[(size_t)v * nf + flat] = tangent_or_value(F[v]);
+  face_flux<T, VISC, SA, FO, PART>(p, Q, a, i, j, k, first_order != 0, F);
+  if constexpr (PART == 2) {
+#pragma unroll
+    for (int v = 1; v < NV; ++v) Fb[(size_t)v * nf + flat] = Fb[(size_t)v * nf + flat] + tangent_or_value(F[v]);
+  } else {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Fb[(size_t)v * nf + flat] = tangent_or_value(F[v]);
+  }
 }
 
 // Phase 2: R of cell c from the stored face fluxes (residual_cell's sums and SA source)
@@ -457,20 +519,25 @@ __host__ __device__ void residual_cell_from_faces(const Plan3Dev& p, const T* __
       R[(size_t)v * n + c] = dU ? dU[(size_t)v * n + c] : U[(size_t)v * n + c] - p.P.U_inf[v];
     return;
   }
+  constexpr int NV = SA ? 6 : 5;
   const int i = c / (p.NJ * p.NK), j = (c / p.NK) % p.NJ, k = c % p.NK;
   double acc[NV3_MAX];
-  for (int v = 0; v < p.nvar; ++v) acc[v] = 0.0;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+#pragma unroll
   for (int a = 0; a < 3; ++a) {
     int f1[3] = {i, j, k};
     f1[a] += 1;
     const int lo = face_flat(p, a, i, j, k), hi = face_flat(p, a, f1[0], f1[1], f1[2]);
-    for (int v = 0; v < p.nvar; ++v) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
       const double d = Fb[(size_t)v * nf + hi] - Fb[(size_t)v * nf + lo];
       acc[v] = a == 0 ? d : acc[v] + d;
     }
   }
   if constexpr (SA) acc[5] = acc[5] - tangent_or_value(sa_cell_source(p, Q, c));
-  for (int v = 0; v < p.nvar; ++v) R[(size_t)v * n + c] = acc[v];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) R[(size_t)v * n + c] = acc[v];
 }
 
 }  // namespace jr
