@@ -1,11 +1,15 @@
 """Serving: a request loop with continuous batching.
 
 Requests (2D cases, each with its own section, grid size and flow) arrive over time.
-A pool per grid size holds a device batch of slots (``jr_batch_create``); its slot count
-is set by the free device memory when the pool is first needed.  A request is admitted
-as soon as it has arrived and a slot of its grid size is free: the slot's static tables
-are overwritten with the request's grid (``jr_case_load``), its state reset to the
-request's freestream, and it joins the next block of Newton steps.  Every pool steps all
+Pools of device slots (each a device batch, ``jr_batch_create``) hold the requests of one
+grid size.  A request is admitted as soon as it has arrived and a slot of its grid size
+is free: the slot's static tables are overwritten with the request's grid
+(``jr_case_load``), its state reset to the request's freestream, and it joins the next
+block of Newton steps.  When every slot of its size is taken, another pool of that size
+is made if the free device memory allows (``Admission``: a share of the free memory,
+keeping room for the grid sizes not seen yet); otherwise the request waits, and while a
+request waits for memory, pools that have gone idle and whose size has no request
+waiting are released, so the memory moves to the sizes in demand.  Every pool steps all
 its live slots with one captured graph per Newton step, on its own stream, so the pools'
 work overlaps on the device.  After each block the host runs each live request's exit
 test (``jaxrans_b200.solver.CaseMonitor``, the exit test of a single run); a finished
@@ -137,13 +141,41 @@ class Pool:
         return any(h is not None for h in self.holder)
 
 
+@dataclass
+class Admission:
+    """The serving loop's use of device memory: how many slots a new pool gets, and which
+    idle pools give their memory back.
+
+    A new pool of grid size ``key`` gets ``memory_fraction`` of the free memory, shared
+    with the grid sizes (of ``n_classes``) that have no pool yet, in slots of
+    ``per_slot`` bytes, at most ``max_slots``; none (the request waits) when not one slot
+    fits.  While some request waits for memory (``starved`` sizes), the pools with no
+    live slot whose size has no request waiting (``waiting`` sizes) are released."""
+
+    max_slots: int = 64
+    memory_fraction: float = 0.8
+    n_classes: int = 4
+
+    def new_pool_slots(self, free: int, per_slot: int, key, keys_with_pools) -> int:
+        unseen = max(0, self.n_classes - len(set(keys_with_pools) | {key}))
+        share = self.memory_fraction * free / (1 + unseen)
+        return int(max(0, min(self.max_slots, share // max(1, per_slot))))
+
+    @staticmethod
+    def releasable(pools, starved, waiting) -> list:
+        if not starved:
+            return []
+        return [p for p in pools if not p.live and p.key not in waiting]
+
+
 def build_grid(case: Case) -> Plan:
     """A request's grid and plan tables (run in a worker process)."""
     return case.grid()
 
 
 class Server:
-    """Continuous batching of requests over pools of device slots, one pool per grid size.
+    """Continuous batching of requests over pools of device slots, pools per grid size
+    made and released by the free device memory (``Admission``).
 
     ``max_slots`` caps a pool; ``memory_fraction`` of the free device memory, shared by
     the grid sizes still without a pool, bounds it when the pool is made.  Each request's
@@ -152,27 +184,54 @@ class Server:
 
     def __init__(self, max_slots: int = 64, memory_fraction: float = 0.8, block_iters: int | None = None,
                  n_classes: int = len(GRID_CLASSES), workers: int = 4):
-        self.max_slots, self.memory_fraction = max_slots, memory_fraction
-        self.n_classes, self.workers = n_classes, workers
+        self.admission = Admission(max_slots, memory_fraction, n_classes)
+        self.workers = workers
         self.block_iters = block_iters
-        self.pools: dict = {}
+        self.pools: list[Pool] = []
+        self.made = 0        # pools made over the stream
+        self.released = 0    # idle pools released for sizes waiting on memory
 
-    def pool_for(self, req: Request, plan: Plan) -> Pool:
-        if req.grid_key in self.pools:
-            return self.pools[req.grid_key]
+    def free_pool(self, key) -> tuple:
+        """A pool of grid size ``key`` with a free slot, and the slot (or (None, None))."""
+        for pool in self.pools:
+            if pool.key == key:
+                slot = pool.free_slot()
+                if slot is not None:
+                    return pool, slot
+        return None, None
+
+    def make_pool(self, req: Request, plan: Plan) -> Pool | None:
+        """Another pool of the request's grid size, as large as the free memory allows;
+        None when not one slot fits."""
         import torch
         from .batch import batch_device
         imp = req.case.implicit
         per = case_bytes(plan, req.case.flow.nvar, imp.krylov_subspace, imp.precision == "mixed")
         free, _ = torch.cuda.mem_get_info()
-        left = max(1, self.n_classes - len(self.pools))
-        slots = int(max(1, min(self.max_slots, self.memory_fraction * free / left // per)))
+        slots = self.admission.new_pool_slots(free, per, req.grid_key, {p.key for p in self.pools})
+        if slots < 1:
+            if not self.pools:   # nothing to wait for: the request can never be admitted
+                raise MemoryError(f"a request of grid size {req.grid_key} needs {per} bytes of device memory; "
+                                  f"{free} are free")
+            return None
         dev = batch_device([req.case] * slots, [plan] * slots)
         for k in range(slots):
             dev.enable(k, False)
         pool = Pool(req.grid_key, dev, slots, [None] * slots, [None] * slots, [0.0] * slots)
-        self.pools[req.grid_key] = pool
+        self.pools.append(pool)
+        self.made += 1
         return pool
+
+    def release(self, pool: Pool) -> None:
+        pool.dev.close()
+        self.pools.remove(pool)
+        self.released += 1
+
+    def slots_by_size(self) -> dict:
+        out: dict = {}
+        for p in self.pools:
+            out[p.key] = out.get(p.key, 0) + p.slots
+        return out
 
     def admit(self, pool: Pool, slot: int, req: Request, plan: Plan, now: float) -> None:
         c = req.case
@@ -204,7 +263,7 @@ class Server:
         def clock():
             return time.perf_counter() - t0
 
-        while pending or any(p.live for p in self.pools.values()):
+        while pending or any(p.live for p in self.pools):
             t = clock() if realtime else float("inf")
             for req in pending:
                 if req.arrival > t:
@@ -212,29 +271,37 @@ class Server:
                 if req.id not in grids:
                     grids[req.id] = workers.submit(build_grid, req.case)
             # admit, in arrival order, every arrived request whose grid is ready and that
-            # has a free slot of its size
+            # finds a free slot of its size, or memory for another pool of it
+            starved = set()
             for req in [r for r in pending if r.id in grids and grids[r.id].done()]:
                 plan = grids[req.id].result()
-                pool = self.pool_for(req, plan)
-                slot = pool.free_slot()
-                if slot is None:
+                pool, slot = self.free_pool(req.grid_key)
+                if pool is None and req.grid_key not in starved:
+                    pool = self.make_pool(req, plan)
+                    slot = pool.free_slot() if pool is not None else None
+                if pool is None:
+                    starved.add(req.grid_key)
                     continue
                 self.admit(pool, slot, req, plan, clock())
                 pending.remove(req)
                 del grids[req.id]
-            live = [p for p in self.pools.values() if p.live]
+            waiting = {r.grid_key for r in pending if r.arrival <= t}
+            for pool in self.admission.releasable(self.pools, starved, waiting):
+                hist_buf.pop(id(pool), None)
+                self.release(pool)
+            live = [p for p in self.pools if p.live]
             if not live:
                 time.sleep(0.01)
                 continue
             # one block of every live pool, each on its own stream: the pools overlap
             for p in live:
-                buf = hist_buf.get(p.key)
+                buf = hist_buf.get(id(p))
                 if buf is None:
-                    buf = hist_buf[p.key] = torch.empty((block, p.slots), dtype=torch.float64, device="cuda")
+                    buf = hist_buf[id(p)] = torch.empty((block, p.slots), dtype=torch.float64, device="cuda")
                 p.dev.newton_steps_async(block, buf)
             for p in live:
                 p.dev.sync()
-                hist = hist_buf[p.key].cpu().numpy()
+                hist = hist_buf[id(p)].cpu().numpy()
                 forces = np.atleast_2d(p.dev.forces())
                 finished_at = clock()
                 for k, req in enumerate(p.holder):
@@ -252,7 +319,7 @@ class Server:
         return sorted(done, key=lambda s: s.request.id)
 
     def close(self) -> None:
-        for p in self.pools.values():
+        for p in self.pools:
             p.dev.close()
         self.pools.clear()
 
@@ -293,9 +360,10 @@ def main(argv=None) -> int:
     wall = time.perf_counter() - t
     out = summary(served, wall)
     out.update({"rate_per_s": args.rate, "seed": args.seed, "precision": args.precision, "limiter": args.limiter,
-                "wall_s": wall, "slots": {f"{k[0]}x{k[1]}": p.slots for k, p in server.pools.items()},
+                "wall_s": wall, "slots": {f"{k[0]}x{k[1]}": n for k, n in server.slots_by_size().items()},
+                "pools_made": server.made, "pools_released": server.released,
                 "per_class": {f"{k[0]}x{k[1]}": summary([x for x in served if x.request.grid_key == k], wall)
-                              for k in server.pools}})
+                              for k in server.slots_by_size()}})
     server.close()
     if args.plain:
         seconds, dcl, dcd, rows = 0.0, [], [], []
