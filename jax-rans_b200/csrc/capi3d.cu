@@ -209,6 +209,20 @@ int jr_plan3d_create(const jr_plan3d_desc* d, jr_plan3d** out) {
     p->allocs.push_back(fb);
     dv.face_buf = static_cast<double*>(fb);
   }
+  if (d->mu_inf > 0.0) {   // viscous: the faces' gradient geometry and the node values
+    const size_t nf = (size_t)(d->NI + 1) * d->NJ * d->NK + (size_t)d->NI * (d->NJ + 1) * d->NK +
+                      (size_t)d->NI * d->NJ * (d->NK + 1);
+    const size_t nn = (size_t)(d->NI + 1) * (d->NJ + 1) * (d->NK + 1);
+    void *geo = nullptr, *nb = nullptr;
+    if (cudaMalloc(&geo, nf * 10 * sizeof(double)) != cudaSuccess ||
+        (p->allocs.push_back(geo), cudaMalloc(&nb, nn * 5 * sizeof(Dual))) != cudaSuccess) {
+      jr_plan3d_destroy(p);
+      return report_error(JR_ENOMEM, "cudaMalloc failed");
+    }
+    p->allocs.push_back(nb);
+    dv.face_geo = static_cast<const double*>(geo);
+    dv.node_buf = nb;
+  }
   const size_t work = (size_t)d->nvar * n * sizeof(Dual);
   if (cudaMalloc(&p->A, work) != cudaSuccess) {
     jr_plan3d_destroy(p);
@@ -237,6 +251,10 @@ int jr_plan3d_create(const jr_plan3d_desc* d, jr_plan3d** out) {
   if (cudaStreamCreateWithFlags(&p->st, cudaStreamNonBlocking) != cudaSuccess) {
     jr_plan3d_destroy(p);
     return report_error(JR_ECUDA, "stream");
+  }
+  if (dv.face_geo != nullptr) {
+    launch_face_geometry3(dv, const_cast<double*>(dv.face_geo), p->st);
+    cudaStreamSynchronize(p->st);
   }
   int rc = check3("jr_plan3d_create");
   if (rc) {

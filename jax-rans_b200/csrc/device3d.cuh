@@ -47,6 +47,10 @@ struct Plan3Dev {
   int line_coupled;            // the SA row coupled to the neighbours' mean flow (6x6 blocks)
   double* face_buf;            // the residual's face fluxes: nvar x (all three families' faces)
   void* ghost_buf;             // one ghost stage's values: nvar x (the largest stage's records), Dual-sized
+  const double* face_geo;      // viscous: per face (flat over the families) its diamond gradient's
+                               // geometry, 10 planes: the cross products c23, c31, c12 (3 each), det
+  void* node_buf;              // viscous: per node (NI+1)(NJ+1)(NK+1) the mean of its eight cells'
+                               // (u, v, w, T[, nu~]), 5 planes, Dual-sized
   const int* ch_cells;         // [chain * chain_L + k], -1 past the chain's end
   const int* ch_face;          // link k -> k+1: flat index into the three face families, concatenated
   const int* ch_sign;          // +1 / -1: the link face's vector points out of / into cell k; 0 none
@@ -236,6 +240,8 @@ void launch_residual3(const Plan3Dev& p, const double* U, double* R, void* A, bo
 void launch_jvp3(const Plan3Dev& p, const double* U, const double* v, double* Jv, void* A, cudaStream_t st);
 void launch_wave_speeds3(const Plan3Dev& p, const double* U, double* lam, cudaStream_t st);
 void launch_wall_loads3(const Plan3Dev& p, const double* U, double* loads, void* A, cudaStream_t st);
+// the viscous faces' diamond-gradient geometry into geo (10 x all faces), once per plan
+void launch_face_geometry3(const Plan3Dev& p, double* geo, cudaStream_t st);
 void launch_line_factor3(const Plan3Dev& p, const double* U, double cfl, void* F, cudaStream_t st);
 void launch_line_apply3(const Plan3Dev& p, const void* F, const double* r, double* z, cudaStream_t st);
 void launch_precondition3(const Plan3Dev& p, const double* U, double cfl, const double* r, double* z, void* F,

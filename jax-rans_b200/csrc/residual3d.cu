@@ -36,6 +36,35 @@ __global__ void k3_ghost_store(Plan3Dev p, const T* __restrict__ buf, int r0, in
 }
 
 // phase 1: every face's flux once (one thread per face of the three families)
+// the diamond gradients' geometry of every face (once per plan, viscous cases)
+__global__ void k3_face_geometry(Plan3Dev p, double* __restrict__ geo, int nf) {
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += gridDim.x * blockDim.x) {
+    int a, i, j, k;
+    face_of(p, f, a, i, j, k);
+    double g[10];
+    face_gradient_geometry(p, a, i, j, k, g);
+    for (int q = 0; q < 10; ++q) geo[(size_t)q * nf + f] = g[q];
+  }
+}
+
+// every node's mean of its eight cells' gradient variables, for the evaluation's canvas Q
+template <class T, int NPHI>
+__global__ void k3_node_phi(Plan3Dev p, const T* __restrict__ Q) {
+  const int nn = node_count(p);
+  T* nb = static_cast<T*>(p.node_buf);
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nn; e += gridDim.x * blockDim.x) {
+    const int I = e / ((p.NJ + 1) * (p.NK + 1)), J = (e / (p.NK + 1)) % (p.NJ + 1), K = e % (p.NK + 1);
+#pragma unroll
+    for (int m = 0; m < NPHI; ++m) nb[(size_t)m * nn + e] = node_phi_m(p, Q, I, J, K, m);
+  }
+}
+
+void launch_face_geometry3(const Plan3Dev& p, double* geo, cudaStream_t st) {
+  const int nf = face_count(p, 0) + face_count(p, 1) + face_count(p, 2);
+  counted3();
+  k3_face_geometry<<<(nf + 127) / 128, 128, 0, st>>>(p, geo, nf);
+}
+
 // (FO 1: the first-order flux, 2: second order; PART 0: the whole flux, 1: its inviscid
 // part, 2: its viscous part added to the stored inviscid part)
 template <class T, bool VISC, bool SA, int FO, int PART>
@@ -45,12 +74,17 @@ __global__ void __launch_bounds__(128) k3_face_flux(Plan3Dev p, const T* __restr
 }
 
 // A viscous flux in two launches (inviscid, then viscous added): each holds half the
-// live values of the whole, so neither spills the way the fused face did.
+// live values of the whole, so neither spills the way the fused face did.  The viscous
+// launch reads its diamond gradient's geometry from the plan (k3_face_geometry) and the
+// node values from this evaluation's node pass (k3_node_phi: each node once, not once
+// for each of the twelve faces round it).
 template <class T, bool VISC, bool SA, int FO>
 static void face_parts(const Plan3Dev& p, const T* A, int nf, cudaStream_t st) {
   const int fblocks = (nf + 127) / 128;
   if constexpr (VISC) {
-    counted3();
+    counted3(2);
+    const int nn = node_count(p);
+    k3_node_phi<T, SA ? 5 : 4><<<(nn + 127) / 128, 128, 0, st>>>(p, A);
     k3_face_flux<T, VISC, SA, FO, 1><<<fblocks, 128, 0, st>>>(p, A, nf);
     k3_face_flux<T, VISC, SA, FO, 2><<<fblocks, 128, 0, st>>>(p, A, nf);
   } else {

@@ -242,6 +242,82 @@ __host__ __device__ __forceinline__ void face_gradient(const Plan3Dev& p, const 
   }
 }
 
+// the geometry of face (fi, fj, fk)'s diamond gradient, face_gradient's own arithmetic:
+// out = c23 (3), c31 (3), c12 (3), det
+__host__ __device__ __forceinline__ void face_gradient_geometry(const Plan3Dev& p, int a, int fi, int fj, int fk,
+                                                                double out[10]) {
+  int lo[3] = {fi, fj, fk}, hi[3] = {fi, fj, fk};
+  lo[a] -= 1;
+  double xl[3], xh[3];
+  centre(p, lo[0], lo[1], lo[2], xl);
+  centre(p, hi[0], hi[1], hi[2], xh);
+  const int b1 = a == 0 ? 1 : 0, b2 = a == 2 ? 1 : 2;
+  int n00[3] = {fi, fj, fk}, n11[3] = {fi, fj, fk}, n10[3] = {fi, fj, fk}, n01[3] = {fi, fj, fk};
+  n11[b1] += 1;
+  n11[b2] += 1;
+  n10[b1] += 1;
+  n01[b2] += 1;
+  double x00[3], x11[3], x10[3], x01[3];
+  node_centre(p, n00[0], n00[1], n00[2], x00);
+  node_centre(p, n11[0], n11[1], n11[2], x11);
+  node_centre(p, n10[0], n10[1], n10[2], x10);
+  node_centre(p, n01[0], n01[1], n01[2], x01);
+  double d1[3], d2[3], d3[3];
+  for (int m = 0; m < 3; ++m) {
+    d1[m] = xh[m] - xl[m];
+    d2[m] = x11[m] - x00[m];
+    d3[m] = x01[m] - x10[m];
+  }
+  cross3(d2, d3, out);
+  cross3(d3, d1, out + 3);
+  cross3(d1, d2, out + 6);
+  out[9] = d1[0] * out[0] + d1[1] * out[1] + d1[2] * out[2];
+}
+
+__host__ __device__ __forceinline__ int node_flat(const Plan3Dev& p, int I, int J, int K) {
+  return (I * (p.NJ + 1) + J) * (p.NK + 1) + K;
+}
+__host__ __device__ __forceinline__ int node_count(const Plan3Dev& p) { return (p.NI + 1) * (p.NJ + 1) * (p.NK + 1); }
+
+// face_gradient from the plan's stored face geometry (p.face_geo) and this evaluation's
+// node values (p.node_buf, filled by k3_node_phi): the same values in the same arithmetic
+template <class T, int NPHI>
+__host__ __device__ __forceinline__ void face_gradient_stored(const Plan3Dev& p, const T* Q, int a, int fi, int fj,
+                                                              int fk, T grad[3][5]) {
+  int lo[3] = {fi, fj, fk};
+  lo[a] -= 1;
+  T pl[5], ph[5];
+  grad_vars(p, Q, cell_index(p, lo[0], lo[1], lo[2]), pl);
+  grad_vars(p, Q, cell_index(p, fi, fj, fk), ph);
+  const size_t nf = (size_t)face_count(p, 0) + face_count(p, 1) + face_count(p, 2);
+  const size_t f = (size_t)face_flat(p, a, fi, fj, fk);
+  double c23[3], c31[3], c12[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    c23[d] = p.face_geo[(size_t)d * nf + f];
+    c31[d] = p.face_geo[(size_t)(3 + d) * nf + f];
+    c12[d] = p.face_geo[(size_t)(6 + d) * nf + f];
+  }
+  const double det = p.face_geo[(size_t)9 * nf + f];
+  const int b1 = a == 0 ? 1 : 0, b2 = a == 2 ? 1 : 2;
+  int n11[3] = {fi, fj, fk}, n10[3] = {fi, fj, fk}, n01[3] = {fi, fj, fk};
+  n11[b1] += 1;
+  n11[b2] += 1;
+  n10[b1] += 1;
+  n01[b2] += 1;
+  const int i00 = node_flat(p, fi, fj, fk), i11 = node_flat(p, n11[0], n11[1], n11[2]);
+  const int i10 = node_flat(p, n10[0], n10[1], n10[2]), i01 = node_flat(p, n01[0], n01[1], n01[2]);
+  const T* nb = static_cast<const T*>(p.node_buf);
+  const size_t nn = (size_t)node_count(p);
+#pragma unroll
+  for (int m = 0; m < NPHI; ++m) {
+    const T f00 = nb[m * nn + i00], f11 = nb[m * nn + i11], f10 = nb[m * nn + i10], f01 = nb[m * nn + i01];
+    T p1 = ph[m] - pl[m], p2 = f11 - f00, p3 = f01 - f10;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) grad[d][m] = (p1 * c23[d] + p2 * c31[d] + p3 * c12[d]) / det;
+  }
+}
+
 template <class T>
 __host__ __device__ __forceinline__ void load_cell(const Plan3Dev& p, const T* Q, int c, T q[NV3_MAX]) {
   const int n = p.NI * p.NJ * p.NK;
@@ -346,7 +422,8 @@ __host__ __device__ void face_flux(const Plan3Dev& p, const T* Q, int a, int fi,
   }
   if constexpr (VISC && PART != 1) {
     T grad[3][5];
-    face_gradient<T, SA ? 5 : 4>(p, Q, a, fi, fj, fk, grad);
+    if constexpr (PART == 2) face_gradient_stored<T, SA ? 5 : 4>(p, Q, a, fi, fj, fk, grad);
+    else face_gradient<T, SA ? 5 : 4>(p, Q, a, fi, fj, fk, grad);
     // face means of the two cells either side
     T extra[3][3];
     T vel[3], Tl = g * qm[4] / qm[0], Th = g * qp[4] / qp[0];
