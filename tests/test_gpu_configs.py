@@ -121,3 +121,40 @@ def test_converged_forces_on_config_1_grid(cuda):
     assert abs(f.cl - ref["forces"][0]) < 1e-6
     assert abs(f.cd - ref["forces"][1]) < 1e-6
     assert abs(f.cm - ref["forces"][2]) < 1e-6
+
+
+@pytest.mark.parametrize("name", ["c_sa_385", "c_sa_513"])
+def test_every_line_schedule_on_config_grids(cuda, configs, name):
+    """Every line-solve schedule the autotuner may pick -- 64, 128 or 256 threads per chain
+    for the factor and for the solve, the solve's factor read from global memory or staged
+    from each level -- on the workloads' own chains (192 and 256 cells through the wake
+    cut): bitwise the same solve, within 1e-10 of the reference's (FP64); and the FP32
+    (mixed) solve bitwise the same under every schedule."""
+    from dataclasses import replace
+    from jaxrans_b200.native import DevicePlan, NativeError
+    z, case, plan, _ = configs(name)
+    U = config_state(z, plan, "sin")
+    ref = z["sin_prec_z"]
+    r = config_vector(plan, "sin", "r", ref.shape[0])
+    for precision in ("fp64", "mixed"):
+        dev = DevicePlan(plan, case.flow, case.numerics, replace(case.implicit, precision=precision))
+        outs = {}
+        try:
+            for f in (64, 128, 256):
+                for a in (64, 128, 256):
+                    for stage in range(5):
+                        try:
+                            dev.line_schedule(f, a, stage)
+                        except NativeError:
+                            continue   # a form that does not fit this plan's chains
+                        outs[(f, a, stage)] = dev.precondition(U, 25.0, r)
+        finally:
+            dev.close()
+        assert len(outs) >= 20
+        first = next(iter(outs.values()))
+        for key, out in outs.items():
+            assert np.array_equal(out, first), (precision, key)
+        if precision == "fp64":
+            assert rel(first, ref) < 1e-10
+        else:
+            assert rel(first, ref) < 1e-4
