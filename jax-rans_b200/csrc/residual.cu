@@ -44,6 +44,37 @@ __device__ __forceinline__ void load_prim(const Canvas& c, const Physics& P, int
   }
 }
 
+// the same with the case's variable count NV (== c.nvar) fixed at compile time, so the
+// cell's values stay in registers
+template <int NV, class T>
+__device__ __forceinline__ void load_prim_n(const Canvas& c, const Physics& P, int idx, const double* U,
+                                            const double* V, const double* qg, const double* dqg, T* q) {
+  const int N = c.ncanvas();
+  if (c.interior[idx]) {
+    T u[5];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      double x = U[v * N + idx];
+      if constexpr (sizeof(T) == sizeof(Dual)) {
+        u[v] = T{x, V[v * N + idx]};
+      } else {
+        u[v] = x;
+      }
+    }
+    to_prim(u, q, NV, P.gamma);
+  } else {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      double x = qg[v * N + idx];
+      if constexpr (sizeof(T) == sizeof(Dual)) {
+        q[v] = T{x, dqg[v * N + idx]};
+      } else {
+        q[v] = x;
+      }
+    }
+  }
+}
+
 // ------------------------------------------------------------------------------------
 // Ghost fill (src/jaxrans/numerics/boundary.py:257-267 and the stages of
 // src/jaxrans/mesh/atlas.py:331-367): one CTA per case; stage 1 (j sides), then
@@ -525,7 +556,7 @@ __global__ void __launch_bounds__(TILE_THREADS, TILE_MIN_BLOCKS)
     int i = i0 - 2 + li, j = j0 - 2 + lj;
     T q[5];
     if (i >= 0 && i < NI && j >= 0 && j < NJ) {
-      load_prim<T>(c, P, i * NJ + j, U, nullptr, qg, nullptr, q);
+      load_prim_n<NV, T>(c, P, i * NJ + j, U, nullptr, qg, nullptr, q);
     } else {
       for (int v = 0; v < NV; ++v) q[v] = cst<T>(1.0);
     }
@@ -736,7 +767,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 3) k_linearize(const CaseDev* __
     int i = i0 - 2 + li, j = j0 - 2 + lj;
     double q[5];
     if (i >= 0 && i < NI && j >= 0 && j < NJ) {
-      load_prim<double>(c, P, i * NJ + j, U, nullptr, qg, nullptr, q);
+      load_prim_n<NV, double>(c, P, i * NJ + j, U, nullptr, qg, nullptr, q);
     } else {
       for (int v = 0; v < NV; ++v) q[v] = 1.0;
     }
@@ -949,7 +980,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_jv(const CaseDev* __restrict__
         // the ghost's tangent from its source cell's, through the record's map; its
         // state from the ghost-filled canvas
         Dual qs[5];
-        load_prim<Dual>(c, P, ghost_source(c, rec), U, V, qg, dqg, qs);
+        load_prim_n<NV, Dual>(c, P, ghost_source(c, rec), U, V, qg, dqg, qs);
         const double* G = cd.gmap + (size_t)rec * NV * NV;
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
@@ -959,7 +990,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_jv(const CaseDev* __restrict__
           q[v] = Dual{qg[v * N + idx], d};
         }
       } else {
-        load_prim<Dual>(c, P, idx, U, V, qg, dqg, q);
+        load_prim_n<NV, Dual>(c, P, idx, U, V, qg, dqg, q);
       }
 #pragma unroll
       for (int v = 0; v < NV; ++v) t[v] = q[v].d;
