@@ -418,6 +418,8 @@ def measure_forms(fp64_value: float, fp64_forces, peaks: dict, served_requests: 
       batch (device clock), the cases' exit times (p50, p99), |dCL|, |dCD| of its 8 deg
       case against the FP64 line's forces, and the J.v and residual tiles' rooflines over
       the batch's 819k cells (each tile timed live with CUDA events on the batch);
+    * config 3's whole batch (``polar64_uneven``, 2.59M cells), mixed: the tiles' kernel
+      times and rooflines after one Newton step (the batch is not solved);
     * served: a seeded Poisson stream (20 requests/s) of ``served_requests`` SA requests of
       the config-4 distribution (van Albada), mixed, continuous batching with up to
       ``served_requests`` slots per grid size; solves/hr over the stream's wall time,
@@ -469,6 +471,24 @@ def measure_forms(fp64_value: float, fp64_forces, peaks: dict, served_requests: 
         "kernel_ms": kern,
         "roofline": roofline_of(kern, "sa", 5, batch_cells, peaks, fp32_faces=True),
         "roofline_residual": roofline_of(kern, "sa", 5, batch_cells, peaks, kernel="residual_tile")}
+    # config 3's whole batch (64 angles and the three uneven grids, 2.59M cells), mixed: the
+    # tiles' rooflines at that size, after one Newton step from the freestream
+    cases = batch_workload("polar64_uneven", **{"implicit.precision": "mixed"})
+    made, grids = {}, []
+    for (w, _), c in zip(BATCHES["polar64_uneven"], cases):
+        if w not in made:
+            made[w] = c.grid()
+        grids.append(made[w])
+    dev = batch_device(cases, grids, autotune=True)
+    start_batch(dev, cases, grids)
+    dev.newton_steps(1)
+    kern = dev.time_kernels(5)
+    dev.close()
+    cells3 = sum(g.cells for g in grids)
+    out["config3_batch_kernels"] = {
+        "workload": "polar64_uneven", "cases": len(cases), "cells": cells3, "precision": "mixed",
+        "kernel_ms": kern, "roofline": roofline_of(kern, "sa", 5, cells3, peaks, fp32_faces=True),
+        "roofline_residual": roofline_of(kern, "sa", 5, cells3, peaks, kernel="residual_tile")}
     # served, mixed, continuous batching
     template = workload("c_sa_385", **{"implicit.precision": "mixed", "convective_fluxes.limiter": "van_albada"})
     requests = poisson_requests(served_requests, template, 20.0, seed=0)
