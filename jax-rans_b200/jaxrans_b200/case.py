@@ -3,7 +3,7 @@
 The keys, types, defaults and cross-key rules are those of the reference's schema and
 loader (``src/jaxrans/case/schema.py:67-216``, ``src/jaxrans/case/loader.py:79-373``),
 so a case directory written for the reference loads here unchanged.  Unknown keys are
-errors naming the key; options this build does not implement (CGNS and multi-element
+errors naming the key; options jaxrans_b200 does not implement (CGNS and multi-element
 grids, blunt trailing edges, swept wings, the explicit solver) are refused by name.
 """
 
@@ -103,7 +103,7 @@ CASE = {
         Key("reference_area", "number|null", None),
         Key("moment_centre", "list", [0.25, 0.0, 0.0]),
         Key("section", "string", "streamwise", choices=("normal", "streamwise")),
-        # this build's own key: the normal-step growth (null: solved to reach the far field)
+        # a key of jaxrans_b200's own: the normal-step growth (null: solved to reach the far field)
         Key("normal_stretching", "number|null", None, grids=GENERATED),
     ),
     "freestream": (Key("mach", "number", REQUIRED), Key("alpha_deg", "number", 0.0),
@@ -134,7 +134,7 @@ NUMERICAL = {
                  Key("krylov_restarts", "integer", _I.krylov_restarts),
                  Key("krylov_success", "number", _I.krylov_success),
                  Key("max_relative_update", "number|null", _I.max_relative_update),
-                 # this build's own key: the plain FP64 path or the mixed form
+                 # a key of jaxrans_b200's own: the plain FP64 path or the mixed form
                  Key("precision", "string", _I.precision, choices=("fp64", "mixed"))),
     "convergence": (Key("max_iters", "integer", _N.max_iters), Key("tol", "number", _N.tol),
                     Key("forces_tol", "number|null", _N.forces_tol), Key("grid_sequencing", "integer", 0),
@@ -181,14 +181,14 @@ class GridSpec:
 
     def build(self, base: Path) -> list[Block]:
         if self.grid not in BUILT_GRIDS:
-            raise CaseError(f"'domain.grid' = {self.grid!r} is not implemented in this build; "
+            raise CaseError(f"'domain.grid' = {self.grid!r} is not implemented in jaxrans_b200; "
                             f"choose from {sorted(BUILT_GRIDS)}")
         if self.grid == "file":
             from .gridfile import PatchRule, load_grid, read_plot3d_2d
             from .gridfile3d import is_3d, load_grid3d
             path = self.resolve(base)
             if self.format == "cgns" or path.suffix.lower() == ".cgns":
-                raise CaseError("a CGNS grid file is not implemented in this build; use Plot3D")
+                raise CaseError("a CGNS grid file is not implemented in jaxrans_b200; use Plot3D")
             try:
                 rules = tuple(PatchRule(**rule) for rule in self.patches)
             except TypeError as error:
@@ -206,7 +206,7 @@ class GridSpec:
                 raise CaseError(str(error)) from None
         section = section_source(self.airfoil, base).normalised()
         if self.trailing_edge == "close" and not section.sharp:
-            raise CaseError("'domain.trailing_edge' = 'close' on a blunt section is not implemented in this build")
+            raise CaseError("'domain.trailing_edge' = 'close' on a blunt section is not implemented in jaxrans_b200")
         if self.grid == "o_grid":
             return [o_grid(section, self.cells_airfoil, self.cells_normal, self.wall_spacing, self.far_field,
                            self.normal_stretching)]
@@ -327,7 +327,7 @@ def _domain_problems(written: dict, domain: dict):
         if kind in key.required_for and domain[name] is None:
             yield f"'domain.{name}' is required for grid {kind!r}"
     if kind not in BUILT_GRIDS:
-        yield f"'domain.grid' = {kind!r} is not implemented in this build; choose from {sorted(BUILT_GRIDS)}"
+        yield f"'domain.grid' = {kind!r} is not implemented in jaxrans_b200; choose from {sorted(BUILT_GRIDS)}"
 
 
 def _flow_problems(written_material: dict, written_turbulence: dict, freestream: dict, material: dict,
@@ -351,7 +351,7 @@ def _flow_problems(written_material: dict, written_turbulence: dict, freestream:
     if turbulence["model"] == "none" and "freestream_nu_tilde_ratio" in written_turbulence:
         yield "'turbulence.freestream_nu_tilde_ratio' given without a model"
     if freestream["sweep_deg"] is not None:
-        yield "'freestream.sweep_deg' (an infinite swept wing) is not implemented in this build"
+        yield "'freestream.sweep_deg' (an infinite swept wing) is not implemented in jaxrans_b200"
 
 
 def _patch_problems(where: str, entry, inviscid: bool):
@@ -457,16 +457,16 @@ def resolve_conditions(named: dict, grid_patches: list, flow: FlowConditions) ->
     return {p: named.get(p, defaults.get(p)) for p in grid_patches}
 
 
-# what this build refuses among the options the schema accepts: (file section, key, accepted
+# what jaxrans_b200 refuses among the options the schema accepts: (file section, key, accepted
 # value, message)
 _NOT_BUILT = (
     ("time_integration", "solver", "implicit",
-     "'time_integration.solver' = 'explicit' (multistage Runge-Kutta) is not implemented in this build; set it "
+     "'time_integration.solver' = 'explicit' (multistage Runge-Kutta) is not implemented in jaxrans_b200; set it "
      "to 'implicit'"),
     ("implicit", "jacobian", "first_order",
-     "'implicit.jacobian' = 'exact' is not implemented in this build; use 'first_order'"),
+     "'implicit.jacobian' = 'exact' is not implemented in jaxrans_b200; use 'first_order'"),
     ("convergence", "grid_sequencing", 0,
-     "'convergence.grid_sequencing' other than 0 is not implemented in this build"),
+     "'convergence.grid_sequencing' other than 0 is not implemented in jaxrans_b200"),
 )
 
 

@@ -47,7 +47,7 @@ class FlowConditions:
         if not self.mach > 0.0:
             raise ValueError(f"mach must be positive, got {self.mach}")
         if self.sweep_deg is not None:
-            raise ValueError("sweep_deg (an infinite swept wing, 2.5D) is not implemented in this build")
+            raise ValueError("sweep_deg (an infinite swept wing, 2.5D) is not implemented in jaxrans_b200")
         if self.mach >= 1.0:
             raise ValueError(f"freestream mach must be subsonic for the characteristic far-field BC, "
                              f"got {self.mach}")
@@ -119,7 +119,7 @@ class NumericsConfig:
         if self.forces_tol is not None and not self.forces_tol > 0.0:
             raise ValueError(f"forces_tol must be positive or null, got {self.forces_tol}")
         if self.n_ghost != 2:
-            raise ValueError(f"n_ghost must be 2 in this build (the MUSCL stencil), got {self.n_ghost}")
+            raise ValueError(f"n_ghost must be 2 in jaxrans_b200 (the MUSCL stencil), got {self.n_ghost}")
         if not -1.0 <= self.kappa <= 1.0:
             raise ValueError(f"muscl_kappa must lie in [-1, 1], got {self.kappa}")
         if self.kappa != 0.0 and self.limiter != "none":

@@ -12,7 +12,7 @@ and registers three CUDA targets:
 
 The plan is a ``native.DevicePlan`` made by the caller and kept alive while the calls
 may run; its handle travels as an int64 attribute.  XLA owns the buffers and the stream.
-JAX is not installed where this build is made and tested, so these functions are
+JAX is not installed where this package is built and tested, so these functions are
 untested; without JAX ``register()`` raises ``ImportError``.
 """
 

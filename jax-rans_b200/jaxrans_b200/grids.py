@@ -278,7 +278,7 @@ def o_grid(section: Section, cells_airfoil: int, cells_normal: int, wall_spacing
     surface first), ``j`` outward; wall on ``j_min``, far field on ``j_max``, the
     seam ``i_min`` <-> ``i_max``."""
     if not section.sharp:
-        raise ValueError("o_grid: a blunt trailing edge is not implemented in this build; "
+        raise ValueError("o_grid: a blunt trailing edge is not implemented in jaxrans_b200; "
                          "use a sharp NACA section (domain.trailing_edge = \"close\")")
     c = section.chord
     x, y = section.at(wall_arcs(section, cells_airfoil))
@@ -301,7 +301,7 @@ def c_grid(section: Section, cells_airfoil: int, cells_wake: int, cells_normal: 
     round the airfoil (lower surface first) and out along the upper wake; the
     wake cut is ``j_min`` against itself, reversed."""
     if not section.sharp:
-        raise ValueError("c_grid: a blunt trailing edge is not implemented in this build; "
+        raise ValueError("c_grid: a blunt trailing edge is not implemented in jaxrans_b200; "
                          "close it (domain.trailing_edge = \"close\")")
     c = section.chord
     x, y = section.at(wall_arcs(section, cells_airfoil))

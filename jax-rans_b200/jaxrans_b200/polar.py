@@ -72,7 +72,7 @@ def run_polar(case: Case, alphas, grid: Plan | None = None, devices: int | None 
     """``case`` at every angle of ``alphas`` (degrees) at once on one GPU;
     ``progress(iteration, CL per angle)`` per block (``src/jaxrans/polar.py:80-121``)."""
     if devices is not None and devices > 1:
-        raise ValueError("a polar runs on one GPU in this build (run one polar per GPU)")
+        raise ValueError("a polar runs on one GPU in jaxrans_b200 (run one polar per GPU)")
     grid = case.grid() if grid is None else grid
     alphas = np.asarray(alphas, dtype=float)
     cases = [at_alpha(case, a) for a in alphas]

@@ -72,7 +72,7 @@ def make_residual(grid: Plan, flow: FlowConditions, numerics: NumericsConfig, fi
     parameters of a sensitivity in the reference) are not supported: the flow's own
     are used, and a value passed is refused."""
     if freestream is not None or mu_inf is not None:
-        raise ValueError("freestream / mu_inf overrides are not implemented in this build; set them in flow")
+        raise ValueError("freestream / mu_inf overrides are not implemented in jaxrans_b200; set them in flow")
     if distance is not None:
         grid.distance = np.asarray(distance, dtype=np.float64)
     if getattr(grid, "dim", 2) == 3:

@@ -355,9 +355,9 @@ def run(case: Case, grid: Plan | None = None, progress=None, on_level=None, devi
     """March ``case`` to steady state on ``grid`` (default ``case.grid()``; a 3D grid
     file gives a 3D plan, marched by ``solver3d.march3d``) on one GPU
     (``src/jaxrans/simulation.py:213-240``).  ``devices`` (slabs over several GPUs) is
-    not part of this build."""
+    not part of jaxrans_b200."""
     if devices is not None and len(devices) > 1:
-        raise ValueError("splitting one case over several devices is not implemented in this build")
+        raise ValueError("splitting one case over several devices is not implemented in jaxrans_b200")
     plan = case.grid() if grid is None else grid
     if on_level is not None:
         on_level(0, plan)

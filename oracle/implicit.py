@@ -248,7 +248,7 @@ def chain_coupling_sa(U, model):
     neighbour's state, ``[-nu_hat vn, nu_hat Sx, nu_hat Sy, 0]``, with the link's face
     vector and sign exactly as the mean-flow blocks use them (``chain_blocks_flow``).
     The mean-flow rows do not depend on rho nu_hat, so the 5x5 blocks are block lower
-    triangular.  This coupled form is this build's 5x5 variant of ``line_j``; the
+    triangular.  This coupled form is jaxrans_b200's 5x5 variant of ``line_j``; the
     reference has only the split form (``preconditioners.py:291-306``)."""
     plan, g = model.plan, model.gamma
     ch = plan.chains

@@ -5,7 +5,7 @@ Each entry mutates a valid pair of documents (a C-grid SA case) in one way -- an
 section or key, a wrong type, an option not in the schema, a cross-key rule broken, a bad
 boundary condition, a malformed override -- and records the ``CaseError`` message the
 reference's own ``parse_case`` / ``apply_override`` raise (under the NumPy stand-in for
-JAX in ``tests/golden/jaxshim``).  ``tests/test_case_errors.py`` checks that this build's
+JAX in ``tests/golden/jaxshim``).  ``tests/test_case_errors.py`` checks that jaxrans_b200's
 loader raises the same messages.
 
     JAXRANS_REFERENCE=<reference checkout> python tests/golden/make_golden_case_errors.py

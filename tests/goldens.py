@@ -1,5 +1,5 @@
 """Loading the golden fixtures (made by ``tests/golden/make_golden.py`` from the
-reference itself) into this build's plan and configs, and the oracle's model."""
+reference itself) into jaxrans_b200's plan and configs, and the oracle's model."""
 
 from __future__ import annotations
 

@@ -1,7 +1,7 @@
 """The loader's error behaviour against the reference's: every malformed document of
 tests/golden/case_errors.json (made by make_golden_case_errors.py from the reference's
 own loader) raises a ``CaseError`` with the reference's message.  The one difference
-allowed: lists of allowed keys or choices also name this build's additions (the domain key
+allowed: lists of allowed keys or choices also name jaxrans_b200's additions (the domain key
 ``normal_stretching``, the preconditioner ``line_j_coupled``)."""
 
 from __future__ import annotations

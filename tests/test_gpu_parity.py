@@ -149,7 +149,7 @@ def test_wall_loads_match_oracle(cuda, name):
 
 @pytest.mark.parametrize("name", ["c_sa", "o_sa_qcr"])
 def test_coupled_line_preconditioner_matches_oracle(cuda, name):
-    """The coupled (5x5) line blocks -- this build's 5x5 form; the reference has the split
+    """The coupled (5x5) line blocks -- jaxrans_b200's 5x5 form; the reference has the split
     form only -- against the oracle's coupled solve (itself checked against dense block
     solves), 1e-10 as the split solve."""
     from oracle import implicit as im
