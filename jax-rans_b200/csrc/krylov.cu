@@ -39,17 +39,15 @@ __device__ void reduce_rows(const double* partial, int stride, int W, int nb, do
   const int t = threadIdx.x, k = t % W, r = t / W;
   if (r < R) {
     double acc = MAX ? -INFINITY : 0.0;
-    int b = r;
-    for (; b + 7 * R < nb; b += 8 * R) {
+    // rows r, r + R, ... in order, eight loads in flight at a time (the last eight
+    // predicated, so the tail costs one round trip, not one per row)
+    for (int b = r; b < nb; b += 8 * R) {
       double x[8];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) x[u] = __ldcg(partial + (size_t)(b + u * R) * stride + k);
+      for (int u = 0; u < 8; ++u) x[u] = b + u * R < nb ? __ldcg(partial + (size_t)(b + u * R) * stride + k) : 0.0;
 #pragma unroll
-      for (int u = 0; u < 8; ++u) acc = MAX ? nmax(acc, x[u]) : acc + x[u];
-    }
-    for (; b < nb; b += R) {
-      const double x = __ldcg(partial + (size_t)b * stride + k);
-      acc = MAX ? nmax(acc, x) : acc + x;
+      for (int u = 0; u < 8; ++u)
+        if (b + u * R < nb) acc = MAX ? nmax(acc, x[u]) : acc + x[u];
     }
     group[t] = acc;
   }
