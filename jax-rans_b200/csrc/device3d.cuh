@@ -141,7 +141,9 @@ template <class T> __host__ __device__ __forceinline__ void hllc3(const T* qL, c
     normal_flux3(qR, n, g, f);
   } else {
     const bool left = val(sm) >= 0.0;
-    const T* q = left ? qL : qR;
+    T q[5];   // the star side's state, selected by value (a selected pointer would put both in local memory)
+#pragma unroll
+    for (int k = 0; k < 5; ++k) q[k] = left ? qL[k] : qR[k];
     T sk = left ? sl : sr;
     T vn = left ? vnl : vnr;
     T wide = left ? dmin(sl - sm, -1e-300) : dmax(sr - sm, 1e-300);

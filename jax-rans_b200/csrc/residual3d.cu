@@ -17,10 +17,19 @@
 
 namespace jr {
 
-template <class T>
+template <class T, int NV>
 __global__ void k3_prim(Plan3Dev p, const double* __restrict__ U, const double* __restrict__ dU, T* __restrict__ Q) {
   const int n = p.NI * p.NJ * p.NK;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) prim_cell(p, U, dU, Q, c);
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+    prim_cell_n<NV>(p, U, dU, Q, c);
+}
+
+// the primitive canvas of U (and dU) into Q
+template <class T>
+static void prim_canvas(const Plan3Dev& p, const double* U, const double* dU, T* Q, cudaStream_t st) {
+  const int blocks = (p.NI * p.NJ * p.NK + 127) / 128;
+  if (p.nvar > 5) k3_prim<T, 6><<<blocks, 128, 0, st>>>(p, U, dU, Q);
+  else k3_prim<T, 5><<<blocks, 128, 0, st>>>(p, U, dU, Q);
 }
 
 template <class T>
@@ -129,7 +138,7 @@ static void residual3_t(const Plan3Dev& p, const double* U, const double* dU, do
   const int n = p.NI * p.NJ * p.NK;
   const int blocks = (n + 127) / 128;
   counted3(2);   // the primitive canvas and, below, the residual
-  k3_prim<T><<<blocks, 128, 0, st>>>(p, U, dU, A);
+  prim_canvas<T>(p, U, dU, A, st);
   fill3(p, A, st);
   const bool visc = p.P.mu_inf > 0.0, sa = p.nvar > 5;
   const int nf = face_count(p, 0) + face_count(p, 1) + face_count(p, 2);
@@ -155,7 +164,7 @@ __global__ void k3_wall_loads(Plan3Dev p, const double* __restrict__ Q, double* 
 void launch_wall_loads3(const Plan3Dev& p, const double* U, double* loads, void* A, cudaStream_t st) {
   const int n = p.NI * p.NJ * p.NK;
   counted3(p.n_walls > 0 ? 2 : 1);
-  k3_prim<double><<<(n + 127) / 128, 128, 0, st>>>(p, U, nullptr, (double*)A);
+  prim_canvas<double>(p, U, nullptr, (double*)A, st);
   fill3(p, (double*)A, st);
   if (p.n_walls > 0) k3_wall_loads<<<(p.n_walls + 127) / 128, 128, 0, st>>>(p, (const double*)A, loads);
 }

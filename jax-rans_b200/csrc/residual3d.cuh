@@ -18,6 +18,19 @@ __host__ __device__ __forceinline__ void prim_cell(const Plan3Dev& p, const doub
   for (int v = 0; v < p.nvar; ++v) Q[(size_t)v * n + c] = q[v];
 }
 
+// the same with the plan's variable count NV (== p.nvar) fixed at compile time
+template <int NV, class T>
+__host__ __device__ __forceinline__ void prim_cell_n(const Plan3Dev& p, const double* U, const double* dU, T* Q,
+                                                     int c) {
+  const int n = p.NI * p.NJ * p.NK;
+  T u[NV3_MAX], q[NV3_MAX];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) u[v] = mk<T>(U[(size_t)v * n + c], dU ? dU[(size_t)v * n + c] : 0.0);
+  to_prim3(u, q, NV, p.P.gamma);
+#pragma unroll
+  for (int v = 0; v < NV; ++v) Q[(size_t)v * n + c] = q[v];
+}
+
 // ghost record r of a stage: out[ghost] = condition(in[source]) (or a copy across a cut)
 template <class T>
 __host__ __device__ __forceinline__ void ghost_record(const Plan3Dev& p, const T* in, T* out, int r) {
@@ -284,10 +297,10 @@ __host__ __device__ __forceinline__ int node_count(const Plan3Dev& p) { return (
 template <class T, int NPHI>
 __host__ __device__ __forceinline__ void face_gradient_stored(const Plan3Dev& p, const T* Q, int a, int fi, int fj,
                                                               int fk, T grad[3][5]) {
-  int lo[3] = {fi, fj, fk};
-  lo[a] -= 1;
+  // (shifts by selects, not by indexing small arrays with the family: those would live in
+  // local memory)
   T pl[5], ph[5];
-  grad_vars(p, Q, cell_index(p, lo[0], lo[1], lo[2]), pl);
+  grad_vars(p, Q, cell_index(p, fi - (a == 0), fj - (a == 1), fk - (a == 2)), pl);
   grad_vars(p, Q, cell_index(p, fi, fj, fk), ph);
   const size_t nf = (size_t)face_count(p, 0) + face_count(p, 1) + face_count(p, 2);
   const size_t f = (size_t)face_flat(p, a, fi, fj, fk);
@@ -300,13 +313,12 @@ __host__ __device__ __forceinline__ void face_gradient_stored(const Plan3Dev& p,
   }
   const double det = p.face_geo[(size_t)9 * nf + f];
   const int b1 = a == 0 ? 1 : 0, b2 = a == 2 ? 1 : 2;
-  int n11[3] = {fi, fj, fk}, n10[3] = {fi, fj, fk}, n01[3] = {fi, fj, fk};
-  n11[b1] += 1;
-  n11[b2] += 1;
-  n10[b1] += 1;
-  n01[b2] += 1;
-  const int i00 = node_flat(p, fi, fj, fk), i11 = node_flat(p, n11[0], n11[1], n11[2]);
-  const int i10 = node_flat(p, n10[0], n10[1], n10[2]), i01 = node_flat(p, n01[0], n01[1], n01[2]);
+  // node (fi, fj, fk) shifted by s1 along axis b1 and s2 along axis b2
+  auto node_at = [&](int s1, int s2) {
+    return node_flat(p, fi + (b1 == 0) * s1 + (b2 == 0) * s2, fj + (b1 == 1) * s1 + (b2 == 1) * s2,
+                     fk + (b1 == 2) * s1 + (b2 == 2) * s2);
+  };
+  const int i00 = node_at(0, 0), i11 = node_at(1, 1), i10 = node_at(1, 0), i01 = node_at(0, 1);
   const T* nb = static_cast<const T*>(p.node_buf);
   const size_t nn = (size_t)node_count(p);
 #pragma unroll
@@ -376,11 +388,8 @@ __host__ __device__ void face_flux(const Plan3Dev& p, const T* Q, int a, int fi,
   const double g = P.gamma;
   int idx[4];
 #pragma unroll
-  for (int o = 0; o < 4; ++o) {
-    int c[3] = {fi, fj, fk};
-    c[a] += o - 2;
-    idx[o] = cell_index(p, c[0], c[1], c[2]);
-  }
+  for (int o = 0; o < 4; ++o)
+    idx[o] = cell_index(p, fi + (a == 0) * (o - 2), fj + (a == 1) * (o - 2), fk + (a == 2) * (o - 2));
   T qmm[NV3_MAX], qm[NV3_MAX], qp[NV3_MAX], qpp[NV3_MAX];
   load_cell_n<NV>(p, Q, idx[1], qm);
   load_cell_n<NV>(p, Q, idx[2], qp);
@@ -444,8 +453,10 @@ __host__ __device__ void face_flux(const Plan3Dev& p, const T* Q, int a, int fi,
     T div = grad[0][0] + grad[1][1] + grad[2][2];
     T ttd = (2.0 / 3.0) * div;
     T force[3];
+#pragma unroll
     for (int c = 0; c < 3; ++c) {
       T tau[3];
+#pragma unroll
       for (int d = 0; d < 3; ++d) {
         if (c == d) {
           tau[d] = mu * (2.0 * grad[c][c] - ttd);
