@@ -204,7 +204,9 @@ __host__ __device__ __forceinline__ void hllc_flux(const T* qL, const T* qR, dou
   } else {
     // star flux of one side of the contact: F_K + S_K (U*_K - U_K)
     const bool left = val(sm) >= 0.0;
-    const T* q = left ? qL : qR;
+    T q[4];   // the star side's state, selected by value (a selected pointer would put both in local memory)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) q[k] = left ? qL[k] : qR[k];
     T sk = left ? sl : sr;
     T vn = left ? vnl : vnr;
     T wide = left ? dmin(sl - sm, -1e-300) : dmax(sr - sm, 1e-300);
