@@ -303,6 +303,32 @@ static int build_case(jr_plan* plan, const jr_plan_desc* d, CaseDev& cd, size_t&
   return JR_OK;
 }
 
+// The line solve reads its chains' factor once per Arnoldi step, and inside the step the
+// linearisation and the Krylov basis evict it from L2 between reads.  Where the whole flow
+// factor fits the device's persisting-L2 maximum (one case or a small batch), the Krylov
+// cycles' capture stream gets an access-policy window over it, so its lines persist (the
+// context's persisting size is raised to cover it, never lowered); larger factors are left
+// to the normal policy, which measured as well or better for them.  A cache policy only:
+// results are bitwise the same.
+static void keep_factor_in_l2(cudaStream_t st, void* factor, size_t bytes) {
+  int dev = 0, max_persist = 0, max_window = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev);
+  cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev);
+  if (bytes == 0 || bytes > (size_t)max_persist || bytes > (size_t)max_window) return;
+  size_t now = 0;
+  if (cudaDeviceGetLimit(&now, cudaLimitPersistingL2CacheSize) == cudaSuccess && now < bytes)
+    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, bytes);
+  cudaStreamAttrValue a{};
+  a.accessPolicyWindow.base_ptr = factor;
+  a.accessPolicyWindow.num_bytes = bytes;
+  a.accessPolicyWindow.hitRatio = 1.0f;
+  a.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+  a.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+  cudaStreamSetAttribute(st, cudaStreamAttributeAccessPolicyWindow, &a);
+  cudaGetLastError();   // a device without persisting L2 refuses quietly: the normal policy stays
+}
+
 // Work buffers: each kind is one allocation holding every case's part back to back.
 static int build_buffers(jr_plan* p, const std::vector<size_t>& factor_rows) {
   const int nc = p->n_cases;
@@ -406,6 +432,7 @@ static int build_buffers(jr_plan* p, const std::vector<size_t>& factor_rows) {
   TRY(dev_alloc(p, (void**)&p->cycles, sizeof(unsigned long long)));
   if (cudaStreamCreateWithFlags(&p->body_st, cudaStreamNonBlocking) != cudaSuccess)
     return fail(JR_ECUDA, "cudaStreamCreate failed");
+  keep_factor_in_l2(p->body_st, fflow, fb * 80 * tb);
   if (cudaMemcpy(p->cases, p->host.data(), (size_t)nc * sizeof(CaseDev), cudaMemcpyHostToDevice) != cudaSuccess)
     return cuda_check("case table");
   return JR_OK;
