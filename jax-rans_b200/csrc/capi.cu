@@ -307,7 +307,8 @@ static int build_case(jr_plan* plan, const jr_plan_desc* d, CaseDev& cd, size_t&
 // linearisation and the Krylov basis evict it from L2 between reads.  Where the whole flow
 // factor fits the device's persisting-L2 maximum (one case or a small batch), the Krylov
 // cycles' capture stream gets an access-policy window over it, so its lines persist (the
-// context's persisting size is raised to cover it, never lowered); larger factors are left
+// context's persisting size -- a limit of this process's context, gone with it -- is raised
+// to cover it, never lowered); larger factors are left
 // to the normal policy, which measured as well or better for them.  A cache policy only:
 // results are bitwise the same.
 static void keep_factor_in_l2(cudaStream_t st, void* factor, size_t bytes) {
