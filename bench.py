@@ -50,7 +50,7 @@ METRIC = "converged RANS solves/hr"
 # Newton steps of one converged solve of each workload from the freestream (FP64): the
 # device path's own count (the bench line's config.newton_steps_per_solve, which it
 # measures every run); the CPU samples, a few Newton steps each, are scaled by it.
-STEPS_PER_SOLVE = {"c_sa_385": 640, "o_euler_257": 3840}
+STEPS_PER_SOLVE = {"c_sa_385": 680, "o_euler_257": 3840}
 # coefficients of the linearisation the J.v tile reads per face and per cell (the
 # kernel's JacShape and JCELL): inviscid 4 x 4 per side, the SA convection's 3, the
 # viscous tail's derivatives its dependences allow (19 laminar, 33 SA)
@@ -702,7 +702,10 @@ def run_device(args) -> int:
         if world == 1 and not args.no_cpu_baseline:
             from jaxrans_b200.workloads import BATCHES
             name = BATCHES[args.workload][0][0] if args.workload in BATCHES else args.workload
-            cpu = cpu_rate(name, args.steps, args.warmup, args.precision, STEPS_PER_SOLVE[name])
+            # scaled by this run's own Newton steps per solve (the reference arm, a separate
+            # process, uses STEPS_PER_SOLVE, this count as last measured)
+            per_solve = int(np.median(iters)) if n_cases == 1 else STEPS_PER_SOLVE[name]
+            cpu = cpu_rate(name, args.steps, args.warmup, args.precision, per_solve)
             cpu.pop("seconds_per_step")
             result["cpu_baseline"] = cpu
         print(json.dumps(result), flush=True)
